@@ -1,0 +1,337 @@
+"""Benchmark of the hot path: the 60M-row selective scan + scalar int128 sum.
+
+Workload (one step): WHERE ship_day in a 365-day window AND discount_pct
+BETWEEN 5 AND 7 AND quantity < 24 → sum(price_cents * discount_pct) as exact
+int128, plus count, over 60M seeded synthetic rows (TPC-H Q6 shape; the data
+set itself is not available, so seeded columns with its distributions stand in).
+
+* ``value``  — rows/s with the table resident in HBM (K calls of tgp_execute,
+  CUDA events on the library's stream, max over ranks).
+* ``e2e``    — rows/s through the C ABI from pinned HOST buffers: every step
+  copies the four columns host→device (tgp_table_reload) and reads the result
+  back (tgp_execute).
+* ``roofline`` — the scan kernel's algorithmic bytes (20 B/row) per launch ÷
+  its CUDA-event duration, against the measured HBM copy bandwidth.
+* ``cpu_baseline`` — the C++ restatement of the reference's CPU path on this
+  host's cores, on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU restatement alone (rank 0) and prints its
+own line. Under torchrun, each rank scans its own 60M-row shard (weak
+scaling); per-step partial sums are merged with an NCCL all-gather.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ROWS = 60_000_000
+BYTES_PER_ROW = 20  # ship_day 4 + discount_pct 4 + quantity 4 + price_cents 8
+METRIC = "rows/s & HBM GB/s vs 8 TB/s; batched QPS at p99 vs plain per-query launch"
+SCAN_COLUMNS = ("ship_day", "discount_pct", "quantity", "price_cents")
+L2_NOTE = "inputs 1.2 GB per rank > 126 MB L2 (no flush needed)"
+
+
+def peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch() -> float | None:
+    """DRAM bytes per scan launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "selective_scan_sum_60M_scan_kernel.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t: threading.Thread | None = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def gen_scan_table(rows: int, seed: int) -> dict[str, np.ndarray]:
+    from turbogp_b200 import datagen
+    full = datagen.lineitem(0, seed)  # column names / dtypes
+    out = {}
+    for name in SCAN_COLUMNS:
+        rng = datagen._rng(seed, name)
+        lo_hi = {"quantity": (1, 51), "price_cents": (90_000, 10_500_001), "discount_pct": (0, 11),
+                 "ship_day": (datagen.DAY0, datagen.DAY0 + datagen.NDAYS)}[name]
+        out[name] = rng.integers(lo_hi[0], lo_hi[1], rows, dtype=full[name].dtype)
+    return out
+
+
+def cpu_baseline(cols: dict, tpl, sample_rows: int, threads: int | None) -> dict:
+    """The reference-path restatement on a bounded sample (rows/s)."""
+    import oracle
+    from oracle import refpath
+    sample = {k: v[:sample_rows] for k, v in cols.items()}
+    res = refpath.selective_scan_sum(sample, tpl, threads=threads)
+    return res
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def run_reference(args, world: int, rank: int) -> None:
+    if rank != 0:
+        return
+    from turbogp_b200 import workloads
+    tpl = workloads.selective_scan_sum()
+    rows = args.reference_rows
+    cols = gen_scan_table(rows, seed=1)
+    from oracle import refpath
+    times = []
+    threads = os.cpu_count() or 1
+    for i in range(args.warmup + args.steps):
+        r = refpath.selective_scan_sum(cols, tpl, threads=threads)
+        if i >= args.warmup:
+            times.append(r["seconds"])
+    sec = sum(times)
+    value = rows * len(times) / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded; TPC-H lineitem shapes)",
+        "config": {"workload": "selective_scan_sum (60M-row scan, 1.81% selectivity, int128 sum)",
+                   "rows_per_step": rows},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                         "sample": f"{rows} rows per step (the full 60M-row workload), "
+                                   f"C++ restatement of the reference CPU path, {r['threads']} threads"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--reference-rows", type=int, default=ROWS)
+    ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from turbogp_b200 import workloads
+    from turbogp_b200.engine import Context
+
+    rows = args.rows
+    tpl = workloads.selective_scan_sum()
+    host = gen_scan_table(rows, seed=1 + rank)
+    ctx = Context(local)
+    coltypes = {"ship_day": "date", "discount_pct": "int", "quantity": "int", "price_cents": "int"}
+    table = ctx.register(host, coltypes)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+    def merge(out):
+        """Exact cross-rank merge of the partial int128 sum and count (NCCL all-gather)."""
+        if world == 1:
+            return out.values[0][0].value, out.values[0][1].value
+        import torch.distributed as dist
+        s, c = out.values[0][0].value, out.values[0][1].value
+        mine = torch.tensor([s & 0xFFFFFFFFFFFFFFFF, s >> 64, c], dtype=torch.int64, device="cuda")
+        mine[0] = torch.tensor(np.array([s & 0xFFFFFFFFFFFFFFFF], dtype=np.uint64).view(np.int64)[0])
+        parts = [torch.empty_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine)
+        tot_s, tot_c = 0, 0
+        for p in parts:
+            lo, hi, cc = [int(x) for x in p.cpu()]
+            tot_s += (hi << 64) | (lo & 0xFFFFFFFFFFFFFFFF)
+            tot_c += cc
+        return tot_s, tot_c
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Warm-up.
+    for _ in range(args.warmup):
+        out = table.aggregate(tpl.aggs, tpl.group_by, tpl.where)
+        merge(out)
+    expect = merge(out)
+
+    # ---- value: table resident in HBM -------------------------------------
+    ctx.profile(True)
+    ctx.profile_read()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            out = table.aggregate(tpl.aggs, tpl.group_by, tpl.where)
+            got = merge(out)
+        ev1.record(stream)
+        ev1.synchronize()
+    ctx.sync()
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches, kernel_ms = ctx.profile_read()
+    ctx.profile(False)
+    if got != expect:
+        raise SystemExit(f"result changed between steps: {got} != {expect}")
+    clk = clocks.summary()
+    kernel_avg_ms = max_over_ranks(kernel_ms / max(1, launches))
+    value = rows * world * args.steps / (ms / 1000.0)
+
+    # ---- e2e: pinned host buffers, H2D + execute + D2H every step ----------
+    pinned = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
+    pinned_np = {k: v.numpy() for k, v in pinned.items()}
+    h2d = sum(v.nbytes for v in pinned_np.values())
+    d2h = 8 * 6  # accumulator words + counters read back per step
+    table.reload(pinned_np)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        table.reload(pinned_np)
+        out = table.aggregate(tpl.aggs, tpl.group_by, tpl.where)
+        got = merge(out)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = rows * world * args.e2e_steps / (e2e_ms / 1000.0)
+    if got != expect:
+        raise SystemExit("e2e result differs")
+
+    # ---- CPU baseline (rank 0, N=1 only) -----------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refpath
+        sample = min(args.cpu_sample_rows, rows)
+        r = refpath.selective_scan_sum({k: v[:sample] for k, v in host.items()}, tpl,
+                                       threads=os.cpu_count() or 1)
+        cpu = {"value": sample / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+               "sample": f"first {sample} rows of the same table, one pass, C++ restatement of the "
+                         f"reference CPU path (AVX-512 filters into bitmaps, set-bit collect, f64 sum)"}
+
+    peak, peak_kind = peak_hbm()
+    achieved = rows * BYTES_PER_ROW / (kernel_avg_ms / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H lineitem shapes)",
+        "config": {"workload": "selective_scan_sum (60M-row scan, 1.81% selectivity, int128 sum)",
+                   "rows_per_rank": rows, "bytes_per_row": BYTES_PER_ROW, "l2": L2_NOTE,
+                   "parallelism": f"row shards x{world}"},
+        "hbm_gbs": rows * world * BYTES_PER_ROW * args.steps / (ms / 1000.0) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_launch(),
+                     "kernel_ms": kernel_avg_ms, "kernel": "tgp::scan_kernel<MODE_SCALAR>"},
+        "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+        "result": {"sum": str(expect[0]), "count": expect[1]},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    table.drop()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

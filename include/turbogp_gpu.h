@@ -1,0 +1,433 @@
+/*
+ * turbogp_gpu.h — C ABI of the B200 (sm_100a) execution backend for turboGP's
+ * data-parallel hot path: predicate scan/filter into selection bitmaps,
+ * hash-join build and probe, and grouped/scalar hash aggregation.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers, sizes and POD
+ * structs, never throws, and reports failures through `tgp_status`.
+ * Column and output pointers may be host memory (pageable or pinned) or device
+ * memory of the context's GPU; the library detects which.
+ *
+ * Reference interfaces these entry points replace (paths inside pkhairkh/turboGP):
+ *   - src/kernel/mod.rs:48-177    Operator / PredicateOp / KernelParams /
+ *                                 KernelResult / trait Kernel::execute
+ *   - src/kernel/mod.rs:188-242   KernelTable::{new, select, register, list}
+ *   - src/memory/tier.rs:11-29    MemoryTier (the HBM tier the GPU kernels use)
+ *   - src/exec/bitmap.rs:42-316   Bitmap (LSB-first packed selection bitmap),
+ *                                 filter_* and iter_set_bits
+ *   - src/engine/query_interpreter/expr.rs:419,633,1468  build_mask → bitmap
+ *   - src/engine/query_interpreter/aggregate.rs:507,1270,1291  grouped/scalar agg
+ *   - src/engine/query_interpreter/accum_grouped.rs:55   accumulator GROUP BY
+ *   - src/engine/query_interpreter/join.rs:544           hash_join_with_keys
+ *   - src/exec/join_hash_table.rs:55-212                 JoinHashTable
+ */
+#ifndef TURBOGP_GPU_H
+#define TURBOGP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TGP_ABI_VERSION 1u
+
+#if defined(__GNUC__)
+#define TGP_API __attribute__((visibility("default")))
+#else
+#define TGP_API
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* The reference's Kernel trait has no error channel (src/kernel/mod.rs:158-177;
+ * callers map a missing kernel to Error::Unsupported, src/engine/executor.rs:1015).
+ * The C ABI returns one of these from every call instead. */
+typedef enum tgp_status {
+    TGP_OK = 0,
+    TGP_INVALID_ARG = 1,   /* null pointer, bad index, misaligned device column, bad program */
+    TGP_OOM = 2,           /* device or pinned-host allocation failed, or over the memory budget */
+    TGP_UNSUPPORTED = 3,   /* query shape this backend does not execute */
+    TGP_TIMEOUT = 4,       /* a bounded device wait gave up; the context stays usable */
+    TGP_DEVICE_ERROR = 5,  /* CUDA runtime error */
+    TGP_NOT_FOUND = 6,     /* unknown table / join / ticket id */
+    TGP_CAPACITY = 7       /* caller-provided output buffer too small; required size reported */
+} tgp_status;
+
+/* Human-readable name of a status code (static storage). */
+TGP_API const char* tgp_status_string(int status);
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct tgp_ctx tgp_ctx;
+
+/* Opens a context on CUDA device `device`: a stream, a device scratch arena
+ * and pinned staging buffers. One context may be used from one host thread at
+ * a time. */
+TGP_API int tgp_init(tgp_ctx** out, int device);
+TGP_API int tgp_shutdown(tgp_ctx* ctx);
+
+/* Last error message recorded on this context (static until the next call). */
+TGP_API const char* tgp_last_error(const tgp_ctx* ctx);
+
+/* The cudaStream_t (as void*) every kernel of this context is launched on. */
+TGP_API void* tgp_ctx_stream(tgp_ctx* ctx);
+
+/* Number of streaming multiprocessors of the context's device. */
+TGP_API int tgp_ctx_sm_count(const tgp_ctx* ctx);
+
+/* Blocks until all work enqueued on the context's stream has finished. */
+TGP_API int tgp_sync(tgp_ctx* ctx);
+
+/* When enabled, the context records CUDA events on its stream around every
+ * scan-kernel launch; tgp_profile_read returns the launches recorded since the
+ * last read and their summed device time (ms), then resets the record. */
+TGP_API int tgp_profile_enable(tgp_ctx* ctx, int on);
+TGP_API int tgp_profile_read(tgp_ctx* ctx, uint64_t* launches, double* total_ms);
+
+/* ------------------------------------------------------------------------ */
+/* Kernel table boundary (mirrors src/kernel/mod.rs)                         */
+/* ------------------------------------------------------------------------ */
+
+/* Mirrors `enum Operator` (src/kernel/mod.rs:48-74), same order. */
+typedef enum tgp_operator {
+    TGP_OP_SCAN_EQ_U64 = 0,
+    TGP_OP_SCAN_RANGE_U64 = 1,
+    TGP_OP_SCAN_MULTI_PREDICATE = 2,
+    TGP_OP_HASH_BUILD = 3,
+    TGP_OP_HASH_PROBE = 4,
+    TGP_OP_AGGREGATE_SUM_F64 = 5,
+    TGP_OP_AGGREGATE_COUNT_DISTINCT = 6,
+    TGP_OP_SIMILARITY_HAMMING = 7,   /* not implemented on the GPU: TGP_UNSUPPORTED */
+    TGP_OP_LEAPFROG_JOIN = 8         /* not implemented on the GPU: TGP_UNSUPPORTED */
+} tgp_operator;
+
+/* Mirrors `enum PredicateOp` (src/kernel/mod.rs:84-92). */
+typedef enum tgp_predicate_op {
+    TGP_PRED_EQ = 0,
+    TGP_PRED_GT = 1,
+    TGP_PRED_LT = 2
+} tgp_predicate_op;
+
+/* Mirrors `enum MemoryTier` (src/memory/tier.rs:11-29), same order. */
+typedef enum tgp_memory_tier {
+    TGP_TIER_L1L2 = 0,
+    TGP_TIER_L3 = 1,
+    TGP_TIER_DDR5 = 2,
+    TGP_TIER_HBM = 3,
+    TGP_TIER_CXL = 4,
+    TGP_TIER_NVME = 5,
+    TGP_TIER_NVMEOF = 6,
+    TGP_TIER_NETWORK = 7
+} tgp_memory_tier;
+
+/* Mirrors `enum CpuTarget` (src/kernel/cpu.rs:31-43) plus the new GPU target
+ * the B200 kernels register under. */
+typedef enum tgp_cpu_target {
+    TGP_CPU_SCALAR = 0,
+    TGP_CPU_X86_AVX2 = 1,
+    TGP_CPU_X86_AVX512 = 2,
+    TGP_CPU_ARM_NEON = 3,
+    TGP_CPU_ARM_SVE = 4,
+    TGP_CPU_GPU_SM100A = 5
+} tgp_cpu_target;
+
+/* Field-for-field mirror of `struct KernelParams` (src/kernel/mod.rs:96-119).
+ * The Rust struct has no #[repr(C)], so a Rust caller declares a #[repr(C)]
+ * twin of this layout and converts field by field. */
+typedef struct tgp_kernel_params {
+    uint64_t target_u64;
+    uint64_t low_u64;
+    uint64_t high_u64;
+    uint32_t max_distance;
+    uint32_t _pad0;
+    uint64_t cell_count;
+    uint64_t target2_u64;
+    uint64_t target3_u64;
+    uint8_t pred1_op;          /* tgp_predicate_op */
+    uint8_t pred2_op;
+    uint8_t pred3_op;
+    uint8_t predicate_count;   /* 0..=3 */
+    uint32_t _pad1;
+} tgp_kernel_params;
+
+/* Mirror of `struct KernelResult` (src/kernel/mod.rs:140-148). */
+typedef struct tgp_kernel_result {
+    uint64_t count;
+    double sum;
+    uint64_t mask;
+} tgp_kernel_result;
+
+/* One GPU kernel as it registers into the reference's KernelTable:
+ * key (operator, cpu, tier) as in src/kernel/mod.rs:39, plus its name. */
+typedef struct tgp_kernel_info {
+    uint32_t op;      /* tgp_operator */
+    uint32_t cpu;     /* tgp_cpu_target (always TGP_CPU_GPU_SM100A) */
+    uint32_t tier;    /* tgp_memory_tier (always TGP_TIER_HBM) */
+    uint32_t _pad;
+    const char* name; /* static storage */
+} tgp_kernel_info;
+
+/* Number of GPU kernels this library registers, and the i-th one. Replaces the
+ * register_*_kernels functions of src/kernel/mod.rs:245-375 for the GPU. */
+TGP_API uint32_t tgp_kernel_count(void);
+TGP_API int tgp_kernel_info_at(uint32_t i, tgp_kernel_info* out);
+
+/* Replaces `unsafe fn Kernel::execute(&self, input, output, params)`
+ * (src/kernel/mod.rs:171-176) for every operator the GPU registers.
+ *
+ * Input layouts follow the reference exactly:
+ *  - scan / sum / count-distinct: `input` = `cell_count` u64 cells
+ *    (src/kernel/scan.rs:45-48, src/kernel/aggregate.rs:36-41).
+ *  - HASH_BUILD: `input` = `cell_count` u64 keys; `output` receives an opaque
+ *    table handle in its first 8 bytes (src/kernel/hash.rs:135-147). Free it
+ *    with tgp_hash_table_free (the reference frees its Box with
+ *    Box::from_raw, src/kernel/hash.rs:284).
+ *  - HASH_PROBE: `input` = [handle: 8 bytes][cell_count u64 probe keys]
+ *    (src/kernel/hash.rs:171-178); result.count = number of matching
+ *    (probe, build) pairs.
+ * `input` may be host or device memory. `output` is caller-owned host memory of
+ * at least 64 bytes (callers pass `[0u8; 64]`, src/engine/executor.rs:1018),
+ * or NULL for operators other than HASH_BUILD.
+ * Scan kernels fill `mask` with the match bits of the first 64 cells, as the
+ * scalar kernel does (src/kernel/scan.rs:50-62). */
+TGP_API int tgp_kernel_execute(tgp_ctx* ctx, uint32_t op, const void* input, void* output,
+                       const tgp_kernel_params* params, tgp_kernel_result* result);
+
+/* Frees a table handle produced by TGP_OP_HASH_BUILD. */
+TGP_API int tgp_hash_table_free(tgp_ctx* ctx, void* handle);
+
+/* ------------------------------------------------------------------------ */
+/* HBM-resident tables (device tier for src/datasource/table.rs:25-66)       */
+/* ------------------------------------------------------------------------ */
+
+/* Physical element type of a resident column. The reference stores every
+ * value as one u64 cell (src/datasource/table.rs:27-30); a narrow column's
+ * cell value is its sign-extended (I32, I64) or zero-extended (U8) value,
+ * which is exactly the cell the reference would hold for the same integer. */
+typedef enum tgp_dtype {
+    TGP_DT_U8 = 1,
+    TGP_DT_I32 = 2,
+    TGP_DT_I64 = 3,
+    TGP_DT_U64 = 4,  /* a raw reference cell */
+    TGP_DT_F64 = 5   /* f64 stored as its bits, as the reference does */
+} tgp_dtype;
+
+/* How a column's cells compare, mirroring `ColType` (src/engine/
+ * query_interpreter/types.rs:79): Int compares as signed i64, Date as
+ * unsigned u64 (expr.rs:1482-1506), Float as f64. */
+typedef enum tgp_coltype {
+    TGP_CT_INT = 0,
+    TGP_CT_DATE = 1,
+    TGP_CT_FLOAT = 2
+} tgp_coltype;
+
+typedef struct tgp_column_desc {
+    uint32_t dtype;     /* tgp_dtype */
+    uint32_t coltype;   /* tgp_coltype used by predicates on this column */
+    const void* data;   /* `rows` elements, host or device memory */
+} tgp_column_desc;
+
+typedef uint64_t tgp_table_id;
+
+/* Copies `ncols` host (or device) columns of `rows` rows into device memory
+ * owned by the context, computes per-column min/max statistics, and returns a
+ * table id. */
+TGP_API int tgp_table_register(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols,
+                       uint64_t rows, tgp_table_id* out);
+
+/* Registers device columns without copying (the caller keeps them alive until
+ * tgp_table_drop). Device column pointers must be 16-byte aligned. */
+TGP_API int tgp_table_register_device(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols,
+                              uint64_t rows, tgp_table_id* out);
+
+/* Replaces the contents of every column of a registered (copying) table from
+ * new host buffers of the same row count, reusing its device memory. */
+TGP_API int tgp_table_reload(tgp_ctx* ctx, tgp_table_id table, const tgp_column_desc* cols,
+                     uint32_t ncols);
+
+TGP_API int tgp_table_drop(tgp_ctx* ctx, tgp_table_id table);
+
+/* Row count and the device pointer of column `col` (for callers that launch
+ * their own work on resident data). */
+TGP_API int tgp_table_info(tgp_ctx* ctx, tgp_table_id table, uint64_t* rows, uint32_t* ncols);
+TGP_API int tgp_table_column_stats(tgp_ctx* ctx, tgp_table_id table, uint32_t col, int64_t* min_cell,
+                           int64_t* max_cell);
+
+/* ------------------------------------------------------------------------ */
+/* Predicate programs (WHERE → selection bitmap)                             */
+/* ------------------------------------------------------------------------ */
+
+/* Comparison of one column against literal(s). Semantics per column coltype
+ * follow apply_comparison (expr.rs:1468-1530) and BETWEEN (expr.rs:687-760):
+ * BETWEEN = lit <= cell AND cell <= lit2; NOT_BETWEEN = cell < lit OR cell > lit2.
+ * For FLOAT, EQ is the reference's epsilon equality (|x - v| <= 1e-6*max(|v|,1),
+ * bitmap.rs:505-515) and NE is its negation (bitmap.rs:498-500). */
+typedef enum tgp_cmp {
+    TGP_CMP_EQ = 0,
+    TGP_CMP_NE = 1,
+    TGP_CMP_LT = 2,
+    TGP_CMP_LE = 3,
+    TGP_CMP_GT = 4,
+    TGP_CMP_GE = 5,
+    TGP_CMP_BETWEEN = 6,
+    TGP_CMP_NOT_BETWEEN = 7
+} tgp_cmp;
+
+/* Node kinds of a postfix predicate program. AND/OR pop two masks and push
+ * one; NOT pops one. The program must leave exactly one mask on the stack.
+ * An empty program selects every row (Bitmap::all_ones, bitmap.rs:57). */
+typedef enum tgp_pred_kind {
+    TGP_PN_LEAF = 0,
+    TGP_PN_AND = 1,
+    TGP_PN_OR = 2,
+    TGP_PN_NOT = 3
+} tgp_pred_kind;
+
+#define TGP_MAX_PRED_NODES 16
+
+typedef struct tgp_pred_node {
+    uint32_t kind;    /* tgp_pred_kind */
+    uint32_t column;  /* LEAF: column index in the table */
+    uint32_t cmp;     /* LEAF: tgp_cmp */
+    uint32_t _pad;
+    uint64_t lit;     /* LEAF: literal bits (i64 for INT, u64 for DATE, f64 bits for FLOAT) */
+    uint64_t lit2;    /* LEAF: upper bound for BETWEEN / NOT_BETWEEN */
+} tgp_pred_node;
+
+/* Evaluates a predicate program over a resident table.
+ *  bitmap_out: NULL or ((rows + 7) / 8) bytes, LSB-first (bitmap.rs:36-40);
+ *              tail bits of the last byte are zero.
+ *  rowids_out: NULL or `rowids_cap` u32 entries, receives the selected row
+ *              indices in ascending order (Bitmap::iter_set_bits, bitmap.rs:224).
+ *  count_out:  number of selected rows (always written on TGP_OK and
+ *              TGP_CAPACITY). Output pointers may be host or device memory. */
+TGP_API int tgp_filter(tgp_ctx* ctx, tgp_table_id table, const tgp_pred_node* pred, uint32_t npred,
+               uint8_t* bitmap_out, uint32_t* rowids_out, uint64_t rowids_cap,
+               uint64_t* count_out);
+
+/* ------------------------------------------------------------------------ */
+/* Aggregation queries (scalar, grouped, and join + grouped)                 */
+/* ------------------------------------------------------------------------ */
+
+typedef enum tgp_agg_func {
+    TGP_AGG_COUNT_STAR = 0,    /* COUNT(*) */
+    TGP_AGG_COUNT_NONZERO = 1, /* COUNT(col): the reference counts cells != 0
+                                  (aggregate.rs:1364-1367, accum_grouped.rs:243-246) */
+    TGP_AGG_SUM = 2,           /* exact int128 sum of the per-row i64 argument */
+    TGP_AGG_AVG = 3,           /* f64(sum) / f64(count), aggregate.rs:1416-1424 */
+    TGP_AGG_MIN = 4,           /* signed i64 min of the argument, aggregate.rs:1822-1836 */
+    TGP_AGG_MAX = 5
+} tgp_agg_func;
+
+/* Which table a column reference reads in a join query. */
+typedef enum tgp_side {
+    TGP_SIDE_PROBE = 0,  /* the query's own table (the probe side of a join) */
+    TGP_SIDE_BUILD = 1   /* the joined build table */
+} tgp_side;
+
+#define TGP_MAX_FACTORS 4
+#define TGP_MAX_AGGS 8
+#define TGP_MAX_GROUP_KEYS 4
+
+/* One affine factor `mul * cell + add` (wrapping i64). column = -1 means the
+ * constant `add`. The per-row argument of an aggregate is the wrapping i64
+ * product of its factors, which is exactly the reference's per-row
+ * Int x Int evaluation (expr.rs:2063-2076) of expressions such as
+ * `price`, `price * disc`, `price * (100 - disc) * (100 + tax)`. */
+typedef struct tgp_factor {
+    int32_t column;
+    uint32_t side;   /* tgp_side */
+    int64_t mul;
+    int64_t add;
+} tgp_factor;
+
+typedef struct tgp_agg {
+    uint32_t func;      /* tgp_agg_func */
+    uint32_t nfactors;  /* 0..=TGP_MAX_FACTORS (COUNT_STAR uses 0) */
+    tgp_factor f[TGP_MAX_FACTORS];
+} tgp_agg;
+
+typedef struct tgp_group_key {
+    uint32_t column;
+    uint32_t side;   /* tgp_side */
+} tgp_group_key;
+
+typedef uint64_t tgp_join_id;
+
+typedef struct tgp_query {
+    tgp_table_id table;              /* table scanned (probe side when join != 0) */
+    const tgp_pred_node* pred;       /* WHERE program on `table` (may be NULL) */
+    uint32_t npred;
+    uint32_t ngroup;                 /* 0 = scalar aggregate */
+    const tgp_group_key* group;
+    uint32_t nagg;
+    uint32_t _pad;
+    const tgp_agg* aggs;
+    tgp_join_id join;                /* 0 = no join */
+    uint32_t probe_key_column;       /* join key column of `table` */
+    uint32_t flags;                  /* reserved, 0 */
+} tgp_query;
+
+/* Value of one aggregate of one group. (lo, hi) is a two's-complement int128:
+ * COUNT* → count; SUM/AVG → exact sum; MIN/MAX → value. `as_f64` is the
+ * reference's f64 view (AVG result; f64(sum) for SUM). */
+typedef struct tgp_agg_value {
+    uint64_t lo;
+    int64_t hi;
+    uint64_t count;   /* rows that reached this aggregate */
+    double as_f64;
+} tgp_agg_value;
+
+typedef struct tgp_query_result {
+    uint64_t rows_scanned;
+    uint64_t rows_selected;    /* rows passing WHERE (join: probe rows passing WHERE) */
+    uint64_t ngroups;          /* groups produced (1 for a scalar aggregate) */
+    uint32_t flags;            /* TGP_RESULT_* bits */
+    uint32_t _pad;
+} tgp_query_result;
+
+/* Set when some per-row argument wrapped in i64, as the reference's own
+ * wrapping arithmetic would (expr.rs:2063-2076). */
+#define TGP_RESULT_ROW_OVERFLOW 1u
+
+/* Executes one aggregation query.
+ *  keys_out:  group_cap * ngroup u64 cells (group key values), may be NULL for
+ *             a scalar query;
+ *  vals_out:  group_cap * nagg values;
+ * Groups are returned sorted by key tuple (ascending signed cells), so results
+ * compare as multisets independent of hash order. Returns TGP_CAPACITY (with
+ * result->ngroups set) when group_cap is too small. */
+TGP_API int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out,
+                uint64_t group_cap, tgp_query_result* result);
+
+/* ------------------------------------------------------------------------ */
+/* Hash join (src/engine/query_interpreter/join.rs:544-939)                  */
+/* ------------------------------------------------------------------------ */
+
+/* Builds a device hash table over the rows of `build_table` that pass `pred`
+ * (the single-table build filter of join.rs:79-100), keyed by `key_column`.
+ * Duplicate keys are kept (join_hash_table.rs:27-30). */
+TGP_API int tgp_join_build(tgp_ctx* ctx, tgp_table_id build_table, uint32_t key_column,
+                   const tgp_pred_node* pred, uint32_t npred, tgp_join_id* out);
+TGP_API int tgp_join_drop(tgp_ctx* ctx, tgp_join_id join);
+
+/* Inner equi-join probe that emits the (probe_row, build_row) pairs, as the
+ * reference's probe loop does (join.rs:748-790). Pairs are returned sorted by
+ * (probe_row, build_row). Returns TGP_CAPACITY with *npairs set when `cap` is
+ * too small. */
+TGP_API int tgp_join_probe_pairs(tgp_ctx* ctx, tgp_join_id join, tgp_table_id probe_table,
+                         uint32_t probe_key_column, const tgp_pred_node* pred, uint32_t npred,
+                         uint32_t* probe_rows, uint32_t* build_rows, uint64_t cap,
+                         uint64_t* npairs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TURBOGP_GPU_H */

@@ -1,0 +1,182 @@
+"""GPU results against the CPU oracle on seeded inputs: bit-exact bitmaps,
+row ids, join pairs, counts and int128 sums."""
+import numpy as np
+import pytest
+
+import oracle
+from turbogp_b200 import _capi as A
+from turbogp_b200 import datagen, workloads
+from turbogp_b200.engine import avg, build_col, col, count_col, count_star, max_, min_, sum_
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [0, 1, 7, 31, 32, 33, 255, 2047, 2048, 2049, 4096, 10_007, 100_003]
+CT = datagen.LINEITEM_COLTYPES
+
+
+def bits(bm, n):
+    return np.unpackbits(bm, bitorder="little")[:n]
+
+
+def same_query(a, b):
+    assert a.rows_selected == b.rows_selected
+    assert a.keys == b.keys
+    assert len(a.values) == len(b.values)
+    for ga, gb in zip(a.values, b.values):
+        for x, y in zip(ga, gb):
+            assert x.count == y.count
+            if x.count:
+                assert x.value == y.value
+                assert x.as_f64 == y.as_f64 or abs(x.as_f64 - y.as_f64) <= 1e-12 * abs(y.as_f64)
+
+
+def predicates(d0=datagen.DAY0):
+    c = col
+    return [
+        None,
+        c("ship_day") <= d0 + 2435,
+        (c("ship_day") >= d0 + 730) & (c("ship_day") < d0 + 1095) & c("discount_pct").between(5, 7) & (c("quantity") < 24),
+        (c("flag_a") == 1) | (c("flag_b") == 0),
+        ~((c("quantity") > 10) & (c("price_cents") <= 5_000_000)) | c("tax_pct").not_between(2, 6),
+        c("price_cents") != 1_000_000,
+        (c("quantity") < -5) | (c("discount_pct") >= 11),        # nothing passes
+        c("quantity") >= -(2**40),                                # everything passes (literal beyond i32)
+        c("ship_day") < 2**40,                                    # DATE compare, literal beyond i32
+        (c("flag_a") <= 300) & (c("flag_b") >= -1),
+    ]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_filter_bitmaps_and_rowids(ctx, n):
+    t_host = datagen.lineitem(n, seed=11 + n)
+    t = ctx.register(t_host, CT)
+    for i, p in enumerate(predicates()):
+        g = t.filter(p)
+        o = oracle.filter(t_host, CT, p)
+        assert g.count == o.count, (n, i)
+        assert np.array_equal(bits(g.bitmap, n), bits(o.bitmap, n)), (n, i)
+        if n:
+            # tail bits beyond n are zero
+            assert np.all(np.unpackbits(g.bitmap, bitorder="little")[n:] == 0)
+        assert np.array_equal(g.rowids, o.rowids), (n, i)
+    t.drop()
+
+
+def test_filter_all_dtypes_and_signedness(ctx):
+    rng = np.random.default_rng(5)
+    n = 5000
+    cols = {
+        "u8": rng.integers(0, 256, n, dtype=np.uint8),
+        "i32": rng.integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32),
+        "i64": rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64),
+        "u64": rng.integers(0, 2**64 - 1, n, dtype=np.uint64),
+        "f64": rng.normal(0, 100, n),
+    }
+    cols["i32"][:4] = [-2**31, 2**31 - 1, 0, -1]
+    cols["i64"][:4] = [-2**63, 2**63 - 1, 0, -1]
+    for ct_name in ["int", "date"]:
+        cts = {k: ct_name for k in ["u8", "i32", "i64", "u64"]}
+        cts["f64"] = "float"
+        t = ctx.register(cols, cts)
+        for name in ["u8", "i32", "i64", "u64"]:
+            for v in [0, 1, -1, 7, 200, 255, 256, -2**31, 2**31 - 1, 2**31, -2**63, 2**63 - 1, 2**64 - 1]:
+                for op in ["__eq__", "__ne__", "__lt__", "__le__", "__gt__", "__ge__"]:
+                    p = getattr(col(name), op)(v)
+                    assert t.filter(p, rowids=False).count == oracle.filter(cols, cts, p).count, (ct_name, name, v, op)
+                for lo, hi in [(-5, 5), (10, 3), (0, 2**64 - 1), (-2**63, 2**63 - 1)]:
+                    for p in [col(name).between(lo, hi), col(name).not_between(lo, hi)]:
+                        g = t.filter(p)
+                        o = oracle.filter(cols, cts, p)
+                        assert np.array_equal(g.rowids, o.rowids), (ct_name, name, lo, hi)
+        for v in [0.0, 1.5, -3.25, 100.0]:
+            for op in ["__eq__", "__ne__", "__lt__", "__le__", "__gt__", "__ge__"]:
+                p = getattr(col("f64"), op)(v)
+                assert np.array_equal(t.filter(p).rowids, oracle.filter(cols, cts, p).rowids), (v, op)
+        t.drop()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2049, 100_003, 1_000_000])
+def test_templates_match_oracle(ctx, n):
+    t_host = datagen.lineitem(n, seed=3)
+    t = ctx.register(t_host, CT)
+    for tpl in [workloads.filtered_group_agg(), workloads.selective_scan_sum()]:
+        g = t.aggregate(tpl.aggs, tpl.group_by, tpl.where)
+        o = oracle.aggregate(t_host, CT, tpl.aggs, tpl.group_by, tpl.where)
+        same_query(g, o)
+    t.drop()
+
+
+def test_group_modes(ctx):
+    """Direct private / shared / global tables and the global hash table."""
+    n = 300_000
+    t_host = datagen.lineitem(n, seed=21)
+    t = ctx.register(t_host, CT)
+    aggs = [count_star(), sum_(col("price_cents") * (100 - col("discount_pct"))), min_(col("quantity")),
+            max_(col("price_cents")), avg(col("quantity")), count_col(col("discount_pct"))]
+    for gb in [("flag_a",), ("flag_a", "flag_b"), ("tax_pct", "flag_a", "flag_b"), ("ship_day",),
+               ("ship_day", "quantity"), ("price_cents",), ("quantity", "price_cents")]:
+        g = t.aggregate(aggs, gb, col("discount_pct") <= 8)
+        o = oracle.aggregate(t_host, CT, aggs, gb, col("discount_pct") <= 8)
+        same_query(g, o)
+    t.drop()
+
+
+def test_int128_sums_and_overflow_flag(ctx):
+    n = 100_000
+    big = np.full(n, 2**62 + 12345, dtype=np.int64)
+    grp = (np.arange(n) % 3).astype(np.uint8)
+    cols = {"v": big, "g": grp, "neg": -big}
+    t = ctx.register(cols)
+    for aggs in [[sum_(col("v")), sum_(col("neg")), count_star()], [sum_(col("v") * 3)], [sum_(col("v") * col("v"))]]:
+        for gb in [(), ("g",)]:
+            g = t.aggregate(aggs, gb)
+            o = oracle.aggregate(cols, None, aggs, gb)
+            same_query(g, o)
+            assert g.flags == o.flags
+    t.drop()
+
+
+def test_join_pairs_and_join_aggregate(ctx):
+    dim = datagen.dimension(50_000, seed=7)
+    fact = datagen.fact_fk(400_000, 50_000, 0.8, seed=8)
+    fact["fk"][:100] = 60_000  # keys beyond the build side
+    d = ctx.register(dim, datagen.DIMENSION_COLTYPES)
+    f = ctx.register(fact, {**CT, "fk": "int"})
+    tpl = workloads.join_group_agg()
+    j = d.join_build("key", tpl.build_where)
+    pr, br = j.probe_pairs(f, "fk", col("quantity") < 30)
+    opr, obr = oracle.join_pairs(fact, {**CT, "fk": "int"}, "fk", col("quantity") < 30, dim,
+                                 datagen.DIMENSION_COLTYPES, "key", tpl.build_where)
+    assert np.array_equal(pr, opr) and np.array_equal(br, obr)
+    for where in [None, col("quantity") < 30]:
+        g = f.aggregate(tpl.aggs, tpl.group_by, where, join=j, probe_key="fk")
+        o = oracle.aggregate(fact, {**CT, "fk": "int"}, tpl.aggs, tpl.group_by, where,
+                             build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where), probe_key="fk")
+        same_query(g, o)
+    # Scalar aggregate over the join and duplicate build keys.
+    dup = {"key": np.repeat(np.arange(1, 1001, dtype=np.int32), 3), "w": np.arange(3000, dtype=np.int32)}
+    dd = ctx.register(dup)
+    jd = dd.join_build("key")
+    aggs = [count_star(), sum_(col("price_cents") * build_col("w"))]
+    small = {k: v[:20_000] for k, v in fact.items()}
+    fs = ctx.register(small, {**CT, "fk": "int"})
+    g = fs.aggregate(aggs, (), None, join=jd, probe_key="fk")
+    o = oracle.aggregate(small, {**CT, "fk": "int"}, aggs, (), None, build=(dup, None, "key", None), probe_key="fk")
+    same_query(g, o)
+    pr, br = jd.probe_pairs(fs, "fk")
+    opr, obr = oracle.join_pairs(small, {**CT, "fk": "int"}, "fk", None, dup, None, "key", None)
+    assert np.array_equal(pr, opr) and np.array_equal(br, obr)
+
+
+def test_full_size_selective_scan(ctx):
+    """The 60M-row scan workload at full size against the oracle."""
+    n = 60_000_000
+    t_host = datagen.lineitem(n, seed=1)
+    t = ctx.register(t_host, CT)
+    tpl = workloads.selective_scan_sum()
+    g = t.aggregate(tpl.aggs, tpl.group_by, tpl.where)
+    o = oracle.aggregate(t_host, CT, tpl.aggs, tpl.group_by, tpl.where)
+    same_query(g, o)
+    # Size-independent property: the filter's count equals the aggregate's count.
+    assert t.filter(tpl.where, bitmap=False, rowids=False).count == g.values[0][1].value
+    t.drop()

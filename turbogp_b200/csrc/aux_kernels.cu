@@ -1,0 +1,280 @@
+// aux_kernels.cu — the smaller kernels around the scan engine:
+//   * column statistics (signed min / max of cells) computed at registration,
+//   * bitmap → ascending row-id compaction (Bitmap::iter_set_bits,
+//     src/exec/bitmap.rs:224-316),
+//   * the AggregateSumF64 kernel-table operator (src/kernel/aggregate.rs:19-148)
+//     with double-double compensated summation,
+//   * the AggregateCountDistinct operator (src/kernel/aggregate.rs:160-185),
+//     an exact hash set instead of the reference's HashSet,
+//   * sorting of packed join pairs and their split into two u32 arrays.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cub/cub.cuh>
+
+#include "device_common.cuh"
+#include "plan.hpp"
+
+namespace tgp {
+
+constexpr int kAuxThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Column statistics
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kAuxThreads) column_minmax_kernel(const uint8_t* col, uint32_t dtype,
+                                                                   uint64_t n, long long* out /* [min, max] */) {
+    long long lo = 0x7fffffffffffffffll, hi = static_cast<long long>(0x8000000000000000ull);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        long long v;
+        if (dtype == DT_U8) v = col[i];
+        else if (dtype == DT_I32) v = reinterpret_cast<const int32_t*>(col)[i];
+        else v = reinterpret_cast<const long long*>(col)[i];
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = min(lo, __shfl_down_sync(0xffffffffu, lo, d));
+        hi = max(hi, __shfl_down_sync(0xffffffffu, hi, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(out, lo);
+        atomicMax(out + 1, hi);
+    }
+}
+
+cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
+                                 int sms, cudaStream_t st) {
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    const uint64_t cap = static_cast<uint64_t>(sms) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) return cudaSuccess;
+    column_minmax_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(col, dtype, n, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Bitmap compaction: one CTA per scan tile (kTileRows bits = 64 words).
+// tile_base[t] = exclusive prefix of selected rows before tile t.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) compact_rowids_kernel(const uint32_t* bitmap, uint64_t nwords,
+                                                           const unsigned long long* tile_base,
+                                                           uint32_t* rowids, uint64_t cap) {
+    constexpr int kWordsPerTile = kTileRows / 32;
+    __shared__ uint32_t scan[kWordsPerTile];
+    const uint64_t t = blockIdx.x;
+    const uint64_t w = t * kWordsPerTile + threadIdx.x;
+    const uint32_t word = w < nwords ? bitmap[w] : 0u;
+    const uint32_t c = __popc(word);
+    // Block exclusive scan of 64 counts (two warps).
+    uint32_t incl = c;
+    const uint32_t lane = threadIdx.x & 31;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += y;
+    }
+    scan[threadIdx.x] = incl;
+    __syncthreads();
+    uint32_t excl = incl - c;
+    if (threadIdx.x >= 32) excl += scan[31];
+    unsigned long long o = tile_base[t] + excl;
+    uint32_t bits = word;
+    while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (o < cap) rowids[o] = static_cast<uint32_t>(w * 32 + b);
+        ++o;
+    }
+}
+
+// Exclusive prefix sum of per-tile counts (u32 → u64) with CUB.
+cudaError_t tile_prefix(const uint32_t* counts, unsigned long long* out, uint64_t n, void* tmp,
+                        size_t* tmp_bytes, cudaStream_t st) {
+    return cub::DeviceScan::ExclusiveSum(tmp, *tmp_bytes, counts, out, static_cast<int>(n), st);
+}
+
+cudaError_t launch_compact(const uint32_t* bitmap, uint64_t nwords, uint64_t ntiles,
+                           const unsigned long long* tile_base, uint32_t* rowids, uint64_t cap,
+                           cudaStream_t st) {
+    if (ntiles == 0) return cudaSuccess;
+    compact_rowids_kernel<<<static_cast<unsigned>(ntiles), kTileRows / 32, 0, st>>>(bitmap, nwords, tile_base,
+                                                                                   rowids, cap);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// AggregateSumF64: Σ f64 cells with double-double (TwoSum) accumulation, so the
+// result is within a few ulps of the exactly rounded sum for inputs without
+// catastrophic cancellation. Each block writes one (hi, lo) pair; the host
+// adds the pairs in double-double.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    const double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double bh, double bl) {
+    double s, e;
+    two_sum(hi, bh, s, e);
+    e += lo + bl;
+    hi = s + e;
+    lo = e - (hi - s);
+}
+
+__global__ void __launch_bounds__(kAuxThreads) sum_f64_kernel(const double* x, uint64_t n, double* out) {
+    double hi = 0.0, lo = 0.0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        dd_add(hi, lo, x[i], 0.0);
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        const double oh = __shfl_down_sync(0xffffffffu, hi, d);
+        const double ol = __shfl_down_sync(0xffffffffu, lo, d);
+        dd_add(hi, lo, oh, ol);
+    }
+    __shared__ double sh[kAuxThreads / 32][2];
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5][0] = hi;
+        sh[threadIdx.x >> 5][1] = lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double h = sh[0][0], l = sh[0][1];
+        for (int w = 1; w < kAuxThreads / 32; ++w) dd_add(h, l, sh[w][0], sh[w][1]);
+        out[2 * blockIdx.x] = h;
+        out[2 * blockIdx.x + 1] = l;
+    }
+}
+
+cudaError_t launch_sum_f64(const double* x, uint64_t n, double* out, int blocks, cudaStream_t st) {
+    sum_f64_kernel<<<blocks, kAuxThreads, 0, st>>>(x, n, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// AggregateCountDistinct: exact distinct count of u64 cells through an
+// open-addressing set (EMPTY = ~0; the value ~0 itself is tracked by a flag).
+// counters[0] += newly inserted keys; counters[1] |= saw ~0.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kAuxThreads) count_distinct_kernel(const unsigned long long* x, uint64_t n,
+                                                                    unsigned long long* set, uint64_t mask,
+                                                                    uint32_t log2cap,
+                                                                    unsigned long long* counters,
+                                                                    uint32_t* err) {
+    unsigned long long local = 0;
+    bool saw_empty = false;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long k = x[i];
+        if (k == ~0ull) {
+            saw_empty = true;
+            continue;
+        }
+        uint64_t h = hash_slot(k, log2cap);
+        bool placed = false;
+        for (uint64_t p = 0; p <= mask; ++p) {
+            unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(set + h);
+            if (cur == k) {
+                placed = true;
+                break;
+            }
+            if (cur == ~0ull) {
+                cur = atomicCAS(set + h, ~0ull, k);
+                if (cur == ~0ull) {
+                    ++local;
+                    placed = true;
+                    break;
+                }
+                if (cur == k) {
+                    placed = true;
+                    break;
+                }
+            }
+            h = (h + 1) & mask;
+        }
+        if (!placed) atomicOr(err, kErrHashFull);
+    }
+    for (int d = 16; d > 0; d >>= 1) local += __shfl_down_sync(0xffffffffu, local, d);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(counters, local);
+    if (saw_empty) atomicOr(counters + 1, 1ull);
+}
+
+cudaError_t launch_count_distinct(const unsigned long long* x, uint64_t n, unsigned long long* set,
+                                  uint64_t mask, uint32_t log2cap, unsigned long long* counters,
+                                  uint32_t* err, int blocks, cudaStream_t st) {
+    count_distinct_kernel<<<blocks, kAuxThreads, 0, st>>>(x, n, set, mask, log2cap, counters, err);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Join pairs: sort packed (probe << 32 | build) pairs, then split.
+// ---------------------------------------------------------------------------
+cudaError_t sort_pairs(const unsigned long long* in, unsigned long long* out, uint64_t n, void* tmp,
+                       size_t* tmp_bytes, cudaStream_t st) {
+    return cub::DeviceRadixSort::SortKeys(tmp, *tmp_bytes, in, out, static_cast<int>(n), 0, 64, st);
+}
+
+__global__ void split_pairs_kernel(const unsigned long long* pairs, uint64_t n, uint32_t* probe,
+                                   uint32_t* build) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long p = pairs[i];
+        probe[i] = static_cast<uint32_t>(p >> 32);
+        build[i] = static_cast<uint32_t>(p & 0xffffffffull);
+    }
+}
+
+cudaError_t launch_split_pairs(const unsigned long long* pairs, uint64_t n, uint32_t* probe,
+                               uint32_t* build, int sms, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    split_pairs_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(pairs, n, probe, build);
+    return cudaGetLastError();
+}
+
+// Fill a u64 buffer with a value (hash-table EMPTY markers).
+__global__ void fill_u64_kernel(unsigned long long* p, uint64_t n, unsigned long long v) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        p[i] = v;
+}
+
+cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, int sms,
+                            cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    fill_u64_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+// Scatter the occupied slots of a group hash table into a compact array
+// (keys + slot words) for the host to sort; counters[0] = occupied slots.
+__global__ void gather_groups_kernel(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
+                                     unsigned long long* out, uint64_t cap,
+                                     unsigned long long* counter) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nslots;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long* s = htab + i * stride;
+        if (s[0] == ~0ull) continue;
+        const unsigned long long o = atomicAdd(counter, 1ull);
+        if (o < cap)
+            for (uint32_t w = 0; w < stride; ++w) out[o * stride + w] = s[w];
+    }
+}
+
+cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
+                                 unsigned long long* out, uint64_t cap, unsigned long long* counter,
+                                 int sms, cudaStream_t st) {
+    if (nslots == 0) return cudaSuccess;
+    uint64_t blocks = (nslots + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    gather_groups_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(htab, nslots, stride, out,
+                                                                               cap, counter);
+    return cudaGetLastError();
+}
+
+}  // namespace tgp

@@ -1,0 +1,1603 @@
+// capi.cu — implementation of the C ABI declared in include/turbogp_gpu.h:
+// context, resident tables, the query planner that lowers C-ABI descriptors
+// into a Plan, launches, and result decoding. Host code only; kernels live in
+// scan_engine.cu and aux_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "runtime.hpp"
+
+using namespace tgp;
+
+namespace {
+
+constexpr unsigned long long kEmptySlot = ~0ull;
+constexpr uint64_t kDirectMaxGroups = 1ull << 22;
+
+int fail(tgp_ctx* ctx, int st, const std::string& m) {
+    if (ctx) ctx->err = m;
+    return st;
+}
+
+#define TGP_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(ctx, TGP_DEVICE_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TGP_TRY(expr)              \
+    do {                           \
+        int st_ = (expr);          \
+        if (st_ != TGP_OK) return st_; \
+    } while (0)
+
+uint32_t dtype_width(uint32_t dt) {
+    switch (dt) {
+        case DT_U8: return 1;
+        case DT_I32: return 4;
+        case DT_I64:
+        case DT_U64:
+        case DT_F64: return 8;
+        default: return 0;
+    }
+}
+
+bool is_device_ptr(const void* p) {
+    if (p == nullptr) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+uint64_t next_pow2(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+uint32_t log2u(uint64_t p) {
+    uint32_t l = 0;
+    while ((1ull << l) < p) ++l;
+    return l;
+}
+
+// --------------------------------------------------------------------------
+// Scratch arena: one grow-only device buffer carved per call.
+// --------------------------------------------------------------------------
+struct Carve {
+    uint8_t* base;
+    size_t off = 0;
+    size_t cap;
+    template <typename T>
+    T* take(size_t count) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+int arena_reserve(tgp_ctx* ctx, size_t bytes, Carve* out) {
+    bytes = bytes + 4096;
+    if (bytes > ctx->arena.cap) {
+        TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->arena.base) cudaFree(ctx->arena.base);
+        ctx->arena.base = nullptr;
+        ctx->arena.cap = 0;
+        size_t want = std::max(bytes, ctx->arena.cap * 2);
+        if (cudaMalloc(&ctx->arena.base, want) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, TGP_OOM, "device scratch allocation failed");
+        }
+        ctx->arena.cap = want;
+    }
+    out->base = ctx->arena.base;
+    out->off = 0;
+    out->cap = ctx->arena.cap;
+    return TGP_OK;
+}
+
+int pinned_reserve(tgp_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->hpin_cap) return TGP_OK;
+    if (ctx->hpin) cudaFreeHost(ctx->hpin);
+    ctx->hpin = nullptr;
+    ctx->hpin_cap = 0;
+    size_t want = std::max<size_t>(bytes, 1 << 16);
+    if (cudaMallocHost(&ctx->hpin, want) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, TGP_OOM, "pinned host allocation failed");
+    }
+    ctx->hpin_cap = want;
+    return TGP_OK;
+}
+
+// Copies `bytes` from device memory to `dst` (host or device).
+int copy_out(tgp_ctx* ctx, void* dst, const void* src_dev, size_t bytes) {
+    if (bytes == 0) return TGP_OK;
+    TGP_CUDA(cudaMemcpyAsync(dst, src_dev, bytes, cudaMemcpyDefault, ctx->stream));
+    return TGP_OK;
+}
+
+// Reads the device error word and maps kernel error bits to a status.
+int check_kernel_err(tgp_ctx* ctx, uint32_t err) {
+    if (err & kErrWaitTimeout) return fail(ctx, TGP_TIMEOUT, "a bounded device wait gave up");
+    if (err & kErrHashFull) return fail(ctx, TGP_DEVICE_ERROR, "device hash table overflowed");
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Predicate lowering
+// --------------------------------------------------------------------------
+// Interval [a, b] over order keys (signed order: key = cell ^ 2^63, unsigned:
+// key = cell), optionally negated, or a constant.
+struct Interval {
+    bool is_const = false;
+    bool value = false;
+    uint64_t a = 0, b = 0;
+    bool negate = false;
+};
+
+Interval cmp_interval(uint32_t cmp, uint64_t L, uint64_t L2) {
+    Interval iv;
+    const uint64_t MAX = ~0ull;
+    switch (cmp) {
+        case 0: iv.a = L; iv.b = L; break;                                   // EQ
+        case 1: iv.a = L; iv.b = L; iv.negate = true; break;                 // NE
+        case 2:                                                              // LT
+            if (L == 0) { iv.is_const = true; iv.value = false; }
+            else { iv.a = 0; iv.b = L - 1; }
+            break;
+        case 3: iv.a = 0; iv.b = L; break;                                   // LE
+        case 4:                                                              // GT
+            if (L == MAX) { iv.is_const = true; iv.value = false; }
+            else { iv.a = L + 1; iv.b = MAX; }
+            break;
+        case 5: iv.a = L; iv.b = MAX; break;                                 // GE
+        case 6:                                                              // BETWEEN
+            if (L > L2) { iv.is_const = true; iv.value = false; }
+            else { iv.a = L; iv.b = L2; }
+            break;
+        default:                                                             // NOT_BETWEEN
+            if (L > L2) { iv.is_const = true; iv.value = true; }
+            else { iv.a = L; iv.b = L2; iv.negate = true; }
+            break;
+    }
+    return iv;
+}
+
+void set_const(Leaf& lf, bool v) {
+    lf.kind = LK_CONST;
+    lf.negate = v ? 1 : 0;
+}
+
+int lower_leaf(tgp_ctx* ctx, const Column& c, const tgp_pred_node& n, uint8_t slot, Leaf& lf) {
+    std::memset(&lf, 0, sizeof(lf));
+    lf.slot = slot;
+    if (n.cmp > TGP_CMP_NOT_BETWEEN) return fail(ctx, TGP_INVALID_ARG, "bad comparison code");
+    if (c.coltype == TGP_CT_FLOAT) {
+        if (c.dtype != DT_F64) return fail(ctx, TGP_INVALID_ARG, "FLOAT comparison on a non-f64 column");
+        double v, v2;
+        std::memcpy(&v, &n.lit, 8);
+        std::memcpy(&v2, &n.lit2, 8);
+        lf.kind = LK_F64;
+        lf.f1 = v;
+        lf.f2 = v2;
+        static const uint8_t fmap[8] = {FOP_EQ_EPS, FOP_NE, FOP_LT, FOP_LE, FOP_GT, FOP_GE, FOP_BETWEEN,
+                                        FOP_NOT_BETWEEN};
+        lf.fop = fmap[n.cmp];
+        if (n.cmp == TGP_CMP_EQ || n.cmp == TGP_CMP_NE) lf.f2 = 1e-6 * std::max(std::fabs(v), 1.0);
+        return TGP_OK;
+    }
+    const bool sgn = c.coltype == TGP_CT_INT;
+    const uint64_t flip = sgn ? (1ull << 63) : 0ull;
+    Interval iv = cmp_interval(n.cmp, n.lit ^ flip, n.lit2 ^ flip);
+    if (iv.is_const) {
+        set_const(lf, iv.value);
+        return TGP_OK;
+    }
+    lf.negate = iv.negate ? 1 : 0;
+    if (c.width == 8) {
+        lf.kind = LK_64;
+        lf.xor64 = flip;
+        lf.lo64 = iv.a;
+        lf.span64 = iv.b - iv.a;
+        return TGP_OK;
+    }
+    // Narrow columns: map the order-key interval onto the 32-bit physical key.
+    uint64_t a = iv.a, b = iv.b;
+    uint32_t lo32 = 0, hi32 = 0;
+    bool empty = false;
+    if (c.dtype == DT_U8) {
+        const uint64_t base = sgn ? (1ull << 63) : 0ull;  // order key of cell 0
+        const uint64_t ka = std::max(a, base), kb = std::min(b, base + 255);
+        if (ka > kb) empty = true;
+        else { lo32 = static_cast<uint32_t>(ka - base); hi32 = static_cast<uint32_t>(kb - base); }
+        lf.kind = LK_U8;
+        lf.xor32 = 0;
+    } else {  // DT_I32
+        lf.kind = LK_I32;
+        if (sgn) {
+            const uint64_t base = (1ull << 63) - (1ull << 31);  // order key of INT32_MIN
+            const uint64_t top = (1ull << 63) + (1ull << 31) - 1;
+            const uint64_t ka = std::max(a, base), kb = std::min(b, top);
+            if (ka > kb) empty = true;
+            else { lo32 = static_cast<uint32_t>(ka - base); hi32 = static_cast<uint32_t>(kb - base); }
+            lf.xor32 = 0x80000000u;
+        } else {
+            // cells: [0, 2^31-1] (v >= 0) and [2^64-2^31, 2^64-1] (v < 0); key32 = (u32)v.
+            const uint64_t neg0 = ~0ull - (1ull << 31) + 1;  // 2^64 - 2^31
+            const uint64_t shift = ~0ull - (1ull << 32) + 1;  // 2^64 - 2^32
+            uint64_t ca, cb;
+            if (a <= 0x7fffffffull) ca = a;
+            else if (a <= neg0) ca = 0x80000000ull;
+            else ca = a - shift;
+            if (b >= neg0) cb = b - shift;
+            else if (b >= 0x7fffffffull) cb = 0x7fffffffull;
+            else cb = b;
+            if (ca > cb) empty = true;
+            else { lo32 = static_cast<uint32_t>(ca); hi32 = static_cast<uint32_t>(cb); }
+            lf.xor32 = 0;
+        }
+    }
+    if (empty) {
+        set_const(lf, iv.negate);
+        return TGP_OK;
+    }
+    lf.lo32 = lo32;
+    lf.span32 = hi32 - lo32;
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Query builder
+// --------------------------------------------------------------------------
+struct Bound {  // |value| bound; exact in 128-bit
+    __int128 lo, hi;
+};
+
+__int128 abs128(__int128 x) { return x < 0 ? -x : x; }
+
+struct Builder {
+    tgp_ctx* ctx;
+    const Table* T;
+    const Table* B = nullptr;       // build table of a join
+    const JoinTable* J = nullptr;
+    Plan P;
+    std::vector<int> col2slot;
+    uint64_t max_abs_val = 0;       // max |per-row value| over all values (saturating)
+    bool unbounded = false;         // some value may exceed 2^62 in magnitude
+
+    Builder(tgp_ctx* c, const Table* t) : ctx(c), T(t) {
+        std::memset(&P, 0, sizeof(P));
+        col2slot.assign(t->cols.size(), -1);
+        P.nrows = t->rows;
+        P.jslot = -1;
+        P.flush_limit = ~0ull;
+    }
+
+    int slot_of(uint32_t col, int* out) {
+        if (col >= T->cols.size()) return fail(ctx, TGP_INVALID_ARG, "column index out of range");
+        if (col2slot[col] < 0) {
+            if (P.nslots >= static_cast<uint32_t>(kMaxSlots))
+                return fail(ctx, TGP_UNSUPPORTED, "query references more than 8 columns");
+            const Column& c = T->cols[col];
+            SlotDesc& s = P.slot[P.nslots];
+            s.ptr = c.dptr;
+            s.width = c.width;
+            s.dtype = c.dtype;
+            s.smem_off = P.stage_bytes;
+            P.stage_bytes += kTileRows * c.width;
+            col2slot[col] = static_cast<int>(P.nslots++);
+        }
+        *out = col2slot[col];
+        return TGP_OK;
+    }
+
+    int add_pred(const tgp_pred_node* pred, uint32_t npred) {
+        if (npred == 0) return TGP_OK;
+        if (pred == nullptr) return fail(ctx, TGP_INVALID_ARG, "null predicate program");
+        if (npred > static_cast<uint32_t>(kMaxPredOps)) return fail(ctx, TGP_UNSUPPORTED, "predicate program too long");
+        int depth = 0, maxdepth = 0;
+        uint32_t nand = 0;
+        bool only_and = true;
+        for (uint32_t i = 0; i < npred; ++i) {
+            const tgp_pred_node& n = pred[i];
+            switch (n.kind) {
+                case TGP_PN_LEAF: {
+                    if (P.nleaf >= static_cast<uint32_t>(kMaxLeaves))
+                        return fail(ctx, TGP_UNSUPPORTED, "more than 16 predicate leaves");
+                    int slot;
+                    TGP_TRY(slot_of(n.column, &slot));
+                    TGP_TRY(lower_leaf(ctx, T->cols[n.column], n, static_cast<uint8_t>(slot), P.leaf[P.nleaf]));
+                    P.ops[i] = static_cast<uint8_t>(P.nleaf++);
+                    ++depth;
+                    break;
+                }
+                case TGP_PN_AND:
+                case TGP_PN_OR:
+                    if (depth < 2) return fail(ctx, TGP_INVALID_ARG, "AND/OR needs two operands");
+                    --depth;
+                    P.ops[i] = n.kind == TGP_PN_AND ? OP_AND : OP_OR;
+                    if (n.kind == TGP_PN_AND) ++nand; else only_and = false;
+                    break;
+                case TGP_PN_NOT:
+                    if (depth < 1) return fail(ctx, TGP_INVALID_ARG, "NOT needs one operand");
+                    P.ops[i] = OP_NOT;
+                    only_and = false;
+                    break;
+                default:
+                    return fail(ctx, TGP_INVALID_ARG, "bad predicate node kind");
+            }
+            maxdepth = std::max(maxdepth, depth);
+        }
+        if (depth != 1) return fail(ctx, TGP_INVALID_ARG, "predicate program must leave one value");
+        if (maxdepth > 8) return fail(ctx, TGP_UNSUPPORTED, "predicate program deeper than 8");
+        P.nops = npred;
+        P.all_and = (only_and && nand + 1 == P.nleaf) ? 1u : 0u;
+        return TGP_OK;
+    }
+
+    int lower_factor(const tgp_factor& f, Factor& out, __int128* blo, __int128* bhi) {
+        std::memset(&out, 0, sizeof(out));
+        out.mul = f.mul;
+        out.add = f.add;
+        out.slot = -1;
+        if (f.column < 0) {
+            *blo = *bhi = static_cast<__int128>(f.add);
+            return TGP_OK;
+        }
+        const Table* S = T;
+        if (f.side == TGP_SIDE_BUILD) {
+            if (!B) return fail(ctx, TGP_INVALID_ARG, "build-side column without a join");
+            S = B;
+        } else if (f.side != TGP_SIDE_PROBE) {
+            return fail(ctx, TGP_INVALID_ARG, "bad side");
+        }
+        if (static_cast<uint32_t>(f.column) >= S->cols.size()) return fail(ctx, TGP_INVALID_ARG, "factor column out of range");
+        const Column& c = S->cols[f.column];
+        if (c.coltype == TGP_CT_FLOAT) return fail(ctx, TGP_UNSUPPORTED, "aggregate arguments over FLOAT columns");
+        if (f.side == TGP_SIDE_BUILD) {
+            out.build_side = 1;
+            out.dtype = static_cast<uint8_t>(c.dtype);
+            out.bptr = c.dptr;
+        } else {
+            int slot;
+            TGP_TRY(slot_of(static_cast<uint32_t>(f.column), &slot));
+            out.slot = static_cast<int8_t>(slot);
+        }
+        const __int128 m = f.mul, a = f.add;
+        const __int128 x0 = m * c.min + a, x1 = m * c.max + a;
+        *blo = std::min(x0, x1);
+        *bhi = std::max(x0, x1);
+        return TGP_OK;
+    }
+
+    // Returns the value index for (kind, factors), deduplicating.
+    int add_value(uint8_t kind, const tgp_agg& a, int* idx) {
+        if (a.nfactors > static_cast<uint32_t>(kMaxFactors)) return fail(ctx, TGP_UNSUPPORTED, "more than 4 factors");
+        ValDesc v;
+        std::memset(&v, 0, sizeof(v));
+        v.kind = kind;
+        v.nf = static_cast<uint8_t>(a.nfactors);
+        __int128 lo = 1, hi = 1;
+        bool big = false;
+        const __int128 lim = static_cast<__int128>(1) << 63;
+        for (uint32_t f = 0; f < a.nfactors; ++f) {
+            __int128 flo, fhi;
+            TGP_TRY(lower_factor(a.f[f], v.f[f], &flo, &fhi));
+            if (abs128(flo) >= lim || abs128(fhi) >= lim) big = true;
+            if (f == 0) {
+                lo = flo;
+                hi = fhi;
+            } else if (!big) {
+                const __int128 c[4] = {lo * flo, lo * fhi, hi * flo, hi * fhi};
+                lo = *std::min_element(c, c + 4);
+                hi = *std::max_element(c, c + 4);
+                if (abs128(lo) >= lim || abs128(hi) >= lim) big = true;
+            }
+        }
+        if (big) {
+            P.check_ovf = 1;
+            unbounded = true;
+        } else {
+            const __int128 m = std::max(abs128(lo), abs128(hi));
+            if (kind == VK_SUM && m > (static_cast<__int128>(1) << 62)) unbounded = true;
+            if (kind == VK_SUM || kind == VK_COUNT_NZ) {
+                const uint64_t mm = kind == VK_COUNT_NZ ? 1ull : static_cast<uint64_t>(m);
+                max_abs_val = std::max(max_abs_val, mm);
+            }
+        }
+        for (uint32_t i = 0; i < P.nval; ++i) {
+            if (std::memcmp(&P.val[i], &v, sizeof(v)) == 0) {
+                *idx = static_cast<int>(i);
+                return TGP_OK;
+            }
+        }
+        if (P.nval >= static_cast<uint32_t>(kMaxVals)) return fail(ctx, TGP_UNSUPPORTED, "more than 8 distinct aggregates");
+        P.val[P.nval] = v;
+        *idx = static_cast<int>(P.nval++);
+        return TGP_OK;
+    }
+};
+
+// Per-aggregate mapping to accumulator slots.
+struct AggMap {
+    uint32_t func;
+    int val;  // value index, -1 for COUNT_STAR
+};
+
+int lower_aggs(Builder& b, const tgp_agg* aggs, uint32_t nagg, std::vector<AggMap>* map) {
+    if (nagg > 0 && aggs == nullptr) return fail(b.ctx, TGP_INVALID_ARG, "null aggregate list");
+    map->clear();
+    for (uint32_t i = 0; i < nagg; ++i) {
+        const tgp_agg& a = aggs[i];
+        AggMap m{a.func, -1};
+        switch (a.func) {
+            case TGP_AGG_COUNT_STAR: break;
+            case TGP_AGG_COUNT_NONZERO: TGP_TRY(b.add_value(VK_COUNT_NZ, a, &m.val)); break;
+            case TGP_AGG_SUM:
+            case TGP_AGG_AVG: TGP_TRY(b.add_value(VK_SUM, a, &m.val)); break;
+            case TGP_AGG_MIN: TGP_TRY(b.add_value(VK_MIN, a, &m.val)); break;
+            case TGP_AGG_MAX: TGP_TRY(b.add_value(VK_MAX, a, &m.val)); break;
+            default: return fail(b.ctx, TGP_INVALID_ARG, "bad aggregate function");
+        }
+        map->push_back(m);
+    }
+    return TGP_OK;
+}
+
+double i128_to_f64(uint64_t lo, int64_t hi) {
+    const __int128 v = (static_cast<__int128>(hi) << 64) | static_cast<__int128>(lo);
+    return static_cast<double>(v);
+}
+
+void fill_value(const AggMap& m, const unsigned long long* slot /* [nv1][2] */, const Plan& P,
+                tgp_agg_value* out) {
+    const uint64_t cnt = slot[0];
+    out->count = cnt;
+    if (m.val < 0) {
+        out->lo = cnt;
+        out->hi = 0;
+        out->as_f64 = static_cast<double>(cnt);
+        return;
+    }
+    const unsigned long long* s = slot + 2 * (m.val + 1);
+    const uint8_t kind = P.val[m.val].kind;
+    if (kind == VK_MIN || kind == VK_MAX) {
+        const int64_t v = static_cast<int64_t>(s[0]);
+        out->lo = static_cast<uint64_t>(v);
+        out->hi = v < 0 ? -1 : 0;
+        out->as_f64 = static_cast<double>(v);
+        return;
+    }
+    out->lo = s[0];
+    out->hi = static_cast<int64_t>(s[1]);
+    const double f = i128_to_f64(out->lo, out->hi);
+    if (m.func == TGP_AGG_AVG) out->as_f64 = cnt ? f / static_cast<double>(cnt) : 0.0;
+    else out->as_f64 = f;
+}
+
+// Chooses shared-memory stages for a plan given per-mode scratch bytes.
+int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes) {
+    const size_t static_smem = scan_kernel_static_smem();
+    const size_t budget = ctx->max_dyn_smem > static_smem ? ctx->max_dyn_smem - static_smem : 0;
+    size_t stage = P.stage_bytes;
+    if (stage == 0) {
+        // Nothing to stage (e.g. COUNT(*) without WHERE): stage one tiny dummy.
+        stage = 0;
+    }
+    const size_t per_cta = budget / static_cast<size_t>(std::max(1, ctx->ctas_per_sm));
+    size_t avail = per_cta > kBarrierBytes + extra_bytes ? per_cta - kBarrierBytes - extra_bytes : 0;
+    uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1;
+    if (S == 0) {
+        // Fall back to a single CTA per SM.
+        avail = budget > kBarrierBytes + extra_bytes ? budget - kBarrierBytes - extra_bytes : 0;
+        S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1;
+        if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "query does not fit in shared memory");
+    }
+    P.nstages = S;
+    P.extra_off = static_cast<uint32_t>(kBarrierBytes + static_cast<size_t>(S) * stage);
+    P.extra_off = (P.extra_off + 127u) & ~127u;
+    P.smem_bytes = static_cast<uint32_t>(P.extra_off + extra_bytes);
+    return TGP_OK;
+}
+
+int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
+    const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
+    if (ntiles == 0) return TGP_OK;
+    int occ = scan_occupancy(mode, acc128, P.smem_bytes);
+    if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
+    const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * occ);
+    std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+    if (ctx->profile) {
+        if (ctx->prof_used == ctx->prof_events.size()) {
+            std::pair<cudaEvent_t, cudaEvent_t> p;
+            TGP_CUDA(cudaEventCreate(&p.first));
+            TGP_CUDA(cudaEventCreate(&p.second));
+            ctx->prof_events.push_back(p);
+        }
+        ev = &ctx->prof_events[ctx->prof_used++];
+        TGP_CUDA(cudaEventRecord(ev->first, ctx->stream));
+    }
+    cudaError_t e = launch_scan(P, mode, acc128, static_cast<int>(grid), ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("scan launch: ") + cudaGetErrorString(e));
+    if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
+    return TGP_OK;
+}
+
+int get_table(tgp_ctx* ctx, tgp_table_id id, const Table** out) {
+    auto it = ctx->tables.find(id);
+    if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
+    *out = &it->second;
+    return TGP_OK;
+}
+
+// Device buffers every scan call needs: accumulators, counters, error word.
+struct ScanScratch {
+    unsigned long long* acc = nullptr;
+    unsigned long long* counters = nullptr;
+    uint32_t* err = nullptr;
+};
+
+// Initial accumulator image: per group [count][v lo][v hi]...; MIN/MAX start
+// at the identity of their operation.
+void init_acc_image(const Plan& P, uint64_t ngroups, std::vector<unsigned long long>* img) {
+    const uint32_t nv1 = P.nval + 1;
+    img->assign(ngroups * nv1 * 2, 0ull);
+    for (uint32_t v = 0; v < P.nval; ++v) {
+        unsigned long long init = 0;
+        if (P.val[v].kind == VK_MIN) init = 0x7fffffffffffffffull;
+        else if (P.val[v].kind == VK_MAX) init = 0x8000000000000000ull;
+        if (!init) continue;
+        for (uint64_t g = 0; g < ngroups; ++g) (*img)[(g * nv1 + v + 1) * 2] = init;
+    }
+}
+
+int upload(tgp_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return TGP_OK;
+    TGP_TRY(pinned_reserve(ctx, bytes));
+    std::memcpy(ctx->hpin, src, bytes);
+    TGP_CUDA(cudaMemcpyAsync(dst, ctx->hpin, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TGP_OK;
+}
+
+}  // namespace
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+const char* tgp_status_string(int s) {
+    switch (s) {
+        case TGP_OK: return "OK";
+        case TGP_INVALID_ARG: return "INVALID_ARG";
+        case TGP_OOM: return "OOM";
+        case TGP_UNSUPPORTED: return "UNSUPPORTED";
+        case TGP_TIMEOUT: return "TIMEOUT";
+        case TGP_DEVICE_ERROR: return "DEVICE_ERROR";
+        case TGP_NOT_FOUND: return "NOT_FOUND";
+        case TGP_CAPACITY: return "CAPACITY";
+        default: return "UNKNOWN";
+    }
+}
+
+int tgp_init(tgp_ctx** out, int device) {
+    if (!out) return TGP_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return TGP_DEVICE_ERROR;
+    }
+    tgp_ctx* ctx = new (std::nothrow) tgp_ctx();
+    if (!ctx) return TGP_OOM;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return TGP_DEVICE_ERROR;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete ctx;
+        return TGP_DEVICE_ERROR;
+    }
+    if (prop.major < 10) {
+        delete ctx;
+        return TGP_UNSUPPORTED;  // built for sm_100a only
+    }
+    ctx->sms = prop.multiProcessorCount;
+    ctx->max_dyn_smem = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return TGP_DEVICE_ERROR;
+    }
+    if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("TGP_MAX_STAGES"))
+        ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
+    *out = ctx;
+    return TGP_OK;
+}
+
+int tgp_shutdown(tgp_ctx* ctx) {
+    if (!ctx) return TGP_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->tables)
+        for (auto& c : kv.second.cols)
+            if (c.owned && c.dptr) cudaFree(c.dptr);
+    for (auto& kv : ctx->joins)
+        if (kv.second.tab) cudaFree(kv.second.tab);
+    for (void* h : ctx->hash_handles) {
+        JoinTable* J = static_cast<JoinTable*>(h);
+        if (J->tab) cudaFree(J->tab);
+        delete J;
+    }
+    if (ctx->arena.base) cudaFree(ctx->arena.base);
+    if (ctx->kin) cudaFree(ctx->kin);
+    if (ctx->hpin) cudaFreeHost(ctx->hpin);
+    for (auto& p : ctx->prof_events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TGP_OK;
+}
+
+const char* tgp_last_error(const tgp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* tgp_ctx_stream(tgp_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int tgp_ctx_sm_count(const tgp_ctx* ctx) { return ctx ? ctx->sms : 0; }
+
+int tgp_sync(tgp_ctx* ctx) {
+    if (!ctx) return TGP_INVALID_ARG;
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TGP_OK;
+}
+
+int tgp_profile_enable(tgp_ctx* ctx, int on) {
+    if (!ctx) return TGP_INVALID_ARG;
+    ctx->profile = on != 0;
+    ctx->prof_used = 0;
+    return TGP_OK;
+}
+
+int tgp_profile_read(tgp_ctx* ctx, uint64_t* launches, double* total_ms) {
+    if (!ctx || !launches || !total_ms) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    double t = 0.0;
+    for (size_t i = 0; i < ctx->prof_used; ++i) {
+        float ms = 0.f;
+        TGP_CUDA(cudaEventElapsedTime(&ms, ctx->prof_events[i].first, ctx->prof_events[i].second));
+        t += ms;
+    }
+    *launches = ctx->prof_used;
+    *total_ms = t;
+    ctx->prof_used = 0;
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Tables
+// --------------------------------------------------------------------------
+static int compute_stats(tgp_ctx* ctx, Table& t) {
+    if (t.cols.empty()) return TGP_OK;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, t.cols.size() * 16, &cv));
+    long long* mm = cv.take<long long>(2 * t.cols.size());
+    std::vector<long long> init(2 * t.cols.size());
+    for (size_t i = 0; i < t.cols.size(); ++i) {
+        init[2 * i] = 0x7fffffffffffffffll;
+        init[2 * i + 1] = static_cast<long long>(0x8000000000000000ull);
+    }
+    TGP_TRY(upload(ctx, mm, init.data(), init.size() * 8));
+    for (size_t i = 0; i < t.cols.size(); ++i) {
+        TGP_CUDA(launch_column_minmax(t.cols[i].dptr, t.cols[i].dtype, t.rows, mm + 2 * i, ctx->sms, ctx->stream));
+    }
+    std::vector<long long> res(2 * t.cols.size());
+    TGP_CUDA(cudaMemcpyAsync(res.data(), mm, res.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < t.cols.size(); ++i) {
+        t.cols[i].min = res[2 * i];
+        t.cols[i].max = res[2 * i + 1];
+        if (t.rows == 0) {
+            t.cols[i].min = 0;
+            t.cols[i].max = 0;
+        }
+    }
+    return TGP_OK;
+}
+
+static int register_impl(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols, uint64_t rows,
+                         bool copy, tgp_table_id* out) {
+    if (!ctx || !out || (ncols && !cols)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (rows >= (1ull << 32)) return fail(ctx, TGP_UNSUPPORTED, "tables hold fewer than 2^32 rows (u32 row ids)");
+    TGP_CUDA(cudaSetDevice(ctx->device));
+    Table t;
+    t.rows = rows;
+    for (uint32_t i = 0; i < ncols; ++i) {
+        Column c;
+        c.dtype = cols[i].dtype;
+        c.coltype = cols[i].coltype;
+        c.width = dtype_width(c.dtype);
+        if (c.width == 0) return fail(ctx, TGP_INVALID_ARG, "bad column dtype");
+        if (c.coltype > TGP_CT_FLOAT) return fail(ctx, TGP_INVALID_ARG, "bad column coltype");
+        if (rows && !cols[i].data) return fail(ctx, TGP_INVALID_ARG, "null column data");
+        const size_t bytes = rows * c.width;
+        if (copy) {
+            // Pad to whole tiles so bulk copies of the last full tile stay in bounds.
+            const size_t alloc = std::max<size_t>(16, ((bytes + 255) / 256) * 256);
+            if (cudaMalloc(&c.dptr, alloc) != cudaSuccess) {
+                cudaGetLastError();
+                for (auto& p : t.cols) cudaFree(p.dptr);
+                return fail(ctx, TGP_OOM, "column allocation failed");
+            }
+            c.owned = true;
+            if (bytes) {
+                cudaError_t e = cudaMemcpyAsync(c.dptr, cols[i].data, bytes, cudaMemcpyDefault, ctx->stream);
+                if (e != cudaSuccess) {
+                    for (auto& p : t.cols) cudaFree(p.dptr);
+                    cudaFree(c.dptr);
+                    return fail(ctx, TGP_DEVICE_ERROR, cudaGetErrorString(e));
+                }
+            }
+        } else {
+            if (rows && !is_device_ptr(cols[i].data)) return fail(ctx, TGP_INVALID_ARG, "column is not device memory");
+            if (reinterpret_cast<uintptr_t>(cols[i].data) % 16 != 0)
+                return fail(ctx, TGP_INVALID_ARG, "device column not 16-byte aligned");
+            c.dptr = static_cast<uint8_t*>(const_cast<void*>(cols[i].data));
+        }
+        t.cols.push_back(c);
+    }
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    int st = compute_stats(ctx, t);
+    if (st != TGP_OK) {
+        for (auto& c : t.cols)
+            if (c.owned) cudaFree(c.dptr);
+        return st;
+    }
+    const uint64_t id = ctx->next_id++;
+    ctx->tables.emplace(id, std::move(t));
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_table_register(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols, uint64_t rows,
+                       tgp_table_id* out) {
+    return register_impl(ctx, cols, ncols, rows, true, out);
+}
+
+int tgp_table_register_device(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols, uint64_t rows,
+                              tgp_table_id* out) {
+    return register_impl(ctx, cols, ncols, rows, false, out);
+}
+
+int tgp_table_reload(tgp_ctx* ctx, tgp_table_id id, const tgp_column_desc* cols, uint32_t ncols) {
+    if (!ctx || (ncols && !cols)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    auto it = ctx->tables.find(id);
+    if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
+    Table& t = it->second;
+    if (ncols != t.cols.size()) return fail(ctx, TGP_INVALID_ARG, "column count differs");
+    for (uint32_t i = 0; i < ncols; ++i) {
+        if (!t.cols[i].owned) return fail(ctx, TGP_INVALID_ARG, "reload of a borrowed device table");
+        if (cols[i].dtype != t.cols[i].dtype) return fail(ctx, TGP_INVALID_ARG, "column dtype differs");
+        if (t.rows)
+            TGP_CUDA(cudaMemcpyAsync(t.cols[i].dptr, cols[i].data, t.rows * t.cols[i].width, cudaMemcpyDefault,
+                                     ctx->stream));
+    }
+    return compute_stats(ctx, t);
+}
+
+int tgp_table_drop(tgp_ctx* ctx, tgp_table_id id) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->tables.find(id);
+    if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (auto& c : it->second.cols)
+        if (c.owned) cudaFree(c.dptr);
+    ctx->tables.erase(it);
+    return TGP_OK;
+}
+
+int tgp_table_info(tgp_ctx* ctx, tgp_table_id id, uint64_t* rows, uint32_t* ncols) {
+    const Table* t;
+    TGP_TRY(get_table(ctx, id, &t));
+    if (rows) *rows = t->rows;
+    if (ncols) *ncols = static_cast<uint32_t>(t->cols.size());
+    return TGP_OK;
+}
+
+int tgp_table_column_stats(tgp_ctx* ctx, tgp_table_id id, uint32_t col, int64_t* mn, int64_t* mx) {
+    const Table* t;
+    TGP_TRY(get_table(ctx, id, &t));
+    if (col >= t->cols.size()) return fail(ctx, TGP_INVALID_ARG, "column index out of range");
+    if (mn) *mn = t->cols[col].min;
+    if (mx) *mx = t->cols[col].max;
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Filter → bitmap / row ids
+// --------------------------------------------------------------------------
+static int filter_impl(tgp_ctx* ctx, const Table* T, const tgp_pred_node* pred, uint32_t npred,
+                       uint8_t* bitmap_out, uint32_t* rowids_out, uint64_t rowids_cap, uint64_t* count_out,
+                       uint32_t first_words /* >0: only first words into bitmap_out (kernel table) */) {
+    Builder b(ctx, T);
+    TGP_TRY(b.add_pred(pred, npred));
+    const uint64_t ntiles = (T->rows + kTileRows - 1) / kTileRows;
+    const uint64_t nwords = (T->rows + 31) / 32;
+    const bool need_words = bitmap_out || rowids_out || first_words;
+    const uint64_t words = first_words ? std::min<uint64_t>(first_words, nwords) : (need_words ? nwords : 0);
+    size_t cub_bytes = 0;
+    if (rowids_out && ntiles) tile_prefix(nullptr, nullptr, ntiles, nullptr, &cub_bytes, ctx->stream);
+    const bool host_rowids = rowids_out && !is_device_ptr(rowids_out);
+    // Host row-id output is compacted into scratch first (worst case: all rows).
+    const uint64_t rowid_scratch = host_rowids ? std::min<uint64_t>(T->rows, rowids_cap) : 0;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, 64 + words * 4 + ntiles * 12 + cub_bytes + rowid_scratch * 4 + 2048, &cv));
+    ScanScratch ss;
+    ss.counters = cv.take<unsigned long long>(4);
+    ss.err = cv.take<uint32_t>(4);
+    uint32_t* bm = cv.take<uint32_t>(std::max<uint64_t>(words, 1));
+    uint32_t* tc = cv.take<uint32_t>(std::max<uint64_t>(ntiles, 1));
+    unsigned long long* tb = cv.take<unsigned long long>(std::max<uint64_t>(ntiles, 1));
+    void* cub_tmp = cv.take<uint8_t>(cub_bytes + 16);
+    uint32_t* rid_tmp = cv.take<uint32_t>(std::max<uint64_t>(rowid_scratch, 1));
+    TGP_CUDA(cudaMemsetAsync(ss.counters, 0, 32 + 16, ctx->stream));
+    if (words) TGP_CUDA(cudaMemsetAsync(bm, 0, words * 4, ctx->stream));
+    Plan& P = b.P;
+    P.bitmap = bm;
+    P.bitmap_words = static_cast<uint32_t>(std::min<uint64_t>(words, 0xffffffffull));
+    P.tile_counts = rowids_out ? tc : nullptr;
+    P.counters = ss.counters;
+    P.err = ss.err;
+    TGP_TRY(size_smem(ctx, P, 0));
+    TGP_TRY(launch(ctx, P, MODE_FILTER, false));
+    unsigned long long cnt = 0;
+    uint32_t err = 0;
+    TGP_CUDA(cudaMemcpyAsync(&cnt, ss.counters, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaMemcpyAsync(&err, ss.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    TGP_TRY(check_kernel_err(ctx, err));
+    if (count_out) *count_out = cnt;
+    if (first_words) {
+        TGP_TRY(copy_out(ctx, bitmap_out, bm, words * 4));
+        TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+        return TGP_OK;
+    }
+    if (bitmap_out) TGP_TRY(copy_out(ctx, bitmap_out, bm, (T->rows + 7) / 8));
+    if (rowids_out) {
+        if (cnt > rowids_cap) {
+            TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+            return fail(ctx, TGP_CAPACITY, "row-id buffer too small");
+        }
+        if (ntiles && cnt) {
+            TGP_CUDA(tile_prefix(tc, tb, ntiles, cub_tmp, &cub_bytes, ctx->stream));
+            if (!host_rowids) {
+                TGP_CUDA(launch_compact(bm, nwords, ntiles, tb, rowids_out, rowids_cap, ctx->stream));
+            } else {
+                TGP_CUDA(launch_compact(bm, nwords, ntiles, tb, rid_tmp, cnt, ctx->stream));
+                TGP_TRY(copy_out(ctx, rowids_out, rid_tmp, cnt * 4));
+            }
+        }
+    }
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TGP_OK;
+}
+
+int tgp_filter(tgp_ctx* ctx, tgp_table_id table, const tgp_pred_node* pred, uint32_t npred, uint8_t* bitmap_out,
+               uint32_t* rowids_out, uint64_t rowids_cap, uint64_t* count_out) {
+    if (!ctx) return TGP_INVALID_ARG;
+    const Table* T;
+    TGP_TRY(get_table(ctx, table, &T));
+    return filter_impl(ctx, T, pred, npred, bitmap_out, rowids_out, rowids_cap, count_out, 0);
+}
+
+// --------------------------------------------------------------------------
+// Aggregation queries
+// --------------------------------------------------------------------------
+static int join_lookup(tgp_ctx* ctx, tgp_join_id id, const JoinTable** out) {
+    auto it = ctx->joins.find(id);
+    if (it == ctx->joins.end()) return fail(ctx, TGP_NOT_FOUND, "unknown join id");
+    *out = &it->second;
+    return TGP_OK;
+}
+
+static void attach_join(Plan& P, const JoinTable& J, int key_slot) {
+    P.jtab = J.tab;
+    P.jmask = J.cap - 1;
+    P.jlog2 = J.log2;
+    P.jwide = J.wide ? 1u : 0u;
+    P.jslot = key_slot;
+    P.jkmin = J.kmin;
+    // An empty build side matches nothing: make every key fall out of range.
+    P.jkrange = J.empty_range ? 0 : J.krange;
+    if (J.empty_range) P.jkmin = 0;
+}
+
+int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
+                tgp_query_result* result) {
+    if (!ctx || !q || !result) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    std::memset(result, 0, sizeof(*result));
+    const Table* T;
+    TGP_TRY(get_table(ctx, q->table, &T));
+    Builder b(ctx, T);
+    const JoinTable* J = nullptr;
+    if (q->join) {
+        TGP_TRY(join_lookup(ctx, q->join, &J));
+        TGP_TRY(get_table(ctx, J->build_table, &b.B));
+        b.J = J;
+    }
+    TGP_TRY(b.add_pred(q->pred, q->npred));
+    if (J) {
+        if (q->probe_key_column >= T->cols.size()) return fail(ctx, TGP_INVALID_ARG, "probe key column out of range");
+        if (T->cols[q->probe_key_column].coltype == TGP_CT_FLOAT)
+            return fail(ctx, TGP_UNSUPPORTED, "FLOAT join keys");
+        int ks;
+        TGP_TRY(b.slot_of(q->probe_key_column, &ks));
+        attach_join(b.P, *J, ks);
+    }
+    std::vector<AggMap> amap;
+    TGP_TRY(lower_aggs(b, q->aggs, q->nagg, &amap));
+    Plan& P = b.P;
+    const uint32_t nv1 = P.nval + 1;
+
+    // Group keys.
+    if (q->ngroup > static_cast<uint32_t>(kMaxGroupKeys)) return fail(ctx, TGP_UNSUPPORTED, "more than 4 group keys");
+    if (q->ngroup && !q->group) return fail(ctx, TGP_INVALID_ARG, "null group key list");
+    std::vector<uint64_t> dom(q->ngroup);
+    std::vector<int64_t> kmin(q->ngroup);
+    unsigned __int128 D = 1;
+    uint32_t total_bits = 0;
+    std::vector<uint32_t> bits(q->ngroup);
+    for (uint32_t k = 0; k < q->ngroup; ++k) {
+        const tgp_group_key& gk = q->group[k];
+        const Table* S = gk.side == TGP_SIDE_BUILD ? b.B : T;
+        if (!S) return fail(ctx, TGP_INVALID_ARG, "build-side group key without a join");
+        if (gk.column >= S->cols.size()) return fail(ctx, TGP_INVALID_ARG, "group column out of range");
+        const Column& c = S->cols[gk.column];
+        GKey& K = P.gkey[k];
+        std::memset(&K, 0, sizeof(K));
+        if (gk.side == TGP_SIDE_BUILD) {
+            K.build_side = 1;
+            K.dtype = static_cast<uint8_t>(c.dtype);
+            K.bptr = c.dptr;
+            K.slot = -1;
+        } else {
+            int s;
+            TGP_TRY(b.slot_of(gk.column, &s));
+            K.slot = static_cast<int8_t>(s);
+        }
+        K.min = c.min;
+        kmin[k] = c.min;
+        const uint64_t range = static_cast<uint64_t>(c.max) - static_cast<uint64_t>(c.min);
+        dom[k] = range == ~0ull ? 0 : range + 1;  // 0 = full 64-bit domain
+        D = dom[k] ? D * dom[k] : (static_cast<unsigned __int128>(1) << 64) * D;
+        uint32_t bw = 0;
+        while (bw < 64 && (range >> bw) != 0) ++bw;
+        bits[k] = bw;
+        total_bits += bw;
+    }
+    P.ngkey = q->ngroup;
+
+    uint32_t mode;
+    bool acc128 = false;
+    uint64_t ngroups_direct = 1;
+    size_t extra = 0;
+    const bool join = J != nullptr;
+    if (q->ngroup == 0) {
+        mode = MODE_SCALAR;
+        P.ngroups = 1;
+    } else if (D <= kDirectMaxGroups) {
+        ngroups_direct = static_cast<uint64_t>(D);
+        P.ngroups = static_cast<uint32_t>(ngroups_direct);
+        uint64_t stride = 1;
+        for (int k = static_cast<int>(q->ngroup) - 1; k >= 0; --k) {
+            P.gkey[k].stride = stride;
+            stride *= dom[k];
+        }
+        acc128 = b.unbounded;
+        const size_t priv = static_cast<size_t>(ngroups_direct) * nv1 * kThreads * 8 * (acc128 ? 2 : 1);
+        const size_t shared_tab = static_cast<size_t>(ngroups_direct) * nv1 * 16;
+        const size_t budget = ctx->max_dyn_smem - scan_kernel_static_smem() - kBarrierBytes;
+        if (priv + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+            mode = MODE_GROUP_PRIVATE;
+            extra = priv;
+            if (!acc128) {
+                const uint64_t lim = b.max_abs_val ? (0x7fffffffffffffffull / b.max_abs_val) : ~0ull;
+                P.flush_limit = std::max<uint64_t>(1, lim);
+            }
+        } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+            mode = MODE_GROUP_SHARED;
+            extra = shared_tab;
+            acc128 = false;
+        } else {
+            mode = MODE_GROUP_GLOBAL;
+            acc128 = false;
+        }
+    } else {
+        mode = MODE_GROUP_HASH;
+        if (total_bits > 64 || (q->ngroup > 1 && total_bits > 63))
+            return fail(ctx, TGP_UNSUPPORTED, "group key tuple wider than 63 bits");
+        uint32_t shift = 0;
+        for (int k = static_cast<int>(q->ngroup) - 1; k >= 0; --k) {
+            P.gkey[k].shift = static_cast<uint8_t>(shift);
+            shift += bits[k];
+        }
+        if (q->ngroup == 1 && bits[0] == 64 && dom[0] == 0)
+            return fail(ctx, TGP_UNSUPPORTED, "group key spans all 2^64 values");
+    }
+
+    // Hash table sizing: twice the bound on distinct groups.
+    uint64_t hcap = 0;
+    if (mode == MODE_GROUP_HASH) {
+        const unsigned __int128 est = std::min<unsigned __int128>(D, static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
+                                                                          (join ? 4 : 1));
+        hcap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(est) * 2));
+        P.hstride = 2 + 2 * P.nval;
+        P.hlog2 = log2u(hcap);
+        P.hmask = hcap - 1;
+    }
+
+    // Scratch: accumulators (direct/scalar) or hash table, counters, error word.
+    const uint64_t acc_words = (mode == MODE_GROUP_HASH) ? 0 : ngroups_direct * nv1 * 2;
+    const uint64_t htab_words = hcap * P.hstride;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, acc_words * 8 + htab_words * 8 + 256, &cv));
+    P.acc = cv.take<unsigned long long>(std::max<uint64_t>(acc_words, 2));
+    P.htab = mode == MODE_GROUP_HASH ? cv.take<unsigned long long>(htab_words) : nullptr;
+    P.counters = cv.take<unsigned long long>(4);
+    P.err = cv.take<uint32_t>(4);
+    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
+    if (acc_words) {
+        std::vector<unsigned long long> img;
+        init_acc_image(P, ngroups_direct, &img);
+        bool has_minmax = false;
+        for (uint32_t v = 0; v < P.nval; ++v) has_minmax |= (P.val[v].kind == VK_MIN || P.val[v].kind == VK_MAX);
+        if (has_minmax) {
+            TGP_TRY(upload(ctx, P.acc, img.data(), img.size() * 8));
+        } else {
+            TGP_CUDA(cudaMemsetAsync(P.acc, 0, acc_words * 8, ctx->stream));
+        }
+    }
+    if (mode == MODE_GROUP_HASH) {
+        // Keys EMPTY, counters 0, value limbs: MIN/MAX identity or 0.
+        TGP_CUDA(launch_fill_u64(P.htab, htab_words, 0ull, ctx->sms, ctx->stream));
+        std::vector<unsigned long long> slot_init(P.hstride, 0ull);
+        slot_init[0] = kEmptySlot;
+        for (uint32_t v = 0; v < P.nval; ++v) {
+            if (P.val[v].kind == VK_MIN) slot_init[2 + 2 * v] = 0x7fffffffffffffffull;
+            if (P.val[v].kind == VK_MAX) slot_init[2 + 2 * v] = 0x8000000000000000ull;
+        }
+        // Key words only need EMPTY; MIN/MAX limbs need identities.
+        bool simple = true;
+        for (uint32_t w = 1; w < P.hstride; ++w) simple &= slot_init[w] == 0;
+        if (simple) {
+            TGP_CUDA(cudaMemset2DAsync(P.htab, P.hstride * 8, 0xff, 8, hcap, ctx->stream));
+        } else {
+            std::vector<unsigned long long> img(htab_words);
+            for (uint64_t s = 0; s < hcap; ++s)
+                std::memcpy(&img[s * P.hstride], slot_init.data(), P.hstride * 8);
+            TGP_TRY(upload(ctx, P.htab, img.data(), img.size() * 8));
+        }
+    }
+    TGP_TRY(size_smem(ctx, P, extra));
+    TGP_TRY(launch(ctx, P, mode, acc128));
+
+    unsigned long long counters[4] = {0, 0, 0, 0};
+    uint32_t err = 0;
+    TGP_CUDA(cudaMemcpyAsync(counters, P.counters, 32, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<unsigned long long> accv(acc_words);
+    if (acc_words) TGP_CUDA(cudaMemcpyAsync(accv.data(), P.acc, acc_words * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    TGP_TRY(check_kernel_err(ctx, err));
+
+    result->rows_scanned = T->rows;
+    result->rows_selected = counters[0];
+    result->flags = (err & kErrRowOverflow) ? TGP_RESULT_ROW_OVERFLOW : 0u;
+    const uint32_t nagg = q->nagg;
+
+    if (mode != MODE_GROUP_HASH) {
+        // Direct / scalar: emit groups with a nonzero row count in index order
+        // (index order is ascending lexicographic key order).
+        std::vector<uint64_t> present;
+        if (mode == MODE_SCALAR) {
+            present.push_back(0);
+        } else {
+            for (uint64_t g = 0; g < ngroups_direct; ++g)
+                if (accv[g * nv1 * 2] != 0) present.push_back(g);
+        }
+        result->ngroups = present.size();
+        if (present.size() > group_cap) return fail(ctx, TGP_CAPACITY, "group buffer too small");
+        for (size_t i = 0; i < present.size(); ++i) {
+            const uint64_t g = present[i];
+            if (keys_out) {
+                for (uint32_t k = 0; k < q->ngroup; ++k) {
+                    const uint64_t digit = (g / P.gkey[k].stride) % dom[k];
+                    keys_out[i * q->ngroup + k] = static_cast<uint64_t>(kmin[k]) + digit;
+                }
+            }
+            if (vals_out)
+                for (uint32_t a = 0; a < nagg; ++a) fill_value(amap[a], &accv[g * nv1 * 2], P, &vals_out[i * nagg + a]);
+        }
+        return TGP_OK;
+    }
+
+    // Hash groups: gather occupied slots, sort by key on the host.
+    // Counter word 2 counts the gathered slots.
+    TGP_CUDA(cudaMemsetAsync(P.counters + 2, 0, 8, ctx->stream));
+    unsigned long long* packed = nullptr;
+    const uint64_t max_groups = std::min<uint64_t>(hcap, static_cast<uint64_t>(std::min<unsigned __int128>(D, hcap)));
+    if (cudaMalloc(&packed, std::max<uint64_t>(max_groups, 1) * P.hstride * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, TGP_OOM, "group gather allocation failed");
+    }
+    TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream));
+    unsigned long long ng = 0;
+    TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<unsigned long long> slots(ng * P.hstride);
+    if (ng) TGP_CUDA(cudaMemcpyAsync(slots.data(), packed, ng * P.hstride * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(packed);
+    result->ngroups = ng;
+    if (ng > group_cap) return fail(ctx, TGP_CAPACITY, "group buffer too small");
+    // Packed key order == ascending lexicographic key order (key 0 in the top bits).
+    std::vector<uint64_t> order(ng);
+    for (uint64_t i = 0; i < ng; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](uint64_t x, uint64_t y) { return slots[x * P.hstride] < slots[y * P.hstride]; });
+    std::vector<unsigned long long> tmp(nv1 * 2);
+    for (uint64_t i = 0; i < ng; ++i) {
+        const unsigned long long* s = &slots[order[i] * P.hstride];
+        if (keys_out) {
+            for (uint32_t k = 0; k < q->ngroup; ++k) {
+                const uint64_t mask = bits[k] >= 64 ? ~0ull : ((1ull << bits[k]) - 1);
+                const uint64_t rel = (s[0] >> P.gkey[k].shift) & mask;
+                keys_out[i * q->ngroup + k] = static_cast<uint64_t>(kmin[k]) + rel;
+            }
+        }
+        if (vals_out) {
+            tmp[0] = s[1];
+            tmp[1] = 0;
+            for (uint32_t v = 0; v < P.nval; ++v) {
+                tmp[2 * (v + 1)] = s[2 + 2 * v];
+                tmp[2 * (v + 1) + 1] = s[3 + 2 * v];
+            }
+            for (uint32_t a = 0; a < nagg; ++a) fill_value(amap[a], tmp.data(), P, &vals_out[i * nagg + a]);
+        }
+    }
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Joins
+// --------------------------------------------------------------------------
+static int build_join(tgp_ctx* ctx, const Table* T, tgp_table_id table_id, uint32_t key_col,
+                      const tgp_pred_node* pred, uint32_t npred, JoinTable* out) {
+    if (key_col >= T->cols.size()) return fail(ctx, TGP_INVALID_ARG, "key column out of range");
+    const Column& kc = T->cols[key_col];
+    if (kc.coltype == TGP_CT_FLOAT) return fail(ctx, TGP_UNSUPPORTED, "FLOAT join keys");
+    Builder b(ctx, T);
+    TGP_TRY(b.add_pred(pred, npred));
+    int ks;
+    TGP_TRY(b.slot_of(key_col, &ks));
+    JoinTable J;
+    J.build_table = table_id;
+    J.key_col = key_col;
+    J.kmin = kc.min;
+    J.krange = static_cast<uint64_t>(kc.max) - static_cast<uint64_t>(kc.min);
+    J.empty_range = T->rows == 0;
+    J.wide = J.krange >= 0xffffffffull;
+    // Directory of next_pow2(2 n) slots, as JoinHashTable::new does (join_hash_table.rs:76-86).
+    J.cap = next_pow2(std::max<uint64_t>(16, 2 * T->rows));
+    J.log2 = log2u(J.cap);
+    const uint64_t words = J.cap * (J.wide ? 2 : 1);
+    if (cudaMalloc(&J.tab, words * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, TGP_OOM, "join table allocation failed");
+    }
+    if (J.wide) TGP_CUDA(cudaMemsetAsync(J.tab, 0, words * 8, ctx->stream));
+    else TGP_CUDA(cudaMemsetAsync(J.tab, 0xff, words * 8, ctx->stream));
+    Plan& P = b.P;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, 256, &cv));
+    P.counters = cv.take<unsigned long long>(4);
+    P.err = cv.take<uint32_t>(4);
+    P.acc = cv.take<unsigned long long>(2);
+    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
+    P.jtab = J.tab;
+    P.jmask = J.cap - 1;
+    P.jlog2 = J.log2;
+    P.jwide = J.wide;
+    P.jslot = ks;
+    P.jkmin = J.kmin;
+    P.jkrange = J.krange;
+    int st = size_smem(ctx, P, 0);
+    if (st == TGP_OK) st = launch(ctx, P, MODE_JOIN_BUILD, false);
+    unsigned long long cnt = 0;
+    uint32_t err = 0;
+    if (st == TGP_OK) {
+        cudaMemcpyAsync(&cnt, P.counters, 8, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, "join build failed");
+        else st = check_kernel_err(ctx, err);
+    }
+    if (st != TGP_OK) {
+        cudaFree(J.tab);
+        return st;
+    }
+    J.entries = cnt;
+    *out = J;
+    return TGP_OK;
+}
+
+int tgp_join_build(tgp_ctx* ctx, tgp_table_id build_table, uint32_t key_column, const tgp_pred_node* pred,
+                   uint32_t npred, tgp_join_id* out) {
+    if (!ctx || !out) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    const Table* T;
+    TGP_TRY(get_table(ctx, build_table, &T));
+    JoinTable J;
+    TGP_TRY(build_join(ctx, T, build_table, key_column, pred, npred, &J));
+    const uint64_t id = ctx->next_id++;
+    ctx->joins.emplace(id, J);
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_join_drop(tgp_ctx* ctx, tgp_join_id id) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->joins.find(id);
+    if (it == ctx->joins.end()) return fail(ctx, TGP_NOT_FOUND, "unknown join id");
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(it->second.tab);
+    ctx->joins.erase(it);
+    return TGP_OK;
+}
+
+int tgp_join_probe_pairs(tgp_ctx* ctx, tgp_join_id join, tgp_table_id probe_table, uint32_t probe_key_column,
+                         const tgp_pred_node* pred, uint32_t npred, uint32_t* probe_rows, uint32_t* build_rows,
+                         uint64_t cap, uint64_t* npairs) {
+    if (!ctx || !npairs) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    const JoinTable* J;
+    TGP_TRY(join_lookup(ctx, join, &J));
+    const Table* T;
+    TGP_TRY(get_table(ctx, probe_table, &T));
+    if (probe_key_column >= T->cols.size()) return fail(ctx, TGP_INVALID_ARG, "probe key column out of range");
+    Builder b(ctx, T);
+    TGP_TRY(b.add_pred(pred, npred));
+    int ks;
+    TGP_TRY(b.slot_of(probe_key_column, &ks));
+    Plan& P = b.P;
+    attach_join(P, *J, ks);
+    // Pass 1 counts pairs (out_cap 0), pass 2 writes them.
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, 256, &cv));
+    P.counters = cv.take<unsigned long long>(4);
+    P.err = cv.take<uint32_t>(4);
+    P.acc = cv.take<unsigned long long>(2);
+    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
+    P.out_pairs = nullptr;
+    P.out_cap = 0;
+    TGP_TRY(size_smem(ctx, P, 0));
+    TGP_TRY(launch(ctx, P, MODE_JOIN_PAIRS, false));
+    unsigned long long counters[4];
+    uint32_t err = 0;
+    TGP_CUDA(cudaMemcpyAsync(counters, P.counters, 32, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    TGP_TRY(check_kernel_err(ctx, err));
+    const uint64_t n = counters[1];
+    *npairs = n;
+    if (n > cap) return fail(ctx, TGP_CAPACITY, "pair buffers too small");
+    if (n == 0) return TGP_OK;
+    if (!probe_rows || !build_rows) return fail(ctx, TGP_INVALID_ARG, "null pair buffers");
+    size_t sort_bytes = 0;
+    sort_pairs(nullptr, nullptr, n, nullptr, &sort_bytes, ctx->stream);
+    const bool dev_out = is_device_ptr(probe_rows) && is_device_ptr(build_rows);
+    TGP_TRY(arena_reserve(ctx, n * 16 + sort_bytes + (dev_out ? 0 : n * 8) + 1024, &cv));
+    unsigned long long* pa = cv.take<unsigned long long>(n);
+    unsigned long long* pb = cv.take<unsigned long long>(n);
+    void* stmp = cv.take<uint8_t>(sort_bytes + 16);
+    P.counters = cv.take<unsigned long long>(4);
+    P.err = cv.take<uint32_t>(4);
+    P.acc = cv.take<unsigned long long>(2);
+    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
+    P.out_pairs = pa;
+    P.out_cap = n;
+    TGP_TRY(launch(ctx, P, MODE_JOIN_PAIRS, false));
+    TGP_CUDA(sort_pairs(pa, pb, n, stmp, &sort_bytes, ctx->stream));
+    if (dev_out) {
+        TGP_CUDA(launch_split_pairs(pb, n, probe_rows, build_rows, ctx->sms, ctx->stream));
+    } else {
+        uint32_t* sp = cv.take<uint32_t>(n);
+        uint32_t* sb = cv.take<uint32_t>(n);
+        TGP_CUDA(launch_split_pairs(pb, n, sp, sb, ctx->sms, ctx->stream));
+        TGP_TRY(copy_out(ctx, probe_rows, sp, n * 4));
+        TGP_TRY(copy_out(ctx, build_rows, sb, n * 4));
+    }
+    TGP_CUDA(cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return check_kernel_err(ctx, err);
+}
+
+
+// --------------------------------------------------------------------------
+// Kernel-table boundary (src/kernel/mod.rs)
+// --------------------------------------------------------------------------
+static const tgp_kernel_info kGpuKernels[] = {
+    {TGP_OP_SCAN_EQ_U64, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "scan_eq_u64_sm100a_hbm"},
+    {TGP_OP_SCAN_RANGE_U64, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "scan_range_u64_sm100a_hbm"},
+    {TGP_OP_SCAN_MULTI_PREDICATE, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "scan_multi_predicate_sm100a_hbm"},
+    {TGP_OP_HASH_BUILD, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "hash_build_sm100a_hbm"},
+    {TGP_OP_HASH_PROBE, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "hash_probe_sm100a_hbm"},
+    {TGP_OP_AGGREGATE_SUM_F64, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "sum_f64_sm100a_hbm"},
+    {TGP_OP_AGGREGATE_COUNT_DISTINCT, TGP_CPU_GPU_SM100A, TGP_TIER_HBM, 0, "count_distinct_sm100a_hbm"},
+};
+
+uint32_t tgp_kernel_count(void) { return sizeof(kGpuKernels) / sizeof(kGpuKernels[0]); }
+
+int tgp_kernel_info_at(uint32_t i, tgp_kernel_info* out) {
+    if (!out || i >= tgp_kernel_count()) return TGP_INVALID_ARG;
+    *out = kGpuKernels[i];
+    return TGP_OK;
+}
+
+// Places `bytes` of kernel input (host or device memory) in 16-byte-aligned
+// device memory. Aligned device input is used in place.
+static int stage_input(tgp_ctx* ctx, const void* input, size_t bytes, const uint8_t** dev) {
+    if (bytes == 0) {
+        *dev = nullptr;
+        return TGP_OK;
+    }
+    if (is_device_ptr(input) && reinterpret_cast<uintptr_t>(input) % 16 == 0) {
+        *dev = static_cast<const uint8_t*>(input);
+        return TGP_OK;
+    }
+    const size_t need = ((bytes + 255) / 256) * 256;
+    if (need > ctx->kin_cap) {
+        TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->kin) cudaFree(ctx->kin);
+        ctx->kin = nullptr;
+        ctx->kin_cap = 0;
+        if (cudaMalloc(&ctx->kin, need) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, TGP_OOM, "kernel input staging allocation failed");
+        }
+        ctx->kin_cap = need;
+    }
+    TGP_CUDA(cudaMemcpyAsync(ctx->kin, input, bytes, cudaMemcpyDefault, ctx->stream));
+    *dev = ctx->kin;
+    return TGP_OK;
+}
+
+// A one-column table of u64 cells over staged device memory.
+static Table cell_table(const uint8_t* dev, uint64_t n) {
+    Table t;
+    t.rows = n;
+    Column c;
+    c.dtype = DT_U64;
+    c.coltype = TGP_CT_DATE;  // raw cells compare unsigned (src/kernel/scan.rs:99-115)
+    c.width = 8;
+    c.dptr = const_cast<uint8_t*>(dev);
+    t.cols.push_back(c);
+    return t;
+}
+
+static tgp_pred_node leaf_node(uint32_t cmp, uint64_t lit, uint64_t lit2 = 0) {
+    tgp_pred_node n;
+    std::memset(&n, 0, sizeof(n));
+    n.kind = TGP_PN_LEAF;
+    n.column = 0;
+    n.cmp = cmp;
+    n.lit = lit;
+    n.lit2 = lit2;
+    return n;
+}
+
+// Number of (probe, build) key matches of n staged probe cells.
+static int count_matches(tgp_ctx* ctx, const Table& probe, const JoinTable& J, uint64_t* out) {
+    Builder b(ctx, &probe);
+    int ks;
+    TGP_TRY(b.slot_of(0, &ks));
+    attach_join(b.P, J, ks);
+    Plan& P = b.P;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, 256, &cv));
+    P.acc = cv.take<unsigned long long>(2);
+    P.counters = cv.take<unsigned long long>(4);
+    P.err = cv.take<uint32_t>(4);
+    TGP_CUDA(cudaMemsetAsync(P.acc, 0, 16, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
+    P.ngroups = 1;
+    TGP_TRY(size_smem(ctx, P, 0));
+    TGP_TRY(launch(ctx, P, MODE_SCALAR, false));
+    unsigned long long acc[2];
+    uint32_t err = 0;
+    TGP_CUDA(cudaMemcpyAsync(acc, P.acc, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    TGP_TRY(check_kernel_err(ctx, err));
+    *out = acc[0];
+    return TGP_OK;
+}
+
+int tgp_kernel_execute(tgp_ctx* ctx, uint32_t op, const void* input, void* output, const tgp_kernel_params* p,
+                       tgp_kernel_result* r) {
+    if (!ctx || !p || !r) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    std::memset(r, 0, sizeof(*r));
+    const uint64_t n = p->cell_count;
+    if (n >= (1ull << 32)) return fail(ctx, TGP_UNSUPPORTED, "cell_count must be below 2^32");
+    if (n && !input) return fail(ctx, TGP_INVALID_ARG, "null input");
+    TGP_CUDA(cudaSetDevice(ctx->device));
+    switch (op) {
+        case TGP_OP_SCAN_EQ_U64:
+        case TGP_OP_SCAN_RANGE_U64:
+        case TGP_OP_SCAN_MULTI_PREDICATE: {
+            const uint8_t* dev;
+            TGP_TRY(stage_input(ctx, input, n * 8, &dev));
+            Table t = cell_table(dev, n);
+            tgp_pred_node prog[5];
+            uint32_t np = 0;
+            if (op == TGP_OP_SCAN_EQ_U64) {
+                prog[np++] = leaf_node(TGP_CMP_EQ, p->target_u64);
+            } else if (op == TGP_OP_SCAN_RANGE_U64) {
+                prog[np++] = leaf_node(TGP_CMP_BETWEEN, p->low_u64, p->high_u64);
+            } else {
+                // ScanMultiPredicateScalar (src/kernel/scan.rs:124-160): AND of the
+                // first min(predicate_count, 3) predicates; none = every cell.
+                const uint32_t k = std::min<uint32_t>(p->predicate_count, 3);
+                const uint8_t ops[3] = {p->pred1_op, p->pred2_op, p->pred3_op};
+                const uint64_t tg[3] = {p->target_u64, p->target2_u64, p->target3_u64};
+                for (uint32_t i = 0; i < k; ++i) {
+                    const uint32_t cmp = ops[i] == TGP_PRED_GT ? TGP_CMP_GT : ops[i] == TGP_PRED_LT ? TGP_CMP_LT : TGP_CMP_EQ;
+                    if (ops[i] > TGP_PRED_LT) return fail(ctx, TGP_INVALID_ARG, "bad predicate op");
+                    prog[np++] = leaf_node(cmp, tg[i]);
+                    if (i > 0) {
+                        std::memset(&prog[np], 0, sizeof(tgp_pred_node));
+                        prog[np++].kind = TGP_PN_AND;
+                    }
+                }
+            }
+            uint32_t words[2] = {0, 0};
+            uint64_t cnt = 0;
+            const bool want_mask = op == TGP_OP_SCAN_EQ_U64 && n > 0;
+            TGP_TRY(filter_impl(ctx, &t, prog, np, want_mask ? reinterpret_cast<uint8_t*>(words) : nullptr, nullptr,
+                                0, &cnt, want_mask ? 2u : 0u));
+            r->count = cnt;
+            if (want_mask) {
+                uint64_t m = static_cast<uint64_t>(words[0]) | (static_cast<uint64_t>(words[1]) << 32);
+                if (n < 64) m &= (1ull << n) - 1;
+                r->mask = m;
+            }
+            return TGP_OK;
+        }
+        case TGP_OP_AGGREGATE_SUM_F64: {
+            r->count = n;
+            if (n == 0) return TGP_OK;
+            const uint8_t* dev;
+            TGP_TRY(stage_input(ctx, input, n * 8, &dev));
+            const int blocks = static_cast<int>(std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(ctx->sms) * 4));
+            Carve cv;
+            TGP_TRY(arena_reserve(ctx, blocks * 16 + 256, &cv));
+            double* part = cv.take<double>(2 * blocks);
+            TGP_CUDA(launch_sum_f64(reinterpret_cast<const double*>(dev), n, part, blocks, ctx->stream));
+            std::vector<double> h(2 * blocks);
+            TGP_CUDA(cudaMemcpyAsync(h.data(), part, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+            // Double-double accumulation of the per-block pairs.
+            double hi = 0.0, lo = 0.0;
+            for (int i = 0; i < blocks; ++i) {
+                const double bh = h[2 * i], bl = h[2 * i + 1];
+                const double s = hi + bh;
+                const double bb = s - hi;
+                double e = (hi - (s - bb)) + (bh - bb);
+                e += lo + bl;
+                hi = s + e;
+                lo = e - (hi - s);
+            }
+            r->sum = hi;
+            return TGP_OK;
+        }
+        case TGP_OP_AGGREGATE_COUNT_DISTINCT: {
+            if (n == 0) return TGP_OK;
+            const uint8_t* dev;
+            TGP_TRY(stage_input(ctx, input, n * 8, &dev));
+            const uint64_t cap = next_pow2(std::max<uint64_t>(16, 2 * n));
+            Carve cv;
+            TGP_TRY(arena_reserve(ctx, cap * 8 + 256, &cv));
+            unsigned long long* set = cv.take<unsigned long long>(cap);
+            unsigned long long* counters = cv.take<unsigned long long>(2);
+            uint32_t* err = cv.take<uint32_t>(4);
+            TGP_CUDA(cudaMemsetAsync(set, 0xff, cap * 8, ctx->stream));
+            TGP_CUDA(cudaMemsetAsync(counters, 0, 16, ctx->stream));
+            TGP_CUDA(cudaMemsetAsync(err, 0, 16, ctx->stream));
+            const int blocks = static_cast<int>(std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(ctx->sms) * 8));
+            TGP_CUDA(launch_count_distinct(reinterpret_cast<const unsigned long long*>(dev), n, set, cap - 1, log2u(cap),
+                                           counters, err, blocks, ctx->stream));
+            unsigned long long hc[2];
+            uint32_t herr = 0;
+            TGP_CUDA(cudaMemcpyAsync(hc, counters, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            TGP_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+            TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+            TGP_TRY(check_kernel_err(ctx, herr));
+            r->count = hc[0] + (hc[1] ? 1 : 0);
+            return TGP_OK;
+        }
+        case TGP_OP_HASH_BUILD: {
+            if (!output) return fail(ctx, TGP_INVALID_ARG, "HashBuild needs an output slot for the table handle");
+            const uint8_t* dev;
+            TGP_TRY(stage_input(ctx, input, n * 8, &dev));
+            Table t = cell_table(dev, n);
+            t.cols[0].coltype = TGP_CT_INT;
+            TGP_TRY(compute_stats(ctx, t));
+            JoinTable* J = new (std::nothrow) JoinTable();
+            if (!J) return fail(ctx, TGP_OOM, "host allocation failed");
+            int st = build_join(ctx, &t, 0, 0, nullptr, 0, J);
+            if (st != TGP_OK) {
+                delete J;
+                return st;
+            }
+            ctx->hash_handles.insert(J);
+            void* handle = J;
+            if (is_device_ptr(output)) {
+                TGP_CUDA(cudaMemcpy(output, &handle, 8, cudaMemcpyHostToDevice));
+            } else {
+                std::memcpy(output, &handle, 8);
+            }
+            r->count = n;
+            return TGP_OK;
+        }
+        case TGP_OP_HASH_PROBE: {
+            // input = [handle: 8 bytes][cell_count u64 keys] (src/kernel/hash.rs:171-178).
+            void* handle = nullptr;
+            if (is_device_ptr(input)) TGP_CUDA(cudaMemcpy(&handle, input, 8, cudaMemcpyDeviceToHost));
+            else std::memcpy(&handle, input, 8);
+            if (!ctx->hash_handles.count(handle)) return fail(ctx, TGP_INVALID_ARG, "unknown hash table handle");
+            if (n == 0) return TGP_OK;
+            const uint8_t* dev;
+            TGP_TRY(stage_input(ctx, static_cast<const uint8_t*>(input) + 8, n * 8, &dev));
+            Table t = cell_table(dev, n);
+            uint64_t matches = 0;
+            TGP_TRY(count_matches(ctx, t, *static_cast<JoinTable*>(handle), &matches));
+            r->count = matches;
+            return TGP_OK;
+        }
+        default:
+            return fail(ctx, TGP_UNSUPPORTED, "operator has no GPU kernel");
+    }
+}
+
+int tgp_hash_table_free(tgp_ctx* ctx, void* handle) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->hash_handles.find(handle);
+    if (it == ctx->hash_handles.end()) return fail(ctx, TGP_INVALID_ARG, "unknown hash table handle");
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    JoinTable* J = static_cast<JoinTable*>(handle);
+    if (J->tab) cudaFree(J->tab);
+    delete J;
+    ctx->hash_handles.erase(it);
+    return TGP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+// plan.hpp — the lowered form of one scan over one resident table, shared by
+// the host planner (capi.cpp) and the device kernels (scan_engine.cu).
+//
+// A plan is a POD passed by value as a __grid_constant__ kernel parameter, so
+// launching a query needs no descriptor copy. Host code lowers the C-ABI
+// query (predicate program, aggregates, group keys, join) into it.
+#pragma once
+
+#include <cstdint>
+
+namespace tgp {
+
+constexpr int kThreads = 256;                        // threads per CTA
+constexpr int kRowsPerThread = 8;                    // rows a thread owns per tile
+constexpr int kTileRows = kThreads * kRowsPerThread; // 2048 rows per tile
+constexpr int kMaxSlots = 8;       // distinct columns staged per scan
+constexpr int kMaxLeaves = 16;     // predicate leaves
+constexpr int kMaxPredOps = 32;    // postfix program length
+constexpr int kMaxVals = 8;        // value accumulators per group
+constexpr int kMaxFactors = 4;
+constexpr int kMaxGroupKeys = 4;
+constexpr int kMaxStages = 8;
+constexpr int kBarrierBytes = 128; // shared bytes reserved for the stage mbarriers
+
+// Error bits a kernel raises in its plan's error word (never __trap()).
+enum : uint32_t {
+    kErrWaitTimeout = 1u,   // an mbarrier wait gave up
+    kErrHashFull = 2u,      // a hash table ran out of slots
+    kErrOutputFull = 4u,    // an output buffer reservation ran past its capacity
+    kErrRowOverflow = 8u    // a per-row i64 argument wrapped (informational)
+};
+
+// Physical column types (values match tgp_dtype).
+enum : uint32_t { DT_U8 = 1, DT_I32 = 2, DT_I64 = 3, DT_U64 = 4, DT_F64 = 5 };
+
+// Scan modes (one kernel instantiation each).
+enum : uint32_t {
+    MODE_FILTER = 0,         // count selected rows; write bitmap words; per-tile counts
+    MODE_SCALAR = 1,         // scalar aggregate in registers
+    MODE_GROUP_PRIVATE = 2,  // direct-indexed groups, per-thread shared accumulators
+    MODE_GROUP_SHARED = 3,   // direct-indexed groups, per-CTA shared table with atomics
+    MODE_GROUP_GLOBAL = 4,   // direct-indexed groups, global int128 atomics
+    MODE_GROUP_HASH = 5,     // open-addressing global hash table of groups
+    MODE_JOIN_BUILD = 6,     // insert selected rows into a join hash table
+    MODE_JOIN_PAIRS = 7      // probe and emit (probe_row, build_row) pairs
+};
+
+// A staged column.
+struct SlotDesc {
+    const uint8_t* ptr;   // device column base (16-byte aligned)
+    uint32_t width;       // bytes per row: 1, 4 or 8
+    uint32_t dtype;       // DT_*
+    uint32_t smem_off;    // offset of this column's tile inside a stage
+    uint32_t _pad;
+};
+
+// Leaf kinds after lowering. Integer leaves test (key - lo) <= span as
+// unsigned integers, where key = cell ^ xor maps the column's comparison
+// order onto unsigned order; `negate` flips the result.
+enum : uint8_t { LK_U8 = 0, LK_I32 = 1, LK_64 = 2, LK_F64 = 3, LK_CONST = 4 };
+enum : uint8_t { FOP_EQ_EPS = 0, FOP_NE = 1, FOP_LT = 2, FOP_LE = 3, FOP_GT = 4, FOP_GE = 5,
+                 FOP_BETWEEN = 6, FOP_NOT_BETWEEN = 7 };
+
+struct Leaf {
+    uint8_t slot;
+    uint8_t kind;     // LK_*
+    uint8_t negate;   // 0 or 1 (LK_CONST: the constant value)
+    uint8_t fop;      // FOP_* for LK_F64
+    uint32_t xor32;
+    uint32_t lo32;
+    uint32_t span32;
+    uint64_t xor64;
+    uint64_t lo64;
+    uint64_t span64;
+    double f1;        // LK_F64 literal / lower bound / epsilon target
+    double f2;        // LK_F64 upper bound or epsilon
+};
+
+// Postfix program opcodes: values < kMaxLeaves push leaf i.
+enum : uint8_t { OP_AND = 0x80, OP_OR = 0x81, OP_NOT = 0x82 };
+
+// Value accumulator kinds.
+enum : uint8_t { VK_SUM = 0, VK_MIN = 1, VK_MAX = 2, VK_COUNT_NZ = 3 };
+
+struct Factor {
+    int8_t slot;          // staged column slot, or -1 for a constant
+    uint8_t build_side;   // 1: gather from a build-side column at the matched build row
+    uint8_t dtype;        // build-side gather dtype
+    uint8_t _pad[5];
+    const uint8_t* bptr;  // build-side column (device)
+    int64_t mul;
+    int64_t add;
+};
+
+struct ValDesc {
+    uint8_t kind;   // VK_*
+    uint8_t nf;     // number of factors
+    uint8_t _pad[6];
+    Factor f[kMaxFactors];
+};
+
+struct GKey {
+    int8_t slot;          // staged slot (probe/own side)
+    uint8_t build_side;   // 1: key column lives on the build side
+    uint8_t dtype;        // build-side gather dtype
+    uint8_t shift;        // MODE_GROUP_HASH: bit position in the packed key
+    uint32_t _pad;
+    const uint8_t* bptr;
+    int64_t min;          // key cell minimum (from column statistics)
+    uint64_t stride;      // direct modes: multiplier of (cell - min) in the group index
+};
+
+struct Plan {
+    uint64_t nrows;
+    uint32_t nslots;
+    uint32_t stage_bytes;   // bytes of one stage (all slots of one tile)
+    uint32_t nstages;
+    uint32_t extra_off;     // shared offset of per-mode scratch (accumulators)
+    uint32_t smem_bytes;    // total dynamic shared memory
+    uint32_t bitmap_words;  // MODE_FILTER: bitmap words written (0 = none)
+    SlotDesc slot[kMaxSlots];
+
+    // WHERE program
+    uint32_t nleaf;
+    uint32_t nops;
+    uint32_t all_and;       // program is a conjunction of all leaves
+    uint32_t _p0;
+    Leaf leaf[kMaxLeaves];
+    uint8_t ops[kMaxPredOps];
+
+    // Values (per group: slot 0 = row count, slots 1..nval = values)
+    uint32_t nval;
+    uint32_t check_ovf;     // per-row overflow detection needed
+    uint64_t flush_limit;   // MODE_GROUP_PRIVATE int64: per-thread updates between flushes
+    ValDesc val[kMaxVals];
+
+    // Group keys
+    uint32_t ngkey;
+    uint32_t ngroups;       // direct modes: number of group indices
+    GKey gkey[kMaxGroupKeys];
+
+    // Group hash table (MODE_GROUP_HASH): slot = [key][count][v0 lo][v0 hi]...
+    unsigned long long* htab;
+    uint64_t hmask;
+    uint32_t hlog2;
+    uint32_t hstride;       // u64 words per slot
+
+    // Join table (probe side: MODE_GROUP_* / MODE_SCALAR with join, MODE_JOIN_PAIRS;
+    // build side: MODE_JOIN_BUILD). Packed slots: (key_rel << 32) | build_row.
+    // Wide slots: [key_rel][build_row + 1].
+    unsigned long long* jtab;
+    uint64_t jmask;
+    uint32_t jlog2;
+    uint32_t jwide;
+    int32_t jslot;          // staged slot of the join key (-1 = no join)
+    uint32_t _p1;
+    int64_t jkmin;
+    uint64_t jkrange;       // kmax - kmin (unsigned)
+
+    // Outputs
+    unsigned long long* acc;        // direct/scalar accumulators [g][1 + nval][2]
+    uint32_t* bitmap;               // MODE_FILTER bitmap words
+    uint32_t* tile_counts;          // MODE_FILTER per-tile selected counts
+    unsigned long long* counters;   // [0] selected rows [1] pairs reserved [2] matches
+    uint32_t* err;                  // kErr* bits
+    unsigned long long* out_pairs;  // MODE_JOIN_PAIRS: (probe_row << 32) | build_row
+    uint64_t out_cap;
+};
+
+// Multiplicative hash of a relative key into a power-of-two table.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline uint64_t hash_slot(uint64_t key_rel, uint32_t log2cap) {
+    return (key_rel * 0x9E3779B97F4A7C15ull) >> (64u - log2cap);
+}
+
+}  // namespace tgp

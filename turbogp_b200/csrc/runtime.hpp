@@ -1,0 +1,108 @@
+// runtime.hpp — host-side state behind the C ABI: the context, the
+// HBM-resident table registry (the device tier the reference's MemoryTier::Hbm
+// names, src/memory/tier.rs:20), join tables, and the scratch arena.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+#include "plan.hpp"
+#include "turbogp_gpu.h"
+
+namespace tgp {
+
+// Launchers implemented in the .cu files.
+cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st);
+int scan_occupancy(uint32_t mode, bool acc128, size_t dyn_smem);
+size_t scan_kernel_static_smem();
+cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
+                                 int sms, cudaStream_t st);
+cudaError_t tile_prefix(const uint32_t* counts, unsigned long long* out, uint64_t n, void* tmp,
+                        size_t* tmp_bytes, cudaStream_t st);
+cudaError_t launch_compact(const uint32_t* bitmap, uint64_t nwords, uint64_t ntiles,
+                           const unsigned long long* tile_base, uint32_t* rowids, uint64_t cap,
+                           cudaStream_t st);
+cudaError_t launch_sum_f64(const double* x, uint64_t n, double* out, int blocks, cudaStream_t st);
+cudaError_t launch_count_distinct(const unsigned long long* x, uint64_t n, unsigned long long* set,
+                                  uint64_t mask, uint32_t log2cap, unsigned long long* counters,
+                                  uint32_t* err, int blocks, cudaStream_t st);
+cudaError_t sort_pairs(const unsigned long long* in, unsigned long long* out, uint64_t n, void* tmp,
+                       size_t* tmp_bytes, cudaStream_t st);
+cudaError_t launch_split_pairs(const unsigned long long* pairs, uint64_t n, uint32_t* probe,
+                               uint32_t* build, int sms, cudaStream_t st);
+cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, int sms,
+                            cudaStream_t st);
+cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
+                                 unsigned long long* out, uint64_t cap, unsigned long long* counter,
+                                 int sms, cudaStream_t st);
+
+struct Column {
+    uint32_t dtype = 0;
+    uint32_t coltype = 0;
+    uint32_t width = 0;
+    uint8_t* dptr = nullptr;
+    bool owned = false;
+    int64_t min = 0;
+    int64_t max = 0;
+};
+
+struct Table {
+    uint64_t rows = 0;
+    std::vector<Column> cols;
+};
+
+// Device join hash table over the selected rows of a build table.
+struct JoinTable {
+    tgp_table_id build_table = 0;
+    uint32_t key_col = 0;
+    unsigned long long* tab = nullptr;  // packed u64 slots or wide [key_rel, row+1] pairs
+    uint64_t cap = 0;                   // slots (power of two)
+    uint32_t log2 = 0;
+    bool wide = false;
+    int64_t kmin = 0;
+    uint64_t krange = 0;
+    uint64_t entries = 0;               // build rows inserted
+    bool empty_range = false;           // no build key statistics (empty build side)
+};
+
+// Grow-only device scratch carved per call.
+struct Arena {
+    uint8_t* base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+};
+
+}  // namespace tgp
+
+struct tgp_ctx {
+    int device = 0;
+    int sms = 0;
+    size_t max_dyn_smem = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::unordered_map<uint64_t, tgp::Table> tables;
+    std::unordered_map<uint64_t, tgp::JoinTable> joins;
+    uint64_t next_id = 1;
+    tgp::Arena arena;
+    // Pinned host staging for small readbacks.
+    uint8_t* hpin = nullptr;
+    size_t hpin_cap = 0;
+    // Device staging of kernel-table inputs (kept apart from the arena so
+    // scans that grow the arena never move a staged input).
+    uint8_t* kin = nullptr;
+    size_t kin_cap = 0;
+    // Live HashBuild handles (opaque pointers handed to callers).
+    std::unordered_set<void*> hash_handles;
+    // Launch profiling: event pairs around scan-kernel launches.
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    size_t prof_used = 0;
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES).
+    int ctas_per_sm = 1;
+    int max_stages = tgp::kMaxStages;
+};

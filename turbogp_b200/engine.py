@@ -1,0 +1,527 @@
+"""Host-side API over the C ABI: resident tables, predicates, aggregates, joins.
+
+This mirrors what the reference's query interpreter hands to its vectorized
+operators (src/engine/query_interpreter/expr.rs:419 ``build_mask``,
+aggregate.rs:507 ``execute_grouped``, join.rs:544 ``hash_join_with_keys``):
+a WHERE tree over typed columns, GROUP BY columns and aggregate expressions,
+lowered here into the C ABI's postfix predicate program and affine-product
+aggregate arguments. All compute runs in the CUDA library; nothing here falls
+back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _capi as A
+
+_NP_DTYPE = {np.dtype(np.uint8): A.DT_U8, np.dtype(np.int32): A.DT_I32, np.dtype(np.int64): A.DT_I64,
+             np.dtype(np.uint64): A.DT_U64, np.dtype(np.float64): A.DT_F64}
+_DT_NP = {v: k for k, v in _NP_DTYPE.items()}
+_COLTYPE = {"int": A.CT_INT, "date": A.CT_DATE, "float": A.CT_FLOAT}
+
+
+def _u64(v: int) -> int:
+    return int(v) & 0xFFFFFFFFFFFFFFFF
+
+
+# ---------------------------------------------------------------------------
+# Expressions
+# ---------------------------------------------------------------------------
+@dataclass(frozen=True)
+class Factor:
+    """``mul * column + add`` (column None = the constant ``add``)."""
+    column: str | None
+    mul: int = 1
+    add: int = 0
+    side: int = A.SIDE_PROBE
+
+
+class Term:
+    """A product of affine factors: the per-row argument of an aggregate."""
+
+    def __init__(self, factors: Sequence[Factor]):
+        self.factors = tuple(factors)
+
+    def __mul__(self, other):
+        o = _as_term(other)
+        return Term(self.factors + o.factors)
+
+    __rmul__ = __mul__
+
+    def _affine(self) -> Factor:
+        if len(self.factors) != 1:
+            raise ValueError("only a single column can be offset: write (k - col) or (col + k)")
+        return self.factors[0]
+
+    def __add__(self, k):
+        if isinstance(k, (Term, Col)):
+            raise ValueError("sums of columns are not affine factors")
+        f = self._affine()
+        return Term([Factor(f.column, f.mul, f.add + int(k), f.side)])
+
+    __radd__ = __add__
+
+    def __sub__(self, k):
+        if isinstance(k, (Term, Col)):
+            raise ValueError("differences of columns are not affine factors")
+        return self + (-int(k))
+
+    def __rsub__(self, k):
+        f = self._affine()
+        return Term([Factor(f.column, -f.mul, int(k) - f.add, f.side)])
+
+    def __neg__(self):
+        f = self._affine()
+        return Term([Factor(f.column, -f.mul, -f.add, f.side)])
+
+
+class Col(Term):
+    """A column reference usable in predicates and aggregate arguments."""
+
+    def __init__(self, name: str, side: int = A.SIDE_PROBE):
+        super().__init__([Factor(name, 1, 0, side)])
+        self.name = name
+        self.side = side
+
+    def _leaf(self, cmp, lit, lit2=0):
+        if self.side != A.SIDE_PROBE:
+            raise ValueError("predicates apply to the scanned table only")
+        return Pred([("leaf", self.name, cmp, lit, lit2)])
+
+    def __eq__(self, v):  # type: ignore[override]
+        return self._leaf(A.CMP_EQ, v)
+
+    def __ne__(self, v):  # type: ignore[override]
+        return self._leaf(A.CMP_NE, v)
+
+    def __lt__(self, v):
+        return self._leaf(A.CMP_LT, v)
+
+    def __le__(self, v):
+        return self._leaf(A.CMP_LE, v)
+
+    def __gt__(self, v):
+        return self._leaf(A.CMP_GT, v)
+
+    def __ge__(self, v):
+        return self._leaf(A.CMP_GE, v)
+
+    def between(self, lo, hi):
+        return self._leaf(A.CMP_BETWEEN, lo, hi)
+
+    def not_between(self, lo, hi):
+        return self._leaf(A.CMP_NOT_BETWEEN, lo, hi)
+
+    __hash__ = object.__hash__
+
+
+def col(name: str) -> Col:
+    return Col(name, A.SIDE_PROBE)
+
+
+def build_col(name: str) -> Col:
+    """A column of the joined build table."""
+    return Col(name, A.SIDE_BUILD)
+
+
+def lit(k: int) -> Term:
+    return Term([Factor(None, 0, int(k))])
+
+
+def _as_term(x) -> Term:
+    if isinstance(x, Term):
+        return x
+    return lit(int(x))
+
+
+class Pred:
+    """A WHERE tree in postfix form."""
+
+    def __init__(self, ops):
+        self.ops = list(ops)
+
+    def __and__(self, o: "Pred") -> "Pred":
+        return Pred(self.ops + o.ops + [("and",)])
+
+    def __or__(self, o: "Pred") -> "Pred":
+        return Pred(self.ops + o.ops + [("or",)])
+
+    def __invert__(self) -> "Pred":
+        return Pred(self.ops + [("not",)])
+
+
+# ---------------------------------------------------------------------------
+# Aggregates
+# ---------------------------------------------------------------------------
+@dataclass
+class Agg:
+    func: int
+    term: Term | None = None
+
+
+def count_star() -> Agg:
+    return Agg(A.AGG_COUNT_STAR)
+
+
+def count_col(c: Col) -> Agg:
+    return Agg(A.AGG_COUNT_NONZERO, c)
+
+
+def sum_(t) -> Agg:
+    return Agg(A.AGG_SUM, _as_term(t))
+
+
+def avg(t) -> Agg:
+    return Agg(A.AGG_AVG, _as_term(t))
+
+
+def min_(t) -> Agg:
+    return Agg(A.AGG_MIN, _as_term(t))
+
+
+def max_(t) -> Agg:
+    return Agg(A.AGG_MAX, _as_term(t))
+
+
+@dataclass
+class AggResult:
+    """One aggregate of one group: exact integer value, row count, f64 view."""
+    value: int
+    count: int
+    as_f64: float
+
+
+@dataclass
+class QueryOutput:
+    keys: list[tuple[int, ...]]
+    values: list[list[AggResult]]
+    rows_scanned: int
+    rows_selected: int
+    flags: int
+
+    @property
+    def ngroups(self) -> int:
+        return len(self.values)
+
+
+@dataclass
+class FilterOutput:
+    count: int
+    bitmap: np.ndarray | None = None
+    rowids: np.ndarray | None = None
+
+
+# ---------------------------------------------------------------------------
+# Context / tables
+# ---------------------------------------------------------------------------
+class Context:
+    """One CUDA device's execution context (tgp_init / tgp_shutdown)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = A.load()
+        h = C.c_void_p()
+        st = self.lib.tgp_init(C.byref(h), device)
+        if st != A.OK:
+            raise A.TgpError(st, f"tgp_init(device={device}) failed")
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.tgp_shutdown(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, what: str) -> None:
+        if st != A.OK:
+            msg = self.lib.tgp_last_error(self.h)
+            raise A.TgpError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.tgp_ctx_stream(self.h) or 0)
+
+    @property
+    def sm_count(self) -> int:
+        return int(self.lib.tgp_ctx_sm_count(self.h))
+
+    def sync(self) -> None:
+        self._check(self.lib.tgp_sync(self.h), "tgp_sync")
+
+    def profile(self, on: bool = True) -> None:
+        """Record CUDA events around every scan-kernel launch."""
+        self._check(self.lib.tgp_profile_enable(self.h, 1 if on else 0), "tgp_profile_enable")
+
+    def profile_read(self) -> tuple[int, float]:
+        """(launches, summed device ms) since the last read."""
+        n, ms = C.c_uint64(), C.c_double()
+        self._check(self.lib.tgp_profile_read(self.h, C.byref(n), C.byref(ms)), "tgp_profile_read")
+        return int(n.value), float(ms.value)
+
+    def register(self, columns: dict, coltypes: dict | None = None) -> "Table":
+        """Copies host numpy columns into HBM. ``coltypes`` maps a name to
+        'int' | 'date' | 'float' (default: 'float' for f64, else 'int')."""
+        return self._register(columns, coltypes, device=False)
+
+    def register_device(self, columns: dict, coltypes: dict | None = None) -> "Table":
+        """Registers device tensors (torch CUDA tensors) without copying."""
+        return self._register(columns, coltypes, device=True)
+
+    def _register(self, columns: dict, coltypes: dict | None, device: bool) -> "Table":
+        coltypes = coltypes or {}
+        names = list(columns)
+        descs = (A.ColumnDesc * max(1, len(names)))()
+        keep = []
+        rows = None
+        dtypes = []
+        for i, name in enumerate(names):
+            arr = columns[name]
+            if device:
+                import torch
+                t = arr
+                npdt = np.dtype(str(t.dtype).replace("torch.", ""))
+                ptr = t.data_ptr()
+                n = t.numel()
+                keep.append(t)
+            else:
+                a = np.ascontiguousarray(arr)
+                npdt = a.dtype
+                ptr = a.ctypes.data
+                n = a.shape[0]
+                keep.append(a)
+            if npdt not in _NP_DTYPE:
+                raise TypeError(f"column {name}: unsupported dtype {npdt}")
+            dt = _NP_DTYPE[npdt]
+            ct = _COLTYPE[coltypes.get(name, "float" if dt == A.DT_F64 else "int")]
+            descs[i].dtype, descs[i].coltype, descs[i].data = dt, ct, ptr
+            dtypes.append((dt, ct))
+            if rows is None:
+                rows = n
+            elif rows != n:
+                raise ValueError("columns differ in length")
+        rows = rows or 0
+        tid = C.c_uint64()
+        fn = self.lib.tgp_table_register_device if device else self.lib.tgp_table_register
+        self._check(fn(self.h, descs, len(names), rows, C.byref(tid)), "tgp_table_register")
+        return Table(self, int(tid.value), names, rows, dtypes, keep if device else None)
+
+    # -- kernel-table boundary ------------------------------------------------
+    def kernel_execute(self, op: int, input_ptr: int, output_ptr: int | None, params: A.KernelParams):
+        r = A.KernelResultC()
+        self._check(self.lib.tgp_kernel_execute(self.h, op, input_ptr, output_ptr, C.byref(params), C.byref(r)),
+                    "tgp_kernel_execute")
+        return r
+
+    def hash_table_free(self, handle: int) -> None:
+        self._check(self.lib.tgp_hash_table_free(self.h, C.c_void_p(handle)), "tgp_hash_table_free")
+
+
+def _lit_bits(ct: int, v) -> int:
+    if ct == A.CT_FLOAT:
+        return int(np.array([float(v)], dtype=np.float64).view(np.uint64)[0])
+    return _u64(int(v))
+
+
+class Schema:
+    """Column names and (dtype, coltype) pairs; lowers expressions to C-ABI structs."""
+
+    def __init__(self, names, dtypes):
+        self.names = list(names)
+        self.dtypes = list(dtypes)
+        self._index = {n: i for i, n in enumerate(self.names)}
+
+    @classmethod
+    def of(cls, columns: dict, coltypes: dict | None = None) -> "Schema":
+        coltypes = coltypes or {}
+        dts = []
+        for name, a in columns.items():
+            dt = _NP_DTYPE[np.dtype(a.dtype)]
+            dts.append((dt, _COLTYPE[coltypes.get(name, "float" if dt == A.DT_F64 else "int")]))
+        return cls(list(columns), dts)
+
+    def index(self, name: str) -> int:
+        try:
+            return self._index[name]
+        except KeyError:
+            raise KeyError(f"unknown column {name!r}") from None
+
+    def lower_pred(self, pred: Pred | None):
+        if pred is None or not pred.ops:
+            return None, 0
+        nodes = (A.PredNode * len(pred.ops))()
+        for i, op in enumerate(pred.ops):
+            if op[0] == "leaf":
+                _, name, cmp, v, v2 = op
+                ci = self.index(name)
+                ct = self.dtypes[ci][1]
+                nodes[i].kind, nodes[i].column, nodes[i].cmp = A.PN_LEAF, ci, cmp
+                nodes[i].lit = _lit_bits(ct, v)
+                nodes[i].lit2 = _lit_bits(ct, v2)
+            else:
+                nodes[i].kind = {"and": A.PN_AND, "or": A.PN_OR, "not": A.PN_NOT}[op[0]]
+        return nodes, len(pred.ops)
+
+    def _lower_term(self, term: Term | None, agg: A.Agg, build: "Schema | None") -> None:
+        factors = term.factors if term is not None else ()
+        if len(factors) > A.MAX_FACTORS:
+            raise ValueError("at most 4 factors per aggregate")
+        agg.nfactors = len(factors)
+        for j, f in enumerate(factors):
+            if f.column is None:
+                agg.f[j].column = -1
+            elif f.side == A.SIDE_BUILD:
+                if build is None:
+                    raise ValueError("build-side column without a join")
+                agg.f[j].column = build.index(f.column)
+            else:
+                agg.f[j].column = self.index(f.column)
+            agg.f[j].side = f.side
+            agg.f[j].mul = f.mul
+            agg.f[j].add = f.add
+
+    def lower_query(self, aggs: Sequence[Agg], group_by=(), where: Pred | None = None,
+                    build: "Schema | None" = None, probe_key: str | None = None):
+        """Returns (tgp_query, keepalive); q.table and q.join are left 0."""
+        nodes, npred = self.lower_pred(where)
+        q = A.Query()
+        q.pred = nodes if nodes is not None else None
+        q.npred = npred
+        gk = (A.GroupKey * max(1, len(group_by)))()
+        for i, g in enumerate(group_by):
+            c_ = g if isinstance(g, Col) else col(g)
+            if c_.side == A.SIDE_BUILD:
+                if build is None:
+                    raise ValueError("build-side group key without a join")
+                gk[i].column = build.index(c_.name)
+            else:
+                gk[i].column = self.index(c_.name)
+            gk[i].side = c_.side
+        q.ngroup = len(group_by)
+        q.group = gk
+        ag = (A.Agg * max(1, len(aggs)))()
+        for i, a in enumerate(aggs):
+            ag[i].func = a.func
+            self._lower_term(a.term, ag[i], build)
+        q.nagg = len(aggs)
+        q.aggs = ag
+        if probe_key is not None:
+            q.probe_key_column = self.index(probe_key)
+        return q, (nodes, gk, ag)
+
+
+def decode_groups(keys: np.ndarray, vals, ngroups: int, nkeys: int, naggs: int):
+    out_keys, out_vals = [], []
+    for g in range(ngroups):
+        out_keys.append(tuple(int(np.int64(keys[g * nkeys + k])) for k in range(nkeys)))
+        row = []
+        for a in range(naggs):
+            v = vals[g * naggs + a]
+            row.append(AggResult(v.value, int(v.count), float(v.as_f64)))
+        out_vals.append(row)
+    return out_keys, out_vals
+
+
+class Table(Schema):
+    def __init__(self, ctx: Context, tid: int, names, rows, dtypes, keepalive=None):
+        super().__init__(names, dtypes)
+        self.ctx, self.id, self.rows = ctx, tid, rows
+        self._keep = keepalive
+
+    def drop(self) -> None:
+        if self.id:
+            self.ctx._check(self.ctx.lib.tgp_table_drop(self.ctx.h, self.id), "tgp_table_drop")
+            self.id = 0
+
+    def stats(self, name: str) -> tuple[int, int]:
+        lo, hi = C.c_int64(), C.c_int64()
+        self.ctx._check(self.ctx.lib.tgp_table_column_stats(self.ctx.h, self.id, self.index(name), C.byref(lo),
+                                                            C.byref(hi)), "tgp_table_column_stats")
+        return lo.value, hi.value
+
+    def reload(self, columns: dict) -> None:
+        descs = (A.ColumnDesc * len(self.names))()
+        keep = []
+        for i, name in enumerate(self.names):
+            a = np.ascontiguousarray(columns[name])
+            keep.append(a)
+            descs[i].dtype, descs[i].coltype, descs[i].data = self.dtypes[i][0], self.dtypes[i][1], a.ctypes.data
+        self.ctx._check(self.ctx.lib.tgp_table_reload(self.ctx.h, self.id, descs, len(self.names)), "tgp_table_reload")
+
+    # -- operations -----------------------------------------------------------
+    def filter(self, where: Pred | None, bitmap: bool = True, rowids: bool = True) -> FilterOutput:
+        nodes, n = self.lower_pred(where)
+        cnt = C.c_uint64()
+        bm = np.zeros((self.rows + 7) // 8, dtype=np.uint8) if bitmap else None
+        rid = np.zeros(max(1, self.rows), dtype=np.uint32) if rowids else None
+        self.ctx._check(self.ctx.lib.tgp_filter(
+            self.ctx.h, self.id, nodes, n,
+            bm.ctypes.data if bm is not None and bm.size else None,
+            rid.ctypes.data if rid is not None else None,
+            self.rows if rowids else 0, C.byref(cnt)), "tgp_filter")
+        c = int(cnt.value)
+        return FilterOutput(c, bm, rid[:c].copy() if rid is not None else None)
+
+    def aggregate(self, aggs: Sequence[Agg], group_by: Sequence[Col | str] = (), where: Pred | None = None,
+                  join: "JoinTable | None" = None, probe_key: str | None = None,
+                  group_cap: int | None = None) -> QueryOutput:
+        build = join.build if join is not None else None
+        q, keep = self.lower_query(aggs, group_by, where, build, probe_key)
+        q.table = self.id
+        if join is not None:
+            q.join = join.id
+        cap = group_cap if group_cap is not None else 1024
+        nk, na = len(group_by), len(aggs)
+        while True:
+            keys = np.zeros(max(1, cap * max(1, nk)), dtype=np.uint64)
+            vals = (A.AggValue * max(1, cap * max(1, na)))()
+            res = A.QueryResult()
+            st = self.ctx.lib.tgp_execute(self.ctx.h, C.byref(q), keys.ctypes.data, vals, cap, C.byref(res))
+            if st == A.CAPACITY and res.ngroups > cap:
+                cap = int(res.ngroups)
+                continue
+            self.ctx._check(st, "tgp_execute")
+            break
+        ks, vs = decode_groups(keys, vals, int(res.ngroups), nk, na)
+        return QueryOutput(ks, vs, int(res.rows_scanned), int(res.rows_selected), int(res.flags))
+
+    def join_build(self, key: str, where: Pred | None = None) -> "JoinTable":
+        nodes, n = self.lower_pred(where)
+        jid = C.c_uint64()
+        self.ctx._check(self.ctx.lib.tgp_join_build(self.ctx.h, self.id, self.index(key), nodes, n, C.byref(jid)),
+                        "tgp_join_build")
+        return JoinTable(self.ctx, int(jid.value), self)
+
+
+class JoinTable:
+    def __init__(self, ctx: Context, jid: int, build: Table):
+        self.ctx, self.id, self.build = ctx, jid, build
+
+    def drop(self) -> None:
+        if self.id:
+            self.ctx._check(self.ctx.lib.tgp_join_drop(self.ctx.h, self.id), "tgp_join_drop")
+            self.id = 0
+
+    def probe_pairs(self, probe: Table, probe_key: str, where: Pred | None = None):
+        nodes, n = probe.lower_pred(where)
+        npairs = C.c_uint64()
+        st = self.ctx.lib.tgp_join_probe_pairs(self.ctx.h, self.id, probe.id, probe.index(probe_key), nodes, n,
+                                               None, None, 0, C.byref(npairs))
+        if st not in (A.OK, A.CAPACITY):
+            self.ctx._check(st, "tgp_join_probe_pairs")
+        m = int(npairs.value)
+        pr = np.zeros(max(1, m), dtype=np.uint32)
+        br = np.zeros(max(1, m), dtype=np.uint32)
+        if m:
+            self.ctx._check(self.ctx.lib.tgp_join_probe_pairs(
+                self.ctx.h, self.id, probe.id, probe.index(probe_key), nodes, n, pr.ctypes.data, br.ctypes.data, m,
+                C.byref(npairs)), "tgp_join_probe_pairs")
+        return pr[:m], br[:m]
