@@ -282,6 +282,7 @@ struct Builder {
         std::memset(&P, 0, sizeof(P));
         col2slot.assign(t->cols.size(), -1);
         P.nrows = t->rows;
+        P.nthreads = 512;
         P.jslot = -1;
         P.flush_limit = ~0ull;
     }
@@ -345,7 +346,64 @@ struct Builder {
         if (maxdepth > 8) return fail(ctx, TGP_UNSUPPORTED, "predicate program deeper than 8");
         P.nops = npred;
         P.all_and = (only_and && nand + 1 == P.nleaf) ? 1u : 0u;
+        if (P.all_and) merge_conjuncts();
+        bias_leaves();
         return TGP_OK;
+    }
+
+    // In a pure conjunction, leaves on the same column intersect into one
+    // interval test (e.g. ship_day >= a AND ship_day < b), so the column is
+    // read once per row. Intervals are still in unbiased key space here.
+    void merge_conjuncts() {
+        uint32_t n = 0;
+        for (uint32_t i = 0; i < P.nleaf; ++i) {
+            Leaf cur = P.leaf[i];
+            bool merged = false;
+            const bool mergeable = cur.negate == 0 && (cur.kind == LK_U8 || cur.kind == LK_I32 || cur.kind == LK_64);
+            for (uint32_t j = 0; mergeable && j < n; ++j) {
+                Leaf& L = P.leaf[j];
+                if (L.slot != cur.slot || L.kind != cur.kind || L.negate != 0) continue;
+                if (cur.kind == LK_64) {
+                    const uint64_t lo = std::max(L.lo64, cur.lo64);
+                    const uint64_t hi = std::min(L.lo64 + L.span64, cur.lo64 + cur.span64);
+                    if (lo > hi) set_const(L, false);
+                    else { L.lo64 = lo; L.span64 = hi - lo; }
+                } else {
+                    const uint32_t lo = std::max(L.lo32, cur.lo32);
+                    const uint32_t hi = std::min(L.lo32 + L.span32, cur.lo32 + cur.span32);
+                    if (lo > hi) set_const(L, false);
+                    else { L.lo32 = lo; L.span32 = hi - lo; }
+                }
+                merged = true;
+                break;
+            }
+            if (!merged) P.leaf[n++] = cur;
+        }
+        // Order by kind so the device runs one branch-free loop per kind.
+        auto rank = [](uint8_t k) { return k == LK_I32 ? 0 : k == LK_U8 ? 1 : k == LK_64 ? 2 : 3; };
+        std::stable_sort(P.leaf, P.leaf + n, [&](const Leaf& x, const Leaf& y) { return rank(x.kind) < rank(y.kind); });
+        for (uint32_t r = 0; r < 3; ++r) {
+            uint32_t e = 0;
+            while (e < n && rank(P.leaf[e].kind) <= static_cast<int>(r)) ++e;
+            P.kend[r] = static_cast<uint8_t>(e);
+        }
+        P.kend[3] = static_cast<uint8_t>(n);
+        P.nleaf = n;
+        P.nops = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            P.ops[P.nops++] = static_cast<uint8_t>(i);
+            if (i > 0) P.ops[P.nops++] = OP_AND;
+        }
+    }
+
+    // The device tests (x - lo) <= span on the stored word x; key = x ^ xor
+    // equals x + xor modulo 2^bits, so key - lo = x - (lo - xor).
+    void bias_leaves() {
+        for (uint32_t i = 0; i < P.nleaf; ++i) {
+            Leaf& L = P.leaf[i];
+            if (L.kind == LK_64) L.lo64 -= L.xor64;
+            else if (L.kind == LK_U8 || L.kind == LK_I32) L.lo32 -= L.xor32;
+        }
     }
 
     int lower_factor(const tgp_factor& f, Factor& out, __int128* blo, __int128* bhi) {
@@ -516,7 +574,7 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes) {
 int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     if (ntiles == 0) return TGP_OK;
-    int occ = scan_occupancy(mode, acc128, P.smem_bytes);
+    int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes);
     if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
     const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * occ);
     std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
@@ -857,8 +915,10 @@ static int filter_impl(tgp_ctx* ctx, const Table* T, const tgp_pred_node* pred, 
     unsigned long long* tb = cv.take<unsigned long long>(std::max<uint64_t>(ntiles, 1));
     void* cub_tmp = cv.take<uint8_t>(cub_bytes + 16);
     uint32_t* rid_tmp = cv.take<uint32_t>(std::max<uint64_t>(rowid_scratch, 1));
-    TGP_CUDA(cudaMemsetAsync(ss.counters, 0, 32 + 16, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(ss.counters, 0, 32, ctx->stream));
+    TGP_CUDA(cudaMemsetAsync(ss.err, 0, 16, ctx->stream));
     if (words) TGP_CUDA(cudaMemsetAsync(bm, 0, words * 4, ctx->stream));
+    if (rowids_out && ntiles) TGP_CUDA(cudaMemsetAsync(tc, 0, ntiles * 4, ctx->stream));
     Plan& P = b.P;
     P.bitmap = bm;
     P.bitmap_words = static_cast<uint32_t>(std::min<uint64_t>(words, 0xffffffffull));
@@ -999,10 +1059,8 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     uint64_t ngroups_direct = 1;
     size_t extra = 0;
     const bool join = J != nullptr;
-    if (q->ngroup == 0) {
-        mode = MODE_SCALAR;
-        P.ngroups = 1;
-    } else if (D <= kDirectMaxGroups) {
+    // A scalar aggregate is the direct-indexed case with one group (D = 1).
+    if (D <= kDirectMaxGroups) {
         ngroups_direct = static_cast<uint64_t>(D);
         P.ngroups = static_cast<uint32_t>(ngroups_direct);
         uint64_t stride = 1;
@@ -1011,12 +1069,22 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             stride *= dom[k];
         }
         acc128 = b.unbounded;
-        const size_t priv = static_cast<size_t>(ngroups_direct) * nv1 * kThreads * 8 * (acc128 ? 2 : 1);
+        const size_t per_thread = static_cast<size_t>(ngroups_direct) * nv1 * 8 * (acc128 ? 2 : 1);
         const size_t shared_tab = static_cast<size_t>(ngroups_direct) * nv1 * 16;
         const size_t budget = ctx->max_dyn_smem - scan_kernel_static_smem() - kBarrierBytes;
-        if (priv + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+        // Per-thread private accumulators: 512 threads when two stages still
+        // fit beside them, else 256 threads (twice the rows per thread).
+        uint32_t nt = 0;
+        for (uint32_t cand : {512u, 256u}) {
+            if (per_thread * cand + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+                nt = cand;
+                break;
+            }
+        }
+        if (nt) {
             mode = MODE_GROUP_PRIVATE;
-            extra = priv;
+            P.nthreads = nt;
+            extra = per_thread * nt;
             if (!acc128) {
                 const uint64_t lim = b.max_abs_val ? (0x7fffffffffffffffull / b.max_abs_val) : ~0ull;
                 P.flush_limit = std::max<uint64_t>(1, lim);
@@ -1117,7 +1185,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         // Direct / scalar: emit groups with a nonzero row count in index order
         // (index order is ascending lexicographic key order).
         std::vector<uint64_t> present;
-        if (mode == MODE_SCALAR) {
+        if (q->ngroup == 0) {
             present.push_back(0);
         } else {
             for (uint64_t g = 0; g < ngroups_direct; ++g)
@@ -1430,8 +1498,9 @@ static int count_matches(tgp_ctx* ctx, const Table& probe, const JoinTable& J, u
     TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
     TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
     P.ngroups = 1;
-    TGP_TRY(size_smem(ctx, P, 0));
-    TGP_TRY(launch(ctx, P, MODE_SCALAR, false));
+    P.nthreads = 512;
+    TGP_TRY(size_smem(ctx, P, 512 * 8));  // one private count slot per thread
+    TGP_TRY(launch(ctx, P, MODE_GROUP_PRIVATE, false));
     unsigned long long acc[2];
     uint32_t err = 0;
     TGP_CUDA(cudaMemcpyAsync(acc, P.acc, 16, cudaMemcpyDeviceToHost, ctx->stream));

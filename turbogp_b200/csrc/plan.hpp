@@ -10,9 +10,10 @@
 
 namespace tgp {
 
-constexpr int kThreads = 256;                        // threads per CTA
-constexpr int kRowsPerThread = 8;                    // rows a thread owns per tile
-constexpr int kTileRows = kThreads * kRowsPerThread; // 2048 rows per tile
+// A tile is kTileRows consecutive rows; a CTA of NT threads (256 or 512, a
+// template parameter of the scan kernel) gives each thread kTileRows / NT
+// consecutive rows of it.
+constexpr int kTileRows = 2048;
 constexpr int kMaxSlots = 8;       // distinct columns staged per scan
 constexpr int kMaxLeaves = 16;     // predicate leaves
 constexpr int kMaxPredOps = 32;    // postfix program length
@@ -20,7 +21,7 @@ constexpr int kMaxVals = 8;        // value accumulators per group
 constexpr int kMaxFactors = 4;
 constexpr int kMaxGroupKeys = 4;
 constexpr int kMaxStages = 8;
-constexpr int kBarrierBytes = 128; // shared bytes reserved for the stage mbarriers
+constexpr int kBarrierBytes = 128; // shared bytes for the stage mbarriers (full[8], empty[8])
 
 // Error bits a kernel raises in its plan's error word (never __trap()).
 enum : uint32_t {
@@ -36,7 +37,7 @@ enum : uint32_t { DT_U8 = 1, DT_I32 = 2, DT_I64 = 3, DT_U64 = 4, DT_F64 = 5 };
 // Scan modes (one kernel instantiation each).
 enum : uint32_t {
     MODE_FILTER = 0,         // count selected rows; write bitmap words; per-tile counts
-    MODE_SCALAR = 1,         // scalar aggregate in registers
+    MODE_SCALAR = 1,         // scalar aggregate (host: MODE_GROUP_PRIVATE with one group)
     MODE_GROUP_PRIVATE = 2,  // direct-indexed groups, per-thread shared accumulators
     MODE_GROUP_SHARED = 3,   // direct-indexed groups, per-CTA shared table with atomics
     MODE_GROUP_GLOBAL = 4,   // direct-indexed groups, global int128 atomics
@@ -54,9 +55,11 @@ struct SlotDesc {
     uint32_t _pad;
 };
 
-// Leaf kinds after lowering. Integer leaves test (key - lo) <= span as
-// unsigned integers, where key = cell ^ xor maps the column's comparison
-// order onto unsigned order; `negate` flips the result.
+// Leaf kinds after lowering. Integer leaves test (x - lo) <= span as unsigned
+// integers on the raw stored word x (u8 zero-extended, i32 as u32, 64-bit as
+// u64): lo is pre-biased so that this equals testing key - lo' with
+// key = x ^ xor, which maps the column's comparison order onto unsigned
+// order (xor with the sign bit = adding it). `negate` flips the result.
 enum : uint8_t { LK_U8 = 0, LK_I32 = 1, LK_64 = 2, LK_F64 = 3, LK_CONST = 4 };
 enum : uint8_t { FOP_EQ_EPS = 0, FOP_NE = 1, FOP_LT = 2, FOP_LE = 3, FOP_GT = 4, FOP_GE = 5,
                  FOP_BETWEEN = 6, FOP_NOT_BETWEEN = 7 };
@@ -118,13 +121,17 @@ struct Plan {
     uint32_t extra_off;     // shared offset of per-mode scratch (accumulators)
     uint32_t smem_bytes;    // total dynamic shared memory
     uint32_t bitmap_words;  // MODE_FILTER: bitmap words written (0 = none)
+    uint32_t nthreads;      // CTA size the plan's shared memory was sized for (256 or 512)
+    uint32_t _p2;
     SlotDesc slot[kMaxSlots];
 
     // WHERE program
     uint32_t nleaf;
     uint32_t nops;
     uint32_t all_and;       // program is a conjunction of all leaves
-    uint32_t _p0;
+    // For conjunctions the host orders leaves by kind: [0, kend[0]) LK_I32,
+    // [kend[0], kend[1]) LK_U8, [kend[1], kend[2]) LK_64, the rest any kind.
+    uint8_t kend[4];
     Leaf leaf[kMaxLeaves];
     uint8_t ops[kMaxPredOps];
 

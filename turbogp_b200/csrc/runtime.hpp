@@ -18,7 +18,7 @@ namespace tgp {
 
 // Launchers implemented in the .cu files.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st);
-int scan_occupancy(uint32_t mode, bool acc128, size_t dyn_smem);
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem);
 size_t scan_kernel_static_smem();
 cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
                                  int sms, cudaStream_t st);

@@ -4,12 +4,15 @@
 // One CTA per SM slot walks tiles of kTileRows rows (tile = blockIdx.x +
 // k * gridDim.x). Thread 0 streams the referenced columns of upcoming tiles
 // into a ring of shared-memory stages with 1-D bulk copies
-// (cp.async.bulk ... mbarrier::complete_tx); every thread evaluates the
-// lowered WHERE program on its 8 rows of the current stage into an 8-bit
-// mask, then feeds the selected rows to the mode's sink (bitmap words, scalar
-// int128 registers, per-thread or per-CTA group accumulators, global hash
-// groups, join build / probe). The final partial tile is read straight from
-// global memory with bounds checks.
+// (cp.async.bulk ... mbarrier::complete_tx). Each of the NT threads owns
+// R = kTileRows / NT consecutive rows of the current stage: it reads them with
+// 128-bit shared loads (chunk order rotated per thread so a quarter-warp never
+// hits the same banks twice), evaluates the lowered WHERE program into an
+// R-bit mask with one subtract and one unsigned compare per row and leaf, and
+// feeds the selected rows to the mode's sink (bitmap words, per-thread or
+// per-CTA group accumulators, global group / join hash tables, join pairs).
+// The final partial tile is read straight from global memory with bounds
+// checks.
 //
 // Reference semantics each piece restates:
 //   predicate leaves  — apply_comparison (src/engine/query_interpreter/expr.rs:1468-1530),
@@ -53,15 +56,9 @@ __device__ __forceinline__ int64_t load_cell_ro(const uint8_t* base, uint32_t dt
     return static_cast<int64_t>(__ldg(reinterpret_cast<const long long*>(base) + row));
 }
 
-__device__ __forceinline__ uint32_t valid_bits(uint32_t tid, uint32_t nrem) {
-    uint32_t v = 0;
-#pragma unroll
-    for (int j = 0; j < kRowsPerThread; ++j) v |= (j * kThreads + tid < nrem ? 1u : 0u) << j;
-    return v;
-}
-
 // ---------------------------------------------------------------------------
-// Predicate evaluation: 8 rows (j * kThreads + tid) per call → 8-bit mask.
+// Predicate evaluation: thread t owns rows R*t .. R*t+R-1 of the tile; the
+// result is an R-bit mask (bit j = row R*t + j).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool f64_leaf(uint8_t fop, double x, double a, double b) {
     switch (fop) {
@@ -76,75 +73,147 @@ __device__ __forceinline__ bool f64_leaf(uint8_t fop, double x, double a, double
     }
 }
 
-template <bool TAIL>
-__device__ __forceinline__ uint32_t eval_leaf(const Leaf& L, const uint8_t* base, uint32_t tid,
-                                              uint32_t nrem) {
+__device__ __forceinline__ uint32_t in32(uint32_t x, uint32_t lo, uint32_t sp) {
+    return (x - lo) <= sp ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint32_t in64(uint64_t x, uint64_t lo, uint64_t sp) {
+    return (x - lo) <= sp ? 1u : 0u;
+}
+
+// Loads the C 16-byte chunks of thread t's span (C * 16 bytes at base + C*16*t)
+// in rotated order and calls f(chunk_index, value). Rotating by t / (8 / C)
+// makes the 8 threads of a shared-memory phase touch 8 different 16-byte bank
+// groups, so every load is conflict-free.
+template <int C, typename F>
+__device__ __forceinline__ void for_chunks(const uint8_t* base, uint32_t t, F&& f) {
+    const uint4* p = reinterpret_cast<const uint4*>(base) + static_cast<size_t>(C) * t;
+    const uint32_t rot = (C == 1) ? 0u : (t / (8 / C)) & (C - 1);
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        const uint32_t q = (k + rot) & (C - 1);
+        f(q, p[q]);
+    }
+}
+
+template <int R>
+__device__ __forceinline__ uint32_t leaf_smem(const Leaf& L, const uint8_t* base, uint32_t t) {
     uint32_t m = 0;
     switch (L.kind) {
         case LK_U8: {
-            const uint32_t x = L.xor32, lo = L.lo32, sp = L.span32;
+            const uint32_t lo = L.lo32, sp = L.span32;
+            if (R == 4) {
+                const uint32_t w = reinterpret_cast<const uint32_t*>(base)[t];
 #pragma unroll
-            for (int j = 0; j < kRowsPerThread; ++j) {
-                const uint32_t r = j * kThreads + tid;
-                if (!TAIL || r < nrem) {
-                    const uint32_t k = static_cast<uint32_t>(base[r]) ^ x;
-                    m |= ((k - lo) <= sp ? 1u : 0u) << j;
+                for (int e = 0; e < 4; ++e) m |= in32((w >> (8 * e)) & 0xffu, lo, sp) << e;
+            } else {
+                const uint2 w = reinterpret_cast<const uint2*>(base)[t];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    m |= in32((w.x >> (8 * e)) & 0xffu, lo, sp) << e;
+                    m |= in32((w.y >> (8 * e)) & 0xffu, lo, sp) << (e + 4);
                 }
             }
             break;
         }
         case LK_I32: {
-            const uint32_t* c = reinterpret_cast<const uint32_t*>(base);
-            const uint32_t x = L.xor32, lo = L.lo32, sp = L.span32;
-#pragma unroll
-            for (int j = 0; j < kRowsPerThread; ++j) {
-                const uint32_t r = j * kThreads + tid;
-                if (!TAIL || r < nrem) {
-                    const uint32_t k = c[r] ^ x;
-                    m |= ((k - lo) <= sp ? 1u : 0u) << j;
-                }
-            }
+            const uint32_t lo = L.lo32, sp = L.span32;
+            for_chunks<R / 4>(base, t, [&](uint32_t q, const uint4& v) {
+                const uint32_t b = in32(v.x, lo, sp) | (in32(v.y, lo, sp) << 1) | (in32(v.z, lo, sp) << 2) |
+                                   (in32(v.w, lo, sp) << 3);
+                m |= b << (4 * q);
+            });
             break;
         }
         case LK_64: {
-            const uint64_t* c = reinterpret_cast<const uint64_t*>(base);
-            const uint64_t x = L.xor64, lo = L.lo64, sp = L.span64;
-#pragma unroll
-            for (int j = 0; j < kRowsPerThread; ++j) {
-                const uint32_t r = j * kThreads + tid;
-                if (!TAIL || r < nrem) {
-                    const uint64_t k = c[r] ^ x;
-                    m |= ((k - lo) <= sp ? 1u : 0u) << j;
-                }
-            }
+            const uint64_t lo = L.lo64, sp = L.span64;
+            for_chunks<R / 2>(base, t, [&](uint32_t q, const uint4& v) {
+                const uint64_t a = (static_cast<uint64_t>(v.y) << 32) | v.x;
+                const uint64_t b = (static_cast<uint64_t>(v.w) << 32) | v.z;
+                m |= (in64(a, lo, sp) | (in64(b, lo, sp) << 1)) << (2 * q);
+            });
             break;
         }
         case LK_F64: {
-            const double* c = reinterpret_cast<const double*>(base);
-#pragma unroll
-            for (int j = 0; j < kRowsPerThread; ++j) {
-                const uint32_t r = j * kThreads + tid;
-                if (!TAIL || r < nrem) m |= (f64_leaf(L.fop, c[r], L.f1, L.f2) ? 1u : 0u) << j;
-            }
+            for_chunks<R / 2>(base, t, [&](uint32_t q, const uint4& v) {
+                const double a = __longlong_as_double(static_cast<long long>((static_cast<uint64_t>(v.y) << 32) | v.x));
+                const double b = __longlong_as_double(static_cast<long long>((static_cast<uint64_t>(v.w) << 32) | v.z));
+                const uint32_t r = (f64_leaf(L.fop, a, L.f1, L.f2) ? 1u : 0u) |
+                                   ((f64_leaf(L.fop, b, L.f1, L.f2) ? 1u : 0u) << 1);
+                m |= r << (2 * q);
+            });
             break;
         }
         default:
-            return L.negate ? 0xFFu : 0u;  // LK_CONST
+            return L.negate ? 0xffffffffu : 0u;  // LK_CONST
     }
-    return L.negate ? (m ^ 0xFFu) : m;
+    return L.negate ? ~m : m;
 }
 
-template <bool TAIL>
-__device__ __forceinline__ uint32_t eval_pred(const Plan& P, const uint8_t* stage, uint64_t r0,
-                                              uint32_t tid, uint32_t nrem) {
-    const uint32_t valid = TAIL ? valid_bits(tid, nrem) : 0xFFu;
+// Tail tile: global memory, rows past nrem are never read.
+template <int R>
+__device__ __forceinline__ uint32_t leaf_global(const Leaf& L, const uint8_t* base, uint32_t t,
+                                                uint32_t nrem, uint32_t dtype) {
+    if (L.kind == LK_CONST) return L.negate ? 0xffffffffu : 0u;
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const uint32_t r = R * t + j;
+        if (r >= nrem) break;
+        uint32_t c;
+        if (L.kind == LK_F64) {
+            c = f64_leaf(L.fop, reinterpret_cast<const double*>(base)[r], L.f1, L.f2) ? 1u : 0u;
+        } else if (L.kind == LK_64) {
+            c = in64(reinterpret_cast<const uint64_t*>(base)[r], L.lo64, L.span64);
+        } else {
+            const uint32_t x = dtype == DT_U8 ? static_cast<uint32_t>(base[r]) : reinterpret_cast<const uint32_t*>(base)[r];
+            c = in32(x, L.lo32, L.span32);
+        }
+        m |= c << j;
+    }
+    return L.negate ? ~m : m;
+}
+
+template <int R, bool TAIL>
+__device__ __forceinline__ uint32_t eval_leaf(const Plan& P, const Leaf& L, const uint8_t* stage, uint64_t r0,
+                                              uint32_t t, uint32_t nrem) {
+    const uint8_t* base = slot_base<TAIL>(P, stage, L.slot, r0);
+    if (TAIL) return leaf_global<R>(L, base, t, nrem, P.slot[L.slot].dtype);
+    return leaf_smem<R>(L, base, t);
+}
+
+template <int R>
+__device__ __forceinline__ uint32_t leaf_i32(const Leaf& L, const uint8_t* stage, const Plan& P, uint32_t t) {
+    const uint8_t* base = stage + P.slot[L.slot].smem_off;
+    const uint32_t lo = L.lo32, sp = L.span32;
+    uint32_t m = 0;
+    for_chunks<R / 4>(base, t, [&](uint32_t q, const uint4& v) {
+        const uint32_t b = in32(v.x, lo, sp) | (in32(v.y, lo, sp) << 1) | (in32(v.z, lo, sp) << 2) |
+                           (in32(v.w, lo, sp) << 3);
+        m |= b << (4 * q);
+    });
+    return L.negate ? ~m : m;
+}
+
+template <int R, bool TAIL>
+__device__ __forceinline__ uint32_t eval_pred(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t t,
+                                              uint32_t nrem) {
+    constexpr uint32_t kAll = (R == 32) ? 0xffffffffu : ((1u << R) - 1u);
+    uint32_t valid = kAll;
+    if (TAIL) {
+        const uint32_t first = R * t;
+        valid = first >= nrem ? 0u : (nrem - first >= static_cast<uint32_t>(R) ? kAll : ((1u << (nrem - first)) - 1u));
+    }
     if (P.nleaf == 0) return valid;
     if (P.all_and) {
         uint32_t m = valid;
-        for (uint32_t i = 0; i < P.nleaf; ++i) {
-            const Leaf& L = P.leaf[i];
-            m &= eval_leaf<TAIL>(L, slot_base<TAIL>(P, stage, L.slot, r0), tid, nrem);
+        uint32_t i = 0;
+        if (!TAIL) {
+            // Leaves grouped by kind: branch-free loop bodies for the common kinds.
+            for (; i < P.kend[0]; ++i) m &= leaf_i32<R>(P.leaf[i], stage, P, t);
+            for (; i < P.kend[2]; ++i) m &= leaf_smem<R>(P.leaf[i], stage + P.slot[P.leaf[i].slot].smem_off, t);
         }
+        for (; i < P.nleaf; ++i) m &= eval_leaf<R, TAIL>(P, P.leaf[i], stage, r0, t, nrem);
         return m;
     }
     // General postfix program on an 8-deep register stack (depth checked on host).
@@ -152,11 +221,10 @@ __device__ __forceinline__ uint32_t eval_pred(const Plan& P, const uint8_t* stag
     for (uint32_t i = 0; i < P.nops; ++i) {
         const uint8_t op = P.ops[i];
         if (op < kMaxLeaves) {
-            const Leaf& L = P.leaf[op];
-            const uint32_t v = eval_leaf<TAIL>(L, slot_base<TAIL>(P, stage, L.slot, r0), tid, nrem);
+            const uint32_t v = eval_leaf<R, TAIL>(P, P.leaf[op], stage, r0, t, nrem);
             s7 = s6; s6 = s5; s5 = s4; s4 = s3; s3 = s2; s2 = s1; s1 = s0; s0 = v;
         } else if (op == OP_NOT) {
-            s0 = s0 ^ 0xFFu;
+            s0 = ~s0;
         } else {
             s0 = (op == OP_AND) ? (s0 & s1) : (s0 | s1);
             s1 = s2; s2 = s3; s3 = s4; s4 = s5; s5 = s6; s6 = s7; s7 = 0;
@@ -168,51 +236,48 @@ __device__ __forceinline__ uint32_t eval_pred(const Plan& P, const uint8_t* stag
 // ---------------------------------------------------------------------------
 // Per-row argument of a value accumulator: wrapping i64 product of affine
 // factors (mul * cell + add). `brow` is the matched build row for factors that
-// read the build side of a join.
+// read the build side of a join. Loops stay rolled: the code runs only for
+// selected rows, and a small body keeps the hot loop in the instruction cache.
 // ---------------------------------------------------------------------------
 template <bool TAIL>
-__device__ __forceinline__ int64_t eval_val(const Plan& P, const ValDesc& V, const uint8_t* stage,
-                                            uint64_t r0, uint32_t rl, uint32_t brow,
-                                            uint32_t& ovf) {
+__device__ __forceinline__ int64_t eval_val(const Plan& P, const ValDesc& V, const uint8_t* stage, uint64_t r0,
+                                            uint32_t rl, uint32_t brow, uint32_t& ovf) {
     int64_t acc = 1;
-#pragma unroll
-    for (int f = 0; f < kMaxFactors; ++f) {
-        if (f < V.nf) {
-            const Factor& F = V.f[f];
-            int64_t x = 0;
-            if (F.slot >= 0) {
-                x = load_cell(slot_base<TAIL>(P, stage, F.slot, r0), P.slot[F.slot].dtype, rl);
-            } else if (F.build_side) {
-                x = load_cell_ro(F.bptr, F.dtype, brow);
-            }
-            int64_t t;
-            if (P.check_ovf) {
-                t = add_wrap_checked(mul_wrap_checked(F.mul, x, ovf), F.add, ovf);
-                acc = (f == 0) ? t : mul_wrap_checked(acc, t, ovf);
-            } else {
-                t = static_cast<int64_t>(static_cast<uint64_t>(F.mul) * static_cast<uint64_t>(x) +
-                                         static_cast<uint64_t>(F.add));
-                acc = (f == 0) ? t
-                               : static_cast<int64_t>(static_cast<uint64_t>(acc) *
-                                                      static_cast<uint64_t>(t));
-            }
+#pragma unroll 1
+    for (int f = 0; f < V.nf; ++f) {
+        const Factor& F = V.f[f];
+        int64_t x = 0;
+        if (F.slot >= 0) {
+            x = load_cell(slot_base<TAIL>(P, stage, F.slot, r0), P.slot[F.slot].dtype, rl);
+        } else if (F.build_side) {
+            x = load_cell_ro(F.bptr, F.dtype, brow);
+        }
+        int64_t t;
+        if (P.check_ovf) {
+            t = add_wrap_checked(mul_wrap_checked(F.mul, x, ovf), F.add, ovf);
+            acc = (f == 0) ? t : mul_wrap_checked(acc, t, ovf);
+        } else {
+            t = static_cast<int64_t>(static_cast<uint64_t>(F.mul) * static_cast<uint64_t>(x) +
+                                     static_cast<uint64_t>(F.add));
+            acc = (f == 0) ? t : static_cast<int64_t>(static_cast<uint64_t>(acc) * static_cast<uint64_t>(t));
         }
     }
     return acc;
 }
 
 template <bool TAIL>
-__device__ __forceinline__ int64_t key_cell(const Plan& P, const GKey& K, const uint8_t* stage,
-                                            uint64_t r0, uint32_t rl, uint32_t brow) {
+__device__ __forceinline__ int64_t key_cell(const Plan& P, const GKey& K, const uint8_t* stage, uint64_t r0,
+                                            uint32_t rl, uint32_t brow) {
     if (K.build_side) return load_cell_ro(K.bptr, K.dtype, brow);
     return load_cell(slot_base<TAIL>(P, stage, K.slot, r0), P.slot[K.slot].dtype, rl);
 }
 
 // Direct group index: sum over keys of (cell - min) * stride.
 template <bool TAIL>
-__device__ __forceinline__ uint32_t group_index(const Plan& P, const uint8_t* stage, uint64_t r0,
-                                                uint32_t rl, uint32_t brow) {
+__device__ __forceinline__ uint32_t group_index(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t rl,
+                                                uint32_t brow) {
     uint64_t g = 0;
+#pragma unroll 1
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         const GKey& K = P.gkey[k];
         const int64_t c = key_cell<TAIL>(P, K, stage, r0, rl, brow);
@@ -223,9 +288,10 @@ __device__ __forceinline__ uint32_t group_index(const Plan& P, const uint8_t* st
 
 // Packed exact key for MODE_GROUP_HASH.
 template <bool TAIL>
-__device__ __forceinline__ uint64_t group_hash_key(const Plan& P, const uint8_t* stage,
-                                                   uint64_t r0, uint32_t rl, uint32_t brow) {
+__device__ __forceinline__ uint64_t group_hash_key(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t rl,
+                                                   uint32_t brow) {
     uint64_t key = 0;
+#pragma unroll 1
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         const GKey& K = P.gkey[k];
         const int64_t c = key_cell<TAIL>(P, K, stage, r0, rl, brow);
@@ -263,8 +329,17 @@ __device__ __forceinline__ void join_foreach(const Plan& P, uint64_t rel, F&& f)
 // ---------------------------------------------------------------------------
 // Accumulator helpers
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint8_t slot_kind(const Plan& P, uint32_t v) {
+    return v == 0 ? VK_SUM : P.val[v - 1].kind;  // value slot 0 is the row count
+}
+
+__device__ __forceinline__ long long kind_identity(uint8_t kind) {
+    return kind == VK_MIN ? 0x7fffffffffffffffll
+                          : kind == VK_MAX ? static_cast<long long>(0x8000000000000000ull) : 0ll;
+}
+
 __device__ __forceinline__ void acc_init(I128& a, uint8_t kind) {
-    a.lo = (kind == VK_MIN) ? 0x7fffffffffffffffull : (kind == VK_MAX ? 0x8000000000000000ull : 0ull);
+    a.lo = static_cast<uint64_t>(kind_identity(kind));
     a.hi = 0;
 }
 
@@ -290,7 +365,11 @@ __device__ __forceinline__ void acc_combine(I128& a, uint8_t kind, const I128& b
     }
 }
 
-// Global accumulator pair at word index `w` (lo at w, hi at w + 1).
+__device__ __forceinline__ bool acc_untouched(const I128& a, uint8_t kind) {
+    return a.lo == static_cast<uint64_t>(kind_identity(kind)) && a.hi == 0;
+}
+
+// Global accumulator pair (lo at slot[0], hi at slot[1]).
 __device__ __forceinline__ void acc_global(unsigned long long* slot, uint8_t kind, const I128& v) {
     if (kind == VK_MIN) {
         atomicMin(reinterpret_cast<long long*>(slot), static_cast<long long>(v.lo));
@@ -314,31 +393,56 @@ __device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory layout of per-mode scratch
+// Sinks. Shared-memory scratch layouts (nv1 = 1 + nval; value slot 0 is the
+// group's row count):
+//   MODE_GROUP_PRIVATE, int64 partials:  word (g * nv1 + v) * NT + t
+//   MODE_GROUP_PRIVATE, int128 partials: words ((g * nv1 + v) * 2 + limb) * NT + t
+//   MODE_GROUP_SHARED:                   words (g * nv1 + v) * 2 + limb (carry atomics)
+// MODE_SCALAR runs as MODE_GROUP_PRIVATE with a single group.
 // ---------------------------------------------------------------------------
-// MODE_GROUP_PRIVATE, int64 partials: word ((g * nv1 + v) * kThreads + tid)
-// MODE_GROUP_PRIVATE, int128 partials: words ((g * nv1 + v) * 2 + limb) * kThreads + tid
-// MODE_GROUP_SHARED: words (g * nv1 + v) * 2 + limb (int128 via carry atomics)
-// (nv1 = 1 + nval; value slot 0 is the group's row count.)
+// Barrier 1 over the NT consumer threads only (the producer warp never joins).
+template <int NT>
+__device__ __forceinline__ void consumer_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
 
-template <uint32_t MODE, bool ACC128>
+template <uint32_t MODE, bool ACC128, int NT>
 struct Sink {
-    // Scalar-mode registers.
-    I128 acc[kMaxVals];
-    unsigned long long count;
     uint32_t ovf;
-    uint64_t upd;   // MODE_GROUP_PRIVATE int64: updates since the last flush
+    uint64_t upd;  // MODE_GROUP_PRIVATE int64: updates since the last flush
+
+    __device__ __forceinline__ void init(const Plan& P, uint8_t* extra, uint32_t t) {
+        ovf = 0;
+        upd = 0;
+        const uint32_t nv1 = P.nval + 1;
+        long long* w = reinterpret_cast<long long*>(extra);
+        if (MODE == MODE_GROUP_PRIVATE) {
+            for (uint32_t i = 0; i < P.ngroups * nv1; ++i) {
+                const long long init = kind_identity(slot_kind(P, i % nv1));
+                if (ACC128) {
+                    w[(i * 2 + 0) * NT + t] = init;
+                    w[(i * 2 + 1) * NT + t] = 0;
+                } else {
+                    w[i * NT + t] = init;
+                }
+            }
+        } else if (MODE == MODE_GROUP_SHARED) {
+            for (uint32_t i = t; i < P.ngroups * nv1; i += NT) {
+                w[2 * i] = kind_identity(slot_kind(P, i % nv1));
+                w[2 * i + 1] = 0;
+            }
+        }
+    }
 
     // Moves this thread's int64 private partials into the global int128
     // accumulators and resets them.
-    __device__ __forceinline__ void flush_private_thread(const Plan& P, uint8_t* extra, uint32_t tid) {
+    __device__ __noinline__ void flush_private_thread(const Plan& P, uint8_t* extra, uint32_t t) {
         const uint32_t nv1 = P.nval + 1;
         long long* w = reinterpret_cast<long long*>(extra);
         for (uint32_t i = 0; i < P.ngroups * nv1; ++i) {
-            const uint32_t v = i % nv1;
-            const uint8_t kind = v == 0 ? VK_SUM : P.val[v - 1].kind;
+            const uint8_t kind = slot_kind(P, i % nv1);
             if (kind == VK_MIN || kind == VK_MAX) continue;
-            long long& a = w[i * kThreads + tid];
+            long long& a = w[i * NT + t];
             if (a != 0) {
                 I128 x;
                 x.lo = static_cast<uint64_t>(a);
@@ -349,80 +453,38 @@ struct Sink {
         }
     }
 
-    __device__ __forceinline__ void init(const Plan& P, uint8_t* extra, uint32_t tid) {
-        count = 0;
-        ovf = 0;
-        upd = 0;
-#pragma unroll
-        for (int v = 0; v < kMaxVals; ++v) acc_init(acc[v], v < (int)P.nval ? P.val[v].kind : VK_SUM);
-        if (MODE == MODE_GROUP_PRIVATE) {
-            const uint32_t nv1 = P.nval + 1;
-            long long* w = reinterpret_cast<long long*>(extra);
-            for (uint32_t g = 0; g < P.ngroups; ++g) {
-                for (uint32_t v = 0; v < nv1; ++v) {
-                    const uint8_t kind = v == 0 ? VK_SUM : P.val[v - 1].kind;
-                    const long long init = kind == VK_MIN ? 0x7fffffffffffffffll
-                                           : kind == VK_MAX ? static_cast<long long>(0x8000000000000000ull) : 0ll;
-                    if (ACC128) {
-                        w[((g * nv1 + v) * 2 + 0) * kThreads + tid] = init;
-                        w[((g * nv1 + v) * 2 + 1) * kThreads + tid] = 0;
-                    } else {
-                        w[(g * nv1 + v) * kThreads + tid] = init;
-                    }
-                }
-            }
-        } else if (MODE == MODE_GROUP_SHARED) {
-            const uint32_t nv1 = P.nval + 1;
-            long long* w = reinterpret_cast<long long*>(extra);
-            for (uint32_t i = tid; i < P.ngroups * nv1; i += kThreads) {
-                const uint32_t v = i % nv1;
-                const uint8_t kind = v == 0 ? VK_SUM : P.val[v - 1].kind;
-                w[2 * i] = kind == VK_MIN ? 0x7fffffffffffffffll
-                           : kind == VK_MAX ? static_cast<long long>(0x8000000000000000ull) : 0ll;
-                w[2 * i + 1] = 0;
-            }
-        }
-    }
-
     // One selected (row[, build row]) pair.
     template <bool TAIL>
-    __device__ __forceinline__ void row(const Plan& P, uint8_t* extra, const uint8_t* stage,
-                                        uint64_t r0, uint32_t rl, uint32_t brow, uint32_t tid) {
-        if (MODE == MODE_SCALAR) {
-            count += 1;
-#pragma unroll
-            for (int v = 0; v < kMaxVals; ++v) {
-                if (v < (int)P.nval) {
-                    const int64_t x = eval_val<TAIL>(P, P.val[v], stage, r0, rl, brow, ovf);
-                    acc_update(acc[v], P.val[v].kind, x);
-                }
-            }
-        } else if (MODE == MODE_GROUP_PRIVATE) {
-            const uint32_t nv1 = P.nval + 1;
+    __device__ __forceinline__ void row(const Plan& P, uint8_t* extra, const uint8_t* stage, uint64_t r0,
+                                        uint32_t rl, uint32_t brow, uint32_t t) {
+        const uint32_t nv1 = P.nval + 1;
+        if (MODE == MODE_GROUP_PRIVATE) {
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
             long long* w = reinterpret_cast<long long*>(extra);
             if (ACC128) {
-                uint64_t* lo = reinterpret_cast<uint64_t*>(&w[((g * nv1) * 2 + 0) * kThreads + tid]);
-                long long* hi = &w[((g * nv1) * 2 + 1) * kThreads + tid];
+                uint64_t* lo = reinterpret_cast<uint64_t*>(&w[((g * nv1) * 2 + 0) * NT + t]);
+                long long* hi = &w[((g * nv1) * 2 + 1) * NT + t];
                 const uint64_t nl = *lo + 1;
                 *hi += (nl == 0) ? 1 : 0;
                 *lo = nl;
+#pragma unroll 1
                 for (uint32_t v = 1; v < nv1; ++v) {
                     const ValDesc& V = P.val[v - 1];
                     const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                    uint64_t* plo = reinterpret_cast<uint64_t*>(&w[((g * nv1 + v) * 2 + 0) * kThreads + tid]);
-                    long long* phi = &w[((g * nv1 + v) * 2 + 1) * kThreads + tid];
+                    uint64_t* plo = reinterpret_cast<uint64_t*>(&w[((g * nv1 + v) * 2 + 0) * NT + t]);
+                    long long* phi = &w[((g * nv1 + v) * 2 + 1) * NT + t];
                     I128 a{*plo, *phi};
                     acc_update(a, V.kind, x);
                     *plo = a.lo;
                     *phi = a.hi;
                 }
             } else {
-                w[(g * nv1) * kThreads + tid] += 1;
+                w[(g * nv1) * NT + t] += 1;
+#pragma unroll 1
                 for (uint32_t v = 1; v < nv1; ++v) {
                     const ValDesc& V = P.val[v - 1];
                     const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                    long long& a = w[(g * nv1 + v) * kThreads + tid];
+                    long long& a = w[(g * nv1 + v) * NT + t];
                     if (V.kind == VK_SUM) a = static_cast<long long>(static_cast<uint64_t>(a) + static_cast<uint64_t>(x));
                     else if (V.kind == VK_COUNT_NZ) a += (x != 0);
                     else if (V.kind == VK_MIN) a = min(a, static_cast<long long>(x));
@@ -432,16 +494,15 @@ struct Sink {
                 // int64 partial could be one update away from wrapping: move
                 // this thread's partials into the global int128 accumulators.
                 if (++upd >= P.flush_limit) {
-                    flush_private_thread(P, extra, tid);
+                    flush_private_thread(P, extra, t);
                     upd = 0;
                 }
             }
         } else if (MODE == MODE_GROUP_SHARED) {
-            // Per-CTA int128 table: word pair ((g * nv1 + v) * 2, +1).
-            const uint32_t nv1 = P.nval + 1;
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
             unsigned long long* w = reinterpret_cast<unsigned long long*>(extra);
             atomicAdd(&w[(g * nv1) * 2], 1ull);
+#pragma unroll 1
             for (uint32_t v = 1; v < nv1; ++v) {
                 const ValDesc& V = P.val[v - 1];
                 const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
@@ -463,14 +524,13 @@ struct Sink {
                 }
             }
         } else if (MODE == MODE_GROUP_GLOBAL) {
-            const uint32_t nv1 = P.nval + 1;
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
             unsigned long long* a = P.acc + static_cast<uint64_t>(g) * nv1 * 2;
             atomicAdd(a, 1ull);
+#pragma unroll 1
             for (uint32_t v = 1; v < nv1; ++v) {
                 const ValDesc& V = P.val[v - 1];
-                const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                acc_global_i64(a + 2 * v, V.kind, x);
+                acc_global_i64(a + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf));
             }
         } else if (MODE == MODE_GROUP_HASH) {
             const uint64_t key = group_hash_key<TAIL>(P, stage, r0, rl, brow);
@@ -491,10 +551,10 @@ struct Sink {
                 return;
             }
             atomicAdd(slot + 1, 1ull);
+#pragma unroll 1
             for (uint32_t v = 0; v < P.nval; ++v) {
                 const ValDesc& V = P.val[v];
-                const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                acc_global_i64(slot + 2 + 2 * v, V.kind, x);
+                acc_global_i64(slot + 2 + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf));
             }
         } else if (MODE == MODE_JOIN_BUILD) {
             // Scanned table is the build side; P.jslot is its key column.
@@ -505,13 +565,10 @@ struct Sink {
             bool done = false;
             for (uint64_t n = 0; n <= P.jmask && !done; ++n) {
                 if (!P.jwide) {
-                    const unsigned long long e = (rel << 32) | row;
-                    done = atomicCAS(P.jtab + h, kEmpty, e) == kEmpty;
-                } else {
-                    if (atomicCAS(P.jtab + 2 * h + 1, 0ull, static_cast<unsigned long long>(row) + 1) == 0ull) {
-                        P.jtab[2 * h] = rel;
-                        done = true;
-                    }
+                    done = atomicCAS(P.jtab + h, kEmpty, (rel << 32) | row) == kEmpty;
+                } else if (atomicCAS(P.jtab + 2 * h + 1, 0ull, static_cast<unsigned long long>(row) + 1) == 0ull) {
+                    P.jtab[2 * h] = rel;
+                    done = true;
                 }
                 h = (h + 1) & P.jmask;
             }
@@ -520,52 +577,23 @@ struct Sink {
     }
 
     // End of kernel: merge partials into global results.
-    __device__ __forceinline__ void flush(const Plan& P, uint8_t* extra, uint32_t tid,
-                                          I128* red /* shared: 8 warps x kMaxVals */,
-                                          unsigned long long* redc) {
-        const uint32_t lane = tid & 31u, warp = tid >> 5;
-        if (MODE == MODE_SCALAR) {
-            unsigned long long c = count;
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
-            if (lane == 0) redc[warp] = c;
-#pragma unroll
-            for (int v = 0; v < kMaxVals; ++v) {
-                if (v < (int)P.nval) {
-                    I128 a = acc[v];
-                    const uint8_t kind = P.val[v].kind;
-#pragma unroll
-                    for (int d = 16; d > 0; d >>= 1) acc_combine(a, kind, shfl_down_i128(a, d));
-                    if (lane == 0) red[warp * kMaxVals + v] = a;
-                }
-            }
-            __syncthreads();
-            if (tid == 0) {
-                unsigned long long tc = 0;
-                for (int w = 0; w < kThreads / 32; ++w) tc += redc[w];
-                if (tc) atomicAdd(P.acc, tc);
-                for (uint32_t v = 0; v < P.nval; ++v) {
-                    I128 a = red[v];
-                    for (int w = 1; w < kThreads / 32; ++w) acc_combine(a, P.val[v].kind, red[w * kMaxVals + v]);
-                    acc_global(P.acc + 2 * (v + 1), P.val[v].kind, a);
-                }
-            }
-        } else if (MODE == MODE_GROUP_PRIVATE) {
-            __syncthreads();
-            const uint32_t nv1 = P.nval + 1;
+    __device__ __forceinline__ void flush(const Plan& P, uint8_t* extra, uint32_t t) {
+        const uint32_t lane = t & 31u, warp = t >> 5;
+        const uint32_t nv1 = P.nval + 1;
+        if (MODE == MODE_GROUP_PRIVATE) {
+            consumer_sync<NT>();
             const long long* w = reinterpret_cast<const long long*>(extra);
-            for (uint32_t idx = warp; idx < P.ngroups * nv1; idx += kThreads / 32) {
-                const uint32_t v = idx % nv1;
-                const uint8_t kind = v == 0 ? VK_SUM : P.val[v - 1].kind;
+            for (uint32_t idx = warp; idx < P.ngroups * nv1; idx += NT / 32) {
+                const uint8_t kind = slot_kind(P, idx % nv1);
                 I128 a;
                 acc_init(a, kind);
-                for (uint32_t t = lane; t < kThreads; t += 32) {
+                for (uint32_t u = lane; u < static_cast<uint32_t>(NT); u += 32) {
                     I128 b;
                     if (ACC128) {
-                        b.lo = static_cast<uint64_t>(w[(idx * 2 + 0) * kThreads + t]);
-                        b.hi = w[(idx * 2 + 1) * kThreads + t];
+                        b.lo = static_cast<uint64_t>(w[(idx * 2 + 0) * NT + u]);
+                        b.hi = w[(idx * 2 + 1) * NT + u];
                     } else {
-                        const long long x = w[idx * kThreads + t];
+                        const long long x = w[idx * NT + u];
                         b.lo = static_cast<uint64_t>(x);
                         b.hi = (kind == VK_MIN || kind == VK_MAX) ? 0 : (x >> 63);
                     }
@@ -573,27 +601,17 @@ struct Sink {
                 }
 #pragma unroll
                 for (int d = 16; d > 0; d >>= 1) acc_combine(a, kind, shfl_down_i128(a, d));
-                if (lane == 0) {
-                    const bool untouched = (kind == VK_MIN) ? (a.lo == 0x7fffffffffffffffull)
-                                           : (kind == VK_MAX) ? (a.lo == 0x8000000000000000ull)
-                                                              : (a.lo == 0 && a.hi == 0);
-                    if (!untouched) acc_global(P.acc + 2ull * idx, kind, a);
-                }
+                if (lane == 0 && !acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
             }
         } else if (MODE == MODE_GROUP_SHARED) {
-            __syncthreads();
-            const uint32_t nv1 = P.nval + 1;
+            consumer_sync<NT>();
             const long long* w = reinterpret_cast<const long long*>(extra);
-            for (uint32_t idx = tid; idx < P.ngroups * nv1; idx += kThreads) {
-                const uint32_t v = idx % nv1;
-                const uint8_t kind = v == 0 ? VK_SUM : P.val[v - 1].kind;
+            for (uint32_t idx = t; idx < P.ngroups * nv1; idx += NT) {
+                const uint8_t kind = slot_kind(P, idx % nv1);
                 I128 a;
                 a.lo = static_cast<uint64_t>(w[2 * idx]);
                 a.hi = w[2 * idx + 1];
-                const bool untouched = (kind == VK_MIN) ? (a.lo == 0x7fffffffffffffffull)
-                                       : (kind == VK_MAX) ? (a.lo == 0x8000000000000000ull)
-                                                          : (a.lo == 0 && a.hi == 0);
-                if (!untouched) acc_global(P.acc + 2ull * idx, kind, a);
+                if (!acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
             }
         }
         if (ovf) atomicOr(P.err, kErrRowOverflow);
@@ -601,263 +619,246 @@ struct Sink {
 };
 
 // ---------------------------------------------------------------------------
-// Tile processing
+// Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128, bool TAIL>
-__device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128>& sink,
-                                             uint8_t* extra, const uint8_t* stage, uint64_t tile,
-                                             uint32_t tid, unsigned long long* tile_sel) {
+template <uint32_t MODE, bool ACC128, int NT, bool TAIL>
+__device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
+                                             const uint8_t* stage, uint64_t tile, uint32_t t,
+                                             unsigned long long& selected) {
+    constexpr int R = kTileRows / NT;
     const uint64_t r0 = tile * kTileRows;
-    const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : kTileRows;
-    const uint32_t m = eval_pred<TAIL>(P, stage, r0, tid, nrem);
-    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
+    const uint32_t m = eval_pred<R, TAIL>(P, stage, r0, t, nrem);
+    const uint32_t lane = t & 31u;
+    selected += __popc(m);
 
     if (MODE == MODE_FILTER) {
-        const uint64_t w0 = r0 / 32;
+        // 32 / R consecutive lanes hold the bits of one 32-row bitmap word.
+        constexpr uint32_t G = 32 / R;
+        uint32_t v = m << (R * (lane % G));
 #pragma unroll
-        for (int j = 0; j < kRowsPerThread; ++j) {
-            const uint32_t word = __ballot_sync(kFull, (m >> j) & 1u);
-            const uint64_t wi = w0 + j * (kThreads / 32) + warp;
-            if (lane == 0 && wi < P.bitmap_words) P.bitmap[wi] = word;
+        for (uint32_t d = 1; d < G; d <<= 1) v |= __shfl_xor_sync(kFull, v, d);
+        if (lane % G == 0) {
+            const uint64_t wi = (r0 + static_cast<uint64_t>(R) * t) / 32;
+            if (wi < P.bitmap_words) P.bitmap[wi] = v;
         }
-        unsigned c = __popc(m);
+        if (P.tile_counts) {
+            unsigned c = __popc(m);
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
-        if (lane == 0 && c) atomicAdd(tile_sel, static_cast<unsigned long long>(c));
-        return;
-    }
-
-    unsigned csel = __popc(m);
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) csel += __shfl_down_sync(kFull, csel, d);
-    if (lane == 0 && csel) atomicAdd(tile_sel, static_cast<unsigned long long>(csel));
-
-    if (MODE == MODE_SCALAR && P.jslot < 0) {
-        sink.count += __popc(m);
-        if (P.nval == 0) return;
-#pragma unroll
-        for (int j = 0; j < kRowsPerThread; ++j) {
-            const bool take = (m >> j) & 1u;
-            if (__any_sync(kFull, take) && take) {
-                const uint32_t rl = j * kThreads + tid;
-#pragma unroll
-                for (int v = 0; v < kMaxVals; ++v) {
-                    if (v < (int)P.nval) {
-                        const int64_t x = eval_val<TAIL>(P, P.val[v], stage, r0, rl, 0, sink.ovf);
-                        acc_update(sink.acc[v], P.val[v].kind, x);
-                    }
-                }
-            }
+            for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(kFull, c, d);
+            if (lane == 0 && c) atomicAdd(P.tile_counts + tile, c);
         }
         return;
     }
 
     if (MODE == MODE_JOIN_PAIRS) {
-#pragma unroll 1
-        for (int j = 0; j < kRowsPerThread; ++j) {
-            const bool take = (m >> j) & 1u;
-            if (!__any_sync(kFull, take)) continue;
-            const uint32_t rl = j * kThreads + tid;
-            uint64_t rel = 0;
-            uint32_t nmatch = 0;
-            bool probe = false;
-            if (take) {
-                const int64_t c = load_cell(slot_base<TAIL>(P, stage, P.jslot, r0), P.slot[P.jslot].dtype, rl);
-                probe = join_rel(P, c, rel);
-                if (probe) join_foreach(P, rel, [&](uint32_t) { ++nmatch; });
-            }
-            // Warp-aggregated reservation of nmatch output pairs.
-            uint32_t incl = nmatch;
+        const uint8_t* kb = slot_base<TAIL>(P, stage, P.jslot, r0);
+        const uint32_t kdt = P.slot[P.jslot].dtype;
+        uint32_t nmatch = 0;
+        for (uint32_t sel = m; sel; sel &= sel - 1) {
+            uint64_t rel;
+            if (join_rel(P, load_cell(kb, kdt, R * t + __ffs(sel) - 1), rel))
+                join_foreach(P, rel, [&](uint32_t) { ++nmatch; });
+        }
+        // Warp-aggregated reservation of this warp's output pairs.
+        uint32_t incl = nmatch;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t y = __shfl_up_sync(kFull, incl, d);
-                if (lane >= (uint32_t)d) incl += y;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            unsigned long long base = 0;
-            if (lane == 31 && total) base = atomicAdd(P.counters + 1, static_cast<unsigned long long>(total));
-            base = __shfl_sync(kFull, base, 31);
-            if (nmatch) {
-                unsigned long long o = base + incl - nmatch;
-                const uint32_t prow = static_cast<uint32_t>(r0 + rl);
-                unsigned long long* out = P.out_pairs;
-                join_foreach(P, rel, [&](uint32_t b) {
-                    if (o < P.out_cap) out[o] = (static_cast<unsigned long long>(prow) << 32) | b;
-                    ++o;
-                });
-            }
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= static_cast<uint32_t>(d)) incl += y;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        unsigned long long base = 0;
+        if (lane == 31 && total) base = atomicAdd(P.counters + 1, static_cast<unsigned long long>(total));
+        base = __shfl_sync(kFull, base, 31);
+        unsigned long long o = base + incl - nmatch;
+        for (uint32_t sel = nmatch ? m : 0u; sel; sel &= sel - 1) {
+            const uint32_t rl = R * t + __ffs(sel) - 1;
+            uint64_t rel;
+            if (!join_rel(P, load_cell(kb, kdt, rl), rel)) continue;
+            const unsigned long long prow = static_cast<unsigned long long>(r0 + rl) << 32;
+            join_foreach(P, rel, [&](uint32_t b) {
+                if (o < P.out_cap) P.out_pairs[o] = prow | b;
+                ++o;
+            });
         }
         return;
     }
 
-    // Generic sink path: grouped modes, join build, and joined aggregates.
-#pragma unroll 1
-    for (int j = 0; j < kRowsPerThread; ++j) {
-        const bool take = (m >> j) & 1u;
-        if (!__any_sync(kFull, take) || !take) continue;
-        const uint32_t rl = j * kThreads + tid;
+    // Grouped / scalar aggregates, join build, and joined aggregates.
+    for (uint32_t sel = m; sel; sel &= sel - 1) {
+        const uint32_t rl = R * t + __ffs(sel) - 1;
         if (P.jslot >= 0 && MODE != MODE_JOIN_BUILD) {
             const int64_t c = load_cell(slot_base<TAIL>(P, stage, P.jslot, r0), P.slot[P.jslot].dtype, rl);
             uint64_t rel;
-            if (join_rel(P, c, rel)) {
-                join_foreach(P, rel, [&](uint32_t b) { sink.template row<TAIL>(P, extra, stage, r0, rl, b, tid); });
-            }
+            if (join_rel(P, c, rel))
+                join_foreach(P, rel, [&](uint32_t b) { sink.template row<TAIL>(P, extra, stage, r0, rl, b, t); });
         } else {
-            sink.template row<TAIL>(P, extra, stage, r0, rl, 0, tid);
+            sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t);
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// The persistent kernel
+// The persistent kernel: NT consumer threads + one producer warp.
+//
+// Stage s has two mbarriers: full[s] (producer arrive + TMA transaction bytes)
+// and empty[s] (one arrive per consumer warp once it has read the stage). The
+// producer waits on empty[s] before refilling stage s; consumers wait on
+// full[s]. No CTA-wide barrier runs per tile. Every wait is bounded; a wait
+// that gives up raises kErrWaitTimeout and the CTA drains its copies.
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128>
-__global__ void __launch_bounds__(kThreads, 1) scan_kernel(const __grid_constant__ Plan P) {
+template <uint32_t MODE, bool ACC128, int NT>
+__global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant__ Plan P) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + kMaxStages;
     uint8_t* stages = smem + kBarrierBytes;
     uint8_t* extra = smem + P.extra_off;
-    __shared__ I128 red[(kThreads / 32) * kMaxVals];
-    __shared__ unsigned long long redc[kThreads / 32];
-    __shared__ unsigned long long tile_sel;
+    __shared__ uint32_t abort_flag;
 
-    const uint32_t tid = threadIdx.x;
+    const uint32_t t = threadIdx.x;
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     const uint64_t nfull = P.nrows / kTileRows;
     const uint32_t S = P.nstages;
     const uint64_t G = gridDim.x;
+    constexpr uint32_t kConsumerWarps = NT / 32;
 
-    Sink<MODE, ACC128> sink;
-    sink.init(P, extra, tid);
-
-    uint64_t policy = 0;
-    if (tid == 0) {
-        for (uint32_t s = 0; s < S; ++s) mbar_init(&full[s], 1);
+    Sink<MODE, ACC128, NT> sink;
+    if (t < static_cast<uint32_t>(NT)) sink.init(P, extra, t);
+    if (t == static_cast<uint32_t>(NT)) {
+        for (uint32_t s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
         fence_barrier_init();
-        policy = l2_policy_evict_first();
+        abort_flag = 0;
     }
-    if (tid == 0) tile_sel = 0;
     __syncthreads();
 
-    auto issue = [&](uint64_t tile, uint32_t s) {
-        uint8_t* dst = stages + static_cast<size_t>(s) * P.stage_bytes;
-        mbar_arrive_expect_tx(&full[s], P.stage_bytes);
-        for (uint32_t c = 0; c < P.nslots; ++c) {
-            const uint32_t bytes = kTileRows * P.slot[c].width;
-            bulk_g2s(dst + P.slot[c].smem_off, P.slot[c].ptr + tile * bytes, bytes, &full[s], policy);
-        }
-    };
-
-    if (tid == 0) {
-        for (uint32_t s = 0; s < S; ++s) {
-            const uint64_t t = blockIdx.x + s * G;
-            if (t < nfull) issue(t, s);
-        }
-    }
-
-    bool timed_out = false;
-    uint64_t k = 0;
-    for (;; ++k) {
-        const uint64_t t = blockIdx.x + k * G;
-        if (t >= ntiles) break;
-        if (t < nfull) {
+    if (t >= static_cast<uint32_t>(NT)) {
+        // ---------------- producer warp (lane 0 issues) ----------------
+        if (t != static_cast<uint32_t>(NT)) return;
+        const uint64_t policy = l2_policy_evict_first();
+        uint64_t issued = 0;
+        for (uint64_t k = 0;; ++k) {
+            const uint64_t tl = blockIdx.x + k * G;
+            if (tl >= nfull) break;
             const uint32_t s = static_cast<uint32_t>(k % S);
-            const uint32_t parity = static_cast<uint32_t>((k / S) & 1u);
-            const bool ok = mbar_wait_bounded(&full[s], parity);
-            if (__syncthreads_or(!ok)) {
-                timed_out = true;
-                break;
+            if (k >= S) {
+                // Wait until every consumer warp has released tile k - S.
+                if (!mbar_wait_bounded(&empty[s], static_cast<uint32_t>(((k / S) - 1) & 1u))) {
+                    atomicOr(P.err, kErrWaitTimeout);
+                    atomicExch(&abort_flag, 1u);
+                    break;
+                }
             }
-            process_tile<MODE, ACC128, false>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
-                                              t, tid, &tile_sel);
-            __syncthreads();
-            if (tid == 0) {
-                if (MODE == MODE_FILTER && P.tile_counts) P.tile_counts[t] = static_cast<uint32_t>(tile_sel);
-                if (tile_sel) atomicAdd(P.counters, tile_sel);
-                tile_sel = 0;
-                const uint64_t tn = t + S * G;
-                if (tn < nfull) issue(tn, s);
+            if (*reinterpret_cast<volatile uint32_t*>(&abort_flag)) break;
+            uint8_t* dst = stages + static_cast<size_t>(s) * P.stage_bytes;
+            mbar_arrive_expect_tx(&full[s], P.stage_bytes);
+            for (uint32_t c = 0; c < P.nslots; ++c) {
+                const uint32_t bytes = kTileRows * P.slot[c].width;
+                bulk_g2s(dst + P.slot[c].smem_off, P.slot[c].ptr + tl * bytes, bytes, &full[s], policy);
             }
-        } else {
-            process_tile<MODE, ACC128, true>(P, sink, extra, nullptr, t, tid, &tile_sel);
-            __syncthreads();
-            if (tid == 0) {
-                if (MODE == MODE_FILTER && P.tile_counts) P.tile_counts[t] = static_cast<uint32_t>(tile_sel);
-                if (tile_sel) atomicAdd(P.counters, tile_sel);
-                tile_sel = 0;
-            }
+            ++issued;
         }
-        __syncthreads();
-    }
-
-    if (timed_out) {
-        // Let every copy this CTA issued land (bounded) before the CTA exits.
-        if (tid == 0) {
-            atomicOr(P.err, kErrWaitTimeout);
-            for (uint64_t i = k; i < k + S; ++i) {
-                const uint64_t t = blockIdx.x + i * G;
-                if (t >= nfull) break;
-                mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u));
-            }
-        }
-        __syncthreads();
+        // Drain: the last min(S, issued) copies have landed before this thread
+        // exits (earlier ones were waited for through empty[]).
+        const uint64_t first = issued > S ? issued - S : 0;
+        for (uint64_t i = first; i < issued; ++i)
+            if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P.err, kErrWaitTimeout);
         return;
     }
-    sink.flush(P, extra, tid, red, redc);
+
+    // ---------------- consumers ----------------
+    const uint32_t lane = t & 31u;
+    unsigned long long selected = 0;
+    bool ok = true;
+    for (uint64_t k = 0;; ++k) {
+        const uint64_t tl = blockIdx.x + k * G;
+        if (tl >= ntiles) break;
+        if (tl < nfull) {
+            const uint32_t s = static_cast<uint32_t>(k % S);
+            const uint32_t parity = static_cast<uint32_t>((k / S) & 1u);
+            bool landed = false;
+            if (lane == 0) landed = mbar_wait_bounded(&full[s], parity);
+            landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
+            if (!landed || *reinterpret_cast<volatile uint32_t*>(&abort_flag)) {
+                if (lane == 0) {
+                    atomicOr(P.err, kErrWaitTimeout);
+                    atomicExch(&abort_flag, 1u);
+                }
+                ok = false;
+                break;
+            }
+            // Lanes other than 0 observe the completed phase through a cheap
+            // try_wait so their shared-memory reads are ordered after the copy.
+            mbar_try_wait(&full[s], parity);
+            process_tile<MODE, ACC128, NT, false>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
+                                                  tl, t, selected);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        } else {
+            process_tile<MODE, ACC128, NT, true>(P, sink, extra, nullptr, tl, t, selected);
+        }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) selected += __shfl_down_sync(kFull, selected, d);
+    if (lane == 0 && selected) atomicAdd(P.counters, selected);
+    // Every consumer reaches the flush, also after a timeout (the host then
+    // discards the result), so the consumer barrier inside it always completes.
+    (void)ok;
+    sink.flush(P, extra, t);
 }
 
 // ---------------------------------------------------------------------------
-// Host launcher
+// Host launchers
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128>
-static cudaError_t launch_mode(const Plan& P, int grid, cudaStream_t st) {
-    auto kern = scan_kernel<MODE, ACC128>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(P.smem_bytes));
-    if (e != cudaSuccess) return e;
-    kern<<<grid, kThreads, P.smem_bytes, st>>>(P);
-    return cudaGetLastError();
+template <uint32_t MODE, bool ACC128, int NT>
+static const void* kernel_ptr() {
+    return reinterpret_cast<const void*>(scan_kernel<MODE, ACC128, NT>);
 }
 
+template <int NT>
+static const void* select_kernel(uint32_t mode, bool acc128) {
+    switch (mode) {
+        case MODE_FILTER: return kernel_ptr<MODE_FILTER, false, NT>();
+        case MODE_SCALAR:
+        case MODE_GROUP_PRIVATE:
+            return acc128 ? kernel_ptr<MODE_GROUP_PRIVATE, true, NT>() : kernel_ptr<MODE_GROUP_PRIVATE, false, NT>();
+        case MODE_GROUP_SHARED: return kernel_ptr<MODE_GROUP_SHARED, false, NT>();
+        case MODE_GROUP_GLOBAL: return kernel_ptr<MODE_GROUP_GLOBAL, false, NT>();
+        case MODE_GROUP_HASH: return kernel_ptr<MODE_GROUP_HASH, false, NT>();
+        case MODE_JOIN_BUILD: return kernel_ptr<MODE_JOIN_BUILD, false, NT>();
+        case MODE_JOIN_PAIRS: return kernel_ptr<MODE_JOIN_PAIRS, false, NT>();
+        default: return nullptr;
+    }
+}
+
+static const void* select_kernel(uint32_t mode, bool acc128, int nt) {
+    return nt == 512 ? select_kernel<512>(mode, acc128) : nt == 256 ? select_kernel<256>(mode, acc128) : nullptr;
+}
+
+// Launches with blockDim = nthreads consumers + one producer warp.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st) {
-    switch (mode) {
-        case MODE_FILTER: return launch_mode<MODE_FILTER, false>(P, grid, st);
-        case MODE_SCALAR: return launch_mode<MODE_SCALAR, false>(P, grid, st);
-        case MODE_GROUP_PRIVATE:
-            return acc128 ? launch_mode<MODE_GROUP_PRIVATE, true>(P, grid, st)
-                          : launch_mode<MODE_GROUP_PRIVATE, false>(P, grid, st);
-        case MODE_GROUP_SHARED: return launch_mode<MODE_GROUP_SHARED, false>(P, grid, st);
-        case MODE_GROUP_GLOBAL: return launch_mode<MODE_GROUP_GLOBAL, false>(P, grid, st);
-        case MODE_GROUP_HASH: return launch_mode<MODE_GROUP_HASH, false>(P, grid, st);
-        case MODE_JOIN_BUILD: return launch_mode<MODE_JOIN_BUILD, false>(P, grid, st);
-        case MODE_JOIN_PAIRS: return launch_mode<MODE_JOIN_PAIRS, false>(P, grid, st);
-        default: return cudaErrorInvalidValue;
-    }
+    const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads));
+    if (!f) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P.smem_bytes));
+    if (e != cudaSuccess) return e;
+    void* args[] = {const_cast<Plan*>(&P)};
+    return cudaLaunchKernel(f, dim3(grid), dim3(P.nthreads + 32), args, P.smem_bytes, st);
 }
 
-int scan_occupancy(uint32_t mode, bool acc128, size_t dyn_smem) {
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem) {
+    const void* f = select_kernel(mode, acc128, nt);
+    if (!f) return 0;
     int n = 0;
-    const void* f = nullptr;
-    switch (mode) {
-        case MODE_FILTER: f = (const void*)scan_kernel<MODE_FILTER, false>; break;
-        case MODE_SCALAR: f = (const void*)scan_kernel<MODE_SCALAR, false>; break;
-        case MODE_GROUP_PRIVATE:
-            f = acc128 ? (const void*)scan_kernel<MODE_GROUP_PRIVATE, true>
-                       : (const void*)scan_kernel<MODE_GROUP_PRIVATE, false>;
-            break;
-        case MODE_GROUP_SHARED: f = (const void*)scan_kernel<MODE_GROUP_SHARED, false>; break;
-        case MODE_GROUP_GLOBAL: f = (const void*)scan_kernel<MODE_GROUP_GLOBAL, false>; break;
-        case MODE_GROUP_HASH: f = (const void*)scan_kernel<MODE_GROUP_HASH, false>; break;
-        case MODE_JOIN_BUILD: f = (const void*)scan_kernel<MODE_JOIN_BUILD, false>; break;
-        case MODE_JOIN_PAIRS: f = (const void*)scan_kernel<MODE_JOIN_PAIRS, false>; break;
-        default: return 0;
-    }
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn_smem)) !=
         cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kThreads, dyn_smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, nt + 32, dyn_smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -865,8 +866,6 @@ int scan_occupancy(uint32_t mode, bool acc128, size_t dyn_smem) {
 }
 
 // Static shared memory used by scan_kernel besides the dynamic stages.
-size_t scan_kernel_static_smem() {
-    return sizeof(I128) * (kThreads / 32) * kMaxVals + sizeof(unsigned long long) * (kThreads / 32 + 1);
-}
+size_t scan_kernel_static_smem() { return 128; }
 
 }  // namespace tgp
