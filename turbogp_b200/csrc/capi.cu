@@ -433,6 +433,8 @@ struct Builder {
             int slot;
             TGP_TRY(slot_of(static_cast<uint32_t>(f.column), &slot));
             out.slot = static_cast<int8_t>(slot);
+            out.dtype = static_cast<uint8_t>(P.slot[slot].dtype);
+            out.soff = P.slot[slot].smem_off;
         }
         const __int128 m = f.mul, a = f.add;
         const __int128 x0 = m * c.min + a, x1 = m * c.max + a;
@@ -1041,6 +1043,8 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             int s;
             TGP_TRY(b.slot_of(gk.column, &s));
             K.slot = static_cast<int8_t>(s);
+            K.dtype = static_cast<uint8_t>(b.P.slot[s].dtype);
+            K.soff = b.P.slot[s].smem_off;
         }
         K.min = c.min;
         kmin[k] = c.min;

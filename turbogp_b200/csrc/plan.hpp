@@ -88,8 +88,9 @@ enum : uint8_t { VK_SUM = 0, VK_MIN = 1, VK_MAX = 2, VK_COUNT_NZ = 3 };
 struct Factor {
     int8_t slot;          // staged column slot, or -1 for a constant
     uint8_t build_side;   // 1: gather from a build-side column at the matched build row
-    uint8_t dtype;        // build-side gather dtype
-    uint8_t _pad[5];
+    uint8_t dtype;        // dtype of the staged or build-side column
+    uint8_t _pad;
+    uint32_t soff;        // staged: the slot's offset inside a stage
     const uint8_t* bptr;  // build-side column (device)
     int64_t mul;
     int64_t add;
@@ -105,9 +106,9 @@ struct ValDesc {
 struct GKey {
     int8_t slot;          // staged slot (probe/own side)
     uint8_t build_side;   // 1: key column lives on the build side
-    uint8_t dtype;        // build-side gather dtype
+    uint8_t dtype;        // dtype of the staged or build-side column
     uint8_t shift;        // MODE_GROUP_HASH: bit position in the packed key
-    uint32_t _pad;
+    uint32_t soff;        // staged: the slot's offset inside a stage
     const uint8_t* bptr;
     int64_t min;          // key cell minimum (from column statistics)
     uint64_t stride;      // direct modes: multiplier of (cell - min) in the group index

@@ -248,7 +248,7 @@ __device__ __forceinline__ int64_t eval_val(const Plan& P, const ValDesc& V, con
         const Factor& F = V.f[f];
         int64_t x = 0;
         if (F.slot >= 0) {
-            x = load_cell(slot_base<TAIL>(P, stage, F.slot, r0), P.slot[F.slot].dtype, rl);
+            x = load_cell(TAIL ? slot_base<true>(P, stage, F.slot, r0) : stage + F.soff, F.dtype, rl);
         } else if (F.build_side) {
             x = load_cell_ro(F.bptr, F.dtype, brow);
         }
@@ -269,7 +269,7 @@ template <bool TAIL>
 __device__ __forceinline__ int64_t key_cell(const Plan& P, const GKey& K, const uint8_t* stage, uint64_t r0,
                                             uint32_t rl, uint32_t brow) {
     if (K.build_side) return load_cell_ro(K.bptr, K.dtype, brow);
-    return load_cell(slot_base<TAIL>(P, stage, K.slot, r0), P.slot[K.slot].dtype, rl);
+    return load_cell(TAIL ? slot_base<true>(P, stage, K.slot, r0) : stage + K.soff, K.dtype, rl);
 }
 
 // Direct group index: sum over keys of (cell - min) * stride.
@@ -686,8 +686,7 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     }
 
     // Grouped / scalar aggregates, join build, and joined aggregates.
-    for (uint32_t sel = m; sel; sel &= sel - 1) {
-        const uint32_t rl = R * t + __ffs(sel) - 1;
+    auto one_row = [&](uint32_t rl) {
         if (P.jslot >= 0 && MODE != MODE_JOIN_BUILD) {
             const int64_t c = load_cell(slot_base<TAIL>(P, stage, P.jslot, r0), P.slot[P.jslot].dtype, rl);
             uint64_t rel;
@@ -696,7 +695,10 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
         } else {
             sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t);
         }
-    }
+    };
+    // Each iteration handles the next selected row of every lane at once, so a
+    // sparse selection costs max(rows per lane) iterations, not the total.
+    for (uint32_t sel = m; sel; sel &= sel - 1) one_row(R * t + __ffs(sel) - 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -741,13 +743,14 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
         if (t != static_cast<uint32_t>(NT)) return;
         const uint64_t policy = l2_policy_evict_first();
         uint64_t issued = 0;
+        uint32_t s = 0, phase = 0;  // stage and phase of tile k (k = issued)
         for (uint64_t k = 0;; ++k) {
             const uint64_t tl = blockIdx.x + k * G;
             if (tl >= nfull) break;
-            const uint32_t s = static_cast<uint32_t>(k % S);
             if (k >= S) {
-                // Wait until every consumer warp has released tile k - S.
-                if (!mbar_wait_bounded(&empty[s], static_cast<uint32_t>(((k / S) - 1) & 1u))) {
+                // Wait until every consumer warp has released tile k - S
+                // (the previous use of stage s, one phase earlier).
+                if (!mbar_wait_bounded(&empty[s], phase ^ 1u)) {
                     atomicOr(P.err, kErrWaitTimeout);
                     atomicExch(&abort_flag, 1u);
                     break;
@@ -761,6 +764,10 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
                 bulk_g2s(dst + P.slot[c].smem_off, P.slot[c].ptr + tl * bytes, bytes, &full[s], policy);
             }
             ++issued;
+            if (++s == S) {
+                s = 0;
+                phase ^= 1u;
+            }
         }
         // Drain: the last min(S, issued) copies have landed before this thread
         // exits (earlier ones were waited for through empty[]).
@@ -774,14 +781,11 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
     const uint32_t lane = t & 31u;
     unsigned long long selected = 0;
     bool ok = true;
-    for (uint64_t k = 0;; ++k) {
-        const uint64_t tl = blockIdx.x + k * G;
-        if (tl >= ntiles) break;
+    uint32_t s = 0, phase = 0;  // stage and phase of the k-th full tile
+    for (uint64_t tl = blockIdx.x; tl < ntiles; tl += G) {
         if (tl < nfull) {
-            const uint32_t s = static_cast<uint32_t>(k % S);
-            const uint32_t parity = static_cast<uint32_t>((k / S) & 1u);
             bool landed = false;
-            if (lane == 0) landed = mbar_wait_bounded(&full[s], parity);
+            if (lane == 0) landed = mbar_wait_bounded(&full[s], phase);
             landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
             if (!landed || *reinterpret_cast<volatile uint32_t*>(&abort_flag)) {
                 if (lane == 0) {
@@ -793,11 +797,15 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
             }
             // Lanes other than 0 observe the completed phase through a cheap
             // try_wait so their shared-memory reads are ordered after the copy.
-            mbar_try_wait(&full[s], parity);
+            mbar_try_wait(&full[s], phase);
             process_tile<MODE, ACC128, NT, false>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
                                                   tl, t, selected);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
+            if (++s == S) {
+                s = 0;
+                phase ^= 1u;
+            }
         } else {
             process_tile<MODE, ACC128, NT, true>(P, sink, extra, nullptr, tl, t, selected);
         }
