@@ -282,7 +282,7 @@ struct Builder {
         std::memset(&P, 0, sizeof(P));
         col2slot.assign(t->cols.size(), -1);
         P.nrows = t->rows;
-        P.nthreads = 512;
+        P.nthreads = static_cast<uint32_t>(c->scan_threads);
         P.jslot = -1;
         P.flush_limit = ~0ull;
     }
@@ -685,6 +685,7 @@ int tgp_init(tgp_ctx** out, int device) {
         return TGP_DEVICE_ERROR;
     }
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("TGP_SCAN_THREADS")) ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
     if (const char* e = std::getenv("TGP_MAX_STAGES"))
         ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
     *out = ctx;
@@ -1079,7 +1080,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         // Per-thread private accumulators: 512 threads when two stages still
         // fit beside them, else 256 threads (twice the rows per thread).
         uint32_t nt = 0;
-        for (uint32_t cand : {512u, 256u}) {
+        for (uint32_t cand : {static_cast<uint32_t>(ctx->scan_threads), 256u}) {
             if (per_thread * cand + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
                 nt = cand;
                 break;
@@ -1088,6 +1089,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         if (nt) {
             mode = MODE_GROUP_PRIVATE;
             P.nthreads = nt;
+            P.count_by_tile = (q->ngroup == 0 && !J) ? 1u : 0u;
             extra = per_thread * nt;
             if (!acc128) {
                 const uint64_t lim = b.max_abs_val ? (0x7fffffffffffffffull / b.max_abs_val) : ~0ull;

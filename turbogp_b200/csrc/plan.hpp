@@ -139,6 +139,8 @@ struct Plan {
     // Values (per group: slot 0 = row count, slots 1..nval = values)
     uint32_t nval;
     uint32_t check_ovf;     // per-row overflow detection needed
+    uint32_t count_by_tile; // MODE_GROUP_PRIVATE, one group, no join: row count = popcount per tile
+    uint32_t _p3;
     uint64_t flush_limit;   // MODE_GROUP_PRIVATE int64: per-thread updates between flushes
     ValDesc val[kMaxVals];
 

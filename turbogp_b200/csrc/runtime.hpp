@@ -102,7 +102,8 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS).
     int ctas_per_sm = 1;
+    int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
 };

@@ -195,6 +195,59 @@ __device__ __forceinline__ uint32_t leaf_i32(const Leaf& L, const uint8_t* stage
     return L.negate ? ~m : m;
 }
 
+// A conjunction of at most kRegLeaves I32 leaves, kept in registers for the
+// whole kernel (no constant-bank loads per tile).
+constexpr int kRegLeaves = 4;
+struct RegLeaves {
+    uint32_t n;       // 0 = not applicable
+    uint32_t neg;     // bit i: leaf i negated
+    uint32_t soff[kRegLeaves];
+    uint32_t lo[kRegLeaves];
+    uint32_t sp[kRegLeaves];
+};
+
+__device__ __forceinline__ void load_reg_leaves(const Plan& P, RegLeaves& L) {
+    L.n = (P.all_and && P.nleaf <= kRegLeaves && P.kend[0] == P.nleaf) ? P.nleaf : 0u;
+    L.neg = 0;
+#pragma unroll
+    for (int i = 0; i < kRegLeaves; ++i) {
+        const bool use = static_cast<uint32_t>(i) < L.n;
+        L.soff[i] = use ? P.slot[P.leaf[i].slot].smem_off : 0u;
+        L.lo[i] = use ? P.leaf[i].lo32 : 0u;
+        L.sp[i] = use ? P.leaf[i].span32 : 0u;
+        if (use && P.leaf[i].negate) L.neg |= 1u << i;
+    }
+}
+
+template <int R, int N>
+__device__ __forceinline__ uint32_t eval_reg_leaves_n(const RegLeaves& L, const uint8_t* stage, uint32_t t) {
+    uint32_t m = 0xffffffffu;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const uint32_t lo = L.lo[i], sp = L.sp[i];
+        uint32_t b = 0;
+        for_chunks<R / 4>(stage + L.soff[i], t, [&](uint32_t q, const uint4& v) {
+            const uint32_t c = in32(v.x, lo, sp) | (in32(v.y, lo, sp) << 1) | (in32(v.z, lo, sp) << 2) |
+                               (in32(v.w, lo, sp) << 3);
+            b |= c << (4 * q);
+        });
+        m &= ((L.neg >> i) & 1u) ? ~b : b;
+    }
+    return m & ((1u << R) - 1u);
+}
+
+// Straight-line code per leaf count, so loads of all leaves can be in flight
+// together.
+template <int R>
+__device__ __forceinline__ uint32_t eval_reg_leaves(const RegLeaves& L, const uint8_t* stage, uint32_t t) {
+    switch (L.n) {
+        case 1: return eval_reg_leaves_n<R, 1>(L, stage, t);
+        case 2: return eval_reg_leaves_n<R, 2>(L, stage, t);
+        case 3: return eval_reg_leaves_n<R, 3>(L, stage, t);
+        default: return eval_reg_leaves_n<R, 4>(L, stage, t);
+    }
+}
+
 template <int R, bool TAIL>
 __device__ __forceinline__ uint32_t eval_pred(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t t,
                                               uint32_t nrem) {
@@ -462,11 +515,13 @@ struct Sink {
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
             long long* w = reinterpret_cast<long long*>(extra);
             if (ACC128) {
-                uint64_t* lo = reinterpret_cast<uint64_t*>(&w[((g * nv1) * 2 + 0) * NT + t]);
-                long long* hi = &w[((g * nv1) * 2 + 1) * NT + t];
-                const uint64_t nl = *lo + 1;
-                *hi += (nl == 0) ? 1 : 0;
-                *lo = nl;
+                if (!P.count_by_tile) {
+                    uint64_t* lo = reinterpret_cast<uint64_t*>(&w[((g * nv1) * 2 + 0) * NT + t]);
+                    long long* hi = &w[((g * nv1) * 2 + 1) * NT + t];
+                    const uint64_t nl = *lo + 1;
+                    *hi += (nl == 0) ? 1 : 0;
+                    *lo = nl;
+                }
 #pragma unroll 1
                 for (uint32_t v = 1; v < nv1; ++v) {
                     const ValDesc& V = P.val[v - 1];
@@ -479,7 +534,7 @@ struct Sink {
                     *phi = a.hi;
                 }
             } else {
-                w[(g * nv1) * NT + t] += 1;
+                if (!P.count_by_tile) w[(g * nv1) * NT + t] += 1;
 #pragma unroll 1
                 for (uint32_t v = 1; v < nv1; ++v) {
                     const ValDesc& V = P.val[v - 1];
@@ -619,18 +674,98 @@ struct Sink {
 };
 
 // ---------------------------------------------------------------------------
+// Register-resident value descriptors for the scalar fast path: up to two
+// SUM values, each a product of up to two staged affine factors, int64
+// private partials, no per-row overflow checks (the host proved the bound).
+// ---------------------------------------------------------------------------
+struct RegVals {
+    uint32_t on;        // fast path applies
+    uint32_t nv;        // 1 or 2
+    uint32_t nf[2];     // 1 or 2
+    uint32_t soff[2][2];
+    uint32_t dt[2][2];
+    int64_t mul[2][2];
+    int64_t add[2][2];
+};
+
+template <uint32_t MODE, bool ACC128>
+__device__ __forceinline__ void load_reg_vals(const Plan& P, RegVals& V) {
+    bool on = MODE == MODE_GROUP_PRIVATE && !ACC128 && P.count_by_tile && !P.check_ovf && P.jslot < 0 &&
+              P.ngkey == 0 && P.nval >= 1 && P.nval <= 2;
+    V.nv = P.nval;
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+        const bool use = static_cast<uint32_t>(v) < P.nval;
+        const ValDesc& D = P.val[use ? v : 0];
+        if (use && (D.kind != VK_SUM || D.nf < 1 || D.nf > 2)) on = false;
+        V.nf[v] = use ? D.nf : 0u;
+#pragma unroll
+        for (int f = 0; f < 2; ++f) {
+            const bool uf = use && static_cast<uint32_t>(f) < D.nf;
+            const Factor& F = D.f[uf ? f : 0];
+            if (uf && F.slot < 0) on = false;
+            V.soff[v][f] = uf ? F.soff : 0u;
+            V.dt[v][f] = uf ? F.dtype : static_cast<uint32_t>(DT_I64);
+            V.mul[v][f] = uf ? F.mul : 0;
+            V.add[v][f] = uf ? F.add : 1;  // an absent factor multiplies by 1
+        }
+    }
+    V.on = on ? 1u : 0u;
+}
+
+__device__ __forceinline__ int64_t fast_factor(const uint8_t* stage, uint32_t soff, uint32_t dt, int64_t mul,
+                                               int64_t add, uint32_t rl) {
+    const int64_t x = load_cell(stage + soff, dt, rl);
+    return static_cast<int64_t>(static_cast<uint64_t>(mul) * static_cast<uint64_t>(x) + static_cast<uint64_t>(add));
+}
+
+template <int NT>
+__device__ __forceinline__ void fast_row(const Plan& P, const RegVals& V, uint8_t* extra, const uint8_t* stage,
+                                         uint32_t rl, uint32_t t, uint64_t& upd, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
+    long long* w = reinterpret_cast<long long*>(extra);
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+        if (static_cast<uint32_t>(v) < V.nv) {
+            const int64_t a = fast_factor(stage, V.soff[v][0], V.dt[v][0], V.mul[v][0], V.add[v][0], rl);
+            const int64_t b = V.nf[v] > 1 ? fast_factor(stage, V.soff[v][1], V.dt[v][1], V.mul[v][1], V.add[v][1], rl)
+                                          : int64_t{1};
+            const uint64_t x = static_cast<uint64_t>(a) * static_cast<uint64_t>(b);
+            long long& s = w[(v + 1) * NT + t];
+            s = static_cast<long long>(static_cast<uint64_t>(s) + x);
+        }
+    }
+    if (++upd >= P.flush_limit) {
+        sink.flush_private_thread(P, extra, t);
+        upd = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL>
 __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
                                              const uint8_t* stage, uint64_t tile, uint32_t t,
-                                             unsigned long long& selected) {
+                                             unsigned long long& selected, const RegLeaves& RL,
+                                             const RegVals& RV) {
     constexpr int R = kTileRows / NT;
     const uint64_t r0 = tile * kTileRows;
     const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
-    const uint32_t m = eval_pred<R, TAIL>(P, stage, r0, t, nrem);
+    const uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
     const uint32_t lane = t & 31u;
     selected += __popc(m);
+    if (MODE == MODE_GROUP_PRIVATE && P.count_by_tile) {
+        // Scalar aggregate: the group's row count is the number of selected rows.
+        long long* w = reinterpret_cast<long long*>(extra);
+        if (ACC128) {
+            uint64_t* lo = reinterpret_cast<uint64_t*>(&w[t]);
+            const uint64_t nl = *lo + __popc(m);
+            w[NT + t] += (nl < *lo) ? 1 : 0;
+            *lo = nl;
+        } else {
+            w[t] += __popc(m);
+        }
+    }
 
     if (MODE == MODE_FILTER) {
         // 32 / R consecutive lanes hold the bits of one 32-row bitmap word.
@@ -698,6 +833,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     };
     // Each iteration handles the next selected row of every lane at once, so a
     // sparse selection costs max(rows per lane) iterations, not the total.
+    if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
+        if (!TAIL && RV.on) {
+            for (uint32_t sel = m; sel; sel &= sel - 1) fast_row<NT>(P, RV, extra, stage, R * t + __ffs(sel) - 1, t, sink.upd, sink);
+            return;
+        }
+    }
     for (uint32_t sel = m; sel; sel &= sel - 1) one_row(R * t + __ffs(sel) - 1);
 }
 
@@ -779,6 +920,10 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
 
     // ---------------- consumers ----------------
     const uint32_t lane = t & 31u;
+    RegLeaves RL;
+    load_reg_leaves(P, RL);
+    RegVals RV;
+    load_reg_vals<MODE, ACC128>(P, RV);
     unsigned long long selected = 0;
     bool ok = true;
     uint32_t s = 0, phase = 0;  // stage and phase of the k-th full tile
@@ -799,7 +944,7 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
             // try_wait so their shared-memory reads are ordered after the copy.
             mbar_try_wait(&full[s], phase);
             process_tile<MODE, ACC128, NT, false>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
-                                                  tl, t, selected);
+                                                  tl, t, selected, RL, RV);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
             if (++s == S) {
@@ -807,7 +952,7 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
                 phase ^= 1u;
             }
         } else {
-            process_tile<MODE, ACC128, NT, true>(P, sink, extra, nullptr, tl, t, selected);
+            process_tile<MODE, ACC128, NT, true>(P, sink, extra, nullptr, tl, t, selected, RL, RV);
         }
     }
 #pragma unroll
