@@ -426,6 +426,50 @@ TGP_API int tgp_join_probe_pairs(tgp_ctx* ctx, tgp_join_id join, tgp_table_id pr
                          uint32_t* probe_rows, uint32_t* build_rows, uint64_t cap,
                          uint64_t* npairs);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free aggregate                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Size of the library's fixed device scratch for tgp_aggregate_noalloc. */
+#define TGP_NOALLOC_SCRATCH_BYTES (256u * 1024u)
+
+/* One GROUP BY column of tgp_aggregate_noalloc and the values it may hold:
+ * every cell lies in [min, min + count). */
+typedef struct tgp_key_domain {
+    uint32_t column;
+    uint32_t _pad;
+    int64_t min;
+    uint64_t count;
+} tgp_key_domain;
+
+/* Has no counterpart in the reference: an entry point for callers that cannot
+ * allocate GPU memory — code recording a CUDA graph, running under an
+ * allocator that owns the whole device, or bound by a no-allocation-after-
+ * start-up policy. It computes the same scalar or grouped aggregate as
+ * tgp_execute over caller-owned, 16-byte-aligned DEVICE columns, without a
+ * context and without calling cudaMalloc, cudaFree or any allocating routine:
+ * its accumulators live in a fixed TGP_NOALLOC_SCRATCH_BYTES device array that
+ * every GPU loading the library keeps until the process exits.
+ *
+ *  - Groups are dense: group g enumerates the key domains with the first key
+ *    most significant; vals_out (HOST memory) receives ngroups * nagg values in
+ *    that order (ngroups = product of the domain counts), with count = 0 for
+ *    empty groups. A key cell outside its declared domain is rejected
+ *    (TGP_INVALID_ARG) before any accumulation.
+ *  - Queries whose scratch exceeds TGP_NOALLOC_SCRATCH_BYTES (many groups times
+ *    many aggregates) are rejected with TGP_CAPACITY and a message.
+ *  - The first call on a device looks up the array's device address; make it
+ *    before any stream capture. All calls share the array: calls that overlap
+ *    on the GPU race and must be serialised by the caller.
+ *  - `stream` is a cudaStream_t (NULL = the default stream); the call returns
+ *    after its work on that stream has finished. Failures carry a message in
+ *    err_msg (may be NULL). */
+TGP_API int tgp_aggregate_noalloc(int device, void* stream, const tgp_column_desc* cols, uint32_t ncols,
+                                  uint64_t rows, const tgp_pred_node* pred, uint32_t npred,
+                                  const tgp_key_domain* keys, uint32_t nkeys, const tgp_agg* aggs, uint32_t nagg,
+                                  tgp_agg_value* vals_out, uint64_t vals_cap, tgp_query_result* result,
+                                  char* err_msg, size_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif

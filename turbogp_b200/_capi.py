@@ -88,6 +88,10 @@ class KernelParams(C.Structure):
     ]
 
 
+class KeyDomain(C.Structure):
+    _fields_ = [("column", C.c_uint32), ("_pad", C.c_uint32), ("min", C.c_int64), ("count", C.c_uint64)]
+
+
 class KernelResultC(C.Structure):
     _fields_ = [("count", C.c_uint64), ("sum", C.c_double), ("mask", C.c_uint64)]
 
@@ -133,7 +137,13 @@ PROTOTYPES = [
     ("tgp_join_probe_pairs", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.c_void_p, C.c_void_p,
       C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("tgp_aggregate_noalloc", C.c_int,
+     [C.c_int, C.c_void_p, C.POINTER(ColumnDesc), C.c_uint32, C.c_uint64, C.POINTER(PredNode), C.c_uint32,
+      C.POINTER(KeyDomain), C.c_uint32, C.POINTER(Agg), C.c_uint32, C.POINTER(AggValue), C.c_uint64,
+      C.POINTER(QueryResult), C.c_char_p, C.c_size_t]),
 ]
+
+NOALLOC_SCRATCH_BYTES = 256 * 1024
 
 _lib: C.CDLL | None = None
 

@@ -136,6 +136,13 @@ int check_kernel_err(tgp_ctx* ctx, uint32_t err) {
     return TGP_OK;
 }
 
+}  // namespace
+
+// The predicate lowering below is shared with the allocation-free entry point
+// (noalloc.cu), so it lives in namespace tgp rather than in this file's
+// anonymous namespace.
+namespace tgp {
+
 // --------------------------------------------------------------------------
 // Predicate lowering
 // --------------------------------------------------------------------------
@@ -258,6 +265,10 @@ int lower_leaf(tgp_ctx* ctx, const Column& c, const tgp_pred_node& n, uint8_t sl
     lf.span32 = hi32 - lo32;
     return TGP_OK;
 }
+
+}  // namespace tgp
+
+namespace {
 
 // --------------------------------------------------------------------------
 // Query builder

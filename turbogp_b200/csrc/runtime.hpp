@@ -14,6 +14,8 @@
 #include "plan.hpp"
 #include "turbogp_gpu.h"
 
+struct tgp_ctx;
+
 namespace tgp {
 
 // Launchers implemented in the .cu files.
@@ -40,6 +42,11 @@ cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long lon
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
                                  int sms, cudaStream_t st);
+
+struct Column;
+// Lowers one predicate leaf over column `c` staged in `slot` (capi.cu).
+// `ctx` may be null (no error message is recorded then).
+int lower_leaf(tgp_ctx* ctx, const Column& c, const tgp_pred_node& n, uint8_t slot, Leaf& lf);
 
 struct Column {
     uint32_t dtype = 0;
