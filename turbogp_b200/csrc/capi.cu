@@ -1142,23 +1142,24 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     const uint64_t acc_words = (mode == MODE_GROUP_HASH) ? 0 : ngroups_direct * nv1 * 2;
     const uint64_t htab_words = hcap * P.hstride;
     Carve cv;
-    TGP_TRY(arena_reserve(ctx, acc_words * 8 + htab_words * 8 + 256, &cv));
-    P.acc = cv.take<unsigned long long>(std::max<uint64_t>(acc_words, 2));
+    TGP_TRY(arena_reserve(ctx, acc_words * 8 + htab_words * 8 + 1024, &cv));
+    // One result block [counters: 4 words][error word: 2 words][accumulators],
+    // cleared with one memset and read back with one copy.
+    const uint64_t block_words = 6 + acc_words;
+    unsigned long long* block = cv.take<unsigned long long>(block_words);
+    P.counters = block;
+    P.err = reinterpret_cast<uint32_t*>(block + 4);
+    P.acc = acc_words ? block + 6 : cv.take<unsigned long long>(2);
     P.htab = mode == MODE_GROUP_HASH ? cv.take<unsigned long long>(htab_words) : nullptr;
-    P.counters = cv.take<unsigned long long>(4);
-    P.err = cv.take<uint32_t>(4);
-    TGP_CUDA(cudaMemsetAsync(P.counters, 0, 32, ctx->stream));
-    TGP_CUDA(cudaMemsetAsync(P.err, 0, 16, ctx->stream));
-    if (acc_words) {
+    bool has_minmax = false;
+    for (uint32_t v = 0; v < P.nval; ++v) has_minmax |= (P.val[v].kind == VK_MIN || P.val[v].kind == VK_MAX);
+    if (acc_words && has_minmax) {
+        TGP_CUDA(cudaMemsetAsync(block, 0, 48, ctx->stream));
         std::vector<unsigned long long> img;
         init_acc_image(P, ngroups_direct, &img);
-        bool has_minmax = false;
-        for (uint32_t v = 0; v < P.nval; ++v) has_minmax |= (P.val[v].kind == VK_MIN || P.val[v].kind == VK_MAX);
-        if (has_minmax) {
-            TGP_TRY(upload(ctx, P.acc, img.data(), img.size() * 8));
-        } else {
-            TGP_CUDA(cudaMemsetAsync(P.acc, 0, acc_words * 8, ctx->stream));
-        }
+        TGP_TRY(upload(ctx, P.acc, img.data(), img.size() * 8));
+    } else {
+        TGP_CUDA(cudaMemsetAsync(block, 0, block_words * 8, ctx->stream));
     }
     if (mode == MODE_GROUP_HASH) {
         // Keys EMPTY, counters 0, value limbs: MIN/MAX identity or 0.
@@ -1184,13 +1185,13 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     TGP_TRY(size_smem(ctx, P, extra));
     TGP_TRY(launch(ctx, P, mode, acc128));
 
-    unsigned long long counters[4] = {0, 0, 0, 0};
-    uint32_t err = 0;
-    TGP_CUDA(cudaMemcpyAsync(counters, P.counters, 32, cudaMemcpyDeviceToHost, ctx->stream));
-    TGP_CUDA(cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<unsigned long long> accv(acc_words);
-    if (acc_words) TGP_CUDA(cudaMemcpyAsync(accv.data(), P.acc, acc_words * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_TRY(pinned_reserve(ctx, block_words * 8));
+    TGP_CUDA(cudaMemcpyAsync(ctx->hpin, block, block_words * 8, cudaMemcpyDeviceToHost, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    const unsigned long long* hb = reinterpret_cast<const unsigned long long*>(ctx->hpin);
+    unsigned long long counters[4] = {hb[0], hb[1], hb[2], hb[3]};
+    const uint32_t err = static_cast<uint32_t>(hb[4] & 0xffffffffull);
+    std::vector<unsigned long long> accv(hb + 6, hb + 6 + acc_words);
     TGP_TRY(check_kernel_err(ctx, err));
 
     result->rows_scanned = T->rows;

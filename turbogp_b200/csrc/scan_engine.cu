@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "device_common.cuh"
 #include "plan.hpp"
@@ -993,11 +994,51 @@ static const void* select_kernel(uint32_t mode, bool acc128, int nt) {
 }
 
 // Launches with blockDim = nthreads consumers + one producer warp.
+// Per (device, kernel): the dynamic shared-memory limit already raised, and
+// occupancies already queried, so a launch costs one cudaLaunchKernel.
+struct KernelCacheEntry {
+    int device;
+    const void* f;
+    int smem_limit;
+    size_t occ_smem[4];
+    int occ[4];
+    int nocc;
+};
+
+static std::mutex g_kcache_mu;
+static KernelCacheEntry g_kcache[128];
+static int g_kcache_n = 0;
+
+static KernelCacheEntry* kernel_entry(const void* f) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    for (int i = 0; i < g_kcache_n; ++i)
+        if (g_kcache[i].f == f && g_kcache[i].device == dev) return &g_kcache[i];
+    if (g_kcache_n == static_cast<int>(sizeof(g_kcache) / sizeof(g_kcache[0]))) return nullptr;
+    KernelCacheEntry& e = g_kcache[g_kcache_n++];
+    e.device = dev;
+    e.f = f;
+    e.smem_limit = 0;
+    e.nocc = 0;
+    return &e;
+}
+
+static cudaError_t ensure_smem_limit(KernelCacheEntry* e, const void* f, int smem) {
+    if (e && e->smem_limit >= smem) return cudaSuccess;
+    const cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (r == cudaSuccess && e) e->smem_limit = smem;
+    return r;
+}
+
+// Launches with blockDim = nthreads consumers + one producer warp.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st) {
     const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads));
     if (!f) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P.smem_bytes));
-    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(g_kcache_mu);
+        const cudaError_t e = ensure_smem_limit(kernel_entry(f), f, static_cast<int>(P.smem_bytes));
+        if (e != cudaSuccess) return e;
+    }
     void* args[] = {const_cast<Plan*>(&P)};
     return cudaLaunchKernel(f, dim3(grid), dim3(P.nthreads + 32), args, P.smem_bytes, st);
 }
@@ -1005,15 +1046,24 @@ cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cud
 int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem) {
     const void* f = select_kernel(mode, acc128, nt);
     if (!f) return 0;
-    int n = 0;
-    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn_smem)) !=
-        cudaSuccess) {
+    std::lock_guard<std::mutex> lock(g_kcache_mu);
+    KernelCacheEntry* e = kernel_entry(f);
+    if (e)
+        for (int i = 0; i < e->nocc; ++i)
+            if (e->occ_smem[i] == dyn_smem) return e->occ[i];
+    if (ensure_smem_limit(e, f, static_cast<int>(dyn_smem)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
+    int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, nt + 32, dyn_smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
+    }
+    if (e) {
+        const int slot = e->nocc < 4 ? e->nocc++ : 0;
+        e->occ_smem[slot] = dyn_smem;
+        e->occ[slot] = n;
     }
     return n;
 }

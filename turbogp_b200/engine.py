@@ -470,28 +470,16 @@ class Table(Schema):
         c = int(cnt.value)
         return FilterOutput(c, bm, rid[:c].copy() if rid is not None else None)
 
+    def prepare(self, aggs: Sequence[Agg], group_by: Sequence[Col | str] = (), where: Pred | None = None,
+                join: "JoinTable | None" = None, probe_key: str | None = None,
+                group_cap: int = 1024) -> "PreparedQuery":
+        """Lowers a query once; ``run()`` executes it with no per-call lowering."""
+        return PreparedQuery(self, aggs, group_by, where, join, probe_key, group_cap)
+
     def aggregate(self, aggs: Sequence[Agg], group_by: Sequence[Col | str] = (), where: Pred | None = None,
                   join: "JoinTable | None" = None, probe_key: str | None = None,
                   group_cap: int | None = None) -> QueryOutput:
-        build = join.build if join is not None else None
-        q, keep = self.lower_query(aggs, group_by, where, build, probe_key)
-        q.table = self.id
-        if join is not None:
-            q.join = join.id
-        cap = group_cap if group_cap is not None else 1024
-        nk, na = len(group_by), len(aggs)
-        while True:
-            keys = np.zeros(max(1, cap * max(1, nk)), dtype=np.uint64)
-            vals = (A.AggValue * max(1, cap * max(1, na)))()
-            res = A.QueryResult()
-            st = self.ctx.lib.tgp_execute(self.ctx.h, C.byref(q), keys.ctypes.data, vals, cap, C.byref(res))
-            if st == A.CAPACITY and res.ngroups > cap:
-                cap = int(res.ngroups)
-                continue
-            self.ctx._check(st, "tgp_execute")
-            break
-        ks, vs = decode_groups(keys, vals, int(res.ngroups), nk, na)
-        return QueryOutput(ks, vs, int(res.rows_scanned), int(res.rows_selected), int(res.flags))
+        return self.prepare(aggs, group_by, where, join, probe_key, group_cap or 1024).run()
 
     def join_build(self, key: str, where: Pred | None = None) -> "JoinTable":
         nodes, n = self.lower_pred(where)
@@ -499,6 +487,40 @@ class Table(Schema):
         self.ctx._check(self.ctx.lib.tgp_join_build(self.ctx.h, self.id, self.index(key), nodes, n, C.byref(jid)),
                         "tgp_join_build")
         return JoinTable(self.ctx, int(jid.value), self)
+
+
+class PreparedQuery:
+    """A lowered tgp_query with its output buffers (tgp_execute per ``run``)."""
+
+    def __init__(self, table: Table, aggs, group_by, where, join, probe_key, group_cap: int):
+        build = join.build if join is not None else None
+        self.table = table
+        self.q, self._keep = table.lower_query(aggs, group_by, where, build, probe_key)
+        self.q.table = table.id
+        if join is not None:
+            self.q.join = join.id
+        self.nk, self.na = len(group_by), len(aggs)
+        self._alloc(group_cap)
+        self.res = A.QueryResult()
+        self._fn = table.ctx.lib.tgp_execute
+
+    def _alloc(self, cap: int) -> None:
+        self.cap = cap
+        self.keys = np.zeros(max(1, cap * max(1, self.nk)), dtype=np.uint64)
+        self.vals = (A.AggValue * max(1, cap * max(1, self.na)))()
+
+    def run(self) -> QueryOutput:
+        ctx = self.table.ctx
+        while True:
+            st = self._fn(ctx.h, C.byref(self.q), self.keys.ctypes.data, self.vals, self.cap, C.byref(self.res))
+            if st == A.CAPACITY and self.res.ngroups > self.cap:
+                self._alloc(int(self.res.ngroups))
+                continue
+            ctx._check(st, "tgp_execute")
+            break
+        r = self.res
+        ks, vs = decode_groups(self.keys, self.vals, int(r.ngroups), self.nk, self.na)
+        return QueryOutput(ks, vs, int(r.rows_scanned), int(r.rows_selected), int(r.flags))
 
 
 class JoinTable:
