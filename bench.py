@@ -181,6 +181,164 @@ def run_reference(args, world: int, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_workload(args, world: int, rank: int, local: int) -> None:
+    """The other hot-path workloads, one JSON line each (same keys as the default line).
+
+    filtered_group_agg: 6M rows, WHERE ship_day <= max - 90, GROUP BY (flag_a, flag_b),
+      count + 4 int128 sums + avg (26 B/row).
+    join_group_agg: dimension 1.5M rows filtered on order_day, fact 60M rows with a
+      Zipf(0.8) foreign key; each step builds the join table and runs the fused
+      probe + GROUP BY segment aggregate (build 9 B/row, probe 16 B/row).
+    highcard_group: 100M rows, GROUP BY key (Zipf(1.1) over 10M values), count +
+      sum(value) through the global group hash table (12 B/row).
+    Under torchrun every rank runs an independent replica on its own data.
+    """
+    import torch
+    import oracle
+    from turbogp_b200 import datagen, workloads
+    from turbogp_b200.engine import Context, col, count_star, sum_
+
+    name = args.workload
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    CT = datagen.LINEITEM_COLTYPES
+    probe_only = None  # (callable, algorithmic bytes per launch) when the step has several kernels
+    if name == "filtered_group_agg":
+        n = args.rows if args.rows != ROWS else 6_000_000
+        tpl = workloads.filtered_group_agg()
+        host = datagen.lineitem(n, seed=1 + rank)
+        t = ctx.register(host, CT)
+        q = t.prepare(tpl.aggs, tpl.group_by, tpl.where)
+        step = q.run
+        tables = [(t, host)]
+        rows_step, bytes_step, kernel_bytes = n, 26 * n, 26 * n
+        dominant = "scan_kernel<MODE_GROUP_PRIVATE> (6 direct groups, 4 int128 values)"
+        desc = f"filtered_group_agg ({n} rows, WHERE ship_day <= max-90, GROUP BY flag_a, flag_b, 6 aggregates)"
+        cpu_sample = {k: v[:2_000_000] for k, v in host.items()}
+        cpu_run = lambda: oracle.aggregate(cpu_sample, CT, tpl.aggs, tpl.group_by, tpl.where)
+        cpu_rows = min(n, 2_000_000)
+    elif name == "join_group_agg":
+        n = args.rows if args.rows != ROWS else 60_000_000
+        nb = 1_500_000
+        tpl = workloads.join_group_agg()
+        dim = datagen.dimension(nb, seed=2 + rank)
+        fact_full = datagen.fact_fk(n, nb, 0.8, seed=3 + rank)
+        fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
+        del fact_full
+        fct = {"fk": "int", "price_cents": "int", "discount_pct": "int"}
+        d = ctx.register(dim, datagen.DIMENSION_COLTYPES)
+        f = ctx.register(fact, fct)
+
+        def step():
+            j = d.join_build("key", tpl.build_where)
+            out = f.aggregate(tpl.aggs, tpl.group_by, tpl.where, join=j, probe_key="fk")
+            j.drop()
+            return out
+
+        j0 = d.join_build("key", tpl.build_where)
+        pq = f.prepare(tpl.aggs, tpl.group_by, tpl.where, join=j0, probe_key="fk")
+        probe_only = (pq.run, 16 * n)
+        tables = [(d, dim), (f, fact)]
+        rows_step, bytes_step, kernel_bytes = n + nb, 16 * n + 9 * nb, 16 * n
+        dominant = "scan_kernel probe + join + GROUP BY segment (25 groups, int128)"
+        desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
+                f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
+        cs = min(n, 2_000_000)
+        cpu_fact = {k: v[:cs] for k, v in fact.items()}
+        cpu_run = lambda: oracle.aggregate(cpu_fact, fct, tpl.aggs, tpl.group_by, tpl.where,
+                                           build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
+                                           probe_key="fk")
+        cpu_rows = cs
+    else:  # highcard_group
+        n = args.rows if args.rows != ROWS else 100_000_000
+        host = datagen.highcard(n, 10_000_000, 1.1, seed=4 + rank)
+        t = ctx.register(host)
+        aggs = [count_star(), sum_(col("value"))]
+        q = t.prepare(aggs, ("key",), None, group_cap=10_000_000)
+        step = lambda: q.run(decode=False)
+        tables = [(t, host)]
+        rows_step, bytes_step, kernel_bytes = n, 12 * n, 12 * n
+        dominant = "scan_kernel<MODE_GROUP_HASH> (global open-addressing group table)"
+        desc = f"highcard_group ({n} rows, GROUP BY key Zipf(1.1) over 10M values, count + sum(value))"
+        cs = min(n, 2_000_000)
+        cpu_sample = {k: v[:cs] for k, v in host.items()}
+        cpu_run = lambda: oracle.aggregate(cpu_sample, None, aggs, ("key",))
+        cpu_rows = cs
+
+    for _ in range(args.warmup):
+        step()
+    steps = args.steps if args.steps != 3000 else 20
+    ctx.profile(True)
+    ctx.profile_read()
+    torch.cuda.synchronize()
+    ctx.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+    launches, kernel_total = ctx.profile_read()
+    ms = ev0.elapsed_time(ev1)
+    if probe_only is not None:
+        run_probe, kernel_bytes = probe_only
+        for _ in range(3):
+            run_probe()
+        ctx.profile_read()
+        for _ in range(steps):
+            run_probe()
+        pl, pms = ctx.profile_read()
+        kernel_avg = pms / max(1, pl)
+    else:
+        kernel_avg = kernel_total / max(1, launches)
+    ctx.profile(False)
+
+    # e2e: pinned host buffers re-uploaded every step, result read back.
+    pinned = [(tb, {k: torch.from_numpy(v).pin_memory().numpy() for k, v in h.items()}) for tb, h in tables]
+    h2d = sum(a.nbytes for _, h in pinned for a in h.values())
+    e2e_steps = max(1, min(args.e2e_steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for tb, h in pinned:
+            tb.reload(h)
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        cpu_run()
+        sec = time.perf_counter() - t0
+        cpu = {"value": cpu_rows / sec, "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"first {cpu_rows} rows of the same data through the exact C++ oracle "
+                         f"(row-at-a-time restatement of the reference semantics), one pass"}
+    peak, peak_kind = peak_hbm()
+    achieved = kernel_bytes / (kernel_avg / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": rows_step * world * steps / (ms / 1000.0), "unit": "rows/s", "n_gpus": world,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H shapes)",
+        "config": {"workload": desc, "rows_per_step": rows_step, "bytes_per_step": bytes_step,
+                   "l2": "inputs larger than the 126 MB L2" if bytes_step > 126e6 else "inputs smaller than L2"},
+        "hbm_gbs": bytes_step * world * steps / (ms / 1000.0) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "kernel_ms": kernel_avg, "kernel": dominant},
+        "e2e": {"value": rows_step * e2e_steps / (e2e_ms / 1000.0), "unit": "rows/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": None},
+        "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,10 +350,15 @@ def main() -> None:
     ap.add_argument("--reference-rows", type=int, default=ROWS)
     ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="selective_scan_sum",
+                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     world, rank, local = dist_setup(args.gpus)
+    if args.workload != "selective_scan_sum":
+        run_workload(args, world, rank, local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:

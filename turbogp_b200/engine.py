@@ -509,7 +509,9 @@ class PreparedQuery:
         self.keys = np.zeros(max(1, cap * max(1, self.nk)), dtype=np.uint64)
         self.vals = (A.AggValue * max(1, cap * max(1, self.na)))()
 
-    def run(self) -> QueryOutput:
+    def run(self, decode: bool = True) -> QueryOutput:
+        """Executes the query; with decode=False only the counts are returned
+        (the raw results stay in ``keys`` / ``vals``)."""
         ctx = self.table.ctx
         while True:
             st = self._fn(ctx.h, C.byref(self.q), self.keys.ctypes.data, self.vals, self.cap, C.byref(self.res))
@@ -519,6 +521,8 @@ class PreparedQuery:
             ctx._check(st, "tgp_execute")
             break
         r = self.res
+        if not decode:
+            return QueryOutput([], [], int(r.rows_scanned), int(r.rows_selected), int(r.flags))
         ks, vs = decode_groups(self.keys, self.vals, int(r.ngroups), self.nk, self.na)
         return QueryOutput(ks, vs, int(r.rows_scanned), int(r.rows_selected), int(r.flags))
 
