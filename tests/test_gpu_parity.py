@@ -180,3 +180,50 @@ def test_full_size_selective_scan(ctx):
     # Size-independent property: the filter's count equals the aggregate's count.
     assert t.filter(tpl.where, bitmap=False, rowids=False).count == g.values[0][1].value
     t.drop()
+
+
+def test_dense_value_programs(ctx):
+    """Grouped aggregates whose value lists share factor prefixes, constants,
+    MIN / MAX / COUNT(col), 0-2 group keys, at selectivities that mix dense and
+    sparse warps, with tails, against the oracle."""
+    from turbogp_b200.engine import lit
+    p, d, t, q = col("price_cents"), col("discount_pct"), col("tax_pct"), col("quantity")
+    programs = [
+        [count_star(), sum_(q), sum_(p), sum_(p * (100 - d)), sum_(p * (100 - d) * (100 + t)), avg(q)],
+        [sum_(p * d), sum_(p * d * 3), min_(p * d), max_(q - 60), count_col(d - 5)],
+        [sum_(lit(7)), sum_(q * (-3)), sum_(-q + 11), sum_(q * q * q), max_(d), sum_(p)],
+        [min_(q), max_(q), sum_(q), count_star()],
+        [sum_(p * t * d * q)],
+    ]
+    keys = [(), ("flag_a",), ("flag_a", "flag_b"), ("tax_pct", "flag_b"), ("discount_pct",)]
+    wheres = [None, col("ship_day") <= datagen.DAY0 + 1500, col("quantity") <= 15, col("discount_pct") == 3]
+    for n in [2048 * 37 + 5, 250_000]:
+        t_host = datagen.lineitem(n, seed=31 + n)
+        t_host["price_cents"][::7] *= -1          # negative values and products
+        tb = ctx.register(t_host, CT)
+        for aggs in programs:
+            for gb in keys:
+                for w in wheres:
+                    g = tb.aggregate(aggs, gb, w)
+                    o = oracle.aggregate(t_host, CT, aggs, gb, w)
+                    same_query(g, o)
+        tb.drop()
+
+
+def test_dense_flushes_near_int64_bound(ctx):
+    """Per-row values near 2^60 force the int64 partials to flush every few
+    rows; sums stay exact in int128."""
+    n = 400_003
+    rng = np.random.default_rng(5)
+    cols = {"v": rng.integers(2**59, 2**60, n, dtype=np.int64),
+            "w": rng.integers(-2**60, -2**59, n, dtype=np.int64),
+            "g": rng.integers(0, 5, n, dtype=np.uint8),
+            "s": rng.integers(0, 100, n, dtype=np.int32)}
+    tb = ctx.register(cols)
+    aggs = [count_star(), sum_(col("v")), sum_(col("w")), max_(col("v"))]
+    for gb in [(), ("g",)]:
+        for w in [None, col("s") < 70]:
+            g = tb.aggregate(aggs, gb, w)
+            o = oracle.aggregate(cols, None, aggs, gb, w)
+            same_query(g, o)
+    tb.drop()

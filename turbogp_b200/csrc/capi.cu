@@ -502,6 +502,81 @@ struct Builder {
     }
 };
 
+// Lowers the values of a MODE_GROUP_PRIVATE int64 plan into the dense step
+// program (ChainProg). A value whose factor list extends the previous value's
+// continues its running product; any other value starts a new one. Returns
+// false (dense path off) when a factor or key is not staged, more than two
+// keys group, or the program needs more than kMaxSteps steps.
+bool compile_chain(Builder& b) {
+    Plan& P = b.P;
+    if (P.ngkey > 2) return false;
+    for (uint32_t k = 0; k < P.ngkey; ++k)
+        if (P.gkey[k].slot < 0 || P.gkey[k].build_side) return false;
+    std::vector<int> slot2col(P.nslots, -1);
+    for (size_t c = 0; c < b.col2slot.size(); ++c)
+        if (b.col2slot[c] >= 0) slot2col[b.col2slot[c]] = static_cast<int>(c);
+    ChainProg C;
+    std::memset(&C, 0, sizeof(C));
+    const ValDesc* prev = nullptr;
+    for (uint32_t v = 0; v < P.nval; ++v) {
+        const ValDesc& V = P.val[v];
+        for (uint32_t f = 0; f < V.nf; ++f)
+            if (V.f[f].build_side || (V.f[f].slot < 0 && V.f[f].bptr != nullptr)) return false;
+        // Shared prefix with the previous value's whole factor list.
+        uint32_t start = 0;
+        if (prev && prev->nf >= 1 && prev->nf <= V.nf &&
+            std::memcmp(prev->f, V.f, sizeof(Factor) * prev->nf) == 0)
+            start = prev->nf;
+        if (V.nf == 0) {
+            // A value of no factors is the constant 1.
+            if (C.nsteps >= static_cast<uint32_t>(kMaxSteps)) return false;
+            ChainStep& S = C.s[C.nsteps++];
+            S.add = 1;
+            S.add32 = 1;
+        }
+        for (uint32_t f = start; f < V.nf; ++f) {
+            if (C.nsteps >= static_cast<uint32_t>(kMaxSteps)) return false;
+            const Factor& F = V.f[f];
+            ChainStep& S = C.s[C.nsteps++];
+            S.mul = F.mul;
+            S.add = F.add;
+            S.flags = f > 0 ? CS_CHAIN : 0;
+            if (F.slot >= 0) {
+                S.flags |= CS_COL;
+                S.soff = F.soff;
+                S.dtype = F.dtype;
+                const Column& c = b.T->cols[slot2col[F.slot]];
+                const __int128 x0 = static_cast<__int128>(F.mul) * c.min + F.add;
+                const __int128 x1 = static_cast<__int128>(F.mul) * c.max + F.add;
+                const __int128 lim = static_cast<__int128>(1) << 31;
+                const bool small = F.mul >= INT32_MIN && F.mul <= INT32_MAX && F.add >= INT32_MIN && F.add <= INT32_MAX;
+                if (F.dtype != DT_F64 && small && std::min(x0, x1) >= -lim && std::max(x0, x1) < lim &&
+                    (F.dtype == DT_U8 || F.dtype == DT_I32)) {
+                    S.flags |= CS_NARROW;
+                    S.mul32 = static_cast<int32_t>(F.mul);
+                    S.add32 = static_cast<int32_t>(F.add);
+                } else if (F.mul == 1 && F.add == 0) {
+                    S.flags |= CS_IDENT;
+                }
+            }
+        }
+        if (C.nsteps == 0 || (start == V.nf && V.nf > 0 && C.s[C.nsteps - 1].acc != 0)) {
+            // Same factor list as the previous value (a different kind): one
+            // step that re-multiplies by 1 and accumulates.
+            if (C.nsteps >= static_cast<uint32_t>(kMaxSteps)) return false;
+            ChainStep& S = C.s[C.nsteps++];
+            S.flags = CS_CHAIN;
+            S.add = 1;
+            S.add32 = 1;
+        }
+        C.s[C.nsteps - 1].acc = static_cast<uint8_t>(v + 1);
+        C.s[C.nsteps - 1].kind = V.kind;
+        prev = &V;
+    }
+    P.chain = C;
+    return true;
+}
+
 // Per-aggregate mapping to accumulator slots.
 struct AggMap {
     uint32_t func;
@@ -696,6 +771,7 @@ int tgp_init(tgp_ctx** out, int device) {
         return TGP_DEVICE_ERROR;
     }
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_SCAN_THREADS")) ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
     if (const char* e = std::getenv("TGP_MAX_STAGES"))
         ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
@@ -1106,6 +1182,10 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
                 const uint64_t lim = b.max_abs_val ? (0x7fffffffffffffffull / b.max_abs_val) : ~0ull;
                 P.flush_limit = std::max<uint64_t>(1, lim);
             }
+            // Dense column program: int64 partials, no join, no per-row
+            // overflow checks.
+            if (!acc128 && !J && !P.check_ovf && ctx->dense_path)
+                P.dense_vec = compile_chain(b) ? 1u : 0u;
         } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;

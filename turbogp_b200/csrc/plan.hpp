@@ -103,6 +103,32 @@ struct ValDesc {
     Factor f[kMaxFactors];
 };
 
+// One step of a dense value program (MODE_GROUP_PRIVATE, int64 partials).
+// Values that extend the previous value's factor list share its running
+// product: sum(p), sum(p * (100 - d)), sum(p * (100 - d) * (100 + t)) run as
+// three steps, not six factor evaluations.
+constexpr int kMaxSteps = 8;
+enum : uint8_t {
+    CS_COL = 1,     // factor reads a staged column (else the constant `add`)
+    CS_CHAIN = 2,   // multiply into the running product (else start a new one)
+    CS_NARROW = 4,  // mul * x + add fits int32 for every cell: 32-bit arithmetic
+    CS_IDENT = 8    // mul == 1 and add == 0: the factor is the cell itself
+};
+struct ChainStep {
+    uint32_t soff;   // staged column offset inside a stage
+    uint8_t dtype;   // staged column dtype
+    uint8_t flags;   // CS_*
+    uint8_t acc;     // value slot (1..nval) the running product goes to; 0 = none
+    uint8_t kind;    // VK_* of that value
+    int32_t mul32, add32;
+    int64_t mul, add;
+};
+struct ChainProg {
+    uint32_t nsteps;
+    uint32_t _pad;
+    ChainStep s[kMaxSteps];
+};
+
 struct GKey {
     int8_t slot;          // staged slot (probe/own side)
     uint8_t build_side;   // 1: key column lives on the build side
@@ -140,9 +166,11 @@ struct Plan {
     uint32_t nval;
     uint32_t check_ovf;     // per-row overflow detection needed
     uint32_t count_by_tile; // MODE_GROUP_PRIVATE, one group, no join: row count = popcount per tile
-    uint32_t _p3;
+    uint32_t dense_vec;     // MODE_GROUP_PRIVATE int64: `chain` holds the dense value program
     uint64_t flush_limit;   // MODE_GROUP_PRIVATE int64: per-thread updates between flushes
     ValDesc val[kMaxVals];
+
+    ChainProg chain;
 
     // Group keys
     uint32_t ngkey;

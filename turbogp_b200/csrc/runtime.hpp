@@ -109,8 +109,9 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
+    bool dense_path = true;  // dense column programs for MODE_GROUP_PRIVATE (TGP_NO_DENSE=1 turns them off)
 };

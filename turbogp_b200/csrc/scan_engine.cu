@@ -742,6 +742,189 @@ __device__ __forceinline__ void fast_row(const Plan& P, const RegVals& V, uint8_
 }
 
 // ---------------------------------------------------------------------------
+// Dense tiles of MODE_GROUP_PRIVATE with int64 partials (no join, staged keys
+// and factors): the thread's R rows are processed column by column in
+// straight-line code. Unselected rows add 0 (MIN / MAX skip them), so the
+// per-row loop has no data-dependent branch; every step of the host's value
+// program (ChainProg) is uniform across the CTA.
+// ---------------------------------------------------------------------------
+// The R cells of thread t (rows R*t .. R*t+R-1) as 64-bit integers.
+template <int R>
+__device__ __forceinline__ void load_cells64(const uint8_t* base, uint32_t dtype, uint32_t t, int64_t (&x)[R]) {
+    if (dtype == DT_U8) {
+        if constexpr (R == 4) {
+            const uint32_t w = reinterpret_cast<const uint32_t*>(base)[t];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x[e] = (w >> (8 * e)) & 0xffu;
+        } else {
+            const uint2 w = reinterpret_cast<const uint2*>(base)[t];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                x[e] = (w.x >> (8 * e)) & 0xffu;
+                x[e + 4] = (w.y >> (8 * e)) & 0xffu;
+            }
+        }
+    } else if (dtype == DT_I32) {
+        const uint4* p = reinterpret_cast<const uint4*>(base) + (R / 4) * t;
+#pragma unroll
+        for (int c = 0; c < R / 4; ++c) {
+            const uint4 v = p[c];
+            x[4 * c + 0] = static_cast<int32_t>(v.x);
+            x[4 * c + 1] = static_cast<int32_t>(v.y);
+            x[4 * c + 2] = static_cast<int32_t>(v.z);
+            x[4 * c + 3] = static_cast<int32_t>(v.w);
+        }
+    } else {
+        const uint4* p = reinterpret_cast<const uint4*>(base) + (R / 2) * t;
+#pragma unroll
+        for (int c = 0; c < R / 2; ++c) {
+            const uint4 v = p[c];
+            x[2 * c + 0] = static_cast<int64_t>((static_cast<uint64_t>(v.y) << 32) | v.x);
+            x[2 * c + 1] = static_cast<int64_t>((static_cast<uint64_t>(v.w) << 32) | v.z);
+        }
+    }
+}
+
+// The low 32 bits of the same cells (u8 zero-extended, i32 as stored).
+template <int R>
+__device__ __forceinline__ void load_cells32(const uint8_t* base, uint32_t dtype, uint32_t t, uint32_t (&x)[R]) {
+    if (dtype == DT_U8) {
+        if constexpr (R == 4) {
+            const uint32_t w = reinterpret_cast<const uint32_t*>(base)[t];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x[e] = (w >> (8 * e)) & 0xffu;
+        } else {
+            const uint2 w = reinterpret_cast<const uint2*>(base)[t];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                x[e] = (w.x >> (8 * e)) & 0xffu;
+                x[e + 4] = (w.y >> (8 * e)) & 0xffu;
+            }
+        }
+    } else if (dtype == DT_I32) {
+        const uint4* p = reinterpret_cast<const uint4*>(base) + (R / 4) * t;
+#pragma unroll
+        for (int c = 0; c < R / 4; ++c) {
+            const uint4 v = p[c];
+            x[4 * c + 0] = v.x;
+            x[4 * c + 1] = v.y;
+            x[4 * c + 2] = v.z;
+            x[4 * c + 3] = v.w;
+        }
+    } else {
+        const uint4* p = reinterpret_cast<const uint4*>(base) + (R / 2) * t;
+#pragma unroll
+        for (int c = 0; c < R / 2; ++c) {
+            const uint4 v = p[c];
+            x[2 * c + 0] = v.x;
+            x[2 * c + 1] = v.z;
+        }
+    }
+}
+
+template <int NT>
+__device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                                   uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
+    constexpr int R = kTileRows / NT;
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(extra);
+    // The int64 partials stay below 2^63 in magnitude: flush before this
+    // tile's updates could pass the host's bound.
+    const uint32_t nsel = __popc(m);
+    if (sink.upd + nsel > P.flush_limit) {
+        sink.flush_private_thread(P, extra, t);
+        sink.upd = 0;
+    }
+    sink.upd += nsel;
+
+    // Direct group index of each row: sum over keys of (cell - min) * stride,
+    // exact in 32 bits because the group count is below 2^31.
+    uint32_t g[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (static_cast<uint32_t>(k) < P.ngkey) {
+            const GKey& K = P.gkey[k];
+            uint32_t x[R];
+            load_cells32<R>(stage + K.soff, K.dtype, t, x);
+            const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
+#pragma unroll
+            for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
+        }
+    }
+    const uint32_t gstride = (P.nval + 1) * static_cast<uint32_t>(NT);
+    uint32_t base[R];  // word of row r's group count; value v is at base + v * NT
+#pragma unroll
+    for (int r = 0; r < R; ++r) base[r] = g[r] * gstride + t;
+    if (!P.count_by_tile) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) atomicAdd(&w[base[r]], static_cast<unsigned long long>((m >> r) & 1u));
+    }
+
+    int64_t cur[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) cur[r] = 0;
+#pragma unroll
+    for (int s = 0; s < kMaxSteps; ++s) {
+        if (static_cast<uint32_t>(s) >= P.chain.nsteps) break;
+        const ChainStep& S = P.chain.s[s];
+        int64_t f[R];
+        if (S.flags & CS_COL) {
+            if (S.flags & CS_NARROW) {
+                uint32_t x[R];
+                load_cells32<R>(stage + S.soff, S.dtype, t, x);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    f[r] = static_cast<int32_t>(static_cast<uint32_t>(S.mul32) * x[r] + static_cast<uint32_t>(S.add32));
+            } else {
+                int64_t x[R];
+                load_cells64<R>(stage + S.soff, S.dtype, t, x);
+                if (S.flags & CS_IDENT) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) f[r] = x[r];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        f[r] = static_cast<int64_t>(static_cast<uint64_t>(S.mul) * static_cast<uint64_t>(x[r]) +
+                                                    static_cast<uint64_t>(S.add));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) f[r] = S.add;
+        }
+        if (S.flags & CS_CHAIN) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                cur[r] = static_cast<int64_t>(static_cast<uint64_t>(cur[r]) * static_cast<uint64_t>(f[r]));
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) cur[r] = f[r];
+        }
+        if (S.acc) {
+            const uint32_t off = S.acc * static_cast<uint32_t>(NT);
+            if (S.kind == VK_SUM) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    atomicAdd(&w[base[r] + off], ((m >> r) & 1u) ? static_cast<unsigned long long>(cur[r]) : 0ull);
+            } else if (S.kind == VK_COUNT_NZ) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    atomicAdd(&w[base[r] + off], (((m >> r) & 1u) && cur[r] != 0) ? 1ull : 0ull);
+            } else {
+                long long* a = reinterpret_cast<long long*>(w);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (!((m >> r) & 1u)) continue;
+                    if (S.kind == VK_MIN) atomicMin(&a[base[r] + off], static_cast<long long>(cur[r]));
+                    else atomicMax(&a[base[r] + off], static_cast<long long>(cur[r]));
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL>
@@ -837,6 +1020,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
         if (!TAIL && RV.on) {
             for (uint32_t sel = m; sel; sel &= sel - 1) fast_row<NT>(P, RV, extra, stage, R * t + __ffs(sel) - 1, t, sink.upd, sink);
+            return;
+        }
+        // A warp whose rows are at least a quarter selected runs the dense
+        // column program; sparser warps loop over their selected rows only.
+        if (!TAIL && P.dense_vec && __reduce_add_sync(kFull, __popc(m)) >= 8u * R) {
+            chain_private_tile<NT>(P, extra, stage, t, m, sink);
             return;
         }
     }
