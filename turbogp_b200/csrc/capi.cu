@@ -553,6 +553,7 @@ bool compile_chain(Builder& b) {
                 if (F.dtype != DT_F64 && small && std::min(x0, x1) >= -lim && std::max(x0, x1) < lim &&
                     (F.dtype == DT_U8 || F.dtype == DT_I32)) {
                     S.flags |= CS_NARROW;
+                    if (std::min(x0, x1) >= 0) S.flags |= CS_NONNEG;
                     S.mul32 = static_cast<int32_t>(F.mul);
                     S.add32 = static_cast<int32_t>(F.add);
                 } else if (F.mul == 1 && F.add == 0) {
@@ -653,6 +654,9 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes) {
         if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "query does not fit in shared memory");
     }
     P.nstages = S;
+    // L2 prefetch ahead of the stage copies measured neutral on the scan and
+    // grouped-aggregate workloads, so it is off unless TGP_L2_AHEAD asks.
+    P.l2_ahead = ctx->l2_ahead >= 0 ? static_cast<uint32_t>(ctx->l2_ahead) : 0u;
     P.extra_off = static_cast<uint32_t>(kBarrierBytes + static_cast<size_t>(S) * stage);
     P.extra_off = (P.extra_off + 127u) & ~127u;
     P.smem_bytes = static_cast<uint32_t>(P.extra_off + extra_bytes);
@@ -662,7 +666,7 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes) {
 int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     if (ntiles == 0) return TGP_OK;
-    int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes);
+    int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
     if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
     const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * occ);
     std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
@@ -772,6 +776,8 @@ int tgp_init(tgp_ctx** out, int device) {
     }
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_L2_AHEAD")) ctx->l2_ahead = std::min(64, std::max(0, std::atoi(e)));
+    if (const char* e = std::getenv("TGP_NO_DENSE_SHAPES")) ctx->dense_shapes = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_SCAN_THREADS")) ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
     if (const char* e = std::getenv("TGP_MAX_STAGES"))
         ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
@@ -1186,6 +1192,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             // overflow checks.
             if (!acc128 && !J && !P.check_ovf && ctx->dense_path)
                 P.dense_vec = compile_chain(b) ? 1u : 0u;
+            if (P.dense_vec && ctx->dense_shapes) P.shape = dense_shape_of(P);
         } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;

@@ -25,8 +25,38 @@ constexpr uint64_t kWaitLimitNs = 1000ull * 1000ull * 1000ull;  // 1 s
 // ---------------------------------------------------------------------------
 // mbarrier (shared-memory transaction barrier)
 // ---------------------------------------------------------------------------
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory loads and stores on 32-bit shared addresses. They are
+// volatile so they keep their program order (a thread's read-modify-writes of
+// its private accumulators rely on it) and stay after the mbarrier waits.
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint2 lds_v2(uint32_t a) {
+    uint2 v;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint4 lds_v4(uint32_t a) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+    return v;
+}
+template <uint32_t OFF>
+__device__ __forceinline__ unsigned long long lds_u64(uint32_t a) {
+    unsigned long long v;
+    asm volatile("ld.shared.u64 %0, [%1+%2];" : "=l"(v) : "r"(a), "n"(OFF));
+    return v;
+}
+template <uint32_t OFF>
+__device__ __forceinline__ void sts_u64(uint32_t a, unsigned long long v) {
+    asm volatile("st.shared.u64 [%0+%1], %2;" ::"r"(a), "n"(OFF), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -96,6 +126,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
         " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst_smem)),
         "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar)), "l"(l2_policy)
         : "memory");
+}
+
+// Bulk prefetch of global memory into L2 (no shared memory, no completion).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src_gmem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src_gmem), "r"(bytes) : "memory");
 }
 
 // L2 policy for data read exactly once: evict first.

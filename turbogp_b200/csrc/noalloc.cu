@@ -371,7 +371,7 @@ extern "C" int tgp_aggregate_noalloc(int device, void* stream, const tgp_column_
 
     const uint64_t ntiles = (rows + kTileRows - 1) / kTileRows;
     if (ntiles) {
-        const int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes);
+        const int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
         if (occ <= 0) return report(err_msg, err_cap, TGP_DEVICE_ERROR, "scan kernel cannot be resident");
         const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(sms) * occ);
         NA_CUDA(launch_scan(P, mode, acc128, static_cast<int>(grid), st));

@@ -112,7 +112,8 @@ enum : uint8_t {
     CS_COL = 1,     // factor reads a staged column (else the constant `add`)
     CS_CHAIN = 2,   // multiply into the running product (else start a new one)
     CS_NARROW = 4,  // mul * x + add fits int32 for every cell: 32-bit arithmetic
-    CS_IDENT = 8    // mul == 1 and add == 0: the factor is the cell itself
+    CS_IDENT = 8,   // mul == 1 and add == 0: the factor is the cell itself
+    CS_NONNEG = 16  // CS_NARROW and mul * x + add >= 0 for every cell
 };
 struct ChainStep {
     uint32_t soff;   // staged column offset inside a stage
@@ -149,7 +150,7 @@ struct Plan {
     uint32_t smem_bytes;    // total dynamic shared memory
     uint32_t bitmap_words;  // MODE_FILTER: bitmap words written (0 = none)
     uint32_t nthreads;      // CTA size the plan's shared memory was sized for (256 or 512)
-    uint32_t _p2;
+    uint32_t l2_ahead;      // tiles a CTA prefetches into L2 ahead of its next stage copy (0 = none)
     SlotDesc slot[kMaxSlots];
 
     // WHERE program
@@ -167,6 +168,8 @@ struct Plan {
     uint32_t check_ovf;     // per-row overflow detection needed
     uint32_t count_by_tile; // MODE_GROUP_PRIVATE, one group, no join: row count = popcount per tile
     uint32_t dense_vec;     // MODE_GROUP_PRIVATE int64: `chain` holds the dense value program
+    uint32_t shape;         // ahead-of-time kernel for `chain` (0 = interpreted)
+    uint32_t _p4;
     uint64_t flush_limit;   // MODE_GROUP_PRIVATE int64: per-thread updates between flushes
     ValDesc val[kMaxVals];
 

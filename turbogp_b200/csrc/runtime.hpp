@@ -20,7 +20,10 @@ namespace tgp {
 
 // Launchers implemented in the .cu files.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st);
-int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem);
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape = 0);
+// Index (>= 1) of the ahead-of-time dense kernel matching the plan's key
+// dtypes and value program, or 0 (the interpreted dense program runs).
+uint32_t dense_shape_of(const Plan& P);
 size_t scan_kernel_static_smem();
 cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
                                  int sms, cudaStream_t st);
@@ -109,9 +112,11 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_L2_AHEAD).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
     bool dense_path = true;  // dense column programs for MODE_GROUP_PRIVATE (TGP_NO_DENSE=1 turns them off)
+    int l2_ahead = -1;         // L2 prefetch distance in tiles (TGP_L2_AHEAD; -1 = off)
+    bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
 };

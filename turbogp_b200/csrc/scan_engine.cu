@@ -26,6 +26,8 @@
 
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
+#include <utility>
 
 #include "device_common.cuh"
 #include "plan.hpp"
@@ -856,9 +858,11 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
     uint32_t base[R];  // word of row r's group count; value v is at base + v * NT
 #pragma unroll
     for (int r = 0; r < R; ++r) base[r] = g[r] * gstride + t;
+    // The slots are private to this thread, so plain read-modify-writes in
+    // program order are exact (64-bit shared atomics would run as CAS loops).
     if (!P.count_by_tile) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) atomicAdd(&w[base[r]], static_cast<unsigned long long>((m >> r) & 1u));
+        for (int r = 0; r < R; ++r) w[base[r]] += (m >> r) & 1u;
     }
 
     int64_t cur[R];
@@ -906,18 +910,17 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
             if (S.kind == VK_SUM) {
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    atomicAdd(&w[base[r] + off], ((m >> r) & 1u) ? static_cast<unsigned long long>(cur[r]) : 0ull);
+                    w[base[r] + off] += ((m >> r) & 1u) ? static_cast<unsigned long long>(cur[r]) : 0ull;
             } else if (S.kind == VK_COUNT_NZ) {
 #pragma unroll
-                for (int r = 0; r < R; ++r)
-                    atomicAdd(&w[base[r] + off], (((m >> r) & 1u) && cur[r] != 0) ? 1ull : 0ull);
+                for (int r = 0; r < R; ++r) w[base[r] + off] += (((m >> r) & 1u) && cur[r] != 0) ? 1ull : 0ull;
             } else {
                 long long* a = reinterpret_cast<long long*>(w);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (!((m >> r) & 1u)) continue;
-                    if (S.kind == VK_MIN) atomicMin(&a[base[r] + off], static_cast<long long>(cur[r]));
-                    else atomicMax(&a[base[r] + off], static_cast<long long>(cur[r]));
+                    long long& x = a[base[r] + off];
+                    x = S.kind == VK_MIN ? min(x, static_cast<long long>(cur[r])) : max(x, static_cast<long long>(cur[r]));
                 }
             }
         }
@@ -925,9 +928,214 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
 }
 
 // ---------------------------------------------------------------------------
+// Dense value programs of a fixed shape. The key dtypes and every step's
+// dtype / flags / kind / value slot are template constants (literals and
+// column offsets still come from the plan), so a tile runs as one
+// straight-line block: all shared-memory loads first, then the arithmetic,
+// then one batch of read-modify-writes per row.
+// Step code: dtype | flags << 4 | kind << 10 | value slot << 13.
+// ---------------------------------------------------------------------------
+constexpr uint32_t step_code(uint32_t dt, uint32_t fl, uint32_t kind, uint32_t acc) {
+    return dt | (fl << 4) | (kind << 10) | (acc << 13);
+}
+
+template <uint32_t NKEY, uint32_t KDT0, uint32_t KDT1, uint32_t... STEPS>
+struct DenseShape {
+    static constexpr uint32_t nkey = NKEY;
+    static constexpr uint32_t kdt0 = KDT0;
+    static constexpr uint32_t kdt1 = KDT1;
+    static constexpr uint32_t nsteps = sizeof...(STEPS);
+    static constexpr uint32_t step[sizeof...(STEPS)] = {STEPS...};
+    __host__ __device__ static constexpr uint32_t max_acc() {
+        uint32_t m = 0;
+        for (uint32_t i = 0; i < sizeof...(STEPS); ++i) m = ((step[i] >> 13) > m) ? (step[i] >> 13) : m;
+        return m;
+    }
+    static constexpr uint32_t nv1 = max_acc() + 1;  // value slots per group (slot 0 = row count)
+    __host__ __device__ static constexpr uint32_t kind_of(uint32_t v) {  // VK_* accumulated into value slot v
+        uint32_t k = VK_SUM;
+        for (uint32_t i = 0; i < sizeof...(STEPS); ++i)
+            if ((step[i] >> 13) == v) k = (step[i] >> 10) & 7u;
+        return k;
+    }
+};
+
+template <int... I, typename F>
+__device__ __forceinline__ void static_for_impl(std::integer_sequence<int, I...>, F&& f) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_impl(std::make_integer_sequence<int, N>{}, f);
+}
+
+// Thread t's R cells of a staged column at shared address `a` (low 32 bits).
+template <int R, uint32_t DT>
+__device__ __forceinline__ void lds_cells32(uint32_t a, uint32_t t, uint32_t (&x)[R]) {
+    if constexpr (DT == DT_U8) {
+        if constexpr (R == 4) {
+            const uint32_t w = lds_u32(a + 4u * t);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) x[e] = (w >> (8 * e)) & 0xffu;
+        } else {
+            const uint2 w = lds_v2(a + 8u * t);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                x[e] = (w.x >> (8 * e)) & 0xffu;
+                x[e + 4] = (w.y >> (8 * e)) & 0xffu;
+            }
+        }
+    } else if constexpr (DT == DT_I32) {
+#pragma unroll
+        for (int c = 0; c < R / 4; ++c) {
+            const uint4 v = lds_v4(a + 16u * ((R / 4) * t + c));
+            x[4 * c + 0] = v.x;
+            x[4 * c + 1] = v.y;
+            x[4 * c + 2] = v.z;
+            x[4 * c + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < R / 2; ++c) {
+            const uint4 v = lds_v4(a + 16u * ((R / 2) * t + c));
+            x[2 * c + 0] = v.x;
+            x[2 * c + 1] = v.z;
+        }
+    }
+}
+
+template <int R, uint32_t DT>
+__device__ __forceinline__ void lds_cells64(uint32_t a, uint32_t t, uint64_t (&x)[R]) {
+    if constexpr (DT == DT_I64 || DT == DT_U64) {
+#pragma unroll
+        for (int c = 0; c < R / 2; ++c) {
+            const uint4 v = lds_v4(a + 16u * ((R / 2) * t + c));
+            x[2 * c + 0] = (static_cast<uint64_t>(v.y) << 32) | v.x;
+            x[2 * c + 1] = (static_cast<uint64_t>(v.w) << 32) | v.z;
+        }
+    } else {
+        uint32_t y[R];
+        lds_cells32<R, DT>(a, t, y);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            x[r] = DT == DT_I32 ? static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(y[r]))) : y[r];
+    }
+}
+
+template <int NT, class SH>
+__device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                                  uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
+    constexpr int R = kTileRows / NT;
+    constexpr int NS = static_cast<int>(SH::nsteps);
+    constexpr uint32_t NV1 = SH::nv1;
+    const uint32_t sa = smem_addr(stage);
+
+    // Shared-memory loads of every referenced column, issued back to back.
+    uint32_t kx0[R], kx1[R];
+    if constexpr (SH::nkey >= 1) lds_cells32<R, SH::kdt0>(sa + P.gkey[0].soff, t, kx0);
+    if constexpr (SH::nkey >= 2) lds_cells32<R, SH::kdt1>(sa + P.gkey[1].soff, t, kx1);
+    uint32_t c32[NS][R];
+    uint64_t c64[NS][R];
+    static_for<NS>([&](auto I) {
+        constexpr uint32_t c = SH::step[I.value];
+        constexpr uint32_t dt = c & 15u, fl = (c >> 4) & 63u;
+        if constexpr ((fl & CS_COL) != 0) {
+            if constexpr ((fl & CS_NARROW) != 0) lds_cells32<R, dt>(sa + P.chain.s[I.value].soff, t, c32[I.value]);
+            else lds_cells64<R, dt>(sa + P.chain.s[I.value].soff, t, c64[I.value]);
+        }
+    });
+
+    const uint32_t nsel = __popc(m);
+    if (sink.upd + nsel > P.flush_limit) {
+        sink.flush_private_thread(P, extra, t);
+        sink.upd = 0;
+    }
+    sink.upd += nsel;
+
+    uint32_t sm[R];  // all ones for a selected row, else 0
+#pragma unroll
+    for (int r = 0; r < R; ++r) sm[r] = 0u - ((m >> r) & 1u);
+
+    // Values. A product starts from its first factor masked by the selection,
+    // so unselected rows carry 0 through every chained step.
+    uint64_t val[NV1][R];
+    uint64_t cur[R];
+    static_for<NS>([&](auto I) {
+        constexpr int s = I.value;
+        constexpr uint32_t c = SH::step[s];
+        constexpr uint32_t fl = (c >> 4) & 63u, acc = c >> 13;
+        constexpr bool chain = (fl & CS_CHAIN) != 0;
+        const ChainStep& S = P.chain.s[s];
+        if constexpr ((fl & CS_COL) != 0 && (fl & CS_NARROW) != 0) {
+            const uint32_t mu = static_cast<uint32_t>(S.mul32), ad = static_cast<uint32_t>(S.add32);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint32_t f = mu * c32[s][r] + ad;
+                if constexpr (!chain) f &= sm[r];
+                const uint64_t fw = (fl & CS_NONNEG) ? static_cast<uint64_t>(f)
+                                                     : static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(f)));
+                cur[r] = chain ? cur[r] * fw : fw;
+            }
+        } else if constexpr ((fl & CS_COL) != 0) {
+            const uint64_t mu = static_cast<uint64_t>(S.mul), ad = static_cast<uint64_t>(S.add);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint64_t f = (fl & CS_IDENT) ? c64[s][r] : mu * c64[s][r] + ad;
+                if constexpr (!chain) f &= static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(sm[r])));
+                cur[r] = chain ? cur[r] * f : f;
+            }
+        } else {
+            const uint64_t k = static_cast<uint64_t>(S.add);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                cur[r] = chain ? cur[r] * k : (k & static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(sm[r]))));
+        }
+        if constexpr (acc != 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) val[acc][r] = cur[r];
+        }
+    });
+
+    // Read-modify-writes of the thread's private slots, row by row (rows of
+    // one group share slots, so each row reads what the previous one wrote).
+    constexpr uint32_t kGroupBytes = NV1 * NT * 8u;
+    const uint32_t wa = smem_addr(extra) + 8u * t;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        uint32_t g = 0;
+        if constexpr (SH::nkey >= 1)
+            g += (kx0[r] - static_cast<uint32_t>(P.gkey[0].min)) * static_cast<uint32_t>(P.gkey[0].stride);
+        if constexpr (SH::nkey >= 2)
+            g += (kx1[r] - static_cast<uint32_t>(P.gkey[1].min)) * static_cast<uint32_t>(P.gkey[1].stride);
+        const uint32_t a = wa + g * kGroupBytes;
+        unsigned long long old[NV1];
+        static_for<NV1>([&](auto V) {
+            constexpr uint32_t v = V.value;
+            if constexpr (v > 0 || SH::nkey > 0) old[v] = lds_u64<v * NT * 8u>(a);
+        });
+        static_for<NV1>([&](auto V) {
+            constexpr uint32_t v = V.value;
+            if constexpr (v == 0) {
+                // The row count (a scalar aggregate counts by popcount per tile).
+                if constexpr (SH::nkey > 0) sts_u64<0>(a, old[0] + (sm[r] & 1u));
+            } else {
+                constexpr uint32_t kind = SH::kind_of(v);
+                unsigned long long nw;
+                const long long x = static_cast<long long>(val[v][r]);
+                if constexpr (kind == VK_SUM) nw = old[v] + val[v][r];
+                else if constexpr (kind == VK_COUNT_NZ) nw = old[v] + (val[v][r] != 0 ? 1ull : 0ull);
+                else if constexpr (kind == VK_MIN) nw = sm[r] ? static_cast<unsigned long long>(min(static_cast<long long>(old[v]), x)) : old[v];
+                else nw = sm[r] ? static_cast<unsigned long long>(max(static_cast<long long>(old[v]), x)) : old[v];
+                sts_u64<v * NT * 8u>(a, nw);
+            }
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128, int NT, bool TAIL>
+template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
 __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
                                              const uint8_t* stage, uint64_t tile, uint32_t t,
                                              unsigned long long& selected, const RegLeaves& RL,
@@ -1025,7 +1233,8 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
         // A warp whose rows are at least a quarter selected runs the dense
         // column program; sparser warps loop over their selected rows only.
         if (!TAIL && P.dense_vec && __reduce_add_sync(kFull, __popc(m)) >= 8u * R) {
-            chain_private_tile<NT>(P, extra, stage, t, m, sink);
+            if constexpr (std::is_void<SH>::value) chain_private_tile<NT>(P, extra, stage, t, m, sink);
+            else chain_tile_static<NT, SH>(P, extra, stage, t, m, sink);
             return;
         }
     }
@@ -1041,7 +1250,7 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
 // full[s]. No CTA-wide barrier runs per tile. Every wait is bounded; a wait
 // that gives up raises kErrWaitTimeout and the CTA drains its copies.
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128, int NT>
+template <uint32_t MODE, bool ACC128, int NT, class SH = void>
 __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant__ Plan P) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -1073,11 +1282,25 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
         // ---------------- producer warp (lane 0 issues) ----------------
         if (t != static_cast<uint32_t>(NT)) return;
         const uint64_t policy = l2_policy_evict_first();
+        // Tile j of this CTA is prefetched into L2 when tile j - l2_ahead is
+        // copied into its stage, so a stage copy reads L2 instead of waiting
+        // out the HBM latency (shared memory then need not cover it).
+        const uint32_t D = P.l2_ahead;
+        auto prefetch = [&](uint64_t j) {
+            const uint64_t tj = blockIdx.x + j * G;
+            if (tj >= nfull) return;
+            for (uint32_t c = 0; c < P.nslots; ++c) {
+                const uint32_t bytes = kTileRows * P.slot[c].width;
+                bulk_prefetch_l2(P.slot[c].ptr + tj * bytes, bytes);
+            }
+        };
+        for (uint64_t j = S; j < D; ++j) prefetch(j);
         uint64_t issued = 0;
         uint32_t s = 0, phase = 0;  // stage and phase of tile k (k = issued)
         for (uint64_t k = 0;; ++k) {
             const uint64_t tl = blockIdx.x + k * G;
             if (tl >= nfull) break;
+            if (D && k + D >= S) prefetch(k + D);
             if (k >= S) {
                 // Wait until every consumer warp has released tile k - S
                 // (the previous use of stage s, one phase earlier).
@@ -1113,7 +1336,8 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
     RegLeaves RL;
     load_reg_leaves(P, RL);
     RegVals RV;
-    load_reg_vals<MODE, ACC128>(P, RV);
+    if constexpr (std::is_void<SH>::value) load_reg_vals<MODE, ACC128>(P, RV);
+    else RV.on = 0;  // a fixed-shape kernel never takes the scalar fast path
     unsigned long long selected = 0;
     bool ok = true;
     uint32_t s = 0, phase = 0;  // stage and phase of the k-th full tile
@@ -1133,7 +1357,7 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
             // Lanes other than 0 observe the completed phase through a cheap
             // try_wait so their shared-memory reads are ordered after the copy.
             mbar_try_wait(&full[s], phase);
-            process_tile<MODE, ACC128, NT, false>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
+            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
                                                   tl, t, selected, RL, RV);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
@@ -1142,7 +1366,7 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
                 phase ^= 1u;
             }
         } else {
-            process_tile<MODE, ACC128, NT, true>(P, sink, extra, nullptr, tl, t, selected, RL, RV);
+            process_tile<MODE, ACC128, NT, true, SH>(P, sink, extra, nullptr, tl, t, selected, RL, RV);
         }
     }
 #pragma unroll
@@ -1178,7 +1402,69 @@ static const void* select_kernel(uint32_t mode, bool acc128) {
     }
 }
 
-static const void* select_kernel(uint32_t mode, bool acc128, int nt) {
+// Dense value-program shapes compiled ahead of time (index = Plan::shape).
+// The TPC-H Q1 shape: GROUP BY two u8 flags; sum(i32), sum(i64),
+// sum(i64 * (k - i32)), sum(i64 * (k - i32) * (k + i32)).
+constexpr uint32_t kNarrowPos = CS_COL | CS_NARROW | CS_NONNEG;
+using ShapeQ1 = DenseShape<2, DT_U8, DT_U8, step_code(DT_I32, kNarrowPos, VK_SUM, 1),
+                           step_code(DT_I64, CS_COL | CS_IDENT, VK_SUM, 2),
+                           step_code(DT_I32, kNarrowPos | CS_CHAIN, VK_SUM, 3),
+                           step_code(DT_I32, kNarrowPos | CS_CHAIN, VK_SUM, 4)>;
+
+struct ShapeEntry {
+    uint32_t nkey, kdt0, kdt1, nsteps;
+    uint32_t code[kMaxSteps];
+    const void* k256;
+    const void* k512;
+};
+
+template <class SH>
+static ShapeEntry shape_entry() {
+    ShapeEntry e{};
+    e.nkey = SH::nkey;
+    e.kdt0 = SH::nkey >= 1 ? SH::kdt0 : 0u;
+    e.kdt1 = SH::nkey >= 2 ? SH::kdt1 : 0u;
+    e.nsteps = SH::nsteps;
+    for (uint32_t i = 0; i < SH::nsteps; ++i) e.code[i] = SH::step[i];
+    e.k256 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 256, SH>);
+    e.k512 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 512, SH>);
+    return e;
+}
+
+static const ShapeEntry* shape_table(uint32_t* n) {
+    static const ShapeEntry table[] = {shape_entry<ShapeQ1>()};
+    *n = sizeof(table) / sizeof(table[0]);
+    return table;
+}
+
+uint32_t dense_shape_of(const Plan& P) {
+    if (!P.dense_vec || P.chain.nsteps == 0) return 0;
+    uint32_t code[kMaxSteps] = {};
+    for (uint32_t i = 0; i < P.chain.nsteps; ++i) {
+        const ChainStep& S = P.chain.s[i];
+        code[i] = step_code((S.flags & CS_COL) ? S.dtype : 0u, S.flags, S.kind, S.acc);
+    }
+    uint32_t n = 0;
+    const ShapeEntry* tab = shape_table(&n);
+    for (uint32_t j = 0; j < n; ++j) {
+        const ShapeEntry& e = tab[j];
+        if (e.nkey != P.ngkey || e.nsteps != P.chain.nsteps) continue;
+        if (e.nkey >= 1 && e.kdt0 != P.gkey[0].dtype) continue;
+        if (e.nkey >= 2 && e.kdt1 != P.gkey[1].dtype) continue;
+        bool same = true;
+        for (uint32_t i = 0; i < e.nsteps; ++i) same = same && e.code[i] == code[i];
+        if (same) return j + 1;
+    }
+    return 0;
+}
+
+static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t shape = 0) {
+    if (shape && mode == MODE_GROUP_PRIVATE && !acc128) {
+        uint32_t n = 0;
+        const ShapeEntry* tab = shape_table(&n);
+        if (shape <= n) return nt == 512 ? tab[shape - 1].k512 : nt == 256 ? tab[shape - 1].k256 : nullptr;
+        return nullptr;
+    }
     return nt == 512 ? select_kernel<512>(mode, acc128) : nt == 256 ? select_kernel<256>(mode, acc128) : nullptr;
 }
 
@@ -1221,7 +1507,7 @@ static cudaError_t ensure_smem_limit(KernelCacheEntry* e, const void* f, int sme
 
 // Launches with blockDim = nthreads consumers + one producer warp.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st) {
-    const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads));
+    const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads), P.shape);
     if (!f) return cudaErrorInvalidValue;
     {
         std::lock_guard<std::mutex> lock(g_kcache_mu);
@@ -1232,8 +1518,8 @@ cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cud
     return cudaLaunchKernel(f, dim3(grid), dim3(P.nthreads + 32), args, P.smem_bytes, st);
 }
 
-int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem) {
-    const void* f = select_kernel(mode, acc128, nt);
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape) {
+    const void* f = select_kernel(mode, acc128, nt, shape);
     if (!f) return 0;
     std::lock_guard<std::mutex> lock(g_kcache_mu);
     KernelCacheEntry* e = kernel_entry(f);

@@ -195,16 +195,44 @@ class AggResult:
     as_f64: float
 
 
-@dataclass
+_AGGVALUE_DTYPE = np.dtype([("lo", "<u8"), ("hi", "<i8"), ("count", "<u8"), ("as_f64", "<f8")])
+
+
 class QueryOutput:
-    keys: list[tuple[int, ...]]
-    values: list[list[AggResult]]
-    rows_scanned: int
-    rows_selected: int
-    flags: int
+    """Groups (key tuples) and their aggregates. A result read back from the
+    device keeps its raw arrays and builds the Python lists on first access."""
+
+    def __init__(self, keys, values, rows_scanned: int, rows_selected: int, flags: int, raw=None):
+        self._keys, self._values = keys, values
+        self.rows_scanned, self.rows_selected, self.flags = rows_scanned, rows_selected, flags
+        self._raw = raw  # (keys u64 array, AggValue records, ngroups, nkeys, naggs)
+
+    def _decode(self) -> None:
+        keys, vals, ng, nk, na = self._raw
+        kk = keys[:ng * nk].view(np.int64).reshape(ng, nk).tolist() if nk else [[] for _ in range(ng)]
+        lo, hi = vals["lo"].tolist(), vals["hi"].tolist()
+        cnt, f = vals["count"].tolist(), vals["as_f64"].tolist()
+        self._keys = [tuple(k) for k in kk]
+        self._values = [[AggResult((hi[i] << 64) | lo[i], cnt[i], f[i]) for i in range(g * na, g * na + na)]
+                        for g in range(ng)]
+        self._raw = None
+
+    @property
+    def keys(self) -> list[tuple[int, ...]]:
+        if self._keys is None:
+            self._decode()
+        return self._keys
+
+    @property
+    def values(self) -> list[list[AggResult]]:
+        if self._values is None:
+            self._decode()
+        return self._values
 
     @property
     def ngroups(self) -> int:
+        if self._raw is not None:
+            return self._raw[2]
         return len(self.values)
 
 
@@ -508,6 +536,7 @@ class PreparedQuery:
         self.cap = cap
         self.keys = np.zeros(max(1, cap * max(1, self.nk)), dtype=np.uint64)
         self.vals = (A.AggValue * max(1, cap * max(1, self.na)))()
+        self._vals_np = np.frombuffer(self.vals, dtype=_AGGVALUE_DTYPE)
 
     def run(self, decode: bool = True) -> QueryOutput:
         """Executes the query; with decode=False only the counts are returned
@@ -523,8 +552,9 @@ class PreparedQuery:
         r = self.res
         if not decode:
             return QueryOutput([], [], int(r.rows_scanned), int(r.rows_selected), int(r.flags))
-        ks, vs = decode_groups(self.keys, self.vals, int(r.ngroups), self.nk, self.na)
-        return QueryOutput(ks, vs, int(r.rows_scanned), int(r.rows_selected), int(r.flags))
+        ng = int(r.ngroups)
+        raw = (self.keys[:ng * self.nk].copy(), self._vals_np[:ng * self.na].copy(), ng, self.nk, self.na)
+        return QueryOutput(None, None, int(r.rows_scanned), int(r.rows_selected), int(r.flags), raw)
 
 
 class JoinTable:
