@@ -227,3 +227,66 @@ def test_dense_flushes_near_int64_bound(ctx):
             o = oracle.aggregate(cols, None, aggs, gb, w)
             same_query(g, o)
     tb.drop()
+
+
+def test_join_payload_and_hash_probe_paths(ctx):
+    """Joined aggregates through the unique-key payload array (dense build key
+    range) and through the hash table (duplicate keys, sparse key range), with
+    build-side, probe-side and mixed group keys."""
+    nb, n = 40_000, 300_000
+    dim = datagen.dimension(nb, seed=17)
+    fact = datagen.fact_fk(n, nb, 0.8, seed=18)
+    fact["fk"][::97] = nb + 5          # keys past the build range
+    fact["fk"][::89] = 0               # keys below it
+    fct = {**CT, "fk": "int"}
+    f = ctx.register(fact, fct)
+    variants = {
+        "dense": dim,
+        "sparse": {**dim, "key": (dim["key"].astype(np.int64) * 1_000_003).astype(np.int64)},
+        "dup": {**dim, "key": (dim["key"] // 2 + 1).astype(np.int32)},
+    }
+    p, d = col("price_cents"), col("discount_pct")
+    aggs = [sum_(p * (100 - d)), count_star(), max_(col("quantity")), sum_(col("quantity"))]
+    for name, dh in variants.items():
+        probe = dict(fact)
+        if name == "sparse":
+            probe = {**fact, "fk": (fact["fk"].astype(np.int64) * 1_000_003)}
+        fp = ctx.register(probe, fct) if name == "sparse" else f
+        dt = ctx.register(dh, datagen.DIMENSION_COLTYPES)
+        j = dt.join_build("key", col("order_day") < datagen.DAY0 + datagen.NDAYS // 2)
+        for gb in [(build_col("segment"),), (), (build_col("segment"), "flag_a"), ("flag_b",)]:
+            for where in [None, col("quantity") < 30]:
+                g = fp.aggregate(aggs, gb, where, join=j, probe_key="fk")
+                o = oracle.aggregate(probe, fct, aggs, gb, where,
+                                     build=(dh, datagen.DIMENSION_COLTYPES, "key",
+                                            col("order_day") < datagen.DAY0 + datagen.NDAYS // 2),
+                                     probe_key="fk")
+                same_query(g, o)
+        j.drop()
+        dt.drop()
+        if fp is not f:
+            fp.drop()
+    f.drop()
+
+
+def test_hash_grouping_hot_keys_and_device_format(ctx):
+    """Hash grouping over Zipf keys (shared pre-aggregation of hot keys, then
+    the global table), multi-key packed tuples, results sorted and formatted
+    on the device; large values switch the pre-aggregation off."""
+    n = 2_000_003
+    h = datagen.highcard(n, 200_000, 1.1, seed=9)
+    rng = np.random.default_rng(3)
+    h["k2"] = rng.integers(-3, 4, n, dtype=np.int32)
+    h["big"] = rng.integers(-2**40, 2**40, n, dtype=np.int64)
+    t = ctx.register(h)
+    cases = [
+        ([count_star(), sum_(col("value")), avg(col("value")), count_col(col("value"))], ("key",), None),
+        ([count_star(), sum_((col("value") - 7) * 3)], ("key", "k2"), col("value") < 900),
+        ([sum_(col("big")), count_star(), min_(col("value"))], ("key",), None),
+        ([count_star()], ("k2", "key"), col("value") >= 500),
+    ]
+    for aggs, gb, where in cases:
+        g = t.aggregate(aggs, gb, where, group_cap=1 << 20)
+        o = oracle.aggregate(h, None, aggs, gb, where)
+        same_query(g, o)
+    t.drop()

@@ -14,6 +14,7 @@
 
 #include "device_common.cuh"
 #include "plan.hpp"
+#include "turbogp_gpu.h"
 
 namespace tgp {
 
@@ -275,6 +276,118 @@ cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots
     gather_groups_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(htab, nslots, stride, out,
                                                                                cap, counter);
     return cudaGetLastError();
+}
+
+// Join payload: for every entry (key_rel, row) of a packed join table with
+// unique keys, pay[key_rel] = sum over build-side group keys of
+// (cell[row] - min) * stride. Unset entries keep 0xffffffff (no match).
+__device__ __forceinline__ int64_t pay_cell(const uint8_t* base, uint32_t dtype, uint32_t row) {
+    if (dtype == DT_U8) return static_cast<int64_t>(__ldg(base + row));
+    if (dtype == DT_I32) return static_cast<int64_t>(__ldg(reinterpret_cast<const int32_t*>(base) + row));
+    return static_cast<int64_t>(__ldg(reinterpret_cast<const long long*>(base) + row));
+}
+
+__global__ void join_pay_kernel(const unsigned long long* tab, uint64_t cap, const PayKeys K, uint32_t* pay) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < cap;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long e = tab[i];
+        if (e == ~0ull) continue;
+        const uint32_t row = static_cast<uint32_t>(e & 0xffffffffull);
+        uint64_t g = 0;
+        for (uint32_t k = 0; k < K.n; ++k)
+            g += (static_cast<uint64_t>(pay_cell(K.ptr[k], K.dtype[k], row)) - static_cast<uint64_t>(K.min[k])) *
+                 K.stride[k];
+        pay[e >> 32] = static_cast<uint32_t>(g);
+    }
+}
+
+cudaError_t launch_join_pay(const unsigned long long* tab, uint64_t cap, const PayKeys& K, uint32_t* pay,
+                            uint64_t pay_entries, int sms, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(pay, 0xff, pay_entries * 4, st);
+    if (e != cudaSuccess) return e;
+    uint64_t blocks = (cap + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    join_pay_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(tab, cap, K, pay);
+    return cudaGetLastError();
+}
+
+// Hash-grouped results on the device: sort the gathered slots by packed key
+// and write the caller's layout (keys per group, tgp_agg_value per aggregate).
+__global__ void extract_keys_kernel(const unsigned long long* packed, uint64_t n, uint32_t stride,
+                                    unsigned long long* keys, uint32_t* idx) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        keys[i] = packed[i * stride];
+        idx[i] = static_cast<uint32_t>(i);
+    }
+}
+
+__global__ void format_hash_groups_kernel(const unsigned long long* packed, const uint32_t* order, uint64_t n,
+                                          const HashFormat F, uint64_t* keys_out, tgp_agg_value* vals_out) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long* s = packed + static_cast<uint64_t>(order[i]) * F.hstride;
+        if (keys_out)
+            for (uint32_t k = 0; k < F.nkey; ++k)
+                keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((s[0] >> F.key_shift[k]) & F.key_mask[k]);
+        if (!vals_out) continue;
+        const uint64_t cnt = s[1];
+        for (uint32_t a = 0; a < F.nagg; ++a) {
+            tgp_agg_value o;
+            o.count = cnt;
+            if (F.val[a] < 0) {
+                o.lo = cnt;
+                o.hi = 0;
+                o.as_f64 = static_cast<double>(cnt);
+            } else {
+                const unsigned long long* v = s + 2 + 2 * F.val[a];
+                if (F.kind[a] == VK_MIN || F.kind[a] == VK_MAX) {
+                    const int64_t x = static_cast<int64_t>(v[0]);
+                    o.lo = static_cast<uint64_t>(x);
+                    o.hi = x < 0 ? -1 : 0;
+                    o.as_f64 = static_cast<double>(x);
+                } else {
+                    o.lo = v[0];
+                    o.hi = static_cast<int64_t>(v[1]);
+                    const double f = i128_to_f64_rn(o.lo, o.hi);
+                    o.as_f64 = F.func[a] == TGP_AGG_AVG ? (cnt ? f / static_cast<double>(cnt) : 0.0) : f;
+                }
+            }
+            vals_out[i * F.nagg + a] = o;
+        }
+    }
+}
+
+cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, const HashFormat& F, uint32_t key_bits,
+                               void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
+                               int sms, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    // scratch: keys[2n] u64, idx[2n] u32, then CUB temporary storage.
+    unsigned long long* k0 = static_cast<unsigned long long*>(scratch);
+    unsigned long long* k1 = k0 + n;
+    uint32_t* i0 = reinterpret_cast<uint32_t*>(k1 + n);
+    uint32_t* i1 = i0 + n;
+    uint8_t* tmp = reinterpret_cast<uint8_t*>(i1 + n);
+    const size_t head = n * 16 + n * 8;
+    size_t tmp_bytes = scratch_bytes > head ? scratch_bytes - head : 0;
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    extract_keys_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(packed, n, F.hstride, k0, i0);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, i0, i1, static_cast<int>(n), 0,
+                                                    static_cast<int>(key_bits ? key_bits : 1), st);
+    if (e != cudaSuccess) return e;
+    format_hash_groups_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(packed, i1, n, F, keys_out,
+                                                                                     vals_out);
+    return cudaGetLastError();
+}
+
+size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits) {
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, static_cast<unsigned long long*>(nullptr),
+                                    static_cast<unsigned long long*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                    static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0,
+                                    static_cast<int>(key_bits ? key_bits : 1));
+    return n * 24 + tmp + 256;
 }
 
 }  // namespace tgp

@@ -88,14 +88,30 @@ struct Carve {
     }
 };
 
+// Per-call device buffers (join tables, payloads, gathered groups) come from
+// the stream-ordered pool, which keeps freed memory for the next call.
+int dev_alloc(tgp_ctx* ctx, void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (cudaMallocAsync(p, std::max<size_t>(bytes, 256), ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(ctx, TGP_OOM, what);
+    }
+    return TGP_OK;
+}
+
+void dev_free(tgp_ctx* ctx, void* p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 int arena_reserve(tgp_ctx* ctx, size_t bytes, Carve* out) {
     bytes = bytes + 4096;
     if (bytes > ctx->arena.cap) {
         TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+        const size_t want = std::max(bytes, ctx->arena.cap * 2);
         if (ctx->arena.base) cudaFree(ctx->arena.base);
         ctx->arena.base = nullptr;
         ctx->arena.cap = 0;
-        size_t want = std::max(bytes, ctx->arena.cap * 2);
         if (cudaMalloc(&ctx->arena.base, want) != cudaSuccess) {
             cudaGetLastError();
             return fail(ctx, TGP_OOM, "device scratch allocation failed");
@@ -507,11 +523,13 @@ struct Builder {
 // continues its running product; any other value starts a new one. Returns
 // false (dense path off) when a factor or key is not staged, more than two
 // keys group, or the program needs more than kMaxSteps steps.
-bool compile_chain(Builder& b) {
+bool compile_chain(Builder& b, bool build_keys_in_payload) {
     Plan& P = b.P;
     if (P.ngkey > 2) return false;
-    for (uint32_t k = 0; k < P.ngkey; ++k)
+    for (uint32_t k = 0; k < P.ngkey; ++k) {
+        if (P.gkey[k].build_side && build_keys_in_payload) continue;
         if (P.gkey[k].slot < 0 || P.gkey[k].build_side) return false;
+    }
     std::vector<int> slot2col(P.nslots, -1);
     for (size_t c = 0; c < b.col2slot.size(); ++c)
         if (b.col2slot[c] >= 0) slot2col[b.col2slot[c]] = static_cast<int>(c);
@@ -723,6 +741,13 @@ int upload(tgp_ctx* ctx, void* dst, const void* src, size_t bytes) {
     return TGP_OK;
 }
 
+void free_join(tgp_ctx* ctx, JoinTable& J) {
+    dev_free(ctx, J.tab);
+    dev_free(ctx, J.pay);
+    J.tab = nullptr;
+    J.pay = nullptr;
+}
+
 }  // namespace
 
 // ==========================================================================
@@ -774,8 +799,18 @@ int tgp_init(tgp_ctx** out, int device) {
         delete ctx;
         return TGP_DEVICE_ERROR;
     }
+    // The stream-ordered pool keeps memory freed by this process for reuse
+    // (a per-process setting of the device's default pool).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_NO_HASH_PRESUM")) ctx->hash_presum = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_L2_AHEAD")) ctx->l2_ahead = std::min(64, std::max(0, std::atoi(e)));
     if (const char* e = std::getenv("TGP_NO_DENSE_SHAPES")) ctx->dense_shapes = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_SCAN_THREADS")) ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
@@ -792,13 +827,13 @@ int tgp_shutdown(tgp_ctx* ctx) {
     for (auto& kv : ctx->tables)
         for (auto& c : kv.second.cols)
             if (c.owned && c.dptr) cudaFree(c.dptr);
-    for (auto& kv : ctx->joins)
-        if (kv.second.tab) cudaFree(kv.second.tab);
+    for (auto& kv : ctx->joins) free_join(ctx, kv.second);
     for (void* h : ctx->hash_handles) {
         JoinTable* J = static_cast<JoinTable*>(h);
-        if (J->tab) cudaFree(J->tab);
+        free_join(ctx, *J);
         delete J;
     }
+    cudaStreamSynchronize(ctx->stream);
     if (ctx->arena.base) cudaFree(ctx->arena.base);
     if (ctx->kin) cudaFree(ctx->kin);
     if (ctx->hpin) cudaFreeHost(ctx->hpin);
@@ -1066,7 +1101,7 @@ int tgp_filter(tgp_ctx* ctx, tgp_table_id table, const tgp_pred_node* pred, uint
 // --------------------------------------------------------------------------
 // Aggregation queries
 // --------------------------------------------------------------------------
-static int join_lookup(tgp_ctx* ctx, tgp_join_id id, const JoinTable** out) {
+static int join_lookup(tgp_ctx* ctx, tgp_join_id id, JoinTable** out) {
     auto it = ctx->joins.find(id);
     if (it == ctx->joins.end()) return fail(ctx, TGP_NOT_FOUND, "unknown join id");
     *out = &it->second;
@@ -1092,7 +1127,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     const Table* T;
     TGP_TRY(get_table(ctx, q->table, &T));
     Builder b(ctx, T);
-    const JoinTable* J = nullptr;
+    JoinTable* J = nullptr;
     if (q->join) {
         TGP_TRY(join_lookup(ctx, q->join, &J));
         TGP_TRY(get_table(ctx, J->build_table, &b.B));
@@ -1152,6 +1187,14 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     }
     P.ngkey = q->ngroup;
 
+    // Join payload: with unique build keys over a dense key range, and no
+    // build-side aggregate arguments, a probe row needs one lookup,
+    // pay[key - kmin] = the build-side part of its group index.
+    bool pay_ok = J && J->unique && !J->empty_range && ctx->join_payload &&
+                  J->krange + 1 <= std::min<uint64_t>(1ull << 28, std::max<uint64_t>(1ull << 22, 8 * J->entries));
+    for (uint32_t v = 0; pay_ok && v < P.nval; ++v)
+        for (uint32_t f = 0; f < P.val[v].nf; ++f) pay_ok = pay_ok && !P.val[v].f[f].build_side;
+
     uint32_t mode;
     bool acc128 = false;
     uint64_t ngroups_direct = 1;
@@ -1190,9 +1233,9 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             }
             // Dense column program: int64 partials, no join, no per-row
             // overflow checks.
-            if (!acc128 && !J && !P.check_ovf && ctx->dense_path)
-                P.dense_vec = compile_chain(b) ? 1u : 0u;
-            if (P.dense_vec && ctx->dense_shapes) P.shape = dense_shape_of(P);
+            if (!acc128 && (!J || pay_ok) && !P.check_ovf && ctx->dense_path)
+                P.dense_vec = compile_chain(b, pay_ok) ? 1u : 0u;
+            if (P.dense_vec && ctx->dense_shapes && !J) P.shape = dense_shape_of(P);
         } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;
@@ -1214,6 +1257,33 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             return fail(ctx, TGP_UNSUPPORTED, "group key spans all 2^64 values");
     }
 
+    if (pay_ok && mode != MODE_GROUP_HASH) {
+        PayKeys K;
+        std::memset(&K, 0, sizeof(K));
+        std::vector<uint64_t> sig;
+        for (uint32_t k = 0; k < P.ngkey; ++k) {
+            if (!P.gkey[k].build_side) continue;
+            K.ptr[K.n] = P.gkey[k].bptr;
+            K.dtype[K.n] = P.gkey[k].dtype;
+            K.min[K.n] = P.gkey[k].min;
+            K.stride[K.n] = P.gkey[k].stride;
+            ++K.n;
+            sig.insert(sig.end(), {q->group[k].column, static_cast<uint64_t>(P.gkey[k].min), P.gkey[k].stride});
+        }
+        const uint64_t entries = J->krange + 1;
+        if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) {
+            if (J->pay && J->pay_entries != entries) {
+                dev_free(ctx, J->pay);
+                J->pay = nullptr;
+            }
+            if (!J->pay) TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&J->pay), entries * 4, "join payload allocation failed"));
+            J->pay_entries = entries;
+            J->pay_sig = sig;
+            TGP_CUDA(launch_join_pay(J->tab, J->cap, K, J->pay, entries, ctx->sms, ctx->stream));
+        }
+        P.jpay = J->pay;
+    }
+
     // Hash table sizing: twice the bound on distinct groups.
     uint64_t hcap = 0;
     if (mode == MODE_GROUP_HASH) {
@@ -1223,6 +1293,20 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         P.hstride = 2 + 2 * P.nval;
         P.hlog2 = log2u(hcap);
         P.hmask = hcap - 1;
+        // Shared pre-aggregation of repeated keys: SUM / COUNT(col) values,
+        // no join, no per-row overflow checks; its i32 partials are bounded
+        // below once the launch grid is known.
+        bool presum = ctx->hash_presum && !join && !P.check_ovf;
+        for (uint32_t v = 0; presum && v < P.nval; ++v)
+            presum = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
+        const uint32_t HS = 4096;
+        const size_t bytes = static_cast<size_t>(HS) * (12 + 4 * P.nval);
+        const size_t budget = ctx->max_dyn_smem - scan_kernel_static_smem() - kBarrierBytes;
+        if (presum && bytes + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+            P.hsm_slots = HS;
+            P.hsm_log2 = log2u(HS);
+            extra = bytes;
+        }
     }
 
     // Scratch: accumulators (direct/scalar) or hash table, counters, error word.
@@ -1270,6 +1354,16 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         }
     }
     TGP_TRY(size_smem(ctx, P, extra));
+    if (P.hsm_slots) {
+        // Rows one CTA scans, at the grid launch() uses: each i32 partial
+        // stays below 2^31 in magnitude.
+        const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
+        const int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
+        const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * std::max(occ, 1)));
+        const unsigned __int128 rows_cta = static_cast<unsigned __int128>((ntiles + grid - 1) / grid) * kTileRows;
+        const unsigned __int128 bound = rows_cta * std::max<uint64_t>(b.max_abs_val, 1);
+        if (bound >= (static_cast<unsigned __int128>(1) << 31)) P.hsm_slots = 0;
+    }
     TGP_TRY(launch(ctx, P, mode, acc128));
 
     TGP_TRY(pinned_reserve(ctx, block_words * 8));
@@ -1317,20 +1411,58 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     TGP_CUDA(cudaMemsetAsync(P.counters + 2, 0, 8, ctx->stream));
     unsigned long long* packed = nullptr;
     const uint64_t max_groups = std::min<uint64_t>(hcap, static_cast<uint64_t>(std::min<unsigned __int128>(D, hcap)));
-    if (cudaMalloc(&packed, std::max<uint64_t>(max_groups, 1) * P.hstride * 8) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, TGP_OOM, "group gather allocation failed");
-    }
+    TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&packed), std::max<uint64_t>(max_groups, 1) * P.hstride * 8,
+                      "group gather allocation failed"));
     TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream));
     unsigned long long ng = 0;
     TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    result->ngroups = ng;
+    if (ng > group_cap) {
+        dev_free(ctx, packed);
+        return fail(ctx, TGP_CAPACITY, "group buffer too small");
+    }
+    if (nagg <= static_cast<uint32_t>(kMaxFormatAggs)) {
+        // Sort by packed key (= ascending lexicographic key order, key 0 in
+        // the top bits) and format on the device; copy the caller's arrays once.
+        HashFormat F;
+        std::memset(&F, 0, sizeof(F));
+        F.nkey = q->ngroup;
+        F.nagg = nagg;
+        F.hstride = P.hstride;
+        for (uint32_t k = 0; k < q->ngroup; ++k) {
+            F.key_shift[k] = P.gkey[k].shift;
+            F.key_mask[k] = bits[k] >= 64 ? ~0ull : ((1ull << bits[k]) - 1);
+            F.key_min[k] = kmin[k];
+        }
+        for (uint32_t a = 0; a < nagg; ++a) {
+            F.func[a] = static_cast<uint8_t>(amap[a].func);
+            F.val[a] = static_cast<int8_t>(amap[a].val);
+            F.kind[a] = amap[a].val >= 0 ? P.val[amap[a].val].kind : VK_SUM;
+        }
+        const size_t sbytes = format_hash_groups_scratch(ng, total_bits);
+        const size_t kbytes = (keys_out ? ng * q->ngroup * 8 : 0), vbytes = (vals_out ? ng * nagg * sizeof(tgp_agg_value) : 0);
+        uint8_t* buf = nullptr;
+        const size_t kofs = (sbytes + 255) & ~size_t{255}, vofs = kofs + ((kbytes + 255) & ~size_t{255});
+        if (int st = dev_alloc(ctx, reinterpret_cast<void**>(&buf), vofs + vbytes, "group format allocation failed")) {
+            dev_free(ctx, packed);
+            return st;
+        }
+        uint64_t* dkeys = kbytes ? reinterpret_cast<uint64_t*>(buf + kofs) : nullptr;
+        tgp_agg_value* dvals = vbytes ? reinterpret_cast<tgp_agg_value*>(buf + vofs) : nullptr;
+        cudaError_t e = format_hash_groups(packed, ng, F, total_bits, buf, sbytes, dkeys, dvals, ctx->sms, ctx->stream);
+        if (e == cudaSuccess && kbytes) e = cudaMemcpyAsync(keys_out, dkeys, kbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && vbytes) e = cudaMemcpyAsync(vals_out, dvals, vbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        dev_free(ctx, buf);
+        dev_free(ctx, packed);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("group format: ") + cudaGetErrorString(e));
+        return TGP_OK;
+    }
     std::vector<unsigned long long> slots(ng * P.hstride);
     if (ng) TGP_CUDA(cudaMemcpyAsync(slots.data(), packed, ng * P.hstride * 8, cudaMemcpyDeviceToHost, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaFree(packed);
-    result->ngroups = ng;
-    if (ng > group_cap) return fail(ctx, TGP_CAPACITY, "group buffer too small");
+    dev_free(ctx, packed);
     // Packed key order == ascending lexicographic key order (key 0 in the top bits).
     std::vector<uint64_t> order(ng);
     for (uint64_t i = 0; i < ng; ++i) order[i] = i;
@@ -1382,10 +1514,7 @@ static int build_join(tgp_ctx* ctx, const Table* T, tgp_table_id table_id, uint3
     J.cap = next_pow2(std::max<uint64_t>(16, 2 * T->rows));
     J.log2 = log2u(J.cap);
     const uint64_t words = J.cap * (J.wide ? 2 : 1);
-    if (cudaMalloc(&J.tab, words * 8) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, TGP_OOM, "join table allocation failed");
-    }
+    TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&J.tab), words * 8, "join table allocation failed"));
     if (J.wide) TGP_CUDA(cudaMemsetAsync(J.tab, 0, words * 8, ctx->stream));
     else TGP_CUDA(cudaMemsetAsync(J.tab, 0xff, words * 8, ctx->stream));
     Plan& P = b.P;
@@ -1405,19 +1534,20 @@ static int build_join(tgp_ctx* ctx, const Table* T, tgp_table_id table_id, uint3
     P.jkrange = J.krange;
     int st = size_smem(ctx, P, 0);
     if (st == TGP_OK) st = launch(ctx, P, MODE_JOIN_BUILD, false);
-    unsigned long long cnt = 0;
+    unsigned long long cnt[4] = {0, 0, 0, 0};
     uint32_t err = 0;
     if (st == TGP_OK) {
-        cudaMemcpyAsync(&cnt, P.counters, 8, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(cnt, P.counters, 32, cudaMemcpyDeviceToHost, ctx->stream);
         cudaMemcpyAsync(&err, P.err, 4, cudaMemcpyDeviceToHost, ctx->stream);
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, "join build failed");
         else st = check_kernel_err(ctx, err);
     }
     if (st != TGP_OK) {
-        cudaFree(J.tab);
+        free_join(ctx, J);
         return st;
     }
-    J.entries = cnt;
+    J.entries = cnt[0];
+    J.unique = !J.wide && cnt[3] == 0;
     *out = J;
     return TGP_OK;
 }
@@ -1439,8 +1569,7 @@ int tgp_join_drop(tgp_ctx* ctx, tgp_join_id id) {
     if (!ctx) return TGP_INVALID_ARG;
     auto it = ctx->joins.find(id);
     if (it == ctx->joins.end()) return fail(ctx, TGP_NOT_FOUND, "unknown join id");
-    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
-    cudaFree(it->second.tab);
+    free_join(ctx, it->second);
     ctx->joins.erase(it);
     return TGP_OK;
 }
@@ -1449,7 +1578,7 @@ int tgp_join_probe_pairs(tgp_ctx* ctx, tgp_join_id join, tgp_table_id probe_tabl
                          const tgp_pred_node* pred, uint32_t npred, uint32_t* probe_rows, uint32_t* build_rows,
                          uint64_t cap, uint64_t* npairs) {
     if (!ctx || !npairs) return fail(ctx, TGP_INVALID_ARG, "null argument");
-    const JoinTable* J;
+    JoinTable* J;
     TGP_TRY(join_lookup(ctx, join, &J));
     const Table* T;
     TGP_TRY(get_table(ctx, probe_table, &T));
@@ -1768,7 +1897,7 @@ int tgp_hash_table_free(tgp_ctx* ctx, void* handle) {
     if (it == ctx->hash_handles.end()) return fail(ctx, TGP_INVALID_ARG, "unknown hash table handle");
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
     JoinTable* J = static_cast<JoinTable*>(handle);
-    if (J->tab) cudaFree(J->tab);
+    free_join(ctx, *J);
     delete J;
     ctx->hash_handles.erase(it);
     return TGP_OK;

@@ -185,6 +185,9 @@ struct Plan {
     uint64_t hmask;
     uint32_t hlog2;
     uint32_t hstride;       // u64 words per slot
+    uint32_t hsm_slots;     // per-CTA shared pre-aggregation slots (power of two; 0 = none):
+                            // [keys u64][counts u32][value partials i32 x nval], SUM / COUNT_NZ only
+    uint32_t hsm_log2;
 
     // Join table (probe side: MODE_GROUP_* / MODE_SCALAR with join, MODE_JOIN_PAIRS;
     // build side: MODE_JOIN_BUILD). Packed slots: (key_rel << 32) | build_row.
@@ -197,6 +200,7 @@ struct Plan {
     uint32_t _p1;
     int64_t jkmin;
     uint64_t jkrange;       // kmax - kmin (unsigned)
+    const uint32_t* jpay;   // unique build keys: per-key payload (build-side group index part), or null
 
     // Outputs
     unsigned long long* acc;        // direct/scalar accumulators [g][1 + nval][2]
@@ -206,6 +210,71 @@ struct Plan {
     uint32_t* err;                  // kErr* bits
     unsigned long long* out_pairs;  // MODE_JOIN_PAIRS: (probe_row << 32) | build_row
     uint64_t out_cap;
+};
+
+// Build-side group keys folded into a join payload array.
+struct PayKeys {
+    uint32_t n;
+    uint32_t dtype[kMaxGroupKeys];
+    const uint8_t* ptr[kMaxGroupKeys];
+    int64_t min[kMaxGroupKeys];
+    uint64_t stride[kMaxGroupKeys];
+};
+
+#if defined(__CUDACC__)
+#define TGP_HD __host__ __device__
+#else
+#define TGP_HD
+#endif
+
+// The int128 (hi:lo two's complement) nearest to a double, round to nearest
+// even: the same value on host and device.
+TGP_HD inline double i128_to_f64_rn(uint64_t lo, int64_t hi) {
+    const bool neg = hi < 0;
+    unsigned __int128 m = (static_cast<unsigned __int128>(static_cast<uint64_t>(hi)) << 64) | lo;
+    if (neg) m = ~m + 1;
+    const uint64_t mhi = static_cast<uint64_t>(m >> 64), mlo = static_cast<uint64_t>(m);
+    double d;
+    if (mhi == 0 && (mlo >> 53) == 0) {
+        d = static_cast<double>(mlo);  // exact
+    } else {
+#if defined(__CUDA_ARCH__)
+        const int msb = mhi ? 127 - __clzll(static_cast<long long>(mhi)) : 63 - __clzll(static_cast<long long>(mlo));
+#else
+        const int msb = mhi ? 127 - __builtin_clzll(mhi) : 63 - __builtin_clzll(mlo);
+#endif
+        int shift = msb - 52;
+        unsigned __int128 mant = m >> shift;
+        const unsigned __int128 rem = m & ((static_cast<unsigned __int128>(1) << shift) - 1);
+        const unsigned __int128 half = static_cast<unsigned __int128>(1) << (shift - 1);
+        if (rem > half || (rem == half && (mant & 1))) {
+            mant += 1;
+            if (mant >> 53) {
+                mant >>= 1;
+                shift += 1;
+            }
+        }
+        const uint64_t bits = (static_cast<uint64_t>(shift + 52 + 1023) << 52) |
+                              (static_cast<uint64_t>(mant) & ((1ull << 52) - 1));
+#if defined(__CUDA_ARCH__)
+        d = __longlong_as_double(static_cast<long long>(bits));
+#else
+        __builtin_memcpy(&d, &bits, 8);
+#endif
+    }
+    return neg ? -d : d;
+}
+
+// Output layout of hash-grouped results (tgp_execute with hash grouping).
+constexpr int kMaxFormatAggs = 32;
+struct HashFormat {
+    uint32_t nkey, nagg, hstride, _pad;
+    uint32_t key_shift[kMaxGroupKeys];
+    uint64_t key_mask[kMaxGroupKeys];
+    int64_t key_min[kMaxGroupKeys];
+    uint8_t func[kMaxFormatAggs];   // tgp_agg_func
+    int8_t val[kMaxFormatAggs];     // value index, -1 = COUNT(*)
+    uint8_t kind[kMaxFormatAggs];   // VK_* of that value
 };
 
 // Multiplicative hash of a relative key into a power-of-two table.

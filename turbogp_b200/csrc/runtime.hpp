@@ -42,6 +42,12 @@ cudaError_t launch_split_pairs(const unsigned long long* pairs, uint64_t n, uint
                                uint32_t* build, int sms, cudaStream_t st);
 cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, int sms,
                             cudaStream_t st);
+cudaError_t launch_join_pay(const unsigned long long* tab, uint64_t cap, const PayKeys& K, uint32_t* pay,
+                            uint64_t pay_entries, int sms, cudaStream_t st);
+cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, const HashFormat& F, uint32_t key_bits,
+                               void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
+                               int sms, cudaStream_t st);
+size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits);
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
                                  int sms, cudaStream_t st);
@@ -78,6 +84,11 @@ struct JoinTable {
     uint64_t krange = 0;
     uint64_t entries = 0;               // build rows inserted
     bool empty_range = false;           // no build key statistics (empty build side)
+    bool unique = false;                // no two build rows share a key (packed tables only)
+    // Cached payload array for one build-side group-key layout (see PayKeys).
+    uint32_t* pay = nullptr;
+    uint64_t pay_entries = 0;
+    std::vector<uint64_t> pay_sig;      // (column, min, stride) per build-side key
 };
 
 // Grow-only device scratch carved per call.
@@ -112,11 +123,13 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_L2_AHEAD).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
     bool dense_path = true;  // dense column programs for MODE_GROUP_PRIVATE (TGP_NO_DENSE=1 turns them off)
     int l2_ahead = -1;         // L2 prefetch distance in tiles (TGP_L2_AHEAD; -1 = off)
+    bool join_payload = true;  // unique-key join payload arrays (TGP_NO_JOIN_PAYLOAD=1 turns them off)
+    bool hash_presum = true;   // shared pre-aggregation for hash grouping (TGP_NO_HASH_PRESUM=1 turns it off)
     bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
 };

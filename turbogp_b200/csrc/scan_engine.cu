@@ -329,13 +329,17 @@ __device__ __forceinline__ int64_t key_cell(const Plan& P, const GKey& K, const 
 }
 
 // Direct group index: sum over keys of (cell - min) * stride.
+// With a join payload (gpay != kNoPay), the build-side keys' part of the
+// index is gpay and only probe-side keys are read.
+constexpr uint32_t kNoPay = 0xffffffffu;
 template <bool TAIL>
 __device__ __forceinline__ uint32_t group_index(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t rl,
-                                                uint32_t brow) {
-    uint64_t g = 0;
+                                                uint32_t brow, uint32_t gpay = kNoPay) {
+    uint64_t g = gpay != kNoPay ? gpay : 0u;
 #pragma unroll 1
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         const GKey& K = P.gkey[k];
+        if (gpay != kNoPay && K.build_side) continue;
         const int64_t c = key_cell<TAIL>(P, K, stage, r0, rl, brow);
         g += (static_cast<uint64_t>(c) - static_cast<uint64_t>(K.min)) * K.stride;
     }
@@ -462,6 +466,22 @@ __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
 }
 
+// Slot of `key` in the global group hash table (inserted if absent), or null
+// with kErrHashFull raised.
+constexpr uint32_t kSmemProbes = 8;
+__device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, uint64_t key) {
+    uint64_t h = hash_slot(key, P.hlog2);
+    for (uint64_t n = 0; n <= P.hmask; ++n) {
+        unsigned long long* s = P.htab + h * P.hstride;
+        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(s);
+        if (k == kEmpty) k = atomicCAS(s, kEmpty, key);
+        if (k == kEmpty || k == key) return s;
+        h = (h + 1) & P.hmask;
+    }
+    atomicOr(P.err, kErrHashFull);
+    return nullptr;
+}
+
 template <uint32_t MODE, bool ACC128, int NT>
 struct Sink {
     uint32_t ovf;
@@ -486,6 +506,16 @@ struct Sink {
             for (uint32_t i = t; i < P.ngroups * nv1; i += NT) {
                 w[2 * i] = kind_identity(slot_kind(P, i % nv1));
                 w[2 * i + 1] = 0;
+            }
+        } else if (MODE == MODE_GROUP_HASH && P.hsm_slots) {
+            const uint32_t HS = P.hsm_slots;
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
+            uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
+            int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
+            for (uint32_t i = t; i < HS; i += NT) {
+                keys[i] = kEmpty;
+                cnt[i] = 0;
+                for (uint32_t v = 0; v < P.nval; ++v) sums[v * HS + i] = 0;
             }
         }
     }
@@ -512,10 +542,10 @@ struct Sink {
     // One selected (row[, build row]) pair.
     template <bool TAIL>
     __device__ __forceinline__ void row(const Plan& P, uint8_t* extra, const uint8_t* stage, uint64_t r0,
-                                        uint32_t rl, uint32_t brow, uint32_t t) {
+                                        uint32_t rl, uint32_t brow, uint32_t t, uint32_t gpay = kNoPay) {
         const uint32_t nv1 = P.nval + 1;
         if (MODE == MODE_GROUP_PRIVATE) {
-            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
+            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
             long long* w = reinterpret_cast<long long*>(extra);
             if (ACC128) {
                 if (!P.count_by_tile) {
@@ -557,7 +587,7 @@ struct Sink {
                 }
             }
         } else if (MODE == MODE_GROUP_SHARED) {
-            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
+            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
             unsigned long long* w = reinterpret_cast<unsigned long long*>(extra);
             atomicAdd(&w[(g * nv1) * 2], 1ull);
 #pragma unroll 1
@@ -582,7 +612,7 @@ struct Sink {
                 }
             }
         } else if (MODE == MODE_GROUP_GLOBAL) {
-            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow);
+            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
             unsigned long long* a = P.acc + static_cast<uint64_t>(g) * nv1 * 2;
             atomicAdd(a, 1ull);
 #pragma unroll 1
@@ -592,22 +622,33 @@ struct Sink {
             }
         } else if (MODE == MODE_GROUP_HASH) {
             const uint64_t key = group_hash_key<TAIL>(P, stage, r0, rl, brow);
-            uint64_t h = hash_slot(key, P.hlog2);
-            unsigned long long* slot = nullptr;
-            for (uint64_t n = 0; n <= P.hmask; ++n) {
-                unsigned long long* s = P.htab + h * P.hstride;
-                unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(s);
-                if (k == kEmpty) k = atomicCAS(s, kEmpty, key);
-                if (k == kEmpty || k == key) {
-                    slot = s;
-                    break;
+            if (P.hsm_slots) {
+                // This CTA's shared pre-aggregation table absorbs repeated
+                // (hot) keys with native 32-bit shared atomics.
+                const uint32_t HS = P.hsm_slots;
+                unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
+                uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
+                int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
+                uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
+#pragma unroll 1
+                for (uint32_t n = 0; n < kSmemProbes; ++n) {
+                    unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
+                    if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
+                    if (k == kEmpty || k == key) {
+                        atomicAdd(&cnt[h], 1u);
+#pragma unroll 1
+                        for (uint32_t v = 0; v < P.nval; ++v) {
+                            const ValDesc& V = P.val[v];
+                            const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
+                            atomicAdd(&sums[v * HS + h], static_cast<int32_t>(V.kind == VK_COUNT_NZ ? (x != 0) : x));
+                        }
+                        return;
+                    }
+                    h = (h + 1) & (HS - 1);
                 }
-                h = (h + 1) & P.hmask;
             }
-            if (slot == nullptr) {
-                atomicOr(P.err, kErrHashFull);
-                return;
-            }
+            unsigned long long* slot = hash_group_slot(P, key);
+            if (slot == nullptr) return;
             atomicAdd(slot + 1, 1ull);
 #pragma unroll 1
             for (uint32_t v = 0; v < P.nval; ++v) {
@@ -623,7 +664,11 @@ struct Sink {
             bool done = false;
             for (uint64_t n = 0; n <= P.jmask && !done; ++n) {
                 if (!P.jwide) {
-                    done = atomicCAS(P.jtab + h, kEmpty, (rel << 32) | row) == kEmpty;
+                    // A failed CAS returns the slot's entry: an equal key there
+                    // means the build side has duplicate keys (counter word 3).
+                    const unsigned long long old = atomicCAS(P.jtab + h, kEmpty, (rel << 32) | row);
+                    done = old == kEmpty;
+                    if (!done && (old >> 32) == rel) atomicAdd(P.counters + 3, 1ull);
                 } else if (atomicCAS(P.jtab + 2 * h + 1, 0ull, static_cast<unsigned long long>(row) + 1) == 0ull) {
                     P.jtab[2 * h] = rel;
                     done = true;
@@ -670,6 +715,26 @@ struct Sink {
                 a.lo = static_cast<uint64_t>(w[2 * idx]);
                 a.hi = w[2 * idx + 1];
                 if (!acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
+            }
+        } else if (MODE == MODE_GROUP_HASH && P.hsm_slots) {
+            consumer_sync<NT>();
+            const uint32_t HS = P.hsm_slots;
+            const unsigned long long* keys = reinterpret_cast<const unsigned long long*>(extra);
+            const uint32_t* cnt = reinterpret_cast<const uint32_t*>(keys + HS);
+            const int32_t* sums = reinterpret_cast<const int32_t*>(cnt + HS);
+            for (uint32_t i = t; i < HS; i += NT) {
+                const unsigned long long key = keys[i];
+                if (key == kEmpty) continue;
+                unsigned long long* slot = hash_group_slot(P, key);
+                if (slot == nullptr) continue;
+                atomicAdd(slot + 1, static_cast<unsigned long long>(cnt[i]));
+                for (uint32_t v = 0; v < P.nval; ++v) {
+                    const int64_t x = sums[v * HS + i];
+                    I128 a;
+                    a.lo = static_cast<uint64_t>(x);
+                    a.hi = x >> 63;
+                    atomic_add_i128(slot + 2 + 2 * v, a);
+                }
             }
         }
         if (ovf) atomicOr(P.err, kErrRowOverflow);
@@ -826,7 +891,8 @@ __device__ __forceinline__ void load_cells32(const uint8_t* base, uint32_t dtype
 
 template <int NT>
 __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
-                                                   uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
+                                                   uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink,
+                                                   const uint32_t* gin = nullptr) {
     constexpr int R = kTileRows / NT;
     unsigned long long* w = reinterpret_cast<unsigned long long*>(extra);
     // The int64 partials stay below 2^63 in magnitude: flush before this
@@ -840,12 +906,13 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
 
     // Direct group index of each row: sum over keys of (cell - min) * stride,
     // exact in 32 bits because the group count is below 2^31.
+    // With a join payload, gin holds the build-side keys' part.
     uint32_t g[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) g[r] = 0;
+    for (int r = 0; r < R; ++r) g[r] = gin ? gin[r] : 0u;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        if (static_cast<uint32_t>(k) < P.ngkey) {
+        if (static_cast<uint32_t>(k) < P.ngkey && !P.gkey[k].build_side) {
             const GKey& K = P.gkey[k];
             uint32_t x[R];
             load_cells32<R>(stage + K.soff, K.dtype, t, x);
@@ -1133,6 +1200,31 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
 }
 
 // ---------------------------------------------------------------------------
+// Join probe through the payload array (unique build keys, dense key range):
+// pay[key - kmin] is the build-side part of the group index of the one
+// matching build row, or kNoPay. The R lookups of a thread are independent
+// loads, so they are all in flight at once.
+// ---------------------------------------------------------------------------
+template <int R>
+__device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t* stage, uint32_t t, uint32_t m,
+                                                   uint32_t (&g)[R]) {
+    const uint8_t* kb = stage + P.slot[P.jslot].smem_off;
+    const uint32_t kdt = P.slot[P.jslot].dtype;
+    int64_t cell[R];
+    load_cells64<R>(kb, kdt, t, cell);
+    uint32_t hit = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint64_t rel = static_cast<uint64_t>(cell[r]) - static_cast<uint64_t>(P.jkmin);
+        const bool probe = ((m >> r) & 1u) && rel <= P.jkrange;
+        g[r] = probe ? __ldg(P.jpay + rel) : kNoPay;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) hit |= (g[r] != kNoPay ? 1u : 0u) << r;
+    return hit;
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
@@ -1223,6 +1315,26 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t);
         }
     };
+    if constexpr (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL) {
+        if (!TAIL && P.jpay) {
+            uint32_t g[R];
+            const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
+            if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
+                if (P.dense_vec && __reduce_add_sync(kFull, __popc(hit)) >= 8u * R) {
+                    chain_private_tile<NT>(P, extra, stage, t, hit, sink, g);
+                    return;
+                }
+            }
+            const uint8_t* kb = stage + P.slot[P.jslot].smem_off;
+            const uint32_t kdt = P.slot[P.jslot].dtype;
+            for (uint32_t sel = hit; sel; sel &= sel - 1) {
+                const uint32_t rl = R * t + __ffs(sel) - 1;
+                const uint64_t rel = static_cast<uint64_t>(load_cell(kb, kdt, rl)) - static_cast<uint64_t>(P.jkmin);
+                sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t, __ldg(P.jpay + rel));
+            }
+            return;
+        }
+    }
     // Each iteration handles the next selected row of every lane at once, so a
     // sparse selection costs max(rows per lane) iterations, not the total.
     if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
