@@ -339,6 +339,114 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         dist.destroy_process_group()
 
 
+def batch_queries(ctx, fact_dev: dict, dim_host: dict, nq: int, seed: int):
+    """The batching workload's queries: nq prepared queries, each over a prefix
+    view of the resident 60M-row fact table whose size is log-uniform in
+    [10K, 60M] rows, with a template drawn from (selective scan + sum,
+    filtered grouped aggregate, join + grouped aggregate) and random literals
+    (selectivity about 0.1% to 90%). Views share the device columns."""
+    import numpy as np
+    from turbogp_b200 import datagen, workloads
+    from turbogp_b200.engine import col
+    rng = np.random.default_rng(seed)
+    d = ctx.register(dim_host, datagen.DIMENSION_COLTYPES)
+    tj = workloads.join_group_agg()
+    j = d.join_build("key", tj.build_where)
+    fct = {**datagen.LINEITEM_COLTYPES, "fk": "int"}
+    n_all = next(iter(fact_dev.values())).numel()
+    views, pqs, rows, nbytes = {}, [], [], []
+    for _ in range(nq):
+        n = int(min(n_all, round(float(np.exp(rng.uniform(np.log(1e4), np.log(6e7)))))))
+        if n not in views:
+            views[n] = ctx.register_device({k: v[:n] for k, v in fact_dev.items()}, fct)
+        t = views[n]
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            tpl = workloads.selective_scan_sum(day_lo=datagen.DAY0 + int(rng.integers(0, 2000)),
+                                               days=int(rng.integers(30, 526)), disc_lo=int(rng.integers(0, 6)),
+                                               disc_hi=int(rng.integers(5, 11)), qty_lt=int(rng.integers(2, 51)))
+            pqs.append(t.prepare(tpl.aggs, tpl.group_by, tpl.where))
+            nbytes.append(20 * n)   # ship_day, discount_pct, quantity, price_cents
+        elif kind == 1:
+            tpl = workloads.filtered_group_agg(ship_max=datagen.DAY0 + int(rng.integers(3, datagen.NDAYS)))
+            pqs.append(t.prepare(tpl.aggs, tpl.group_by, tpl.where))
+            nbytes.append(26 * n)   # the seven lineitem columns
+        else:
+            pqs.append(t.prepare(tj.aggs, tj.group_by, col("quantity") < int(rng.integers(2, 51)), join=j,
+                                 probe_key="fk"))
+            nbytes.append(20 * n)   # fk, price_cents, discount_pct, quantity
+        rows.append(n)
+    return pqs, rows, nbytes, (d, j, views)
+
+
+def run_batch(args, world: int, rank: int, local: int) -> None:
+    """Batching: 256 queries of uneven sizes (see batch_queries) per step, run
+    as one tgp_batch_submit (persistent launch over a device morsel queue)
+    against the same 256 queries issued one by one (plan, launch, readback
+    per query). value = batched queries/s; plain_qps beside it."""
+    import numpy as np
+    import torch
+    from turbogp_b200 import datagen
+    from turbogp_b200.engine import Context
+    nq = 256
+    ctx = Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    n = args.rows if args.rows != ROWS else 60_000_000
+    host = datagen.fact_fk(n, 1_500_000, 0.8, seed=3 + rank)
+    fact = {k: torch.from_numpy(v).to(f"cuda:{local}") for k, v in host.items()}
+    del host
+    dim = datagen.dimension(1_500_000, seed=2 + rank)
+    pqs, rows, nbytes, keep = batch_queries(ctx, fact, dim, nq, seed=11 + rank)
+    total_rows = sum(rows)
+    steps = args.steps if args.steps != 3000 else 5
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    batch = lambda: ctx.submit(pqs, decode=False).wait()
+    plain = lambda: [q.run(decode=False) for q in pqs]
+    for _ in range(args.warmup):
+        batch()
+        plain()
+    ctx.profile(True)
+    ctx.profile_read()
+    with ClockSampler(local) as clocks:
+        ms_batch = timed(batch, steps)
+    launches, kern_ms = ctx.profile_read()
+    ms_plain = timed(plain, max(1, steps // 2)) / max(1, steps // 2) * steps
+    ctx.profile(False)
+    peak, peak_kind = peak_hbm()
+    achieved = sum(nbytes) / (kern_ms / steps / 1000.0) / 1e9 if kern_ms else None
+    line = {
+        "metric": METRIC, "value": nq * world * steps / (ms_batch / 1000.0), "unit": "queries/s",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms_batch / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded; TPC-H shapes)",
+        "config": {"workload": f"batch of {nq} queries (sizes log-uniform 10K-60M rows over prefix views of a "
+                               f"{n}-row resident table; selective scan+sum / filtered grouped aggregate / "
+                               f"join+grouped aggregate with random literals) per step",
+                   "rows_per_step": total_rows, "l2": "inputs larger than the 126 MB L2"},
+        "plain_qps": nq * steps / (ms_plain / 1000.0), "ms_plain_per_step": ms_plain / steps,
+        "rows_per_s": total_rows * steps / (ms_batch / 1000.0),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None,
+                     "peak_kind": peak_kind, "traffic": None, "kernel_ms_per_step": kern_ms / steps,
+                     "kernel": "batch_kernel (persistent, device morsel queue)"},
+        "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del keep
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -351,11 +459,14 @@ def main() -> None:
     ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="selective_scan_sum",
-                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group"])
+                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     world, rank, local = dist_setup(args.gpus)
+    if args.workload == "batch":
+        run_batch(args, world, rank, local)
+        return
     if args.workload != "selective_scan_sum":
         run_workload(args, world, rank, local)
         return

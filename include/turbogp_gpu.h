@@ -54,7 +54,8 @@ typedef enum tgp_status {
     TGP_TIMEOUT = 4,       /* a bounded device wait gave up; the context stays usable */
     TGP_DEVICE_ERROR = 5,  /* CUDA runtime error */
     TGP_NOT_FOUND = 6,     /* unknown table / join / ticket id */
-    TGP_CAPACITY = 7       /* caller-provided output buffer too small; required size reported */
+    TGP_CAPACITY = 7,      /* caller-provided output buffer too small; required size reported */
+    TGP_PENDING = 8        /* tgp_batch_poll: the batch has not finished yet */
 } tgp_status;
 
 /* Human-readable name of a status code (static storage). */
@@ -425,6 +426,40 @@ TGP_API int tgp_join_probe_pairs(tgp_ctx* ctx, tgp_join_id join, tgp_table_id pr
                          uint32_t probe_key_column, const tgp_pred_node* pred, uint32_t npred,
                          uint32_t* probe_rows, uint32_t* build_rows, uint64_t cap,
                          uint64_t* npairs);
+
+/* ------------------------------------------------------------------------ */
+/* Batches: many queries, one persistent launch                              */
+/* ------------------------------------------------------------------------ */
+
+/* One query of a batch and its outputs (the arguments of tgp_execute). The
+ * caller keeps `query` (and what it points to) and the output buffers alive
+ * until tgp_batch_poll reports the batch done; `result` and `status` are
+ * written then. */
+typedef struct tgp_batch_item {
+    const tgp_query* query;
+    uint64_t* keys_out;
+    tgp_agg_value* vals_out;
+    uint64_t group_cap;
+    tgp_query_result result;
+    int32_t status;            /* tgp_status of this query */
+    uint32_t _pad;
+} tgp_batch_item;
+
+typedef uint64_t tgp_batch_id;
+
+/* Plans every query and launches them without waiting: the direct-indexed and
+ * scalar aggregates run in one persistent kernel per CTA shape whose blocks
+ * take (query, tile range) morsels from a device work counter, with one
+ * upload of all plans and one readback of all result blocks; other queries
+ * (hash grouping, ...) run one by one inside this call. This is the batched
+ * counterpart of issuing tgp_execute n times. Per-query planning errors land
+ * in items[i].status; the call itself fails only when nothing can run. */
+TGP_API int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_id* out);
+
+/* Completes a batch: with wait != 0 blocks until its GPU work is done;
+ * otherwise returns TGP_PENDING if it is still running. On completion fills
+ * every item's result and status, releases the batch and returns TGP_OK. */
+TGP_API int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id batch, int wait);
 
 /* ------------------------------------------------------------------------ */
 /* Allocation-free aggregate                                                 */

@@ -290,3 +290,55 @@ def test_hash_grouping_hot_keys_and_device_format(ctx):
         o = oracle.aggregate(h, None, aggs, gb, where)
         same_query(g, o)
     t.drop()
+
+
+def test_batch_persistent_launch_matches_single_queries(ctx):
+    """A batch of queries of uneven sizes and all three templates (scan +
+    scalar sum, grouped Q1 shape, join + group) through the persistent
+    launch, plus hash-grouped and empty queries that run alone: each result
+    equals the oracle's, whatever morsels the CTAs took."""
+    rng = np.random.default_rng(12)
+    sizes = [0, 1, 2047, 2049, 70_001, 1_000_003, 3_000_000]
+    tabs = {n: datagen.lineitem(n, seed=100 + i) for i, n in enumerate(sizes)}
+    regs = {n: ctx.register(h, CT) for n, h in tabs.items()}
+    dim = datagen.dimension(30_000, seed=5)
+    fact = datagen.fact_fk(500_000, 30_000, 0.8, seed=6)
+    fct = {**CT, "fk": "int"}
+    d = ctx.register(dim, datagen.DIMENSION_COLTYPES)
+    f = ctx.register(fact, fct)
+    tj = workloads.join_group_agg()
+    j = d.join_build("key", tj.build_where)
+    pqs, expect = [], []
+    for k in range(40):
+        n = sizes[k % len(sizes)]
+        kind = k % 4
+        if kind == 0:
+            tpl = workloads.selective_scan_sum(day_lo=datagen.DAY0 + int(rng.integers(0, 2000)),
+                                               days=int(rng.integers(1, 500)), qty_lt=int(rng.integers(1, 51)))
+        elif kind == 1:
+            tpl = workloads.filtered_group_agg(ship_max=datagen.DAY0 + int(rng.integers(0, datagen.NDAYS)))
+        elif kind == 2:
+            tpl = None
+        else:
+            tpl = workloads.filtered_group_agg()
+            tpl.group_by = ("price_cents",)                       # hash grouping: runs alone
+        if tpl is None:
+            where = col("quantity") < int(rng.integers(1, 51))
+            pqs.append(f.prepare(tj.aggs, tj.group_by, where, join=j, probe_key="fk"))
+            expect.append(oracle.aggregate(fact, fct, tj.aggs, tj.group_by, where,
+                                           build=(dim, datagen.DIMENSION_COLTYPES, "key", tj.build_where),
+                                           probe_key="fk"))
+            continue
+        pqs.append(regs[n].prepare(tpl.aggs, tpl.group_by, tpl.where, group_cap=1 << 20))
+        expect.append(oracle.aggregate(tabs[n], CT, tpl.aggs, tpl.group_by, tpl.where))
+    outs = ctx.submit(pqs).wait()
+    assert len(outs) == len(pqs)
+    for o, e in zip(outs, expect):
+        same_query(o, e)
+    # Polling form, and the same queries again (plans and buffers reused).
+    h = ctx.submit(pqs[:9])
+    while not h.poll():
+        pass
+    for o, e in zip(h.wait(), expect[:9]):
+        same_query(o, e)
+    j.drop()

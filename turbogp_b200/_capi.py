@@ -13,7 +13,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libturbogp_b200.so"
 
 # --- status codes ----------------------------------------------------------
-OK, INVALID_ARG, OOM, UNSUPPORTED, TIMEOUT, DEVICE_ERROR, NOT_FOUND, CAPACITY = range(8)
+OK, INVALID_ARG, OOM, UNSUPPORTED, TIMEOUT, DEVICE_ERROR, NOT_FOUND, CAPACITY, PENDING = range(9)
 
 # --- enums -------------------------------------------------------------------
 DT_U8, DT_I32, DT_I64, DT_U64, DT_F64 = 1, 2, 3, 4, 5
@@ -78,6 +78,13 @@ class QueryResult(C.Structure):
     ]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [
+        ("query", C.POINTER(Query)), ("keys_out", C.c_void_p), ("vals_out", C.POINTER(AggValue)),
+        ("group_cap", C.c_uint64), ("result", QueryResult), ("status", C.c_int32), ("_pad", C.c_uint32),
+    ]
+
+
 class KernelParams(C.Structure):
     _fields_ = [
         ("target_u64", C.c_uint64), ("low_u64", C.c_uint64), ("high_u64", C.c_uint64),
@@ -137,6 +144,8 @@ PROTOTYPES = [
     ("tgp_join_probe_pairs", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.c_void_p, C.c_void_p,
       C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("tgp_batch_submit", C.c_int, [C.c_void_p, C.POINTER(BatchItem), C.c_uint32, C.POINTER(C.c_uint64)]),
+    ("tgp_batch_poll", C.c_int, [C.c_void_p, C.c_uint64, C.c_int]),
     ("tgp_aggregate_noalloc", C.c_int,
      [C.c_int, C.c_void_p, C.POINTER(ColumnDesc), C.c_uint32, C.c_uint64, C.POINTER(PredNode), C.c_uint32,
       C.POINTER(KeyDomain), C.c_uint32, C.POINTER(Agg), C.c_uint32, C.POINTER(AggValue), C.c_uint64,
@@ -176,4 +185,4 @@ class TgpError(RuntimeError):
 
 STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", UNSUPPORTED: "UNSUPPORTED",
                 TIMEOUT: "TIMEOUT", DEVICE_ERROR: "DEVICE_ERROR", NOT_FOUND: "NOT_FOUND",
-                CAPACITY: "CAPACITY"}
+                CAPACITY: "CAPACITY", PENDING: "PENDING"}

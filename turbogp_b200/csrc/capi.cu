@@ -10,6 +10,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "runtime.hpp"
@@ -304,8 +305,9 @@ struct Builder {
     std::vector<int> col2slot;
     uint64_t max_abs_val = 0;       // max |per-row value| over all values (saturating)
     bool unbounded = false;         // some value may exceed 2^62 in magnitude
+    size_t static_smem = 0;         // static shared bytes of the kernel the plan is sized for
 
-    Builder(tgp_ctx* c, const Table* t) : ctx(c), T(t) {
+    Builder(tgp_ctx* c, const Table* t) : ctx(c), T(t), static_smem(scan_kernel_static_smem()) {
         std::memset(&P, 0, sizeof(P));
         col2slot.assign(t->cols.size(), -1);
         P.nrows = t->rows;
@@ -654,8 +656,7 @@ void fill_value(const AggMap& m, const unsigned long long* slot /* [nv1][2] */, 
 }
 
 // Chooses shared-memory stages for a plan given per-mode scratch bytes.
-int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes) {
-    const size_t static_smem = scan_kernel_static_smem();
+int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = scan_kernel_static_smem()) {
     const size_t budget = ctx->max_dyn_smem > static_smem ? ctx->max_dyn_smem - static_smem : 0;
     size_t stage = P.stage_bytes;
     if (stage == 0) {
@@ -750,6 +751,9 @@ void free_join(tgp_ctx* ctx, JoinTable& J) {
 
 }  // namespace
 
+// Releases a batch record (defined with the batch entry points).
+extern "C" void tgp_batch_free_rec(tgp_ctx* ctx, void* rec);
+
 // ==========================================================================
 // C ABI
 // ==========================================================================
@@ -765,6 +769,7 @@ const char* tgp_status_string(int s) {
         case TGP_DEVICE_ERROR: return "DEVICE_ERROR";
         case TGP_NOT_FOUND: return "NOT_FOUND";
         case TGP_CAPACITY: return "CAPACITY";
+        case TGP_PENDING: return "PENDING";
         default: return "UNKNOWN";
     }
 }
@@ -809,6 +814,7 @@ int tgp_init(tgp_ctx** out, int device) {
     cudaGetLastError();
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_BATCH_MORSEL_TILES")) ctx->morsel_tiles = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_HASH_PRESUM")) ctx->hash_presum = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_L2_AHEAD")) ctx->l2_ahead = std::min(64, std::max(0, std::atoi(e)));
@@ -833,7 +839,11 @@ int tgp_shutdown(tgp_ctx* ctx) {
         free_join(ctx, *J);
         delete J;
     }
+    for (auto& kv : ctx->batches) tgp_batch_free_rec(ctx, kv.second);
+    ctx->batches.clear();
     cudaStreamSynchronize(ctx->stream);
+    for (auto& pb : ctx->pinned_pool) cudaFreeHost(pb.p);
+    ctx->pinned_pool.clear();
     if (ctx->arena.base) cudaFree(ctx->arena.base);
     if (ctx->kin) cudaFree(ctx->kin);
     if (ctx->hpin) cudaFreeHost(ctx->hpin);
@@ -1120,14 +1130,46 @@ static void attach_join(Plan& P, const JoinTable& J, int key_slot) {
     if (J.empty_range) P.jkmin = 0;
 }
 
-int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
-                tgp_query_result* result) {
-    if (!ctx || !q || !result) return fail(ctx, TGP_INVALID_ARG, "null argument");
-    std::memset(result, 0, sizeof(*result));
-    const Table* T;
-    TGP_TRY(get_table(ctx, q->table, &T));
-    Builder b(ctx, T);
+// A planned query: the lowered plan and what decoding its result block needs.
+struct QueryState {
+    const tgp_query* q = nullptr;
+    const Table* T = nullptr;
     JoinTable* J = nullptr;
+    std::unique_ptr<Builder> b;
+    std::vector<AggMap> amap;
+    uint32_t nv1 = 1;
+    std::vector<uint64_t> dom;
+    std::vector<int64_t> kmin;
+    std::vector<uint32_t> bits;
+    unsigned __int128 D = 1;
+    uint32_t total_bits = 0;
+    uint32_t mode = MODE_GROUP_PRIVATE;
+    bool acc128 = false;
+    uint64_t ngroups_direct = 1;
+    size_t extra = 0;     // per-mode shared scratch bytes
+    uint64_t hcap = 0;    // hash table slots (MODE_GROUP_HASH)
+    uint64_t acc_words() const { return mode == MODE_GROUP_HASH ? 0 : ngroups_direct * nv1 * 2; }
+    uint64_t block_words() const { return 6 + acc_words(); }  // [counters 4][error 2][accumulators]
+    bool has_minmax() const {
+        for (uint32_t v = 0; v < b->P.nval; ++v)
+            if (b->P.val[v].kind == VK_MIN || b->P.val[v].kind == VK_MAX) return true;
+        return false;
+    }
+};
+
+// Lowers a query (predicate, aggregates, keys, join payload) and chooses its
+// mode and shared-memory layout for a kernel with `static_smem` static bytes.
+// Result pointers (counters, err, acc, htab) are left for the caller.
+static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem) {
+    if (!ctx || !q) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    qs.q = q;
+    TGP_TRY(get_table(ctx, q->table, &qs.T));
+    const Table* T = qs.T;
+    qs.b.reset(new Builder(ctx, T));
+    Builder& b = *qs.b;
+    b.static_smem = static_smem;
+    JoinTable*& J = qs.J;
+    J = nullptr;
     if (q->join) {
         TGP_TRY(join_lookup(ctx, q->join, &J));
         TGP_TRY(get_table(ctx, J->build_table, &b.B));
@@ -1142,19 +1184,24 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         TGP_TRY(b.slot_of(q->probe_key_column, &ks));
         attach_join(b.P, *J, ks);
     }
-    std::vector<AggMap> amap;
+    std::vector<AggMap>& amap = qs.amap;
     TGP_TRY(lower_aggs(b, q->aggs, q->nagg, &amap));
     Plan& P = b.P;
-    const uint32_t nv1 = P.nval + 1;
+    const uint32_t nv1 = qs.nv1 = P.nval + 1;
 
     // Group keys.
     if (q->ngroup > static_cast<uint32_t>(kMaxGroupKeys)) return fail(ctx, TGP_UNSUPPORTED, "more than 4 group keys");
     if (q->ngroup && !q->group) return fail(ctx, TGP_INVALID_ARG, "null group key list");
-    std::vector<uint64_t> dom(q->ngroup);
-    std::vector<int64_t> kmin(q->ngroup);
-    unsigned __int128 D = 1;
-    uint32_t total_bits = 0;
-    std::vector<uint32_t> bits(q->ngroup);
+    std::vector<uint64_t>& dom = qs.dom;
+    std::vector<int64_t>& kmin = qs.kmin;
+    std::vector<uint32_t>& bits = qs.bits;
+    dom.assign(q->ngroup, 0);
+    kmin.assign(q->ngroup, 0);
+    bits.assign(q->ngroup, 0);
+    unsigned __int128& D = qs.D;
+    D = 1;
+    uint32_t& total_bits = qs.total_bits;
+    total_bits = 0;
     for (uint32_t k = 0; k < q->ngroup; ++k) {
         const tgp_group_key& gk = q->group[k];
         const Table* S = gk.side == TGP_SIDE_BUILD ? b.B : T;
@@ -1195,10 +1242,13 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     for (uint32_t v = 0; pay_ok && v < P.nval; ++v)
         for (uint32_t f = 0; f < P.val[v].nf; ++f) pay_ok = pay_ok && !P.val[v].f[f].build_side;
 
-    uint32_t mode;
-    bool acc128 = false;
-    uint64_t ngroups_direct = 1;
-    size_t extra = 0;
+    uint32_t& mode = qs.mode;
+    bool& acc128 = qs.acc128;
+    acc128 = false;
+    uint64_t& ngroups_direct = qs.ngroups_direct;
+    ngroups_direct = 1;
+    size_t& extra = qs.extra;
+    extra = 0;
     const bool join = J != nullptr;
     // A scalar aggregate is the direct-indexed case with one group (D = 1).
     if (D <= kDirectMaxGroups) {
@@ -1212,7 +1262,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         acc128 = b.unbounded;
         const size_t per_thread = static_cast<size_t>(ngroups_direct) * nv1 * 8 * (acc128 ? 2 : 1);
         const size_t shared_tab = static_cast<size_t>(ngroups_direct) * nv1 * 16;
-        const size_t budget = ctx->max_dyn_smem - scan_kernel_static_smem() - kBarrierBytes;
+        const size_t budget = ctx->max_dyn_smem - static_smem - kBarrierBytes;
         // Per-thread private accumulators: 512 threads when two stages still
         // fit beside them, else 256 threads (twice the rows per thread).
         uint32_t nt = 0;
@@ -1285,7 +1335,8 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     }
 
     // Hash table sizing: twice the bound on distinct groups.
-    uint64_t hcap = 0;
+    uint64_t& hcap = qs.hcap;
+    hcap = 0;
     if (mode == MODE_GROUP_HASH) {
         const unsigned __int128 est = std::min<unsigned __int128>(D, static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
                                                                           (join ? 4 : 1));
@@ -1301,7 +1352,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             presum = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
         const uint32_t HS = 4096;
         const size_t bytes = static_cast<size_t>(HS) * (12 + 4 * P.nval);
-        const size_t budget = ctx->max_dyn_smem - scan_kernel_static_smem() - kBarrierBytes;
+        const size_t budget = ctx->max_dyn_smem - static_smem - kBarrierBytes;
         if (presum && bytes + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             P.hsm_slots = HS;
             P.hsm_log2 = log2u(HS);
@@ -1309,14 +1360,82 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         }
     }
 
+    return TGP_OK;
+}
+
+// Fills the caller's outputs of a direct-indexed / scalar query from a host
+// copy of its result block.
+static int decode_direct(tgp_ctx* ctx, const QueryState& qs, const unsigned long long* hb, uint64_t* keys_out,
+                         tgp_agg_value* vals_out, uint64_t group_cap, tgp_query_result* result) {
+    const tgp_query* q = qs.q;
+    const Plan& P = qs.b->P;
+    const uint32_t nv1 = qs.nv1;
+    const uint64_t ngroups_direct = qs.ngroups_direct;
+    const std::vector<uint64_t>& dom = qs.dom;
+    const std::vector<int64_t>& kmin = qs.kmin;
+    const std::vector<AggMap>& amap = qs.amap;
+    const uint32_t nagg = q->nagg;
+    const uint32_t err = static_cast<uint32_t>(hb[4] & 0xffffffffull);
+    TGP_TRY(check_kernel_err(ctx, err));
+    result->rows_scanned = qs.T->rows;
+    result->rows_selected = hb[0];
+    result->flags = (err & kErrRowOverflow) ? TGP_RESULT_ROW_OVERFLOW : 0u;
+    const unsigned long long* accv = hb + 6;
+        // Direct / scalar: emit groups with a nonzero row count in index order
+        // (index order is ascending lexicographic key order).
+        std::vector<uint64_t> present;
+        if (q->ngroup == 0) {
+            present.push_back(0);
+        } else {
+            for (uint64_t g = 0; g < ngroups_direct; ++g)
+                if (accv[g * nv1 * 2] != 0) present.push_back(g);
+        }
+        result->ngroups = present.size();
+        if (present.size() > group_cap) return fail(ctx, TGP_CAPACITY, "group buffer too small");
+        for (size_t i = 0; i < present.size(); ++i) {
+            const uint64_t g = present[i];
+            if (keys_out) {
+                for (uint32_t k = 0; k < q->ngroup; ++k) {
+                    const uint64_t digit = (g / P.gkey[k].stride) % dom[k];
+                    keys_out[i * q->ngroup + k] = static_cast<uint64_t>(kmin[k]) + digit;
+                }
+            }
+            if (vals_out)
+                for (uint32_t a = 0; a < nagg; ++a) fill_value(amap[a], accv + g * nv1 * 2, P, &vals_out[i * nagg + a]);
+        }
+        return TGP_OK;
+    }
+
+int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
+                tgp_query_result* result) {
+    if (!ctx || !q || !result) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    std::memset(result, 0, sizeof(*result));
+    QueryState qs;
+    TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem()));
+    Builder& b = *qs.b;
+    Plan& P = b.P;
+    const Table* T = qs.T;
+    const uint32_t mode = qs.mode;
+    const bool acc128 = qs.acc128;
+    const uint64_t ngroups_direct = qs.ngroups_direct;
+    const size_t extra = qs.extra;
+    const uint64_t hcap = qs.hcap;
+    const uint32_t nv1 = qs.nv1;
+    const std::vector<uint32_t>& bits = qs.bits;
+    const std::vector<int64_t>& kmin = qs.kmin;
+    const std::vector<AggMap>& amap = qs.amap;
+    const unsigned __int128 D = qs.D;
+    const uint32_t total_bits = qs.total_bits;
+    (void)nv1;
+
     // Scratch: accumulators (direct/scalar) or hash table, counters, error word.
-    const uint64_t acc_words = (mode == MODE_GROUP_HASH) ? 0 : ngroups_direct * nv1 * 2;
+    const uint64_t acc_words = qs.acc_words();
     const uint64_t htab_words = hcap * P.hstride;
     Carve cv;
     TGP_TRY(arena_reserve(ctx, acc_words * 8 + htab_words * 8 + 1024, &cv));
     // One result block [counters: 4 words][error word: 2 words][accumulators],
     // cleared with one memset and read back with one copy.
-    const uint64_t block_words = 6 + acc_words;
+    const uint64_t block_words = qs.block_words();
     unsigned long long* block = cv.take<unsigned long long>(block_words);
     P.counters = block;
     P.err = reinterpret_cast<uint32_t*>(block + 4);
@@ -1372,7 +1491,6 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     const unsigned long long* hb = reinterpret_cast<const unsigned long long*>(ctx->hpin);
     unsigned long long counters[4] = {hb[0], hb[1], hb[2], hb[3]};
     const uint32_t err = static_cast<uint32_t>(hb[4] & 0xffffffffull);
-    std::vector<unsigned long long> accv(hb + 6, hb + 6 + acc_words);
     TGP_TRY(check_kernel_err(ctx, err));
 
     result->rows_scanned = T->rows;
@@ -1380,31 +1498,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     result->flags = (err & kErrRowOverflow) ? TGP_RESULT_ROW_OVERFLOW : 0u;
     const uint32_t nagg = q->nagg;
 
-    if (mode != MODE_GROUP_HASH) {
-        // Direct / scalar: emit groups with a nonzero row count in index order
-        // (index order is ascending lexicographic key order).
-        std::vector<uint64_t> present;
-        if (q->ngroup == 0) {
-            present.push_back(0);
-        } else {
-            for (uint64_t g = 0; g < ngroups_direct; ++g)
-                if (accv[g * nv1 * 2] != 0) present.push_back(g);
-        }
-        result->ngroups = present.size();
-        if (present.size() > group_cap) return fail(ctx, TGP_CAPACITY, "group buffer too small");
-        for (size_t i = 0; i < present.size(); ++i) {
-            const uint64_t g = present[i];
-            if (keys_out) {
-                for (uint32_t k = 0; k < q->ngroup; ++k) {
-                    const uint64_t digit = (g / P.gkey[k].stride) % dom[k];
-                    keys_out[i * q->ngroup + k] = static_cast<uint64_t>(kmin[k]) + digit;
-                }
-            }
-            if (vals_out)
-                for (uint32_t a = 0; a < nagg; ++a) fill_value(amap[a], &accv[g * nv1 * 2], P, &vals_out[i * nagg + a]);
-        }
-        return TGP_OK;
-    }
+    if (mode != MODE_GROUP_HASH) return decode_direct(ctx, qs, hb, keys_out, vals_out, group_cap, result);
 
     // Hash groups: gather occupied slots, sort by key on the host.
     // Counter word 2 counts the gathered slots.
@@ -1488,6 +1582,235 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             for (uint32_t a = 0; a < nagg; ++a) fill_value(amap[a], tmp.data(), P, &vals_out[i * nagg + a]);
         }
     }
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Batches
+// --------------------------------------------------------------------------
+static uint8_t* pinned_acquire(tgp_ctx* ctx, size_t bytes) {
+    for (auto& b : ctx->pinned_pool)
+        if (!b.busy && b.cap >= bytes) {
+            b.busy = true;
+            return b.p;
+        }
+    void* p = nullptr;
+    const size_t cap = std::max<size_t>(bytes, 1 << 20);
+    if (cudaMallocHost(&p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    ctx->pinned_pool.push_back({static_cast<uint8_t*>(p), cap, true});
+    return static_cast<uint8_t*>(p);
+}
+
+static void pinned_release(tgp_ctx* ctx, uint8_t* p) {
+    for (auto& b : ctx->pinned_pool)
+        if (b.p == p) b.busy = false;
+}
+
+struct BatchRec {
+    tgp_batch_item* items = nullptr;
+    uint32_t n = 0;
+    std::vector<QueryState> qs;
+    std::vector<uint8_t> batched;     // item runs in the persistent launch
+    std::vector<size_t> block_off;    // its result block's byte offset in the readback area
+    uint8_t* dev = nullptr;
+    uint8_t* host = nullptr;
+    size_t readback_off = 0;          // host offset of the readback area
+    cudaEvent_t done = nullptr;
+};
+
+void tgp_batch_free_rec(tgp_ctx* ctx, void* r) {
+    BatchRec* B = static_cast<BatchRec*>(r);
+    if (!B) return;
+    dev_free(ctx, B->dev);
+    if (B->host) pinned_release(ctx, B->host);
+    if (B->done) cudaEventDestroy(B->done);
+    delete B;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
+
+int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_id* out) {
+    if (!ctx || !out || (n && !items)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    std::unique_ptr<BatchRec> B(new BatchRec());
+    B->items = items;
+    B->n = n;
+    B->qs.resize(n);
+    B->batched.assign(n, 0);
+    B->block_off.assign(n, 0);
+    const size_t bstatic = batch_kernel_static_smem();
+    // 1. Plan; queries the persistent kernel does not take run now, alone.
+    struct Class {
+        bool acc128;
+        uint32_t nt;
+        size_t smem = 0;
+        std::vector<uint32_t> q;
+        int grid = 0;
+        std::vector<Morsel> morsels;
+    };
+    std::vector<Class> classes;
+    std::vector<uint32_t> plan_index(n, 0);
+    uint32_t nplans = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        tgp_batch_item& it = items[i];
+        std::memset(&it.result, 0, sizeof(it.result));
+        it.status = TGP_OK;
+        QueryState& qs = B->qs[i];
+        int st = plan_query(ctx, it.query, qs, bstatic);
+        bool take = st == TGP_OK && qs.mode == MODE_GROUP_PRIVATE;
+        if (take) {
+            qs.b->P.shape = 0;
+            take = size_smem(ctx, qs.b->P, qs.extra, bstatic) == TGP_OK;
+        }
+        if (!take) {
+            if (st == TGP_OK) st = tgp_execute(ctx, it.query, it.keys_out, it.vals_out, it.group_cap, &it.result);
+            it.status = st;
+            continue;
+        }
+        B->batched[i] = 1;
+        plan_index[i] = nplans++;
+        const Plan& P = qs.b->P;
+        Class* c = nullptr;
+        for (auto& k : classes)
+            if (k.acc128 == qs.acc128 && k.nt == P.nthreads) c = &k;
+        if (!c) {
+            classes.push_back(Class{qs.acc128, P.nthreads});
+            c = &classes.back();
+        }
+        c->smem = std::max<size_t>(c->smem, P.smem_bytes);
+        c->q.push_back(i);
+    }
+    if (nplans == 0) {
+        const uint64_t id = ctx->next_id++;
+        ctx->batches.emplace(id, B.release());
+        *out = id;
+        return TGP_OK;
+    }
+    // 2. Morsels: a query of T tiles becomes min(grid, ceil(T / morsel_tiles)) ranges;
+    // each class's morsels are handed out largest first.
+    for (auto& c : classes) {
+        const int occ = batch_occupancy(c.acc128, static_cast<int>(c.nt), c.smem);
+        if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "batch kernel cannot be resident with this shared memory");
+        c.grid = ctx->sms * occ;
+        for (uint32_t i : c.q) {
+            const uint64_t T = (B->qs[i].b->P.nrows + kTileRows - 1) / kTileRows;
+            if (T == 0) continue;
+            const uint64_t per = static_cast<uint64_t>(ctx->morsel_tiles);
+            const uint64_t nm = std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(c.grid), (T + per - 1) / per));
+            const uint64_t size = (T + nm - 1) / nm;
+            for (uint64_t b0 = 0; b0 < T; b0 += size)
+                c.morsels.push_back(Morsel{plan_index[i], 0, b0, std::min(T, b0 + size)});
+        }
+        std::stable_sort(c.morsels.begin(), c.morsels.end(), [](const Morsel& a, const Morsel& b) {
+            return a.tile_end - a.tile_begin > b.tile_end - b.tile_begin;
+        });
+    }
+    // 3. One device region: [plans][morsels per class][counters][result blocks].
+    size_t off = align256(static_cast<size_t>(nplans) * sizeof(Plan));
+    std::vector<size_t> morsel_off(classes.size());
+    for (size_t k = 0; k < classes.size(); ++k) {
+        morsel_off[k] = off;
+        off = align256(off + classes[k].morsels.size() * sizeof(Morsel));
+    }
+    const size_t counter_off = off;
+    off = align256(off + classes.size() * 4);
+    const size_t blocks_off = off;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!B->batched[i]) continue;
+        B->block_off[i] = off - blocks_off;
+        off = align256(off + B->qs[i].block_words() * 8);
+    }
+    const size_t total = off, blocks_bytes = total - blocks_off;
+    TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&B->dev), total, "batch allocation failed"));
+    B->readback_off = align256(total);
+    B->host = pinned_acquire(ctx, B->readback_off + blocks_bytes);
+    if (!B->host) {
+        dev_free(ctx, B->dev);
+        B->dev = nullptr;
+        return fail(ctx, TGP_OOM, "pinned batch staging allocation failed");
+    }
+    uint8_t* h = B->host;
+    std::memset(h, 0, total);
+    Plan* hplans = reinterpret_cast<Plan*>(h);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!B->batched[i]) continue;
+        Plan& P = B->qs[i].b->P;
+        unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + B->block_off[i]);
+        P.counters = blk;
+        P.err = reinterpret_cast<uint32_t*>(blk + 4);
+        P.acc = blk + 6;
+        if (B->qs[i].has_minmax()) {
+            std::vector<unsigned long long> img;
+            init_acc_image(P, B->qs[i].ngroups_direct, &img);
+            std::memcpy(h + blocks_off + B->block_off[i] + 48, img.data(), img.size() * 8);
+        }
+        hplans[plan_index[i]] = P;
+    }
+    for (size_t k = 0; k < classes.size(); ++k)
+        if (!classes[k].morsels.empty())
+            std::memcpy(h + morsel_off[k], classes[k].morsels.data(), classes[k].morsels.size() * sizeof(Morsel));
+    // 4. One upload, the persistent launches, one readback.
+    TGP_CUDA(cudaMemcpyAsync(B->dev, h, total, cudaMemcpyHostToDevice, ctx->stream));
+    for (size_t k = 0; k < classes.size(); ++k) {
+        const Class& c = classes[k];
+        if (c.morsels.empty()) continue;
+        BatchDesc D;
+        std::memset(&D, 0, sizeof(D));
+        D.plans = reinterpret_cast<const Plan*>(B->dev);
+        D.morsels = reinterpret_cast<const Morsel*>(B->dev + morsel_off[k]);
+        D.nmorsels = static_cast<uint32_t>(c.morsels.size());
+        D.next = reinterpret_cast<unsigned int*>(B->dev + counter_off) + k;
+        const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.grid), c.morsels.size()));
+        std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+        if (ctx->profile) {
+            if (ctx->prof_used == ctx->prof_events.size()) {
+                std::pair<cudaEvent_t, cudaEvent_t> pe;
+                TGP_CUDA(cudaEventCreate(&pe.first));
+                TGP_CUDA(cudaEventCreate(&pe.second));
+                ctx->prof_events.push_back(pe);
+            }
+            ev = &ctx->prof_events[ctx->prof_used++];
+            TGP_CUDA(cudaEventRecord(ev->first, ctx->stream));
+        }
+        const cudaError_t e = launch_batch(D, c.acc128, static_cast<int>(c.nt), grid, c.smem, ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("batch launch: ") + cudaGetErrorString(e));
+        if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
+    }
+    TGP_CUDA(cudaMemcpyAsync(h + B->readback_off, B->dev + blocks_off, blocks_bytes, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TGP_CUDA(cudaEventCreateWithFlags(&B->done, cudaEventDisableTiming));
+    TGP_CUDA(cudaEventRecord(B->done, ctx->stream));
+    const uint64_t id = ctx->next_id++;
+    ctx->batches.emplace(id, B.release());
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id id, int wait) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->batches.find(id);
+    if (it == ctx->batches.end()) return fail(ctx, TGP_NOT_FOUND, "unknown batch id");
+    BatchRec* B = static_cast<BatchRec*>(it->second);
+    if (B->done) {
+        if (!wait) {
+            const cudaError_t q = cudaEventQuery(B->done);
+            if (q == cudaErrorNotReady) return TGP_PENDING;
+            if (q != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("batch: ") + cudaGetErrorString(q));
+        } else if (cudaEventSynchronize(B->done) != cudaSuccess) {
+            return fail(ctx, TGP_DEVICE_ERROR, "batch synchronization failed");
+        }
+    }
+    for (uint32_t i = 0; i < B->n; ++i) {
+        if (!B->batched[i]) continue;
+        tgp_batch_item& itm = B->items[i];
+        const unsigned long long* hb =
+            reinterpret_cast<const unsigned long long*>(B->host + B->readback_off + B->block_off[i]);
+        itm.status = decode_direct(ctx, B->qs[i], hb, itm.keys_out, itm.vals_out, itm.group_cap, &itm.result);
+    }
+    tgp_batch_free_rec(ctx, B);
+    ctx->batches.erase(it);
     return TGP_OK;
 }
 

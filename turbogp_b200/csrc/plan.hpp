@@ -141,7 +141,7 @@ struct GKey {
     uint64_t stride;      // direct modes: multiplier of (cell - min) in the group index
 };
 
-struct Plan {
+struct alignas(16) Plan {
     uint64_t nrows;
     uint32_t nslots;
     uint32_t stage_bytes;   // bytes of one stage (all slots of one tile)
@@ -210,6 +210,7 @@ struct Plan {
     uint32_t* err;                  // kErr* bits
     unsigned long long* out_pairs;  // MODE_JOIN_PAIRS: (probe_row << 32) | build_row
     uint64_t out_cap;
+    uint64_t _pad_end;              // sizeof(Plan) is a multiple of 16
 };
 
 // Build-side group keys folded into a join payload array.
@@ -275,6 +276,26 @@ struct HashFormat {
     uint8_t func[kMaxFormatAggs];   // tgp_agg_func
     int8_t val[kMaxFormatAggs];     // value index, -1 = COUNT(*)
     uint8_t kind[kMaxFormatAggs];   // VK_* of that value
+};
+
+static_assert(sizeof(Plan) % 16 == 0, "plans are copied in 16-byte words");
+
+// A range of one query's tiles, processed by one CTA of a batch launch.
+struct Morsel {
+    uint32_t query;
+    uint32_t _pad;
+    uint64_t tile_begin;
+    uint64_t tile_end;
+};
+
+// A persistent batch launch: the plans of its queries (each with its own
+// result pointers), the morsels and the device work counter.
+struct BatchDesc {
+    const Plan* plans;
+    const Morsel* morsels;
+    uint32_t nmorsels;
+    uint32_t _pad;
+    unsigned int* next;
 };
 
 // Multiplicative hash of a relative key into a power-of-two table.

@@ -25,6 +25,9 @@ int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t
 // dtypes and value program, or 0 (the interpreted dense program runs).
 uint32_t dense_shape_of(const Plan& P);
 size_t scan_kernel_static_smem();
+size_t batch_kernel_static_smem();
+int batch_occupancy(bool acc128, int nt, size_t dyn_smem);
+cudaError_t launch_batch(const BatchDesc& B, bool acc128, int nt, int grid, size_t dyn_smem, cudaStream_t st);
 cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
                                  int sms, cudaStream_t st);
 cudaError_t tile_prefix(const uint32_t* counts, unsigned long long* out, uint64_t n, void* tmp,
@@ -117,13 +120,22 @@ struct tgp_ctx {
     // scans that grow the arena never move a staged input).
     uint8_t* kin = nullptr;
     size_t kin_cap = 0;
+    // Pinned host buffers kept for reuse (batch staging and readback).
+    struct PinnedBuf {
+        uint8_t* p;
+        size_t cap;
+        bool busy;
+    };
+    std::vector<PinnedBuf> pinned_pool;
+    // Batches submitted and not yet polled (opaque records owned by capi.cu).
+    std::unordered_map<uint64_t, void*> batches;
     // Live HashBuild handles (opaque pointers handed to callers).
     std::unordered_set<void*> hash_handles;
     // Launch profiling: event pairs around scan-kernel launches.
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
@@ -131,5 +143,6 @@ struct tgp_ctx {
     int l2_ahead = -1;         // L2 prefetch distance in tiles (TGP_L2_AHEAD; -1 = off)
     bool join_payload = true;  // unique-key join payload arrays (TGP_NO_JOIN_PAYLOAD=1 turns them off)
     bool hash_presum = true;   // shared pre-aggregation for hash grouping (TGP_NO_HASH_PRESUM=1 turns it off)
+    int morsel_tiles = 16;     // batch morsel length in tiles (TGP_BATCH_MORSEL_TILES)
     bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
 };

@@ -906,10 +906,12 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
 
     // Direct group index of each row: sum over keys of (cell - min) * stride,
     // exact in 32 bits because the group count is below 2^31.
-    // With a join payload, gin holds the build-side keys' part.
+    // With a join payload, gin holds the build-side keys' part for the rows
+    // in m. Every other row adds 0 to group 0, an in-range slot (its gin is
+    // the no-match sentinel, which must never become an address).
     uint32_t g[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) g[r] = gin ? gin[r] : 0u;
+    for (int r = 0; r < R; ++r) g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         if (static_cast<uint32_t>(k) < P.ngkey && !P.gkey[k].build_side) {
@@ -918,7 +920,7 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
             load_cells32<R>(stage + K.soff, K.dtype, t, x);
             const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
 #pragma unroll
-            for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
+            for (int r = 0; r < R; ++r) g[r] += (gin && !((m >> r) & 1u)) ? 0u : (x[r] - mn) * st;
         }
     }
     const uint32_t gstride = (P.nval + 1) * static_cast<uint32_t>(NT);
@@ -1354,14 +1356,139 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
 }
 
 // ---------------------------------------------------------------------------
-// The persistent kernel: NT consumer threads + one producer warp.
+// The tile pipeline: NT consumer threads + one producer warp.
 //
 // Stage s has two mbarriers: full[s] (producer arrive + TMA transaction bytes)
 // and empty[s] (one arrive per consumer warp once it has read the stage). The
 // producer waits on empty[s] before refilling stage s; consumers wait on
 // full[s]. No CTA-wide barrier runs per tile. Every wait is bounded; a wait
-// that gives up raises kErrWaitTimeout and the CTA drains its copies.
+// that gives up raises kErrWaitTimeout and sets the CTA's abort flag.
+//
+// A CTA walks the tiles first + k * stride (k < count). The full tiles
+// (tile < nfull) go through the stages; the final partial tile is read from
+// global memory. (s, phase, issued) carry over between calls on the same
+// barriers.
 // ---------------------------------------------------------------------------
+struct PipeState {
+    uint32_t s = 0;      // stage of the next full tile
+    uint32_t phase = 0;  // its mbarrier phase
+    uint64_t n = 0;      // full tiles handled so far on these barriers
+};
+
+__device__ __forceinline__ void pipe_produce(const Plan& P, uint64_t* full, uint64_t* empty, uint8_t* stages,
+                                             uint64_t first, uint64_t stride, uint64_t count, PipeState& st,
+                                             uint32_t* abort_flag) {
+    const uint64_t nfull = P.nrows / kTileRows;
+    const uint32_t S = P.nstages;
+    const uint64_t policy = l2_policy_evict_first();
+    // Tile j is prefetched into L2 when tile j - l2_ahead is copied into its
+    // stage, so a stage copy reads L2 instead of waiting out the HBM latency.
+    const uint32_t D = P.l2_ahead;
+    auto prefetch = [&](uint64_t j) {
+        if (j >= count) return;
+        const uint64_t tj = first + j * stride;
+        if (tj >= nfull) return;
+        for (uint32_t c = 0; c < P.nslots; ++c) {
+            const uint32_t bytes = kTileRows * P.slot[c].width;
+            bulk_prefetch_l2(P.slot[c].ptr + tj * bytes, bytes);
+        }
+    };
+    for (uint64_t j = S; j < D; ++j) prefetch(j);
+    for (uint64_t k = 0; k < count; ++k) {
+        const uint64_t tl = first + k * stride;
+        if (tl >= nfull) break;
+        if (D && k + D >= S) prefetch(k + D);
+        if (st.n >= S) {
+            // Wait until every consumer warp has released the previous use of
+            // stage s (one phase earlier).
+            if (!mbar_wait_bounded(&empty[st.s], st.phase ^ 1u)) {
+                atomicOr(P.err, kErrWaitTimeout);
+                atomicExch(abort_flag, 1u);
+                break;
+            }
+        }
+        if (*reinterpret_cast<volatile uint32_t*>(abort_flag)) break;
+        uint8_t* dst = stages + static_cast<size_t>(st.s) * P.stage_bytes;
+        mbar_arrive_expect_tx(&full[st.s], P.stage_bytes);
+        for (uint32_t c = 0; c < P.nslots; ++c) {
+            const uint32_t bytes = kTileRows * P.slot[c].width;
+            bulk_g2s(dst + P.slot[c].smem_off, P.slot[c].ptr + tl * bytes, bytes, &full[st.s], policy);
+        }
+        ++st.n;
+        if (++st.s == S) {
+            st.s = 0;
+            st.phase ^= 1u;
+        }
+    }
+}
+
+// Consumers: returns false after a timeout or abort.
+template <uint32_t MODE, bool ACC128, int NT, class SH>
+__device__ __forceinline__ bool pipe_consume(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
+                                             uint64_t* full, uint64_t* empty, uint8_t* stages, uint64_t first,
+                                             uint64_t stride, uint64_t count, PipeState& st, uint32_t* abort_flag,
+                                             const RegLeaves& RL, const RegVals& RV, unsigned long long& selected) {
+    const uint32_t t = threadIdx.x, lane = t & 31u;
+    const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
+    const uint64_t nfull = P.nrows / kTileRows;
+    const uint32_t S = P.nstages;
+    for (uint64_t k = 0; k < count; ++k) {
+        const uint64_t tl = first + k * stride;
+        if (tl >= ntiles) break;
+        if (tl < nfull) {
+            bool landed = false;
+            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase);
+            landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
+            if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
+                if (lane == 0) {
+                    atomicOr(P.err, kErrWaitTimeout);
+                    atomicExch(abort_flag, 1u);
+                }
+                return false;
+            }
+            // Lanes other than 0 observe the completed phase through a cheap
+            // try_wait so their shared-memory reads are ordered after the copy.
+            mbar_try_wait(&full[st.s], st.phase);
+            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, stages + static_cast<size_t>(st.s) * P.stage_bytes,
+                                                      tl, t, selected, RL, RV);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st.s]);
+            ++st.n;
+            if (++st.s == S) {
+                st.s = 0;
+                st.phase ^= 1u;
+            }
+        } else {
+            process_tile<MODE, ACC128, NT, true, SH>(P, sink, extra, nullptr, tl, t, selected, RL, RV);
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void pipe_init_barriers(uint64_t* full, uint64_t* empty, uint32_t S, uint32_t consumer_warps) {
+    for (uint32_t s = 0; s < S; ++s) {
+        mbar_init(&full[s], 1);
+        mbar_init(&empty[s], consumer_warps);
+    }
+    fence_barrier_init();
+}
+
+// Register-held predicate leaves and fast-path value descriptors of a plan.
+template <uint32_t MODE, bool ACC128, class SH>
+__device__ __forceinline__ void load_regs(const Plan& P, RegLeaves& RL, RegVals& RV) {
+    load_reg_leaves(P, RL);
+    if constexpr (std::is_void<SH>::value) load_reg_vals<MODE, ACC128>(P, RV);
+    else RV.on = 0;  // a fixed-shape kernel never takes the scalar fast path
+}
+
+template <int NT>
+__device__ __forceinline__ void count_selected(const Plan& P, unsigned long long selected) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) selected += __shfl_down_sync(kFull, selected, d);
+    if ((threadIdx.x & 31u) == 0 && selected) atomicAdd(P.counters, selected);
+}
+
+// One query: CTA b walks tiles b, b + gridDim.x, ...
 template <uint32_t MODE, bool ACC128, int NT, class SH = void>
 __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant__ Plan P) {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -1373,121 +1500,105 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
 
     const uint32_t t = threadIdx.x;
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
-    const uint64_t nfull = P.nrows / kTileRows;
-    const uint32_t S = P.nstages;
     const uint64_t G = gridDim.x;
-    constexpr uint32_t kConsumerWarps = NT / 32;
+    const uint64_t count = ntiles > blockIdx.x ? (ntiles - blockIdx.x + G - 1) / G : 0;
 
     Sink<MODE, ACC128, NT> sink;
     if (t < static_cast<uint32_t>(NT)) sink.init(P, extra, t);
     if (t == static_cast<uint32_t>(NT)) {
-        for (uint32_t s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kConsumerWarps);
-        }
-        fence_barrier_init();
+        pipe_init_barriers(full, empty, P.nstages, NT / 32);
         abort_flag = 0;
     }
     __syncthreads();
-
+    PipeState st;
     if (t >= static_cast<uint32_t>(NT)) {
-        // ---------------- producer warp (lane 0 issues) ----------------
         if (t != static_cast<uint32_t>(NT)) return;
-        const uint64_t policy = l2_policy_evict_first();
-        // Tile j of this CTA is prefetched into L2 when tile j - l2_ahead is
-        // copied into its stage, so a stage copy reads L2 instead of waiting
-        // out the HBM latency (shared memory then need not cover it).
-        const uint32_t D = P.l2_ahead;
-        auto prefetch = [&](uint64_t j) {
-            const uint64_t tj = blockIdx.x + j * G;
-            if (tj >= nfull) return;
-            for (uint32_t c = 0; c < P.nslots; ++c) {
-                const uint32_t bytes = kTileRows * P.slot[c].width;
-                bulk_prefetch_l2(P.slot[c].ptr + tj * bytes, bytes);
-            }
-        };
-        for (uint64_t j = S; j < D; ++j) prefetch(j);
-        uint64_t issued = 0;
-        uint32_t s = 0, phase = 0;  // stage and phase of tile k (k = issued)
-        for (uint64_t k = 0;; ++k) {
-            const uint64_t tl = blockIdx.x + k * G;
-            if (tl >= nfull) break;
-            if (D && k + D >= S) prefetch(k + D);
-            if (k >= S) {
-                // Wait until every consumer warp has released tile k - S
-                // (the previous use of stage s, one phase earlier).
-                if (!mbar_wait_bounded(&empty[s], phase ^ 1u)) {
-                    atomicOr(P.err, kErrWaitTimeout);
-                    atomicExch(&abort_flag, 1u);
-                    break;
-                }
-            }
-            if (*reinterpret_cast<volatile uint32_t*>(&abort_flag)) break;
-            uint8_t* dst = stages + static_cast<size_t>(s) * P.stage_bytes;
-            mbar_arrive_expect_tx(&full[s], P.stage_bytes);
-            for (uint32_t c = 0; c < P.nslots; ++c) {
-                const uint32_t bytes = kTileRows * P.slot[c].width;
-                bulk_g2s(dst + P.slot[c].smem_off, P.slot[c].ptr + tl * bytes, bytes, &full[s], policy);
-            }
-            ++issued;
-            if (++s == S) {
-                s = 0;
-                phase ^= 1u;
-            }
-        }
-        // Drain: the last min(S, issued) copies have landed before this thread
+        pipe_produce(P, full, empty, stages, blockIdx.x, G, count, st, &abort_flag);
+        // Drain: the last min(S, n) copies have landed before this thread
         // exits (earlier ones were waited for through empty[]).
-        const uint64_t first = issued > S ? issued - S : 0;
-        for (uint64_t i = first; i < issued; ++i)
+        const uint32_t S = P.nstages;
+        const uint64_t first = st.n > S ? st.n - S : 0;
+        for (uint64_t i = first; i < st.n; ++i)
             if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P.err, kErrWaitTimeout);
         return;
     }
-
-    // ---------------- consumers ----------------
-    const uint32_t lane = t & 31u;
     RegLeaves RL;
-    load_reg_leaves(P, RL);
     RegVals RV;
-    if constexpr (std::is_void<SH>::value) load_reg_vals<MODE, ACC128>(P, RV);
-    else RV.on = 0;  // a fixed-shape kernel never takes the scalar fast path
+    load_regs<MODE, ACC128, SH>(P, RL, RV);
     unsigned long long selected = 0;
-    bool ok = true;
-    uint32_t s = 0, phase = 0;  // stage and phase of the k-th full tile
-    for (uint64_t tl = blockIdx.x; tl < ntiles; tl += G) {
-        if (tl < nfull) {
-            bool landed = false;
-            if (lane == 0) landed = mbar_wait_bounded(&full[s], phase);
-            landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
-            if (!landed || *reinterpret_cast<volatile uint32_t*>(&abort_flag)) {
-                if (lane == 0) {
-                    atomicOr(P.err, kErrWaitTimeout);
-                    atomicExch(&abort_flag, 1u);
-                }
-                ok = false;
-                break;
-            }
-            // Lanes other than 0 observe the completed phase through a cheap
-            // try_wait so their shared-memory reads are ordered after the copy.
-            mbar_try_wait(&full[s], phase);
-            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, stages + static_cast<size_t>(s) * P.stage_bytes,
-                                                  tl, t, selected, RL, RV);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);
-            if (++s == S) {
-                s = 0;
-                phase ^= 1u;
-            }
-        } else {
-            process_tile<MODE, ACC128, NT, true, SH>(P, sink, extra, nullptr, tl, t, selected, RL, RV);
-        }
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) selected += __shfl_down_sync(kFull, selected, d);
-    if (lane == 0 && selected) atomicAdd(P.counters, selected);
+    pipe_consume<MODE, ACC128, NT, SH>(P, sink, extra, full, empty, stages, blockIdx.x, G, count, st, &abort_flag, RL,
+                                       RV, selected);
+    count_selected<NT>(P, selected);
     // Every consumer reaches the flush, also after a timeout (the host then
     // discards the result), so the consumer barrier inside it always completes.
-    (void)ok;
     sink.flush(P, extra, t);
+}
+
+// ---------------------------------------------------------------------------
+// Many queries in one persistent launch. The host splits every query into
+// morsels (a query and a range of its tiles); CTAs take morsels from a device
+// counter until none is left. Per morsel the CTA copies the query's plan into
+// shared memory, re-initializes its stage barriers for that plan's layout,
+// runs the tile pipeline over the range and merges its partial aggregates
+// into the query's accumulators.
+// ---------------------------------------------------------------------------
+template <uint32_t MODE, bool ACC128, int NT>
+__global__ void __launch_bounds__(NT + 32, 1) batch_kernel(const __grid_constant__ BatchDesc B) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + kMaxStages;
+    uint8_t* stages = smem + kBarrierBytes;
+    __shared__ __align__(16) Plan sP;
+    __shared__ uint32_t abort_flag, s_morsel;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) abort_flag = 0;
+    for (;;) {
+        if (t == 0) s_morsel = atomicAdd(B.next, 1u);
+        __syncthreads();
+        const uint32_t mi = s_morsel;
+        if (mi >= B.nmorsels || *reinterpret_cast<volatile uint32_t*>(&abort_flag)) break;
+        const Morsel M = B.morsels[mi];
+        {
+            const uint4* src = reinterpret_cast<const uint4*>(B.plans + M.query);
+            uint4* dst = reinterpret_cast<uint4*>(&sP);
+            for (uint32_t i = t; i < sizeof(Plan) / 16; i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        const Plan& P = sP;
+        uint8_t* extra = smem + P.extra_off;
+        Sink<MODE, ACC128, NT> sink;
+        if (t < static_cast<uint32_t>(NT)) sink.init(P, extra, t);
+        if (t == static_cast<uint32_t>(NT)) pipe_init_barriers(full, empty, P.nstages, NT / 32);
+        __syncthreads();
+        PipeState st;
+        const uint64_t count = M.tile_end - M.tile_begin;
+        if (t == static_cast<uint32_t>(NT)) {
+            pipe_produce(P, full, empty, stages, M.tile_begin, 1, count, st, &abort_flag);
+            // Drain (a no-op unless the consumers gave up): no copy may still
+            // be in flight when the barriers are invalidated.
+            const uint32_t S = P.nstages;
+            for (uint64_t i = st.n > S ? st.n - S : 0; i < st.n; ++i)
+                if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P.err, kErrWaitTimeout);
+        } else if (t < static_cast<uint32_t>(NT)) {
+            RegLeaves RL;
+            RegVals RV;
+            load_regs<MODE, ACC128, void>(P, RL, RV);
+            unsigned long long selected = 0;
+            pipe_consume<MODE, ACC128, NT, void>(P, sink, extra, full, empty, stages, M.tile_begin, 1, count, st,
+                                                 &abort_flag, RL, RV, selected);
+            count_selected<NT>(P, selected);
+            sink.flush(P, extra, t);
+        }
+        // Every stage copy of this morsel was consumed: the barriers and the
+        // shared plan can be reused.
+        __syncthreads();
+        if (t == static_cast<uint32_t>(NT))
+            for (uint32_t s = 0; s < P.nstages; ++s) {
+                mbar_inval(&full[s]);
+                mbar_inval(&empty[s]);
+            }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1657,5 +1768,48 @@ int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t
 
 // Static shared memory used by scan_kernel besides the dynamic stages.
 size_t scan_kernel_static_smem() { return 128; }
+
+// Batch launches (MODE_GROUP_PRIVATE plans): one persistent kernel per
+// (acc128, NT) class; the shared plan copy is static shared memory.
+size_t batch_kernel_static_smem() { return sizeof(Plan) + 128; }
+
+static const void* batch_kernel_ptr(bool acc128, int nt) {
+    if (nt == 512)
+        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 512>)
+                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 512>);
+    if (nt == 256)
+        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 256>)
+                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 256>);
+    return nullptr;
+}
+
+int batch_occupancy(bool acc128, int nt, size_t dyn_smem) {
+    const void* f = batch_kernel_ptr(acc128, nt);
+    if (!f) return 0;
+    std::lock_guard<std::mutex> lock(g_kcache_mu);
+    KernelCacheEntry* e = kernel_entry(f);
+    if (ensure_smem_limit(e, f, static_cast<int>(dyn_smem)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, nt + 32, dyn_smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+cudaError_t launch_batch(const BatchDesc& B, bool acc128, int nt, int grid, size_t dyn_smem, cudaStream_t st) {
+    const void* f = batch_kernel_ptr(acc128, nt);
+    if (!f) return cudaErrorInvalidValue;
+    {
+        std::lock_guard<std::mutex> lock(g_kcache_mu);
+        const cudaError_t e = ensure_smem_limit(kernel_entry(f), f, static_cast<int>(dyn_smem));
+        if (e != cudaSuccess) return e;
+    }
+    void* args[] = {const_cast<BatchDesc*>(&B)};
+    return cudaLaunchKernel(f, dim3(grid), dim3(nt + 32), args, dyn_smem, st);
+}
 
 }  // namespace tgp

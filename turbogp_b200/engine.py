@@ -300,6 +300,11 @@ class Context:
         'int' | 'date' | 'float' (default: 'float' for f64, else 'int')."""
         return self._register(columns, coltypes, device=False)
 
+    def submit(self, queries: Sequence["PreparedQuery"], decode: bool = True) -> "BatchHandle":
+        """Runs prepared queries as one batch (tgp_batch_submit); a query may be
+        in one unfinished batch at a time."""
+        return BatchHandle(self, queries, decode)
+
     def register_device(self, columns: dict, coltypes: dict | None = None) -> "Table":
         """Registers device tensors (torch CUDA tensors) without copying."""
         return self._register(columns, coltypes, device=True)
@@ -549,12 +554,62 @@ class PreparedQuery:
                 continue
             ctx._check(st, "tgp_execute")
             break
-        r = self.res
+        return self._output(self.res, decode)
+
+    def _output(self, r, decode: bool = True) -> QueryOutput:
         if not decode:
             return QueryOutput([], [], int(r.rows_scanned), int(r.rows_selected), int(r.flags))
         ng = int(r.ngroups)
         raw = (self.keys[:ng * self.nk].copy(), self._vals_np[:ng * self.na].copy(), ng, self.nk, self.na)
         return QueryOutput(None, None, int(r.rows_scanned), int(r.rows_selected), int(r.flags), raw)
+
+
+class BatchHandle:
+    """Queries submitted together with tgp_batch_submit (one persistent launch
+    for the direct / scalar aggregates). ``poll()`` is non-blocking; ``wait()``
+    returns one QueryOutput per query, in submission order."""
+
+    def __init__(self, ctx: Context, queries: Sequence["PreparedQuery"], decode: bool = True):
+        self.ctx, self.queries, self.decode = ctx, list(queries), decode
+        self.items = (A.BatchItem * max(1, len(self.queries)))()
+        for i, pq in enumerate(self.queries):
+            it = self.items[i]
+            it.query = C.pointer(pq.q)
+            it.keys_out = pq.keys.ctypes.data
+            it.vals_out = pq.vals
+            it.group_cap = pq.cap
+        bid = C.c_uint64()
+        ctx._check(ctx.lib.tgp_batch_submit(ctx.h, self.items, len(self.queries), C.byref(bid)), "tgp_batch_submit")
+        self.id = int(bid.value)
+        self.outputs: list[QueryOutput] | None = None
+
+    def _finish(self) -> None:
+        outs = []
+        for i, pq in enumerate(self.queries):
+            it = self.items[i]
+            if it.status == A.CAPACITY:
+                outs.append(pq.run(self.decode))  # more groups than the buffer: rerun alone, resized
+                continue
+            if it.status != A.OK:
+                self.ctx._check(it.status, f"batch query {i}")
+            outs.append(pq._output(it.result, self.decode))
+        self.outputs = outs
+
+    def poll(self) -> bool:
+        if self.outputs is not None:
+            return True
+        st = self.ctx.lib.tgp_batch_poll(self.ctx.h, self.id, 0)
+        if st == A.PENDING:
+            return False
+        self.ctx._check(st, "tgp_batch_poll")
+        self._finish()
+        return True
+
+    def wait(self) -> list[QueryOutput]:
+        if self.outputs is None:
+            self.ctx._check(self.ctx.lib.tgp_batch_poll(self.ctx.h, self.id, 1), "tgp_batch_poll")
+            self._finish()
+        return self.outputs
 
 
 class JoinTable:
