@@ -447,6 +447,86 @@ def run_batch(args, world: int, rank: int, local: int) -> None:
     ctx.close()
 
 
+def run_serve(args, world: int, rank: int, local: int) -> None:
+    """Serving: resident 60M-row fact table, 1.5M-row dimension (+ join table)
+    and 100M-row high-cardinality table; an open-loop Poisson stream of
+    requests (selective scan + sum, filtered grouped aggregate, join + grouped
+    aggregate with random literals; GROUP BY key over the high-cardinality
+    table for 1 in 500) served by the continuous-batching server (shared scans,
+    memory-budget admission) and by plain one-at-a-time execution. value =
+    batched completions/s at the offered rate; p50/p99 of both in the line."""
+    import numpy as np
+    import torch
+    from turbogp_b200 import datagen, serving, workloads
+    from turbogp_b200.engine import Context, col, count_star, sum_
+    ctx = Context(local)
+    n = args.rows if args.rows != ROWS else 60_000_000
+    host = datagen.fact_fk(n, 1_500_000, 0.8, seed=3 + rank)
+    f = ctx.register(host, {**datagen.LINEITEM_COLTYPES, "fk": "int"})
+    del host
+    d = ctx.register(datagen.dimension(1_500_000, seed=2 + rank), datagen.DIMENSION_COLTYPES)
+    tj = workloads.join_group_agg()
+    j = d.join_build("key", tj.build_where)
+    hc = ctx.register(datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank))
+    t_scan, t_fga = workloads.selective_scan_sum(), workloads.filtered_group_agg()
+    hc_aggs = [count_star(), sum_(col("value"))]
+    gb = 1 << 30
+    templates = {
+        "scan": serving.Template("scan", lambda: f.prepare(t_scan.aggs, t_scan.group_by, t_scan.where), 1 << 16),
+        "fga": serving.Template("fga", lambda: f.prepare(t_fga.aggs, t_fga.group_by, t_fga.where), 1 << 16),
+        "join": serving.Template("join", lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk"),
+                                 1 << 16),
+        "highcard": serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None),
+                                     2 * gb),
+    }
+    rng = np.random.default_rng(21 + rank)
+    D0, ND = datagen.DAY0, datagen.NDAYS
+
+    def request(t):
+        u = rng.random()
+        if u < 0.002:
+            return serving.Request(t, "highcard", None)
+        k = int(rng.integers(0, 3))
+        if k == 0:
+            lo = D0 + int(rng.integers(0, ND - 30))
+            w = ((col("ship_day") >= lo) & (col("ship_day") < lo + int(rng.integers(30, 366))) &
+                 col("discount_pct").between(int(rng.integers(0, 6)), int(rng.integers(5, 11))) &
+                 (col("quantity") < int(rng.integers(2, 51))))
+            return serving.Request(t, "scan", w)
+        if k == 1:
+            return serving.Request(t, "fga", col("ship_day") <= D0 + int(rng.integers(3, ND)))
+        return serving.Request(t, "join", col("quantity") < int(rng.integers(2, 51)))
+
+    def stream(rate, count):
+        return [request(t) for t in serving.poisson_arrivals(rate, count, rng)]
+
+    rate, count = args.rate, args.requests
+    # Warm-up: every template through both paths.
+    serving.serve_batched(ctx, templates, stream(rate, 64), mem_budget=args.mem_budget)
+    serving.serve_plain(ctx, templates, stream(rate, 16))
+    with ClockSampler(local) as clocks:
+        batched = serving.serve_batched(ctx, templates, stream(rate, count), mem_budget=args.mem_budget)
+    plain = serving.serve_plain(ctx, templates, stream(rate, max(32, count // 8)))
+    peak, peak_kind = peak_hbm()
+    line = {
+        "metric": METRIC, "value": batched.get("qps"), "unit": "queries/s", "n_gpus": world,
+        "steps": count, "warmup": 64, "ms_per_step": batched.get("mean_ms"), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H shapes)",
+        "config": {"workload": f"serving: Poisson arrivals at {rate:g} q/s of scan+sum / filtered grouped "
+                               f"aggregate / join+grouped aggregate over a resident {n}-row fact table (random "
+                               f"literals) and GROUP BY key over a {args.highcard_rows}-row high-cardinality table "
+                               f"(1 in 500); continuous batching with shared scans, admission budget "
+                               f"{args.mem_budget} B",
+                   "offered_qps": rate, "requests": count},
+        "batched": batched, "plain": plain,
+        "roofline": None, "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    j.drop()
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,13 +539,21 @@ def main() -> None:
     ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="selective_scan_sum",
-                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch"])
+                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
+                             "serve"])
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: offered queries/s")
+    ap.add_argument("--requests", type=int, default=4000, help="serve: requests in the timed stream")
+    ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
+    ap.add_argument("--highcard-rows", type=int, default=100_000_000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     world, rank, local = dist_setup(args.gpus)
     if args.workload == "batch":
         run_batch(args, world, rank, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, world, rank, local)
         return
     if args.workload != "selective_scan_sum":
         run_workload(args, world, rank, local)

@@ -11,6 +11,7 @@
 #include <new>
 #include <string>
 #include <memory>
+#include <unordered_map>
 #include <vector>
 
 #include "runtime.hpp"
@@ -814,6 +815,7 @@ int tgp_init(tgp_ctx** out, int device) {
     cudaGetLastError();
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_NO_SHARED_SCANS")) ctx->shared_scans = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_BATCH_MORSEL_TILES")) ctx->morsel_tiles = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_HASH_PRESUM")) ctx->hash_presum = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
@@ -1159,8 +1161,10 @@ struct QueryState {
 
 // Lowers a query (predicate, aggregates, keys, join payload) and chooses its
 // mode and shared-memory layout for a kernel with `static_smem` static bytes.
+// `preseed` (optional) lists columns to stage first, in that order.
 // Result pointers (counters, err, acc, htab) are left for the caller.
-static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem) {
+static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem,
+                      const std::vector<uint32_t>* preseed = nullptr) {
     if (!ctx || !q) return fail(ctx, TGP_INVALID_ARG, "null argument");
     qs.q = q;
     TGP_TRY(get_table(ctx, q->table, &qs.T));
@@ -1168,6 +1172,12 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     qs.b.reset(new Builder(ctx, T));
     Builder& b = *qs.b;
     b.static_smem = static_smem;
+    // A shared scan stages the union of its queries' columns in one order.
+    if (preseed)
+        for (uint32_t c : *preseed) {
+            int slot;
+            TGP_TRY(b.slot_of(c, &slot));
+        }
     JoinTable*& J = qs.J;
     J = nullptr;
     if (q->join) {
@@ -1286,6 +1296,7 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             if (!acc128 && (!J || pay_ok) && !P.check_ovf && ctx->dense_path)
                 P.dense_vec = compile_chain(b, pay_ok) ? 1u : 0u;
             if (P.dense_vec && ctx->dense_shapes && !J) P.shape = dense_shape_of(P);
+            if (!P.shape && !acc128) P.shape = scalar_shape_of(P);
         } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;
@@ -1641,73 +1652,151 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     B->batched.assign(n, 0);
     B->block_off.assign(n, 0);
     const size_t bstatic = batch_kernel_static_smem();
-    // 1. Plan; queries the persistent kernel does not take run now, alone.
-    struct Class {
-        bool acc128;
-        uint32_t nt;
-        size_t smem = 0;
-        std::vector<uint32_t> q;
-        int grid = 0;
-        std::vector<Morsel> morsels;
-    };
-    std::vector<Class> classes;
-    std::vector<uint32_t> plan_index(n, 0);
-    uint32_t nplans = 0;
+    const size_t budget = ctx->max_dyn_smem - bstatic;
+    // 1. Plan alone; the persistent kernel takes the direct-indexed / scalar
+    // plans, everything else runs now, one query at a time.
+    std::vector<uint32_t> take;
     for (uint32_t i = 0; i < n; ++i) {
         tgp_batch_item& it = items[i];
         std::memset(&it.result, 0, sizeof(it.result));
         it.status = TGP_OK;
         QueryState& qs = B->qs[i];
         int st = plan_query(ctx, it.query, qs, bstatic);
-        bool take = st == TGP_OK && qs.mode == MODE_GROUP_PRIVATE;
-        if (take) {
-            qs.b->P.shape = 0;
-            take = size_smem(ctx, qs.b->P, qs.extra, bstatic) == TGP_OK;
-        }
-        if (!take) {
-            if (st == TGP_OK) st = tgp_execute(ctx, it.query, it.keys_out, it.vals_out, it.group_cap, &it.result);
-            it.status = st;
+        if (st == TGP_OK && qs.mode == MODE_GROUP_PRIVATE) {
+            take.push_back(i);
             continue;
         }
-        B->batched[i] = 1;
-        plan_index[i] = nplans++;
-        const Plan& P = qs.b->P;
-        Class* c = nullptr;
-        for (auto& k : classes)
-            if (k.acc128 == qs.acc128 && k.nt == P.nthreads) c = &k;
-        if (!c) {
-            classes.push_back(Class{qs.acc128, P.nthreads});
-            c = &classes.back();
-        }
-        c->smem = std::max<size_t>(c->smem, P.smem_bytes);
-        c->q.push_back(i);
+        if (st == TGP_OK) st = tgp_execute(ctx, it.query, it.keys_out, it.vals_out, it.group_cap, &it.result);
+        it.status = st;
     }
+    // 2. Shared scans: queries over one table are re-planned over the union of
+    // their columns (when it fits the stage's slots) and packed into groups
+    // whose accumulator regions fit beside two stages.
+    struct Group {
+        bool acc128;
+        uint32_t nt;
+        std::vector<uint32_t> q;
+        size_t extra = 0;
+    };
+    std::vector<Group> groups;
+    std::unordered_map<uint64_t, std::vector<uint32_t>> by_table;
+    std::vector<uint64_t> table_order;
+    for (uint32_t i : take) {
+        const uint64_t tid = items[i].query->table;
+        if (!by_table.count(tid)) table_order.push_back(tid);
+        by_table[tid].push_back(i);
+    }
+    for (uint64_t tid : table_order) {
+        std::vector<uint32_t>& qi = by_table[tid];
+        std::vector<uint32_t> cols;
+        for (uint32_t i : qi) {
+            const std::vector<int>& c2s = B->qs[i].b->col2slot;
+            for (uint32_t c = 0; c < c2s.size(); ++c)
+                if (c2s[c] >= 0 && std::find(cols.begin(), cols.end(), c) == cols.end()) cols.push_back(c);
+        }
+        const bool share = ctx->shared_scans && qi.size() > 1 && cols.size() <= static_cast<size_t>(kMaxSlots);
+        for (uint32_t i : qi) {
+            QueryState& qs = B->qs[i];
+            if (share) {
+                QueryState re;
+                if (plan_query(ctx, items[i].query, re, bstatic, &cols) == TGP_OK && re.mode == MODE_GROUP_PRIVATE)
+                    qs = std::move(re);
+            }
+            Plan& P = qs.b->P;
+            // The int64 batch kernels carry the fixed-shape dense path.
+            P.shape = (!qs.acc128 && !qs.J && P.dense_vec && ctx->dense_shapes && dense_shape_of(P) == 1) ? 1u : 0u;
+            const size_t extra = (qs.extra + 127) & ~size_t{127};
+            Group* g = nullptr;
+            if (share)
+                for (auto& k : groups)
+                    if (k.acc128 == qs.acc128 && k.nt == P.nthreads && k.q.size() < static_cast<size_t>(kMaxShare) &&
+                        items[k.q[0]].query->table == tid &&
+                        B->qs[k.q[0]].b->P.stage_bytes == P.stage_bytes &&
+                        k.extra + extra + (k.q.size() + 1) * sizeof(Plan) + 2ull * P.stage_bytes + kBarrierBytes + 256 <=
+                            budget)
+                        g = &k;
+            if (!g) {
+                groups.push_back(Group{qs.acc128, P.nthreads});
+                g = &groups.back();
+            }
+            g->q.push_back(i);
+            g->extra += extra;
+        }
+    }
+    // 3. Shared-memory layout per group: the barriers, the group's plans, the
+    // stages, then each plan's accumulator region.
+    for (const Group& g : groups) {
+        const Plan& P0 = B->qs[g.q[0]].b->P;
+        const size_t stage = P0.stage_bytes;
+        const size_t stage_off = (kBarrierBytes + g.q.size() * sizeof(Plan) + 127) & ~size_t{127};
+        const size_t fixed = stage_off + 128 + g.extra;
+        const size_t avail = budget > fixed ? budget - fixed : 0;
+        const uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1u;
+        if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "batched query does not fit in shared memory");
+        size_t off = (stage_off + static_cast<size_t>(S) * stage + 127) & ~size_t{127};
+        for (uint32_t i : g.q) {
+            Plan& P = B->qs[i].b->P;
+            P.nstages = S;
+            P.l2_ahead = 0;
+            P.stage_off = static_cast<uint32_t>(stage_off);
+            P.extra_off = static_cast<uint32_t>(off);
+            off += (B->qs[i].extra + 127) & ~size_t{127};
+        }
+        for (uint32_t i : g.q) B->qs[i].b->P.smem_bytes = static_cast<uint32_t>(off);
+    }
+    uint32_t nplans = 0;
+    std::vector<uint32_t> plan_index(n, 0);
+    for (const Group& g : groups)
+        for (uint32_t i : g.q) {
+            B->batched[i] = 1;
+            plan_index[i] = nplans++;
+        }
     if (nplans == 0) {
         const uint64_t id = ctx->next_id++;
         ctx->batches.emplace(id, B.release());
         *out = id;
         return TGP_OK;
     }
-    // 2. Morsels: a query of T tiles becomes min(grid, ceil(T / morsel_tiles)) ranges;
-    // each class's morsels are handed out largest first.
+    // 4. Launch classes (acc128, NT) and morsels: a group over T tiles becomes
+    // min(grid, ceil(T / morsel_tiles)) ranges, handed out largest first.
+    struct Class {
+        bool acc128;
+        uint32_t nt;
+        size_t smem = 0;
+        int grid = 0;
+        std::vector<Morsel> morsels;
+    };
+    std::vector<Class> classes;
+    std::vector<size_t> group_class(groups.size());
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        size_t k = 0;
+        while (k < classes.size() && !(classes[k].acc128 == g.acc128 && classes[k].nt == g.nt)) ++k;
+        if (k == classes.size()) classes.push_back(Class{g.acc128, g.nt});
+        classes[k].smem = std::max<size_t>(classes[k].smem, B->qs[g.q[0]].b->P.smem_bytes);
+        group_class[gi] = k;
+    }
     for (auto& c : classes) {
         const int occ = batch_occupancy(c.acc128, static_cast<int>(c.nt), c.smem);
         if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "batch kernel cannot be resident with this shared memory");
         c.grid = ctx->sms * occ;
-        for (uint32_t i : c.q) {
-            const uint64_t T = (B->qs[i].b->P.nrows + kTileRows - 1) / kTileRows;
-            if (T == 0) continue;
-            const uint64_t per = static_cast<uint64_t>(ctx->morsel_tiles);
-            const uint64_t nm = std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(c.grid), (T + per - 1) / per));
-            const uint64_t size = (T + nm - 1) / nm;
-            for (uint64_t b0 = 0; b0 < T; b0 += size)
-                c.morsels.push_back(Morsel{plan_index[i], 0, b0, std::min(T, b0 + size)});
-        }
-        std::stable_sort(c.morsels.begin(), c.morsels.end(), [](const Morsel& a, const Morsel& b) {
-            return a.tile_end - a.tile_begin > b.tile_end - b.tile_begin;
-        });
     }
-    // 3. One device region: [plans][morsels per class][counters][result blocks].
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        const Group& g = groups[gi];
+        Class& c = classes[group_class[gi]];
+        const uint64_t T = (B->qs[g.q[0]].b->P.nrows + kTileRows - 1) / kTileRows;
+        if (T == 0) continue;
+        const uint64_t per = static_cast<uint64_t>(ctx->morsel_tiles);
+        const uint64_t nm = std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(c.grid), (T + per - 1) / per));
+        const uint64_t size = (T + nm - 1) / nm;
+        for (uint64_t b0 = 0; b0 < T; b0 += size)
+            c.morsels.push_back(Morsel{plan_index[g.q[0]], static_cast<uint32_t>(g.q.size()), b0, std::min(T, b0 + size)});
+    }
+    for (auto& c : classes)
+        std::stable_sort(c.morsels.begin(), c.morsels.end(), [](const Morsel& a, const Morsel& b) {
+            return (a.tile_end - a.tile_begin) * a.count > (b.tile_end - b.tile_begin) * b.count;
+        });
+    // 5. One device region: [plans][morsels per class][counters][result blocks].
     size_t off = align256(static_cast<size_t>(nplans) * sizeof(Plan));
     std::vector<size_t> morsel_off(classes.size());
     for (size_t k = 0; k < classes.size(); ++k) {
@@ -1751,7 +1840,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     for (size_t k = 0; k < classes.size(); ++k)
         if (!classes[k].morsels.empty())
             std::memcpy(h + morsel_off[k], classes[k].morsels.data(), classes[k].morsels.size() * sizeof(Morsel));
-    // 4. One upload, the persistent launches, one readback.
+    // 6. One upload, the persistent launches, one readback.
     TGP_CUDA(cudaMemcpyAsync(B->dev, h, total, cudaMemcpyHostToDevice, ctx->stream));
     for (size_t k = 0; k < classes.size(); ++k) {
         const Class& c = classes[k];

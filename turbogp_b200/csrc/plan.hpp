@@ -73,11 +73,20 @@ struct Leaf {
     uint32_t lo32;
     uint32_t span32;
     uint64_t xor64;
-    uint64_t lo64;
-    uint64_t span64;
-    double f1;        // LK_F64 literal / lower bound / epsilon target
-    double f2;        // LK_F64 upper bound or epsilon
+    union {
+        struct {
+            uint64_t lo64;
+            uint64_t span64;
+        };
+        struct {
+            double f1;  // LK_F64 literal / lower bound / epsilon target
+            double f2;  // LK_F64 upper bound or epsilon
+        };
+    };
 };
+
+// Plan::shape of scalar aggregates on the register fast path.
+constexpr uint32_t kShapeScalar = 0xffffu;
 
 // Postfix program opcodes: values < kMaxLeaves push leaf i.
 enum : uint8_t { OP_AND = 0x80, OP_OR = 0x81, OP_NOT = 0x82 };
@@ -168,8 +177,8 @@ struct alignas(16) Plan {
     uint32_t check_ovf;     // per-row overflow detection needed
     uint32_t count_by_tile; // MODE_GROUP_PRIVATE, one group, no join: row count = popcount per tile
     uint32_t dense_vec;     // MODE_GROUP_PRIVATE int64: `chain` holds the dense value program
-    uint32_t shape;         // ahead-of-time kernel for `chain` (0 = interpreted)
-    uint32_t _p4;
+    uint32_t shape;         // ahead-of-time kernel for `chain` (0 = interpreted; kShapeScalar: scalar fast path)
+    uint32_t stage_off;     // batch launches: shared offset of the stage ring (plans precede it)
     uint64_t flush_limit;   // MODE_GROUP_PRIVATE int64: per-thread updates between flushes
     ValDesc val[kMaxVals];
 
@@ -280,10 +289,13 @@ struct HashFormat {
 
 static_assert(sizeof(Plan) % 16 == 0, "plans are copied in 16-byte words");
 
-// A range of one query's tiles, processed by one CTA of a batch launch.
+// A range of tiles of one table, processed by one CTA of a batch launch for
+// `count` consecutive plans starting at `first` (a shared scan when count > 1:
+// the plans share one stage layout and have disjoint accumulator regions).
+constexpr int kMaxShare = 16;
 struct Morsel {
-    uint32_t query;
-    uint32_t _pad;
+    uint32_t first;
+    uint32_t count;
     uint64_t tile_begin;
     uint64_t tile_end;
 };

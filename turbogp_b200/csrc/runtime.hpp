@@ -24,6 +24,9 @@ int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t
 // Index (>= 1) of the ahead-of-time dense kernel matching the plan's key
 // dtypes and value program, or 0 (the interpreted dense program runs).
 uint32_t dense_shape_of(const Plan& P);
+// kShapeScalar when the plan is a scalar aggregate the register fast path
+// takes (one or two SUMs of one or two staged factors, bounded), else 0.
+uint32_t scalar_shape_of(const Plan& P);
 size_t scan_kernel_static_smem();
 size_t batch_kernel_static_smem();
 int batch_occupancy(bool acc128, int nt, size_t dyn_smem);
@@ -135,7 +138,7 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
@@ -144,5 +147,6 @@ struct tgp_ctx {
     bool join_payload = true;  // unique-key join payload arrays (TGP_NO_JOIN_PAYLOAD=1 turns them off)
     bool hash_presum = true;   // shared pre-aggregation for hash grouping (TGP_NO_HASH_PRESUM=1 turns it off)
     int morsel_tiles = 16;     // batch morsel length in tiles (TGP_BATCH_MORSEL_TILES)
+    bool shared_scans = true;  // batches merge same-table queries into shared scans (TGP_NO_SHARED_SCANS=1: off)
     bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
 };

@@ -1008,6 +1008,9 @@ constexpr uint32_t step_code(uint32_t dt, uint32_t fl, uint32_t kind, uint32_t a
     return dt | (fl << 4) | (kind << 10) | (acc << 13);
 }
 
+// Kernel tag: scalar aggregates on the register fast path (RegVals).
+struct ScalarTag {};
+
 template <uint32_t NKEY, uint32_t KDT0, uint32_t KDT1, uint32_t... STEPS>
 struct DenseShape {
     static constexpr uint32_t nkey = NKEY;
@@ -1317,7 +1320,10 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t);
         }
     };
-    if constexpr (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL) {
+    // The scalar kernel (SH = ScalarTag) carries only the register fast path
+    // and the generic row loop.
+    constexpr bool kScalar = std::is_same<SH, ScalarTag>::value;
+    if constexpr (!kScalar && (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL)) {
         if (!TAIL && P.jpay) {
             uint32_t g[R];
             const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
@@ -1346,9 +1352,14 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
         }
         // A warp whose rows are at least a quarter selected runs the dense
         // column program; sparser warps loop over their selected rows only.
-        if (!TAIL && P.dense_vec && __reduce_add_sync(kFull, __popc(m)) >= 8u * R) {
-            if constexpr (std::is_void<SH>::value) chain_private_tile<NT>(P, extra, stage, t, m, sink);
-            else chain_tile_static<NT, SH>(P, extra, stage, t, m, sink);
+        if (!kScalar && !TAIL && P.dense_vec && __reduce_add_sync(kFull, __popc(m)) >= 8u * R) {
+            if constexpr (kScalar) {
+            } else if constexpr (std::is_void<SH>::value) {
+                chain_private_tile<NT>(P, extra, stage, t, m, sink);
+            } else {
+                if (P.shape) chain_tile_static<NT, SH>(P, extra, stage, t, m, sink);
+                else chain_private_tile<NT>(P, extra, stage, t, m, sink);
+            }
             return;
         }
     }
@@ -1474,11 +1485,14 @@ __device__ __forceinline__ void pipe_init_barriers(uint64_t* full, uint64_t* emp
 }
 
 // Register-held predicate leaves and fast-path value descriptors of a plan.
-template <uint32_t MODE, bool ACC128, class SH>
+template <uint32_t MODE, bool ACC128, class SH, bool MIXED = false>
 __device__ __forceinline__ void load_regs(const Plan& P, RegLeaves& RL, RegVals& RV) {
     load_reg_leaves(P, RL);
-    if constexpr (std::is_void<SH>::value) load_reg_vals<MODE, ACC128>(P, RV);
-    else RV.on = 0;  // a fixed-shape kernel never takes the scalar fast path
+    // A fixed-shape kernel of one query never takes the scalar fast path; a
+    // batch kernel (MIXED) serves both kinds of plan.
+    if constexpr (std::is_void<SH>::value || MIXED || std::is_same<SH, ScalarTag>::value)
+        load_reg_vals<MODE, ACC128>(P, RV);
+    else RV.on = 0;
 }
 
 template <int NT>
@@ -1535,20 +1549,74 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------------------
-// Many queries in one persistent launch. The host splits every query into
-// morsels (a query and a range of its tiles); CTAs take morsels from a device
-// counter until none is left. Per morsel the CTA copies the query's plan into
-// shared memory, re-initializes its stage barriers for that plan's layout,
-// runs the tile pipeline over the range and merges its partial aggregates
-// into the query's accumulators.
+// Many queries in one persistent launch. The host splits the work into
+// morsels: a group of plans over the same table that share one stage layout
+// (the union of their columns; each plan has its own accumulator region) and
+// a range of tiles. CTAs take morsels from a device counter until none is
+// left. Per morsel the CTA re-initializes its stage barriers for the group's
+// layout, streams each tile once and runs every plan of the group on it (a
+// shared scan), then merges each plan's partial aggregates into that query's
+// accumulators. Plans are read from global memory (L1-resident, uniform).
 // ---------------------------------------------------------------------------
-template <uint32_t MODE, bool ACC128, int NT>
+template <uint32_t MODE, bool ACC128, int NT, class SH>
+__device__ __forceinline__ void consume_group(const Plan* plans, uint32_t np, Sink<MODE, ACC128, NT>* sinks,
+                                              uint8_t* smem, uint64_t* full, uint64_t* empty, uint8_t* stages,
+                                              uint64_t first, uint64_t count, PipeState& st, uint32_t* abort_flag,
+                                              unsigned long long* selected) {
+    const Plan& P0 = plans[0];
+    const uint32_t t = threadIdx.x, lane = t & 31u;
+    const uint64_t ntiles = (P0.nrows + kTileRows - 1) / kTileRows;
+    const uint64_t nfull = P0.nrows / kTileRows;
+    const uint32_t S = P0.nstages;
+    for (uint64_t k = 0; k < count; ++k) {
+        const uint64_t tl = first + k;
+        if (tl >= ntiles) break;
+        const bool staged = tl < nfull;
+        uint8_t* stage = nullptr;
+        if (staged) {
+            bool landed = false;
+            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase);
+            landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
+            if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
+                if (lane == 0) {
+                    atomicOr(P0.err, kErrWaitTimeout);
+                    atomicExch(abort_flag, 1u);
+                }
+                return;
+            }
+            mbar_try_wait(&full[st.s], st.phase);
+            stage = stages + static_cast<size_t>(st.s) * P0.stage_bytes;
+        }
+#pragma unroll 1
+        for (uint32_t q = 0; q < np; ++q) {
+            const Plan& P = plans[q];
+            RegLeaves RL;
+            RegVals RV;
+            load_regs<MODE, ACC128, SH, true>(P, RL, RV);
+            if (staged)
+                process_tile<MODE, ACC128, NT, false, SH>(P, sinks[q], smem + P.extra_off, stage, tl, t, selected[q],
+                                                          RL, RV);
+            else
+                process_tile<MODE, ACC128, NT, true, SH>(P, sinks[q], smem + P.extra_off, nullptr, tl, t,
+                                                         selected[q], RL, RV);
+        }
+        if (staged) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st.s]);
+            ++st.n;
+            if (++st.s == S) {
+                st.s = 0;
+                st.phase ^= 1u;
+            }
+        }
+    }
+}
+
+template <uint32_t MODE, bool ACC128, int NT, class SH>
 __global__ void __launch_bounds__(NT + 32, 1) batch_kernel(const __grid_constant__ BatchDesc B) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + kMaxStages;
-    uint8_t* stages = smem + kBarrierBytes;
-    __shared__ __align__(16) Plan sP;
     __shared__ uint32_t abort_flag, s_morsel;
     const uint32_t t = threadIdx.x;
     if (t == 0) abort_flag = 0;
@@ -1558,42 +1626,48 @@ __global__ void __launch_bounds__(NT + 32, 1) batch_kernel(const __grid_constant
         const uint32_t mi = s_morsel;
         if (mi >= B.nmorsels || *reinterpret_cast<volatile uint32_t*>(&abort_flag)) break;
         const Morsel M = B.morsels[mi];
+        const uint32_t np = M.count;
+        // The group's plans go to shared memory (after the barriers, before
+        // the stage ring at plans[0].stage_off).
         {
-            const uint4* src = reinterpret_cast<const uint4*>(B.plans + M.query);
-            uint4* dst = reinterpret_cast<uint4*>(&sP);
-            for (uint32_t i = t; i < sizeof(Plan) / 16; i += blockDim.x) dst[i] = src[i];
+            const uint4* src = reinterpret_cast<const uint4*>(B.plans + M.first);
+            uint4* dst = reinterpret_cast<uint4*>(smem + kBarrierBytes);
+            const uint32_t words = np * static_cast<uint32_t>(sizeof(Plan) / 16);
+            for (uint32_t i = t; i < words; i += blockDim.x) dst[i] = src[i];
         }
         __syncthreads();
-        const Plan& P = sP;
-        uint8_t* extra = smem + P.extra_off;
-        Sink<MODE, ACC128, NT> sink;
-        if (t < static_cast<uint32_t>(NT)) sink.init(P, extra, t);
-        if (t == static_cast<uint32_t>(NT)) pipe_init_barriers(full, empty, P.nstages, NT / 32);
+        const Plan* plans = reinterpret_cast<const Plan*>(smem + kBarrierBytes);
+        const Plan& P0 = plans[0];
+        uint8_t* stages = smem + P0.stage_off;
+        Sink<MODE, ACC128, NT> sinks[kMaxShare];
+        if (t < static_cast<uint32_t>(NT))
+            for (uint32_t q = 0; q < np; ++q) sinks[q].init(plans[q], smem + plans[q].extra_off, t);
+        if (t == static_cast<uint32_t>(NT)) pipe_init_barriers(full, empty, P0.nstages, NT / 32);
         __syncthreads();
         PipeState st;
         const uint64_t count = M.tile_end - M.tile_begin;
         if (t == static_cast<uint32_t>(NT)) {
-            pipe_produce(P, full, empty, stages, M.tile_begin, 1, count, st, &abort_flag);
+            pipe_produce(P0, full, empty, stages, M.tile_begin, 1, count, st, &abort_flag);
             // Drain (a no-op unless the consumers gave up): no copy may still
             // be in flight when the barriers are invalidated.
-            const uint32_t S = P.nstages;
+            const uint32_t S = P0.nstages;
             for (uint64_t i = st.n > S ? st.n - S : 0; i < st.n; ++i)
-                if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P.err, kErrWaitTimeout);
+                if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P0.err, kErrWaitTimeout);
         } else if (t < static_cast<uint32_t>(NT)) {
-            RegLeaves RL;
-            RegVals RV;
-            load_regs<MODE, ACC128, void>(P, RL, RV);
-            unsigned long long selected = 0;
-            pipe_consume<MODE, ACC128, NT, void>(P, sink, extra, full, empty, stages, M.tile_begin, 1, count, st,
-                                                 &abort_flag, RL, RV, selected);
-            count_selected<NT>(P, selected);
-            sink.flush(P, extra, t);
+            unsigned long long selected[kMaxShare];
+            for (uint32_t q = 0; q < np; ++q) selected[q] = 0;
+            consume_group<MODE, ACC128, NT, SH>(plans, np, sinks, smem, full, empty, stages, M.tile_begin, count, st,
+                                                &abort_flag, selected);
+            for (uint32_t q = 0; q < np; ++q) {
+                count_selected<NT>(plans[q], selected[q]);
+                sinks[q].flush(plans[q], smem + plans[q].extra_off, t);
+            }
         }
-        // Every stage copy of this morsel was consumed: the barriers and the
-        // shared plan can be reused.
+        // Every stage copy of this morsel was consumed: the barriers can be
+        // re-initialized for the next morsel's layout.
         __syncthreads();
         if (t == static_cast<uint32_t>(NT))
-            for (uint32_t s = 0; s < P.nstages; ++s) {
+            for (uint32_t s = 0; s < P0.nstages; ++s) {
                 mbar_inval(&full[s]);
                 mbar_inval(&empty[s]);
             }
@@ -1660,6 +1734,17 @@ static const ShapeEntry* shape_table(uint32_t* n) {
     return table;
 }
 
+uint32_t scalar_shape_of(const Plan& P) {
+    if (!(P.count_by_tile && !P.check_ovf && P.jslot < 0 && P.ngkey == 0 && P.nval >= 1 && P.nval <= 2)) return 0;
+    for (uint32_t v = 0; v < P.nval; ++v) {
+        const ValDesc& D = P.val[v];
+        if (D.kind != VK_SUM || D.nf < 1 || D.nf > 2) return 0;
+        for (uint32_t f = 0; f < D.nf; ++f)
+            if (D.f[f].slot < 0) return 0;
+    }
+    return kShapeScalar;
+}
+
 uint32_t dense_shape_of(const Plan& P) {
     if (!P.dense_vec || P.chain.nsteps == 0) return 0;
     uint32_t code[kMaxSteps] = {};
@@ -1682,6 +1767,11 @@ uint32_t dense_shape_of(const Plan& P) {
 }
 
 static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t shape = 0) {
+    if (shape == kShapeScalar && mode == MODE_GROUP_PRIVATE && !acc128) {
+        return nt == 512 ? reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 512, ScalarTag>)
+             : nt == 256 ? reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 256, ScalarTag>)
+                         : nullptr;
+    }
     if (shape && mode == MODE_GROUP_PRIVATE && !acc128) {
         uint32_t n = 0;
         const ShapeEntry* tab = shape_table(&n);
@@ -1770,16 +1860,18 @@ int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t
 size_t scan_kernel_static_smem() { return 128; }
 
 // Batch launches (MODE_GROUP_PRIVATE plans): one persistent kernel per
-// (acc128, NT) class; the shared plan copy is static shared memory.
-size_t batch_kernel_static_smem() { return sizeof(Plan) + 128; }
+// (acc128, NT) class.
+size_t batch_kernel_static_smem() { return 16; }
 
+// The int64 kernels carry the fixed-shape dense path (plans with shape 1);
+// every other plan runs the interpreted paths.
 static const void* batch_kernel_ptr(bool acc128, int nt) {
     if (nt == 512)
-        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 512>)
-                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 512>);
+        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 512, void>)
+                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 512, ShapeQ1>);
     if (nt == 256)
-        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 256>)
-                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 256>);
+        return acc128 ? reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, true, 256, void>)
+                      : reinterpret_cast<const void*>(batch_kernel<MODE_GROUP_PRIVATE, false, 256, ShapeQ1>);
     return nullptr;
 }
 

@@ -537,6 +537,15 @@ class PreparedQuery:
         self.res = A.QueryResult()
         self._fn = table.ctx.lib.tgp_execute
 
+    def rebind(self, where: Pred | None) -> "PreparedQuery":
+        """Replaces the WHERE program (new literals or shape); the rest of the
+        lowered query and the output buffers are kept."""
+        nodes, n = self.table.lower_pred(where)
+        self.q.pred = nodes if nodes is not None else None
+        self.q.npred = n
+        self._keep = (nodes,) + tuple(self._keep[1:])
+        return self
+
     def _alloc(self, cap: int) -> None:
         self.cap = cap
         self.keys = np.zeros(max(1, cap * max(1, self.nk)), dtype=np.uint64)
