@@ -578,13 +578,15 @@ def main() -> None:
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
 
     def merge(out):
-        """Exact cross-rank merge of the partial int128 sum and count (NCCL all-gather)."""
+        """Exact cross-rank merge of the partial int128 sum and count: one NCCL
+        all-gather of three int64 words per rank (turbogp_b200.shard holds the
+        general merge of grouped results)."""
         if world == 1:
             return out.values[0][0].value, out.values[0][1].value
         import torch.distributed as dist
         s, c = out.values[0][0].value, out.values[0][1].value
-        mine = torch.tensor([s & 0xFFFFFFFFFFFFFFFF, s >> 64, c], dtype=torch.int64, device="cuda")
-        mine[0] = torch.tensor(np.array([s & 0xFFFFFFFFFFFFFFFF], dtype=np.uint64).view(np.int64)[0])
+        lo = int(np.array([s & 0xFFFFFFFFFFFFFFFF], dtype=np.uint64).view(np.int64)[0])
+        mine = torch.tensor([lo, s >> 64, c], dtype=torch.int64, device="cuda")
         parts = [torch.empty_like(mine) for _ in range(world)]
         dist.all_gather(parts, mine)
         tot_s, tot_c = 0, 0

@@ -816,6 +816,7 @@ int tgp_init(tgp_ctx** out, int device) {
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_NO_SHARED_SCANS")) ctx->shared_scans = std::atoi(e) == 0;
+    if (const char* e = std::getenv("TGP_SHARE_EXTRA_MAX")) ctx->share_extra_max = static_cast<size_t>(std::atoll(e));
     if (const char* e = std::getenv("TGP_BATCH_MORSEL_TILES")) ctx->morsel_tiles = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("TGP_NO_HASH_PRESUM")) ctx->hash_presum = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
@@ -1677,6 +1678,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         uint32_t nt;
         std::vector<uint32_t> q;
         size_t extra = 0;
+        bool light = true;
     };
     std::vector<Group> groups;
     std::unordered_map<uint64_t, std::vector<uint32_t>> by_table;
@@ -1697,7 +1699,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         const bool share = ctx->shared_scans && qi.size() > 1 && cols.size() <= static_cast<size_t>(kMaxSlots);
         for (uint32_t i : qi) {
             QueryState& qs = B->qs[i];
-            if (share) {
+            if (share && ((qs.extra + 127) & ~size_t{127}) <= ctx->share_extra_max) {
                 QueryState re;
                 if (plan_query(ctx, items[i].query, re, bstatic, &cols) == TGP_OK && re.mode == MODE_GROUP_PRIVATE)
                     qs = std::move(re);
@@ -1707,16 +1709,20 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             P.shape = (!qs.acc128 && !qs.J && P.dense_vec && ctx->dense_shapes && dense_shape_of(P) == 1) ? 1u : 0u;
             const size_t extra = (qs.extra + 127) & ~size_t{127};
             Group* g = nullptr;
-            if (share)
+            // Plans with a large accumulator table (dense grouping, joins) are
+            // compute-bound: they run in their own group, whose layout keeps
+            // the most stages and threads; light plans share scans.
+            const bool light = extra <= ctx->share_extra_max;
+            if (share && light)
                 for (auto& k : groups)
-                    if (k.acc128 == qs.acc128 && k.nt == P.nthreads && k.q.size() < static_cast<size_t>(kMaxShare) &&
+                    if (k.light && k.acc128 == qs.acc128 && k.nt == P.nthreads && k.q.size() < static_cast<size_t>(kMaxShare) &&
                         items[k.q[0]].query->table == tid &&
                         B->qs[k.q[0]].b->P.stage_bytes == P.stage_bytes &&
                         k.extra + extra + (k.q.size() + 1) * sizeof(Plan) + 2ull * P.stage_bytes + kBarrierBytes + 256 <=
                             budget)
                         g = &k;
             if (!g) {
-                groups.push_back(Group{qs.acc128, P.nthreads});
+                groups.push_back(Group{qs.acc128, P.nthreads, {}, 0, light});
                 g = &groups.back();
             }
             g->q.push_back(i);

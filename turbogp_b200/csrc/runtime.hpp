@@ -138,7 +138,7 @@ struct tgp_ctx {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS).
+    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS, TGP_SHARE_EXTRA_MAX).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
     int max_stages = tgp::kMaxStages;
@@ -147,6 +147,7 @@ struct tgp_ctx {
     bool join_payload = true;  // unique-key join payload arrays (TGP_NO_JOIN_PAYLOAD=1 turns them off)
     bool hash_presum = true;   // shared pre-aggregation for hash grouping (TGP_NO_HASH_PRESUM=1 turns it off)
     int morsel_tiles = 16;     // batch morsel length in tiles (TGP_BATCH_MORSEL_TILES)
-    bool shared_scans = true;  // batches merge same-table queries into shared scans (TGP_NO_SHARED_SCANS=1: off)
+    bool shared_scans = true;
+    size_t share_extra_max = 32768;  // largest accumulator region of a plan that joins a shared scan (TGP_SHARE_EXTRA_MAX)  // batches merge same-table queries into shared scans (TGP_NO_SHARED_SCANS=1: off)
     bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
 };
