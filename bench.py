@@ -506,7 +506,7 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     serving.serve_plain(ctx, templates, stream(rate, 16))
     with ClockSampler(local) as clocks:
         batched = serving.serve_batched(ctx, templates, stream(rate, count), mem_budget=args.mem_budget)
-    plain = serving.serve_plain(ctx, templates, stream(rate, max(32, count // 8)))
+    plain = serving.serve_plain(ctx, templates, stream(rate, count))
     peak, peak_kind = peak_hbm()
     line = {
         "metric": METRIC, "value": batched.get("qps"), "unit": "queries/s", "n_gpus": world,

@@ -270,16 +270,20 @@ def test_join_payload_and_hash_probe_paths(ctx):
 
 
 def test_hash_grouping_hot_keys_and_device_format(ctx):
-    """Hash grouping over Zipf keys (shared pre-aggregation of hot keys, then
-    the global table), multi-key packed tuples, results sorted and formatted
-    on the device; large values switch the pre-aggregation off."""
+    """Zipf keys through direct global grouping and hash grouping (shared
+    pre-aggregation of hot keys in both, then the global tables), multi-key
+    tuples, hash results sorted and formatted on the device; large values
+    switch the pre-aggregation off."""
     n = 2_000_003
     h = datagen.highcard(n, 200_000, 1.1, seed=9)
     rng = np.random.default_rng(3)
     h["k2"] = rng.integers(-3, 4, n, dtype=np.int32)
     h["big"] = rng.integers(-2**40, 2**40, n, dtype=np.int64)
+    h["wide"] = h["key"] * 50          # a key range past the direct-indexed limit: hash grouping
     t = ctx.register(h)
     cases = [
+        ([count_star(), sum_(col("value")), count_col(col("value"))], ("wide",), None),
+        ([count_star(), sum_(col("big"))], ("wide",), col("value") < 700),
         ([count_star(), sum_(col("value")), avg(col("value")), count_col(col("value"))], ("key",), None),
         ([count_star(), sum_((col("value") - 7) * 3)], ("key", "k2"), col("value") < 900),
         ([sum_(col("big")), count_star(), min_(col("value"))], ("key",), None),

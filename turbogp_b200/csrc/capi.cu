@@ -1356,10 +1356,12 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         P.hstride = 2 + 2 * P.nval;
         P.hlog2 = log2u(hcap);
         P.hmask = hcap - 1;
-        // Shared pre-aggregation of repeated keys: SUM / COUNT(col) values,
-        // no join, no per-row overflow checks; its i32 partials are bounded
-        // below once the launch grid is known.
-        bool presum = ctx->hash_presum && !join && !P.check_ovf;
+    }
+    // Shared pre-aggregation of repeated keys (hash and global direct
+    // grouping): SUM / COUNT(col) values, no join, no per-row overflow checks;
+    // its i32 partials are bounded once the launch grid is known.
+    if (mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) {
+        bool presum = ctx->hash_presum && !join && !P.check_ovf && !acc128;
         for (uint32_t v = 0; presum && v < P.nval; ++v)
             presum = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
         const uint32_t HS = 4096;
@@ -1373,6 +1375,19 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     }
 
     return TGP_OK;
+}
+
+// Keeps the shared pre-aggregation only when, at the grid launch() uses, no
+// CTA scans enough rows for an i32 partial to reach 2^31 in magnitude.
+static void bound_presum(tgp_ctx* ctx, QueryState& qs) {
+    Plan& P = qs.b->P;
+    if (!P.hsm_slots) return;
+    const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
+    const int occ = scan_occupancy(qs.mode, qs.acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * std::max(occ, 1)));
+    const unsigned __int128 rows_cta = static_cast<unsigned __int128>((ntiles + grid - 1) / grid) * kTileRows;
+    const unsigned __int128 bound = rows_cta * std::max<uint64_t>(qs.b->max_abs_val, 1);
+    if (bound >= (static_cast<unsigned __int128>(1) << 31)) P.hsm_slots = 0;
 }
 
 // Fills the caller's outputs of a direct-indexed / scalar query from a host
@@ -1485,16 +1500,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         }
     }
     TGP_TRY(size_smem(ctx, P, extra));
-    if (P.hsm_slots) {
-        // Rows one CTA scans, at the grid launch() uses: each i32 partial
-        // stays below 2^31 in magnitude.
-        const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
-        const int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
-        const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * std::max(occ, 1)));
-        const unsigned __int128 rows_cta = static_cast<unsigned __int128>((ntiles + grid - 1) / grid) * kTileRows;
-        const unsigned __int128 bound = rows_cta * std::max<uint64_t>(b.max_abs_val, 1);
-        if (bound >= (static_cast<unsigned __int128>(1) << 31)) P.hsm_slots = 0;
-    }
+    bound_presum(ctx, qs);
     TGP_TRY(launch(ctx, P, mode, acc128));
 
     TGP_TRY(pinned_reserve(ctx, block_words * 8));
@@ -1654,21 +1660,53 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     B->block_off.assign(n, 0);
     const size_t bstatic = batch_kernel_static_smem();
     const size_t budget = ctx->max_dyn_smem - bstatic;
-    // 1. Plan alone; the persistent kernel takes the direct-indexed / scalar
-    // plans, everything else runs now, one query at a time.
-    std::vector<uint32_t> take;
+    // 1. Plan each query as tgp_execute would. Hash grouping runs now, alone
+    // (its result size is only known after the scan). A direct-indexed query
+    // goes to the persistent kernel when it is small (a launch of its own
+    // would leave most SMs idle) or shares its table with other light
+    // queries (a shared scan); every other one gets a launch of its own in
+    // this batch's stream, with no synchronization between queries.
+    std::vector<uint32_t> take, solo;
+    const uint64_t small_tiles = static_cast<uint64_t>(ctx->sms) * 4;
+    std::unordered_map<uint64_t, uint32_t> light_per_table;
     for (uint32_t i = 0; i < n; ++i) {
         tgp_batch_item& it = items[i];
         std::memset(&it.result, 0, sizeof(it.result));
         it.status = TGP_OK;
         QueryState& qs = B->qs[i];
-        int st = plan_query(ctx, it.query, qs, bstatic);
-        if (st == TGP_OK && qs.mode == MODE_GROUP_PRIVATE) {
-            take.push_back(i);
+        int st = plan_query(ctx, it.query, qs, scan_kernel_static_smem());
+        if (st == TGP_OK && qs.mode != MODE_GROUP_HASH) {
+            if (qs.mode == MODE_GROUP_PRIVATE && ((qs.extra + 127) & ~size_t{127}) <= ctx->share_extra_max)
+                ++light_per_table[it.query->table];
             continue;
         }
         if (st == TGP_OK) st = tgp_execute(ctx, it.query, it.keys_out, it.vals_out, it.group_cap, &it.result);
         it.status = st;
+        B->qs[i].b.reset();
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        QueryState& qs = B->qs[i];
+        if (!qs.b) continue;
+        const uint64_t T = (qs.b->P.nrows + kTileRows - 1) / kTileRows;
+        const bool light = qs.mode == MODE_GROUP_PRIVATE && ((qs.extra + 127) & ~size_t{127}) <= ctx->share_extra_max;
+        const bool shared = ctx->shared_scans && light && light_per_table[items[i].query->table] > 1;
+        if (qs.mode == MODE_GROUP_PRIVATE && (T < small_tiles || shared)) {
+            QueryState re;
+            if (plan_query(ctx, items[i].query, re, bstatic) == TGP_OK && re.mode == MODE_GROUP_PRIVATE) {
+                qs = std::move(re);
+                take.push_back(i);
+                continue;
+            }
+        }
+        const int sst = size_smem(ctx, qs.b->P, qs.extra);
+        if (sst == TGP_OK) bound_presum(ctx, qs);
+        if (sst != TGP_OK) {
+            items[i].status = tgp_execute(ctx, items[i].query, items[i].keys_out, items[i].vals_out, items[i].group_cap,
+                                          &items[i].result);
+            qs.b.reset();
+            continue;
+        }
+        solo.push_back(i);
     }
     // 2. Shared scans: queries over one table are re-planned over the union of
     // their columns (when it fits the stage's slots) and packed into groups
@@ -1752,12 +1790,15 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     }
     uint32_t nplans = 0;
     std::vector<uint32_t> plan_index(n, 0);
+    std::vector<uint8_t> in_group(n, 0);
     for (const Group& g : groups)
         for (uint32_t i : g.q) {
             B->batched[i] = 1;
+            in_group[i] = 1;
             plan_index[i] = nplans++;
         }
-    if (nplans == 0) {
+    for (uint32_t i : solo) B->batched[i] = 1;
+    if (nplans == 0 && solo.empty()) {
         const uint64_t id = ctx->next_id++;
         ctx->batches.emplace(id, B.release());
         *out = id;
@@ -1841,13 +1882,15 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             init_acc_image(P, B->qs[i].ngroups_direct, &img);
             std::memcpy(h + blocks_off + B->block_off[i] + 48, img.data(), img.size() * 8);
         }
-        hplans[plan_index[i]] = P;
+        if (in_group[i]) hplans[plan_index[i]] = P;
     }
     for (size_t k = 0; k < classes.size(); ++k)
         if (!classes[k].morsels.empty())
             std::memcpy(h + morsel_off[k], classes[k].morsels.data(), classes[k].morsels.size() * sizeof(Morsel));
-    // 6. One upload, the persistent launches, one readback.
+    // 6. One upload, the queries with launches of their own, the persistent
+    // launches, one readback.
     TGP_CUDA(cudaMemcpyAsync(B->dev, h, total, cudaMemcpyHostToDevice, ctx->stream));
+    for (uint32_t i : solo) TGP_TRY(launch(ctx, B->qs[i].b->P, B->qs[i].mode, B->qs[i].acc128));
     for (size_t k = 0; k < classes.size(); ++k) {
         const Class& c = classes[k];
         if (c.morsels.empty()) continue;

@@ -482,6 +482,38 @@ __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, ui
     return nullptr;
 }
 
+// This CTA's shared pre-aggregation table (P.hsm_slots slots: u64 keys,
+// u32 counts, i32 partials per value) absorbs repeated (hot) keys with native
+// 32-bit shared atomics. Returns false when the key found no slot within
+// kSmemProbes probes (the caller updates the global table instead). The host
+// proves that no partial can pass 2^31 in magnitude.
+template <bool TAIL>
+__device__ __forceinline__ bool presum_add(const Plan& P, uint8_t* extra, uint64_t key, const uint8_t* stage,
+                                           uint64_t r0, uint32_t rl, uint32_t brow, uint32_t& ovf) {
+    const uint32_t HS = P.hsm_slots;
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
+    int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
+    uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
+#pragma unroll 1
+    for (uint32_t n = 0; n < kSmemProbes; ++n) {
+        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
+        if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
+        if (k == kEmpty || k == key) {
+            atomicAdd(&cnt[h], 1u);
+#pragma unroll 1
+            for (uint32_t v = 0; v < P.nval; ++v) {
+                const ValDesc& V = P.val[v];
+                const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
+                atomicAdd(&sums[v * HS + h], static_cast<int32_t>(V.kind == VK_COUNT_NZ ? (x != 0) : x));
+            }
+            return true;
+        }
+        h = (h + 1) & (HS - 1);
+    }
+    return false;
+}
+
 template <uint32_t MODE, bool ACC128, int NT>
 struct Sink {
     uint32_t ovf;
@@ -507,7 +539,7 @@ struct Sink {
                 w[2 * i] = kind_identity(slot_kind(P, i % nv1));
                 w[2 * i + 1] = 0;
             }
-        } else if (MODE == MODE_GROUP_HASH && P.hsm_slots) {
+        } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             const uint32_t HS = P.hsm_slots;
             unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
             uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
@@ -613,6 +645,7 @@ struct Sink {
             }
         } else if (MODE == MODE_GROUP_GLOBAL) {
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
+            if (P.hsm_slots && presum_add<TAIL>(P, extra, g, stage, r0, rl, brow, ovf)) return;
             unsigned long long* a = P.acc + static_cast<uint64_t>(g) * nv1 * 2;
             atomicAdd(a, 1ull);
 #pragma unroll 1
@@ -622,31 +655,7 @@ struct Sink {
             }
         } else if (MODE == MODE_GROUP_HASH) {
             const uint64_t key = group_hash_key<TAIL>(P, stage, r0, rl, brow);
-            if (P.hsm_slots) {
-                // This CTA's shared pre-aggregation table absorbs repeated
-                // (hot) keys with native 32-bit shared atomics.
-                const uint32_t HS = P.hsm_slots;
-                unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
-                uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
-                int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
-                uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
-#pragma unroll 1
-                for (uint32_t n = 0; n < kSmemProbes; ++n) {
-                    unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
-                    if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
-                    if (k == kEmpty || k == key) {
-                        atomicAdd(&cnt[h], 1u);
-#pragma unroll 1
-                        for (uint32_t v = 0; v < P.nval; ++v) {
-                            const ValDesc& V = P.val[v];
-                            const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                            atomicAdd(&sums[v * HS + h], static_cast<int32_t>(V.kind == VK_COUNT_NZ ? (x != 0) : x));
-                        }
-                        return;
-                    }
-                    h = (h + 1) & (HS - 1);
-                }
-            }
+            if (P.hsm_slots && presum_add<TAIL>(P, extra, key, stage, r0, rl, brow, ovf)) return;
             unsigned long long* slot = hash_group_slot(P, key);
             if (slot == nullptr) return;
             atomicAdd(slot + 1, 1ull);
@@ -716,7 +725,7 @@ struct Sink {
                 a.hi = w[2 * idx + 1];
                 if (!acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
             }
-        } else if (MODE == MODE_GROUP_HASH && P.hsm_slots) {
+        } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             consumer_sync<NT>();
             const uint32_t HS = P.hsm_slots;
             const unsigned long long* keys = reinterpret_cast<const unsigned long long*>(extra);
@@ -725,15 +734,26 @@ struct Sink {
             for (uint32_t i = t; i < HS; i += NT) {
                 const unsigned long long key = keys[i];
                 if (key == kEmpty) continue;
-                unsigned long long* slot = hash_group_slot(P, key);
-                if (slot == nullptr) continue;
-                atomicAdd(slot + 1, static_cast<unsigned long long>(cnt[i]));
+                // Hash slots are [key][count][v0 lo][v0 hi]...; direct
+                // accumulators are [count lo][count hi][v0 lo][v0 hi]...
+                unsigned long long* base;
+                uint32_t vofs;
+                if (MODE == MODE_GROUP_HASH) {
+                    unsigned long long* slot = hash_group_slot(P, key);
+                    if (slot == nullptr) continue;
+                    base = slot + 1;
+                    vofs = 1;
+                } else {
+                    base = P.acc + key * (P.nval + 1) * 2;
+                    vofs = 2;
+                }
+                atomicAdd(base, static_cast<unsigned long long>(cnt[i]));
                 for (uint32_t v = 0; v < P.nval; ++v) {
                     const int64_t x = sums[v * HS + i];
                     I128 a;
                     a.lo = static_cast<uint64_t>(x);
                     a.hi = x >> 63;
-                    atomic_add_i128(slot + 2 + 2 * v, a);
+                    atomic_add_i128(base + vofs + 2 * v, a);
                 }
             }
         }
