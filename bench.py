@@ -501,7 +501,9 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
         return [request(t) for t in serving.poisson_arrivals(rate, count, rng)]
 
     rate, count = args.rate, args.requests
-    # Warm-up: every template through both paths.
+    # Warm-up: every template's prepared queries built and sized (the
+    # high-cardinality one included), then both paths once.
+    serving.prewarm(templates, [request(0.0) for _ in range(2000)], per_template=3)
     serving.serve_batched(ctx, templates, stream(rate, 64), mem_budget=args.mem_budget)
     serving.serve_plain(ctx, templates, stream(rate, 16))
     with ClockSampler(local) as clocks:

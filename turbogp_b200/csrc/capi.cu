@@ -1882,7 +1882,10 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             init_acc_image(P, B->qs[i].ngroups_direct, &img);
             std::memcpy(h + blocks_off + B->block_off[i] + 48, img.data(), img.size() * 8);
         }
-        if (in_group[i]) hplans[plan_index[i]] = P;
+        if (in_group[i]) {
+            fill_reg_block(P);
+            hplans[plan_index[i]] = P;
+        }
     }
     for (size_t k = 0; k < classes.size(); ++k)
         if (!classes[k].morsels.empty())

@@ -150,6 +150,27 @@ struct GKey {
     uint64_t stride;      // direct modes: multiplier of (cell - min) in the group index
 };
 
+// Register images the scan kernel loads once per plan (host-computed, so a
+// load is a few independent reads instead of dependent field walks): a
+// conjunction of up to four int32 leaves, and the scalar fast path's values
+// (one or two SUMs of one or two staged affine factors).
+constexpr int kRegLeaves = 4;
+struct alignas(16) RegBlock {
+    uint32_t leaf_n;                // 0 = the register leaves do not apply
+    uint32_t leaf_neg;              // bit i: leaf i negated
+    uint32_t leaf_soff[kRegLeaves];
+    uint32_t leaf_lo[kRegLeaves];
+    uint32_t leaf_sp[kRegLeaves];
+    uint32_t vals_on;               // scalar fast path applies (MODE_GROUP_PRIVATE, int64)
+    uint32_t vals_nv;
+    uint32_t vals_nf[2];
+    uint32_t vals_soff[2][2];
+    uint32_t vals_dt[2][2];
+    uint32_t _pad[2];
+    int64_t vals_mul[2][2];
+    int64_t vals_add[2][2];
+};
+
 struct alignas(16) Plan {
     uint64_t nrows;
     uint32_t nslots;
@@ -220,6 +241,7 @@ struct alignas(16) Plan {
     unsigned long long* out_pairs;  // MODE_JOIN_PAIRS: (probe_row << 32) | build_row
     uint64_t out_cap;
     uint64_t _pad_end;              // sizeof(Plan) is a multiple of 16
+    RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 
 // Build-side group keys folded into a join payload array.

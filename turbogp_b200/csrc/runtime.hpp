@@ -27,6 +27,9 @@ uint32_t dense_shape_of(const Plan& P);
 // kShapeScalar when the plan is a scalar aggregate the register fast path
 // takes (one or two SUMs of one or two staged factors, bounded), else 0.
 uint32_t scalar_shape_of(const Plan& P);
+// Fills P.rb (the register images the kernels load) from the rest of the plan;
+// every launch path calls it once the plan is final.
+void fill_reg_block(Plan& P);
 size_t scan_kernel_static_smem();
 size_t batch_kernel_static_smem();
 int batch_occupancy(bool acc128, int nt, size_t dyn_smem);

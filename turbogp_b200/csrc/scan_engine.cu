@@ -200,7 +200,6 @@ __device__ __forceinline__ uint32_t leaf_i32(const Leaf& L, const uint8_t* stage
 
 // A conjunction of at most kRegLeaves I32 leaves, kept in registers for the
 // whole kernel (no constant-bank loads per tile).
-constexpr int kRegLeaves = 4;
 struct RegLeaves {
     uint32_t n;       // 0 = not applicable
     uint32_t neg;     // bit i: leaf i negated
@@ -210,15 +209,13 @@ struct RegLeaves {
 };
 
 __device__ __forceinline__ void load_reg_leaves(const Plan& P, RegLeaves& L) {
-    L.n = (P.all_and && P.nleaf <= kRegLeaves && P.kend[0] == P.nleaf) ? P.nleaf : 0u;
-    L.neg = 0;
+    L.n = P.rb.leaf_n;
+    L.neg = P.rb.leaf_neg;
 #pragma unroll
     for (int i = 0; i < kRegLeaves; ++i) {
-        const bool use = static_cast<uint32_t>(i) < L.n;
-        L.soff[i] = use ? P.slot[P.leaf[i].slot].smem_off : 0u;
-        L.lo[i] = use ? P.leaf[i].lo32 : 0u;
-        L.sp[i] = use ? P.leaf[i].span32 : 0u;
-        if (use && P.leaf[i].negate) L.neg |= 1u << i;
+        L.soff[i] = P.rb.leaf_soff[i];
+        L.lo[i] = P.rb.leaf_lo[i];
+        L.sp[i] = P.rb.leaf_sp[i];
     }
 }
 
@@ -778,27 +775,20 @@ struct RegVals {
 
 template <uint32_t MODE, bool ACC128>
 __device__ __forceinline__ void load_reg_vals(const Plan& P, RegVals& V) {
-    bool on = MODE == MODE_GROUP_PRIVATE && !ACC128 && P.count_by_tile && !P.check_ovf && P.jslot < 0 &&
-              P.ngkey == 0 && P.nval >= 1 && P.nval <= 2;
-    V.nv = P.nval;
+    const RegBlock& B = P.rb;
+    V.on = (MODE == MODE_GROUP_PRIVATE && !ACC128) ? B.vals_on : 0u;
+    V.nv = B.vals_nv;
 #pragma unroll
     for (int v = 0; v < 2; ++v) {
-        const bool use = static_cast<uint32_t>(v) < P.nval;
-        const ValDesc& D = P.val[use ? v : 0];
-        if (use && (D.kind != VK_SUM || D.nf < 1 || D.nf > 2)) on = false;
-        V.nf[v] = use ? D.nf : 0u;
+        V.nf[v] = B.vals_nf[v];
 #pragma unroll
         for (int f = 0; f < 2; ++f) {
-            const bool uf = use && static_cast<uint32_t>(f) < D.nf;
-            const Factor& F = D.f[uf ? f : 0];
-            if (uf && F.slot < 0) on = false;
-            V.soff[v][f] = uf ? F.soff : 0u;
-            V.dt[v][f] = uf ? F.dtype : static_cast<uint32_t>(DT_I64);
-            V.mul[v][f] = uf ? F.mul : 0;
-            V.add[v][f] = uf ? F.add : 1;  // an absent factor multiplies by 1
+            V.soff[v][f] = B.vals_soff[v][f];
+            V.dt[v][f] = B.vals_dt[v][f];
+            V.mul[v][f] = B.vals_mul[v][f];
+            V.add[v][f] = B.vals_add[v][f];
         }
     }
-    V.on = on ? 1u : 0u;
 }
 
 __device__ __forceinline__ int64_t fast_factor(const uint8_t* stage, uint32_t soff, uint32_t dt, int64_t mul,
@@ -1754,6 +1744,36 @@ static const ShapeEntry* shape_table(uint32_t* n) {
     return table;
 }
 
+void fill_reg_block(Plan& P) {
+    RegBlock& B = P.rb;
+    B = RegBlock{};
+    B.leaf_n = (P.all_and && P.nleaf <= kRegLeaves && P.kend[0] == P.nleaf) ? P.nleaf : 0u;
+    for (uint32_t i = 0; i < B.leaf_n; ++i) {
+        B.leaf_soff[i] = P.slot[P.leaf[i].slot].smem_off;
+        B.leaf_lo[i] = P.leaf[i].lo32;
+        B.leaf_sp[i] = P.leaf[i].span32;
+        if (P.leaf[i].negate) B.leaf_neg |= 1u << i;
+    }
+    bool on = P.count_by_tile && !P.check_ovf && P.jslot < 0 && P.ngkey == 0 && P.nval >= 1 && P.nval <= 2;
+    B.vals_nv = P.nval;
+    for (int v = 0; v < 2; ++v) {
+        const bool use = static_cast<uint32_t>(v) < P.nval;
+        const ValDesc& D = P.val[use ? v : 0];
+        if (use && (D.kind != VK_SUM || D.nf < 1 || D.nf > 2)) on = false;
+        B.vals_nf[v] = use ? D.nf : 0u;
+        for (int f = 0; f < 2; ++f) {
+            const bool uf = use && static_cast<uint32_t>(f) < D.nf;
+            const Factor& F = D.f[uf ? f : 0];
+            if (uf && F.slot < 0) on = false;
+            B.vals_soff[v][f] = uf ? F.soff : 0u;
+            B.vals_dt[v][f] = uf ? F.dtype : static_cast<uint32_t>(DT_I64);
+            B.vals_mul[v][f] = uf ? F.mul : 0;
+            B.vals_add[v][f] = uf ? F.add : 1;  // an absent factor multiplies by 1
+        }
+    }
+    B.vals_on = on ? 1u : 0u;
+}
+
 uint32_t scalar_shape_of(const Plan& P) {
     if (!(P.count_by_tile && !P.check_ovf && P.jslot < 0 && P.ngkey == 0 && P.nval >= 1 && P.nval <= 2)) return 0;
     for (uint32_t v = 0; v < P.nval; ++v) {
@@ -1847,8 +1867,11 @@ cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cud
         const cudaError_t e = ensure_smem_limit(kernel_entry(f), f, static_cast<int>(P.smem_bytes));
         if (e != cudaSuccess) return e;
     }
-    void* args[] = {const_cast<Plan*>(&P)};
-    return cudaLaunchKernel(f, dim3(grid), dim3(P.nthreads + 32), args, P.smem_bytes, st);
+    // The register images are derived here, once the plan is final.
+    Plan L = P;
+    fill_reg_block(L);
+    void* args[] = {&L};
+    return cudaLaunchKernel(f, dim3(grid), dim3(L.nthreads + 32), args, L.smem_bytes, st);
 }
 
 int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape) {

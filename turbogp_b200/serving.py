@@ -46,6 +46,21 @@ class Template:
         self.pool.append(pq)
 
 
+def prewarm(templates: dict[str, Template], requests: list[Request], per_template: int = 3) -> None:
+    """Creates and runs ``per_template`` prepared queries of every template
+    (one request's predicate each), so that the timed run neither builds
+    prepared queries nor grows their output buffers (a high-cardinality
+    GROUP BY resizes them to its group count on first use)."""
+    for name, tpl in templates.items():
+        sample = next((r for r in requests if r.template == name), None)
+        where = sample.where if sample is not None else None
+        pqs = [tpl.take() for _ in range(per_template)]
+        for pq in pqs:
+            pq.rebind(where).run(decode=False)
+        for pq in pqs:
+            tpl.give(pq)
+
+
 def poisson_arrivals(rate: float, n: int, rng: np.random.Generator) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate, n))
 
