@@ -1271,26 +1271,35 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             stride *= dom[k];
         }
         acc128 = b.unbounded;
-        const size_t per_thread = static_cast<size_t>(ngroups_direct) * nv1 * 8 * (acc128 ? 2 : 1);
+        // Per-thread private accumulators: int128 partials, or u32 row counts
+        // and int64 values.
+        auto private_bytes = [&](uint32_t nt) -> size_t {
+            if (acc128) return static_cast<size_t>(ngroups_direct) * nv1 * 16 * nt;
+            return priv_count_bytes(static_cast<uint32_t>(ngroups_direct), nt) +
+                   static_cast<size_t>(ngroups_direct) * P.nval * 8 * nt;
+        };
         const size_t shared_tab = static_cast<size_t>(ngroups_direct) * nv1 * 16;
         const size_t budget = ctx->max_dyn_smem - static_smem - kBarrierBytes;
-        // Per-thread private accumulators: 512 threads when two stages still
-        // fit beside them, else 256 threads (twice the rows per thread).
+        // 512 threads when two stages still fit beside them, else 256 threads
+        // (twice the rows per thread).
         uint32_t nt = 0;
-        for (uint32_t cand : {static_cast<uint32_t>(ctx->scan_threads), 256u}) {
-            if (per_thread * cand + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
-                nt = cand;
-                break;
+        if (ngroups_direct * static_cast<uint64_t>(nv1) * 512 < (1ull << 31))
+            for (uint32_t cand : {static_cast<uint32_t>(ctx->scan_threads), 256u}) {
+                if (private_bytes(cand) + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+                    nt = cand;
+                    break;
+                }
             }
-        }
         if (nt) {
             mode = MODE_GROUP_PRIVATE;
             P.nthreads = nt;
             P.count_by_tile = (q->ngroup == 0 && !J) ? 1u : 0u;
-            extra = per_thread * nt;
+            extra = private_bytes(nt);
             if (!acc128) {
+                // Flush before an int64 value partial could wrap or a u32 row
+                // count could pass 2^32.
                 const uint64_t lim = b.max_abs_val ? (0x7fffffffffffffffull / b.max_abs_val) : ~0ull;
-                P.flush_limit = std::max<uint64_t>(1, lim);
+                P.flush_limit = std::min<uint64_t>(std::max<uint64_t>(1, lim), 0xffffffffull);
             }
             // Dense column program: int64 partials, no join, no per-row
             // overflow checks.

@@ -54,6 +54,9 @@ __device__ __forceinline__ unsigned long long lds_u64(uint32_t a) {
     asm volatile("ld.shared.u64 %0, [%1+%2];" : "=l"(v) : "r"(a), "n"(OFF));
     return v;
 }
+__device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v) {
+    asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
 template <uint32_t OFF>
 __device__ __forceinline__ void sts_u64(uint32_t a, unsigned long long v) {
     asm volatile("st.shared.u64 [%0+%1], %2;" ::"r"(a), "n"(OFF), "l"(v) : "memory");

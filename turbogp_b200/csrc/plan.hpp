@@ -297,6 +297,13 @@ TGP_HD inline double i128_to_f64_rn(uint64_t lo, int64_t hi) {
     return neg ? -d : d;
 }
 
+// MODE_GROUP_PRIVATE with int64 partials keeps, per consumer thread, u32 row
+// counts [group][thread] followed (16-byte aligned) by int64 values
+// [group][value][thread]. Bytes of the count array:
+TGP_HD inline uint32_t priv_count_bytes(uint32_t ngroups, uint32_t nt) {
+    return (ngroups * nt * 4u + 15u) & ~15u;
+}
+
 // Output layout of hash-grouped results (tgp_execute with hash grouping).
 constexpr int kMaxFormatAggs = 32;
 struct HashFormat {

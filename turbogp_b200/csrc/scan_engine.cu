@@ -452,7 +452,9 @@ __device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t
 // ---------------------------------------------------------------------------
 // Sinks. Shared-memory scratch layouts (nv1 = 1 + nval; value slot 0 is the
 // group's row count):
-//   MODE_GROUP_PRIVATE, int64 partials:  word (g * nv1 + v) * NT + t
+//   MODE_GROUP_PRIVATE, int64 partials:  u32 counts [g * NT + t], then (at
+//                                        priv_count_bytes) int64 values
+//                                        [(g * nval + v - 1) * NT + t]
 //   MODE_GROUP_PRIVATE, int128 partials: words ((g * nv1 + v) * 2 + limb) * NT + t
 //   MODE_GROUP_SHARED:                   words (g * nv1 + v) * 2 + limb (carry atomics)
 // MODE_SCALAR runs as MODE_GROUP_PRIVATE with a single group.
@@ -461,6 +463,12 @@ __device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t
 template <int NT>
 __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
+
+__device__ __forceinline__ uint32_t* priv_counts(uint8_t* extra) { return reinterpret_cast<uint32_t*>(extra); }
+template <int NT>
+__device__ __forceinline__ long long* priv_values(const Plan& P, uint8_t* extra) {
+    return reinterpret_cast<long long*>(extra + priv_count_bytes(P.ngroups, NT));
 }
 
 // Slot of `key` in the global group hash table (inserted if absent), or null
@@ -521,16 +529,16 @@ struct Sink {
         upd = 0;
         const uint32_t nv1 = P.nval + 1;
         long long* w = reinterpret_cast<long long*>(extra);
-        if (MODE == MODE_GROUP_PRIVATE) {
+        if (MODE == MODE_GROUP_PRIVATE && ACC128) {
             for (uint32_t i = 0; i < P.ngroups * nv1; ++i) {
-                const long long init = kind_identity(slot_kind(P, i % nv1));
-                if (ACC128) {
-                    w[(i * 2 + 0) * NT + t] = init;
-                    w[(i * 2 + 1) * NT + t] = 0;
-                } else {
-                    w[i * NT + t] = init;
-                }
+                w[(i * 2 + 0) * NT + t] = kind_identity(slot_kind(P, i % nv1));
+                w[(i * 2 + 1) * NT + t] = 0;
             }
+        } else if (MODE == MODE_GROUP_PRIVATE) {
+            uint32_t* cnt = priv_counts(extra);
+            long long* val = priv_values<NT>(P, extra);
+            for (uint32_t g = 0; g < P.ngroups; ++g) cnt[g * NT + t] = 0;
+            for (uint32_t i = 0; i < P.ngroups * P.nval; ++i) val[i * NT + t] = kind_identity(P.val[i % P.nval].kind);
         } else if (MODE == MODE_GROUP_SHARED) {
             for (uint32_t i = t; i < P.ngroups * nv1; i += NT) {
                 w[2 * i] = kind_identity(slot_kind(P, i % nv1));
@@ -553,16 +561,25 @@ struct Sink {
     // accumulators and resets them.
     __device__ __noinline__ void flush_private_thread(const Plan& P, uint8_t* extra, uint32_t t) {
         const uint32_t nv1 = P.nval + 1;
-        long long* w = reinterpret_cast<long long*>(extra);
-        for (uint32_t i = 0; i < P.ngroups * nv1; ++i) {
-            const uint8_t kind = slot_kind(P, i % nv1);
+        uint32_t* cnt = priv_counts(extra);
+        long long* val = priv_values<NT>(P, extra);
+        for (uint32_t g = 0; g < P.ngroups; ++g) {
+            uint32_t& c = cnt[g * NT + t];
+            if (c != 0) {
+                atomic_add_i128(P.acc + 2ull * g * nv1, I128{c, 0});
+                c = 0;
+            }
+        }
+        for (uint32_t i = 0; i < P.ngroups * P.nval; ++i) {
+            const uint32_t g = i / P.nval, v = i % P.nval;
+            const uint8_t kind = P.val[v].kind;
             if (kind == VK_MIN || kind == VK_MAX) continue;
-            long long& a = w[i * NT + t];
+            long long& a = val[i * NT + t];
             if (a != 0) {
                 I128 x;
                 x.lo = static_cast<uint64_t>(a);
                 x.hi = a >> 63;
-                atomic_add_i128(P.acc + 2ull * i, x);
+                atomic_add_i128(P.acc + 2ull * (g * nv1 + 1 + v), x);
                 a = 0;
             }
         }
@@ -596,12 +613,13 @@ struct Sink {
                     *phi = a.hi;
                 }
             } else {
-                if (!P.count_by_tile) w[(g * nv1) * NT + t] += 1;
+                if (!P.count_by_tile) priv_counts(extra)[g * NT + t] += 1;
+                long long* val = priv_values<NT>(P, extra);
 #pragma unroll 1
                 for (uint32_t v = 1; v < nv1; ++v) {
                     const ValDesc& V = P.val[v - 1];
                     const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                    long long& a = w[(g * nv1 + v) * NT + t];
+                    long long& a = val[(g * P.nval + v - 1) * NT + t];
                     if (V.kind == VK_SUM) a = static_cast<long long>(static_cast<uint64_t>(a) + static_cast<uint64_t>(x));
                     else if (V.kind == VK_COUNT_NZ) a += (x != 0);
                     else if (V.kind == VK_MIN) a = min(a, static_cast<long long>(x));
@@ -701,8 +719,12 @@ struct Sink {
                     if (ACC128) {
                         b.lo = static_cast<uint64_t>(w[(idx * 2 + 0) * NT + u]);
                         b.hi = w[(idx * 2 + 1) * NT + u];
+                    } else if (idx % nv1 == 0) {
+                        b.lo = priv_counts(extra)[(idx / nv1) * NT + u];
+                        b.hi = 0;
                     } else {
-                        const long long x = w[idx * NT + u];
+                        const long long x =
+                            priv_values<NT>(P, extra)[((idx / nv1) * P.nval + idx % nv1 - 1) * NT + u];
                         b.lo = static_cast<uint64_t>(x);
                         b.hi = (kind == VK_MIN || kind == VK_MAX) ? 0 : (x >> 63);
                     }
@@ -800,7 +822,7 @@ __device__ __forceinline__ int64_t fast_factor(const uint8_t* stage, uint32_t so
 template <int NT>
 __device__ __forceinline__ void fast_row(const Plan& P, const RegVals& V, uint8_t* extra, const uint8_t* stage,
                                          uint32_t rl, uint32_t t, uint64_t& upd, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
-    long long* w = reinterpret_cast<long long*>(extra);
+    long long* w = priv_values<NT>(P, extra);
 #pragma unroll
     for (int v = 0; v < 2; ++v) {
         if (static_cast<uint32_t>(v) < V.nv) {
@@ -808,7 +830,7 @@ __device__ __forceinline__ void fast_row(const Plan& P, const RegVals& V, uint8_
             const int64_t b = V.nf[v] > 1 ? fast_factor(stage, V.soff[v][1], V.dt[v][1], V.mul[v][1], V.add[v][1], rl)
                                           : int64_t{1};
             const uint64_t x = static_cast<uint64_t>(a) * static_cast<uint64_t>(b);
-            long long& s = w[(v + 1) * NT + t];
+            long long& s = w[v * NT + t];  // group 0, value v
             s = static_cast<long long>(static_cast<uint64_t>(s) + x);
         }
     }
@@ -933,15 +955,17 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
             for (int r = 0; r < R; ++r) g[r] += (gin && !((m >> r) & 1u)) ? 0u : (x[r] - mn) * st;
         }
     }
-    const uint32_t gstride = (P.nval + 1) * static_cast<uint32_t>(NT);
-    uint32_t base[R];  // word of row r's group count; value v is at base + v * NT
+    uint32_t* cnt = priv_counts(extra);
+    w = reinterpret_cast<unsigned long long*>(priv_values<NT>(P, extra));
+    const uint32_t gstride = P.nval * static_cast<uint32_t>(NT);
+    uint32_t base[R];  // value word of row r's group; value v (1-based) is at base + (v - 1) * NT
 #pragma unroll
     for (int r = 0; r < R; ++r) base[r] = g[r] * gstride + t;
     // The slots are private to this thread, so plain read-modify-writes in
     // program order are exact (64-bit shared atomics would run as CAS loops).
     if (!P.count_by_tile) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) w[base[r]] += (m >> r) & 1u;
+        for (int r = 0; r < R; ++r) cnt[g[r] * NT + t] += (m >> r) & 1u;
     }
 
     int64_t cur[R];
@@ -985,7 +1009,7 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
             for (int r = 0; r < R; ++r) cur[r] = f[r];
         }
         if (S.acc) {
-            const uint32_t off = S.acc * static_cast<uint32_t>(NT);
+            const uint32_t off = (S.acc - 1u) * static_cast<uint32_t>(NT);
             if (S.kind == VK_SUM) {
 #pragma unroll
                 for (int r = 0; r < R; ++r)
@@ -1180,8 +1204,9 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
 
     // Read-modify-writes of the thread's private slots, row by row (rows of
     // one group share slots, so each row reads what the previous one wrote).
-    constexpr uint32_t kGroupBytes = NV1 * NT * 8u;
-    const uint32_t wa = smem_addr(extra) + 8u * t;
+    constexpr uint32_t kGroupBytes = (NV1 - 1) * NT * 8u;
+    const uint32_t ca0 = smem_addr(extra) + 4u * t;
+    const uint32_t wa = smem_addr(extra) + priv_count_bytes(P.ngroups, NT) + 8u * t;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         uint32_t g = 0;
@@ -1190,17 +1215,19 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
         if constexpr (SH::nkey >= 2)
             g += (kx1[r] - static_cast<uint32_t>(P.gkey[1].min)) * static_cast<uint32_t>(P.gkey[1].stride);
         const uint32_t a = wa + g * kGroupBytes;
+        const uint32_t ca = ca0 + g * static_cast<uint32_t>(NT) * 4u;
         unsigned long long old[NV1];
+        uint32_t oldc = 0;
+        // The row count (a scalar aggregate counts by popcount per tile).
+        if constexpr (SH::nkey > 0) oldc = lds_u32(ca);
         static_for<NV1>([&](auto V) {
             constexpr uint32_t v = V.value;
-            if constexpr (v > 0 || SH::nkey > 0) old[v] = lds_u64<v * NT * 8u>(a);
+            if constexpr (v > 0) old[v] = lds_u64<(v - 1) * NT * 8u>(a);
         });
+        if constexpr (SH::nkey > 0) sts_u32(ca, oldc + (sm[r] & 1u));
         static_for<NV1>([&](auto V) {
             constexpr uint32_t v = V.value;
-            if constexpr (v == 0) {
-                // The row count (a scalar aggregate counts by popcount per tile).
-                if constexpr (SH::nkey > 0) sts_u64<0>(a, old[0] + (sm[r] & 1u));
-            } else {
+            if constexpr (v > 0) {
                 constexpr uint32_t kind = SH::kind_of(v);
                 unsigned long long nw;
                 const long long x = static_cast<long long>(val[v][r]);
@@ -1208,7 +1235,7 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
                 else if constexpr (kind == VK_COUNT_NZ) nw = old[v] + (val[v][r] != 0 ? 1ull : 0ull);
                 else if constexpr (kind == VK_MIN) nw = sm[r] ? static_cast<unsigned long long>(min(static_cast<long long>(old[v]), x)) : old[v];
                 else nw = sm[r] ? static_cast<unsigned long long>(max(static_cast<long long>(old[v]), x)) : old[v];
-                sts_u64<v * NT * 8u>(a, nw);
+                sts_u64<(v - 1) * NT * 8u>(a, nw);
             }
         });
     }
@@ -1262,7 +1289,7 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             w[NT + t] += (nl < *lo) ? 1 : 0;
             *lo = nl;
         } else {
-            w[t] += __popc(m);
+            priv_counts(extra)[t] += __popc(m);
         }
     }
 
