@@ -246,7 +246,8 @@ def test_join_payload_and_hash_probe_paths(ctx):
         "dup": {**dim, "key": (dim["key"] // 2 + 1).astype(np.int32)},
     }
     p, d = col("price_cents"), col("discount_pct")
-    aggs = [sum_(p * (100 - d)), count_star(), max_(col("quantity")), sum_(col("quantity"))]
+    agg_sets = [[sum_(p * (100 - d)), count_star(), max_(col("quantity")), sum_(col("quantity"))],
+                [sum_(p * (100 - d)), count_star()]]          # the join template's own shape
     for name, dh in variants.items():
         probe = dict(fact)
         if name == "sparse":
@@ -254,7 +255,8 @@ def test_join_payload_and_hash_probe_paths(ctx):
         fp = ctx.register(probe, fct) if name == "sparse" else f
         dt = ctx.register(dh, datagen.DIMENSION_COLTYPES)
         j = dt.join_build("key", col("order_day") < datagen.DAY0 + datagen.NDAYS // 2)
-        for gb in [(build_col("segment"),), (), (build_col("segment"), "flag_a"), ("flag_b",)]:
+        for gb, aggs in [(g, a) for g in [(build_col("segment"),), (), (build_col("segment"), "flag_a"), ("flag_b",)]
+                         for a in agg_sets]:
             for where in [None, col("quantity") < 30]:
                 g = fp.aggregate(aggs, gb, where, join=j, probe_key="fk")
                 o = oracle.aggregate(probe, fct, aggs, gb, where,

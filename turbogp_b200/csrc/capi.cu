@@ -1305,8 +1305,10 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             // overflow checks.
             if (!acc128 && (!J || pay_ok) && !P.check_ovf && ctx->dense_path)
                 P.dense_vec = compile_chain(b, pay_ok) ? 1u : 0u;
-            if (P.dense_vec && ctx->dense_shapes && !J) P.shape = dense_shape_of(P);
-            if (!P.shape && !acc128) P.shape = scalar_shape_of(P);
+            // Scalar aggregates prefer the register fast path; a join's dense
+            // program implies its payload path.
+            if (!acc128) P.shape = scalar_shape_of(P);
+            if (!P.shape && P.dense_vec && ctx->dense_shapes && (!J || pay_ok)) P.shape = dense_shape_of(P);
         } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;

@@ -1045,6 +1045,8 @@ constexpr uint32_t step_code(uint32_t dt, uint32_t fl, uint32_t kind, uint32_t a
 // Kernel tag: scalar aggregates on the register fast path (RegVals).
 struct ScalarTag {};
 
+
+
 template <uint32_t NKEY, uint32_t KDT0, uint32_t KDT1, uint32_t... STEPS>
 struct DenseShape {
     static constexpr uint32_t nkey = NKEY;
@@ -1058,6 +1060,7 @@ struct DenseShape {
         return m;
     }
     static constexpr uint32_t nv1 = max_acc() + 1;  // value slots per group (slot 0 = row count)
+    static constexpr bool dense_shape = true;
     __host__ __device__ static constexpr uint32_t kind_of(uint32_t v) {  // VK_* accumulated into value slot v
         uint32_t k = VK_SUM;
         for (uint32_t i = 0; i < sizeof...(STEPS); ++i)
@@ -1130,7 +1133,8 @@ __device__ __forceinline__ void lds_cells64(uint32_t a, uint32_t t, uint64_t (&x
 
 template <int NT, class SH>
 __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
-                                                  uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink) {
+                                                  uint32_t m, Sink<MODE_GROUP_PRIVATE, false, NT>& sink,
+                                                  const uint32_t* gin = nullptr) {
     constexpr int R = kTileRows / NT;
     constexpr int NS = static_cast<int>(SH::nsteps);
     constexpr uint32_t NV1 = SH::nv1;
@@ -1209,7 +1213,9 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
     const uint32_t wa = smem_addr(extra) + priv_count_bytes(P.ngroups, NT) + 8u * t;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        uint32_t g = 0;
+        // With a join payload, gin holds the (build-side) group index of the
+        // rows in m; every other row adds 0 to group 0.
+        uint32_t g = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
         if constexpr (SH::nkey >= 1)
             g += (kx0[r] - static_cast<uint32_t>(P.gkey[0].min)) * static_cast<uint32_t>(P.gkey[0].stride);
         if constexpr (SH::nkey >= 2)
@@ -1219,12 +1225,13 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
         unsigned long long old[NV1];
         uint32_t oldc = 0;
         // The row count (a scalar aggregate counts by popcount per tile).
-        if constexpr (SH::nkey > 0) oldc = lds_u32(ca);
+        const bool count_rows = SH::nkey > 0 || !P.count_by_tile;
+        if (count_rows) oldc = lds_u32(ca);
         static_for<NV1>([&](auto V) {
             constexpr uint32_t v = V.value;
             if constexpr (v > 0) old[v] = lds_u64<(v - 1) * NT * 8u>(a);
         });
-        if constexpr (SH::nkey > 0) sts_u32(ca, oldc + (sm[r] & 1u));
+        if (count_rows) sts_u32(ca, oldc + (sm[r] & 1u));
         static_for<NV1>([&](auto V) {
             constexpr uint32_t v = V.value;
             if constexpr (v > 0) {
@@ -1366,7 +1373,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
             if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
                 if (P.dense_vec && __reduce_add_sync(kFull, __popc(hit)) >= 8u * R) {
-                    chain_private_tile<NT>(P, extra, stage, t, hit, sink, g);
+                    if constexpr (!std::is_void<SH>::value && !kScalar) {
+                        if (P.shape) chain_tile_static<NT, SH>(P, extra, stage, t, hit, sink, g);
+                        else chain_private_tile<NT>(P, extra, stage, t, hit, sink, g);
+                    } else {
+                        chain_private_tile<NT>(P, extra, stage, t, hit, sink, g);
+                    }
                     return;
                 }
             }
@@ -1745,6 +1757,11 @@ using ShapeQ1 = DenseShape<2, DT_U8, DT_U8, step_code(DT_I32, kNarrowPos, VK_SUM
                            step_code(DT_I32, kNarrowPos | CS_CHAIN, VK_SUM, 3),
                            step_code(DT_I32, kNarrowPos | CS_CHAIN, VK_SUM, 4)>;
 
+// The join + grouped aggregate shape: groups from the join payload, no staged
+// key; sum(i64 * (k - i32)).
+using ShapeJoin = DenseShape<0, 0, 0, step_code(DT_I64, CS_COL | CS_IDENT, VK_SUM, 0),
+                             step_code(DT_I32, kNarrowPos | CS_CHAIN, VK_SUM, 1)>;
+
 struct ShapeEntry {
     uint32_t nkey, kdt0, kdt1, nsteps;
     uint32_t code[kMaxSteps];
@@ -1766,7 +1783,7 @@ static ShapeEntry shape_entry() {
 }
 
 static const ShapeEntry* shape_table(uint32_t* n) {
-    static const ShapeEntry table[] = {shape_entry<ShapeQ1>()};
+    static const ShapeEntry table[] = {shape_entry<ShapeQ1>(), shape_entry<ShapeJoin>()};
     *n = sizeof(table) / sizeof(table[0]);
     return table;
 }
@@ -1823,7 +1840,12 @@ uint32_t dense_shape_of(const Plan& P) {
     const ShapeEntry* tab = shape_table(&n);
     for (uint32_t j = 0; j < n; ++j) {
         const ShapeEntry& e = tab[j];
-        if (e.nkey != P.ngkey || e.nsteps != P.chain.nsteps) continue;
+        // Build-side keys come from the join payload; a shape's keys are the
+        // staged ones, and the two kinds do not mix.
+        uint32_t staged = 0, build = 0;
+        for (uint32_t k = 0; k < P.ngkey; ++k) (P.gkey[k].build_side ? build : staged) += 1;
+        if (build && staged) continue;
+        if (e.nkey != staged || e.nsteps != P.chain.nsteps) continue;
         if (e.nkey >= 1 && e.kdt0 != P.gkey[0].dtype) continue;
         if (e.nkey >= 2 && e.kdt1 != P.gkey[1].dtype) continue;
         bool same = true;
