@@ -281,17 +281,18 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         ev1.synchronize()
     launches, kernel_total = ctx.profile_read()
     ms = ev0.elapsed_time(ev1)
+    # Kernel time alone: the launch queued behind a short device delay.
+    ctx.profile(True, gated=True)
+    run_one = probe_only[0] if probe_only is not None else step
     if probe_only is not None:
-        run_probe, kernel_bytes = probe_only
-        for _ in range(3):
-            run_probe()
-        ctx.profile_read()
-        for _ in range(steps):
-            run_probe()
-        pl, pms = ctx.profile_read()
-        kernel_avg = pms / max(1, pl)
-    else:
-        kernel_avg = kernel_total / max(1, launches)
+        kernel_bytes = probe_only[1]
+    for _ in range(3):
+        run_one()
+    ctx.profile_read()
+    for _ in range(steps):
+        run_one()
+    pl, pms = ctx.profile_read()
+    kernel_avg = pms / max(1, pl)
     ctx.profile(False)
 
     # e2e: pinned host buffers re-uploaded every step, result read back.
@@ -641,7 +642,17 @@ def main() -> None:
     if got != expect:
         raise SystemExit(f"result changed between steps: {got} != {expect}")
     clk = clocks.summary()
-    kernel_avg_ms = max_over_ranks(kernel_ms / max(1, launches))
+    kernel_avg_ungated_ms = max_over_ranks(kernel_ms / max(1, launches))
+    # Kernel time alone: device events around each launch, with the launch
+    # queued behind a short device delay so the host's submission of it (the
+    # GPU is idle between synchronous queries) is not counted.
+    ctx.profile(True, gated=True)
+    ctx.profile_read()
+    for _ in range(min(args.steps, 200)):
+        query.run(decode=False)
+    glaunch, gms = ctx.profile_read()
+    ctx.profile(False)
+    kernel_avg_ms = max_over_ranks(gms / max(1, glaunch))
     value = rows * world * args.steps / (ms / 1000.0)
 
     # ---- e2e: pinned host buffers, H2D + execute + D2H every step ----------
@@ -690,7 +701,9 @@ def main() -> None:
         "hbm_gbs": rows * world * BYTES_PER_ROW * args.steps / (ms / 1000.0) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_launch(),
-                     "kernel_ms": kernel_avg_ms, "kernel": "tgp::scan_kernel<MODE_SCALAR>"},
+                     "kernel_ms": kernel_avg_ms, "kernel_ms_ungated": kernel_avg_ungated_ms,
+                     "timing": "device events around each launch, launch queued behind a device delay",
+                     "kernel": "scan_kernel<MODE_GROUP_PRIVATE, int64, 512, ScalarTag>"},
         "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "cpu_baseline": cpu,
         "clocks": clk,

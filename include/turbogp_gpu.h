@@ -87,7 +87,10 @@ TGP_API int tgp_sync(tgp_ctx* ctx);
 
 /* When enabled, the context records CUDA events on its stream around every
  * scan-kernel launch; tgp_profile_read returns the launches recorded since the
- * last read and their summed device time (ms), then resets the record. */
+ * last read and their summed device time (ms), then resets the record.
+ * on = 1: events only (a launch issued to an idle GPU also counts the host's
+ * submission time). on = 2: each timed launch is queued behind a one-thread
+ * device delay (50 us), so the events bracket the kernel alone. 0: off. */
 TGP_API int tgp_profile_enable(tgp_ctx* ctx, int on);
 TGP_API int tgp_profile_read(tgp_ctx* ctx, uint64_t* launches, double* total_ms);
 

@@ -390,4 +390,17 @@ size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits) {
     return n * 24 + tmp + 256;
 }
 
+// A bounded busy wait of one thread (profiling: keeps the GPU busy while the
+// host submits the launch that follows).
+__global__ void delay_kernel(uint64_t ns) {
+    const uint64_t t0 = global_ns();
+    while (global_ns() - t0 < ns) {
+    }
+}
+
+cudaError_t launch_delay(uint64_t ns, cudaStream_t st) {
+    delay_kernel<<<1, 1, 0, st>>>(ns < 1000000ull ? ns : 1000000ull);
+    return cudaGetLastError();
+}
+
 }  // namespace tgp

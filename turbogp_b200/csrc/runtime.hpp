@@ -57,6 +57,8 @@ cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, con
                                void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
                                int sms, cudaStream_t st);
 size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits);
+// One thread that spins on %globaltimer for `ns` nanoseconds (at most 1 ms).
+cudaError_t launch_delay(uint64_t ns, cudaStream_t st);
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
                                  int sms, cudaStream_t st);
@@ -139,6 +141,7 @@ struct tgp_ctx {
     std::unordered_set<void*> hash_handles;
     // Launch profiling: event pairs around scan-kernel launches.
     bool profile = false;
+    bool profile_gate = false;  // queue a device delay before each timed launch
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
     // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS, TGP_SHARE_EXTRA_MAX).

@@ -285,9 +285,11 @@ class Context:
     def sync(self) -> None:
         self._check(self.lib.tgp_sync(self.h), "tgp_sync")
 
-    def profile(self, on: bool = True) -> None:
-        """Record CUDA events around every scan-kernel launch."""
-        self._check(self.lib.tgp_profile_enable(self.h, 1 if on else 0), "tgp_profile_enable")
+    def profile(self, on: bool = True, gated: bool = False) -> None:
+        """Record CUDA events around every scan-kernel launch; with ``gated``
+        each timed launch waits behind a short device delay, so the events
+        bracket the kernel alone (not the host's submission of it)."""
+        self._check(self.lib.tgp_profile_enable(self.h, (2 if gated else 1) if on else 0), "tgp_profile_enable")
 
     def profile_read(self) -> tuple[int, float]:
         """(launches, summed device ms) since the last read."""
