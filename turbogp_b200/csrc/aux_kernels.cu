@@ -243,6 +243,27 @@ __global__ void fill_u64_kernel(unsigned long long* p, uint64_t n, unsigned long
         p[i] = v;
 }
 
+// Writes the slot image `init` (stride words) into every slot of a table: one
+// pass, slot i's words w at p[i * stride + w] (adjacent threads, adjacent words).
+// (Slots are an even number of words, 16-byte aligned: written as pairs.)
+__global__ void fill_slots_kernel(unsigned long long* p, uint64_t nslots, const SlotImage img) {
+    const uint32_t pairs = img.stride / 2;
+    ulonglong2* q = reinterpret_cast<ulonglong2*>(p);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nslots;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        for (uint32_t w = 0; w < pairs; ++w) q[i * pairs + w] = make_ulonglong2(img.w[2 * w], img.w[2 * w + 1]);
+}
+
+cudaError_t launch_fill_slots(unsigned long long* p, uint64_t nslots, const SlotImage& img, int sms, cudaStream_t st) {
+    if (nslots == 0) return cudaSuccess;
+    if ((img.stride & 1u) || (reinterpret_cast<uintptr_t>(p) & 15u)) return cudaErrorInvalidValue;
+    const uint64_t n = nslots;
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 16) blocks = static_cast<uint64_t>(sms) * 16;
+    fill_slots_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(p, nslots, img);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, int sms,
                             cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -257,11 +278,21 @@ cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long lon
 __global__ void gather_groups_kernel(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                      unsigned long long* out, uint64_t cap,
                                      unsigned long long* counter) {
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < nslots;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    // Whole warps walk the table (the loop bound is rounded up to a warp) so
+    // one atomic per warp reserves the output rows of its occupied slots.
+    const uint64_t step = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t end = (nslots + 31) & ~31ull;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < end; i += step) {
         const unsigned long long* s = htab + i * stride;
-        if (s[0] == ~0ull) continue;
-        const unsigned long long o = atomicAdd(counter, 1ull);
+        const bool occ = i < nslots && s[0] != ~0ull;
+        const unsigned mask = __ballot_sync(0xffffffffu, occ);
+        if (mask == 0) continue;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, static_cast<unsigned long long>(__popc(mask)));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (!occ) continue;
+        const unsigned long long o = base + __popc(mask & ((1u << lane) - 1u));
         if (o < cap)
             for (uint32_t w = 0; w < stride; ++w) out[o * stride + w] = s[w];
     }

@@ -1361,13 +1361,15 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         P.jpay = J->pay;
     }
 
-    // Hash table sizing: twice the bound on distinct groups.
+    // Hash table sizing: 1.25x the bound on distinct groups, to a power of two.
     uint64_t& hcap = qs.hcap;
     hcap = 0;
     if (mode == MODE_GROUP_HASH) {
         const unsigned __int128 est = std::min<unsigned __int128>(D, static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
                                                                           (join ? 4 : 1));
-        hcap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(est) * 2));
+        // Distinct groups never exceed `est`: a load factor of at most 0.8
+        // keeps linear probes short and the table (and its misses) small.
+        hcap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(est) + static_cast<uint64_t>(est) / 4));
         P.hstride = 2 + 2 * P.nval;
         P.hlog2 = log2u(hcap);
         P.hmask = hcap - 1;
@@ -1494,25 +1496,16 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         TGP_CUDA(cudaMemsetAsync(block, 0, block_words * 8, ctx->stream));
     }
     if (mode == MODE_GROUP_HASH) {
-        // Keys EMPTY, counters 0, value limbs: MIN/MAX identity or 0.
-        TGP_CUDA(launch_fill_u64(P.htab, htab_words, 0ull, ctx->sms, ctx->stream));
-        std::vector<unsigned long long> slot_init(P.hstride, 0ull);
-        slot_init[0] = kEmptySlot;
+        // Keys EMPTY, counters 0, value limbs: MIN/MAX identity or 0 (one pass).
+        SlotImage img;
+        std::memset(&img, 0, sizeof(img));
+        img.stride = P.hstride;
+        img.w[0] = kEmptySlot;
         for (uint32_t v = 0; v < P.nval; ++v) {
-            if (P.val[v].kind == VK_MIN) slot_init[2 + 2 * v] = 0x7fffffffffffffffull;
-            if (P.val[v].kind == VK_MAX) slot_init[2 + 2 * v] = 0x8000000000000000ull;
+            if (P.val[v].kind == VK_MIN) img.w[2 + 2 * v] = 0x7fffffffffffffffull;
+            if (P.val[v].kind == VK_MAX) img.w[2 + 2 * v] = 0x8000000000000000ull;
         }
-        // Key words only need EMPTY; MIN/MAX limbs need identities.
-        bool simple = true;
-        for (uint32_t w = 1; w < P.hstride; ++w) simple &= slot_init[w] == 0;
-        if (simple) {
-            TGP_CUDA(cudaMemset2DAsync(P.htab, P.hstride * 8, 0xff, 8, hcap, ctx->stream));
-        } else {
-            std::vector<unsigned long long> img(htab_words);
-            for (uint64_t s = 0; s < hcap; ++s)
-                std::memcpy(&img[s * P.hstride], slot_init.data(), P.hstride * 8);
-            TGP_TRY(upload(ctx, P.htab, img.data(), img.size() * 8));
-        }
+        TGP_CUDA(launch_fill_slots(P.htab, hcap, img, ctx->sms, ctx->stream));
     }
     TGP_TRY(size_smem(ctx, P, extra));
     bound_presum(ctx, qs);

@@ -304,6 +304,13 @@ TGP_HD inline uint32_t priv_count_bytes(uint32_t ngroups, uint32_t nt) {
     return (ngroups * nt * 4u + 15u) & ~15u;
 }
 
+// The initial contents of one group hash table slot (at most 2 + 2 * kMaxVals words).
+struct SlotImage {
+    uint32_t stride;
+    uint32_t _pad;
+    unsigned long long w[2 + 2 * kMaxVals];
+};
+
 // Output layout of hash-grouped results (tgp_execute with hash grouping).
 constexpr int kMaxFormatAggs = 32;
 struct HashFormat {

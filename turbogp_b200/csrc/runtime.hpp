@@ -59,6 +59,7 @@ cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, con
 size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits);
 // One thread that spins on %globaltimer for `ns` nanoseconds (at most 1 ms).
 cudaError_t launch_delay(uint64_t ns, cudaStream_t st);
+cudaError_t launch_fill_slots(unsigned long long* p, uint64_t nslots, const SlotImage& img, int sms, cudaStream_t st);
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
                                  int sms, cudaStream_t st);
