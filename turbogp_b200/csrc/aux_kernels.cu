@@ -379,7 +379,7 @@ __global__ void format_hash_groups_kernel(const unsigned long long* packed, cons
                     o.as_f64 = static_cast<double>(x);
                 } else {
                     o.lo = v[0];
-                    o.hi = static_cast<int64_t>(v[1]);
+                    o.hi = F.sum64 ? (static_cast<int64_t>(v[0]) >> 63) : static_cast<int64_t>(v[1]);
                     const double f = i128_to_f64_rn(o.lo, o.hi);
                     o.as_f64 = F.func[a] == TGP_AGG_AVG ? (cnt ? f / static_cast<double>(cnt) : 0.0) : f;
                 }

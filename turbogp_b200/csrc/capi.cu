@@ -650,7 +650,7 @@ void fill_value(const AggMap& m, const unsigned long long* slot /* [nv1][2] */, 
         return;
     }
     out->lo = s[0];
-    out->hi = static_cast<int64_t>(s[1]);
+    out->hi = P.sum64 ? (static_cast<int64_t>(s[0]) >> 63) : static_cast<int64_t>(s[1]);
     const double f = i128_to_f64(out->lo, out->hi);
     if (m.func == TGP_AGG_AVG) out->as_f64 = cnt ? f / static_cast<double>(cnt) : 0.0;
     else out->as_f64 = f;
@@ -1374,6 +1374,13 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         P.hlog2 = log2u(hcap);
         P.hmask = hcap - 1;
     }
+    // Global / hash sums that provably fit int64 (no join, no per-row
+    // overflow, rows x max|value| < 2^63) accumulate with non-returning adds.
+    if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && !b.unbounded) {
+        const unsigned __int128 bound = static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
+                                        std::max<uint64_t>(b.max_abs_val, 1);
+        if (bound < (static_cast<unsigned __int128>(1) << 63)) P.sum64 = 1;
+    }
     // Shared pre-aggregation of repeated keys (hash and global direct
     // grouping): SUM / COUNT(col) values, no join, no per-row overflow checks;
     // its i32 partials are bounded once the launch grid is known.
@@ -1550,6 +1557,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         F.nkey = q->ngroup;
         F.nagg = nagg;
         F.hstride = P.hstride;
+        F.sum64 = P.sum64;
         for (uint32_t k = 0; k < q->ngroup; ++k) {
             F.key_shift[k] = P.gkey[k].shift;
             F.key_mask[k] = bits[k] >= 64 ? ~0ull : ((1ull << bits[k]) - 1);

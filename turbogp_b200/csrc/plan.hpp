@@ -227,7 +227,7 @@ struct alignas(16) Plan {
     uint32_t jlog2;
     uint32_t jwide;
     int32_t jslot;          // staged slot of the join key (-1 = no join)
-    uint32_t _p1;
+    uint32_t sum64;         // global / hash sums fit int64 (host-proven): plain atomic adds, lo limb only
     int64_t jkmin;
     uint64_t jkrange;       // kmax - kmin (unsigned)
     const uint32_t* jpay;   // unique build keys: per-key payload (build-side group index part), or null
@@ -314,7 +314,7 @@ struct SlotImage {
 // Output layout of hash-grouped results (tgp_execute with hash grouping).
 constexpr int kMaxFormatAggs = 32;
 struct HashFormat {
-    uint32_t nkey, nagg, hstride, _pad;
+    uint32_t nkey, nagg, hstride, sum64;  // sum64: value limbs hold int64 sums (hi = sign of lo)
     uint32_t key_shift[kMaxGroupKeys];
     uint64_t key_mask[kMaxGroupKeys];
     int64_t key_min[kMaxGroupKeys];

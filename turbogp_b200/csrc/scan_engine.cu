@@ -449,6 +449,18 @@ __device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t
     acc_global(slot, kind, x);
 }
 
+// With sum64 (every group's sum provably fits int64) SUM / COUNT(col) add
+// to the low limb with a non-returning atomic; the high limb stays 0 and the
+// host sign-extends the low one.
+__device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t kind, int64_t v, bool sum64) {
+    if (sum64 && (kind == VK_SUM || kind == VK_COUNT_NZ)) {
+        const unsigned long long add = kind == VK_SUM ? static_cast<unsigned long long>(v) : (v != 0 ? 1ull : 0ull);
+        if (add) atomicAdd(slot, add);
+        return;
+    }
+    acc_global_i64(slot, kind, v);
+}
+
 // ---------------------------------------------------------------------------
 // Sinks. Shared-memory scratch layouts (nv1 = 1 + nval; value slot 0 is the
 // group's row count):
@@ -666,7 +678,7 @@ struct Sink {
 #pragma unroll 1
             for (uint32_t v = 1; v < nv1; ++v) {
                 const ValDesc& V = P.val[v - 1];
-                acc_global_i64(a + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf));
+                acc_global_i64(a + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf), P.sum64 != 0);
             }
         } else if (MODE == MODE_GROUP_HASH) {
             const uint64_t key = group_hash_key<TAIL>(P, stage, r0, rl, brow);
@@ -677,7 +689,7 @@ struct Sink {
 #pragma unroll 1
             for (uint32_t v = 0; v < P.nval; ++v) {
                 const ValDesc& V = P.val[v];
-                acc_global_i64(slot + 2 + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf));
+                acc_global_i64(slot + 2 + 2 * v, V.kind, eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf), P.sum64 != 0);
             }
         } else if (MODE == MODE_JOIN_BUILD) {
             // Scanned table is the build side; P.jslot is its key column.
@@ -769,6 +781,10 @@ struct Sink {
                 atomicAdd(base, static_cast<unsigned long long>(cnt[i]));
                 for (uint32_t v = 0; v < P.nval; ++v) {
                     const int64_t x = sums[v * HS + i];
+                    if (P.sum64) {
+                        if (x) atomicAdd(base + vofs + 2 * v, static_cast<unsigned long long>(x));
+                        continue;
+                    }
                     I128 a;
                     a.lo = static_cast<uint64_t>(x);
                     a.hi = x >> 63;
