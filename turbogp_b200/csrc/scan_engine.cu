@@ -485,7 +485,7 @@ __device__ __forceinline__ long long* priv_values(const Plan& P, uint8_t* extra)
 
 // Slot of `key` in the global group hash table (inserted if absent), or null
 // with kErrHashFull raised.
-constexpr uint32_t kSmemProbes = 8;
+constexpr uint32_t kSmemProbes = 2;
 __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, uint64_t key) {
     uint64_t h = hash_slot(key, P.hlog2);
     for (uint64_t n = 0; n <= P.hmask; ++n) {
