@@ -1374,6 +1374,16 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         P.hlog2 = log2u(hcap);
         P.hmask = hcap - 1;
     }
+    // One staged key and at most two SUM / COUNT(col) values of one staged
+    // factor each: the column path of global / hash grouping.
+    if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && P.ngkey == 1 &&
+        !P.gkey[0].build_side && P.gkey[0].slot >= 0 && P.nval <= 2) {
+        bool ok = true;
+        for (uint32_t v = 0; v < P.nval; ++v)
+            ok = ok && (P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ) && P.val[v].nf == 1 &&
+                 P.val[v].f[0].slot >= 0;
+        P.hash_fast = ok ? 1u : 0u;
+    }
     // Global / hash sums that provably fit int64 (no join, no per-row
     // overflow, rows x max|value| < 2^63) accumulate with non-returning adds.
     if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && !b.unbounded) {

@@ -240,7 +240,9 @@ struct alignas(16) Plan {
     uint32_t* err;                  // kErr* bits
     unsigned long long* out_pairs;  // MODE_JOIN_PAIRS: (probe_row << 32) | build_row
     uint64_t out_cap;
-    uint64_t _pad_end;              // sizeof(Plan) is a multiple of 16
+    uint32_t hash_fast;             // global / hash grouping by one staged key, values SUM / COUNT(col)
+                                    // of one staged factor each (at most two): the column path
+    uint32_t _pad_end;              // sizeof(Plan) is a multiple of 16
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 

@@ -531,6 +531,27 @@ __device__ __forceinline__ bool presum_add(const Plan& P, uint8_t* extra, uint64
     return false;
 }
 
+// presum_add with the row's value arguments already computed (x[v]).
+__device__ __forceinline__ bool presum_add_x(const Plan& P, uint8_t* extra, uint64_t key, const int64_t* x) {
+    const uint32_t HS = P.hsm_slots;
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
+    int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
+    uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
+#pragma unroll
+    for (uint32_t n = 0; n < kSmemProbes; ++n) {
+        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
+        if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
+        if (k == kEmpty || k == key) {
+            atomicAdd(&cnt[h], 1u);
+            for (uint32_t v = 0; v < P.nval; ++v) atomicAdd(&sums[v * HS + h], static_cast<int32_t>(x[v]));
+            return true;
+        }
+        h = (h + 1) & (HS - 1);
+    }
+    return false;
+}
+
 template <uint32_t MODE, bool ACC128, int NT>
 struct Sink {
     uint32_t ovf;
@@ -1290,6 +1311,54 @@ __device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t*
 }
 
 // ---------------------------------------------------------------------------
+// Global / hash grouping by one staged key with one or two values, each a
+// SUM or COUNT(col) of one staged affine factor (P.hash_fast): the thread's R
+// key and value cells are loaded column by column, then each selected row
+// goes to the shared pre-aggregation table or, failing that, the global one.
+// COUNT(col) arguments arrive already reduced to 0 / 1.
+// ---------------------------------------------------------------------------
+template <uint32_t MODE, int R>
+__device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                               uint32_t m) {
+    const GKey& K = P.gkey[0];
+    int64_t kc[R], vc[2][R];
+    load_cells64<R>(stage + K.soff, K.dtype, t, kc);
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+        if (static_cast<uint32_t>(v) < P.nval) load_cells64<R>(stage + P.val[v].f[0].soff, P.val[v].f[0].dtype, t, vc[v]);
+    const uint32_t nv1 = P.nval + 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (!((m >> r) & 1u)) continue;
+        int64_t x[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            if (static_cast<uint32_t>(v) >= P.nval) continue;
+            const Factor& F = P.val[v].f[0];
+            const int64_t a = static_cast<int64_t>(static_cast<uint64_t>(F.mul) * static_cast<uint64_t>(vc[v][r]) +
+                                                   static_cast<uint64_t>(F.add));
+            x[v] = P.val[v].kind == VK_COUNT_NZ ? (a != 0 ? 1 : 0) : a;
+        }
+        const uint64_t rel = static_cast<uint64_t>(kc[r]) - static_cast<uint64_t>(K.min);
+        const uint64_t key = MODE == MODE_GROUP_HASH ? (rel << K.shift) : rel * K.stride;
+        if (P.hsm_slots && presum_add_x(P, extra, key, x)) continue;
+        unsigned long long* base;
+        if (MODE == MODE_GROUP_HASH) {
+            unsigned long long* slot = hash_group_slot(P, key);
+            if (slot == nullptr) continue;
+            base = slot + 1;   // [key][count][v0 lo][v0 hi]...
+        } else {
+            base = P.acc + key * nv1 * 2;   // [count lo][count hi][v0 lo][v0 hi]...
+        }
+        atomicAdd(base, 1ull);
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+            if (static_cast<uint32_t>(v) < P.nval)
+                acc_global_i64(base + (MODE == MODE_GROUP_HASH ? 1 : 2) + 2 * v, VK_SUM, x[v], P.sum64 != 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
@@ -1425,6 +1494,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
                 if (P.shape) chain_tile_static<NT, SH>(P, extra, stage, t, m, sink);
                 else chain_private_tile<NT>(P, extra, stage, t, m, sink);
             }
+            return;
+        }
+    }
+    if constexpr (MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) {
+        if (!TAIL && P.hash_fast) {
+            hash_fast_tile<MODE, R>(P, extra, stage, t, m);
             return;
         }
     }
