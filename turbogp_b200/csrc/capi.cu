@@ -1384,9 +1384,10 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
                  P.val[v].f[0].slot >= 0;
         P.hash_fast = ok ? 1u : 0u;
     }
-    // Global / hash sums that provably fit int64 (no join, no per-row
-    // overflow, rows x max|value| < 2^63) accumulate with non-returning adds.
-    if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && !b.unbounded) {
+    // Sums that provably fit int64 (no per-row overflow, at most one build
+    // match per row, rows x max|value| < 2^63) accumulate in the low limb with
+    // non-returning adds; the high limb is the low one's sign.
+    if ((!join || J->unique) && !P.check_ovf && !b.unbounded && !acc128) {
         const unsigned __int128 bound = static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
                                         std::max<uint64_t>(b.max_abs_val, 1);
         if (bound < (static_cast<unsigned __int128>(1) << 63)) P.sum64 = 1;

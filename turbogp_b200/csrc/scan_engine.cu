@@ -461,6 +461,16 @@ __device__ __forceinline__ void acc_global_i64(unsigned long long* slot, uint8_t
     acc_global_i64(slot, kind, v);
 }
 
+// acc_global with the sum64 form: SUM / COUNT partials add to the low limb
+// without waiting for the old value.
+__device__ __forceinline__ void acc_global_s(unsigned long long* slot, uint8_t kind, const I128& v, bool sum64) {
+    if (sum64 && kind != VK_MIN && kind != VK_MAX) {
+        if (v.lo) atomicAdd(slot, static_cast<unsigned long long>(v.lo));
+        return;
+    }
+    acc_global(slot, kind, v);
+}
+
 // ---------------------------------------------------------------------------
 // Sinks. Shared-memory scratch layouts (nv1 = 1 + nval; value slot 0 is the
 // group's row count):
@@ -599,7 +609,7 @@ struct Sink {
         for (uint32_t g = 0; g < P.ngroups; ++g) {
             uint32_t& c = cnt[g * NT + t];
             if (c != 0) {
-                atomic_add_i128(P.acc + 2ull * g * nv1, I128{c, 0});
+                acc_global_s(P.acc + 2ull * g * nv1, VK_SUM, I128{c, 0}, P.sum64 != 0);
                 c = 0;
             }
         }
@@ -612,7 +622,7 @@ struct Sink {
                 I128 x;
                 x.lo = static_cast<uint64_t>(a);
                 x.hi = a >> 63;
-                atomic_add_i128(P.acc + 2ull * (g * nv1 + 1 + v), x);
+                acc_global_s(P.acc + 2ull * (g * nv1 + 1 + v), VK_SUM, x, P.sum64 != 0);
                 a = 0;
             }
         }
@@ -765,7 +775,7 @@ struct Sink {
                 }
 #pragma unroll
                 for (int d = 16; d > 0; d >>= 1) acc_combine(a, kind, shfl_down_i128(a, d));
-                if (lane == 0 && !acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
+                if (lane == 0 && !acc_untouched(a, kind)) acc_global_s(P.acc + 2ull * idx, kind, a, P.sum64 != 0);
             }
         } else if (MODE == MODE_GROUP_SHARED) {
             consumer_sync<NT>();
@@ -775,7 +785,7 @@ struct Sink {
                 I128 a;
                 a.lo = static_cast<uint64_t>(w[2 * idx]);
                 a.hi = w[2 * idx + 1];
-                if (!acc_untouched(a, kind)) acc_global(P.acc + 2ull * idx, kind, a);
+                if (!acc_untouched(a, kind)) acc_global_s(P.acc + 2ull * idx, kind, a, P.sum64 != 0);
             }
         } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             consumer_sync<NT>();
