@@ -465,6 +465,35 @@ TGP_API int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tg
 TGP_API int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id batch, int wait);
 
 /* ------------------------------------------------------------------------ */
+/* Captured queries: one CUDA graph per query template                       */
+/* ------------------------------------------------------------------------ */
+
+/* The reference plans and interprets every statement again on each call
+ * (route_and_execute, src/engine/mod.rs:527-533; execute_shape,
+ * src/engine/dispatch.rs:364). A captured query is planned once: its result
+ * clear, scan launch and result readback are recorded as one CUDA graph that
+ * tgp_graph_launch replays with one launch and one synchronisation.
+ *
+ * Direct-indexed and scalar aggregates only (hash grouping sizes its result
+ * from the data: TGP_UNSUPPORTED). The graph reads the table's and join's
+ * device memory as they were at capture: launching after the table or join was
+ * dropped, or after a join's payload array was rebuilt for another key layout,
+ * returns TGP_NOT_FOUND (capture again). Reloading a table in place
+ * (tgp_table_reload) keeps the graph valid, and the graph sees the new rows,
+ * as long as every column's min / max stays as it was (the plan's bounds are
+ * proven from them); otherwise the launch returns TGP_NOT_FOUND as well. */
+typedef uint64_t tgp_graph_id;
+
+TGP_API int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out);
+
+/* Runs a captured query on the context's stream and waits for it; outputs as
+ * tgp_execute. */
+TGP_API int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id graph, uint64_t* keys_out, tgp_agg_value* vals_out,
+                             uint64_t group_cap, tgp_query_result* result);
+
+TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free aggregate                                                 */
 /* ------------------------------------------------------------------------ */
 

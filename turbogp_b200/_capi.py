@@ -146,6 +146,10 @@ PROTOTYPES = [
       C.c_uint64, C.POINTER(C.c_uint64)]),
     ("tgp_batch_submit", C.c_int, [C.c_void_p, C.POINTER(BatchItem), C.c_uint32, C.POINTER(C.c_uint64)]),
     ("tgp_batch_poll", C.c_int, [C.c_void_p, C.c_uint64, C.c_int]),
+    ("tgp_graph_capture", C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    ("tgp_graph_launch", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(AggValue), C.c_uint64, C.POINTER(QueryResult)]),
+    ("tgp_graph_drop", C.c_int, [C.c_void_p, C.c_uint64]),
     ("tgp_aggregate_noalloc", C.c_int,
      [C.c_int, C.c_void_p, C.POINTER(ColumnDesc), C.c_uint32, C.c_uint64, C.POINTER(PredNode), C.c_uint32,
       C.POINTER(KeyDomain), C.c_uint32, C.POINTER(Agg), C.c_uint32, C.POINTER(AggValue), C.c_uint64,

@@ -757,6 +757,8 @@ void free_join(tgp_ctx* ctx, JoinTable& J) {
 
 // Releases a batch record (defined with the batch entry points).
 extern "C" void tgp_batch_free_rec(tgp_ctx* ctx, void* rec);
+// Releases a captured-query record (defined with the graph entry points).
+extern "C" void tgp_graph_free_rec(void* rec);
 
 // ==========================================================================
 // C ABI
@@ -825,7 +827,10 @@ int tgp_init(tgp_ctx** out, int device) {
     if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
     if (const char* e = std::getenv("TGP_L2_AHEAD")) ctx->l2_ahead = std::min(64, std::max(0, std::atoi(e)));
     if (const char* e = std::getenv("TGP_NO_DENSE_SHAPES")) ctx->dense_shapes = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_SCAN_THREADS")) ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
+    if (const char* e = std::getenv("TGP_SCAN_THREADS")) {
+        ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
+        ctx->scan_threads_set = true;
+    }
     if (const char* e = std::getenv("TGP_MAX_STAGES"))
         ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
     *out = ctx;
@@ -847,6 +852,8 @@ int tgp_shutdown(tgp_ctx* ctx) {
     }
     for (auto& kv : ctx->batches) tgp_batch_free_rec(ctx, kv.second);
     ctx->batches.clear();
+    for (auto& kv : ctx->graphs) tgp_graph_free_rec(kv.second);
+    ctx->graphs.clear();
     cudaStreamSynchronize(ctx->stream);
     for (auto& pb : ctx->pinned_pool) cudaFreeHost(pb.p);
     ctx->pinned_pool.clear();
@@ -1294,6 +1301,17 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
                     break;
                 }
             }
+        // When 512 threads' accumulators leave room for only two stages (one
+        // tile in flight while the other is consumed) and 256 threads leave
+        // room for four or more, the deeper pipeline wins: 60M-row join probe
+        // with 25 groups 0.50 -> 0.46 ms. With three stages at 256 threads the
+        // halved warp count loses (6M-row grouped aggregate 0.054 -> 0.068 ms).
+        if (nt == 512 && P.stage_bytes && !ctx->scan_threads_set) {
+            const size_t st = P.stage_bytes;
+            const size_t s512 = budget > private_bytes(512) ? (budget - private_bytes(512)) / st : 0;
+            const size_t s256 = budget > private_bytes(256) ? (budget - private_bytes(256)) / st : 0;
+            if (s512 == 2 && std::min<size_t>(s256, ctx->max_stages) >= 4) nt = 256;
+        }
         if (nt) {
             mode = MODE_GROUP_PRIVATE;
             P.nthreads = nt;
@@ -1979,6 +1997,162 @@ int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id id, int wait) {
     }
     tgp_batch_free_rec(ctx, B);
     ctx->batches.erase(it);
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Captured queries
+// --------------------------------------------------------------------------
+namespace {
+
+// One captured query: its plan, the graph (clear, scan, readback) and the
+// buffers the graph reads and writes, plus what it was captured against.
+struct GraphRec {
+    QueryState qs;
+    tgp_query q{};                          // counts only (pointers cleared)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long* block = nullptr;   // device result block
+    unsigned long long* image = nullptr;   // MIN/MAX identity image of the accumulators
+    unsigned long long* host = nullptr;    // pinned readback of the block
+    uint64_t block_words = 0;
+    tgp_table_id table = 0;
+    const Table* T = nullptr;
+    std::vector<const uint8_t*> cols;      // device column pointers at capture
+    std::vector<std::pair<int64_t, int64_t>> stats;  // column min / max at capture
+    tgp_join_id join = 0;
+    const JoinTable* J = nullptr;
+    const unsigned long long* jtab = nullptr;
+    const uint32_t* jpay = nullptr;
+};
+
+void graph_release(GraphRec* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->block) cudaFree(g->block);
+    if (g->image) cudaFree(g->image);
+    if (g->host) cudaFreeHost(g->host);
+    delete g;
+}
+
+// The table / join the graph reads must be the ones it was captured against,
+// with the statistics its plan's bounds were proven from.
+int graph_check(tgp_ctx* ctx, const GraphRec& g) {
+    auto it = ctx->tables.find(g.table);
+    if (it == ctx->tables.end() || &it->second != g.T || it->second.rows != g.qs.T->rows ||
+        it->second.cols.size() != g.cols.size())
+        return fail(ctx, TGP_NOT_FOUND, "captured query: table dropped or replaced; capture again");
+    for (size_t c = 0; c < g.cols.size(); ++c) {
+        const Column& col = it->second.cols[c];
+        if (col.dptr != g.cols[c] || col.min != g.stats[c].first || col.max != g.stats[c].second)
+            return fail(ctx, TGP_NOT_FOUND, "captured query: column moved or its min / max changed; capture again");
+    }
+    if (g.join) {
+        auto jt = ctx->joins.find(g.join);
+        if (jt == ctx->joins.end() || &jt->second != g.J || jt->second.tab != g.jtab || jt->second.pay != g.jpay)
+            return fail(ctx, TGP_NOT_FOUND, "captured query: join dropped or its payload rebuilt; capture again");
+    }
+    return TGP_OK;
+}
+
+}  // namespace
+
+void tgp_graph_free_rec(void* r) { graph_release(static_cast<GraphRec*>(r)); }
+
+int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out) {
+    if (!ctx || !q || !out) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    *out = 0;
+    std::unique_ptr<GraphRec, void (*)(GraphRec*)> rec(new GraphRec(), graph_release);
+    GraphRec& g = *rec;
+    QueryState& qs = g.qs;
+    TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem()));
+    if (qs.mode == MODE_GROUP_HASH)
+        return fail(ctx, TGP_UNSUPPORTED, "hash-grouped queries size their result from the data and are not captured");
+    Plan& P = qs.b->P;
+    g.q = *q;
+    g.q.pred = nullptr;
+    g.q.group = nullptr;
+    g.q.aggs = nullptr;
+    qs.q = &g.q;
+    g.table = q->table;
+    g.T = qs.T;
+    for (const Column& c : qs.T->cols) {
+        g.cols.push_back(c.dptr);
+        g.stats.emplace_back(c.min, c.max);
+    }
+    if (qs.J) {
+        g.join = q->join;
+        g.J = qs.J;
+        g.jtab = qs.J->tab;
+        g.jpay = qs.J->pay;
+    }
+
+    g.block_words = qs.block_words();
+    const uint64_t acc_words = qs.acc_words();
+    TGP_CUDA(cudaMalloc(reinterpret_cast<void**>(&g.block), g.block_words * 8));
+    TGP_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g.host), g.block_words * 8, cudaHostAllocDefault));
+    P.counters = g.block;
+    P.err = reinterpret_cast<uint32_t*>(g.block + 4);
+    P.acc = g.block + 6;
+    const bool minmax = qs.has_minmax();
+    if (minmax) {
+        std::vector<unsigned long long> img;
+        init_acc_image(P, qs.ngroups_direct, &img);
+        TGP_CUDA(cudaMalloc(reinterpret_cast<void**>(&g.image), acc_words * 8));
+        TGP_TRY(upload(ctx, g.image, img.data(), img.size() * 8));
+    }
+    TGP_TRY(size_smem(ctx, P, qs.extra));
+    // Kernel attributes and occupancy are settled before the capture.
+    if (scan_occupancy(qs.mode, qs.acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape) <= 0)
+        return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
+
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    const bool prof = ctx->profile;
+    ctx->profile = false;
+    int st = TGP_OK;
+    std::string what;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(g.block, 0, minmax ? 48 : g.block_words * 8, ctx->stream);
+        if (e == cudaSuccess && minmax)
+            e = cudaMemcpyAsync(g.block + 6, g.image, acc_words * 8, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess) st = launch(ctx, P, qs.mode, qs.acc128);
+        if (e == cudaSuccess && st == TGP_OK)
+            e = cudaMemcpyAsync(g.host, g.block, g.block_words * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g.graph);
+        if (e == cudaSuccess) e = e2;
+    }
+    ctx->profile = prof;
+    if (st != TGP_OK) return st;
+    if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+    TGP_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    const uint64_t id = ctx->next_id++;
+    ctx->graphs[id] = rec.release();
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id id, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
+                     tgp_query_result* result) {
+    if (!ctx || !result) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    std::memset(result, 0, sizeof(*result));
+    auto it = ctx->graphs.find(id);
+    if (it == ctx->graphs.end()) return fail(ctx, TGP_NOT_FOUND, "unknown graph id");
+    GraphRec& g = *static_cast<GraphRec*>(it->second);
+    TGP_TRY(graph_check(ctx, g));
+    TGP_CUDA(cudaGraphLaunch(g.exec, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return decode_direct(ctx, g.qs, g.host, keys_out, vals_out, group_cap, result);
+}
+
+int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id id) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->graphs.find(id);
+    if (it == ctx->graphs.end()) return fail(ctx, TGP_NOT_FOUND, "unknown graph id");
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    graph_release(static_cast<GraphRec*>(it->second));
+    ctx->graphs.erase(it);
     return TGP_OK;
 }
 

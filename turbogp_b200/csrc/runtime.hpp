@@ -138,6 +138,8 @@ struct tgp_ctx {
     std::vector<PinnedBuf> pinned_pool;
     // Batches submitted and not yet polled (opaque records owned by capi.cu).
     std::unordered_map<uint64_t, void*> batches;
+    // Captured queries (opaque records owned by capi.cu).
+    std::unordered_map<uint64_t, void*> graphs;
     // Live HashBuild handles (opaque pointers handed to callers).
     std::unordered_set<void*> hash_handles;
     // Launch profiling: event pairs around scan-kernel launches.
@@ -148,6 +150,7 @@ struct tgp_ctx {
     // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS, TGP_SHARE_EXTRA_MAX).
     int ctas_per_sm = 1;
     int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
+    bool scan_threads_set = false;  // TGP_SCAN_THREADS given: no pipeline-depth switch to 256
     int max_stages = tgp::kMaxStages;
     bool dense_path = true;  // dense column programs for MODE_GROUP_PRIVATE (TGP_NO_DENSE=1 turns them off)
     int l2_ahead = -1;         // L2 prefetch distance in tiles (TGP_L2_AHEAD; -1 = off)

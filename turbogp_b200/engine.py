@@ -538,6 +538,7 @@ class PreparedQuery:
         self._alloc(group_cap)
         self.res = A.QueryResult()
         self._fn = table.ctx.lib.tgp_execute
+        self.graph = 0
 
     def rebind(self, where: Pred | None) -> "PreparedQuery":
         """Replaces the WHERE program (new literals or shape); the rest of the
@@ -546,7 +547,27 @@ class PreparedQuery:
         self.q.pred = nodes if nodes is not None else None
         self.q.npred = n
         self._keep = (nodes,) + tuple(self._keep[1:])
+        if self.graph:
+            self.capture()
         return self
+
+    def capture(self) -> "PreparedQuery":
+        """Records the query as a CUDA graph (tgp_graph_capture); later ``run``
+        calls replay it with one graph launch and no planning. Direct-indexed
+        and scalar aggregates only (a hash-grouped query raises TgpError
+        UNSUPPORTED)."""
+        ctx = self.table.ctx
+        self.drop_graph()
+        gid = C.c_uint64()
+        ctx._check(ctx.lib.tgp_graph_capture(ctx.h, C.byref(self.q), C.byref(gid)), "tgp_graph_capture")
+        self.graph = int(gid.value)
+        return self
+
+    def drop_graph(self) -> None:
+        if self.graph:
+            ctx = self.table.ctx
+            gid, self.graph = self.graph, 0
+            ctx._check(ctx.lib.tgp_graph_drop(ctx.h, gid), "tgp_graph_drop")
 
     # Output buffers of at least this many bytes are page-locked, so the
     # device-to-host copy of a large grouped result runs at full link speed.
@@ -573,11 +594,15 @@ class PreparedQuery:
         (the raw results stay in ``keys`` / ``vals``)."""
         ctx = self.table.ctx
         while True:
-            st = self._fn(ctx.h, C.byref(self.q), self.keys.ctypes.data, self.vals, self.cap, C.byref(self.res))
+            if self.graph:
+                st = ctx.lib.tgp_graph_launch(ctx.h, self.graph, self.keys.ctypes.data, self.vals, self.cap,
+                                              C.byref(self.res))
+            else:
+                st = self._fn(ctx.h, C.byref(self.q), self.keys.ctypes.data, self.vals, self.cap, C.byref(self.res))
             if st == A.CAPACITY and self.res.ngroups > self.cap:
                 self._alloc(int(self.res.ngroups))
                 continue
-            ctx._check(st, "tgp_execute")
+            ctx._check(st, "tgp_graph_launch" if self.graph else "tgp_execute")
             break
         return self._output(self.res, decode)
 
