@@ -72,6 +72,8 @@ def _sig(lib):
                                    C.c_uint32, C.POINTER(A.ColumnDesc), C.c_uint32, C.c_uint64, C.c_uint32,
                                    C.POINTER(A.PredNode), C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64,
                                    C.POINTER(C.c_uint64)]
+    lib.orc_seq_sum_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
+    lib.orc_seq_sum_f64.restype = None
     lib.orc_kernel_execute.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(A.KernelParams),
                                        C.POINTER(A.KernelResultC)]
     return lib

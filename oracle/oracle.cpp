@@ -384,4 +384,14 @@ int orc_kernel_execute(uint32_t op, const uint64_t* input, const uint64_t* input
     }
 }
 
+// Sequential f64 accumulation in row order, one running sum per group:
+// out[group[i]] += terms[i] for i = 0..n-1. This is the order of the
+// reference's per-group sums: each group's row index list is ascending
+// (chunks of 65,536 rows merged in chunk order, aggregate.rs:580-623) and
+// sum_vec adds one term per index in list order (aggregate.rs:1485-1792).
+void orc_seq_sum_f64(const double* terms, const uint32_t* group, uint64_t n, uint32_t ngroups, double* out) {
+    for (uint32_t g = 0; g < ngroups; ++g) out[g] = 0.0;
+    for (uint64_t i = 0; i < n; ++i) out[group[i]] += terms[i];
+}
+
 }  // extern "C"
