@@ -250,6 +250,36 @@ TGP_API int tgp_table_register(tgp_ctx* ctx, const tgp_column_desc* cols, uint32
 TGP_API int tgp_table_register_device(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_t ncols,
                               uint64_t rows, tgp_table_id* out);
 
+/* One column in the reference's own table layout (src/datasource/table.rs:
+ * 25-66): `cells` is Table::columns[i] (one u64 cell per value) and
+ * `i32_sidecar` is Table::i32_columns[i] when its loader filled one (values
+ * that fit i32, table.rs:52-61), else NULL. `coltype` is the column's ColType.
+ * Host or device memory. */
+typedef struct tgp_cell_column {
+    const uint64_t* cells;
+    const int32_t* i32_sidecar;
+    uint32_t coltype;          /* tgp_coltype */
+    uint32_t _pad;
+} tgp_cell_column;
+
+/* Registers a table given in the reference's layout and keeps each column at
+ * the narrowest width that holds every cell exactly, so scans read 1-4 bytes
+ * per value instead of 8:
+ *  - an i32 sidecar, when present, is taken as the column (4 bytes per value
+ *    cross the link; the cells are not read);
+ *  - Float columns stay f64 bits (TGP_DT_F64);
+ *  - otherwise the cells are copied, their min / max taken on the device, and
+ *    an Int column whose values lie in 0..255 becomes TGP_DT_U8, one within
+ *    the i32 range TGP_DT_I32, else TGP_DT_I64; a Date column (unsigned cells)
+ *    becomes TGP_DT_U8 up to 255, TGP_DT_I32 up to 2^31-1, else TGP_DT_U64.
+ * Every narrow value widens back to its original cell, so predicates and
+ * aggregates give the results the cells would. */
+TGP_API int tgp_table_register_cells(tgp_ctx* ctx, const tgp_cell_column* cols, uint32_t ncols,
+                                     uint64_t rows, tgp_table_id* out);
+
+/* The stored dtype (tgp_dtype) of column `col` of a registered table. */
+TGP_API int tgp_table_column_dtype(tgp_ctx* ctx, tgp_table_id table, uint32_t col, uint32_t* dtype);
+
 /* Replaces the contents of every column of a registered (copying) table from
  * new host buffers of the same row count, reusing its device memory. */
 TGP_API int tgp_table_reload(tgp_ctx* ctx, tgp_table_id table, const tgp_column_desc* cols,

@@ -34,6 +34,10 @@ class ColumnDesc(C.Structure):
     _fields_ = [("dtype", C.c_uint32), ("coltype", C.c_uint32), ("data", C.c_void_p)]
 
 
+class CellColumn(C.Structure):
+    _fields_ = [("cells", C.c_void_p), ("i32_sidecar", C.c_void_p), ("coltype", C.c_uint32), ("_pad", C.c_uint32)]
+
+
 class PredNode(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32), ("column", C.c_uint32), ("cmp", C.c_uint32), ("_pad", C.c_uint32),
@@ -128,6 +132,9 @@ PROTOTYPES = [
      [C.c_void_p, C.POINTER(ColumnDesc), C.c_uint32, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("tgp_table_register_device", C.c_int,
      [C.c_void_p, C.POINTER(ColumnDesc), C.c_uint32, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("tgp_table_register_cells", C.c_int,
+     [C.c_void_p, C.POINTER(CellColumn), C.c_uint32, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("tgp_table_column_dtype", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("tgp_table_reload", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(ColumnDesc), C.c_uint32]),
     ("tgp_table_drop", C.c_int, [C.c_void_p, C.c_uint64]),
     ("tgp_table_info", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),

@@ -56,6 +56,46 @@ cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n,
 }
 
 // ---------------------------------------------------------------------------
+// Narrowing of u64 cells whose values the host proved to fit the target
+// width: U8 (0..255) or I32 (the i32 range). Four values per thread.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kAuxThreads) narrow_cells_kernel(const long long* __restrict__ src, uint64_t n,
+                                                                  uint8_t* __restrict__ dst, uint32_t dtype) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t q = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; 4 * q < n; q += stride) {
+        const uint64_t i = 4 * q;
+        if (i + 4 <= n) {
+            const longlong2 a = reinterpret_cast<const longlong2*>(src)[2 * q];
+            const longlong2 b = reinterpret_cast<const longlong2*>(src)[2 * q + 1];
+            if (dtype == DT_U8) {
+                const uint32_t w = (static_cast<uint32_t>(a.x) & 0xffu) | ((static_cast<uint32_t>(a.y) & 0xffu) << 8) |
+                                   ((static_cast<uint32_t>(b.x) & 0xffu) << 16) |
+                                   ((static_cast<uint32_t>(b.y) & 0xffu) << 24);
+                reinterpret_cast<uint32_t*>(dst)[q] = w;
+            } else {
+                reinterpret_cast<int4*>(dst)[q] = make_int4(static_cast<int>(a.x), static_cast<int>(a.y),
+                                                            static_cast<int>(b.x), static_cast<int>(b.y));
+            }
+        } else {
+            for (uint64_t j = i; j < n; ++j) {
+                if (dtype == DT_U8) dst[j] = static_cast<uint8_t>(src[j]);
+                else reinterpret_cast<int32_t*>(dst)[j] = static_cast<int32_t>(src[j]);
+            }
+        }
+    }
+}
+
+cudaError_t launch_narrow_cells(const long long* src, uint64_t n, uint8_t* dst, uint32_t dtype, int sms,
+                                cudaStream_t st) {
+    uint64_t blocks = (n + 4ull * kAuxThreads - 1) / (4ull * kAuxThreads);
+    const uint64_t cap = static_cast<uint64_t>(sms) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) return cudaSuccess;
+    narrow_cells_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(src, n, dst, dtype);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Bitmap compaction: one CTA per scan tile (kTileRows bits = 64 words).
 // tile_base[t] = exclusive prefix of selected rows before tile t.
 // ---------------------------------------------------------------------------

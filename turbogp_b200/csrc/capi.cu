@@ -999,6 +999,105 @@ int tgp_table_register_device(tgp_ctx* ctx, const tgp_column_desc* cols, uint32_
     return register_impl(ctx, cols, ncols, rows, false, out);
 }
 
+int tgp_table_register_cells(tgp_ctx* ctx, const tgp_cell_column* cols, uint32_t ncols, uint64_t rows,
+                             tgp_table_id* out) {
+    if (!ctx || !out || (ncols && !cols)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (rows >= (1ull << 32)) return fail(ctx, TGP_UNSUPPORTED, "tables hold fewer than 2^32 rows (u32 row ids)");
+    TGP_CUDA(cudaSetDevice(ctx->device));
+    Table t;
+    t.rows = rows;
+    uint8_t* cells = nullptr;  // device copy of the current column's cells
+    auto give_up = [&](int st, const std::string& m) {
+        cudaStreamSynchronize(ctx->stream);
+        if (cells) cudaFree(cells);
+        for (auto& c : t.cols) cudaFree(c.dptr);
+        return fail(ctx, st, m);
+    };
+    // Whole 256-byte blocks, as tgp_table_register pads, so bulk copies of
+    // the last tile stay in bounds.
+    auto alloc = [&](uint8_t** p, size_t bytes) {
+        if (cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(16, ((bytes + 255) / 256) * 256)) == cudaSuccess)
+            return true;
+        cudaGetLastError();
+        *p = nullptr;
+        return false;
+    };
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, 16, &cv));
+    long long* mm = cv.take<long long>(2);
+    for (uint32_t i = 0; i < ncols; ++i) {
+        const tgp_cell_column& in = cols[i];
+        if (in.coltype > TGP_CT_FLOAT) return give_up(TGP_INVALID_ARG, "bad column coltype");
+        Column c;
+        c.coltype = in.coltype;
+        c.owned = true;
+        if (in.i32_sidecar) {
+            c.dtype = DT_I32;
+            c.width = 4;
+            if (!alloc(&c.dptr, rows * 4)) return give_up(TGP_OOM, "column allocation failed");
+            t.cols.push_back(c);
+            if (rows && cudaMemcpyAsync(c.dptr, in.i32_sidecar, rows * 4, cudaMemcpyDefault, ctx->stream) != cudaSuccess)
+                return give_up(TGP_DEVICE_ERROR, "sidecar copy failed");
+            continue;
+        }
+        if (rows && !in.cells) return give_up(TGP_INVALID_ARG, "null column cells");
+        if (!alloc(&cells, rows * 8)) return give_up(TGP_OOM, "column allocation failed");
+        if (rows && cudaMemcpyAsync(cells, in.cells, rows * 8, cudaMemcpyDefault, ctx->stream) != cudaSuccess)
+            return give_up(TGP_DEVICE_ERROR, "cell copy failed");
+        uint32_t dt = in.coltype == TGP_CT_FLOAT ? DT_F64 : in.coltype == TGP_CT_DATE ? DT_U64 : DT_I64;
+        if (in.coltype != TGP_CT_FLOAT && rows) {
+            // Signed min / max of the cells; a Date column narrows only when
+            // every cell is below 2^63 (signed and unsigned order agree).
+            const long long init[2] = {0x7fffffffffffffffll, static_cast<long long>(0x8000000000000000ull)};
+            if (upload(ctx, mm, init, 16) != TGP_OK) return give_up(TGP_DEVICE_ERROR, "statistics upload failed");
+            long long r[2];
+            if (launch_column_minmax(cells, DT_I64, rows, mm, ctx->sms, ctx->stream) != cudaSuccess ||
+                cudaMemcpyAsync(r, mm, 16, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+                cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                return give_up(TGP_DEVICE_ERROR, "column statistics failed");
+            const long long lo = r[0], hi = r[1];
+            if (lo >= 0 && hi <= 255) dt = DT_U8;
+            else if (in.coltype == TGP_CT_INT ? (lo >= INT32_MIN && hi <= INT32_MAX) : (lo >= 0 && hi <= INT32_MAX))
+                dt = DT_I32;
+        }
+        c.dtype = dt;
+        c.width = dtype_width(dt);
+        if (c.width == 8) {
+            c.dptr = cells;
+            cells = nullptr;
+        } else {
+            if (!alloc(&c.dptr, rows * c.width)) return give_up(TGP_OOM, "column allocation failed");
+            t.cols.push_back(c);
+            if (launch_narrow_cells(reinterpret_cast<const long long*>(cells), rows, c.dptr, dt, ctx->sms,
+                                    ctx->stream) != cudaSuccess ||
+                cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                return give_up(TGP_DEVICE_ERROR, "cell narrowing failed");
+            cudaFree(cells);
+            cells = nullptr;
+            continue;
+        }
+        t.cols.push_back(c);
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return give_up(TGP_DEVICE_ERROR, "column copy failed");
+    if (int st = compute_stats(ctx, t)) {
+        for (auto& c : t.cols) cudaFree(c.dptr);
+        return st;
+    }
+    const uint64_t id = ctx->next_id++;
+    ctx->tables.emplace(id, std::move(t));
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_table_column_dtype(tgp_ctx* ctx, tgp_table_id id, uint32_t col, uint32_t* dtype) {
+    if (!ctx || !dtype) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    auto it = ctx->tables.find(id);
+    if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
+    if (col >= it->second.cols.size()) return fail(ctx, TGP_INVALID_ARG, "column index out of range");
+    *dtype = it->second.cols[col].dtype;
+    return TGP_OK;
+}
+
 int tgp_table_reload(tgp_ctx* ctx, tgp_table_id id, const tgp_column_desc* cols, uint32_t ncols) {
     if (!ctx || (ncols && !cols)) return fail(ctx, TGP_INVALID_ARG, "null argument");
     auto it = ctx->tables.find(id);

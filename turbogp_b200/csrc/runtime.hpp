@@ -36,6 +36,10 @@ int batch_occupancy(bool acc128, int nt, size_t dyn_smem);
 cudaError_t launch_batch(const BatchDesc& B, bool acc128, int nt, int grid, size_t dyn_smem, cudaStream_t st);
 cudaError_t launch_column_minmax(const uint8_t* col, uint32_t dtype, uint64_t n, long long* out,
                                  int sms, cudaStream_t st);
+// dst[i] = src[i] narrowed to DT_U8 or DT_I32 (the caller proved every value fits).
+// src 16-byte aligned; dst 16-byte aligned for DT_I32, 4-byte for DT_U8.
+cudaError_t launch_narrow_cells(const long long* src, uint64_t n, uint8_t* dst, uint32_t dtype, int sms,
+                                cudaStream_t st);
 cudaError_t tile_prefix(const uint32_t* counts, unsigned long long* out, uint64_t n, void* tmp,
                         size_t* tmp_bytes, cudaStream_t st);
 cudaError_t launch_compact(const uint32_t* bitmap, uint64_t nwords, uint64_t ntiles,

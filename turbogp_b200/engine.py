@@ -302,6 +302,46 @@ class Context:
         'int' | 'date' | 'float' (default: 'float' for f64, else 'int')."""
         return self._register(columns, coltypes, device=False)
 
+    def register_cells(self, cells: dict, coltypes: dict | None = None, sidecars: dict | None = None) -> "Table":
+        """Registers a table in the reference's layout: one u64 cell per value
+        per column (``Table::columns``), optional i32 sidecars
+        (``Table::i32_columns``). The library stores each column at the
+        narrowest width holding all of its values (tgp_table_register_cells).
+        ``coltypes`` maps a name to 'int' | 'date' | 'float' (default 'int')."""
+        coltypes, sidecars = coltypes or {}, sidecars or {}
+        names = list(cells)
+        descs = (A.CellColumn * max(1, len(names)))()
+        keep, rows = [], None
+        for i, name in enumerate(names):
+            a = np.ascontiguousarray(cells[name])
+            if a.dtype.itemsize != 8:
+                raise TypeError(f"column {name}: cells are 8-byte words")
+            keep.append(a)
+            n = a.shape[0]
+            descs[i].cells = a.ctypes.data
+            sc = sidecars.get(name)
+            if sc is not None:
+                sc = np.ascontiguousarray(sc, dtype=np.int32)
+                if sc.shape[0] != n:
+                    raise ValueError(f"column {name}: sidecar length differs")
+                keep.append(sc)
+                descs[i].i32_sidecar = sc.ctypes.data
+            descs[i].coltype = _COLTYPE[coltypes.get(name, "int")]
+            if rows is None:
+                rows = n
+            elif rows != n:
+                raise ValueError("columns differ in length")
+        rows = rows or 0
+        tid = C.c_uint64()
+        self._check(self.lib.tgp_table_register_cells(self.h, descs, len(names), rows, C.byref(tid)),
+                    "tgp_table_register_cells")
+        dtypes = []
+        for i, name in enumerate(names):
+            dt = C.c_uint32()
+            self._check(self.lib.tgp_table_column_dtype(self.h, tid.value, i, C.byref(dt)), "tgp_table_column_dtype")
+            dtypes.append((int(dt.value), descs[i].coltype))
+        return Table(self, int(tid.value), names, rows, dtypes)
+
     def submit(self, queries: Sequence["PreparedQuery"], decode: bool = True) -> "BatchHandle":
         """Runs prepared queries as one batch (tgp_batch_submit); a query may be
         in one unfinished batch at a time."""
