@@ -53,15 +53,24 @@ def peak_hbm() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def traffic_per_launch() -> float | None:
-    """DRAM bytes per scan launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "selective_scan_sum_60M_scan_kernel.md"
+def traffic_per_launch(profile: str = "selective_scan_sum_60M_scan_kernel.md", rows: int | None = None) -> float | None:
+    """DRAM bytes (read + write) per launch from a committed ncu summary, if
+    present; with ``rows``, scaled from the captured row count (the summary
+    says where its traffic grows in proportion to the rows)."""
+    p = ROOT / "profiles" / profile
     if not p.exists():
         return None
+    vals = {}
     for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            return float(line.split(":", 1)[1])
-    return None
+        for k in ("traffic_bytes_per_launch:", "captured_rows:"):
+            if line.startswith(k):
+                vals[k] = float(line.split(":", 1)[1])
+    t = vals.get("traffic_bytes_per_launch:")
+    if t is None:
+        return None
+    if rows is not None and vals.get("captured_rows:"):
+        t *= rows / vals["captured_rows:"]
+    return t
 
 
 class ClockSampler:
@@ -203,6 +212,8 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     CT = datagen.LINEITEM_COLTYPES
     probe_only = None  # (callable, algorithmic bytes per launch) when the step has several kernels
+    traffic = None     # ncu DRAM bytes per launch of the dominant kernel, where a summary is committed
+    variant = None     # (description, callable): the same query with ORDER BY ... LIMIT, timed beside it
     if name == "filtered_group_agg":
         n = args.rows if args.rows != ROWS else 6_000_000
         tpl = workloads.filtered_group_agg()
@@ -217,6 +228,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         cpu_sample = {k: v[:2_000_000] for k, v in host.items()}
         cpu_run = lambda: oracle.aggregate(cpu_sample, CT, tpl.aggs, tpl.group_by, tpl.where)
         cpu_rows = min(n, 2_000_000)
+        traffic = traffic_per_launch("filtered_group_agg_6M_scan_kernel.md", n)
     elif name == "join_group_agg":
         n = args.rows if args.rows != ROWS else 60_000_000
         nb = 1_500_000
@@ -244,6 +256,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
                 f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
         cs = min(n, 2_000_000)
+        traffic = traffic_per_launch("join_group_agg_probe_kernel.md", n)
         cpu_fact = {k: v[:cs] for k, v in fact.items()}
         cpu_run = lambda: oracle.aggregate(cpu_fact, fct, tpl.aggs, tpl.group_by, tpl.where,
                                            build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
@@ -256,6 +269,8 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         aggs = [count_star(), sum_(col("value"))]
         q = t.prepare(aggs, ("key",), None, group_cap=10_000_000)
         step = lambda: q.run(decode=False)
+        variant = ("ORDER BY count(*) DESC LIMIT 10 (tgp_execute_topn)",
+                   lambda: t.aggregate_topn(aggs, ("key",), None, 0, True, 10))
         tables = [(t, host)]
         rows_step, bytes_step, kernel_bytes = n, 12 * n, 12 * n
         dominant = "scan_kernel<MODE_GROUP_HASH> (global open-addressing group table)"
@@ -309,6 +324,18 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
 
+    variant_line = None
+    if variant is not None:
+        for _ in range(2):
+            variant[1]()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        v0.record(stream)
+        for _ in range(steps):
+            variant[1]()
+        v1.record(stream)
+        v1.synchronize()
+        variant_line = {"query": variant[0], "ms_per_step": v0.elapsed_time(v1) / steps}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t0 = time.perf_counter()
@@ -327,11 +354,13 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
                    "l2": "inputs larger than the 126 MB L2" if bytes_step > 126e6 else "inputs smaller than L2"},
         "hbm_gbs": bytes_step * world * steps / (ms / 1000.0) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "kernel_ms": kernel_avg, "kernel": dominant},
+                     "peak_kind": peak_kind, "traffic": traffic, "kernel_ms": kernel_avg, "kernel": dominant},
         "e2e": {"value": rows_step * e2e_steps / (e2e_ms / 1000.0), "unit": "rows/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": None},
         "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
+    if variant_line is not None:
+        line["variant"] = variant_line
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -440,6 +440,19 @@ typedef struct tgp_query_result {
 TGP_API int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out,
                 uint64_t group_cap, tgp_query_result* result);
 
+/* Executes one aggregation query with ORDER BY aggregate `order_agg`
+ * (ascending, or descending when `descending` != 0) LIMIT `limit`: the
+ * grouped-result ordering of apply_order_by_grouped / topn_indices
+ * (src/engine/query_interpreter/expr.rs:2378-2420, 56-110). keys_out and
+ * vals_out hold `limit` groups; result->ngroups is the number returned,
+ * min(limit, groups). Groups are ordered by the aggregate's exact value (AVG:
+ * its f64), ties in ascending key order. The reference compares the result
+ * cells as f64 bit patterns, which orders non-negative integers the same way
+ * and negative integer results differently. Hash-grouped results are ordered
+ * on the device, and only the returned groups are formatted and copied. */
+TGP_API int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_agg, int descending, uint64_t limit,
+                             uint64_t* keys_out, tgp_agg_value* vals_out, tgp_query_result* result);
+
 /* ------------------------------------------------------------------------ */
 /* Hash join (src/engine/query_interpreter/join.rs:544-939)                  */
 /* ------------------------------------------------------------------------ */

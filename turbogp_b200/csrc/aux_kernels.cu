@@ -461,6 +461,74 @@ size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits) {
     return n * 24 + tmp + 256;
 }
 
+// Radix keys of one LSD pass of the top-N order: an unsigned image of the
+// ordering value whose ascending order is the wanted order (complemented for
+// descending). int128 sums take two passes: low limb (pass 0), then the
+// signed high limb (pass 1). idx[i] carries the slot index along.
+__global__ void order_keys_kernel(const unsigned long long* packed, const uint32_t* perm, uint64_t n, uint32_t hstride,
+                                  const TopNSpec S, int pass, unsigned long long* keys, uint32_t* idx) {
+    constexpr unsigned long long kSign = 0x8000000000000000ull;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t p = perm[i];
+        const unsigned long long* s = packed + static_cast<uint64_t>(p) * hstride;
+        unsigned long long k;
+        if (S.val < 0) {
+            k = s[1];  // row count (unsigned)
+        } else {
+            const unsigned long long* v = s + 2 + 2 * S.val;
+            if (S.kind == VK_MIN || S.kind == VK_MAX) {
+                k = v[0] ^ kSign;
+            } else if (S.func == TGP_AGG_AVG) {
+                const unsigned long long cnt = s[1];
+                const uint64_t lo = v[0];
+                const int64_t hi = S.sum64 ? (static_cast<int64_t>(v[0]) >> 63) : static_cast<int64_t>(v[1]);
+                const double f = cnt ? i128_to_f64_rn(lo, hi) / static_cast<double>(cnt) : 0.0;
+                const unsigned long long u = static_cast<unsigned long long>(__double_as_longlong(f));
+                k = (u & kSign) ? ~u : (u | kSign);
+            } else if (S.sum64) {
+                k = v[0] ^ kSign;
+            } else {
+                k = pass == 0 ? v[0] : (v[1] ^ kSign);
+            }
+        }
+        keys[i] = S.desc ? ~k : k;
+        idx[i] = p;
+    }
+}
+
+cudaError_t topn_hash_groups(const unsigned long long* packed, uint64_t n, const HashFormat& F, uint32_t key_bits,
+                             const TopNSpec& S, uint64_t limit, void* scratch, size_t scratch_bytes,
+                             uint64_t* keys_out, tgp_agg_value* vals_out, int sms, cudaStream_t st) {
+    if (n == 0 || limit == 0) return cudaSuccess;
+    unsigned long long* k0 = static_cast<unsigned long long*>(scratch);
+    unsigned long long* k1 = k0 + n;
+    uint32_t* i0 = reinterpret_cast<uint32_t*>(k1 + n);
+    uint32_t* i1 = i0 + n;
+    uint8_t* tmp = reinterpret_cast<uint8_t*>(i1 + n);
+    const size_t head = n * 16 + n * 8;
+    size_t tmp_bytes = scratch_bytes > head ? scratch_bytes - head : 0;
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    // Key order first, so the stable value passes leave ties in key order.
+    extract_keys_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(packed, n, F.hstride, k0, i0);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, i0, i1, static_cast<int>(n), 0,
+                                                    static_cast<int>(key_bits ? key_bits : 1), st);
+    if (e != cudaSuccess) return e;
+    const bool wide = S.val >= 0 && S.kind != VK_MIN && S.kind != VK_MAX && S.func != TGP_AGG_AVG && !S.sum64;
+    for (int pass = 0; pass < (wide ? 2 : 1); ++pass) {
+        order_keys_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(packed, i1, n, F.hstride, S, pass,
+                                                                                 k0, i0);
+        e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, i0, i1, static_cast<int>(n), 0, 64, st);
+        if (e != cudaSuccess) return e;
+    }
+    const uint64_t m = limit < n ? limit : n;
+    uint64_t fb = (m + kAuxThreads - 1) / kAuxThreads;
+    if (fb > static_cast<uint64_t>(sms) * 8) fb = static_cast<uint64_t>(sms) * 8;
+    format_hash_groups_kernel<<<static_cast<unsigned>(fb), kAuxThreads, 0, st>>>(packed, i1, m, F, keys_out, vals_out);
+    return cudaGetLastError();
+}
+
 // A bounded busy wait of one thread (profiling: keeps the GPU busy while the
 // host submits the launch that follows).
 __global__ void delay_kernel(uint64_t ns) {

@@ -1585,10 +1585,44 @@ static int decode_direct(tgp_ctx* ctx, const QueryState& qs, const unsigned long
         return TGP_OK;
     }
 
-int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
-                tgp_query_result* result) {
+// ORDER BY one aggregate, LIMIT n (tgp_execute_topn).
+struct TopNReq {
+    uint32_t agg;
+    bool desc;
+    uint64_t limit;
+};
+
+// Keeps the first min(limit, n) of n decoded groups in the order of one
+// aggregate's exact value (AVG: its f64), ties in the given (key) order.
+static void host_topn(const TopNReq& tn, uint32_t nkey, uint32_t nagg, const std::vector<uint64_t>& keys,
+                      const std::vector<tgp_agg_value>& vals, uint64_t n, uint32_t func, uint64_t* keys_out,
+                      tgp_agg_value* vals_out, tgp_query_result* result) {
+    std::vector<uint64_t> order(n);
+    for (uint64_t i = 0; i < n; ++i) order[i] = i;
+    auto less = [&](uint64_t x, uint64_t y) {
+        const tgp_agg_value& a = vals[x * nagg + tn.agg];
+        const tgp_agg_value& b = vals[y * nagg + tn.agg];
+        if (func == TGP_AGG_AVG) return tn.desc ? a.as_f64 > b.as_f64 : a.as_f64 < b.as_f64;
+        const __int128 va = (static_cast<__int128>(a.hi) << 64) | static_cast<__int128>(a.lo);
+        const __int128 vb = (static_cast<__int128>(b.hi) << 64) | static_cast<__int128>(b.lo);
+        return tn.desc ? va > vb : va < vb;
+    };
+    std::stable_sort(order.begin(), order.end(), less);
+    const uint64_t m = std::min<uint64_t>(tn.limit, n);
+    for (uint64_t i = 0; i < m; ++i) {
+        if (keys_out)
+            for (uint32_t k = 0; k < nkey; ++k) keys_out[i * nkey + k] = keys[order[i] * nkey + k];
+        if (vals_out)
+            for (uint32_t a = 0; a < nagg; ++a) vals_out[i * nagg + a] = vals[order[i] * nagg + a];
+    }
+    result->ngroups = m;
+}
+
+static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out,
+                        uint64_t group_cap, tgp_query_result* result, const TopNReq* tn) {
     if (!ctx || !q || !result) return fail(ctx, TGP_INVALID_ARG, "null argument");
     std::memset(result, 0, sizeof(*result));
+    if (tn && tn->agg >= q->nagg) return fail(ctx, TGP_INVALID_ARG, "ORDER BY aggregate index out of range");
     QueryState qs;
     TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem()));
     Builder& b = *qs.b;
@@ -1659,7 +1693,14 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     result->flags = (err & kErrRowOverflow) ? TGP_RESULT_ROW_OVERFLOW : 0u;
     const uint32_t nagg = q->nagg;
 
-    if (mode != MODE_GROUP_HASH) return decode_direct(ctx, qs, hb, keys_out, vals_out, group_cap, result);
+    if (mode != MODE_GROUP_HASH) {
+        if (!tn) return decode_direct(ctx, qs, hb, keys_out, vals_out, group_cap, result);
+        std::vector<uint64_t> ak(std::max<uint64_t>(1, ngroups_direct * q->ngroup));
+        std::vector<tgp_agg_value> av(std::max<uint64_t>(1, ngroups_direct * q->nagg));
+        TGP_TRY(decode_direct(ctx, qs, hb, ak.data(), av.data(), ngroups_direct, result));
+        host_topn(*tn, q->ngroup, q->nagg, ak, av, result->ngroups, amap[tn->agg].func, keys_out, vals_out, result);
+        return TGP_OK;
+    }
 
     // Hash groups: gather occupied slots, sort by key on the host.
     // Counter word 2 counts the gathered slots.
@@ -1673,7 +1714,7 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
     TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
     result->ngroups = ng;
-    if (ng > group_cap) {
+    if (!tn && ng > group_cap) {
         dev_free(ctx, packed);
         return fail(ctx, TGP_CAPACITY, "group buffer too small");
     }
@@ -1696,8 +1737,12 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
             F.val[a] = static_cast<int8_t>(amap[a].val);
             F.kind[a] = amap[a].val >= 0 ? P.val[amap[a].val].kind : VK_SUM;
         }
-        const size_t sbytes = format_hash_groups_scratch(ng, total_bits);
-        const size_t kbytes = (keys_out ? ng * q->ngroup * 8 : 0), vbytes = (vals_out ? ng * nagg * sizeof(tgp_agg_value) : 0);
+        // Top-N: only the first min(limit, ng) groups in the aggregate's order
+        // are formatted and copied.
+        const uint64_t nout = tn ? std::min<uint64_t>(tn->limit, ng) : ng;
+        const size_t sbytes = format_hash_groups_scratch(ng, tn ? 64u : total_bits);
+        const size_t kbytes = (keys_out ? nout * q->ngroup * 8 : 0),
+                     vbytes = (vals_out ? nout * nagg * sizeof(tgp_agg_value) : 0);
         uint8_t* buf = nullptr;
         const size_t kofs = (sbytes + 255) & ~size_t{255}, vofs = kofs + ((kbytes + 255) & ~size_t{255});
         if (int st = dev_alloc(ctx, reinterpret_cast<void**>(&buf), vofs + vbytes, "group format allocation failed")) {
@@ -1706,7 +1751,20 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         }
         uint64_t* dkeys = kbytes ? reinterpret_cast<uint64_t*>(buf + kofs) : nullptr;
         tgp_agg_value* dvals = vbytes ? reinterpret_cast<tgp_agg_value*>(buf + vofs) : nullptr;
-        cudaError_t e = format_hash_groups(packed, ng, F, total_bits, buf, sbytes, dkeys, dvals, ctx->sms, ctx->stream);
+        cudaError_t e;
+        if (tn) {
+            TopNSpec S;
+            std::memset(&S, 0, sizeof(S));
+            S.val = amap[tn->agg].val;
+            S.kind = static_cast<uint8_t>(S.val >= 0 ? P.val[S.val].kind : VK_SUM);
+            S.func = static_cast<uint8_t>(amap[tn->agg].func);
+            S.desc = tn->desc ? 1 : 0;
+            S.sum64 = P.sum64 ? 1 : 0;
+            e = topn_hash_groups(packed, ng, F, total_bits, S, nout, buf, sbytes, dkeys, dvals, ctx->sms, ctx->stream);
+            result->ngroups = nout;
+        } else {
+            e = format_hash_groups(packed, ng, F, total_bits, buf, sbytes, dkeys, dvals, ctx->sms, ctx->stream);
+        }
         if (e == cudaSuccess && kbytes) e = cudaMemcpyAsync(keys_out, dkeys, kbytes, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess && vbytes) e = cudaMemcpyAsync(vals_out, dvals, vbytes, cudaMemcpyDeviceToHost, ctx->stream);
         dev_free(ctx, buf);
@@ -1714,6 +1772,10 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("group format: ") + cudaGetErrorString(e));
         return TGP_OK;
+    }
+    if (tn) {
+        dev_free(ctx, packed);
+        return fail(ctx, TGP_UNSUPPORTED, "ORDER BY with more aggregates than the device formatter takes");
     }
     std::vector<unsigned long long> slots(ng * P.hstride);
     if (ng) TGP_CUDA(cudaMemcpyAsync(slots.data(), packed, ng * P.hstride * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1745,6 +1807,17 @@ int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_va
         }
     }
     return TGP_OK;
+}
+
+int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tgp_agg_value* vals_out, uint64_t group_cap,
+                tgp_query_result* result) {
+    return execute_impl(ctx, q, keys_out, vals_out, group_cap, result, nullptr);
+}
+
+int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_agg, int descending, uint64_t limit,
+                     uint64_t* keys_out, tgp_agg_value* vals_out, tgp_query_result* result) {
+    const TopNReq tn{order_agg, descending != 0, limit};
+    return execute_impl(ctx, q, keys_out, vals_out, limit, result, &tn);
 }
 
 // --------------------------------------------------------------------------

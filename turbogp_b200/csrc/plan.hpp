@@ -325,6 +325,16 @@ struct HashFormat {
     uint8_t kind[kMaxFormatAggs];   // VK_* of that value
 };
 
+// ORDER BY one aggregate of a hash-grouped result (top-N): which slot holds
+// the ordering value and how it compares.
+struct TopNSpec {
+    int32_t val;      // value index, -1 = the row count (COUNT(*))
+    uint8_t kind;     // VK_* of that value
+    uint8_t func;     // tgp_agg_func of the ordering aggregate (AVG orders by its f64)
+    uint8_t desc;     // 1 = descending
+    uint8_t sum64;    // value limbs hold int64 sums (hi = sign of lo)
+};
+
 static_assert(sizeof(Plan) % 16 == 0, "plans are copied in 16-byte words");
 
 // A range of tiles of one table, processed by one CTA of a batch launch for

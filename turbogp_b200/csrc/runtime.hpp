@@ -61,6 +61,12 @@ cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, con
                                void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
                                int sms, cudaStream_t st);
 size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits);
+// The first min(limit, n) gathered groups in the order of one aggregate
+// (ties in ascending key order), formatted like format_hash_groups.
+// Scratch: format_hash_groups_scratch(n, 64) bytes.
+cudaError_t topn_hash_groups(const unsigned long long* packed, uint64_t n, const HashFormat& F, uint32_t key_bits,
+                             const TopNSpec& S, uint64_t limit, void* scratch, size_t scratch_bytes,
+                             uint64_t* keys_out, tgp_agg_value* vals_out, int sms, cudaStream_t st);
 // One thread that spins on %globaltimer for `ns` nanoseconds (at most 1 ms).
 cudaError_t launch_delay(uint64_t ns, cudaStream_t st);
 cudaError_t launch_fill_slots(unsigned long long* p, uint64_t nslots, const SlotImage& img, int sms, cudaStream_t st);

@@ -556,6 +556,26 @@ class Table(Schema):
                   group_cap: int | None = None) -> QueryOutput:
         return self.prepare(aggs, group_by, where, join, probe_key, group_cap or 1024).run()
 
+    def aggregate_topn(self, aggs: Sequence[Agg], group_by: Sequence[Col | str], where: Pred | None, order_by: int,
+                       descending: bool, limit: int, join: "JoinTable | None" = None,
+                       probe_key: str | None = None) -> QueryOutput:
+        """GROUP BY ... ORDER BY aggs[order_by] [DESC] LIMIT limit
+        (tgp_execute_topn): at most ``limit`` groups in the aggregate's order,
+        ties in ascending key order."""
+        build = join.build if join is not None else None
+        q, keep = self.lower_query(aggs, group_by, where, build, probe_key)
+        q.table = self.id
+        if join is not None:
+            q.join = join.id
+        nk, na = len(group_by), len(aggs)
+        keys = np.zeros(max(1, limit * max(1, nk)), dtype=np.uint64)
+        vals = (A.AggValue * max(1, limit * max(1, na)))()
+        res = A.QueryResult()
+        self.ctx._check(self.ctx.lib.tgp_execute_topn(self.ctx.h, C.byref(q), order_by, 1 if descending else 0, limit,
+                                                      keys.ctypes.data, vals, C.byref(res)), "tgp_execute_topn")
+        ks, vs = decode_groups(keys, vals, int(res.ngroups), nk, na)
+        return QueryOutput(ks, vs, int(res.rows_scanned), int(res.rows_selected), int(res.flags))
+
     def join_build(self, key: str, where: Pred | None = None) -> "JoinTable":
         nodes, n = self.lower_pred(where)
         jid = C.c_uint64()
