@@ -453,6 +453,17 @@ TGP_API int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
 TGP_API int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_agg, int descending, uint64_t limit,
                              uint64_t* keys_out, tgp_agg_value* vals_out, tgp_query_result* result);
 
+/* COUNT(DISTINCT column) over the rows passing `pred` (all rows when npred =
+ * 0), as the reference evaluates it (aggregate.rs:1301-1325,
+ * src/exec/hll.rs): with fewer than 100,000 selected rows the exact number of
+ * distinct cells (*method = 0); otherwise the HyperLogLog estimate with 2^14
+ * registers over xxh3_64 of each selected row's u64 cell, including its
+ * small-range linear counting (*method = 1, ~0.81 % standard error). The
+ * registers are exact, so the estimate equals the reference's for the same
+ * cells. `method` may be NULL. */
+TGP_API int tgp_count_distinct(tgp_ctx* ctx, tgp_table_id table, uint32_t column, const tgp_pred_node* pred,
+                               uint32_t npred, uint64_t* count, uint32_t* method);
+
 /* ------------------------------------------------------------------------ */
 /* Hash join (src/engine/query_interpreter/join.rs:544-939)                  */
 /* ------------------------------------------------------------------------ */

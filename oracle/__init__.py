@@ -72,6 +72,13 @@ def _sig(lib):
                                    C.c_uint32, C.POINTER(A.ColumnDesc), C.c_uint32, C.c_uint64, C.c_uint32,
                                    C.POINTER(A.PredNode), C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64,
                                    C.POINTER(C.c_uint64)]
+    lib.orc_xxh3_u64.argtypes = [C.c_uint64]
+    lib.orc_xxh3_u64.restype = C.c_uint64
+    lib.orc_hll_estimate.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+    lib.orc_hll_estimate.restype = C.c_uint64
+    lib.orc_count_distinct.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_uint32)]
+    lib.orc_count_distinct.restype = None
     lib.orc_seq_sum_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
     lib.orc_seq_sum_f64.restype = None
     lib.orc_kernel_execute.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(A.KernelParams),
@@ -166,3 +173,26 @@ def kernel_execute(op: int, cells: np.ndarray, params, probe_cells: np.ndarray |
                                  b.shape[0], C.byref(p), C.byref(r)) != 0:
         raise ValueError("operator without an oracle")
     return int(r.count), float(r.sum), int(r.mask)
+
+
+def xxh3_u64(v: int) -> int:
+    """xxh3_64 of the 8 little-endian bytes of a cell (the oracle's restatement)."""
+    return int(_lib().orc_xxh3_u64(v & 0xFFFFFFFFFFFFFFFF))
+
+
+def hll_estimate(cells: np.ndarray, sel_bitmap: np.ndarray | None = None) -> int:
+    """The reference's HyperLogLog estimate over the (selected) u64 cells."""
+    c = np.ascontiguousarray(cells).view(np.uint64)
+    return int(_lib().orc_hll_estimate(c.ctypes.data if c.size else None, c.shape[0],
+                                       sel_bitmap.ctypes.data if sel_bitmap is not None else None))
+
+
+def count_distinct(cells: np.ndarray, sel_bitmap: np.ndarray | None = None) -> tuple[int, str]:
+    """COUNT(DISTINCT) of u64 cells as the reference evaluates it: (count,
+    'exact' | 'hll')."""
+    c = np.ascontiguousarray(cells).view(np.uint64)
+    cnt, method = C.c_uint64(), C.c_uint32()
+    _lib().orc_count_distinct(c.ctypes.data if c.size else None, c.shape[0],
+                              sel_bitmap.ctypes.data if sel_bitmap is not None else None, C.byref(cnt),
+                              C.byref(method))
+    return int(cnt.value), ("hll" if method.value else "exact")

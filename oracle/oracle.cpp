@@ -384,6 +384,69 @@ int orc_kernel_execute(uint32_t op, const uint64_t* input, const uint64_t* input
     }
 }
 
+// XXH3-64 (xxhash-rust 0.8, `xxh3_64`) of the 8 little-endian bytes of a
+// cell, seed 0, default secret: the published algorithm's 4-to-8-byte case,
+// restated from the xxHash specification. Only the secret's bytes 8..24 enter
+// this case (as one xor constant).
+static uint64_t xxh3_8bytes(uint64_t v) {
+    const uint64_t lo = v & 0xffffffffull, hi = v >> 32;
+    const uint64_t secret8 = 0x1cad21f72c81017cull, secret16 = 0xdb979083e96dd4deull;
+    uint64_t x = (hi + (lo << 32)) ^ (secret8 ^ secret16);
+    auto rotl = [](uint64_t a, int r) { return (a << r) | (a >> (64 - r)); };
+    x ^= rotl(x, 49) ^ rotl(x, 24);
+    x *= 0x9fb21c651e98df25ull;
+    x ^= (x >> 35) + 8;
+    x *= 0x9fb21c651e98df25ull;
+    return x ^ (x >> 28);
+}
+
+uint64_t orc_xxh3_u64(uint64_t v) { return xxh3_8bytes(v); }
+
+// The reference's HyperLogLog (exec/hll.rs): 2^14 u8 registers, register
+// h >> 50 keeps the max of leading_zeros(h << 14) + 1, estimate with its
+// small-range linear counting, truncated to u64.
+uint64_t orc_hll_estimate(const uint64_t* cells, uint64_t n, const uint8_t* sel) {
+    std::vector<uint8_t> reg(1u << 14, 0);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (sel && !((sel[i >> 3] >> (i & 7)) & 1)) continue;
+        const uint64_t h = xxh3_8bytes(cells[i]);
+        const uint64_t w = h << 14;
+        const uint8_t lz = static_cast<uint8_t>((w ? __builtin_clzll(w) : 64) + 1);
+        uint8_t& r = reg[h >> 50];
+        if (lz > r) r = lz;
+    }
+    const double m = 16384.0, alpha = 0.7213 / (1.0 + 1.079 / m);
+    double sum = 0.0;
+    uint64_t zeros = 0;
+    for (uint8_t r : reg) {
+        double p = 1.0;  // 2^-r by repeated halving (exact)
+        for (int k = 0; k < r; ++k) p *= 0.5;
+        sum += p;
+        if (r == 0) ++zeros;
+    }
+    const double raw = alpha * m * m / sum;
+    const double est = (raw <= 2.5 * m && zeros > 0) ? m * std::log(m / static_cast<double>(zeros)) : raw;
+    return static_cast<uint64_t>(est);
+}
+
+// COUNT(DISTINCT col) as the reference evaluates it (aggregate.rs:1301-1325):
+// exact below 100,000 selected rows (method 0), else the HyperLogLog
+// estimate (method 1). `sel` is an LSB-first bitmap or NULL (all rows).
+void orc_count_distinct(const uint64_t* cells, uint64_t n, const uint8_t* sel, uint64_t* count, uint32_t* method) {
+    uint64_t nsel = 0;
+    for (uint64_t i = 0; i < n; ++i) nsel += !sel || ((sel[i >> 3] >> (i & 7)) & 1);
+    if (nsel < 100000) {
+        std::unordered_set<uint64_t> seen;
+        for (uint64_t i = 0; i < n; ++i)
+            if (!sel || ((sel[i >> 3] >> (i & 7)) & 1)) seen.insert(cells[i]);
+        *count = seen.size();
+        *method = 0;
+        return;
+    }
+    *count = orc_hll_estimate(cells, n, sel);
+    *method = 1;
+}
+
 // Sequential f64 accumulation in row order, one running sum per group:
 // out[group[i]] += terms[i] for i = 0..n-1. This is the order of the
 // reference's per-group sums: each group's row index list is ascending

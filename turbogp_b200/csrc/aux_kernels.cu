@@ -250,6 +250,133 @@ cudaError_t launch_count_distinct(const unsigned long long* x, uint64_t n, unsig
 }
 
 // ---------------------------------------------------------------------------
+// COUNT(DISTINCT col): the u64 cell of row i of a resident column (narrow
+// values widen as the reference's cells hold them), rows filtered by an
+// optional selection bitmap (LSB-first u32 words).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long cell_at(const uint8_t* col, uint32_t dtype, uint64_t i) {
+    if (dtype == DT_U8) return col[i];
+    if (dtype == DT_I32)
+        return static_cast<unsigned long long>(static_cast<long long>(reinterpret_cast<const int32_t*>(col)[i]));
+    return reinterpret_cast<const unsigned long long*>(col)[i];
+}
+
+__device__ __forceinline__ bool row_selected(const uint32_t* bitmap, uint64_t i) {
+    return !bitmap || ((bitmap[i >> 5] >> (i & 31)) & 1u);
+}
+
+// XXH3-64 of the 8 little-endian bytes of v with seed 0 and the default
+// secret: the specification's 4-to-8-byte path (input = low word << 32 | high
+// word, xored with secret[8..16) ^ secret[16..24), then the rrmxmx finaliser
+// with length 8). This is the hash the reference's HyperLogLog applies to
+// each cell (xxh3_64 of value.to_le_bytes(), exec/hll.rs:34-37).
+__device__ __forceinline__ unsigned long long xxh3_u64(unsigned long long v) {
+    constexpr unsigned long long kBitflip = 0x1cad21f72c81017cull ^ 0xdb979083e96dd4deull;
+    constexpr unsigned long long kMul = 0x9fb21c651e98df25ull;
+    unsigned long long h = ((v << 32) | (v >> 32)) ^ kBitflip;
+    h ^= ((h << 49) | (h >> 15)) ^ ((h << 24) | (h >> 40));
+    h *= kMul;
+    h ^= (h >> 35) + 8ull;
+    h *= kMul;
+    return h ^ (h >> 28);
+}
+
+// Exact distinct count of the selected cells (as count_distinct_kernel).
+__global__ void __launch_bounds__(kAuxThreads) distinct_cells_kernel(const uint8_t* col, uint32_t dtype, uint64_t n,
+                                                                    const uint32_t* bitmap, unsigned long long* set,
+                                                                    uint64_t mask, uint32_t log2cap,
+                                                                    unsigned long long* counters, uint32_t* err) {
+    unsigned long long local = 0;
+    bool saw_empty = false;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (!row_selected(bitmap, i)) continue;
+        const unsigned long long k = cell_at(col, dtype, i);
+        if (k == ~0ull) {
+            saw_empty = true;
+            continue;
+        }
+        uint64_t h = hash_slot(k, log2cap);
+        bool placed = false;
+        for (uint64_t p = 0; p <= mask; ++p) {
+            unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(set + h);
+            if (cur == k) {
+                placed = true;
+                break;
+            }
+            if (cur == ~0ull) {
+                cur = atomicCAS(set + h, ~0ull, k);
+                if (cur == ~0ull) {
+                    ++local;
+                    placed = true;
+                    break;
+                }
+                if (cur == k) {
+                    placed = true;
+                    break;
+                }
+            }
+            h = (h + 1) & mask;
+        }
+        if (!placed) atomicOr(err, kErrHashFull);
+    }
+    for (int d = 16; d > 0; d >>= 1) local += __shfl_down_sync(0xffffffffu, local, d);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(counters, local);
+    if (saw_empty) atomicOr(counters + 1, 1ull);
+}
+
+cudaError_t launch_distinct_cells(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap,
+                                  unsigned long long* set, uint64_t mask, uint32_t log2cap,
+                                  unsigned long long* counters, uint32_t* err, int sms, cudaStream_t st) {
+    uint64_t blocks = (n + kAuxThreads - 1) / kAuxThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    if (blocks == 0) return cudaSuccess;
+    distinct_cells_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(col, dtype, n, bitmap, set, mask,
+                                                                                log2cap, counters, err);
+    return cudaGetLastError();
+}
+
+// HyperLogLog registers (2^14, exec/hll.rs:11-51): for each selected cell,
+// h = xxh3(cell), register h >> 50 takes the max of
+// leading_zeros(h << 14) + 1. Each CTA keeps its registers in shared memory
+// (a shared atomic max only when the value could raise the register) and
+// merges them into the global ones at the end.
+constexpr int kHllRegs = 1 << 14;
+constexpr int kHllThreads = 512;
+
+__global__ void __launch_bounds__(kHllThreads) hll_kernel(const uint8_t* col, uint32_t dtype, uint64_t n,
+                                                         const uint32_t* bitmap, uint32_t* regs) {
+    extern __shared__ uint32_t sreg[];
+    for (int r = threadIdx.x; r < kHllRegs; r += blockDim.x) sreg[r] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (!row_selected(bitmap, i)) continue;
+        const unsigned long long h = xxh3_u64(cell_at(col, dtype, i));
+        const uint32_t idx = static_cast<uint32_t>(h >> 50);
+        const unsigned long long w = h << 14;
+        const uint32_t lz = (w ? static_cast<uint32_t>(__clzll(static_cast<long long>(w))) : 64u) + 1u;
+        if (lz > *reinterpret_cast<volatile uint32_t*>(sreg + idx)) atomicMax(sreg + idx, lz);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < kHllRegs; r += blockDim.x)
+        if (sreg[r] && sreg[r] > *reinterpret_cast<volatile uint32_t*>(regs + r)) atomicMax(regs + r, sreg[r]);
+}
+
+cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint32_t* regs,
+                       int sms, cudaStream_t st) {
+    const size_t smem = kHllRegs * sizeof(uint32_t);
+    const cudaError_t e = cudaFuncSetAttribute(hll_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    uint64_t blocks = (n + kHllThreads - 1) / kHllThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 2) blocks = static_cast<uint64_t>(sms) * 2;
+    if (blocks == 0) return cudaSuccess;
+    hll_kernel<<<static_cast<unsigned>(blocks), kHllThreads, smem, st>>>(col, dtype, n, bitmap, regs);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Join pairs: sort packed (probe << 32 | build) pairs, then split.
 // ---------------------------------------------------------------------------
 cudaError_t sort_pairs(const unsigned long long* in, unsigned long long* out, uint64_t n, void* tmp,

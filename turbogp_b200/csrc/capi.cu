@@ -1221,6 +1221,98 @@ int tgp_filter(tgp_ctx* ctx, tgp_table_id table, const tgp_pred_node* pred, uint
     return filter_impl(ctx, T, pred, npred, bitmap_out, rowids_out, rowids_cap, count_out, 0);
 }
 
+// HyperLogLog estimate from 2^14 registers, in the reference's arithmetic
+// (exec/hll.rs:53-76): sequential f64 sum of 2^-r in register order, raw =
+// alpha * m^2 / sum, linear counting m * ln(m / zeros) when raw <= 2.5 m and
+// some register is zero, truncated to u64.
+static uint64_t hll_estimate(const std::vector<uint32_t>& regs) {
+    constexpr double m = 16384.0;
+    constexpr double alpha = 0.7213 / (1.0 + 1.079 / m);
+    double sum = 0.0;
+    uint64_t zeros = 0;
+    for (uint32_t r : regs) {
+        sum += std::ldexp(1.0, -static_cast<int>(r));
+        zeros += r == 0;
+    }
+    const double raw = alpha * m * m / sum;
+    const double est = (raw <= 2.5 * m && zeros > 0) ? m * std::log(m / static_cast<double>(zeros)) : raw;
+    return static_cast<uint64_t>(est);
+}
+
+int tgp_count_distinct(tgp_ctx* ctx, tgp_table_id table, uint32_t column, const tgp_pred_node* pred, uint32_t npred,
+                       uint64_t* count, uint32_t* method) {
+    if (!ctx || !count) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    *count = 0;
+    if (method) *method = 0;
+    const Table* T;
+    TGP_TRY(get_table(ctx, table, &T));
+    if (column >= T->cols.size()) return fail(ctx, TGP_INVALID_ARG, "column index out of range");
+    const Column& c = T->cols[column];
+    const uint64_t n = T->rows;
+    // Selection: all rows, or the WHERE bitmap.
+    uint32_t* bm = nullptr;
+    uint64_t nsel = n;
+    if (npred) {
+        const uint64_t words = std::max<uint64_t>(1, (n + 31) / 32);
+        TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&bm), words * 4, "selection bitmap allocation failed"));
+        int st = TGP_OK;
+        if (cudaMemsetAsync(bm, 0, words * 4, ctx->stream) != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, "memset");
+        if (st == TGP_OK) st = filter_impl(ctx, T, pred, npred, reinterpret_cast<uint8_t*>(bm), nullptr, 0, &nsel, 0);
+        if (st != TGP_OK) {
+            dev_free(ctx, bm);
+            return st;
+        }
+    }
+    int st = TGP_OK;
+    // The reference counts exactly below 100,000 selected rows and with a
+    // HyperLogLog from there on (aggregate.rs:1308-1325, hll.rs:103-109).
+    if (nsel < 100000) {
+        const uint64_t cap = next_pow2(std::max<uint64_t>(16, 2 * nsel));
+        Carve cv;
+        st = arena_reserve(ctx, cap * 8 + 256, &cv);
+        if (st == TGP_OK && nsel) {
+            unsigned long long* set = cv.take<unsigned long long>(cap);
+            unsigned long long* counters = cv.take<unsigned long long>(2);
+            uint32_t* err = cv.take<uint32_t>(4);
+            unsigned long long hc[2] = {0, 0};
+            uint32_t herr = 0;
+            cudaError_t e = cudaMemsetAsync(set, 0xff, cap * 8, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 16, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 16, ctx->stream);
+            if (e == cudaSuccess)
+                e = launch_distinct_cells(c.dptr, c.dtype, n, bm, set, cap - 1, log2u(cap), counters, err, ctx->sms,
+                                          ctx->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hc, counters, 16, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, std::string("distinct: ") + cudaGetErrorString(e));
+            if (st == TGP_OK) st = check_kernel_err(ctx, herr);
+            if (st == TGP_OK) *count = hc[0] + (hc[1] ? 1 : 0);
+        }
+    } else {
+        Carve cv;
+        st = arena_reserve(ctx, 16384 * 4 + 256, &cv);
+        if (st == TGP_OK) {
+            uint32_t* regs = cv.take<uint32_t>(16384);
+            std::vector<uint32_t> h(16384);
+            cudaError_t e = cudaMemsetAsync(regs, 0, 16384 * 4, ctx->stream);
+            if (e == cudaSuccess) e = launch_hll(c.dptr, c.dtype, n, bm, regs, ctx->sms, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), regs, 16384 * 4, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, std::string("hyperloglog: ") + cudaGetErrorString(e));
+            if (st == TGP_OK) {
+                *count = hll_estimate(h);
+                if (method) *method = 1;
+            }
+        }
+    }
+    if (bm) {
+        cudaStreamSynchronize(ctx->stream);
+        dev_free(ctx, bm);
+    }
+    return st;
+}
+
 // --------------------------------------------------------------------------
 // Aggregation queries
 // --------------------------------------------------------------------------

@@ -46,6 +46,14 @@ cudaError_t launch_compact(const uint32_t* bitmap, uint64_t nwords, uint64_t nti
                            const unsigned long long* tile_base, uint32_t* rowids, uint64_t cap,
                            cudaStream_t st);
 cudaError_t launch_sum_f64(const double* x, uint64_t n, double* out, int blocks, cudaStream_t st);
+// Exact distinct count / HyperLogLog registers (2^14 u32, zeroed by the
+// caller) of the cells of a resident column, rows filtered by an optional
+// selection bitmap.
+cudaError_t launch_distinct_cells(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap,
+                                  unsigned long long* set, uint64_t mask, uint32_t log2cap,
+                                  unsigned long long* counters, uint32_t* err, int sms, cudaStream_t st);
+cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint32_t* regs,
+                       int sms, cudaStream_t st);
 cudaError_t launch_count_distinct(const unsigned long long* x, uint64_t n, unsigned long long* set,
                                   uint64_t mask, uint32_t log2cap, unsigned long long* counters,
                                   uint32_t* err, int blocks, cudaStream_t st);

@@ -576,6 +576,15 @@ class Table(Schema):
         ks, vs = decode_groups(keys, vals, int(res.ngroups), nk, na)
         return QueryOutput(ks, vs, int(res.rows_scanned), int(res.rows_selected), int(res.flags))
 
+    def count_distinct(self, column: str, where: Pred | None = None) -> tuple[int, str]:
+        """COUNT(DISTINCT column) [WHERE where] (tgp_count_distinct): (count,
+        'exact' | 'hll'), exact below 100,000 selected rows as in the reference."""
+        nodes, n = self.lower_pred(where)
+        cnt, method = C.c_uint64(), C.c_uint32()
+        self.ctx._check(self.ctx.lib.tgp_count_distinct(self.ctx.h, self.id, self.index(column), nodes, n,
+                                                        C.byref(cnt), C.byref(method)), "tgp_count_distinct")
+        return int(cnt.value), ("hll" if method.value else "exact")
+
     def join_build(self, key: str, where: Pred | None = None) -> "JoinTable":
         nodes, n = self.lower_pred(where)
         jid = C.c_uint64()
