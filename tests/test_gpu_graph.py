@@ -7,7 +7,7 @@ import pytest
 import oracle
 from turbogp_b200 import _capi as A
 from turbogp_b200 import datagen, workloads
-from turbogp_b200.engine import avg, col, count_star, max_, min_, sum_
+from turbogp_b200.engine import avg, build_col, col, count_star, max_, min_, sum_
 
 from test_gpu_parity import same_query
 
@@ -76,8 +76,21 @@ def test_graph_join_aggregate(ctx):
         for _ in range(2):
             same_query(g.run(), o)
         g.drop_graph()
-    # A dropped join invalidates the graph.
+    # Another key layout rewrites the join's payload array in place: the
+    # graph reading the old layout refuses to run; a fresh capture runs.
     g = f.prepare(tpl.aggs, tpl.group_by, None, join=j, probe_key="fk").capture()
+    other = (build_col("segment"), "flag_a")
+    same_query(f.aggregate(tpl.aggs, other, None, join=j, probe_key="fk"),
+               oracle.aggregate(fact, fct, tpl.aggs, other, None,
+                                build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where), probe_key="fk"))
+    with pytest.raises(A.TgpError) as e:
+        g.run()
+    assert e.value.status == A.NOT_FOUND
+    g.capture()
+    same_query(g.run(), oracle.aggregate(fact, fct, tpl.aggs, tpl.group_by, None,
+                                         build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
+                                         probe_key="fk"))
+    # A dropped join invalidates the graph.
     j.drop()
     with pytest.raises(A.TgpError) as e:
         g.run()

@@ -2288,6 +2288,7 @@ struct GraphRec {
     const JoinTable* J = nullptr;
     const unsigned long long* jtab = nullptr;
     const uint32_t* jpay = nullptr;
+    std::vector<uint64_t> jsig;            // layout of the payload array the plan reads
 };
 
 void graph_release(GraphRec* g) {
@@ -2314,7 +2315,8 @@ int graph_check(tgp_ctx* ctx, const GraphRec& g) {
     }
     if (g.join) {
         auto jt = ctx->joins.find(g.join);
-        if (jt == ctx->joins.end() || &jt->second != g.J || jt->second.tab != g.jtab || jt->second.pay != g.jpay)
+        if (jt == ctx->joins.end() || &jt->second != g.J || jt->second.tab != g.jtab ||
+            (g.jpay && (jt->second.pay != g.jpay || jt->second.pay_sig != g.jsig)))
             return fail(ctx, TGP_NOT_FOUND, "captured query: join dropped or its payload rebuilt; capture again");
     }
     return TGP_OK;
@@ -2349,7 +2351,8 @@ int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out) {
         g.join = q->join;
         g.J = qs.J;
         g.jtab = qs.J->tab;
-        g.jpay = qs.J->pay;
+        g.jpay = P.jpay;
+        if (g.jpay) g.jsig = qs.J->pay_sig;
     }
 
     g.block_words = qs.block_words();
