@@ -497,7 +497,10 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     d = ctx.register(datagen.dimension(1_500_000, seed=2 + rank), datagen.DIMENSION_COLTYPES)
     tj = workloads.join_group_agg()
     j = d.join_build("key", tj.build_where)
-    hc = ctx.register(datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank))
+    # The high-cardinality table lives on a second context (its own stream):
+    # the batched server runs its requests in a heavy lane beside the batches.
+    ctx_heavy = Context(local)
+    hc = ctx_heavy.register(datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank))
     t_scan, t_fga = workloads.selective_scan_sum(), workloads.filtered_group_agg()
     hc_aggs = [count_star(), sum_(col("value"))]
     gb = 1 << 30
@@ -507,7 +510,7 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
         "join": serving.Template("join", lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk"),
                                  1 << 16),
         "highcard": serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None),
-                                     2 * gb),
+                                     2 * gb, heavy=True),
     }
     rng = np.random.default_rng(21 + rank)
     D0, ND = datagen.DAY0, datagen.NDAYS
@@ -548,7 +551,7 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
                                f"aggregate / join+grouped aggregate over a resident {n}-row fact table (random "
                                f"literals) and GROUP BY key over a {args.highcard_rows}-row high-cardinality table "
                                f"(1 in 500); continuous batching with shared scans, admission budget "
-                               f"{args.mem_budget} B",
+                               f"{args.mem_budget} B, high-cardinality requests in a heavy lane (own stream)",
                    "offered_qps": rate, "requests": count},
         "batched": batched, "plain": plain,
         "roofline": None, "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": None,
@@ -556,6 +559,9 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     if rank == 0:
         print(json.dumps(line), flush=True)
     j.drop()
+    for tpl in templates.values():
+        tpl.pool.clear()
+    ctx_heavy.close()
     ctx.close()
 
 

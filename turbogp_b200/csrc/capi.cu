@@ -94,7 +94,10 @@ struct Carve {
 // the stream-ordered pool, which keeps freed memory for the next call.
 int dev_alloc(tgp_ctx* ctx, void** p, size_t bytes, const char* what) {
     *p = nullptr;
-    if (cudaMallocAsync(p, std::max<size_t>(bytes, 256), ctx->stream) != cudaSuccess) {
+    const size_t n = std::max<size_t>(bytes, 256);
+    const cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(p, n, ctx->pool, ctx->stream)
+                                    : cudaMallocAsync(p, n, ctx->stream);
+    if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
         return fail(ctx, TGP_OOM, what);
@@ -810,12 +813,25 @@ int tgp_init(tgp_ctx** out, int device) {
         delete ctx;
         return TGP_DEVICE_ERROR;
     }
-    // The stream-ordered pool keeps memory freed by this process for reuse
-    // (a per-process setting of the device's default pool).
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t keep = ~0ull;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // A stream-ordered pool of this context's own, which keeps freed memory
+    // for the next call. Two contexts sharing the device's default pool could
+    // each reuse memory the other freed, and the pool then makes the reusing
+    // stream wait for the other stream's work. The device's default pool
+    // (same release setting) serves if a pool cannot be created.
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    uint64_t keep = ~0ull;
+    if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        ctx->pool = nullptr;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     cudaGetLastError();
     if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
@@ -865,6 +881,7 @@ int tgp_shutdown(tgp_ctx* ctx) {
         cudaEventDestroy(p.second);
     }
     cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return TGP_OK;
 }

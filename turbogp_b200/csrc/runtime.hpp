@@ -135,6 +135,10 @@ struct tgp_ctx {
     int sms = 0;
     size_t max_dyn_smem = 0;
     cudaStream_t stream = nullptr;
+    // This context's stream-ordered pool (its memory is never handed to another
+    // context's stream, so no cross-stream reuse dependency can chain two
+    // contexts' work); null: the device's default pool.
+    cudaMemPool_t pool = nullptr;
     std::string err;
     std::unordered_map<uint64_t, tgp::Table> tables;
     std::unordered_map<uint64_t, tgp::JoinTable> joins;

@@ -6,12 +6,18 @@ literals. The batched server keeps a queue; whenever fewer than
 ``max_inflight`` batches are running it admits queued requests in arrival
 order while their estimated device memory (group hash tables, join payloads,
 result blocks) fits the budget, submits them as one ``tgp_batch_submit``, and
-completes batches with ``tgp_batch_poll``. A request's latency is its
-completion time minus its arrival time. The plain server runs each request
-alone with ``tgp_execute`` in arrival order.
+completes batches with ``tgp_batch_poll``. Requests of a heavy template (a
+high-cardinality GROUP BY, whose result is gathered, sorted and copied back
+inside the call) go to a heavy lane instead: a worker thread running them one
+by one on their own context, i.e. their own CUDA stream, so that the batching
+loop keeps admitting and completing the light requests meanwhile. A request's
+latency is its completion time minus its arrival time. The plain server runs
+each request alone with ``tgp_execute`` in arrival order.
 """
 from __future__ import annotations
 
+import queue as _queue
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -38,6 +44,7 @@ class Template:
     make: Callable[[], PreparedQuery]
     mem_bytes: int                 # device memory a running query of this shape holds
     pool: list = field(default_factory=list)
+    heavy: bool = False            # served by the heavy lane (its prepared queries live on their own context)
 
     def take(self) -> PreparedQuery:
         return self.pool.pop() if self.pool else self.make()
@@ -73,17 +80,84 @@ def summarize(reqs: list[Request], wall: float) -> dict:
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3)}
 
 
+class HeavyLane:
+    """A worker thread that runs heavy requests one at a time, in arrival
+    order, and stamps their completion times."""
+
+    def __init__(self, t0: float):
+        self.t0 = t0
+        self.jobs: _queue.Queue = _queue.Queue()
+        self.pending = 0
+        self.error: BaseException | None = None
+        self._lock = threading.Lock()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+
+    def submit(self, r: Request, tpl: Template) -> None:
+        with self._lock:
+            self.pending += 1
+        self.jobs.put((r, tpl))
+
+    def busy(self) -> bool:
+        with self._lock:
+            return self.pending > 0
+
+    def _run(self) -> None:
+        while True:
+            job = self.jobs.get()
+            if job is None:
+                return
+            r, tpl = job
+            try:
+                pq = tpl.take().rebind(r.where)
+                pq.run(decode=False)
+                r.done = time.perf_counter() - self.t0
+                tpl.give(pq)
+            except BaseException as e:  # surfaced by the serving loop
+                self.error = e
+            with self._lock:
+                self.pending -= 1
+
+    def close(self) -> None:
+        self.jobs.put(None)
+        self._thread.join()
+
+
 def serve_batched(ctx: Context, templates: dict[str, Template], reqs: list[Request], mem_budget: int,
                   max_batch: int = 256, max_inflight: int = 2) -> dict:
     queue: deque[Request] = deque()
     inflight: deque = deque()      # (handle, [(req, template, pq)])
-    nxt, t0 = 0, time.perf_counter()
-    batches = 0
-    while nxt < len(reqs) or queue or inflight:
+    t0 = time.perf_counter()
+    lane = HeavyLane(t0) if any(t.heavy for t in templates.values()) else None
+    try:
+        batches = _serve_loop(ctx, templates, reqs, mem_budget, max_batch, max_inflight, queue, inflight, lane, t0)
+    finally:
+        # On an error, batches still running are completed before returning.
+        for h, _ in inflight:
+            h.wait()
+        if lane is not None:
+            lane.close()
+    if lane is not None and lane.error is not None:
+        raise lane.error
+    out = summarize(reqs, time.perf_counter() - t0)
+    out["batches"] = batches
+    return out
+
+
+def _serve_loop(ctx, templates, reqs, mem_budget, max_batch, max_inflight, queue, inflight, lane, t0) -> int:
+    """The batching loop of serve_batched; returns the number of batches."""
+    nxt, batches = 0, 0
+    while nxt < len(reqs) or queue or inflight or (lane is not None and lane.busy()):
+        if lane is not None and lane.error is not None:
+            break
         now = time.perf_counter() - t0
         while nxt < len(reqs) and reqs[nxt].arrival <= now:
-            queue.append(reqs[nxt])
+            r = reqs[nxt]
             nxt += 1
+            if lane is not None and templates[r.template].heavy:
+                lane.submit(r, templates[r.template])
+            else:
+                queue.append(r)
         # Complete finished batches (oldest first; they finish in order).
         while inflight and inflight[0][0].poll():
             h, members = inflight.popleft()
@@ -95,8 +169,9 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs: list[Reque
             members, used = [], sum(m[1].mem_bytes for _, ms in inflight for m in ms)
             while queue and len(members) < max_batch:
                 tpl = templates[queue[0].template]
-                if members and used + tpl.mem_bytes > mem_budget:
+                if (members or inflight) and used + tpl.mem_bytes > mem_budget:
                     break                    # admission: wait for memory to be released
+                # (A request larger than the budget runs alone once nothing else does.)
                 r = queue.popleft()
                 used += tpl.mem_bytes
                 members.append((r, tpl, tpl.take().rebind(r.where)))
@@ -106,13 +181,11 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs: list[Reque
                 continue
         if not queue and inflight:
             continue                         # poll again
-        if not queue and nxt < len(reqs):
-            wait = reqs[nxt].arrival - (time.perf_counter() - t0)
+        if not queue:
+            wait = reqs[nxt].arrival - (time.perf_counter() - t0) if nxt < len(reqs) else 0.0005
             if wait > 0:
                 time.sleep(min(wait, 0.0005))
-    out = summarize(reqs, time.perf_counter() - t0)
-    out["batches"] = batches
-    return out
+    return batches
 
 
 def serve_plain(ctx: Context, templates: dict[str, Template], reqs: list[Request]) -> dict:
