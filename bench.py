@@ -221,6 +221,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         t = ctx.register(host, CT)
         q = t.prepare(tpl.aggs, tpl.group_by, tpl.where)
         step = q.run
+        n_keys, n_aggs = len(tpl.group_by), len(tpl.aggs)
         tables = [(t, host)]
         rows_step, bytes_step, kernel_bytes = n, 26 * n, 26 * n
         dominant = "scan_kernel<MODE_GROUP_PRIVATE> (6 direct groups, 4 int128 values)"
@@ -249,6 +250,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
 
         j0 = d.join_build("key", tpl.build_where)
         pq = f.prepare(tpl.aggs, tpl.group_by, tpl.where, join=j0, probe_key="fk")
+        q, n_keys, n_aggs = pq, len(tpl.group_by), len(tpl.aggs)
         probe_only = (pq.run, 16 * n)
         tables = [(d, dim), (f, fact)]
         rows_step, bytes_step, kernel_bytes = n + nb, 16 * n + 9 * nb, 16 * n
@@ -269,6 +271,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         aggs = [count_star(), sum_(col("value"))]
         q = t.prepare(aggs, ("key",), None, group_cap=10_000_000)
         step = lambda: q.run(decode=False)
+        n_keys, n_aggs = 1, len(aggs)
         variant = ("ORDER BY count(*) DESC LIMIT 10 (tgp_execute_topn)",
                    lambda: t.aggregate_topn(aggs, ("key",), None, 0, True, 10))
         tables = [(t, host)]
@@ -319,10 +322,14 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     for _ in range(e2e_steps):
         for tb, h in pinned:
             tb.reload(h)
-        step()
+        out = step()
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
+    # Bytes the step reads back: the group keys (8 B each) and one 32-byte
+    # value record per aggregate and group, plus the result block's counters.
+    ngroups = len(out.keys) if out.keys else int(q.res.ngroups)
+    d2h = ngroups * (8 * n_keys + 32 * n_aggs) + 48
 
     variant_line = None
     if variant is not None:
@@ -356,7 +363,7 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "kernel_ms": kernel_avg, "kernel": dominant},
         "e2e": {"value": rows_step * e2e_steps / (e2e_ms / 1000.0), "unit": "rows/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": None},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
     }
     if variant_line is not None:
