@@ -190,6 +190,82 @@ def run_reference(args, world: int, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_reference_workload(args, world: int, rank: int) -> None:
+    """Reference arm of the grouped / join / high-cardinality workloads: the
+    exact C++ oracle (a row-at-a-time restatement of the reference's
+    semantics) on the host cores, each step one pass over a bounded sample of
+    the workload's rows, sized so the whole run is about a minute of CPU work.
+    The batch and serving workloads have no CPU counterpart in the reference
+    (its server runs one statement at a time), so they print the unavailable
+    line. Under torchrun rank 0 alone runs."""
+    if rank != 0:
+        return
+    name = args.workload
+    if name in ("batch", "serve"):
+        print(json.dumps({"impl": "reference", "unavailable": f"{name}: the reference has no batched-submission "
+                          "or serving CPU path to time (the plain one-query-at-a-time arm is in this "
+                          "workload's own line)"}), flush=True)
+        return
+    import oracle
+    from turbogp_b200 import datagen, workloads
+    from turbogp_b200.engine import col, count_star, sum_
+    CT = datagen.LINEITEM_COLTYPES
+    cap = 2_000_000
+    if name == "filtered_group_agg":
+        n = args.rows if args.rows != ROWS else 6_000_000
+        tpl = workloads.filtered_group_agg()
+        host = datagen.lineitem(min(n, cap), seed=1)
+        run = lambda m: oracle.aggregate({k: v[:m] for k, v in host.items()}, CT, tpl.aggs, tpl.group_by, tpl.where)
+        desc = f"filtered_group_agg ({n} rows, WHERE ship_day <= max-90, GROUP BY flag_a, flag_b, 6 aggregates)"
+        what = "rows of the same lineitem distributions"
+    elif name == "join_group_agg":
+        n = args.rows if args.rows != ROWS else 60_000_000
+        nb = 1_500_000
+        tpl = workloads.join_group_agg()
+        dim = datagen.dimension(nb, seed=2)
+        fact_full = datagen.fact_fk(min(n, cap), nb, 0.8, seed=3)
+        fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
+        fct = {"fk": "int", "price_cents": "int", "discount_pct": "int"}
+        run = lambda m: oracle.aggregate({k: v[:m] for k, v in fact.items()}, fct, tpl.aggs, tpl.group_by, tpl.where,
+                                         build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
+                                         probe_key="fk")
+        desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
+                f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
+        what = "probe rows (Zipf(0.8) fk over the 1.5M-row dimension, which is joined whole)"
+    else:
+        n = args.rows if args.rows != ROWS else 100_000_000
+        host = datagen.highcard(min(n, cap), 10_000_000, 1.1, seed=4)
+        aggs = [count_star(), sum_(col("value"))]
+        run = lambda m: oracle.aggregate({k: v[:m] for k, v in host.items()}, None, aggs, ("key",))
+        desc = f"highcard_group ({n} rows, GROUP BY key Zipf(1.1) over 10M values, count + sum(value))"
+        what = "rows of the same Zipf(1.1) key distribution"
+    rows = min(n, cap)
+    t0 = time.perf_counter()
+    run(min(rows, 100_000))
+    per_row = (time.perf_counter() - t0) / min(rows, 100_000)
+    rows = int(max(100_000, min(rows, 60.0 / (args.warmup + args.steps) / max(per_row, 1e-12))))
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        run(rows)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    sec = sum(times)
+    value = rows * len(times) / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded; TPC-H shapes)",
+        "config": {"workload": desc, "rows_per_step": rows},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "port",
+                         "sample": f"{rows} {what} per step through the exact C++ oracle (row-at-a-time "
+                                   f"restatement of the reference semantics), single-threaded"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_workload(args, world: int, rank: int, local: int) -> None:
     """The other hot-path workloads, one JSON line each (same keys as the default line).
 
@@ -594,6 +670,15 @@ def main() -> None:
     args.warmup = max(3, args.warmup)
 
     world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        if args.workload == "selective_scan_sum":
+            run_reference(args, world, rank)
+        else:
+            run_reference_workload(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "batch":
         run_batch(args, world, rank, local)
         return
@@ -602,12 +687,6 @@ def main() -> None:
         return
     if args.workload != "selective_scan_sum":
         run_workload(args, world, rank, local)
-        return
-    if args.impl == "reference":
-        run_reference(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
         return
 
     import torch
