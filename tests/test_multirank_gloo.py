@@ -75,3 +75,54 @@ def test_two_gloo_ranks_merge_exactly():
     for p in procs:
         p.join(timeout=60)
     assert res == {0: "ok", 1: "ok"}, res
+
+
+def _rank_repartition(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        n = 60_000
+        rng = np.random.default_rng(5)
+        full = {"key": datagen.zipf_ranks(n, 30_000, 1.1, rng) * 1_000_003 - 2**40,   # signed, sparse
+                "g2": rng.integers(0, 4, n).astype(np.int32),
+                "v": rng.integers(-1000, 1001, n).astype(np.int32),
+                "w": rng.integers(0, 2**62, n, dtype=np.int64)}                      # int128 sums
+        lo, hi = shard.row_shard(n, rank, world)
+        mine = {k: v[lo:hi] for k, v in full.items()}
+        aggs = [count_star(), sum_(col("v")), min_(col("v")), max_(col("w")), avg(col("v")), sum_(col("w"))]
+        for gb, where in [(("key",), None), (("key", "g2"), col("v") > -500)]:
+            part = oracle.aggregate(mine, None, aggs, gb, where)
+            got = shard.repartition_partials(part, aggs, len(gb))
+            want = oracle.aggregate(full, None, aggs, gb, where)
+            owner = shard.key_owner(np.array(want.keys, dtype=np.int64).reshape(-1, len(gb)), world)
+            keep = [i for i in range(len(want.keys)) if owner[i] == rank]
+            assert got.keys == [want.keys[i] for i in keep]
+            assert got.rows_scanned == want.rows_scanned and got.rows_selected == want.rows_selected
+            for i, row in zip(keep, got.values):
+                for x, y in zip(row, want.values[i]):
+                    assert (x.value, x.count) == (y.value, y.count)
+                    assert abs(x.as_f64 - y.as_f64) <= 1e-12 * max(1.0, abs(y.as_f64))
+            # Every group lands on exactly one rank.
+            sizes = [None] * world
+            dist.all_gather_object(sizes, len(got.keys))
+            assert sum(sizes) == len(want.keys)
+        q.put((rank, "ok"))
+    except Exception as e:  # report to the parent, which fails the test
+        import traceback
+        q.put((rank, traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_repartitioned_merge_over_three_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_repartition, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=240) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert res == {0: "ok", 1: "ok", 2: "ok"}, res

@@ -235,6 +235,24 @@ class QueryOutput:
             return self._raw[2]
         return len(self.values)
 
+    def arrays(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """(keys int64 [g, k], value low limbs uint64 [g, a], value high limbs
+        int64 [g, a], counts uint64 [g, a]) without building Python lists."""
+        if self._raw is not None:
+            keys, vals, ng, nk, na = self._raw
+            k = keys[:ng * nk].view(np.int64).reshape(ng, nk)
+            v = vals[:ng * na]
+            return (k, v["lo"].reshape(ng, na).copy(), v["hi"].reshape(ng, na).copy(),
+                    v["count"].reshape(ng, na).copy())
+        ng = len(self.keys)
+        nk = len(self.keys[0]) if ng else 0
+        na = len(self.values[0]) if ng else 0
+        k = np.array(self.keys, dtype=np.int64).reshape(ng, nk)
+        lo = np.array([[x.value & 0xFFFFFFFFFFFFFFFF for x in r] for r in self.values], dtype=np.uint64).reshape(ng, na)
+        hi = np.array([[x.value >> 64 for x in r] for r in self.values], dtype=np.int64).reshape(ng, na)
+        cnt = np.array([[x.count for x in r] for r in self.values], dtype=np.uint64).reshape(ng, na)
+        return k, lo, hi, cnt
+
 
 @dataclass
 class FilterOutput:

@@ -9,7 +9,11 @@ f64 view is recomputed from the merged exact value (AVG = sum / count).
 
 ``exchange_partials`` carries the partial integers as int64 limbs through
 ``torch.distributed.all_gather`` (NCCL on GPUs, gloo on CPU); groups are
-matched by key tuple after the gather.
+matched by key tuple after the gather, and every rank ends with the whole
+result. ``repartition_partials`` is the exchange for high-cardinality
+results: each rank sends every group to the rank its key hashes to (one
+``all_to_all_single``), and each rank merges, vectorised, the groups it owns,
+so the result ends partitioned by key across the ranks.
 """
 from __future__ import annotations
 
@@ -121,3 +125,114 @@ def exchange_partials(out: QueryOutput, aggs: Sequence[Agg], device=None, group=
     dist.all_gather(parts, padded, group=group)
     outs = [_decode(p[:int(s.item())].cpu().numpy()) for p, s in zip(parts, sizes)]
     return merge_outputs(outs, aggs)
+
+
+def key_owner(keys: np.ndarray, world: int) -> np.ndarray:
+    """Rank owning each key tuple (rows of an int64 [g, k] array): splitmix64
+    of the key words, chained, modulo the world size."""
+    h = np.full(keys.shape[0], 0x9E3779B97F4A7C15, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        for j in range(keys.shape[1]):
+            z = keys[:, j].view(np.uint64) ^ h
+            z = z + np.uint64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            h = z ^ (z >> np.uint64(31))
+    return (h % np.uint64(world)).astype(np.int64)
+
+
+def _merge_rows(rows: np.ndarray, nk: int, na: int, funcs: Sequence[int]):
+    """Combines received [keys | lo | hi | count] rows with equal keys: counts
+    and sums add (int128 through 32-bit halves and a carry), MIN / MAX take the
+    extreme. Returns (keys, lo, hi, count) sorted by key."""
+    if rows.shape[0] == 0:
+        z = np.zeros((0, na))
+        return (np.zeros((0, nk), np.int64), z.astype(np.uint64), z.astype(np.int64), z.astype(np.uint64))
+    keys = rows[:, :nk]
+    order = np.lexsort(keys.T[::-1])
+    rows = rows[order]
+    keys = rows[:, :nk]
+    lo = rows[:, nk:nk + na].view(np.uint64)
+    hi = rows[:, nk + na:nk + 2 * na]
+    cnt = rows[:, nk + 2 * na:nk + 3 * na].view(np.uint64)
+    new = np.ones(rows.shape[0], dtype=bool)
+    new[1:] = np.any(keys[1:] != keys[:-1], axis=1)
+    starts = np.flatnonzero(new)
+    out_lo = np.empty((starts.size, na), np.uint64)
+    out_hi = np.empty((starts.size, na), np.int64)
+    mask32 = np.uint64(0xFFFFFFFF)
+    for a, f in enumerate(funcs):
+        if f in (A.AGG_MIN, A.AGG_MAX):
+            v = lo[:, a].view(np.int64)
+            r = (np.minimum if f == A.AGG_MIN else np.maximum).reduceat(v, starts)
+            out_lo[:, a] = r.view(np.uint64)
+            out_hi[:, a] = r >> 63
+        else:
+            s_ll = np.add.reduceat(lo[:, a] & mask32, starts)
+            s_lh = np.add.reduceat(lo[:, a] >> np.uint64(32), starts)
+            s_hi = np.add.reduceat(hi[:, a], starts)
+            s_lh = s_lh + (s_ll >> np.uint64(32))
+            out_lo[:, a] = ((s_lh & mask32) << np.uint64(32)) | (s_ll & mask32)
+            out_hi[:, a] = s_hi + (s_lh >> np.uint64(32)).astype(np.int64)
+    out_cnt = np.add.reduceat(cnt, starts, axis=0)
+    return keys[starts], out_lo, out_hi, out_cnt
+
+
+def repartition_partials(out: QueryOutput, aggs: Sequence[Agg], nkeys: int, device=None,
+                         group=None) -> QueryOutput:
+    """Hash-partitioned exact merge of a grouped partial result: every rank
+    passes its partial (any number of groups, ``nkeys`` >= 1 key columns) and
+    returns the merged groups whose key it owns (``key_owner``), sorted by key.
+    The union over the ranks is the merged result of all partials; rows
+    scanned / selected are the totals and flags the OR over the ranks."""
+    import torch
+    import torch.distributed as dist
+    if nkeys < 1:
+        raise ValueError("repartition needs a key; scalar results merge with exchange_partials")
+    world = dist.get_world_size(group)
+    na = len(aggs)
+    keys, lo, hi, cnt = out.arrays()
+    keys = keys.reshape(-1, nkeys)
+    dest = key_owner(keys, world)
+    rows = np.concatenate([keys, lo.view(np.int64), hi, cnt.view(np.int64)], axis=1) if keys.shape[0] else \
+        np.zeros((0, nkeys + 3 * na), np.int64)
+    order = np.argsort(dest, kind="stable")
+    rows = np.ascontiguousarray(rows[order])
+    width = nkeys + 3 * na
+    send_counts = np.bincount(dest, minlength=world).astype(np.int64) * width
+    dev = device if device is not None else torch.device("cpu")
+    sc = torch.from_numpy(send_counts).to(dev)
+    rc = torch.empty_like(sc)
+    dist.all_to_all_single(rc, sc, group=group)
+    recv_counts = rc.cpu().numpy()
+    send = torch.from_numpy(rows.reshape(-1)).to(dev)
+    recv = torch.empty(int(recv_counts.sum()), dtype=torch.int64, device=dev)
+    dist.all_to_all_single(recv, send, output_split_sizes=[int(x) for x in recv_counts],
+                           input_split_sizes=[int(x) for x in send_counts], group=group)
+    meta = torch.tensor([out.rows_scanned, out.rows_selected, out.flags], dtype=torch.int64, device=dev)
+    metas = [torch.empty_like(meta) for _ in range(world)]
+    dist.all_gather(metas, meta, group=group)
+    metas = [m.cpu().numpy() for m in metas]
+    k, mlo, mhi, mcnt = _merge_rows(recv.cpu().numpy().reshape(-1, width), nkeys, na, [a.func for a in aggs])
+    ng = k.shape[0]
+    vals = np.zeros(ng * na, dtype=[("lo", "<u8"), ("hi", "<i8"), ("count", "<u8"), ("as_f64", "<f8")])
+    vals["lo"], vals["hi"], vals["count"] = mlo.reshape(-1), mhi.reshape(-1), mcnt.reshape(-1)
+    # f64 views: the correctly rounded value (int64-representable values
+    # convert exactly-rounded in numpy; wider ones through Python ints); AVG
+    # divides by the merged count.
+    small = (mhi.reshape(-1) == (mlo.reshape(-1).view(np.int64) >> 63))
+    f = mlo.reshape(-1).view(np.int64).astype(np.float64)
+    for i in np.flatnonzero(~small):
+        f[i] = float((int(mhi.reshape(-1)[i]) << 64) | int(mlo.reshape(-1)[i]))
+    funcs = np.tile(np.array([a.func for a in aggs]), ng)
+    c = mcnt.reshape(-1).astype(np.float64)
+    avg = funcs == A.AGG_AVG
+    f[avg] = np.where(c[avg] > 0, f[avg] / np.where(c[avg] > 0, c[avg], 1.0), 0.0)
+    vals["as_f64"] = f
+    scanned = int(sum(int(m[0]) for m in metas))
+    selected = int(sum(int(m[1]) for m in metas))
+    flags = 0
+    for m in metas:
+        flags |= int(m[2])
+    return QueryOutput(None, None, scanned, selected, flags,
+                       raw=(np.ascontiguousarray(k).reshape(-1).view(np.uint64), vals, ng, nkeys, na))
