@@ -340,39 +340,78 @@ cudaError_t launch_distinct_cells(const uint8_t* col, uint32_t dtype, uint64_t n
 // h = xxh3(cell), register h >> 50 takes the max of
 // leading_zeros(h << 14) + 1. Each CTA keeps its registers in shared memory
 // (a shared atomic max only when the value could raise the register) and
-// merges them into the global ones at the end.
+// writes them, one byte each, to its row of `partial`; a second kernel takes
+// the max over the CTAs' rows (no global atomics on 16K hot addresses).
 constexpr int kHllRegs = 1 << 14;
 constexpr int kHllThreads = 512;
 
 __global__ void __launch_bounds__(kHllThreads) hll_kernel(const uint8_t* col, uint32_t dtype, uint64_t n,
-                                                         const uint32_t* bitmap, uint32_t* regs) {
+                                                         const uint32_t* bitmap, uint8_t* partial) {
     extern __shared__ uint32_t sreg[];
     for (int r = threadIdx.x; r < kHllRegs; r += blockDim.x) sreg[r] = 0;
     __syncthreads();
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        if (!row_selected(bitmap, i)) continue;
-        const unsigned long long h = xxh3_u64(cell_at(col, dtype, i));
-        const uint32_t idx = static_cast<uint32_t>(h >> 50);
-        const unsigned long long w = h << 14;
-        const uint32_t lz = (w ? static_cast<uint32_t>(__clzll(static_cast<long long>(w))) : 64u) + 1u;
-        if (lz > *reinterpret_cast<volatile uint32_t*>(sreg + idx)) atomicMax(sreg + idx, lz);
+    // Four rows per thread and pass, their loads issued before any hashing
+    // (rows i, i + T, i + 2T, i + 3T for T threads: coalesced per row).
+    const uint64_t T = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += 4 * T) {
+        unsigned long long c[4];
+        bool on[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t j = i + u * T;
+            on[u] = j < n && row_selected(bitmap, j);
+            c[u] = on[u] ? cell_at(col, dtype, j) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!on[u]) continue;
+            const unsigned long long h = xxh3_u64(c[u]);
+            const uint32_t idx = static_cast<uint32_t>(h >> 50);
+            const unsigned long long w = h << 14;
+            const uint32_t lz = (w ? static_cast<uint32_t>(__clzll(static_cast<long long>(w))) : 64u) + 1u;
+            if (lz > *reinterpret_cast<volatile uint32_t*>(sreg + idx)) atomicMax(sreg + idx, lz);
+        }
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < kHllRegs; r += blockDim.x)
-        if (sreg[r] && sreg[r] > *reinterpret_cast<volatile uint32_t*>(regs + r)) atomicMax(regs + r, sreg[r]);
+    uint8_t* row = partial + static_cast<uint64_t>(blockIdx.x) * kHllRegs;
+    for (int r = 4 * threadIdx.x; r < kHllRegs; r += 4 * blockDim.x)
+        reinterpret_cast<uint32_t*>(row)[r / 4] = sreg[r] | (sreg[r + 1] << 8) | (sreg[r + 2] << 16) | (sreg[r + 3] << 24);
 }
 
-cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint32_t* regs,
-                       int sms, cudaStream_t st) {
+// regs[r] = max over the CTAs' rows of partial[b][r] (four registers a thread).
+__global__ void __launch_bounds__(256) hll_merge_kernel(const uint8_t* partial, uint32_t rows, uint32_t* regs) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= kHllRegs / 4) return;
+    uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    for (uint32_t b = 0; b < rows; ++b) {
+        const uint32_t w = reinterpret_cast<const uint32_t*>(partial + static_cast<uint64_t>(b) * kHllRegs)[q];
+        m0 = max(m0, w & 0xffu);
+        m1 = max(m1, (w >> 8) & 0xffu);
+        m2 = max(m2, (w >> 16) & 0xffu);
+        m3 = max(m3, w >> 24);
+    }
+    regs[4 * q] = m0;
+    regs[4 * q + 1] = m1;
+    regs[4 * q + 2] = m2;
+    regs[4 * q + 3] = m3;
+}
+
+int hll_blocks(uint64_t n, int sms) {
+    uint64_t blocks = (n + kHllThreads - 1) / kHllThreads;
+    if (blocks > static_cast<uint64_t>(sms) * 2) blocks = static_cast<uint64_t>(sms) * 2;
+    return static_cast<int>(blocks);
+}
+
+cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint8_t* partial,
+                       uint32_t* regs, int sms, cudaStream_t st) {
     const size_t smem = kHllRegs * sizeof(uint32_t);
     const cudaError_t e = cudaFuncSetAttribute(hll_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    uint64_t blocks = (n + kHllThreads - 1) / kHllThreads;
-    if (blocks > static_cast<uint64_t>(sms) * 2) blocks = static_cast<uint64_t>(sms) * 2;
-    if (blocks == 0) return cudaSuccess;
-    hll_kernel<<<static_cast<unsigned>(blocks), kHllThreads, smem, st>>>(col, dtype, n, bitmap, regs);
+    const int blocks = hll_blocks(n, sms);
+    if (blocks == 0) return cudaMemsetAsync(regs, 0, kHllRegs * sizeof(uint32_t), st);
+    hll_kernel<<<static_cast<unsigned>(blocks), kHllThreads, smem, st>>>(col, dtype, n, bitmap, partial);
+    hll_merge_kernel<<<(kHllRegs / 4 + 255) / 256, 256, 0, st>>>(partial, static_cast<uint32_t>(blocks), regs);
     return cudaGetLastError();
 }
 

@@ -1308,12 +1308,13 @@ int tgp_count_distinct(tgp_ctx* ctx, tgp_table_id table, uint32_t column, const 
         }
     } else {
         Carve cv;
-        st = arena_reserve(ctx, 16384 * 4 + 256, &cv);
+        const uint64_t prow = static_cast<uint64_t>(hll_blocks(n, ctx->sms));
+        st = arena_reserve(ctx, 16384 * 4 + prow * 16384 + 512, &cv);
         if (st == TGP_OK) {
             uint32_t* regs = cv.take<uint32_t>(16384);
+            uint8_t* partial = cv.take<uint8_t>(std::max<uint64_t>(prow, 1) * 16384);
             std::vector<uint32_t> h(16384);
-            cudaError_t e = cudaMemsetAsync(regs, 0, 16384 * 4, ctx->stream);
-            if (e == cudaSuccess) e = launch_hll(c.dptr, c.dtype, n, bm, regs, ctx->sms, ctx->stream);
+            cudaError_t e = launch_hll(c.dptr, c.dtype, n, bm, partial, regs, ctx->sms, ctx->stream);
             if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), regs, 16384 * 4, cudaMemcpyDeviceToHost, ctx->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
             if (e != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, std::string("hyperloglog: ") + cudaGetErrorString(e));

@@ -52,8 +52,11 @@ cudaError_t launch_sum_f64(const double* x, uint64_t n, double* out, int blocks,
 cudaError_t launch_distinct_cells(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap,
                                   unsigned long long* set, uint64_t mask, uint32_t log2cap,
                                   unsigned long long* counters, uint32_t* err, int sms, cudaStream_t st);
-cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint32_t* regs,
-                       int sms, cudaStream_t st);
+// HyperLogLog: `partial` holds hll_blocks(n, sms) rows of 2^14 bytes (one per
+// CTA, 16-byte aligned); regs gets their max (every register written).
+int hll_blocks(uint64_t n, int sms);
+cudaError_t launch_hll(const uint8_t* col, uint32_t dtype, uint64_t n, const uint32_t* bitmap, uint8_t* partial,
+                       uint32_t* regs, int sms, cudaStream_t st);
 cudaError_t launch_count_distinct(const unsigned long long* x, uint64_t n, unsigned long long* set,
                                   uint64_t mask, uint32_t log2cap, unsigned long long* counters,
                                   uint32_t* err, int blocks, cudaStream_t st);
