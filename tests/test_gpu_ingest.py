@@ -87,3 +87,29 @@ def test_parquet_to_hbm(ctx, tmp_path):
     t = ingest.register_parquet(ctx, p, coltypes={"ship_day": "date"})
     check_lineitem(t, host, 80_000)
     t.drop()
+
+
+def test_string_columns_compare_by_hash(ctx, tmp_path):
+    rng = np.random.default_rng(17)
+    words = np.array(["apple", "banana", "cherry", "", "ünïcødé", "x" * 40])
+    n = 120_000
+    pick = rng.integers(0, len(words), n)
+    s = [None if i % 97 == 0 else str(words[k]) for i, k in enumerate(pick)]
+    qty = rng.integers(1, 51, n).astype(np.int32)
+    p = tmp_path / "strings.parquet"
+    pq.write_table(pa.table({"name": pa.array(s, pa.string()), "quantity": pa.array(qty)}), p)
+    t = ingest.register_parquet(ctx, p)
+    cells, _, cts = ingest.read_parquet(p)
+    host = {"name": cells["name"], "quantity": qty}
+    c = col
+    for where in [c("name") == "banana", c("name") != "cherry", (c("name") == "") & (c("quantity") < 10),
+                  c("name") == "not there", c("name") == "x" * 40]:
+        g, o = t.filter(where), oracle.filter(host, {"name": "int", "quantity": "int"}, where)
+        assert g.count == o.count and np.array_equal(bits(g.bitmap, n), bits(o.bitmap, n))
+    assert t.filter(c("name") == "banana").count == sum(1 for x in s if x == "banana")
+    with pytest.raises(ValueError):
+        t.filter(c("name") < "m")
+    aggs = [count_star(), sum_(c("quantity"))]
+    same_query(t.aggregate(aggs, ("name",), None, group_cap=64),
+               oracle.aggregate(host, {"name": "int", "quantity": "int"}, aggs, ("name",), None))
+    t.drop()

@@ -66,8 +66,22 @@ def test_csv_and_column_selection(tmp_path):
     assert list(cells) == ["c"]
 
 
+def test_strings_and_booleans():
+    import xxhash
+    words = ["", "a", "hello", "ünïcødé", "x" * 300, None]
+    cells, side, ct = ingest.arrow_cells(pa.table({
+        "s": pa.array(words, pa.string()),
+        "ls": pa.array(words, pa.large_string()),
+        "b": pa.array([True, False, None, True, False, True]),
+    }))
+    want = [0 if w is None else xxhash.xxh3_64_intdigest(w.encode("utf-8")) for w in words]
+    assert [int(x) for x in cells["s"]] == want and [int(x) for x in cells["ls"]] == want
+    assert [int(x) for x in cells["b"]] == [1, 0, 0, 1, 0, 1]
+    assert ct["s"] == "int" and ct["b"] == "int" and "s" not in side and side["b"].dtype == np.int32
+
+
 def test_unsupported_types_raise():
     with pytest.raises(TypeError):
-        ingest.arrow_cells(pa.table({"s": pa.array(["x", "y"])}))
+        ingest.arrow_cells(pa.table({"t": pa.array([1, 2], pa.timestamp("s"))}))
     with pytest.raises(TypeError):
-        ingest.arrow_cells(pa.table({"b": pa.array([True, False])}))
+        ingest.arrow_cells(pa.table({"d": pa.array([1.5], pa.float32())}))

@@ -418,7 +418,20 @@ class Context:
         self._check(self.lib.tgp_hash_table_free(self.h, C.c_void_p(handle)), "tgp_hash_table_free")
 
 
+def string_cell(v: str | bytes) -> int:
+    """The cell of a string value as the reference stores it: xxh3_64 of its
+    UTF-8 bytes (src/datasource/parquet.rs:389-406; equality predicates hash
+    their literal the same way, expr.rs:1534-1547)."""
+    try:
+        import xxhash
+    except ImportError as e:  # pragma: no cover - the package ships with the image
+        raise ImportError("string values need the xxhash package (xxh3_64)") from e
+    return int(xxhash.xxh3_64_intdigest(v.encode("utf-8") if isinstance(v, str) else bytes(v)))
+
+
 def _lit_bits(ct: int, v) -> int:
+    if isinstance(v, (str, bytes)):
+        return string_cell(v)
     if ct == A.CT_FLOAT:
         return int(np.array([float(v)], dtype=np.float64).view(np.uint64)[0])
     return _u64(int(v))
@@ -454,6 +467,8 @@ class Schema:
         for i, op in enumerate(pred.ops):
             if op[0] == "leaf":
                 _, name, cmp, v, v2 = op
+                if isinstance(v, (str, bytes)) and cmp not in (A.CMP_EQ, A.CMP_NE):
+                    raise ValueError("string values compare by equality only (their cells are xxh3_64 hashes)")
                 ci = self.index(name)
                 ct = self.dtypes[ci][1]
                 nodes[i].kind, nodes[i].column, nodes[i].cmp = A.PN_LEAF, ci, cmp

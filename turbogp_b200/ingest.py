@@ -8,11 +8,13 @@ exactly those cells, plus an i32 sidecar for columns whose Arrow type is at
 most 32 bits wide (the narrow copy the reference's CSV loader keeps,
 src/datasource/table.rs:52-61); ``register_parquet`` / ``register_csv`` hand
 both to ``tgp_table_register_cells``, which stores each column at the narrowest
-exact width on the device.
+exact width on the device. Booleans become the cells 0 / 1, and Utf8 /
+LargeUtf8 strings the xxh3_64 hash of their bytes (parquet.rs:389-436), which
+equality predicates on string literals compare against (the reference's
+string search index for LIKE is not built).
 
-Differences from the reference, on purpose: a column type the reference fills
-with zeros (Boolean, timestamps, decimals, ...) raises here instead, and Utf8
-columns (hashed with xxh3 by the reference) are not loaded.
+Difference from the reference, on purpose: a column type the reference fills
+with zeros (timestamps, decimals, ...) raises here instead.
 """
 from __future__ import annotations
 
@@ -50,6 +52,15 @@ def arrow_cells(table) -> tuple[dict, dict, dict]:
             cells[name] = vals.astype(np.uint64)
             if vals.dtype.itemsize < 4 or (vals.dtype.itemsize == 4 and (vals.size == 0 or vals.max() <= 2**31 - 1)):
                 sidecars[name] = vals.astype(np.int32)
+            coltypes[name] = "int"
+        elif pa.types.is_boolean(t):
+            vals = arr.fill_null(False).to_numpy(zero_copy_only=False).astype(np.int32)
+            cells[name] = vals.astype(np.uint64)
+            sidecars[name] = vals
+            coltypes[name] = "int"
+        elif pa.types.is_string(t) or pa.types.is_large_string(t):
+            from .engine import string_cell
+            cells[name] = np.array([0 if x is None else string_cell(x) for x in arr.to_pylist()], dtype=np.uint64)
             coltypes[name] = "int"
         elif pa.types.is_float64(t):
             vals = arr.fill_null(0.0).to_numpy(zero_copy_only=False).astype(np.float64)
