@@ -686,6 +686,26 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = sc
     return TGP_OK;
 }
 
+// With profiling on, takes the next pair of timing events and records the
+// first on the context's stream (after a bounded device delay when gated);
+// *ev stays null otherwise.
+int profile_begin(tgp_ctx* ctx, std::pair<cudaEvent_t, cudaEvent_t>** ev) {
+    *ev = nullptr;
+    if (!ctx->profile) return TGP_OK;
+    if (ctx->prof_used == ctx->prof_events.size()) {
+        std::pair<cudaEvent_t, cudaEvent_t> p;
+        TGP_CUDA(cudaEventCreate(&p.first));
+        TGP_CUDA(cudaEventCreate(&p.second));
+        ctx->prof_events.push_back(p);
+    }
+    *ev = &ctx->prof_events[ctx->prof_used++];
+    // Gated timing: the GPU is busy with the delay while the host submits
+    // the launch, so the start event is stamped right before the kernel.
+    if (ctx->profile_gate) TGP_CUDA(launch_delay(50000, ctx->stream));
+    TGP_CUDA(cudaEventRecord((*ev)->first, ctx->stream));
+    return TGP_OK;
+}
+
 int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     if (ntiles == 0) return TGP_OK;
@@ -693,19 +713,7 @@ int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
     if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
     const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * occ);
     std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
-    if (ctx->profile) {
-        if (ctx->prof_used == ctx->prof_events.size()) {
-            std::pair<cudaEvent_t, cudaEvent_t> p;
-            TGP_CUDA(cudaEventCreate(&p.first));
-            TGP_CUDA(cudaEventCreate(&p.second));
-            ctx->prof_events.push_back(p);
-        }
-        ev = &ctx->prof_events[ctx->prof_used++];
-        // Gated timing: the GPU is busy with the delay while the host submits
-        // the launch, so the start event is stamped right before the kernel.
-        if (ctx->profile_gate) TGP_CUDA(launch_delay(50000, ctx->stream));
-        TGP_CUDA(cudaEventRecord(ev->first, ctx->stream));
-    }
+    TGP_TRY(profile_begin(ctx, &ev));
     cudaError_t e = launch_scan(P, mode, acc128, static_cast<int>(grid), ctx->stream);
     if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("scan launch: ") + cudaGetErrorString(e));
     if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
@@ -2426,7 +2434,12 @@ int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id id, uint64_t* keys_out, tgp_agg_
     if (it == ctx->graphs.end()) return fail(ctx, TGP_NOT_FOUND, "unknown graph id");
     GraphRec& g = *static_cast<GraphRec*>(it->second);
     TGP_TRY(graph_check(ctx, g));
+    // Profiling counts the graph (one scan kernel between its clear and its
+    // readback) as one timed launch.
+    std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+    TGP_TRY(profile_begin(ctx, &ev));
     TGP_CUDA(cudaGraphLaunch(g.exec, ctx->stream));
+    if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));
     return decode_direct(ctx, g.qs, g.host, keys_out, vals_out, group_cap, result);
 }
