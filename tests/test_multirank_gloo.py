@@ -107,6 +107,14 @@ def _rank_repartition(rank, world, port, q):
             sizes = [None] * world
             dist.all_gather_object(sizes, len(got.keys))
             assert sum(sizes) == len(want.keys)
+        # Two rows over three ranks: one rank contributes no group at all.
+        tiny = {k: v[:2] for k, v in full.items()}
+        lo, hi = shard.row_shard(2, rank, world)
+        part = oracle.aggregate({k: v[lo:hi] for k, v in tiny.items()}, None, aggs, ("key",), None)
+        got = shard.repartition_partials(part, aggs, 1)
+        want = oracle.aggregate(tiny, None, aggs, ("key",), None)
+        owner = shard.key_owner(np.array(want.keys, dtype=np.int64).reshape(-1, 1), world)
+        assert got.keys == [k for k, o in zip(want.keys, owner) if o == rank]
         q.put((rank, "ok"))
     except Exception as e:  # report to the parent, which fails the test
         import traceback
