@@ -16,11 +16,18 @@
 //      SUM(Col * Col) for Int columns: sum += ca[i] as f64 * cb[i] as f64
 //      (aggregate.rs:1589-1601), COUNT(*) = indices.len() (aggregate.rs:1298).
 // Both steps run on one thread, as in the reference (no rayon on this path).
+// ref_grouped_q1 and ref_highcard restate the grouped paths (execute_grouped
+// and try_accumulator_grouped), whose chunked grouping the reference runs on
+// rayon's thread pool and this file on OpenMP threads.
 #include <immintrin.h>
 
+#include <omp.h>
+
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -162,6 +169,13 @@ std::vector<size_t> iter_set_bits(const Bitmap& bm) {
     return out;
 }
 
+// FxHasher::write_u64 from a fresh hasher: the word times the Fx constant.
+struct FxHash {
+    size_t operator()(uint64_t x) const { return static_cast<size_t>(x * 0x517cc1b727220a95ull); }
+};
+
+constexpr size_t kGroupChunk = 65536;  // GROUP_CHUNK_SIZE (aggregate.rs:582, accum_grouped.rs:197)
+
 }  // namespace
 
 extern "C" {
@@ -177,11 +191,12 @@ struct ref_leaf {
     uint64_t lit2;
 };
 
-// WHERE <conjunction of leaves> → SUM(cells[a] * cells[b]) (f64), COUNT(*).
-// cols: ncols pointers to n u64 cells. Returns wall seconds of the query.
-double ref_scan_sum_mul(const uint64_t* const* cols, uint64_t n, const ref_leaf* leaves, uint32_t nleaves,
-                        uint32_t a, uint32_t b, double* sum_out, uint64_t* count_out) {
-    const auto t0 = std::chrono::steady_clock::now();
+}  // extern "C"
+
+namespace {
+
+// build_mask over a conjunction of leaves (every leaf a fresh bitmap ANDed in).
+Bitmap mask_of(const uint64_t* const* cols, uint64_t n, const ref_leaf* leaves, uint32_t nleaves) {
     Bitmap mask = Bitmap::all_ones(n);
     for (uint32_t i = 0; i < nleaves; ++i) {
         const ref_leaf& L = leaves[i];
@@ -195,6 +210,19 @@ double ref_scan_sum_mul(const uint64_t* const* cols, uint64_t n, const ref_leaf*
             and_inplace(mask, bm);
         }
     }
+    return mask;
+}
+
+}  // namespace
+
+extern "C" {
+
+// WHERE <conjunction of leaves> → SUM(cells[a] * cells[b]) (f64), COUNT(*).
+// cols: ncols pointers to n u64 cells. Returns wall seconds of the query.
+double ref_scan_sum_mul(const uint64_t* const* cols, uint64_t n, const ref_leaf* leaves, uint32_t nleaves,
+                        uint32_t a, uint32_t b, double* sum_out, uint64_t* count_out) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Bitmap mask = mask_of(cols, n, leaves, nleaves);
     const std::vector<size_t> idx = iter_set_bits(mask);
     const uint64_t* ca = cols[a];
     const uint64_t* cb = cols[b];
@@ -203,6 +231,138 @@ double ref_scan_sum_mul(const uint64_t* const* cols, uint64_t n, const ref_leaf*
     const auto t1 = std::chrono::steady_clock::now();
     *sum_out = sum;
     *count_out = idx.size();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The grouped aggregate of the TPC-H Q1 shape the reference's way
+// (execute_grouped, aggregate.rs:507-697): WHERE mask → indices; chunks of
+// 65,536 indices grouped in parallel (rayon there, OpenMP here) into
+// hash → row-list maps, the group key hash h = h * 0x517cc1b727220a95 + cell
+// over the GROUP BY cells (aggregate.rs:594-603); the chunk maps merged in
+// chunk order; then, group by group, each aggregate over the group's rows
+// (eval_agg_expr / sum_vec, aggregate.rs:1291-1792):
+//   COUNT(*) = rows; SUM(q), SUM(p) = wrapping i64 sums of the cells;
+//   SUM(p * (100 - d)) = f64 sum of p as f64 * (100 - d) as f64;
+//   SUM(p * (100 - d) * (100 + t)) = f64 sum of the exact i64 product;
+//   AVG(q) = f64(SUM(q)) / rows.
+// Per group out: keys[2], count, sum_q, sum_p (i64), disc_price, charge,
+// avg_q (f64). Returns wall seconds; *ngroups = groups (at most cap written).
+double ref_grouped_q1(const uint64_t* const* cols, uint64_t n, const ref_leaf* leaves, uint32_t nleaves,
+                      uint32_t ka, uint32_t kb, uint32_t cq, uint32_t cp, uint32_t cd, uint32_t ct, int threads,
+                      uint64_t cap, int64_t* keys, int64_t* ints, double* flts, uint64_t* ngroups) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Bitmap mask = mask_of(cols, n, leaves, nleaves);
+    const std::vector<size_t> idx = iter_set_bits(mask);
+    const size_t nchunks = (idx.size() + kGroupChunk - 1) / kGroupChunk;
+    std::vector<std::unordered_map<uint64_t, std::vector<size_t>, FxHash>> local(nchunks);
+    const uint64_t* gk[2] = {cols[ka], cols[kb]};
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (size_t c = 0; c < nchunks; ++c) {
+        const size_t lo = c * kGroupChunk, hi = std::min(idx.size(), lo + kGroupChunk);
+        auto& m = local[c];
+        for (size_t i = lo; i < hi; ++i) {
+            const size_t r = idx[i];
+            uint64_t h = 0;
+            for (int k = 0; k < 2; ++k) h = h * 0x517cc1b727220a95ull + gk[k][r];
+            m[h].push_back(r);
+        }
+    }
+    std::unordered_map<uint64_t, size_t, FxHash> gid;
+    std::vector<std::vector<size_t>> groups;
+    groups.reserve(1024);
+    for (auto& m : local)
+        for (auto& kv : m) {
+            auto it = gid.find(kv.first);
+            size_t g;
+            if (it == gid.end()) {
+                g = groups.size();
+                gid.emplace(kv.first, g);
+                groups.emplace_back();
+            } else {
+                g = it->second;
+            }
+            groups[g].insert(groups[g].end(), kv.second.begin(), kv.second.end());
+        }
+    const uint64_t *q = cols[cq], *p = cols[cp], *d = cols[cd], *t = cols[ct];
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const std::vector<size_t>& rows = groups[g];
+        uint64_t sq = 0, sp = 0;
+        double dp = 0.0, ch = 0.0;
+        for (size_t r : rows) sq += q[r];
+        for (size_t r : rows) sp += p[r];
+        for (size_t r : rows)
+            dp += static_cast<double>(p[r]) * static_cast<double>(100 - static_cast<int64_t>(d[r]));
+        for (size_t r : rows) {
+            const int64_t v = static_cast<int64_t>(static_cast<uint64_t>(static_cast<int64_t>(p[r])) *
+                                                   static_cast<uint64_t>(100 - static_cast<int64_t>(d[r])) *
+                                                   static_cast<uint64_t>(100 + static_cast<int64_t>(t[r])));
+            ch += static_cast<double>(v);
+        }
+        if (g < cap) {
+            keys[2 * g] = static_cast<int64_t>(gk[0][rows[0]]);
+            keys[2 * g + 1] = static_cast<int64_t>(gk[1][rows[0]]);
+            ints[3 * g] = static_cast<int64_t>(rows.size());
+            ints[3 * g + 1] = static_cast<int64_t>(sq);
+            ints[3 * g + 2] = static_cast<int64_t>(sp);
+            flts[3 * g] = dp;
+            flts[3 * g + 1] = ch;
+            flts[3 * g + 2] = static_cast<double>(static_cast<int64_t>(sq)) / static_cast<double>(rows.size());
+        }
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    *ngroups = groups.size();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// GROUP BY key, COUNT(*), SUM(value) the reference's way
+// (try_accumulator_grouped, accum_grouped.rs:55-300): all rows selected (no
+// WHERE: an all-ones mask → indices); chunks of 65,536 indices accumulated in
+// parallel into hash → slot-vector maps ([key cell, count, wrapping sum], a
+// vector allocated per new group), the key hash being the key cell itself
+// (h = 0 * K + cell); the chunk maps merged one by one into a global map.
+// Per group out: key, count, sum (wrapping i64). Returns wall seconds.
+double ref_highcard(const uint64_t* key, const uint64_t* val, uint64_t n, int threads, uint64_t cap,
+                    int64_t* keys, int64_t* counts, int64_t* sums, uint64_t* ngroups) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Bitmap mask = Bitmap::all_ones(n);
+    const std::vector<size_t> idx = iter_set_bits(mask);
+    const size_t nchunks = (idx.size() + kGroupChunk - 1) / kGroupChunk;
+    std::vector<std::unordered_map<uint64_t, std::vector<uint64_t>, FxHash>> local(nchunks);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (size_t c = 0; c < nchunks; ++c) {
+        const size_t lo = c * kGroupChunk, hi = std::min(idx.size(), lo + kGroupChunk);
+        auto& m = local[c];
+        for (size_t i = lo; i < hi; ++i) {
+            const size_t r = idx[i];
+            auto it = m.find(key[r]);
+            if (it == m.end()) it = m.emplace(key[r], std::vector<uint64_t>{key[r], 0, 0}).first;
+            std::vector<uint64_t>& acc = it->second;
+            acc[1] += 1;
+            acc[2] += val[r];
+        }
+    }
+    std::unordered_map<uint64_t, std::vector<uint64_t>, FxHash> global;
+    for (auto& m : local)
+        for (auto& kv : m) {
+            auto it = global.find(kv.first);
+            if (it == global.end()) {
+                global.emplace(kv.first, std::move(kv.second));
+            } else {
+                it->second[1] += kv.second[1];
+                it->second[2] += kv.second[2];
+            }
+        }
+    const auto t1 = std::chrono::steady_clock::now();
+    uint64_t g = 0;
+    for (auto& kv : global) {
+        if (g < cap) {
+            keys[g] = static_cast<int64_t>(kv.second[0]);
+            counts[g] = static_cast<int64_t>(kv.second[1]);
+            sums[g] = static_cast<int64_t>(kv.second[2]);
+        }
+        ++g;
+    }
+    *ngroups = g;
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
