@@ -192,9 +192,10 @@ def run_reference(args, world: int, rank: int) -> None:
 
 def run_reference_workload(args, world: int, rank: int) -> None:
     """Reference arm of the grouped / join / high-cardinality workloads: the
-    exact C++ oracle (a row-at-a-time restatement of the reference's
-    semantics) on the host cores, each step one pass over a bounded sample of
-    the workload's rows, sized so the whole run is about a minute of CPU work.
+    C++ restatements of the reference's own CPU paths for them
+    (oracle/ref_path.cpp) on all host threads, each step one pass over a
+    bounded sample of the workload's rows, sized so the whole run is about a
+    minute of CPU work.
     The batch and serving workloads have no CPU counterpart in the reference
     (its server runs one statement at a time), so they print the unavailable
     line. Under torchrun rank 0 alone runs."""
@@ -206,14 +207,11 @@ def run_reference_workload(args, world: int, rank: int) -> None:
                           "or serving CPU path to time (the plain one-query-at-a-time arm is in this "
                           "workload's own line)"}), flush=True)
         return
-    import oracle
     from oracle import refpath
     from turbogp_b200 import datagen, workloads
     CT = datagen.LINEITEM_COLTYPES
     cap = 2_000_000
     threads = os.cpu_count() or 1
-    how = "the exact C++ oracle (row-at-a-time restatement of the reference semantics), single-threaded"
-    cores = 1
     if name == "filtered_group_agg":
         n = args.rows if args.rows != ROWS else 6_000_000
         tpl = workloads.filtered_group_agg()
@@ -230,12 +228,15 @@ def run_reference_workload(args, world: int, rank: int) -> None:
         nb = 1_500_000
         tpl = workloads.join_group_agg()
         dim = datagen.dimension(nb, seed=2)
-        fact_full = datagen.fact_fk(min(n, cap), nb, 0.8, seed=3)
+        cap = min(n, 20_000_000)
+        fact_full = datagen.fact_fk(cap, nb, 0.8, seed=3)
         fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
-        fct = {"fk": "int", "price_cents": "int", "discount_pct": "int"}
-        run = lambda m: oracle.aggregate({k: v[:m] for k, v in fact.items()}, fct, tpl.aggs, tpl.group_by, tpl.where,
-                                         build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
-                                         probe_key="fk")
+        day_lt = tpl.build_where.ops[0][3]
+        run = lambda m: refpath.join_group({k: v[:m] for k, v in fact.items()}, dim, day_lt, threads=threads)
+        how = (f"the C++ restatement of the reference's join path (hash_join_with_keys: CRC32-tagged chained "
+               f"table + bloom filter, 65,536-row probe chunks on {threads} threads, materialised join, then "
+               f"execute_grouped)")
+        cores = threads
         desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
                 f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
         what = "probe rows (Zipf(0.8) fk over the 1.5M-row dimension, which is joined whole)"
@@ -352,16 +353,20 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         dominant = "scan_kernel probe + join + GROUP BY segment (25 groups, int128)"
         desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
                 f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
-        cs = min(n, 2_000_000)
         traffic = traffic_per_launch("join_group_agg_probe_kernel.md", n)
+        # CPU baseline: the reference's join path restated (filtered build
+        # side, tagged chained table + bloom filter, parallel chunked probe,
+        # materialised join, then the grouped aggregate) on all host threads.
+        from oracle import refpath
+        cs = min(n, 20_000_000)
         cpu_fact = {k: v[:cs] for k, v in fact.items()}
-        cpu_run = lambda: oracle.aggregate(cpu_fact, fct, tpl.aggs, tpl.group_by, tpl.where,
-                                           build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where),
-                                           probe_key="fk")
+        cpu_threads = os.cpu_count() or 1
+        day_lt = tpl.build_where.ops[0][3]
+        cpu_run = lambda: refpath.join_group(cpu_fact, dim, day_lt, threads=cpu_threads)["seconds"]
         cpu_rows = cs
-        cpu_threads = 1
-        cpu_desc = (f"first {cs} probe rows through the exact C++ oracle (row-at-a-time restatement of the "
-                    f"reference semantics; the reference's join path is not restated), one pass")
+        cpu_desc = (f"first {cs} probe rows, C++ restatement of the reference's join path (hash_join_with_keys: "
+                    f"CRC32-tagged chained table + bloom filter, 65,536-row probe chunks on {cpu_threads} "
+                    f"threads, materialised join, then execute_grouped)")
     else:  # highcard_group
         n = args.rows if args.rows != ROWS else 100_000_000
         host = datagen.highcard(n, 10_000_000, 1.1, seed=4 + rank)

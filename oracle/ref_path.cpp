@@ -366,4 +366,149 @@ double ref_highcard(const uint64_t* key, const uint64_t* val, uint64_t n, int th
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// The join + grouped aggregate the reference's way (hash_join_with_keys,
+// join.rs:544-939, then execute_grouped): the build side is the dimension
+// filtered on order_day < day_lt and materialised (filter_table); a chained
+// hash table (directory of next_pow2(2n) heads carrying an OR of 16-bit tags,
+// CRC32 hash times 0x8648DBDB00000001, join_hash_table.rs:76-200) and a bloom
+// filter (10 bits per key, 3 probes by double hashing of two CRC32 passes,
+// bloom_filter.rs:81-270) over its keys; the fact side probed in parallel
+// chunks of 65,536 rows (bloom test, then the chain), each chunk emitting
+// (probe row, build row) pairs; the joined table materialised column by
+// column; then GROUP BY segment over all its rows: chunked parallel grouping
+// and per group COUNT(*) and the f64 sum of price as f64 * (100 - disc) as f64.
+// Per group out: segment, count, sum. Returns wall seconds.
+double ref_join_group(const uint64_t* fk, const uint64_t* price, const uint64_t* disc, uint64_t nprobe,
+                      const uint64_t* dkey, const uint64_t* dday, const uint64_t* dseg, uint64_t nbuild,
+                      uint64_t day_lt, int threads, uint64_t cap, int64_t* keys, int64_t* counts, double* sums,
+                      uint64_t* ngroups) {
+    const auto t0 = std::chrono::steady_clock::now();
+    // Build side: filter, then gather its columns.
+    Bitmap bm = filter(dday, nbuild, day_lt, LT, false);
+    const std::vector<size_t> bsel = iter_set_bits(bm);
+    const size_t nb = bsel.size();
+    std::vector<uint64_t> bkey(nb), bday(nb), bseg(nb);
+    for (size_t i = 0; i < nb; ++i) {
+        bkey[i] = dkey[bsel[i]];
+        bday[i] = dday[bsel[i]];
+        bseg[i] = dseg[bsel[i]];
+    }
+    // Chained table with tagged heads.
+    size_t dir_size = 16;
+    while (dir_size < 2 * nb) dir_size <<= 1;
+    const int shift = 64 - __builtin_ctzll(dir_size);
+    std::vector<uint64_t> dir(dir_size, 0);
+    struct Entry {
+        uint64_t key;
+        uint32_t row, next;
+    };
+    std::vector<Entry> ent(nb + 1, Entry{0, 0, 0});
+    auto jhash = [](uint64_t k) { return static_cast<uint64_t>(_mm_crc32_u64(0, k)) * 0x8648DBDB00000001ull; };
+    auto tag_of = [](uint64_t h) { return static_cast<uint16_t>((h >> 16) | 1); };
+    // Bloom filter.
+    size_t nwords = 1;
+    while (nwords < (nb * 10 + 63) / 64) nwords <<= 1;
+    std::vector<uint64_t> bloom(nwords, 0);
+    auto mix = [](uint64_t z) {
+        z += 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    auto pair = [&](uint64_t k, uint64_t& h1, uint64_t& h2) {
+        h1 = mix(_mm_crc32_u64(0, k));
+        h2 = mix(_mm_crc32_u64(~0ull, k)) | 1;
+    };
+    for (size_t r = 0; r < nb; ++r) {
+        const uint64_t h = jhash(bkey[r]);
+        const size_t slot = h >> shift;
+        const uint32_t e = static_cast<uint32_t>(r + 1);
+        ent[e] = Entry{bkey[r], static_cast<uint32_t>(r), static_cast<uint32_t>(dir[slot] & 0xFFFFFFFFull)};
+        const uint16_t t = static_cast<uint16_t>(dir[slot] >> 48) | tag_of(h);
+        dir[slot] = (static_cast<uint64_t>(t) << 48) | e;
+        uint64_t h1, h2;
+        pair(bkey[r], h1, h2);
+        for (int i = 0; i < 3; ++i, h1 += h2) bloom[(h1 >> 6) & (nwords - 1)] |= 1ull << (h1 & 63);
+    }
+    // Probe in parallel chunks.
+    const size_t nchunks = (nprobe + kGroupChunk - 1) / kGroupChunk;
+    std::vector<std::vector<uint32_t>> lsrc(nchunks), rsrc(nchunks);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (size_t c = 0; c < nchunks; ++c) {
+        const size_t lo = c * kGroupChunk, hi = std::min<size_t>(nprobe, lo + kGroupChunk);
+        auto& L = lsrc[c];
+        auto& R = rsrc[c];
+        for (size_t p = lo; p < hi; ++p) {
+            const uint64_t k = fk[p];
+            uint64_t h1, h2;
+            pair(k, h1, h2);
+            bool maybe = true;
+            for (int i = 0; i < 3 && maybe; ++i, h1 += h2) maybe = (bloom[(h1 >> 6) & (nwords - 1)] >> (h1 & 63)) & 1;
+            if (!maybe) continue;
+            const uint64_t h = jhash(k);
+            const uint64_t head = dir[h >> shift];
+            const uint16_t t = static_cast<uint16_t>(head >> 48), want = tag_of(h);
+            if (t == 0 || (t & want) != want) continue;
+            for (uint32_t e = static_cast<uint32_t>(head & 0xFFFFFFFFull); e; e = ent[e].next)
+                if (ent[e].key == k) {
+                    L.push_back(static_cast<uint32_t>(p));
+                    R.push_back(ent[e].row);
+                }
+        }
+    }
+    // Materialise the joined table (every column of both sides).
+    std::vector<size_t> off(nchunks + 1, 0);
+    for (size_t c = 0; c < nchunks; ++c) off[c + 1] = off[c] + lsrc[c].size();
+    const size_t nj = off[nchunks];
+    std::vector<uint64_t> jfk(nj), jprice(nj), jdisc(nj), jkey(nj), jday(nj), jseg(nj);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (size_t c = 0; c < nchunks; ++c)
+        for (size_t i = 0; i < lsrc[c].size(); ++i) {
+            const size_t o = off[c] + i, p = lsrc[c][i], b = rsrc[c][i];
+            jfk[o] = fk[p];
+            jprice[o] = price[p];
+            jdisc[o] = disc[p];
+            jkey[o] = bkey[b];
+            jday[o] = bday[b];
+            jseg[o] = bseg[b];
+        }
+    // GROUP BY segment over all joined rows.
+    const std::vector<size_t> idx = iter_set_bits(Bitmap::all_ones(nj));
+    const size_t gch = (idx.size() + kGroupChunk - 1) / kGroupChunk;
+    std::vector<std::unordered_map<uint64_t, std::vector<size_t>, FxHash>> local(gch);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (size_t c = 0; c < gch; ++c) {
+        const size_t lo = c * kGroupChunk, hi = std::min(idx.size(), lo + kGroupChunk);
+        for (size_t i = lo; i < hi; ++i) local[c][jseg[idx[i]]].push_back(idx[i]);
+    }
+    std::unordered_map<uint64_t, size_t, FxHash> gid;
+    std::vector<std::vector<size_t>> groups;
+    for (auto& m : local)
+        for (auto& kv : m) {
+            auto it = gid.find(kv.first);
+            size_t g;
+            if (it == gid.end()) {
+                g = groups.size();
+                gid.emplace(kv.first, g);
+                groups.emplace_back();
+            } else {
+                g = it->second;
+            }
+            groups[g].insert(groups[g].end(), kv.second.begin(), kv.second.end());
+        }
+    for (size_t g = 0; g < groups.size(); ++g) {
+        double sum = 0.0;
+        for (size_t r : groups[g])
+            sum += static_cast<double>(jprice[r]) * static_cast<double>(100 - static_cast<int64_t>(jdisc[r]));
+        if (g < cap) {
+            keys[g] = static_cast<int64_t>(jseg[groups[g][0]]);
+            counts[g] = static_cast<int64_t>(groups[g].size());
+            sums[g] = sum;
+        }
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    *ngroups = groups.size();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
 }  // extern "C"

@@ -130,3 +130,27 @@ def highcard(cols: dict, threads: int | None = None, cap: int | None = None) -> 
     order = np.argsort(k[:g], kind="stable")
     return {"seconds": sec, "ngroups": int(ng.value), "keys": k[:g][order], "counts": c[:g][order],
             "sums": s[:g][order], "threads": threads}
+
+
+def join_group(fact: dict, dim: dict, day_lt: int, threads: int | None = None) -> dict:
+    """The join + GROUP BY segment aggregate (sum(price*(100-disc)), count) the
+    reference's way (``ref_join_group``). Returns the wall seconds and the
+    groups sorted by segment: (segment, count, f64 sum)."""
+    import os
+    lib = load()
+    fn = lib.ref_join_group
+    fn.restype = C.c_double
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                   C.c_uint64, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]
+    f = {k: np.ascontiguousarray(to_cells(fact[k])) for k in ("fk", "price_cents", "discount_pct")}
+    d = {k: np.ascontiguousarray(to_cells(dim[k])) for k in ("key", "order_day", "segment")}
+    threads = threads or os.cpu_count() or 1
+    cap = 1024
+    keys, counts, sums = np.zeros(cap, np.int64), np.zeros(cap, np.int64), np.zeros(cap, np.float64)
+    ng = C.c_uint64()
+    sec = fn(f["fk"].ctypes.data, f["price_cents"].ctypes.data, f["discount_pct"].ctypes.data, f["fk"].shape[0],
+             d["key"].ctypes.data, d["order_day"].ctypes.data, d["segment"].ctypes.data, d["key"].shape[0],
+             int(day_lt), threads, cap, keys.ctypes.data, counts.ctypes.data, sums.ctypes.data, C.byref(ng))
+    g = min(int(ng.value), cap)
+    rows = sorted((int(keys[i]), int(counts[i]), float(sums[i])) for i in range(g))
+    return {"seconds": sec, "groups": rows, "threads": threads}

@@ -42,3 +42,19 @@ def test_highcard_matches_exact():
         assert [int(x) for x in r["keys"]] == [k[0] for k in exact.keys]
         assert [int(x) for x in r["counts"]] == [v[0].value for v in exact.values]
         assert [int(x) for x in r["sums"]] == [v[1].value for v in exact.values]
+
+
+def test_join_group_matches_exact():
+    dim = datagen.dimension(60_000, seed=12)
+    fact = datagen.fact_fk(500_000, 60_000, 0.8, seed=13)
+    fact["fk"][:40] = 90_000   # keys outside the build side
+    tpl = workloads.join_group_agg(order_day_lt=datagen.DAY0 + datagen.NDAYS // 2)
+    fct = {"fk": "int", "price_cents": "int", "discount_pct": "int"}
+    exact = oracle.aggregate({k: fact[k] for k in fct}, fct, tpl.aggs, tpl.group_by, None,
+                             build=(dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where), probe_key="fk")
+    for threads in (1, 4):
+        r = refpath.join_group(fact, dim, datagen.DAY0 + datagen.NDAYS // 2, threads=threads)
+        assert [g[0] for g in r["groups"]] == [k[0] for k in exact.keys]
+        for (seg, cnt, s), vals in zip(r["groups"], exact.values):
+            assert cnt == vals[1].value
+            assert vals[0].value < 2**53 and s == float(vals[0].value)   # exact below 2^53
