@@ -464,6 +464,12 @@ TGP_API int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_ag
 TGP_API int tgp_count_distinct(tgp_ctx* ctx, tgp_table_id table, uint32_t column, const tgp_pred_node* pred,
                                uint32_t npred, uint64_t* count, uint32_t* method);
 
+/* The HyperLogLog estimate tgp_count_distinct makes from 2^14 registers (the
+ * reference's HyperLogLog::estimate, src/exec/hll.rs:53-76), for callers that
+ * merge register sets themselves (the registers of a union are the element-wise
+ * max). Host-only: needs no context or device. */
+TGP_API int tgp_hll_estimate(const uint32_t* regs, uint64_t* out);
+
 /* ------------------------------------------------------------------------ */
 /* Hash join (src/engine/query_interpreter/join.rs:544-939)                  */
 /* ------------------------------------------------------------------------ */

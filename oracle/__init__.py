@@ -76,6 +76,8 @@ def _sig(lib):
     lib.orc_xxh3_u64.restype = C.c_uint64
     lib.orc_hll_estimate.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
     lib.orc_hll_estimate.restype = C.c_uint64
+    lib.orc_hll_estimate_regs.argtypes = [C.c_void_p]
+    lib.orc_hll_estimate_regs.restype = C.c_uint64
     lib.orc_count_distinct.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint32)]
     lib.orc_count_distinct.restype = None

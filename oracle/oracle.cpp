@@ -429,6 +429,22 @@ uint64_t orc_hll_estimate(const uint64_t* cells, uint64_t n, const uint8_t* sel)
     return static_cast<uint64_t>(est);
 }
 
+// The estimate alone, from 2^14 registers (pins the library's host estimator).
+uint64_t orc_hll_estimate_regs(const uint32_t* regs) {
+    const double m = 16384.0, alpha = 0.7213 / (1.0 + 1.079 / m);
+    double sum = 0.0;
+    uint64_t zeros = 0;
+    for (int i = 0; i < 16384; ++i) {
+        double p = 1.0;
+        for (uint32_t k = 0; k < regs[i]; ++k) p *= 0.5;
+        sum += p;
+        if (regs[i] == 0) ++zeros;
+    }
+    const double raw = alpha * m * m / sum;
+    const double est = (raw <= 2.5 * m && zeros > 0) ? m * std::log(m / static_cast<double>(zeros)) : raw;
+    return static_cast<uint64_t>(est);
+}
+
 // COUNT(DISTINCT col) as the reference evaluates it (aggregate.rs:1301-1325):
 // exact below 100,000 selected rows (method 0), else the HyperLogLog
 // estimate (method 1). `sel` is an LSB-first bitmap or NULL (all rows).

@@ -46,3 +46,22 @@ def test_threshold_counts_selected_rows():
     bm = np.packbits(sel, bitorder="little")
     c, m = oracle.count_distinct(cells, bm)
     assert m == "hll" and abs(c - len(np.unique(cells[:100_000]))) / len(np.unique(cells[:100_000])) < 0.03
+
+
+def test_library_estimator_matches_the_oracle():
+    """The library's host-side estimate (tgp_hll_estimate, the arithmetic
+    tgp_count_distinct applies to the device registers) equals the oracle's,
+    in the linear-counting and in the raw regime."""
+    import ctypes as C
+    from turbogp_b200 import _capi as A
+    lib = A.load()
+    rng = np.random.default_rng(4)
+    cases = [np.zeros(16384, np.uint32), np.full(16384, 65, np.uint32)]
+    for zero_frac in (0.999, 0.9, 0.5, 0.1, 0.0):
+        r = rng.geometric(0.5, 16384).astype(np.uint32)
+        r[rng.random(16384) < zero_frac] = 0
+        cases.append(r)
+    for regs in cases:
+        out = C.c_uint64()
+        assert lib.tgp_hll_estimate(regs.ctypes.data, C.byref(out)) == A.OK
+        assert out.value == oracle._lib().orc_hll_estimate_regs(regs.ctypes.data)

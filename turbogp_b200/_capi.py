@@ -151,6 +151,7 @@ PROTOTYPES = [
     ("tgp_count_distinct", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.POINTER(C.c_uint64),
       C.POINTER(C.c_uint32)]),
+    ("tgp_hll_estimate", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("tgp_join_build", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.POINTER(C.c_uint64)]),
     ("tgp_join_drop", C.c_int, [C.c_void_p, C.c_uint64]),

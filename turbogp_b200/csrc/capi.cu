@@ -1264,6 +1264,12 @@ static uint64_t hll_estimate(const std::vector<uint32_t>& regs) {
     return static_cast<uint64_t>(est);
 }
 
+int tgp_hll_estimate(const uint32_t* regs, uint64_t* out) {
+    if (!regs || !out) return TGP_INVALID_ARG;
+    *out = hll_estimate(std::vector<uint32_t>(regs, regs + 16384));
+    return TGP_OK;
+}
+
 int tgp_count_distinct(tgp_ctx* ctx, tgp_table_id table, uint32_t column, const tgp_pred_node* pred, uint32_t npred,
                        uint64_t* count, uint32_t* method) {
     if (!ctx || !count) return fail(ctx, TGP_INVALID_ARG, "null argument");
