@@ -12,6 +12,9 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA (sm_100a) device")
+    # Temporary files (tmp_path) stay inside the repository checkout.
+    if config.option.basetemp is None:
+        config.option.basetemp = str(ROOT / ".pytest_tmp")
 
 
 @pytest.fixture(scope="session")
