@@ -67,6 +67,7 @@ STRUCTS = {
     "tgp_kernel_result": (A.KernelResultC, ["count", "sum", "mask"]),
     "tgp_kernel_info": (A.KernelInfo, ["op", "cpu", "tier", "name"]),
     "tgp_batch_item": (A.BatchItem, ["query", "keys_out", "vals_out", "group_cap", "result", "status"]),
+    "tgp_cell_column": (A.CellColumn, ["cells", "i32_sidecar", "coltype"]),
 }
 
 
