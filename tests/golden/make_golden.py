@@ -132,6 +132,26 @@ group_kats = [
 join_count_kats = [
     {"source": f"{JOINS}:36", "left": [1, 2, 3], "right": [1], "inner_rows": 1},
 ]
+# execute_dispatched over make_table(n): id = i, val = i % 20, grp = i % 5
+# (src/engine/dispatch.rs:1694-1720); the queries of its tests on this path.
+DISPATCH = "src/engine/dispatch.rs"
+dispatch_kats = {
+    "table": {"id": "range", "val": {"mod": 20}, "grp": {"mod": 5}},
+    "cases": [
+        {"source": f"{DISPATCH}:1778", "n": 100, "agg": "count_star", "where": None, "value": 100},
+        {"source": f"{DISPATCH}:1789", "n": 100, "agg": "count_star", "where": ["val", "eq", 5], "value": 5},
+        {"source": f"{DISPATCH}:1800", "n": 100, "agg": ["sum", "val"], "where": ["val", "gt", 15],
+         "value": 350},
+        {"source": f"{DISPATCH}:1813", "n": 100, "agg": "count_star", "group_by": "grp", "where": None,
+         "ngroups": 5},
+        {"source": f"{DISPATCH}:1824", "n": 100, "agg": "count_star", "group_by": "grp", "where": None,
+         "order_by_key_limit": 3, "ngroups": 3},
+        {"source": f"{DISPATCH}:1838", "n": 100, "agg": ["max", "val"], "where": None, "value": 19},
+        {"source": f"{DISPATCH}:1849", "n": 100, "agg": ["count_distinct", "val"], "where": None, "value": 20},
+        {"source": f"{DISPATCH}:1885", "n": 1_000_000, "agg": "count_star", "where": ["val", "eq", 5],
+         "value": 50000},
+    ],
+}
 
 out = {
     "filters": [dict(source=s, dtype=d, coltype=c, column=col, cmp=op, lit=v, expect=e)
@@ -144,6 +164,7 @@ out = {
     "arithmetic": arith,
     "groups": group_kats,
     "join_counts": join_count_kats,
+    "dispatch": dispatch_kats,
 }
 Path(__file__).with_name("reference_kats.json").write_text(json.dumps(out, indent=1) + "\n")
 print("wrote", sum(len(v) if isinstance(v, list) else 1 for v in out.values()), "groups of cases")

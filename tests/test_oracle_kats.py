@@ -126,3 +126,37 @@ def test_reference_path_restatement_matches_oracle():
         o = oracle.aggregate(cols, refpath.COLTYPES, tpl.aggs, tpl.group_by, tpl.where)
         assert r["count"] == o.values[0][1].value
         assert int(r["sum"]) == o.values[0][0].value
+
+
+def test_dispatch_kats(kats):
+    """The reference's dispatcher tests over make_table(n) (src/engine/dispatch.rs)."""
+    from turbogp_b200.engine import col, count_star, max_, sum_
+    d = kats["dispatch"]
+    assert d["table"] == {"id": "range", "val": {"mod": 20}, "grp": {"mod": 5}}
+    for c in d["cases"]:
+        n = c["n"]
+        i = np.arange(n, dtype=np.uint64)
+        t = {"id": i, "val": i % 20, "grp": i % 5}
+        w = None
+        if c["where"]:
+            name, op, lit = c["where"]
+            w = {"eq": col(name) == lit, "gt": col(name) > lit}[op]
+        agg = c["agg"]
+        if agg == "count_star":
+            aggs = [count_star()]
+        elif agg[0] == "sum":
+            aggs = [sum_(col(agg[1]))]
+        elif agg[0] == "max":
+            aggs = [max_(col(agg[1]))]
+        else:
+            got = oracle.count_distinct(t[agg[1]])
+            assert got == (c["value"], "exact"), c["source"]
+            continue
+        gb = (c["group_by"],) if "group_by" in c else ()
+        out = oracle.aggregate(t, None, aggs, gb, w)
+        if "ngroups" in c:
+            keys = out.keys[:c.get("order_by_key_limit", len(out.keys))]
+            assert len(keys) == c["ngroups"], c["source"]
+            assert keys == sorted(keys)
+        else:
+            assert out.values[0][0].value == c["value"], c["source"]
