@@ -27,7 +27,6 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
-#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -169,10 +168,92 @@ std::vector<size_t> iter_set_bits(const Bitmap& bm) {
     return out;
 }
 
-// FxHasher::write_u64 from a fresh hasher: the word times the Fx constant.
-struct FxHash {
-    size_t operator()(uint64_t x) const { return static_cast<size_t>(x * 0x517cc1b727220a95ull); }
+// A u64-keyed open-addressing map with values stored in place, standing in
+// for the reference's FxHashMap (hashbrown: one allocation for the table, FxHash
+// of the key = the key times 0x517cc1b727220a95, grown at 7/8 load). Linear
+// probing on the high bits of the hash.
+template <class V>
+class FlatMap {
+public:
+    FlatMap() { reset(16); }
+    // The value of key k, default-constructed when k is new.
+    V& operator[](uint64_t k) {
+        if ((n_ + 1) * 8 > cap_ * 7) grow();
+        const size_t i = probe(k);
+        if (!used_[i]) {
+            used_[i] = 1;
+            keys_[i] = k;
+            ++n_;
+        }
+        return vals_[i];
+    }
+    V* find(uint64_t k) {
+        const size_t i = probe(k);
+        return used_[i] ? &vals_[i] : nullptr;
+    }
+    template <class F>
+    void for_each(F&& f) {
+        for (size_t i = 0; i < cap_; ++i)
+            if (used_[i]) f(keys_[i], vals_[i]);
+    }
+
+private:
+    size_t probe(uint64_t k) const {
+        size_t i = static_cast<size_t>((k * 0x517cc1b727220a95ull) >> shift_);
+        while (used_[i] && keys_[i] != k) i = (i + 1) & (cap_ - 1);
+        return i;
+    }
+    void reset(size_t cap) {
+        cap_ = cap;
+        shift_ = 64 - __builtin_ctzll(cap);
+        keys_.assign(cap, 0);
+        vals_.clear();
+        vals_.resize(cap);
+        used_.assign(cap, 0);
+        n_ = 0;
+    }
+    void grow() {
+        std::vector<uint64_t> k = std::move(keys_);
+        std::vector<V> v = std::move(vals_);
+        std::vector<uint8_t> u = std::move(used_);
+        reset(cap_ * 2);
+        for (size_t i = 0; i < u.size(); ++i)
+            if (u[i]) {
+                const size_t j = probe(k[i]);
+                used_[j] = 1;
+                keys_[j] = k[i];
+                vals_[j] = std::move(v[i]);
+                ++n_;
+            }
+    }
+    std::vector<uint64_t> keys_;
+    std::vector<V> vals_;
+    std::vector<uint8_t> used_;
+    size_t cap_ = 0, n_ = 0;
+    int shift_ = 0;
 };
+
+// Merges per-chunk hash → row-list maps in chunk order into group row lists
+// (the order the reference's execute_grouped merge appends rows in).
+std::vector<std::vector<size_t>> merge_groups(std::vector<FlatMap<std::vector<size_t>>>& local) {
+    FlatMap<size_t> gid;
+    std::vector<std::vector<size_t>> groups;
+    groups.reserve(1024);
+    for (auto& m : local)
+        m.for_each([&](uint64_t h, std::vector<size_t>& rows) {
+            size_t* g = gid.find(h);
+            size_t id;
+            if (!g) {
+                id = groups.size();
+                gid[h] = id;
+                groups.emplace_back();
+            } else {
+                id = *g;
+            }
+            groups[id].insert(groups[id].end(), rows.begin(), rows.end());
+        });
+    return groups;
+}
 
 constexpr size_t kGroupChunk = 65536;  // GROUP_CHUNK_SIZE (aggregate.rs:582, accum_grouped.rs:197)
 
@@ -254,7 +335,7 @@ double ref_grouped_q1(const uint64_t* const* cols, uint64_t n, const ref_leaf* l
     Bitmap mask = mask_of(cols, n, leaves, nleaves);
     const std::vector<size_t> idx = iter_set_bits(mask);
     const size_t nchunks = (idx.size() + kGroupChunk - 1) / kGroupChunk;
-    std::vector<std::unordered_map<uint64_t, std::vector<size_t>, FxHash>> local(nchunks);
+    std::vector<FlatMap<std::vector<size_t>>> local(nchunks);
     const uint64_t* gk[2] = {cols[ka], cols[kb]};
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (size_t c = 0; c < nchunks; ++c) {
@@ -267,22 +348,7 @@ double ref_grouped_q1(const uint64_t* const* cols, uint64_t n, const ref_leaf* l
             m[h].push_back(r);
         }
     }
-    std::unordered_map<uint64_t, size_t, FxHash> gid;
-    std::vector<std::vector<size_t>> groups;
-    groups.reserve(1024);
-    for (auto& m : local)
-        for (auto& kv : m) {
-            auto it = gid.find(kv.first);
-            size_t g;
-            if (it == gid.end()) {
-                g = groups.size();
-                gid.emplace(kv.first, g);
-                groups.emplace_back();
-            } else {
-                g = it->second;
-            }
-            groups[g].insert(groups[g].end(), kv.second.begin(), kv.second.end());
-        }
+    std::vector<std::vector<size_t>> groups = merge_groups(local);
     const uint64_t *q = cols[cq], *p = cols[cp], *d = cols[cd], *t = cols[ct];
     for (size_t g = 0; g < groups.size(); ++g) {
         const std::vector<size_t>& rows = groups[g];
@@ -327,41 +393,40 @@ double ref_highcard(const uint64_t* key, const uint64_t* val, uint64_t n, int th
     Bitmap mask = Bitmap::all_ones(n);
     const std::vector<size_t> idx = iter_set_bits(mask);
     const size_t nchunks = (idx.size() + kGroupChunk - 1) / kGroupChunk;
-    std::vector<std::unordered_map<uint64_t, std::vector<uint64_t>, FxHash>> local(nchunks);
+    std::vector<FlatMap<std::vector<uint64_t>>> local(nchunks);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (size_t c = 0; c < nchunks; ++c) {
         const size_t lo = c * kGroupChunk, hi = std::min(idx.size(), lo + kGroupChunk);
         auto& m = local[c];
         for (size_t i = lo; i < hi; ++i) {
             const size_t r = idx[i];
-            auto it = m.find(key[r]);
-            if (it == m.end()) it = m.emplace(key[r], std::vector<uint64_t>{key[r], 0, 0}).first;
-            std::vector<uint64_t>& acc = it->second;
+            std::vector<uint64_t>& acc = m[key[r]];
+            if (acc.empty()) acc = {key[r], 0, 0};  // slots allocated per new group
             acc[1] += 1;
             acc[2] += val[r];
         }
     }
-    std::unordered_map<uint64_t, std::vector<uint64_t>, FxHash> global;
+    FlatMap<std::vector<uint64_t>> global;
     for (auto& m : local)
-        for (auto& kv : m) {
-            auto it = global.find(kv.first);
-            if (it == global.end()) {
-                global.emplace(kv.first, std::move(kv.second));
+        m.for_each([&](uint64_t k, std::vector<uint64_t>& acc) {
+            std::vector<uint64_t>* e = global.find(k);
+            if (!e) {
+                global[k] = std::move(acc);
             } else {
-                it->second[1] += kv.second[1];
-                it->second[2] += kv.second[2];
+                (*e)[1] += acc[1];
+                (*e)[2] += acc[2];
             }
-        }
+        });
     const auto t1 = std::chrono::steady_clock::now();
     uint64_t g = 0;
-    for (auto& kv : global) {
+    global.for_each([&](uint64_t, std::vector<uint64_t>& acc) {
         if (g < cap) {
-            keys[g] = static_cast<int64_t>(kv.second[0]);
-            counts[g] = static_cast<int64_t>(kv.second[1]);
-            sums[g] = static_cast<int64_t>(kv.second[2]);
+            keys[g] = static_cast<int64_t>(acc[0]);
+            counts[g] = static_cast<int64_t>(acc[1]);
+            sums[g] = static_cast<int64_t>(acc[2]);
         }
         ++g;
-    }
+    });
     *ngroups = g;
     return std::chrono::duration<double>(t1 - t0).count();
 }
@@ -475,27 +540,13 @@ double ref_join_group(const uint64_t* fk, const uint64_t* price, const uint64_t*
     // GROUP BY segment over all joined rows.
     const std::vector<size_t> idx = iter_set_bits(Bitmap::all_ones(nj));
     const size_t gch = (idx.size() + kGroupChunk - 1) / kGroupChunk;
-    std::vector<std::unordered_map<uint64_t, std::vector<size_t>, FxHash>> local(gch);
+    std::vector<FlatMap<std::vector<size_t>>> local(gch);
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (size_t c = 0; c < gch; ++c) {
         const size_t lo = c * kGroupChunk, hi = std::min(idx.size(), lo + kGroupChunk);
         for (size_t i = lo; i < hi; ++i) local[c][jseg[idx[i]]].push_back(idx[i]);
     }
-    std::unordered_map<uint64_t, size_t, FxHash> gid;
-    std::vector<std::vector<size_t>> groups;
-    for (auto& m : local)
-        for (auto& kv : m) {
-            auto it = gid.find(kv.first);
-            size_t g;
-            if (it == gid.end()) {
-                g = groups.size();
-                gid.emplace(kv.first, g);
-                groups.emplace_back();
-            } else {
-                g = it->second;
-            }
-            groups[g].insert(groups[g].end(), kv.second.begin(), kv.second.end());
-        }
+    std::vector<std::vector<size_t>> groups = merge_groups(local);
     for (size_t g = 0; g < groups.size(); ++g) {
         double sum = 0.0;
         for (size_t r : groups[g])
