@@ -163,8 +163,14 @@ def _merge_rows(rows: np.ndarray, nk: int, na: int, funcs: Sequence[int]):
     mask32 = np.uint64(0xFFFFFFFF)
     for a, f in enumerate(funcs):
         if f in (A.AGG_MIN, A.AGG_MAX):
+            # Partials without rows for this aggregate do not take part (a
+            # group whose partials all lack rows keeps its first value).
             v = lo[:, a].view(np.int64)
-            r = (np.minimum if f == A.AGG_MIN else np.maximum).reduceat(v, starts)
+            ident = np.iinfo(np.int64).max if f == A.AGG_MIN else np.iinfo(np.int64).min
+            has = cnt[:, a] > 0
+            r = (np.minimum if f == A.AGG_MIN else np.maximum).reduceat(np.where(has, v, ident), starts)
+            none = np.add.reduceat(has.astype(np.int64), starts) == 0
+            r = np.where(none, v[starts], r)
             out_lo[:, a] = r.view(np.uint64)
             out_hi[:, a] = r >> 63
         else:
