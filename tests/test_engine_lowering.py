@@ -31,3 +31,28 @@ def test_key_owner_is_deterministic_and_spread():
     # Multi-column keys: every column takes part.
     k2 = np.stack([np.zeros(1000, np.int64), np.arange(1000, dtype=np.int64)], axis=1)
     assert len(set(shard.key_owner(k2, 8).tolist())) == 8
+
+
+def test_merge_rows_int128_carries_and_empty_minmax():
+    from turbogp_b200.engine import count_star, max_, min_, sum_, col
+    aggs = [count_star(), sum_(col("v")), min_(col("v")), max_(col("v"))]
+    funcs = [a.func for a in aggs]
+    M = (1 << 64) - 1
+
+    def row(key, total, count, mn, mx, mcount):
+        vals = [(count, count), (total, count), (mn, mcount), (mx, mcount)]
+        lo = [v & M for v, _ in vals]
+        hi = [v >> 64 for v, _ in vals]
+        cnt = [c for _, c in vals]
+        return [key] + [int(np.uint64(x).view(np.int64)) for x in lo] + hi + cnt
+
+    big = (1 << 100) + 12345          # needs the high limb
+    rows = np.array([row(7, big, 3, -5, 9, 3), row(7, big, 2, -8, 4, 2), row(7, -3, 1, 0, 0, 0),
+                     row(-1, (1 << 64) - 1, 1, 2, 2, 1), row(-1, 1, 1, 1, 1, 1)], dtype=np.int64)
+    keys, lo, hi, cnt = shard._merge_rows(rows, 1, 4, funcs)
+    assert keys.tolist() == [[-1], [7]]
+    val = lambda g, a: (int(hi[g, a]) << 64) | int(lo[g, a])   # noqa: E731
+    assert val(0, 1) == 1 << 64 and val(1, 1) == 2 * big - 3     # carries out of the low limb
+    assert cnt[1].tolist() == [6, 6, 5, 5]
+    assert int(lo[1, 2].view(np.int64)) == -8 and int(lo[1, 3].view(np.int64)) == 9   # the row without rows skipped
+    assert int(lo[0, 2].view(np.int64)) == 1 and int(lo[0, 3].view(np.int64)) == 2
