@@ -13,8 +13,13 @@ LargeUtf8 strings the xxh3_64 hash of their bytes (parquet.rs:389-436), which
 equality predicates on string literals compare against (the reference's
 string search index for LIKE is not built).
 
-Difference from the reference, on purpose: a column type the reference fills
-with zeros (timestamps, decimals, ...) raises here instead.
+Differences from the reference, on purpose: a column type the reference fills
+with zeros (timestamps, decimals, ...) raises here instead; and comparison
+types are inferred from the Arrow type (Date32 → date, Float64 → float, other
+columns int) where the reference types a table without a schema as all Int
+unless it is a TPC-H table (ExecTable::from_catalog,
+src/engine/query_interpreter/types.rs:271-305). ``coltypes`` overrides the
+inference per column, so the reference's typing can be asked for.
 """
 from __future__ import annotations
 
