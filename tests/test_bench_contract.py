@@ -41,6 +41,14 @@ def test_reference_arm_grouped_workload():
     assert d["config"]["workload"].startswith("filtered_group_agg (400000 rows")
 
 
+def test_reference_arm_join_and_highcard_workloads():
+    for w in ("join_group_agg", "highcard_group"):
+        d = run("--workload", w, "--steps", "1", "--warmup", "3", "--rows", "300000")
+        check_line(d)
+        assert d["config"]["workload"].startswith(w) and d["cpu_baseline"]["cores"] >= 1
+        assert "restatement of the reference's" in d["cpu_baseline"]["sample"]
+
+
 def test_reference_arm_unavailable_for_serving():
     for w in ("batch", "serve"):
         d = run("--workload", w, "--steps", "1", "--warmup", "3")
