@@ -558,7 +558,7 @@ TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
 /* ------------------------------------------------------------------------ */
 
 /* Size of the library's fixed device scratch for tgp_aggregate_noalloc. */
-#define TGP_NOALLOC_SCRATCH_BYTES (256u * 1024u)
+#define TGP_NOALLOC_SCRATCH_BYTES (1024u * 1024u)
 
 /* One GROUP BY column of tgp_aggregate_noalloc and the values it may hold:
  * every cell lies in [min, min + count). */
@@ -570,13 +570,16 @@ typedef struct tgp_key_domain {
 } tgp_key_domain;
 
 /* Has no counterpart in the reference: an entry point for callers that cannot
- * allocate GPU memory — code recording a CUDA graph, running under an
- * allocator that owns the whole device, or bound by a no-allocation-after-
- * start-up policy. It computes the same scalar or grouped aggregate as
- * tgp_execute over caller-owned, 16-byte-aligned DEVICE columns, without a
- * context and without calling cudaMalloc, cudaFree or any allocating routine:
- * its accumulators live in a fixed TGP_NOALLOC_SCRATCH_BYTES device array that
- * every GPU loading the library keeps until the process exits.
+ * allocate GPU memory — an embedding engine whose own allocator reserved the
+ * whole device at start-up (a cudaMalloc here would fail, or take memory the
+ * allocator has promised elsewhere), a latency-bound serving thread that may
+ * not take the device-wide synchronisation a cudaMalloc / cudaFree can cause,
+ * or a host bound by a no-allocation-after-start-up policy. It computes the
+ * same scalar or grouped aggregate as tgp_execute over caller-owned,
+ * 16-byte-aligned DEVICE columns on `device`, without a context and without
+ * calling cudaMalloc, cudaFree or any allocating routine: its accumulators live
+ * in a fixed TGP_NOALLOC_SCRATCH_BYTES (1 MiB) device array that every GPU
+ * loading the library keeps until the process exits.
  *
  *  - Groups are dense: group g enumerates the key domains with the first key
  *    most significant; vals_out (HOST memory) receives ngroups * nagg values in
@@ -585,12 +588,17 @@ typedef struct tgp_key_domain {
  *    (TGP_INVALID_ARG) before any accumulation.
  *  - Queries whose scratch exceeds TGP_NOALLOC_SCRATCH_BYTES (many groups times
  *    many aggregates) are rejected with TGP_CAPACITY and a message.
- *  - The first call on a device looks up the array's device address; make it
- *    before any stream capture. All calls share the array: calls that overlap
- *    on the GPU race and must be serialised by the caller.
+ *  - Columns that live on another GPU are rejected (TGP_INVALID_ARG).
+ *  - The first call on a device looks up the array's device address (once per
+ *    device, with that device current); make it before any stream capture. The
+ *    address is kept for the life of the process, so a cudaDeviceReset of that
+ *    device, or a non-primary context made current on it, is not supported.
+ *  - All calls share the array and it keeps the last call's contents; each call
+ *    clears what it accumulates into. Calls that overlap on the GPU (two
+ *    streams, or two host threads) race on it: the caller serialises them.
  *  - `stream` is a cudaStream_t (NULL = the default stream); the call returns
- *    after its work on that stream has finished. Failures carry a message in
- *    err_msg (may be NULL). */
+ *    after its work on that stream has finished, with the caller's current
+ *    device unchanged. Failures carry a message in err_msg (may be NULL). */
 TGP_API int tgp_aggregate_noalloc(int device, void* stream, const tgp_column_desc* cols, uint32_t ncols,
                                   uint64_t rows, const tgp_pred_node* pred, uint32_t npred,
                                   const tgp_key_domain* keys, uint32_t nkeys, const tgp_agg* aggs, uint32_t nagg,

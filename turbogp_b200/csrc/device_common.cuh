@@ -119,7 +119,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // ---------------------------------------------------------------------------
-// 1-D bulk copy global → shared (TMA engine, no tensor map, no multicast).
+// 1-D bulk copy global → shared (TMA engine, no tensor map, one destination
+// CTA, this GPU's own memory only).
 // dst, src and bytes must all be multiples of 16.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes,

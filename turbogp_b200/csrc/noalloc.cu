@@ -1,24 +1,26 @@
 // noalloc.cu — tgp_aggregate_noalloc: the scalar / low-cardinality grouped
 // aggregate of the scan kernel for callers that cannot allocate GPU memory.
 //
-// Who needs it: code that runs where cudaMalloc is off limits — inside a
-// CUDA-graph capture the caller is recording, under a memory manager or
-// allocator that owns every byte of the device, or in a host whose policy
-// forbids allocations after start-up. Such callers pass their own device
-// columns and a host output buffer; this entry point allocates nothing.
+// Who needs it: an embedding engine whose own allocator reserved the whole
+// device at start-up (a cudaMalloc would fail or take memory that allocator
+// promised elsewhere), a latency-bound serving thread that may not take the
+// device-wide synchronisation cudaMalloc / cudaFree can cause, or a host whose
+// policy forbids allocations after start-up. Such callers pass their own
+// device columns and a host output buffer; this entry point allocates nothing.
 //
 // Its scratch (accumulators, row counters, error word, key min/max and the
 // finished per-group values) lives in one file-scope `static __device__`
-// array of TGP_NOALLOC_SCRATCH_BYTES. Every GPU that loads the library keeps
-// that array until the process exits. All calls share it and it keeps the last
-// call's contents, so each call re-initialises what it uses; calls whose work
-// overlaps on the GPU (two streams, or two host threads) race on it and must
-// be serialised by the caller.
+// array of TGP_NOALLOC_SCRATCH_BYTES (1 MiB). Every GPU that loads the library
+// keeps that array until the process exits. All calls share it and it keeps
+// the last call's contents, so each call re-initialises what it uses; calls
+// whose work overlaps on the GPU (two streams, or two host threads) race on it
+// and must be serialised by the caller.
 //
 // The host-side address of the array is only a stand-in; the device address is
 // obtained once per device with cudaGetSymbolAddress while that device is
-// current. The first call on a device performs that set-up, so it should be
-// made before any stream capture begins.
+// current, and kept for the life of the process (a cudaDeviceReset of that
+// device is not supported afterwards). The first call on a device performs
+// that set-up, so it should be made before any stream capture begins.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -125,12 +127,39 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 using namespace tgp;
 
+static int aggregate_noalloc_on(int device, void* stream, const tgp_column_desc* cols, uint32_t ncols,
+                                uint64_t rows, const tgp_pred_node* pred, uint32_t npred,
+                                const tgp_key_domain* keys, uint32_t nkeys, const tgp_agg* aggs, uint32_t nagg,
+                                tgp_agg_value* vals_out, uint64_t vals_cap, tgp_query_result* result,
+                                char* err_msg, size_t err_cap);
+
+// Runs the aggregate with `device` current and gives the caller back the
+// device that was current before the call, whatever the outcome.
 extern "C" int tgp_aggregate_noalloc(int device, void* stream, const tgp_column_desc* cols, uint32_t ncols,
                                      uint64_t rows, const tgp_pred_node* pred, uint32_t npred,
                                      const tgp_key_domain* keys, uint32_t nkeys, const tgp_agg* aggs, uint32_t nagg,
                                      tgp_agg_value* vals_out, uint64_t vals_cap, tgp_query_result* result,
                                      char* err_msg, size_t err_cap) {
     if (err_msg && err_cap) err_msg[0] = '\0';
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+        cudaGetLastError();
+        prev = -1;
+    }
+    const int st = aggregate_noalloc_on(device, stream, cols, ncols, rows, pred, npred, keys, nkeys, aggs, nagg,
+                                        vals_out, vals_cap, result, err_msg, err_cap);
+    if (prev >= 0 && prev != device && cudaSetDevice(prev) != cudaSuccess) {
+        cudaGetLastError();
+        if (st == TGP_OK) return report(err_msg, err_cap, TGP_DEVICE_ERROR, "could not restore the caller's device");
+    }
+    return st;
+}
+
+static int aggregate_noalloc_on(int device, void* stream, const tgp_column_desc* cols, uint32_t ncols,
+                                uint64_t rows, const tgp_pred_node* pred, uint32_t npred,
+                                const tgp_key_domain* keys, uint32_t nkeys, const tgp_agg* aggs, uint32_t nagg,
+                                tgp_agg_value* vals_out, uint64_t vals_cap, tgp_query_result* result,
+                                char* err_msg, size_t err_cap) {
     if (!cols || !result || !vals_out || (nagg && !aggs) || (nkeys && !keys) || (npred && !pred))
         return report(err_msg, err_cap, TGP_INVALID_ARG, "null argument");
     if (ncols == 0 || ncols > kMaxNoAllocCols) return report(err_msg, err_cap, TGP_INVALID_ARG, "1 to 16 columns");
@@ -166,6 +195,10 @@ extern "C" int tgp_aggregate_noalloc(int device, void* stream, const tgp_column_
                 cudaGetLastError();
                 return report(err_msg, err_cap, TGP_INVALID_ARG, "columns must be device memory");
             }
+            // Another GPU's column would be read through a peer mapping (or
+            // fault without one): refuse it on the host, before any launch.
+            if (pa.type == cudaMemoryTypeDevice && pa.device != device)
+                return report(err_msg, err_cap, TGP_INVALID_ARG, "a column lives on another device");
             if (reinterpret_cast<uintptr_t>(cols[i].data) % 16 != 0)
                 return report(err_msg, err_cap, TGP_INVALID_ARG, "device columns must be 16-byte aligned");
         }
