@@ -1,9 +1,10 @@
-"""Benchmark of the hot path: the 60M-row selective scan + scalar int128 sum.
+"""Benchmark of the hot path.
 
-Workload (one step): WHERE ship_day in a 365-day window AND discount_pct
-BETWEEN 5 AND 7 AND quantity < 24 → sum(price_cents * discount_pct) as exact
-int128, plus count, over 60M seeded synthetic rows (TPC-H Q6 shape; the data
-set itself is not available, so seeded columns with its distributions stand in).
+Headline (default) workload, one step: WHERE ship_day in a 365-day window AND
+discount_pct BETWEEN 5 AND 7 AND quantity < 24 → sum(price_cents *
+discount_pct) as exact int128, plus count, over 60M seeded synthetic rows
+(TPC-H Q6 shape; the data set itself is not available, so seeded columns with
+its distributions stand in).
 
 * ``value``  — rows/s with the table resident in HBM (K calls of tgp_execute,
   CUDA events on the library's stream, max over ranks).
@@ -14,10 +15,16 @@ set itself is not available, so seeded columns with its distributions stand in).
   its CUDA-event duration, against the measured HBM copy bandwidth.
 * ``cpu_baseline`` — the C++ restatement of the reference's CPU path on this
   host's cores, on a bounded sample of the same workload.
+* ``workloads`` — at N=1, one record each for the other workloads at their
+  full sizes (filtered grouped aggregate 6M rows, join + grouped aggregate
+  60M x 1.5M rows, GROUP BY key over 100M rows, a batch of 256 uneven
+  queries), with the same keys; each record's CPU leg checks the GPU result
+  against the exact checker before its numbers are reported.
 
 ``--impl reference`` times that CPU restatement alone (rank 0) and prints its
-own line. Under torchrun, each rank scans its own 60M-row shard (weak
-scaling); per-step partial sums are merged with an NCCL all-gather.
+own line (with the same ``config``). Under torchrun, each rank scans its own
+60M-row shard (weak scaling); per-step partial sums are merged with an NCCL
+all-gather.
 """
 from __future__ import annotations
 
@@ -41,6 +48,35 @@ BYTES_PER_ROW = 20  # ship_day 4 + discount_pct 4 + quantity 4 + price_cents 8
 METRIC = "rows/s & HBM GB/s vs 8 TB/s; batched QPS at p99 vs plain per-query launch"
 SCAN_COLUMNS = ("ship_day", "discount_pct", "quantity", "price_cents")
 L2_NOTE = "inputs 1.2 GB per rank > 126 MB L2 (no flush needed)"
+DATA = "synthetic (seeded; TPC-H lineitem shapes)"
+# Full sizes of the other workloads (rows of the scanned / probed table).
+FULL_ROWS = {"filtered_group_agg": 6_000_000, "join_group_agg": 60_000_000, "highcard_group": 100_000_000}
+DIM_ROWS = 1_500_000
+
+
+def headline_config(world: int, rows: int) -> dict:
+    """The headline line's config, identical in both arms."""
+    return {"workload": "selective_scan_sum (60M-row scan, 1.81% selectivity, int128 sum)",
+            "rows_per_step": rows, "bytes_per_row": BYTES_PER_ROW, "l2": L2_NOTE,
+            "parallelism": f"row shards x{world}"}
+
+
+def workload_desc(name: str, n: int) -> str:
+    if name == "filtered_group_agg":
+        return f"filtered_group_agg ({n} rows, WHERE ship_day <= max-90, GROUP BY flag_a, flag_b, 6 aggregates)"
+    if name == "join_group_agg":
+        return (f"join_group_agg (build {DIM_ROWS} rows filtered on order_day < median, probe {n} rows, "
+                f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
+    return f"highcard_group ({n} rows, GROUP BY key Zipf(1.1) over 10M values, count + sum(value))"
+
+
+def workload_config(name: str, n: int) -> dict:
+    """A workload line's config, identical in both arms."""
+    per_row = {"filtered_group_agg": 26, "join_group_agg": 16, "highcard_group": 12}[name]
+    extra = 9 * DIM_ROWS if name == "join_group_agg" else 0
+    b = per_row * n + extra
+    return {"workload": workload_desc(name, n), "rows_per_step": n + (DIM_ROWS if name == "join_group_agg" else 0),
+            "bytes_per_step": b, "l2": "inputs larger than the 126 MB L2" if b > 126e6 else "inputs smaller than L2"}
 
 
 def peak_hbm() -> tuple[float, str]:
@@ -131,15 +167,6 @@ def gen_scan_table(rows: int, seed: int) -> dict[str, np.ndarray]:
     return out
 
 
-def cpu_baseline(cols: dict, tpl, sample_rows: int, threads: int | None) -> dict:
-    """The reference-path restatement on a bounded sample (rows/s)."""
-    import oracle
-    from oracle import refpath
-    sample = {k: v[:sample_rows] for k, v in cols.items()}
-    res = refpath.selective_scan_sum(sample, tpl, threads=threads)
-    return res
-
-
 def dist_setup(n_gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -153,13 +180,87 @@ def dist_setup(n_gpus: int):
     return world, rank, local
 
 
+# ---------------------------------------------------------------------------
+# Reference arm: the C++ restatements of the reference's CPU paths
+# ---------------------------------------------------------------------------
+def cpu_workload_runner(name: str, n: int, threads: int):
+    """(run(m) -> seconds of one pass over the first m rows, sample cap,
+    description of what is timed) for a workload's reference CPU path."""
+    from oracle import refpath
+    from turbogp_b200 import datagen, workloads
+    CT = datagen.LINEITEM_COLTYPES
+    if name == "filtered_group_agg":
+        cap = n
+        tpl = workloads.filtered_group_agg()
+        host = datagen.lineitem(cap, seed=1)
+        run = lambda m: refpath.grouped_q1({k: v[:m] for k, v in host.items()}, tpl, CT, threads=threads)["seconds"]
+        how = (f"rows of the same lineitem distributions through the C++ restatement of the reference's grouped "
+               f"path (execute_grouped: 65,536-row chunks grouped on {threads} threads, per-group i64 / f64 sums)")
+    elif name == "join_group_agg":
+        cap = min(n, 20_000_000)
+        tpl = workloads.join_group_agg()
+        dim = datagen.dimension(DIM_ROWS, seed=2)
+        fact_full = datagen.fact_fk(cap, DIM_ROWS, 0.8, seed=3)
+        fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
+        del fact_full
+        day_lt = tpl.build_where.ops[0][3]
+        run = lambda m: refpath.join_group({k: v[:m] for k, v in fact.items()}, dim, day_lt, threads=threads)["seconds"]
+        how = (f"probe rows (Zipf(0.8) fk over the 1.5M-row dimension, which is joined whole) through the C++ "
+               f"restatement of the reference's join path (hash_join_with_keys: CRC32-tagged chained table + bloom "
+               f"filter, 65,536-row probe chunks on {threads} threads, materialised join, then execute_grouped)")
+    else:
+        cap = min(n, 20_000_000)
+        host = datagen.highcard(cap, 10_000_000, 1.1, seed=4)
+        run = lambda m: refpath.highcard({k: v[:m] for k, v in host.items()}, threads=threads, cap=0)["seconds"]
+        how = (f"rows of the same Zipf(1.1) key distribution through the C++ restatement of the reference's "
+               f"accumulator grouping (try_accumulator_grouped: 65,536-row chunks into per-chunk hash maps on "
+               f"{threads} threads, merged into one map)")
+    return run, cap, how
+
+
+def time_cpu_workload(name: str, n: int, warmup: int, steps: int, budget_s: float) -> dict:
+    """Bounded-sample timing of a workload's reference CPU path: each step is
+    one pass over the first `rows` rows, sized so warmup + steps take about
+    budget_s seconds."""
+    threads = os.cpu_count() or 1
+    run, cap, how = cpu_workload_runner(name, n, threads)
+    probe = min(cap, 100_000)
+    per_row = run(probe) / probe
+    rows = int(max(min(cap, 100_000), min(cap, budget_s / (warmup + steps) / max(per_row, 1e-12))))
+    times = []
+    for i in range(warmup + steps):
+        t = run(rows)
+        if i >= warmup:
+            times.append(t)
+    sec = sum(times)
+    value = rows * len(times) / sec
+    return {"value": value, "unit": "rows/s", "cores": threads, "kind": "port", "rows": rows,
+            "ms_per_step": 1000 * sec / len(times), "sample": f"{rows} {how} per step"}
+
+
+def reference_line(args, world: int, name: str, n: int, cpu: dict, config: dict) -> dict:
+    return {
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
+        "config": config,
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cpu["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, world: int, rank: int) -> None:
+    """The reference arm: the C++ restatement of the reference's CPU path for
+    the scan (single-threaded, as the reference's interpreter runs that query),
+    each step a bounded sample of the 60M rows; at the default workload the
+    line also carries the other workloads' reference CPU paths, on all host
+    threads, as `workloads`."""
     if rank != 0:
         return
+    from oracle import refpath
     from turbogp_b200 import workloads
     tpl = workloads.selective_scan_sum()
     full = gen_scan_table(args.reference_rows, seed=1)
-    from oracle import refpath
     threads = os.cpu_count() or 1
     # Each step is a bounded sample of the workload: one timed full pass sizes
     # it so the whole --warmup + --steps run is about a minute of CPU work.
@@ -169,171 +270,107 @@ def run_reference(args, world: int, rank: int) -> None:
                    max(1_000_000, args.reference_rows * (budget_s / (args.warmup + args.steps)) / max(t_full, 1e-6))))
     cols = {k: v[:rows] for k, v in full.items()}
     times = []
+    r = None
     for i in range(args.warmup + args.steps):
         r = refpath.selective_scan_sum(cols, tpl, threads=threads)
         if i >= args.warmup:
             times.append(r["seconds"])
     sec = sum(times)
     value = rows * len(times) / sec
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic (seeded; TPC-H lineitem shapes)",
-        "config": {"workload": "selective_scan_sum (60M-row scan, 1.81% selectivity, int128 sum)",
-                   "rows_per_step": rows},
-        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": r["threads"], "kind": "port",
-                         "sample": f"first {rows} of the 60M rows per step, C++ restatement of the reference "
-                                   f"CPU path (single-threaded, as the reference runs this query)"},
-        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    cpu = {"value": value, "unit": "rows/s", "cores": r["threads"], "kind": "port",
+           "ms_per_step": 1000 * sec / len(times),
+           "sample": f"first {rows} of the {args.reference_rows} rows per step, C++ restatement of the reference "
+                     f"CPU path (single-threaded, as the reference runs this query)"}
+    line = reference_line(args, world, "selective_scan_sum", args.reference_rows, cpu,
+                          headline_config(world, args.reference_rows))
+    if not args.no_workloads and args.reference_rows == ROWS:
+        recs = {}
+        for name, n in FULL_ROWS.items():
+            c = time_cpu_workload(name, n, 1, 3, budget_s=12.0)
+            recs[name] = {"value": c["value"], "unit": "rows/s", "ms_per_step": c["ms_per_step"],
+                          "config": workload_config(name, n),
+                          "cpu_baseline": {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                          "e2e": {"value": c["value"], "unit": "rows/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}
+        recs["batch"] = {"unavailable": "the reference has no batched-submission CPU path (its interpreter runs "
+                                        "one statement at a time)"}
+        line["workloads"] = recs
     print(json.dumps(line), flush=True)
 
 
 def run_reference_workload(args, world: int, rank: int) -> None:
-    """Reference arm of the grouped / join / high-cardinality workloads: the
-    C++ restatements of the reference's own CPU paths for them
-    (oracle/ref_path.cpp) on all host threads, each step one pass over a
-    bounded sample of the workload's rows, sized so the whole run is about a
-    minute of CPU work.
-    The batch and serving workloads have no CPU counterpart in the reference
-    (its server runs one statement at a time), so they print the unavailable
-    line. Under torchrun rank 0 alone runs."""
+    """Reference arm of one grouped / join / high-cardinality workload (rank 0
+    alone). The batch and serving workloads have no CPU counterpart in the
+    reference (its server runs one statement at a time): they print the
+    unavailable line."""
     if rank != 0:
         return
     name = args.workload
-    if name in ("batch", "serve"):
+    if name in ("batch", "serve", "pgwire"):
         print(json.dumps({"impl": "reference", "unavailable": f"{name}: the reference has no batched-submission "
                           "or serving CPU path to time (the plain one-query-at-a-time arm is in this "
                           "workload's own line)"}), flush=True)
         return
-    from oracle import refpath
-    from turbogp_b200 import datagen, workloads
-    CT = datagen.LINEITEM_COLTYPES
-    cap = 2_000_000
-    threads = os.cpu_count() or 1
-    if name == "filtered_group_agg":
-        n = args.rows if args.rows != ROWS else 6_000_000
-        tpl = workloads.filtered_group_agg()
-        cap = n
-        host = datagen.lineitem(n, seed=1)
-        run = lambda m: refpath.grouped_q1({k: v[:m] for k, v in host.items()}, tpl, CT, threads=threads)
-        desc = f"filtered_group_agg ({n} rows, WHERE ship_day <= max-90, GROUP BY flag_a, flag_b, 6 aggregates)"
-        what = "rows of the same lineitem distributions"
-        how = (f"the C++ restatement of the reference's grouped path (execute_grouped: 65,536-row chunks "
-               f"grouped on {threads} threads, per-group i64 / f64 sums)")
-        cores = threads
-    elif name == "join_group_agg":
-        n = args.rows if args.rows != ROWS else 60_000_000
-        nb = 1_500_000
-        tpl = workloads.join_group_agg()
-        dim = datagen.dimension(nb, seed=2)
-        cap = min(n, 20_000_000)
-        fact_full = datagen.fact_fk(cap, nb, 0.8, seed=3)
-        fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
-        day_lt = tpl.build_where.ops[0][3]
-        run = lambda m: refpath.join_group({k: v[:m] for k, v in fact.items()}, dim, day_lt, threads=threads)
-        how = (f"the C++ restatement of the reference's join path (hash_join_with_keys: CRC32-tagged chained "
-               f"table + bloom filter, 65,536-row probe chunks on {threads} threads, materialised join, then "
-               f"execute_grouped)")
-        cores = threads
-        desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
-                f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
-        what = "probe rows (Zipf(0.8) fk over the 1.5M-row dimension, which is joined whole)"
-    else:
-        n = args.rows if args.rows != ROWS else 100_000_000
-        cap = min(n, 20_000_000)
-        host = datagen.highcard(cap, 10_000_000, 1.1, seed=4)
-        run = lambda m: refpath.highcard({k: v[:m] for k, v in host.items()}, threads=threads, cap=0)
-        desc = f"highcard_group ({n} rows, GROUP BY key Zipf(1.1) over 10M values, count + sum(value))"
-        what = "rows of the same Zipf(1.1) key distribution"
-        how = (f"the C++ restatement of the reference's accumulator grouping (try_accumulator_grouped: "
-               f"65,536-row chunks into per-chunk hash maps on {threads} threads, merged into one map)")
-        cores = threads
-    def timed(m: int) -> float:
-        """Seconds of one pass over m rows: the restated paths report their
-        own query time (the cells are laid out before it starts); the oracle
-        is timed around the call."""
-        t0 = time.perf_counter()
-        r = run(m)
-        return float(r["seconds"]) if isinstance(r, dict) else time.perf_counter() - t0
-
-    rows = min(n, cap)
-    per_row = timed(min(rows, 100_000)) / min(rows, 100_000)
-    rows = int(max(100_000, min(rows, 60.0 / (args.warmup + args.steps) / max(per_row, 1e-12))))
-    times = []
-    for i in range(args.warmup + args.steps):
-        t = timed(rows)
-        if i >= args.warmup:
-            times.append(t)
-    sec = sum(times)
-    value = rows * len(times) / sec
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic (seeded; TPC-H shapes)",
-        "config": {"workload": desc, "rows_per_step": rows},
-        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cores, "kind": "port",
-                         "sample": f"{rows} {what} per step through {how}"},
-        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+    n = args.rows if args.rows != ROWS else FULL_ROWS[name]
+    cpu = time_cpu_workload(name, n, args.warmup, args.steps, budget_s=60.0)
+    print(json.dumps(reference_line(args, world, name, n, cpu, workload_config(name, n))), flush=True)
 
 
-def run_workload(args, world: int, rank: int, local: int) -> None:
-    """The other hot-path workloads, one JSON line each (same keys as the default line).
+# ---------------------------------------------------------------------------
+# The GPU arm of the grouped / join / high-cardinality / batch workloads
+# ---------------------------------------------------------------------------
+def same_output(a, b) -> bool:
+    if a.rows_selected != b.rows_selected or a.keys != b.keys or len(a.values) != len(b.values):
+        return False
+    for ra, rb in zip(a.values, b.values):
+        for x, y in zip(ra, rb):
+            if x.count != y.count or x.value != y.value:
+                return False
+            if not (x.as_f64 == y.as_f64 or abs(x.as_f64 - y.as_f64) <= 1e-12 * abs(y.as_f64)):
+                return False
+    return True
 
-    filtered_group_agg: 6M rows, WHERE ship_day <= max - 90, GROUP BY (flag_a, flag_b),
-      count + 4 int128 sums + avg (26 B/row).
-    join_group_agg: dimension 1.5M rows filtered on order_day, fact 60M rows with a
-      Zipf(0.8) foreign key; each step builds the join table and runs the fused
-      probe + GROUP BY segment aggregate (build 9 B/row, probe 16 B/row).
-    highcard_group: 100M rows, GROUP BY key (Zipf(1.1) over 10M values), count +
-      sum(value) through the global group hash table (12 B/row).
-    Under torchrun every rank runs an independent replica on its own data.
-    """
+
+def result_summary(out, limit: int = 6) -> list:
+    """The first groups of a result as [key..., value...] lists (JSON-safe)."""
+    rows = []
+    for k, vals in list(zip(out.keys, out.values))[:limit]:
+        rows.append([*k, *[str(v.value) for v in vals]])
+    return rows
+
+
+def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, shared: dict | None = None) -> dict:
+    """One workload at full size: timed steps (device events), the dominant
+    kernel's gated launch time (roofline), the end-to-end step from pinned
+    host buffers, and the CPU leg (reference CPU path on a bounded sample, and
+    the exact check of the GPU's first result). Returns the record."""
     import torch
-    import oracle
     from turbogp_b200 import datagen, workloads
-    from turbogp_b200.engine import Context, col, count_star, sum_
-
-    name = args.workload
-    ctx = Context(local)
+    from turbogp_b200.engine import col, count_star, sum_
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     CT = datagen.LINEITEM_COLTYPES
+    shared = shared if shared is not None else {}
     probe_only = None  # (callable, algorithmic bytes per launch) when the step has several kernels
-    traffic = None     # ncu DRAM bytes per launch of the dominant kernel, where a summary is committed
     variant = None     # (description, callable): the same query with ORDER BY ... LIMIT, timed beside it
+    n = args.rows if (args.rows != ROWS and args.workload == name) else FULL_ROWS[name]
     if name == "filtered_group_agg":
-        n = args.rows if args.rows != ROWS else 6_000_000
         tpl = workloads.filtered_group_agg()
         host = datagen.lineitem(n, seed=1 + rank)
         t = ctx.register(host, CT)
         q = t.prepare(tpl.aggs, tpl.group_by, tpl.where)
         step = q.run
-        n_keys, n_aggs = len(tpl.group_by), len(tpl.aggs)
         tables = [(t, host)]
-        rows_step, bytes_step, kernel_bytes = n, 26 * n, 26 * n
-        dominant = "scan_kernel<MODE_GROUP_PRIVATE> (6 direct groups, 4 int128 values)"
-        desc = f"filtered_group_agg ({n} rows, WHERE ship_day <= max-90, GROUP BY flag_a, flag_b, 6 aggregates)"
-        # CPU baseline: the reference's grouped path restated (chunked
-        # grouping on all host threads, then per-group sums), whole table.
-        from oracle import refpath
-        cpu_threads = os.cpu_count() or 1
-        cpu_run = lambda: refpath.grouped_q1(host, tpl, CT, threads=cpu_threads)["seconds"]
-        cpu_rows = n
-        cpu_desc = (f"all {n} rows, C++ restatement of the reference's grouped path (execute_grouped: "
-                    f"65,536-row chunks grouped on {cpu_threads} threads, per-group i64 / f64 sums)")
+        kernel_bytes = 26 * n
+        dominant = "scan_kernel<MODE_GROUP_PRIVATE, int64, DenseShape<Q1>> (6 direct groups)"
         traffic = traffic_per_launch("filtered_group_agg_6M_scan_kernel.md", n)
+        check = lambda out: _check_exact(out, host, CT, tpl.aggs, tpl.group_by, tpl.where)
+        cleanup = [t.drop]
     elif name == "join_group_agg":
-        n = args.rows if args.rows != ROWS else 60_000_000
-        nb = 1_500_000
         tpl = workloads.join_group_agg()
-        dim = datagen.dimension(nb, seed=2 + rank)
-        fact_full = datagen.fact_fk(n, nb, 0.8, seed=3 + rank)
-        fact = {k: fact_full[k] for k in ("fk", "price_cents", "discount_pct")}
-        del fact_full
+        dim = datagen.dimension(DIM_ROWS, seed=2 + rank)
+        fact_full = shared.get("fact") if shared.get("fact") is not None and rank == 0 else \
+            datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
+        fact = {k: np.ascontiguousarray(fact_full[k][:n]) for k in ("fk", "price_cents", "discount_pct")}
         fct = {"fk": "int", "price_cents": "int", "discount_pct": "int"}
         d = ctx.register(dim, datagen.DIMENSION_COLTYPES)
         f = ctx.register(fact, fct)
@@ -346,53 +383,31 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
 
         j0 = d.join_build("key", tpl.build_where)
         pq = f.prepare(tpl.aggs, tpl.group_by, tpl.where, join=j0, probe_key="fk")
-        q, n_keys, n_aggs = pq, len(tpl.group_by), len(tpl.aggs)
+        q = pq
         probe_only = (pq.run, 16 * n)
         tables = [(d, dim), (f, fact)]
-        rows_step, bytes_step, kernel_bytes = n + nb, 16 * n + 9 * nb, 16 * n
-        dominant = "scan_kernel probe + join + GROUP BY segment (25 groups, int128)"
-        desc = (f"join_group_agg (build {nb} rows filtered on order_day < median, probe {n} rows, "
-                f"Zipf(0.8) fk, GROUP BY segment, sum(price*(100-disc)) + count)")
+        kernel_bytes = 16 * n
+        dominant = "scan_kernel join probe + GROUP BY segment (25 groups, payload array)"
         traffic = traffic_per_launch("join_group_agg_probe_kernel.md", n)
-        # CPU baseline: the reference's join path restated (filtered build
-        # side, tagged chained table + bloom filter, parallel chunked probe,
-        # materialised join, then the grouped aggregate) on all host threads.
-        from oracle import refpath
-        cs = min(n, 20_000_000)
-        cpu_fact = {k: v[:cs] for k, v in fact.items()}
-        cpu_threads = os.cpu_count() or 1
-        day_lt = tpl.build_where.ops[0][3]
-        cpu_run = lambda: refpath.join_group(cpu_fact, dim, day_lt, threads=cpu_threads)["seconds"]
-        cpu_rows = cs
-        cpu_desc = (f"first {cs} probe rows, C++ restatement of the reference's join path (hash_join_with_keys: "
-                    f"CRC32-tagged chained table + bloom filter, 65,536-row probe chunks on {cpu_threads} "
-                    f"threads, materialised join, then execute_grouped)")
+        build = (dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where)
+        check = lambda out: _check_exact(out, fact, fct, tpl.aggs, tpl.group_by, tpl.where, build, "fk")
+        cleanup = [j0.drop, f.drop, d.drop]
     else:  # highcard_group
-        n = args.rows if args.rows != ROWS else 100_000_000
         host = datagen.highcard(n, 10_000_000, 1.1, seed=4 + rank)
         t = ctx.register(host)
         aggs = [count_star(), sum_(col("value"))]
         q = t.prepare(aggs, ("key",), None, group_cap=10_000_000)
         step = lambda: q.run(decode=False)
-        n_keys, n_aggs = 1, len(aggs)
         variant = ("ORDER BY count(*) DESC LIMIT 10 (tgp_execute_topn)",
                    lambda: t.aggregate_topn(aggs, ("key",), None, 0, True, 10))
         tables = [(t, host)]
-        rows_step, bytes_step, kernel_bytes = n, 12 * n, 12 * n
+        kernel_bytes = 12 * n
         dominant = "scan_kernel<MODE_GROUP_HASH> (global open-addressing group table)"
-        desc = f"highcard_group ({n} rows, GROUP BY key Zipf(1.1) over 10M values, count + sum(value))"
-        # CPU baseline: the reference's accumulator grouping restated, on all
-        # host threads, over the first 20M rows.
-        from oracle import refpath
-        cs = min(n, 20_000_000)
-        cpu_threads = os.cpu_count() or 1
-        cpu_sample = {k: v[:cs] for k, v in host.items()}
-        cpu_run = lambda: refpath.highcard(cpu_sample, threads=cpu_threads, cap=0)["seconds"]
-        cpu_rows = cs
-        cpu_desc = (f"first {cs} rows, C++ restatement of the reference's accumulator grouping "
-                    f"(try_accumulator_grouped: 65,536-row chunks into per-chunk hash maps on {cpu_threads} "
-                    f"threads, merged into one map)")
+        traffic = traffic_per_launch("highcard_group_hash_kernel.md", n)
+        check = lambda out: _check_highcard(q, host)
+        cleanup = [t.drop]
 
+    first = step() if name != "highcard_group" else q.run()
     for _ in range(args.warmup):
         step()
     steps = args.steps if args.steps != 3000 else 20
@@ -407,13 +422,11 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
             step()
         ev1.record(stream)
         ev1.synchronize()
-    launches, kernel_total = ctx.profile_read()
+    launches, _ = ctx.profile_read()
     ms = ev0.elapsed_time(ev1)
-    # Kernel time alone: the launch queued behind a short device delay.
+    # Kernel time alone: each launch queued behind a short device delay.
     ctx.profile(True, gated=True)
     run_one = probe_only[0] if probe_only is not None else step
-    if probe_only is not None:
-        kernel_bytes = probe_only[1]
     for _ in range(3):
         run_one()
     ctx.profile_read()
@@ -436,10 +449,10 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    # Bytes the step reads back: the group keys (8 B each) and one 32-byte
-    # value record per aggregate and group, plus the result block's counters.
-    ngroups = len(out.keys) if out.keys else int(q.res.ngroups)
-    d2h = ngroups * (8 * n_keys + 32 * n_aggs) + 48
+    ngroups = int(q.res.ngroups)
+    nk, na = q.nk, q.na
+    d2h = ngroups * (8 * nk + 32 * na) + 48   # keys, one 32-byte value record per aggregate, counters
+    del pinned
 
     variant_line = None
     if variant is not None:
@@ -453,37 +466,59 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         v1.synchronize()
         variant_line = {"query": variant[0], "ms_per_step": v0.elapsed_time(v1) / steps}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t0 = time.perf_counter()
-        sec = cpu_run()
-        if not isinstance(sec, float):   # the oracle returns results, not its time
-            sec = time.perf_counter() - t0
-        cpu = {"value": cpu_rows / sec, "unit": "rows/s", "cores": cpu_threads, "kind": "port",
-               "sample": cpu_desc}
+    # CPU leg (rank 0 at N=1): the exact check of the first result, then the
+    # reference's CPU path on a bounded sample.
+    cpu, checked = None, None
+    if rank == 0 and world == 1:
+        checked = check(first)
+        if not checked["ok"]:
+            raise SystemExit(f"{name}: GPU result differs from the exact checker: {checked}")
+        if not args.no_cpu_baseline:
+            c = time_cpu_workload(name, n, 1, 2, budget_s=8.0)
+            cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    for fn in cleanup:
+        fn()
+    rows_step = n + (DIM_ROWS if name == "join_group_agg" else 0)
+    bytes_step = workload_config(name, n)["bytes_per_step"]
     peak, peak_kind = peak_hbm()
     achieved = kernel_bytes / (kernel_avg / 1000.0) / 1e9
-    line = {
+    rec = {
         "metric": METRIC, "value": rows_step * world * steps / (ms / 1000.0), "unit": "rows/s", "n_gpus": world,
         "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H shapes)",
-        "config": {"workload": desc, "rows_per_step": rows_step, "bytes_per_step": bytes_step,
-                   "l2": "inputs larger than the 126 MB L2" if bytes_step > 126e6 else "inputs smaller than L2"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
+        "config": workload_config(name, n),
         "hbm_gbs": bytes_step * world * steps / (ms / 1000.0) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": traffic, "kernel_ms": kernel_avg, "kernel": dominant},
+                     "peak_kind": peak_kind, "traffic": traffic, "kernel_ms": kernel_avg, "kernel": dominant,
+                     "timing": "device events around each launch, launch queued behind a device delay"},
         "e2e": {"value": rows_step * e2e_steps / (e2e_ms / 1000.0), "unit": "rows/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+        "result": checked,
     }
     if variant_line is not None:
-        line["variant"] = variant_line
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+        rec["variant"] = variant_line
+    return rec
+
+
+def _check_exact(out, cols, coltypes, aggs, group_by, where, build=None, probe_key=None) -> dict:
+    """The GPU result against the exact numpy checker (oracle/scale.py)."""
+    from oracle import scale
+    exp = scale.aggregate(cols, coltypes, aggs, group_by, where, build=build, probe_key=probe_key)
+    return {"ok": same_output(out, exp), "checker": "oracle.scale.aggregate (exact)", "groups": len(out.keys),
+            "rows_selected": out.rows_selected, "first_groups": result_summary(out)}
+
+
+def _check_highcard(q, host) -> dict:
+    """Every group of the GROUP BY key result against numpy bincounts."""
+    from oracle import scale
+    keys, lo, hi, cnt = q._output(q.res).arrays()
+    ek, ec, es = scale.group_count_sum(host["key"], host["value"])
+    ok = (keys.shape[0] == ek.shape[0] and np.array_equal(keys[:, 0], ek) and
+          np.array_equal(lo[:, 0].view(np.int64), ec) and np.array_equal(lo[:, 1].view(np.int64), es) and
+          not hi.any())
+    return {"ok": bool(ok), "checker": "oracle.scale.group_count_sum (exact bincounts)", "groups": int(keys.shape[0]),
+            "rows_selected": int(q.res.rows_selected)}
 
 
 def batch_queries(ctx, fact_dev: dict, dim_host: dict, nq: int, seed: int):
@@ -526,23 +561,21 @@ def batch_queries(ctx, fact_dev: dict, dim_host: dict, nq: int, seed: int):
     return pqs, rows, nbytes, (d, j, views)
 
 
-def run_batch(args, world: int, rank: int, local: int) -> None:
+def measure_batch(ctx, args, world: int, rank: int, local: int, fact_host: dict | None = None) -> dict:
     """Batching: 256 queries of uneven sizes (see batch_queries) per step, run
     as one tgp_batch_submit (persistent launch over a device morsel queue)
     against the same 256 queries issued one by one (plan, launch, readback
-    per query). value = batched queries/s; plain_qps beside it."""
-    import numpy as np
+    per query). value = batched queries/s; plain_qps beside it. The CPU leg
+    checks every batched result against the same query run alone, and the
+    smallest and largest query of each template against the exact checker."""
     import torch
-    from turbogp_b200 import datagen
-    from turbogp_b200.engine import Context
+    from turbogp_b200 import datagen, workloads
     nq = 256
-    ctx = Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    n = args.rows if args.rows != ROWS else 60_000_000
-    host = datagen.fact_fk(n, 1_500_000, 0.8, seed=3 + rank)
-    fact = {k: torch.from_numpy(v).to(f"cuda:{local}") for k, v in host.items()}
-    del host
-    dim = datagen.dimension(1_500_000, seed=2 + rank)
+    n = args.rows if (args.rows != ROWS and args.workload == "batch") else 60_000_000
+    host = fact_host if fact_host is not None and rank == 0 else datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
+    fact = {k: torch.from_numpy(v[:n]).to(f"cuda:{local}") for k, v in host.items()}
+    dim = datagen.dimension(DIM_ROWS, seed=2 + rank)
     pqs, rows, nbytes, keep = batch_queries(ctx, fact, dim, nq, seed=11 + rank)
     total_rows = sum(rows)
     steps = args.steps if args.steps != 3000 else 5
@@ -557,25 +590,63 @@ def run_batch(args, world: int, rank: int, local: int) -> None:
         e1.synchronize()
         return e0.elapsed_time(e1)
 
+    first_batched = ctx.submit(pqs).wait()
+    first_plain = [q.run() for q in pqs]
     batch = lambda: ctx.submit(pqs, decode=False).wait()
     plain = lambda: [q.run(decode=False) for q in pqs]
     for _ in range(args.warmup):
         batch()
-        plain()
+    plain()
     ctx.profile(True)
     ctx.profile_read()
     with ClockSampler(local) as clocks:
         ms_batch = timed(batch, steps)
     launches, kern_ms = ctx.profile_read()
-    ms_plain = timed(plain, max(1, steps // 2)) / max(1, steps // 2) * steps
+    k_plain = max(1, steps // 2)
+    ms_plain = timed(plain, k_plain) / k_plain * steps
     ctx.profile(False)
+    # e2e: results read back into host buffers by every query of the batch
+    # (the tables stay resident, as they do for a served query).
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.submit(pqs, decode=True).wait()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    d2h = sum(int(q.res.ngroups) * (8 * q.nk + 32 * q.na) + 48 for q in pqs)
+    checked = None
+    if rank == 0 and world == 1:
+        from oracle import scale
+        same = all(same_output(b, p) for b, p in zip(first_batched, first_plain))
+        tj = workloads.join_group_agg()
+        build = (dim, datagen.DIMENSION_COLTYPES, "key", tj.build_where)
+        fct = {**datagen.LINEITEM_COLTYPES, "fk": "int"}
+        picked = {}
+        for i, pq in enumerate(pqs):
+            shape = (pq.nk, pq.na, int(pq.q.join != 0))
+            lo, hi = picked.get(shape, (i, i))
+            picked[shape] = (lo if rows[lo] <= rows[i] else i, hi if rows[hi] >= rows[i] else i)
+        exact = True
+        sample = sorted({i for pair in picked.values() for i in pair})
+        for i in sample:
+            sp = pqs[i].spec
+            view = {k: v[:rows[i]] for k, v in host.items()}
+            e = scale.aggregate(view, fct, sp["aggs"], sp["group_by"], sp["where"],
+                                build=build if sp["join"] is not None else None,
+                                probe_key="fk" if sp["join"] is not None else None)
+            exact = exact and same_output(first_batched[i], e)
+        checked = {"ok": bool(same and exact), "checker": "every batched result == the query run alone; "
+                   f"{len(sample)} of them (smallest and largest of each template) == oracle.scale.aggregate",
+                   "queries": nq}
+        if not checked["ok"]:
+            raise SystemExit(f"batch: results differ: {checked}")
     peak, peak_kind = peak_hbm()
     achieved = sum(nbytes) / (kern_ms / steps / 1000.0) / 1e9 if kern_ms else None
-    line = {
+    rec = {
         "metric": METRIC, "value": nq * world * steps / (ms_batch / 1000.0), "unit": "queries/s",
         "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms_batch / steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic (seeded; TPC-H shapes)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
         "config": {"workload": f"batch of {nq} queries (sizes log-uniform 10K-60M rows over prefix views of a "
                                f"{n}-row resident table; selective scan+sum / filtered grouped aggregate / "
                                f"join+grouped aggregate with random literals) per step",
@@ -583,15 +654,36 @@ def run_batch(args, world: int, rank: int, local: int) -> None:
         "plain_qps": nq * steps / (ms_plain / 1000.0), "ms_plain_per_step": ms_plain / steps,
         "rows_per_s": total_rows * steps / (ms_batch / 1000.0),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None,
-                     "peak_kind": peak_kind, "traffic": None, "kernel_ms_per_step": kern_ms / steps,
-                     "kernel": "batch_kernel (persistent, device morsel queue)"},
-        "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": launches,
+                     "frac": achieved / peak if achieved else None, "peak_kind": peak_kind, "traffic": None,
+                     "kernel_ms_per_step": kern_ms / steps, "kernel": "batch_kernel (persistent, device morsel queue)",
+                     "timing": "summed device events around the batch's launches"},
+        "e2e": {"value": nq * steps / (e2e_ms / 1000.0), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h,
+                "note": "tables resident in HBM (served-query setting); every result decoded on the host"},
+        "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": launches, "result": checked,
     }
+    d, j, views = keep
+    j.drop()
+    for v in views.values():
+        v.drop()
+    d.drop()
+    return rec
+
+
+def run_workload(args, world: int, rank: int, local: int) -> None:
+    """One JSON line for one non-headline workload (--workload NAME)."""
+    from turbogp_b200.engine import Context
+    ctx = Context(local)
+    if args.workload == "batch":
+        rec = measure_batch(ctx, args, world, rank, local)
+    else:
+        rec = measure_workload(args.workload, ctx, args, world, rank, local)
     if rank == 0:
-        print(json.dumps(line), flush=True)
-    del keep
+        print(json.dumps(rec), flush=True)
     ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def run_serve(args, world: int, rank: int, local: int) -> None:
@@ -603,15 +695,14 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     memory-budget admission) and by plain one-at-a-time execution. value =
     batched completions/s at the offered rate; p50/p99 of both in the line."""
     import numpy as np
-    import torch
     from turbogp_b200 import datagen, serving, workloads
     from turbogp_b200.engine import Context, col, count_star, sum_
     ctx = Context(local)
     n = args.rows if args.rows != ROWS else 60_000_000
-    host = datagen.fact_fk(n, 1_500_000, 0.8, seed=3 + rank)
+    host = datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
     f = ctx.register(host, {**datagen.LINEITEM_COLTYPES, "fk": "int"})
     del host
-    d = ctx.register(datagen.dimension(1_500_000, seed=2 + rank), datagen.DIMENSION_COLTYPES)
+    d = ctx.register(datagen.dimension(DIM_ROWS, seed=2 + rank), datagen.DIMENSION_COLTYPES)
     tj = workloads.join_group_agg()
     j = d.join_build("key", tj.build_where)
     # The high-cardinality table lives on a second context (its own stream):
@@ -620,14 +711,12 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     hc = ctx_heavy.register(datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank))
     t_scan, t_fga = workloads.selective_scan_sum(), workloads.filtered_group_agg()
     hc_aggs = [count_star(), sum_(col("value"))]
-    gb = 1 << 30
     templates = {
-        "scan": serving.Template("scan", lambda: f.prepare(t_scan.aggs, t_scan.group_by, t_scan.where), 1 << 16),
-        "fga": serving.Template("fga", lambda: f.prepare(t_fga.aggs, t_fga.group_by, t_fga.where), 1 << 16),
-        "join": serving.Template("join", lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk"),
-                                 1 << 16),
-        "highcard": serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None),
-                                     2 * gb, heavy=True),
+        "scan": serving.Template("scan", lambda: f.prepare(t_scan.aggs, t_scan.group_by, t_scan.where)),
+        "fga": serving.Template("fga", lambda: f.prepare(t_fga.aggs, t_fga.group_by, t_fga.where)),
+        "join": serving.Template("join", lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk")),
+        "highcard": serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None, group_cap=10_000_000),
+                                     heavy=True),
     }
     rng = np.random.default_rng(21 + rank)
     D0, ND = datagen.DAY0, datagen.NDAYS
@@ -659,11 +748,10 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     with ClockSampler(local) as clocks:
         batched = serving.serve_batched(ctx, templates, stream(rate, count), mem_budget=args.mem_budget)
     plain = serving.serve_plain(ctx, templates, stream(rate, count))
-    peak, peak_kind = peak_hbm()
     line = {
         "metric": METRIC, "value": batched.get("qps"), "unit": "queries/s", "n_gpus": world,
         "steps": count, "warmup": 64, "ms_per_step": batched.get("mean_ms"), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H shapes)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
         "config": {"workload": f"serving: Poisson arrivals at {rate:g} q/s of scan+sum / filtered grouped "
                                f"aggregate / join+grouped aggregate over a resident {n}-row fact table (random "
                                f"literals) and GROUP BY key over a {args.highcard_rows}-row high-cardinality table "
@@ -682,47 +770,10 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     ctx.close()
 
 
-def main() -> None:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3000)
-    ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--rows", type=int, default=ROWS)
-    ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--reference-rows", type=int, default=ROWS)
-    ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="selective_scan_sum",
-                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
-                             "serve"])
-    ap.add_argument("--rate", type=float, default=2000.0, help="serve: offered queries/s")
-    ap.add_argument("--requests", type=int, default=4000, help="serve: requests in the timed stream")
-    ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
-    ap.add_argument("--highcard-rows", type=int, default=100_000_000)
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-
-    world, rank, local = dist_setup(args.gpus)
-    if args.impl == "reference":
-        if args.workload == "selective_scan_sum":
-            run_reference(args, world, rank)
-        else:
-            run_reference_workload(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
-    if args.workload == "batch":
-        run_batch(args, world, rank, local)
-        return
-    if args.workload == "serve":
-        run_serve(args, world, rank, local)
-        return
-    if args.workload != "selective_scan_sum":
-        run_workload(args, world, rank, local)
-        return
-
+# ---------------------------------------------------------------------------
+# Headline: the 60M-row selective scan
+# ---------------------------------------------------------------------------
+def run_headline(args, world: int, rank: int, local: int) -> None:
     import torch
     from turbogp_b200 import workloads
     from turbogp_b200.engine import Context
@@ -768,6 +819,7 @@ def main() -> None:
         return float(t.item())
 
     query = table.prepare(tpl.aggs, tpl.group_by, tpl.where)
+    first = query.run()
     # Warm-up.
     for _ in range(args.warmup):
         out = query.run()
@@ -818,7 +870,6 @@ def main() -> None:
     table.reload(pinned_np)
     barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
@@ -832,27 +883,30 @@ def main() -> None:
     e2e_value = rows * world * args.e2e_steps / (e2e_ms / 1000.0)
     if got != expect:
         raise SystemExit("e2e result differs")
+    del pinned, pinned_np
 
-    # ---- CPU baseline (rank 0, N=1 only) -----------------------------------
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import refpath
-        sample = min(args.cpu_sample_rows, rows)
-        r = refpath.selective_scan_sum({k: v[:sample] for k, v in host.items()}, tpl,
-                                       threads=os.cpu_count() or 1)
-        cpu = {"value": sample / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
-               "sample": f"first {sample} rows of the same table, one pass, C++ restatement of the "
-                         f"reference CPU path (AVX-512 filters into bitmaps, set-bit collect, f64 sum)"}
+    # ---- CPU leg (rank 0, N=1 only): exact check + reference CPU path ------
+    cpu, checked = None, None
+    if rank == 0 and world == 1:
+        checked = _check_exact(first, host, coltypes, tpl.aggs, (), tpl.where)
+        if not checked["ok"]:
+            raise SystemExit(f"selective_scan_sum: GPU result differs from the exact checker: {checked}")
+        if not args.no_cpu_baseline:
+            from oracle import refpath
+            sample = min(args.cpu_sample_rows, rows)
+            r = refpath.selective_scan_sum({k: v[:sample] for k, v in host.items()}, tpl,
+                                           threads=os.cpu_count() or 1)
+            cpu = {"value": sample / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                   "sample": f"first {sample} rows of the same table, one pass, C++ restatement of the "
+                             f"reference CPU path (AVX-512 filters into bitmaps, set-bit collect, f64 sum)"}
 
     peak, peak_kind = peak_hbm()
     achieved = rows * BYTES_PER_ROW / (kernel_avg_ms / 1000.0) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded; TPC-H lineitem shapes)",
-        "config": {"workload": "selective_scan_sum (60M-row scan, 1.81% selectivity, int128 sum)",
-                   "rows_per_rank": rows, "bytes_per_row": BYTES_PER_ROW, "l2": L2_NOTE,
-                   "parallelism": f"row shards x{world}"},
+        "vs_baseline": None, "dtype": "int64", "data": DATA,
+        "config": headline_config(world, rows),
         "hbm_gbs": rows * world * BYTES_PER_ROW * args.steps / (ms / 1000.0) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_per_launch(),
@@ -863,15 +917,68 @@ def main() -> None:
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
-        "result": {"sum": str(expect[0]), "count": expect[1]},
+        "result": {"sum": str(expect[0]), "count": expect[1], **({"check": checked} if checked else {})},
     }
+    table.drop()
+    del host
+    # The other workloads at full size (N=1 only: under torchrun the line
+    # stays the headline's weak-scaling measurement).
+    if world == 1 and not args.no_workloads and rows == ROWS:
+        from turbogp_b200 import datagen
+        recs = {}
+        fact = datagen.fact_fk(60_000_000, DIM_ROWS, 0.8, seed=3)
+        shared = {"fact": fact}
+        for name in ("filtered_group_agg", "join_group_agg", "highcard_group"):
+            recs[name] = measure_workload(name, ctx, args, world, rank, local, shared)
+        recs["batch"] = measure_batch(ctx, args, world, rank, local, fact_host=fact)
+        line["workloads"] = recs
     if rank == 0:
         print(json.dumps(line), flush=True)
-    table.drop()
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--reference-rows", type=int, default=ROWS)
+    ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="headline line only (no `workloads` records)")
+    ap.add_argument("--workload", default="selective_scan_sum",
+                    choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
+                             "serve"])
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: offered queries/s")
+    ap.add_argument("--requests", type=int, default=4000, help="serve: requests in the timed stream")
+    ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
+    ap.add_argument("--highcard-rows", type=int, default=100_000_000)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        if args.workload == "selective_scan_sum":
+            run_reference(args, world, rank)
+        else:
+            run_reference_workload(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.workload == "serve":
+        run_serve(args, world, rank, local)
+        return
+    if args.workload != "selective_scan_sum":
+        run_workload(args, world, rank, local)
+        return
+    run_headline(args, world, rank, local)
 
 
 if __name__ == "__main__":

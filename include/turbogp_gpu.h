@@ -453,6 +453,16 @@ TGP_API int tgp_execute(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
 TGP_API int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_agg, int descending, uint64_t limit,
                              uint64_t* keys_out, tgp_agg_value* vals_out, tgp_query_result* result);
 
+/* Device memory one tgp_execute of `q` holds while it runs, as its plan sizes
+ * it: the result block, the group hash table with the gather and sort
+ * buffers of its result (hash grouping), and a join payload array still to
+ * be built; the resident tables and the join table are not counted. This is
+ * the estimate that a per-query memory budget is compared against — the
+ * reference's `MEMORY BUDGET <bytes>` statement extension
+ * (src/sql/extensions.rs:13,58,155) — and what the serving loop admits
+ * requests by. Plans only: launches nothing, allocates nothing. */
+TGP_API int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes);
+
 /* COUNT(DISTINCT column) over the rows passing `pred` (all rows when npred =
  * 0), as the reference evaluates it (aggregate.rs:1301-1325,
  * src/exec/hll.rs): with fewer than 100,000 selected rows the exact number of

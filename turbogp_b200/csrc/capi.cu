@@ -1385,6 +1385,7 @@ struct QueryState {
     uint64_t ngroups_direct = 1;
     size_t extra = 0;     // per-mode shared scratch bytes
     uint64_t hcap = 0;    // hash table slots (MODE_GROUP_HASH)
+    uint64_t pending_dev_bytes = 0;  // device memory a dry plan would still allocate (join payload)
     uint64_t acc_words() const { return mode == MODE_GROUP_HASH ? 0 : ngroups_direct * nv1 * 2; }
     uint64_t block_words() const { return 6 + acc_words(); }  // [counters 4][error 2][accumulators]
     bool has_minmax() const {
@@ -1399,7 +1400,7 @@ struct QueryState {
 // `preseed` (optional) lists columns to stage first, in that order.
 // Result pointers (counters, err, acc, htab) are left for the caller.
 static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem,
-                      const std::vector<uint32_t>* preseed = nullptr) {
+                      const std::vector<uint32_t>* preseed = nullptr, bool dry = false) {
     if (!ctx || !q) return fail(ctx, TGP_INVALID_ARG, "null argument");
     qs.q = q;
     TGP_TRY(get_table(ctx, q->table, &qs.T));
@@ -1589,7 +1590,11 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             sig.insert(sig.end(), {q->group[k].column, static_cast<uint64_t>(P.gkey[k].min), P.gkey[k].stride});
         }
         const uint64_t entries = J->krange + 1;
-        if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) {
+        if (dry) {
+            // Sizing only (tgp_query_footprint): a payload still to be built
+            // counts as memory the query needs; nothing is launched.
+            if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) qs.pending_dev_bytes += entries * 4;
+        } else if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) {
             if (J->pay && J->pay_entries != entries) {
                 dev_free(ctx, J->pay);
                 J->pay = nullptr;
@@ -1942,6 +1947,26 @@ int tgp_execute_topn(tgp_ctx* ctx, const tgp_query* q, uint32_t order_agg, int d
                      uint64_t* keys_out, tgp_agg_value* vals_out, tgp_query_result* result) {
     const TopNReq tn{order_agg, descending != 0, limit};
     return execute_impl(ctx, q, keys_out, vals_out, limit, result, &tn);
+}
+
+int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes) {
+    if (!ctx || !q || !device_bytes) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    QueryState qs;
+    TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem(), nullptr, /*dry=*/true));
+    const Plan& P = qs.b->P;
+    // What execute_impl carves or allocates for one run of the query.
+    uint64_t bytes = qs.block_words() * 8 + 1024 + qs.pending_dev_bytes;
+    if (qs.mode == MODE_GROUP_HASH) {
+        const uint64_t slot_bytes = static_cast<uint64_t>(P.hstride) * 8;
+        const uint64_t max_groups =
+            std::min<uint64_t>(qs.hcap, static_cast<uint64_t>(std::min<unsigned __int128>(qs.D, qs.hcap)));
+        bytes += qs.hcap * slot_bytes;                                    // the group table
+        bytes += max_groups * slot_bytes;                                 // gathered occupied slots
+        bytes += format_hash_groups_scratch(max_groups, qs.total_bits);   // device sort
+        bytes += max_groups * (8ull * q->ngroup + sizeof(tgp_agg_value) * q->nagg) + 512;  // formatted result
+    }
+    *device_bytes = bytes;
+    return TGP_OK;
 }
 
 // --------------------------------------------------------------------------

@@ -16,7 +16,9 @@ with the stated shapes (one independent numpy PCG64 stream per column):
 """
 from __future__ import annotations
 
+import os
 import zlib
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -31,16 +33,25 @@ def _rng(seed: int, name: str) -> np.random.Generator:
     return np.random.Generator(np.random.PCG64([seed, zlib.crc32(name.encode())]))
 
 
+_LINEITEM = (("quantity", 1, 51, np.int32), ("price_cents", 90_000, 10_500_001, np.int64),
+             ("discount_pct", 0, 11, np.int32), ("tax_pct", 0, 9, np.int32),
+             ("ship_day", DAY0, DAY0 + NDAYS, np.int32), ("flag_a", 0, 3, np.uint8), ("flag_b", 0, 2, np.uint8))
+
+
+def _pool() -> ThreadPoolExecutor:
+    return ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
+
+
 def lineitem(n: int, seed: int = 1) -> dict[str, np.ndarray]:
-    return {
-        "quantity": _rng(seed, "quantity").integers(1, 51, n, dtype=np.int32),
-        "price_cents": _rng(seed, "price_cents").integers(90_000, 10_500_001, n, dtype=np.int64),
-        "discount_pct": _rng(seed, "discount_pct").integers(0, 11, n, dtype=np.int32),
-        "tax_pct": _rng(seed, "tax_pct").integers(0, 9, n, dtype=np.int32),
-        "ship_day": _rng(seed, "ship_day").integers(DAY0, DAY0 + NDAYS, n, dtype=np.int32),
-        "flag_a": _rng(seed, "flag_a").integers(0, 3, n, dtype=np.uint8),
-        "flag_b": _rng(seed, "flag_b").integers(0, 2, n, dtype=np.uint8),
-    }
+    # Each column has its own stream, so drawing them on threads gives the
+    # same values as drawing them one after another.
+    def draw(spec):
+        name, lo, hi, dt = spec
+        return name, _rng(seed, name).integers(lo, hi, n, dtype=dt)
+    if n < (1 << 20):
+        return dict(draw(s) for s in _LINEITEM)
+    with _pool() as ex:
+        return dict(ex.map(draw, _LINEITEM))
 
 
 def dimension(n: int, seed: int = 2) -> dict[str, np.ndarray]:
@@ -52,15 +63,22 @@ def dimension(n: int, seed: int = 2) -> dict[str, np.ndarray]:
     }
 
 
-def zipf_ranks(n: int, nkeys: int, s: float, rng: np.random.Generator, chunk: int = 1 << 24) -> np.ndarray:
+def zipf_ranks(n: int, nkeys: int, s: float, rng: np.random.Generator, chunk: int = 1 << 22) -> np.ndarray:
     """n draws of ranks 1..nkeys with P(r) ∝ r^-s (inverse CDF)."""
     w = np.arange(1, nkeys + 1, dtype=np.float64) ** (-s)
     cdf = np.cumsum(w)
     cdf /= cdf[-1]
     out = np.empty(n, dtype=np.int64)
-    for i in range(0, n, chunk):
-        m = min(chunk, n - i)
-        out[i:i + m] = np.searchsorted(cdf, rng.random(m), side="right") + 1
+    # The uniforms are drawn chunk by chunk in order (so the values do not
+    # depend on the thread count); the searches run on threads.
+    def search(i, u):
+        out[i:i + u.shape[0]] = np.searchsorted(cdf, u, side="right") + 1
+    with _pool() as ex:
+        futs = []
+        for i in range(0, n, chunk):
+            futs.append(ex.submit(search, i, rng.random(min(chunk, n - i))))
+        for f in futs:
+            f.result()
     np.minimum(out, nkeys, out=out)
     return out
 

@@ -637,10 +637,22 @@ class PreparedQuery:
         if join is not None:
             self.q.join = join.id
         self.nk, self.na = len(group_by), len(aggs)
+        # The query as written (checkers and the serving loop re-read it).
+        self.spec = {"aggs": list(aggs), "group_by": tuple(group_by), "where": where, "join": join,
+                     "probe_key": probe_key}
         self._alloc(group_cap)
         self.res = A.QueryResult()
         self._fn = table.ctx.lib.tgp_execute
         self.graph = 0
+
+    def footprint(self) -> int:
+        """Device bytes one run of this query holds while it runs, as its plan
+        sizes them (tgp_query_footprint): result block, group hash table and
+        the buffers of its result, a join payload still to be built."""
+        ctx = self.table.ctx
+        b = C.c_uint64()
+        ctx._check(ctx.lib.tgp_query_footprint(ctx.h, C.byref(self.q), C.byref(b)), "tgp_query_footprint")
+        return int(b.value)
 
     def rebind(self, where: Pred | None) -> "PreparedQuery":
         """Replaces the WHERE program (new literals or shape); the rest of the
@@ -649,6 +661,7 @@ class PreparedQuery:
         self.q.pred = nodes if nodes is not None else None
         self.q.npred = n
         self._keep = (nodes,) + tuple(self._keep[1:])
+        self.spec["where"] = where
         if self.graph:
             self.capture()
         return self

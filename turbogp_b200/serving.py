@@ -39,15 +39,21 @@ class Request:
 @dataclass
 class Template:
     """A query shape served from a pool of prepared queries (one per request in
-    flight), each rebound to the request's predicate."""
+    flight), each rebound to the request's predicate. ``mem_bytes`` is the
+    device memory a running query of this shape holds: by default the
+    planner's own estimate for it (``PreparedQuery.footprint``:
+    tgp_query_footprint), taken from the first prepared query."""
     name: str
     make: Callable[[], PreparedQuery]
-    mem_bytes: int                 # device memory a running query of this shape holds
+    mem_bytes: int | None = None
     pool: list = field(default_factory=list)
     heavy: bool = False            # served by the heavy lane (its prepared queries live on their own context)
 
     def take(self) -> PreparedQuery:
-        return self.pool.pop() if self.pool else self.make()
+        pq = self.pool.pop() if self.pool else self.make()
+        if self.mem_bytes is None:
+            self.mem_bytes = int(pq.footprint())
+        return pq
 
     def give(self, pq: PreparedQuery) -> None:
         self.pool.append(pq)
