@@ -564,6 +564,79 @@ TGP_API int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id graph, uint64_t* keys_ou
 TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
 
 /* ------------------------------------------------------------------------ */
+/* Scan variants and the autotuner                                           */
+/* ------------------------------------------------------------------------ */
+
+/* The knobs of a scan launch that the planner otherwise sets by rule. The
+ * reference picks a CPU kernel per (operator, CPU target, memory tier) from
+ * its kernel table (src/kernel/mod.rs:209-221) and sizes its morsels by a
+ * fixed 65,536-row chunk (aggregate.rs:259); here one query class can run
+ * several variants of the scan kernel, and tgp_autotune measures which is
+ * fastest. */
+typedef struct tgp_variant {
+    uint32_t threads;      /* consumer threads per CTA: 0 = the planner's rule, 256 or 512
+                              (8 or 4 rows per thread of a 2,048-row tile) */
+    uint32_t max_stages;   /* cap on the shared-memory pipeline stages, 1..8 */
+    uint32_t placement;    /* direct groups: 0 = rule, 1 = per-thread private accumulators,
+                              2 = per-CTA shared, 3 = global */
+    uint32_t presum;       /* 1 = shared pre-aggregation of repeated keys (hash / global grouping) allowed */
+    uint32_t dense;        /* 1 = dense column programs (private placement) allowed */
+    uint32_t shapes;       /* 1 = ahead-of-time fixed-shape kernels allowed */
+    uint32_t payload;      /* 1 = unique-key join payload arrays allowed */
+    uint32_t ctas_per_sm;  /* 1 or 2 */
+    uint32_t l2_ahead;     /* tiles of L2 bulk prefetch ahead of the stage copies, 0 = off */
+    uint32_t _pad;
+} tgp_variant;
+
+/* The variant used for every query whose class has no tuned entry (the
+ * planner's rules: threads 0, max_stages 8, placement 0, presum / dense /
+ * shapes / payload 1, ctas_per_sm 1, l2_ahead 0). */
+TGP_API int tgp_set_default_variant(tgp_ctx* ctx, const tgp_variant* v);
+TGP_API int tgp_get_default_variant(tgp_ctx* ctx, tgp_variant* v);
+
+/* Batch shaping: morsel length in tiles (default 16), whether same-table
+ * queries of a batch share scans (default 1), and the largest per-plan
+ * accumulator region that joins a shared scan (default 32 KiB). */
+TGP_API int tgp_batch_config(tgp_ctx* ctx, uint32_t morsel_tiles, int shared_scans, uint64_t share_extra_max);
+
+/* A query's class: its shape (join, number of group keys, of values and of
+ * predicate leaves, direct or hash grouping) and the binary orders of
+ * magnitude of its row count and of its bound on distinct groups. Tuned
+ * variants are kept per class. */
+TGP_API int tgp_tune_class(tgp_ctx* ctx, const tgp_query* q, uint64_t* key);
+TGP_API int tgp_tune_set(tgp_ctx* ctx, uint64_t key, const tgp_variant* v);
+/* *found = 0 when the class has no tuned entry (v then holds the default). */
+TGP_API int tgp_tune_get(tgp_ctx* ctx, uint64_t key, tgp_variant* v, int* found);
+/* The tuned entries in ascending key order (for saving them). */
+TGP_API int tgp_tune_count(tgp_ctx* ctx, uint32_t* n);
+TGP_API int tgp_tune_at(tgp_ctx* ctx, uint32_t i, uint64_t* key, tgp_variant* v);
+TGP_API int tgp_tune_clear(tgp_ctx* ctx);
+
+/* One measured candidate of tgp_autotune. */
+typedef struct tgp_tune_entry {
+    tgp_variant variant;
+    double ms;              /* median scan-kernel time over `reps` runs (CUDA events, each launch
+                               queued behind a short device delay) */
+    int32_t status;         /* TGP_OK, or why the candidate could not run */
+    uint32_t same_result;   /* 1 = its result equals the planner's rule's, bit for bit */
+    uint32_t threads_used;  /* what the plan launched with */
+    uint32_t stages_used;
+    uint32_t mode_used;     /* accumulator placement the plan chose: 2 private, 3 shared, 4 global, 5 hash */
+    uint32_t _pad;
+} tgp_tune_entry;
+
+/* Measures the variants of the query's scan (threads x stage cap x
+ * accumulator placement / dense programs for direct groups, or x
+ * pre-aggregation for hash grouping), each first checked to return the
+ * result of the planner's rule bit for bit, then timed `reps` times; installs
+ * the fastest correct one for the query's class and reports every candidate
+ * (the rule's first) in `entries` (*n of them; only the first `cap` are
+ * written) and the index of the fastest in *best. Launch profiling must be
+ * off. */
+TGP_API int tgp_autotune(tgp_ctx* ctx, const tgp_query* q, uint32_t reps, tgp_tune_entry* entries, uint32_t cap,
+                         uint32_t* n, uint32_t* best, uint64_t* key);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free aggregate                                                 */
 /* ------------------------------------------------------------------------ */
 

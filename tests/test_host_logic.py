@@ -47,3 +47,24 @@ def test_i128_to_f64_rounds_like_the_compiler(tmp_path):
                    check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout
+
+
+def test_tuning_cache_round_trip(tmp_path):
+    """The autotuner's JSON cache keeps every entry and rejects unknown
+    fields and versions."""
+    import json
+    from turbogp_b200.engine import VARIANT_FIELDS, load_tuning_file, save_tuning_file
+    entries = {(3 << 24) | (26 << 16) | 0x45: {f: i for i, f in enumerate(VARIANT_FIELDS)},
+               7: {f: 1 for f in VARIANT_FIELDS}}
+    p = tmp_path / "t.json"
+    save_tuning_file(p, entries)
+    assert load_tuning_file(p) == entries
+    doc = json.loads(p.read_text())
+    assert [e["class"] for e in doc["entries"]] == sorted(entries)
+    doc["entries"][0]["variant"]["bogus"] = 1
+    p.write_text(json.dumps(doc))
+    with pytest.raises(ValueError):
+        load_tuning_file(p)
+    p.write_text(json.dumps({"version": 9, "entries": []}))
+    with pytest.raises(ValueError):
+        load_tuning_file(p)

@@ -30,6 +30,18 @@ MAX_GROUP_KEYS = 4
 MAX_PRED_NODES = 16
 
 
+class Variant(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("max_stages", C.c_uint32), ("placement", C.c_uint32),
+                ("presum", C.c_uint32), ("dense", C.c_uint32), ("shapes", C.c_uint32), ("payload", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("l2_ahead", C.c_uint32), ("_pad", C.c_uint32)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("variant", Variant), ("ms", C.c_double), ("status", C.c_int32), ("same_result", C.c_uint32),
+                ("threads_used", C.c_uint32), ("stages_used", C.c_uint32), ("mode_used", C.c_uint32),
+                ("_pad", C.c_uint32)]
+
+
 class ColumnDesc(C.Structure):
     _fields_ = [("dtype", C.c_uint32), ("coltype", C.c_uint32), ("data", C.c_void_p)]
 
@@ -149,6 +161,17 @@ PROTOTYPES = [
      [C.c_void_p, C.POINTER(Query), C.c_uint32, C.c_int, C.c_uint64, C.c_void_p, C.POINTER(AggValue),
       C.POINTER(QueryResult)]),
     ("tgp_query_footprint", C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    ("tgp_set_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),
+    ("tgp_get_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),
+    ("tgp_batch_config", C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_uint64]),
+    ("tgp_tune_class", C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    ("tgp_tune_set", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Variant)]),
+    ("tgp_tune_get", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Variant), C.POINTER(C.c_int)]),
+    ("tgp_tune_count", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    ("tgp_tune_at", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(Variant)]),
+    ("tgp_tune_clear", C.c_int, [C.c_void_p]),
+    ("tgp_autotune", C.c_int, [C.c_void_p, C.POINTER(Query), C.c_uint32, C.POINTER(TuneEntry), C.c_uint32,
+                               C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     ("tgp_count_distinct", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.POINTER(C.c_uint64),
       C.POINTER(C.c_uint32)]),

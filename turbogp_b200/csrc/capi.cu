@@ -315,7 +315,7 @@ struct Builder {
         std::memset(&P, 0, sizeof(P));
         col2slot.assign(t->cols.size(), -1);
         P.nrows = t->rows;
-        P.nthreads = static_cast<uint32_t>(c->scan_threads);
+        P.nthreads = 512;  // private placement picks its own; a variant may ask for 256
         P.jslot = -1;
         P.flush_limit = ~0ull;
     }
@@ -660,26 +660,29 @@ void fill_value(const AggMap& m, const unsigned long long* slot /* [nv1][2] */, 
 }
 
 // Chooses shared-memory stages for a plan given per-mode scratch bytes.
-int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = scan_kernel_static_smem()) {
+int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = scan_kernel_static_smem(),
+              const Knobs* kn = nullptr) {
+    const Knobs& K = kn ? *kn : ctx->knobs;
     const size_t budget = ctx->max_dyn_smem > static_smem ? ctx->max_dyn_smem - static_smem : 0;
     size_t stage = P.stage_bytes;
     if (stage == 0) {
         // Nothing to stage (e.g. COUNT(*) without WHERE): stage one tiny dummy.
         stage = 0;
     }
-    const size_t per_cta = budget / static_cast<size_t>(std::max(1, ctx->ctas_per_sm));
+    const size_t per_cta = budget / static_cast<size_t>(std::max(1, K.ctas_per_sm));
     size_t avail = per_cta > kBarrierBytes + extra_bytes ? per_cta - kBarrierBytes - extra_bytes : 0;
-    uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1;
+    const size_t cap = static_cast<size_t>(std::max(1, std::min(K.max_stages, kMaxStages)));
+    uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
     if (S == 0) {
         // Fall back to a single CTA per SM.
         avail = budget > kBarrierBytes + extra_bytes ? budget - kBarrierBytes - extra_bytes : 0;
-        S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1;
+        S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
         if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "query does not fit in shared memory");
     }
     P.nstages = S;
     // L2 prefetch ahead of the stage copies measured neutral on the scan and
-    // grouped-aggregate workloads, so it is off unless TGP_L2_AHEAD asks.
-    P.l2_ahead = ctx->l2_ahead >= 0 ? static_cast<uint32_t>(ctx->l2_ahead) : 0u;
+    // grouped-aggregate workloads, so it is off unless a variant asks for it.
+    P.l2_ahead = static_cast<uint32_t>(std::max(0, K.l2_ahead));
     P.extra_off = static_cast<uint32_t>(kBarrierBytes + static_cast<size_t>(S) * stage);
     P.extra_off = (P.extra_off + 127u) & ~127u;
     P.smem_bytes = static_cast<uint32_t>(P.extra_off + extra_bytes);
@@ -842,21 +845,6 @@ int tgp_init(tgp_ctx** out, int device) {
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     cudaGetLastError();
-    if (const char* e = std::getenv("TGP_CTAS_PER_SM")) ctx->ctas_per_sm = std::max(1, std::atoi(e));
-    if (const char* e = std::getenv("TGP_NO_DENSE")) ctx->dense_path = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_NO_SHARED_SCANS")) ctx->shared_scans = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_SHARE_EXTRA_MAX")) ctx->share_extra_max = static_cast<size_t>(std::atoll(e));
-    if (const char* e = std::getenv("TGP_BATCH_MORSEL_TILES")) ctx->morsel_tiles = std::max(1, std::atoi(e));
-    if (const char* e = std::getenv("TGP_NO_HASH_PRESUM")) ctx->hash_presum = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_NO_JOIN_PAYLOAD")) ctx->join_payload = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_L2_AHEAD")) ctx->l2_ahead = std::min(64, std::max(0, std::atoi(e)));
-    if (const char* e = std::getenv("TGP_NO_DENSE_SHAPES")) ctx->dense_shapes = std::atoi(e) == 0;
-    if (const char* e = std::getenv("TGP_SCAN_THREADS")) {
-        ctx->scan_threads = std::atoi(e) == 256 ? 256 : 512;
-        ctx->scan_threads_set = true;
-    }
-    if (const char* e = std::getenv("TGP_MAX_STAGES"))
-        ctx->max_stages = std::min(kMaxStages, std::max(1, std::atoi(e)));
     *out = ctx;
     return TGP_OK;
 }
@@ -1367,6 +1355,23 @@ static void attach_join(Plan& P, const JoinTable& J, int key_slot) {
     if (J.empty_range) P.jkmin = 0;
 }
 
+// The class a query's scan variant is tuned for: its shape (join, number of
+// group keys, values and predicate leaves, direct or hash grouping) and the
+// binary orders of magnitude of its row count and of its group count bound.
+static uint64_t tune_key_of(const tgp_query* q, const Plan& P, uint64_t rows, unsigned __int128 D) {
+    auto log2ceil = [](unsigned __int128 x) -> uint64_t {
+        uint64_t b = 0;
+        while (b < 127 && (static_cast<unsigned __int128>(1) << b) < x) ++b;
+        return b;
+    };
+    const unsigned __int128 groups = std::min<unsigned __int128>(D, std::max<uint64_t>(rows, 1));
+    const uint64_t shape = (q->join ? 1ull : 0ull) | (static_cast<uint64_t>(std::min<uint32_t>(q->ngroup, 7)) << 1) |
+                           (static_cast<uint64_t>(std::min<uint32_t>(P.nval, 15)) << 4) |
+                           ((D > kDirectMaxGroups ? 1ull : 0ull) << 8) |
+                           (static_cast<uint64_t>(std::min<uint32_t>(P.nleaf, 15)) << 9);
+    return shape | (log2ceil(std::max<uint64_t>(rows, 1)) << 16) | (log2ceil(groups) << 24);
+}
+
 // A planned query: the lowered plan and what decoding its result block needs.
 struct QueryState {
     const tgp_query* q = nullptr;
@@ -1386,6 +1391,8 @@ struct QueryState {
     size_t extra = 0;     // per-mode shared scratch bytes
     uint64_t hcap = 0;    // hash table slots (MODE_GROUP_HASH)
     uint64_t pending_dev_bytes = 0;  // device memory a dry plan would still allocate (join payload)
+    Knobs kn;             // the scan variant this plan was made with
+    uint64_t tune_key = 0;  // the query class the variant was looked up under
     uint64_t acc_words() const { return mode == MODE_GROUP_HASH ? 0 : ngroups_direct * nv1 * 2; }
     uint64_t block_words() const { return 6 + acc_words(); }  // [counters 4][error 2][accumulators]
     bool has_minmax() const {
@@ -1480,10 +1487,22 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     }
     P.ngkey = q->ngroup;
 
+    // The query's class and the scan variant for it: a tuned entry if the
+    // autotuner measured this class, else the context's default (the
+    // planner's rules).
+    qs.tune_key = tune_key_of(q, P, T->rows, D);
+    if (ctx->force_knobs) {
+        qs.kn = *ctx->force_knobs;
+    } else {
+        auto it = ctx->tuned.find(qs.tune_key);
+        qs.kn = it != ctx->tuned.end() ? it->second : ctx->knobs;
+    }
+    const Knobs& kn = qs.kn;
+
     // Join payload: with unique build keys over a dense key range, and no
     // build-side aggregate arguments, a probe row needs one lookup,
     // pay[key - kmin] = the build-side part of its group index.
-    bool pay_ok = J && J->unique && !J->empty_range && ctx->join_payload &&
+    bool pay_ok = J && J->unique && !J->empty_range && kn.payload &&
                   J->krange + 1 <= std::min<uint64_t>(1ull << 28, std::max<uint64_t>(1ull << 22, 8 * J->entries));
     for (uint32_t v = 0; pay_ok && v < P.nval; ++v)
         for (uint32_t f = 0; f < P.val[v].nf; ++f) pay_ok = pay_ok && !P.val[v].f[f].build_side;
@@ -1518,8 +1537,9 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         // 512 threads when two stages still fit beside them, else 256 threads
         // (twice the rows per thread).
         uint32_t nt = 0;
-        if (ngroups_direct * static_cast<uint64_t>(nv1) * 512 < (1ull << 31))
-            for (uint32_t cand : {static_cast<uint32_t>(ctx->scan_threads), 256u}) {
+        const uint32_t first = kn.threads == 256 ? 256u : 512u;
+        if (kn.placement <= 1 && ngroups_direct * static_cast<uint64_t>(nv1) * 512 < (1ull << 31))
+            for (uint32_t cand : {first, 256u}) {
                 if (private_bytes(cand) + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
                     nt = cand;
                     break;
@@ -1530,11 +1550,11 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         // room for four or more, the deeper pipeline wins: 60M-row join probe
         // with 25 groups 0.50 -> 0.46 ms. With three stages at 256 threads the
         // halved warp count loses (6M-row grouped aggregate 0.054 -> 0.068 ms).
-        if (nt == 512 && P.stage_bytes && !ctx->scan_threads_set) {
+        if (nt == 512 && P.stage_bytes && kn.threads == 0) {
             const size_t st = P.stage_bytes;
             const size_t s512 = budget > private_bytes(512) ? (budget - private_bytes(512)) / st : 0;
             const size_t s256 = budget > private_bytes(256) ? (budget - private_bytes(256)) / st : 0;
-            if (s512 == 2 && std::min<size_t>(s256, ctx->max_stages) >= 4) nt = 256;
+            if (s512 == 2 && std::min<size_t>(s256, static_cast<size_t>(kn.max_stages)) >= 4) nt = 256;
         }
         if (nt) {
             mode = MODE_GROUP_PRIVATE;
@@ -1549,22 +1569,25 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             }
             // Dense column program: int64 partials, no join, no per-row
             // overflow checks.
-            if (!acc128 && (!J || pay_ok) && !P.check_ovf && ctx->dense_path)
+            if (!acc128 && (!J || pay_ok) && !P.check_ovf && kn.dense)
                 P.dense_vec = compile_chain(b, pay_ok) ? 1u : 0u;
             // Scalar aggregates prefer the register fast path; a join's dense
             // program implies its payload path.
             if (!acc128) P.shape = scalar_shape_of(P);
-            if (!P.shape && P.dense_vec && ctx->dense_shapes && (!J || pay_ok)) P.shape = dense_shape_of(P);
-        } else if (shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
+            if (!P.shape && P.dense_vec && kn.shapes && (!J || pay_ok)) P.shape = dense_shape_of(P);
+        } else if (kn.placement != 3 && shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;
             acc128 = false;
+            if (kn.threads == 256) P.nthreads = 256;
         } else {
             mode = MODE_GROUP_GLOBAL;
             acc128 = false;
+            if (kn.threads == 256) P.nthreads = 256;
         }
     } else {
         mode = MODE_GROUP_HASH;
+        if (kn.threads == 256) P.nthreads = 256;
         if (total_bits > 64 || (q->ngroup > 1 && total_bits > 63))
             return fail(ctx, TGP_UNSUPPORTED, "group key tuple wider than 63 bits");
         uint32_t shift = 0;
@@ -1642,7 +1665,7 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     // grouping): SUM / COUNT(col) values, no join, no per-row overflow checks;
     // its i32 partials are bounded once the launch grid is known.
     if (mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) {
-        bool presum = ctx->hash_presum && !join && !P.check_ovf && !acc128;
+        bool presum = kn.presum && !join && !P.check_ovf && !acc128;
         for (uint32_t v = 0; presum && v < P.nval; ++v)
             presum = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
         const uint32_t HS = 4096;
@@ -1805,7 +1828,7 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
         }
         TGP_CUDA(launch_fill_slots(P.htab, hcap, img, ctx->sms, ctx->stream));
     }
-    TGP_TRY(size_smem(ctx, P, extra));
+    TGP_TRY(size_smem(ctx, P, extra, scan_kernel_static_smem(), &qs.kn));
     bound_presum(ctx, qs);
     TGP_TRY(launch(ctx, P, mode, acc128));
 
@@ -1970,6 +1993,269 @@ int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes
 }
 
 // --------------------------------------------------------------------------
+// Scan variants and the autotuner
+// --------------------------------------------------------------------------
+static Knobs knobs_from(const tgp_variant& v) {
+    Knobs k;
+    k.threads = v.threads == 256 ? 256 : v.threads == 512 ? 512 : 0;
+    k.max_stages = v.max_stages ? std::min<int>(static_cast<int>(v.max_stages), kMaxStages) : kMaxStages;
+    k.placement = v.placement <= 3 ? static_cast<int>(v.placement) : 0;
+    k.presum = v.presum != 0;
+    k.dense = v.dense != 0;
+    k.shapes = v.shapes != 0;
+    k.payload = v.payload != 0;
+    k.ctas_per_sm = v.ctas_per_sm == 2 ? 2 : 1;
+    k.l2_ahead = static_cast<int>(std::min<uint32_t>(v.l2_ahead, 64));
+    return k;
+}
+
+static tgp_variant variant_of(const Knobs& k) {
+    tgp_variant v;
+    std::memset(&v, 0, sizeof(v));
+    v.threads = static_cast<uint32_t>(k.threads);
+    v.max_stages = static_cast<uint32_t>(k.max_stages);
+    v.placement = static_cast<uint32_t>(k.placement);
+    v.presum = k.presum;
+    v.dense = k.dense;
+    v.shapes = k.shapes;
+    v.payload = k.payload;
+    v.ctas_per_sm = static_cast<uint32_t>(k.ctas_per_sm);
+    v.l2_ahead = static_cast<uint32_t>(k.l2_ahead);
+    return v;
+}
+
+static bool same_knobs(const Knobs& a, const Knobs& b) {
+    return a.threads == b.threads && a.max_stages == b.max_stages && a.placement == b.placement &&
+           a.presum == b.presum && a.dense == b.dense && a.shapes == b.shapes && a.payload == b.payload &&
+           a.ctas_per_sm == b.ctas_per_sm && a.l2_ahead == b.l2_ahead;
+}
+
+int tgp_set_default_variant(tgp_ctx* ctx, const tgp_variant* v) {
+    if (!ctx || !v) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    ctx->knobs = knobs_from(*v);
+    return TGP_OK;
+}
+
+int tgp_get_default_variant(tgp_ctx* ctx, tgp_variant* v) {
+    if (!ctx || !v) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    *v = variant_of(ctx->knobs);
+    return TGP_OK;
+}
+
+int tgp_batch_config(tgp_ctx* ctx, uint32_t morsel_tiles, int shared_scans, uint64_t share_extra_max) {
+    if (!ctx || morsel_tiles == 0) return fail(ctx, TGP_INVALID_ARG, "morsel_tiles must be at least 1");
+    ctx->morsel_tiles = static_cast<int>(std::min<uint32_t>(morsel_tiles, 1u << 20));
+    ctx->shared_scans = shared_scans != 0;
+    ctx->share_extra_max = static_cast<size_t>(share_extra_max);
+    return TGP_OK;
+}
+
+int tgp_tune_class(tgp_ctx* ctx, const tgp_query* q, uint64_t* key) {
+    if (!ctx || !q || !key) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    QueryState qs;
+    TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem(), nullptr, /*dry=*/true));
+    *key = qs.tune_key;
+    return TGP_OK;
+}
+
+int tgp_tune_set(tgp_ctx* ctx, uint64_t key, const tgp_variant* v) {
+    if (!ctx || !v) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    ctx->tuned[key] = knobs_from(*v);
+    return TGP_OK;
+}
+
+int tgp_tune_get(tgp_ctx* ctx, uint64_t key, tgp_variant* v, int* found) {
+    if (!ctx || !v || !found) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    auto it = ctx->tuned.find(key);
+    *found = it != ctx->tuned.end();
+    *v = variant_of(*found ? it->second : ctx->knobs);
+    return TGP_OK;
+}
+
+int tgp_tune_count(tgp_ctx* ctx, uint32_t* n) {
+    if (!ctx || !n) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    *n = static_cast<uint32_t>(ctx->tuned.size());
+    return TGP_OK;
+}
+
+int tgp_tune_at(tgp_ctx* ctx, uint32_t i, uint64_t* key, tgp_variant* v) {
+    if (!ctx || !key || !v) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (i >= ctx->tuned.size()) return fail(ctx, TGP_INVALID_ARG, "tuned entry index out of range");
+    std::vector<uint64_t> keys;
+    keys.reserve(ctx->tuned.size());
+    for (const auto& kv : ctx->tuned) keys.push_back(kv.first);
+    std::sort(keys.begin(), keys.end());
+    *key = keys[i];
+    *v = variant_of(ctx->tuned[keys[i]]);
+    return TGP_OK;
+}
+
+int tgp_tune_clear(tgp_ctx* ctx) {
+    if (!ctx) return TGP_INVALID_ARG;
+    ctx->tuned.clear();
+    return TGP_OK;
+}
+
+namespace {
+
+// One run of a query into host vectors (grown to its group count).
+struct HostResult {
+    std::vector<uint64_t> keys;
+    std::vector<tgp_agg_value> vals;
+    tgp_query_result res{};
+};
+
+int run_into(tgp_ctx* ctx, const tgp_query* q, HostResult* r) {
+    uint64_t cap = std::max<uint64_t>(1, r->res.ngroups);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        r->keys.assign(std::max<uint64_t>(1, cap * std::max<uint32_t>(1, q->ngroup)), 0);
+        r->vals.assign(std::max<uint64_t>(1, cap * std::max<uint32_t>(1, q->nagg)), tgp_agg_value{});
+        const int st = execute_impl(ctx, q, r->keys.data(), r->vals.data(), cap, &r->res, nullptr);
+        if (st != TGP_CAPACITY) return st;
+        cap = r->res.ngroups;
+    }
+    return fail(ctx, TGP_CAPACITY, "group count kept growing");
+}
+
+bool same_results(const tgp_query* q, const HostResult& a, const HostResult& b) {
+    if (a.res.rows_scanned != b.res.rows_scanned || a.res.rows_selected != b.res.rows_selected ||
+        a.res.ngroups != b.res.ngroups || a.res.flags != b.res.flags)
+        return false;
+    const uint64_t nk = a.res.ngroups * q->ngroup, nv = a.res.ngroups * q->nagg;
+    if (nk && std::memcmp(a.keys.data(), b.keys.data(), nk * 8) != 0) return false;
+    for (uint64_t i = 0; i < nv; ++i) {
+        const tgp_agg_value &x = a.vals[i], &y = b.vals[i];
+        if (x.lo != y.lo || x.hi != y.hi || x.count != y.count || std::memcmp(&x.as_f64, &y.as_f64, 8) != 0) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+int tgp_autotune(tgp_ctx* ctx, const tgp_query* q, uint32_t reps, tgp_tune_entry* entries, uint32_t cap,
+                 uint32_t* n_out, uint32_t* best_out, uint64_t* key_out) {
+    if (!ctx || !q || !n_out || !best_out || !key_out || (cap && !entries))
+        return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (ctx->profile) return fail(ctx, TGP_INVALID_ARG, "turn launch profiling off before tuning");
+    reps = std::max<uint32_t>(1, std::min<uint32_t>(reps, 64));
+    QueryState base;
+    TGP_TRY(plan_query(ctx, q, base, scan_kernel_static_smem(), nullptr, /*dry=*/true));
+    const uint64_t key = base.tune_key;
+    const bool hash = base.mode == MODE_GROUP_HASH;
+
+    // Candidates: the planner's rules first, then threads x stage cap x
+    // accumulator placement (direct groups) or pre-aggregation (hash).
+    std::vector<Knobs> cands;
+    cands.push_back(ctx->knobs);
+    for (int nt : {512, 256})
+        for (int stg : {2, 4, kMaxStages}) {
+            Knobs k = ctx->knobs;
+            k.threads = nt;
+            k.max_stages = stg;
+            if (hash) {
+                for (bool ps : {true, false}) {
+                    k.presum = ps;
+                    cands.push_back(k);
+                }
+            } else {
+                for (int pl : {1, 2, 3}) {
+                    k.placement = pl;
+                    if (pl == 1) {
+                        for (bool dn : {true, false}) {
+                            k.dense = dn;
+                            cands.push_back(k);
+                        }
+                        k.dense = ctx->knobs.dense;
+                    } else {
+                        cands.push_back(k);
+                    }
+                }
+            }
+        }
+
+    // Reference result: the planner's rules.
+    HostResult ref;
+    ctx->force_knobs = &cands[0];
+    int st = run_into(ctx, q, &ref);
+    ctx->force_knobs = nullptr;
+    TGP_TRY(st);
+
+    uint32_t n = 0, best = 0;
+    double best_ms = 0.0;
+    std::vector<std::pair<Knobs, double>> measured;
+    for (size_t c = 0; c < cands.size(); ++c) {
+        const Knobs& k = cands[c];
+        bool dup = false;
+        for (size_t d = 0; d < c && !dup; ++d) dup = same_knobs(cands[d], k);
+        if (dup) continue;
+        tgp_tune_entry e;
+        std::memset(&e, 0, sizeof(e));
+        e.variant = variant_of(k);
+        ctx->force_knobs = &k;
+        QueryState qs;
+        e.status = plan_query(ctx, q, qs, scan_kernel_static_smem(), nullptr, /*dry=*/true);
+        if (e.status == TGP_OK) {
+            e.threads_used = qs.mode == MODE_GROUP_PRIVATE ? qs.b->P.nthreads : 512u;
+            e.mode_used = qs.mode;
+            Plan P = qs.b->P;
+            if (size_smem(ctx, P, qs.extra, scan_kernel_static_smem(), &qs.kn) == TGP_OK) e.stages_used = P.nstages;
+            HostResult r;
+            r.res.ngroups = ref.res.ngroups;
+            e.status = run_into(ctx, q, &r);
+            e.same_result = (e.status == TGP_OK && same_results(q, ref, r)) ? 1u : 0u;
+        }
+        if (e.status == TGP_OK && e.same_result) {
+            // Gated timing of the scan launch of each run.
+            std::vector<double> t;
+            HostResult r;
+            r.res.ngroups = ref.res.ngroups;
+            ctx->profile = true;
+            ctx->profile_gate = true;
+            for (uint32_t i = 0; i < reps && e.status == TGP_OK; ++i) {
+                ctx->prof_used = 0;
+                e.status = run_into(ctx, q, &r);
+                double ms = 0.0;
+                for (size_t j = 0; j < ctx->prof_used; ++j) {
+                    float f = 0.f;
+                    if (cudaEventElapsedTime(&f, ctx->prof_events[j].first, ctx->prof_events[j].second) == cudaSuccess)
+                        ms += f;
+                }
+                t.push_back(ms);
+            }
+            ctx->profile = false;
+            ctx->profile_gate = false;
+            ctx->prof_used = 0;
+            std::sort(t.begin(), t.end());
+            e.ms = t.empty() ? 0.0 : t[t.size() / 2];
+            if (e.status == TGP_OK && (measured.empty() || e.ms < best_ms)) {
+                best_ms = e.ms;
+                best = n;
+            }
+            if (e.status == TGP_OK) measured.push_back({k, e.ms});
+        }
+        ctx->force_knobs = nullptr;
+        cudaGetLastError();
+        if (n < cap) entries[n] = e;
+        ++n;
+    }
+    ctx->force_knobs = nullptr;
+    if (measured.empty()) return fail(ctx, TGP_DEVICE_ERROR, "no candidate variant ran");
+    // Install the fastest variant that returned the reference result.
+    const Knobs* win = nullptr;
+    double wms = 0.0;
+    for (const auto& m : measured)
+        if (!win || m.second < wms) {
+            win = &m.first;
+            wms = m.second;
+        }
+    ctx->tuned[key] = *win;
+    *n_out = n;
+    *best_out = best;
+    *key_out = key;
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
 // Batches
 // --------------------------------------------------------------------------
 static uint8_t* pinned_acquire(tgp_ctx* ctx, size_t bytes) {
@@ -2064,7 +2350,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
                 continue;
             }
         }
-        const int sst = size_smem(ctx, qs.b->P, qs.extra);
+        const int sst = size_smem(ctx, qs.b->P, qs.extra, scan_kernel_static_smem(), &qs.kn);
         if (sst == TGP_OK) bound_presum(ctx, qs);
         if (sst != TGP_OK) {
             items[i].status = tgp_execute(ctx, items[i].query, items[i].keys_out, items[i].vals_out, items[i].group_cap,
@@ -2110,7 +2396,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             }
             Plan& P = qs.b->P;
             // The int64 batch kernels carry the fixed-shape dense path.
-            P.shape = (!qs.acc128 && !qs.J && P.dense_vec && ctx->dense_shapes && dense_shape_of(P) == 1) ? 1u : 0u;
+            P.shape = (!qs.acc128 && !qs.J && P.dense_vec && qs.kn.shapes && dense_shape_of(P) == 1) ? 1u : 0u;
             const size_t extra = (qs.extra + 127) & ~size_t{127};
             Group* g = nullptr;
             // Plans with a large accumulator table (dense grouping, joins) are
@@ -2141,7 +2427,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         const size_t stage_off = (kBarrierBytes + g.q.size() * sizeof(Plan) + 127) & ~size_t{127};
         const size_t fixed = stage_off + 128 + g.extra;
         const size_t avail = budget > fixed ? budget - fixed : 0;
-        const uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, ctx->max_stages)) : 1u;
+        const uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, static_cast<size_t>(ctx->knobs.max_stages))) : 1u;
         if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "batched query does not fit in shared memory");
         size_t off = (stage_off + static_cast<size_t>(S) * stage + 127) & ~size_t{127};
         for (uint32_t i : g.q) {
@@ -2426,7 +2712,7 @@ int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out) {
         TGP_CUDA(cudaMalloc(reinterpret_cast<void**>(&g.image), acc_words * 8));
         TGP_TRY(upload(ctx, g.image, img.data(), img.size() * 8));
     }
-    TGP_TRY(size_smem(ctx, P, qs.extra));
+    TGP_TRY(size_smem(ctx, P, qs.extra, scan_kernel_static_smem(), &qs.kn));
     // Kernel attributes and occupancy are settled before the capture.
     if (scan_occupancy(qs.mode, qs.acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape) <= 0)
         return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");

@@ -124,6 +124,21 @@ struct JoinTable {
     std::vector<uint64_t> pay_sig;      // (column, min, stride) per build-side key
 };
 
+// Scan variant knobs. The planner's rules fill them by default; the
+// autotuner (tgp_autotune) measures alternatives per query class and keeps
+// the fastest (tgp_variant in the C ABI is their external form).
+struct Knobs {
+    int threads = 0;          // consumer threads per CTA: 0 = the planner's rule, else 256 or 512
+    int max_stages = kMaxStages;
+    int placement = 0;        // direct groups: 0 = rule, 1 = per-thread private, 2 = per-CTA shared, 3 = global
+    bool presum = true;       // shared pre-aggregation for hash / global grouping (when provably exact)
+    bool dense = true;        // dense column programs for private placement
+    bool shapes = true;       // ahead-of-time fixed-shape kernels
+    bool payload = true;      // unique-key join payload arrays
+    int ctas_per_sm = 1;
+    int l2_ahead = 0;         // L2 bulk prefetch distance in tiles (0 = off)
+};
+
 // Grow-only device scratch carved per call.
 struct Arena {
     uint8_t* base = nullptr;
@@ -172,17 +187,14 @@ struct tgp_ctx {
     bool profile_gate = false;  // queue a device delay before each timed launch
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
-    // Tuning knobs (environment: TGP_CTAS_PER_SM, TGP_MAX_STAGES, TGP_SCAN_THREADS, TGP_NO_DENSE, TGP_NO_DENSE_SHAPES, TGP_NO_JOIN_PAYLOAD, TGP_NO_HASH_PRESUM, TGP_L2_AHEAD, TGP_BATCH_MORSEL_TILES, TGP_NO_SHARED_SCANS, TGP_SHARE_EXTRA_MAX).
-    int ctas_per_sm = 1;
-    int scan_threads = 512;  // consumer threads per CTA (TGP_SCAN_THREADS: 256 or 512)
-    bool scan_threads_set = false;  // TGP_SCAN_THREADS given: no pipeline-depth switch to 256
-    int max_stages = tgp::kMaxStages;
-    bool dense_path = true;  // dense column programs for MODE_GROUP_PRIVATE (TGP_NO_DENSE=1 turns them off)
-    int l2_ahead = -1;         // L2 prefetch distance in tiles (TGP_L2_AHEAD; -1 = off)
-    bool join_payload = true;  // unique-key join payload arrays (TGP_NO_JOIN_PAYLOAD=1 turns them off)
-    bool hash_presum = true;   // shared pre-aggregation for hash grouping (TGP_NO_HASH_PRESUM=1 turns it off)
-    int morsel_tiles = 16;     // batch morsel length in tiles (TGP_BATCH_MORSEL_TILES)
-    bool shared_scans = true;
-    size_t share_extra_max = 32768;  // largest accumulator region of a plan that joins a shared scan (TGP_SHARE_EXTRA_MAX)  // batches merge same-table queries into shared scans (TGP_NO_SHARED_SCANS=1: off)
-    bool dense_shapes = true;  // ahead-of-time dense kernels (TGP_NO_DENSE_SHAPES=1 turns them off)
+    // The scan variant used when no tuned entry matches a query's class.
+    tgp::Knobs knobs;
+    // Tuned variants by query class (tgp_autotune / tgp_tune_set).
+    std::unordered_map<uint64_t, tgp::Knobs> tuned;
+    // While the autotuner measures a candidate: the knobs every plan takes.
+    const tgp::Knobs* force_knobs = nullptr;
+    // Batch shaping (tgp_batch_config).
+    int morsel_tiles = 16;           // batch morsel length in tiles
+    bool shared_scans = true;        // batches merge same-table queries into shared scans
+    size_t share_extra_max = 32768;  // largest accumulator region of a plan that joins a shared scan
 };

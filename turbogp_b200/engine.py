@@ -407,6 +407,64 @@ class Context:
         self._check(fn(self.h, descs, len(names), rows, C.byref(tid)), "tgp_table_register")
         return Table(self, int(tid.value), names, rows, dtypes, keep if device else None)
 
+    # -- scan variants and the autotuner --------------------------------------
+    def set_default_variant(self, **knobs) -> None:
+        """Sets knobs of the variant used by queries without a tuned entry
+        (fields of tgp_variant: threads, max_stages, placement, presum, dense,
+        shapes, payload, ctas_per_sm, l2_ahead); others keep their values."""
+        v = A.Variant()
+        self._check(self.lib.tgp_get_default_variant(self.h, C.byref(v)), "tgp_get_default_variant")
+        for k, val in knobs.items():
+            setattr(v, k, int(val))
+        self._check(self.lib.tgp_set_default_variant(self.h, C.byref(v)), "tgp_set_default_variant")
+
+    def batch_config(self, morsel_tiles: int = 16, shared_scans: bool = True, share_extra_max: int = 32768) -> None:
+        self._check(self.lib.tgp_batch_config(self.h, morsel_tiles, 1 if shared_scans else 0, share_extra_max),
+                    "tgp_batch_config")
+
+    def autotune(self, pq: "PreparedQuery", reps: int = 5) -> dict:
+        """Measures the scan variants of a prepared query's class
+        (tgp_autotune), installs the fastest one that returns the planner's
+        result bit for bit, and reports every candidate."""
+        cap = 64
+        entries = (A.TuneEntry * cap)()
+        n, best, key = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        self._check(self.lib.tgp_autotune(self.h, C.byref(pq.q), reps, entries, cap, C.byref(n), C.byref(best),
+                                          C.byref(key)), "tgp_autotune")
+        cands = [{"variant": variant_dict(entries[i].variant), "ms": entries[i].ms, "status": entries[i].status,
+                  "same_result": bool(entries[i].same_result), "threads": entries[i].threads_used,
+                  "stages": entries[i].stages_used, "mode": MODE_NAMES.get(entries[i].mode_used, "?")}
+                 for i in range(min(n.value, cap))]
+        return {"class": int(key.value), "candidates": cands, "best": int(best.value),
+                "rule_ms": cands[0]["ms"] if cands else None,
+                "best_ms": cands[best.value]["ms"] if best.value < len(cands) else None}
+
+    def tuned_variants(self) -> dict[int, dict]:
+        """The tuned entries: {class key: variant fields}."""
+        n = C.c_uint32()
+        self._check(self.lib.tgp_tune_count(self.h, C.byref(n)), "tgp_tune_count")
+        out = {}
+        for i in range(n.value):
+            k, v = C.c_uint64(), A.Variant()
+            self._check(self.lib.tgp_tune_at(self.h, i, C.byref(k), C.byref(v)), "tgp_tune_at")
+            out[int(k.value)] = variant_dict(v)
+        return out
+
+    def save_tuning(self, path) -> None:
+        """Writes the tuned entries as JSON (the autotuner's cache)."""
+        save_tuning_file(path, self.tuned_variants())
+
+    def load_tuning(self, path) -> int:
+        """Installs the entries of a JSON cache written by save_tuning;
+        returns how many."""
+        entries = load_tuning_file(path)
+        for key, fields in entries.items():
+            v = A.Variant()
+            for f, val in fields.items():
+                setattr(v, f, int(val))
+            self._check(self.lib.tgp_tune_set(self.h, key, C.byref(v)), "tgp_tune_set")
+        return len(entries)
+
     # -- kernel-table boundary ------------------------------------------------
     def kernel_execute(self, op: int, input_ptr: int, output_ptr: int | None, params: A.KernelParams):
         r = A.KernelResultC()
@@ -416,6 +474,41 @@ class Context:
 
     def hash_table_free(self, handle: int) -> None:
         self._check(self.lib.tgp_hash_table_free(self.h, C.c_void_p(handle)), "tgp_hash_table_free")
+
+
+MODE_NAMES = {2: "private", 3: "shared", 4: "global", 5: "hash"}
+VARIANT_FIELDS = ("threads", "max_stages", "placement", "presum", "dense", "shapes", "payload", "ctas_per_sm",
+                  "l2_ahead")
+
+
+def variant_dict(v) -> dict:
+    return {f: int(getattr(v, f)) for f in VARIANT_FIELDS}
+
+
+def save_tuning_file(path, entries: dict) -> None:
+    """The autotuner's cache: {"version": 1, "entries": [{"class": key,
+    "variant": {...}}, ...]} in ascending class order."""
+    import json
+    doc = {"version": 1, "entries": [{"class": int(k), "variant": {f: int(v[f]) for f in VARIANT_FIELDS}}
+                                     for k, v in sorted(entries.items())]}
+    with open(path, "w") as fh:
+        json.dump(doc, fh, indent=1)
+
+
+def load_tuning_file(path) -> dict:
+    import json
+    with open(path) as fh:
+        doc = json.load(fh)
+    if doc.get("version") != 1:
+        raise ValueError("unknown tuning cache version")
+    out = {}
+    for e in doc["entries"]:
+        v = e["variant"]
+        unknown = set(v) - set(VARIANT_FIELDS)
+        if unknown:
+            raise ValueError(f"unknown variant fields {sorted(unknown)}")
+        out[int(e["class"])] = {f: int(v.get(f, 0)) for f in VARIANT_FIELDS}
+    return out
 
 
 def string_cell(v: str | bytes) -> int:
