@@ -1,11 +1,12 @@
 """Serving loop over resident tables: continuous batching with memory-budget
 admission, against plain one-query-at-a-time execution.
 
-Requests arrive open-loop (Poisson); each names a query template and its
-literals. The batched server keeps a queue; whenever fewer than
-``max_inflight`` batches are running it admits queued requests in arrival
-order while their estimated device memory (group hash tables, join payloads,
-result blocks) fits the budget, submits them as one ``tgp_batch_submit``, and
+Requests arrive open-loop (Poisson) from a list, or live from a queue (the
+wire front-end); each names a query template and its literals. The batched
+server keeps a queue; whenever fewer than ``max_inflight`` batches are running
+it admits queued requests in arrival order while the device memory their plans
+need (``tgp_query_footprint``: group hash tables, join payloads, result
+blocks) fits the budget, submits them as one ``tgp_batch_submit``, and
 completes batches with ``tgp_batch_poll``. Requests of a heavy template (a
 high-cardinality GROUP BY, whose result is gathered, sorted and copied back
 inside the call) go to a heavy lane instead: a worker thread running them one
@@ -13,6 +14,10 @@ by one on their own context, i.e. their own CUDA stream, so that the batching
 loop keeps admitting and completing the light requests meanwhile. A request's
 latency is its completion time minus its arrival time. The plain server runs
 each request alone with ``tgp_execute`` in arrival order.
+
+A request with ``keep`` set gets its decoded result (``QueryOutput``) in
+``result`` (or the exception its query raised); one with an ``event`` has it
+set when done — that is how the wire front-end's connection threads wait.
 """
 from __future__ import annotations
 
@@ -34,6 +39,9 @@ class Request:
     template: str
     where: object                  # Pred for rebind
     done: float = -1.0
+    keep: bool = False             # decode the result and keep it in `result`
+    result: object = None          # QueryOutput, or the exception the query raised
+    event: threading.Event | None = None
 
 
 @dataclass
@@ -42,12 +50,15 @@ class Template:
     flight), each rebound to the request's predicate. ``mem_bytes`` is the
     device memory a running query of this shape holds: by default the
     planner's own estimate for it (``PreparedQuery.footprint``:
-    tgp_query_footprint), taken from the first prepared query."""
+    tgp_query_footprint), taken from the first prepared query. ``solo``, when
+    set, runs a request outside the batches (ORDER BY ... LIMIT statements):
+    solo(request) -> QueryOutput."""
     name: str
     make: Callable[[], PreparedQuery]
     mem_bytes: int | None = None
     pool: list = field(default_factory=list)
     heavy: bool = False            # served by the heavy lane (its prepared queries live on their own context)
+    solo: Callable | None = None
 
     def take(self) -> PreparedQuery:
         pq = self.pool.pop() if self.pool else self.make()
@@ -86,6 +97,72 @@ def summarize(reqs: list[Request], wall: float) -> dict:
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3)}
 
 
+def _finish(r: Request, t: float, out=None, error: BaseException | None = None) -> None:
+    if r.keep:
+        r.result = error if error is not None else out
+    r.done = t
+    if r.event is not None:
+        r.event.set()
+
+
+# ---------------------------------------------------------------------------
+# Request sources
+# ---------------------------------------------------------------------------
+class ListSource:
+    """Requests with known arrival times (seconds from the run's start)."""
+
+    def __init__(self, reqs: list[Request]):
+        self.reqs, self.nxt = reqs, 0
+
+    def arrived(self, now: float) -> list[Request]:
+        out = []
+        while self.nxt < len(self.reqs) and self.reqs[self.nxt].arrival <= now:
+            out.append(self.reqs[self.nxt])
+            self.nxt += 1
+        return out
+
+    def exhausted(self) -> bool:
+        return self.nxt >= len(self.reqs)
+
+    def wait(self, now: float) -> None:
+        if self.nxt < len(self.reqs):
+            time.sleep(min(max(self.reqs[self.nxt].arrival - now, 0.0), 0.0005))
+
+
+class QueueSource:
+    """Requests offered live by other threads; exhausted once closed and
+    drained."""
+
+    def __init__(self):
+        self._lock = threading.Lock()
+        self._items: deque[Request] = deque()
+        self._ready = threading.Event()
+        self.closed = False
+
+    def offer(self, r: Request) -> None:
+        with self._lock:
+            self._items.append(r)
+        self._ready.set()
+
+    def close(self) -> None:
+        self.closed = True
+        self._ready.set()
+
+    def arrived(self, now: float) -> list[Request]:
+        with self._lock:
+            out = list(self._items)
+            self._items.clear()
+            self._ready.clear()
+        return out
+
+    def exhausted(self) -> bool:
+        with self._lock:
+            return self.closed and not self._items
+
+    def wait(self, now: float) -> None:
+        self._ready.wait(timeout=0.0005)
+
+
 class HeavyLane:
     """A worker thread that runs heavy requests one at a time, in arrival
     order, and stamps their completion times."""
@@ -115,12 +192,18 @@ class HeavyLane:
                 return
             r, tpl = job
             try:
-                pq = tpl.take().rebind(r.where)
-                pq.run(decode=False)
-                r.done = time.perf_counter() - self.t0
-                tpl.give(pq)
-            except BaseException as e:  # surfaced by the serving loop
-                self.error = e
+                if tpl.solo is not None:
+                    out = tpl.solo(r)
+                else:
+                    pq = tpl.take().rebind(r.where)
+                    out = pq.run(decode=r.keep)
+                    tpl.give(pq)
+                _finish(r, time.perf_counter() - self.t0, out)
+            except BaseException as e:  # surfaced by the serving loop (or to the request's waiter)
+                if r.keep:
+                    _finish(r, time.perf_counter() - self.t0, error=e)
+                else:
+                    self.error = e
             with self._lock:
                 self.pending -= 1
 
@@ -129,14 +212,27 @@ class HeavyLane:
         self._thread.join()
 
 
-def serve_batched(ctx: Context, templates: dict[str, Template], reqs: list[Request], mem_budget: int,
-                  max_batch: int = 256, max_inflight: int = 2) -> dict:
+# ---------------------------------------------------------------------------
+# The batching loop
+# ---------------------------------------------------------------------------
+def serve_batched(ctx: Context, templates: dict[str, Template], reqs, mem_budget: int,
+                  max_batch: int = 256, max_inflight: int = 2, t0: float | None = None,
+                  heavy_lane: bool | None = None) -> dict:
+    """Serves `reqs` (a list of Requests with arrival times, or a QueueSource
+    fed live) through continuous batching until every request completed.
+    `heavy_lane` (default: whether any template is heavy) starts the heavy
+    lane; a live source whose templates appear later passes it explicitly."""
+    source = reqs if isinstance(reqs, QueueSource) else ListSource(reqs)
     queue: deque[Request] = deque()
     inflight: deque = deque()      # (handle, [(req, template, pq)])
-    t0 = time.perf_counter()
-    lane = HeavyLane(t0) if any(t.heavy for t in templates.values()) else None
+    t0 = time.perf_counter() if t0 is None else t0
+    if heavy_lane is None:
+        heavy_lane = any(t.heavy for t in templates.values())
+    lane = HeavyLane(t0) if heavy_lane else None
+    seen: list[Request] = []
     try:
-        batches = _serve_loop(ctx, templates, reqs, mem_budget, max_batch, max_inflight, queue, inflight, lane, t0)
+        batches = _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, queue, inflight, lane,
+                              t0, seen)
     finally:
         # On an error, batches still running are completed before returning.
         for h, _ in inflight:
@@ -145,52 +241,79 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs: list[Reque
             lane.close()
     if lane is not None and lane.error is not None:
         raise lane.error
-    out = summarize(reqs, time.perf_counter() - t0)
+    out = summarize(seen, time.perf_counter() - t0)
     out["batches"] = batches
     return out
 
 
-def _serve_loop(ctx, templates, reqs, mem_budget, max_batch, max_inflight, queue, inflight, lane, t0) -> int:
+def _complete(inflight: deque, t0: float, block: bool = False) -> None:
+    """Completes finished batches, oldest first (they finish in order)."""
+    while inflight and (inflight[0][0].poll() if not block else True):
+        h, members = inflight.popleft()
+        outs = h.wait()
+        t = time.perf_counter() - t0
+        for (r, tpl, pq), out in zip(members, outs if outs is not None else [None] * len(members)):
+            _finish(r, t, out)
+            tpl.give(pq)
+        if block:
+            return
+
+
+def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, queue, inflight, lane, t0,
+                seen) -> int:
     """The batching loop of serve_batched; returns the number of batches."""
-    nxt, batches = 0, 0
-    while nxt < len(reqs) or queue or inflight or (lane is not None and lane.busy()):
+    batches = 0
+    while not source.exhausted() or queue or inflight or (lane is not None and lane.busy()):
         if lane is not None and lane.error is not None:
             break
         now = time.perf_counter() - t0
-        while nxt < len(reqs) and reqs[nxt].arrival <= now:
-            r = reqs[nxt]
-            nxt += 1
-            if lane is not None and templates[r.template].heavy:
-                lane.submit(r, templates[r.template])
+        for r in source.arrived(now):
+            seen.append(r)
+            tpl = templates[r.template]
+            if lane is not None and tpl.heavy:
+                lane.submit(r, tpl)
+            elif tpl.solo is not None:
+                # Outside the batches, on this thread (ORDER BY ... LIMIT).
+                try:
+                    out = tpl.solo(r)
+                    _finish(r, time.perf_counter() - t0, out)
+                except Exception as e:
+                    if not r.keep:
+                        raise
+                    _finish(r, time.perf_counter() - t0, error=e)
             else:
                 queue.append(r)
-        # Complete finished batches (oldest first; they finish in order).
-        while inflight and inflight[0][0].poll():
-            h, members = inflight.popleft()
-            t = time.perf_counter() - t0
-            for r, tpl, pq in members:
-                r.done = t
-                tpl.give(pq)
+        _complete(inflight, t0)
         if queue and len(inflight) < max_inflight:
-            members, used = [], sum(m[1].mem_bytes for _, ms in inflight for m in ms)
+            members, used = [], sum(m[1].mem_bytes or 0 for _, ms in inflight for m in ms)
             while queue and len(members) < max_batch:
                 tpl = templates[queue[0].template]
+                pq = tpl.take()
                 if (members or inflight) and used + tpl.mem_bytes > mem_budget:
+                    tpl.give(pq)
                     break                    # admission: wait for memory to be released
                 # (A request larger than the budget runs alone once nothing else does.)
                 r = queue.popleft()
                 used += tpl.mem_bytes
-                members.append((r, tpl, tpl.take().rebind(r.where)))
+                members.append((r, tpl, pq.rebind(r.where)))
             if members:
-                inflight.append((ctx.submit([m[2] for m in members], decode=False), members))
+                keep = any(m[0].keep for m in members)
+                try:
+                    h = ctx.submit([m[2] for m in members], decode=keep)
+                except Exception as e:
+                    if not keep:
+                        raise
+                    for r, tpl, pq in members:
+                        _finish(r, time.perf_counter() - t0, error=e)
+                        tpl.give(pq)
+                    continue
+                inflight.append((h, members))
                 batches += 1
                 continue
         if not queue and inflight:
             continue                         # poll again
         if not queue:
-            wait = reqs[nxt].arrival - (time.perf_counter() - t0) if nxt < len(reqs) else 0.0005
-            if wait > 0:
-                time.sleep(min(wait, 0.0005))
+            source.wait(time.perf_counter() - t0)
     return batches
 
 
@@ -200,9 +323,22 @@ def serve_plain(ctx: Context, templates: dict[str, Template], reqs: list[Request
         now = time.perf_counter() - t0
         if r.arrival > now:
             time.sleep(r.arrival - now)
-        tpl = templates[r.template]
-        pq = tpl.take().rebind(r.where)
-        pq.run(decode=False)
-        r.done = time.perf_counter() - t0
-        tpl.give(pq)
+        run_plain(templates[r.template], r, t0)
     return summarize(reqs, time.perf_counter() - t0)
+
+
+def run_plain(tpl: Template, r: Request, t0: float) -> None:
+    """One request alone: rebind a prepared query of its template, tgp_execute,
+    stamp (and keep) the result."""
+    try:
+        if tpl.solo is not None:
+            out = tpl.solo(r)
+        else:
+            pq = tpl.take().rebind(r.where)
+            out = pq.run(decode=r.keep)
+            tpl.give(pq)
+        _finish(r, time.perf_counter() - t0, out)
+    except Exception as e:
+        if not r.keep:
+            raise
+        _finish(r, time.perf_counter() - t0, error=e)
