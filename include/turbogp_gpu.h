@@ -489,6 +489,21 @@ TGP_API int tgp_hll_estimate(const uint32_t* regs, uint64_t* out);
  * Duplicate keys are kept (join_hash_table.rs:27-30). */
 TGP_API int tgp_join_build(tgp_ctx* ctx, tgp_table_id build_table, uint32_t key_column,
                    const tgp_pred_node* pred, uint32_t npred, tgp_join_id* out);
+/* An inner equi-join of two registered tables, a.key_a = b.key_b, each side
+ * with its own single-table filter: counts both filtered sides on the
+ * device and builds the join table on the side with fewer rows — the left
+ * (a) when it has strictly fewer, else the right (b) — as the reference's
+ * hash_join_with_keys picks its build side for an inner join
+ * (src/engine/query_interpreter/join.rs:557-575) after
+ * join_tables_greedy_core / plan_join_dp ordered a two-table join
+ * (join.rs:250-333, 336-503). *build_is_a says which side was built; the
+ * other side is then the probe side of tgp_execute / tgp_join_probe_pairs
+ * (its filter going into the query's WHERE). *rows_a / *rows_b are the
+ * filtered counts. */
+TGP_API int tgp_join_build_smaller(tgp_ctx* ctx, tgp_table_id table_a, uint32_t key_a, const tgp_pred_node* pred_a,
+                                   uint32_t npred_a, tgp_table_id table_b, uint32_t key_b,
+                                   const tgp_pred_node* pred_b, uint32_t npred_b, tgp_join_id* out,
+                                   uint32_t* build_is_a, uint64_t* rows_a, uint64_t* rows_b);
 TGP_API int tgp_join_drop(tgp_ctx* ctx, tgp_join_id join);
 
 /* Inner equi-join probe that emits the (probe_row, build_row) pairs, as the

@@ -372,6 +372,21 @@ extern "C" {
         npred: u32,
         out: *mut u64,
     ) -> c_int;
+    pub fn tgp_join_build_smaller(
+        ctx: *mut tgp_ctx,
+        table_a: u64,
+        key_a: u32,
+        pred_a: *const tgp_pred_node,
+        npred_a: u32,
+        table_b: u64,
+        key_b: u32,
+        pred_b: *const tgp_pred_node,
+        npred_b: u32,
+        out: *mut u64,
+        build_is_a: *mut u32,
+        rows_a: *mut u64,
+        rows_b: *mut u64,
+    ) -> c_int;
     pub fn tgp_join_drop(ctx: *mut tgp_ctx, join: u64) -> c_int;
     pub fn tgp_join_probe_pairs(
         ctx: *mut tgp_ctx,

@@ -160,6 +160,10 @@ PROTOTYPES = [
     ("tgp_execute_topn", C.c_int,
      [C.c_void_p, C.POINTER(Query), C.c_uint32, C.c_int, C.c_uint64, C.c_void_p, C.POINTER(AggValue),
       C.POINTER(QueryResult)]),
+    ("tgp_join_build_smaller", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(PredNode), C.c_uint32, C.c_uint64, C.c_uint32,
+      C.POINTER(PredNode), C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+      C.POINTER(C.c_uint64)]),
     ("tgp_query_footprint", C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
     ("tgp_set_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),
     ("tgp_get_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),

@@ -2845,6 +2845,35 @@ int tgp_join_build(tgp_ctx* ctx, tgp_table_id build_table, uint32_t key_column, 
     return TGP_OK;
 }
 
+int tgp_join_build_smaller(tgp_ctx* ctx, tgp_table_id table_a, uint32_t key_a, const tgp_pred_node* pred_a,
+                           uint32_t npred_a, tgp_table_id table_b, uint32_t key_b, const tgp_pred_node* pred_b,
+                           uint32_t npred_b, tgp_join_id* out, uint32_t* build_is_a, uint64_t* rows_a,
+                           uint64_t* rows_b) {
+    if (!ctx || !out || !build_is_a || !rows_a || !rows_b) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    const Table *A, *B;
+    TGP_TRY(get_table(ctx, table_a, &A));
+    TGP_TRY(get_table(ctx, table_b, &B));
+    if (key_a >= A->cols.size() || key_b >= B->cols.size()) return fail(ctx, TGP_INVALID_ARG, "key column out of range");
+    // Each side's row count after its own filter (the reference joins the
+    // single-table-filtered tables, join.rs:79-100), counted on the device.
+    uint64_t na = 0, nb = 0;
+    TGP_TRY(filter_impl(ctx, A, pred_a, npred_a, nullptr, nullptr, 0, &na, 0));
+    TGP_TRY(filter_impl(ctx, B, pred_b, npred_b, nullptr, nullptr, 0, &nb, 0));
+    // hash_join_with_keys (join.rs:557-575): an inner join builds on the left
+    // side when it has fewer rows, else on the right.
+    const bool on_a = na < nb;
+    JoinTable J;
+    if (on_a) TGP_TRY(build_join(ctx, A, table_a, key_a, pred_a, npred_a, &J));
+    else TGP_TRY(build_join(ctx, B, table_b, key_b, pred_b, npred_b, &J));
+    const uint64_t id = ctx->next_id++;
+    ctx->joins.emplace(id, J);
+    *out = id;
+    *build_is_a = on_a ? 1u : 0u;
+    *rows_a = na;
+    *rows_b = nb;
+    return TGP_OK;
+}
+
 int tgp_join_drop(tgp_ctx* ctx, tgp_join_id id) {
     if (!ctx) return TGP_INVALID_ARG;
     auto it = ctx->joins.find(id);

@@ -407,6 +407,22 @@ class Context:
         self._check(fn(self.h, descs, len(names), rows, C.byref(tid)), "tgp_table_register")
         return Table(self, int(tid.value), names, rows, dtypes, keep if device else None)
 
+    def join_smaller(self, a: "Table", key_a: str, where_a: "Pred | None", b: "Table", key_b: str,
+                     where_b: "Pred | None") -> "JoinPlan":
+        """Inner join a.key_a = b.key_b with each side's own filter, built on
+        the side with fewer filtered rows (tgp_join_build_smaller, the
+        reference's build-side rule)."""
+        nodes_a, n_a = a.lower_pred(where_a)
+        nodes_b, n_b = b.lower_pred(where_b)
+        jid, on_a, ra, rb = C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+        self._check(self.lib.tgp_join_build_smaller(self.h, a.id, a.index(key_a), nodes_a, n_a, b.id, b.index(key_b),
+                                                    nodes_b, n_b,
+                                                    C.byref(jid), C.byref(on_a), C.byref(ra), C.byref(rb)),
+                    "tgp_join_build_smaller")
+        build, probe = (a, b) if on_a.value else (b, a)
+        return JoinPlan(JoinTable(self, int(jid.value), build), probe, key_b if on_a.value else key_a,
+                        where_b if on_a.value else where_a, bool(on_a.value), int(ra.value), int(rb.value))
+
     # -- scan variants and the autotuner --------------------------------------
     def set_default_variant(self, **knobs) -> None:
         """Sets knobs of the variant used by queries without a tuned entry
@@ -894,3 +910,49 @@ class JoinTable:
                 self.ctx.h, self.id, probe.id, probe.index(probe_key), nodes, n, pr.ctypes.data, br.ctypes.data, m,
                 C.byref(npairs)), "tgp_join_probe_pairs")
         return pr[:m], br[:m]
+
+
+def _flip_side(side: int) -> int:
+    return A.SIDE_BUILD if side == A.SIDE_PROBE else A.SIDE_PROBE
+
+
+def _flip_agg(a: Agg) -> Agg:
+    if a.term is None:
+        return Agg(a.func, None)
+    return Agg(a.func, Term([Factor(f.column, f.mul, f.add, _flip_side(f.side) if f.column is not None else f.side)
+                             for f in a.term.factors]))
+
+
+def _flip_key(k) -> Col:
+    c = k if isinstance(k, Col) else col(k)
+    return Col(c.name, _flip_side(c.side))
+
+
+@dataclass
+class JoinPlan:
+    """An inner join whose build side was chosen by row counts
+    (Context.join_smaller). Queries are written with table a's columns as
+    ``col`` and table b's as ``build_col``; when a was the smaller side (and
+    so was built), the sides are swapped before execution."""
+    join: JoinTable
+    probe: Table
+    probe_key: str
+    probe_where: Pred | None
+    build_is_a: bool
+    rows_a: int
+    rows_b: int
+
+    def aggregate(self, aggs: Sequence[Agg], group_by: Sequence = (), group_cap: int | None = None) -> QueryOutput:
+        if self.build_is_a:
+            aggs = [_flip_agg(a) for a in aggs]
+            group_by = [_flip_key(k) for k in group_by]
+        return self.probe.aggregate(aggs, group_by, self.probe_where, join=self.join, probe_key=self.probe_key,
+                                    group_cap=group_cap)
+
+    def pairs(self) -> tuple[np.ndarray, np.ndarray]:
+        """(row of a, row of b) index pairs in (probe row, build row) order."""
+        pr, br = self.join.probe_pairs(self.probe, self.probe_key, self.probe_where)
+        return (br, pr) if self.build_is_a else (pr, br)
+
+    def drop(self) -> None:
+        self.join.drop()
