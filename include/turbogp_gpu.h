@@ -579,6 +579,33 @@ TGP_API int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id graph, uint64_t* keys_ou
 TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
 
 /* ------------------------------------------------------------------------ */
+/* String columns and LIKE                                                   */
+/* ------------------------------------------------------------------------ */
+
+typedef uint64_t tgp_strings_id;
+
+/* Copies a string column into HBM in the layout of the reference's
+ * StringSearchColumn flat buffer (src/exec/fm_index.rs:273-277): all strings'
+ * bytes back to back (`nbytes`) and n + 1 nondecreasing offsets, string i =
+ * bytes[offsets[i], offsets[i + 1]), offsets[0] = 0, offsets[n] = nbytes.
+ * Host memory. The offsets are checked (TGP_INVALID_ARG otherwise). */
+TGP_API int tgp_strings_register(tgp_ctx* ctx, const uint8_t* bytes, uint64_t nbytes, const uint64_t* offsets,
+                                 uint64_t n, tgp_strings_id* out);
+TGP_API int tgp_strings_drop(tgp_ctx* ctx, tgp_strings_id strings);
+
+/* `column [NOT] LIKE pattern` into a selection bitmap: the reference's LIKE
+ * (the interpreter's like_mask / like, src/engine/query_interpreter/expr.rs:
+ * 1159-1240, 2144-2171): byte-wise, '_' matches one byte, '%' any run of
+ * bytes, a pattern byte equal to the string byte matches it (also '%' or '_'),
+ * no escape character; NOT LIKE is the complement. The pattern is
+ * `pattern_len` bytes (at most 256), not NUL-terminated. bitmap_out: NULL or
+ * (n + 7) / 8 bytes, LSB-first (bitmap.rs:36-40), host or device memory;
+ * *count_out = rows selected. AND it into a WHERE bitmap as the interpreter
+ * does (mask.and_inplace, expr.rs:845-848). */
+TGP_API int tgp_like(tgp_ctx* ctx, tgp_strings_id strings, const char* pattern, uint32_t pattern_len, int negated,
+                     uint8_t* bitmap_out, uint64_t* count_out);
+
+/* ------------------------------------------------------------------------ */
 /* Scan variants and the autotuner                                           */
 /* ------------------------------------------------------------------------ */
 

@@ -415,6 +415,25 @@ extern "C" {
     ) -> c_int;
     pub fn tgp_graph_drop(ctx: *mut tgp_ctx, graph: u64) -> c_int;
 
+    pub fn tgp_strings_register(
+        ctx: *mut tgp_ctx,
+        bytes: *const u8,
+        nbytes: u64,
+        offsets: *const u64,
+        n: u64,
+        out: *mut u64,
+    ) -> c_int;
+    pub fn tgp_strings_drop(ctx: *mut tgp_ctx, strings: u64) -> c_int;
+    pub fn tgp_like(
+        ctx: *mut tgp_ctx,
+        strings: u64,
+        pattern: *const c_char,
+        pattern_len: u32,
+        negated: c_int,
+        bitmap_out: *mut u8,
+        count_out: *mut u64,
+    ) -> c_int;
+
     pub fn tgp_set_default_variant(ctx: *mut tgp_ctx, v: *const tgp_variant) -> c_int;
     pub fn tgp_get_default_variant(ctx: *mut tgp_ctx, v: *mut tgp_variant) -> c_int;
     pub fn tgp_batch_config(ctx: *mut tgp_ctx, morsel_tiles: u32, shared_scans: c_int, share_extra_max: u64) -> c_int;

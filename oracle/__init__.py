@@ -83,6 +83,8 @@ def _sig(lib):
     lib.orc_count_distinct.restype = None
     lib.orc_seq_sum_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
     lib.orc_seq_sum_f64.restype = None
+    lib.orc_like.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_char_p, C.c_uint64, C.c_int, C.c_void_p]
+    lib.orc_like.restype = C.c_uint64
     lib.orc_kernel_execute.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(A.KernelParams),
                                        C.POINTER(A.KernelResultC)]
     return lib
@@ -198,3 +200,24 @@ def count_distinct(cells: np.ndarray, sel_bitmap: np.ndarray | None = None) -> t
                               sel_bitmap.ctypes.data if sel_bitmap is not None else None, C.byref(cnt),
                               C.byref(method))
     return int(cnt.value), ("hll" if method.value else "exact")
+
+
+def flat_strings(values) -> tuple[np.ndarray, np.ndarray]:
+    """(bytes, offsets) of a list of str / bytes: the flat column layout."""
+    bs = [v.encode("utf-8") if isinstance(v, str) else bytes(v) for v in values]
+    offs = np.zeros(len(bs) + 1, dtype=np.uint64)
+    if bs:
+        offs[1:] = np.cumsum([len(b) for b in bs], dtype=np.uint64)
+    return np.frombuffer(b"".join(bs), dtype=np.uint8).copy(), offs
+
+
+def like(values, pattern, negated: bool = False) -> FilterOutput:
+    """``col [NOT] LIKE pattern`` as the reference evaluates it, over a list
+    of strings (or a (bytes, offsets) pair): (count, LSB-first bitmap)."""
+    data, offs = values if isinstance(values, tuple) else flat_strings(values)
+    p = pattern.encode("utf-8") if isinstance(pattern, str) else bytes(pattern)
+    n = offs.shape[0] - 1
+    bm = np.zeros(max(1, (n + 7) // 8), dtype=np.uint8)
+    cnt = _lib().orc_like(data.ctypes.data if data.size else None, offs.ctypes.data, n, p, len(p),
+                          1 if negated else 0, bm.ctypes.data)
+    return FilterOutput(int(cnt), bm[:(n + 7) // 8])

@@ -473,4 +473,46 @@ void orc_seq_sum_f64(const double* terms, const uint32_t* group, uint64_t n, uin
     for (uint64_t i = 0; i < n; ++i) out[group[i]] += terms[i];
 }
 
+// LIKE: the reference's like() (src/engine/query_interpreter/expr.rs:
+// 2144-2171), one string at a time — byte-wise; a pattern byte equal to the
+// string byte or '_' consumes one byte (tested in that order), '%' any run,
+// with the last '%' as the only backtracking point; then trailing '%'s.
+static bool like_bytes(const uint8_t* s, uint64_t n, const uint8_t* p, uint64_t m) {
+    uint64_t si = 0, pi = 0, star_p = UINT64_MAX, star_s = 0;
+    while (si < n) {
+        if (pi < m && (p[pi] == '_' || p[pi] == s[si])) {
+            ++si;
+            ++pi;
+        } else if (pi < m && p[pi] == '%') {
+            star_p = pi;
+            star_s = si;
+            ++pi;
+        } else if (star_p != UINT64_MAX) {
+            pi = star_p + 1;
+            ++star_s;
+            si = star_s;
+        } else {
+            return false;
+        }
+    }
+    while (pi < m && p[pi] == '%') ++pi;
+    return pi == m;
+}
+
+// `col [NOT] LIKE pattern` over a flat string column (bytes + n + 1
+// offsets): LSB-first bitmap of (n + 7) / 8 bytes; returns the count.
+uint64_t orc_like(const uint8_t* bytes, const uint64_t* offs, uint64_t n, const uint8_t* pattern, uint64_t m,
+                  int negated, uint8_t* bitmap) {
+    uint64_t cnt = 0;
+    for (uint64_t i = 0; i < (n + 7) / 8; ++i) bitmap[i] = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const bool hit = like_bytes(bytes + offs[i], offs[i + 1] - offs[i], pattern, m) != (negated != 0);
+        if (hit) {
+            bitmap[i >> 3] |= static_cast<uint8_t>(1u << (i & 7));
+            ++cnt;
+        }
+    }
+    return cnt;
+}
+
 }  // extern "C"

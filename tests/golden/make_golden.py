@@ -22,6 +22,7 @@ AGG = "src/kernel/aggregate.rs"
 JHT = "src/exec/join_hash_table.rs"
 ARITH = "tests/arithmetic_aggregates.rs"
 JOINS = "tests/joins_groupby_orderby.rs"
+FM = "src/exec/fm_index.rs"
 
 ten = {"list": [10, 20, 30, 40, 50, 60, 70, 80, 90, 100]}
 fives = {"list": [1, 5, 5, 3, 5, 7, 8, 5, 9, 10]}
@@ -153,6 +154,21 @@ dispatch_kats = {
     ],
 }
 
+# StringSearchColumn's contains / prefix searches (src/exec/fm_index.rs
+# tests), which are LIKE '%s%' and LIKE 's%' on the interpreter's path.
+urls4 = ["https://google.com/search", "https://yahoo.com", "http://google.com/maps", "https://bing.com"]
+urls3 = ["https://google.com", "http://yahoo.com", "https://bing.com"]
+like_kats = [
+    {"source": f"{FM}:576", "strings": ["google.com", "yahoo.com", "google Maps"], "pattern": "%google%",
+     "expect": [True, False, True]},
+    {"source": f"{FM}:551", "strings": urls4, "pattern": "%google%", "count": 2},
+    {"source": f"{FM}:551", "strings": urls4, "pattern": "%yahoo%", "count": 1},
+    {"source": f"{FM}:551", "strings": urls4, "pattern": "%duckduckgo%", "count": 0},
+    {"source": f"{FM}:564", "strings": urls3, "pattern": "https://%", "count": 2},
+    {"source": f"{FM}:564", "strings": urls3, "pattern": "http://%", "count": 1},
+    {"source": f"{FM}:564", "strings": urls3, "pattern": "ftp://%", "count": 0},
+]
+
 out = {
     "filters": [dict(source=s, dtype=d, coltype=c, column=col, cmp=op, lit=v, expect=e)
                 for s, d, c, col, op, v, e in filters + mix_cases],
@@ -165,6 +181,7 @@ out = {
     "groups": group_kats,
     "join_counts": join_count_kats,
     "dispatch": dispatch_kats,
+    "like": like_kats,
 }
 Path(__file__).with_name("reference_kats.json").write_text(json.dumps(out, indent=1) + "\n")
 print("wrote", sum(len(v) if isinstance(v, list) else 1 for v in out.values()), "groups of cases")

@@ -160,3 +160,36 @@ def test_dispatch_kats(kats):
             assert keys == sorted(keys)
         else:
             assert out.values[0][0].value == c["value"], c["source"]
+
+
+def test_like_kats(kats):
+    """LIKE on the string column: the reference's contains / prefix searches
+    (src/exec/fm_index.rs tests) through the oracle's restatement of like()."""
+    import numpy as np
+    for k in kats["like"]:
+        out = oracle.like(k["strings"], k["pattern"])
+        if "expect" in k:
+            bits = np.unpackbits(out.bitmap, bitorder="little")[:len(k["strings"])]
+            assert bits.astype(bool).tolist() == k["expect"], k["source"]
+        else:
+            assert out.count == k["count"], k["source"]
+
+
+def test_like_semantics_edge_cases():
+    """like() details the reference's loop implies: '_' is one byte, '%' any
+    run, a pattern '%' or '_' also matches itself literally first, trailing
+    '%'s match the empty rest, the empty pattern matches only the empty
+    string, NOT LIKE is the complement."""
+    s = ["", "a", "ab", "abc", "a%c", "a_c", "xabcx", "aXc", "\u00e9t\u00e9"]
+    # "a%c" LIKE 'a%' is false: the string's '%' equals the pattern's '%' and
+    # is consumed literally before the wildcard is considered, leaving no
+    # backtracking point (the reference's loop, expr.rs:2152-2158).
+    cases = {"": [0], "%": list(range(9)), "a": [1], "a%": [1, 2, 3, 5, 7], "%c": [3, 4, 5, 7],
+             "a_c": [3, 4, 5, 7], "a%%c": [3, 4, 5, 7], "%b%": [2, 3, 6], "_": [1], "__": [2],
+             "a%c%": [3, 4, 5, 7], "%%": list(range(9)), "\u00e9%": [8], "_t%": [], "__t%": [8]}
+    for p, want in cases.items():
+        got = oracle.like(s, p)
+        idx = [i for i in range(len(s)) if (got.bitmap[i >> 3] >> (i & 7)) & 1]
+        assert idx == want, (p, idx, want)
+        neg = oracle.like(s, p, negated=True)
+        assert neg.count == len(s) - got.count

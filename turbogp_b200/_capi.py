@@ -165,6 +165,11 @@ PROTOTYPES = [
       C.POINTER(PredNode), C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
       C.POINTER(C.c_uint64)]),
     ("tgp_query_footprint", C.c_int, [C.c_void_p, C.POINTER(Query), C.POINTER(C.c_uint64)]),
+    ("tgp_strings_register", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("tgp_strings_drop", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("tgp_like", C.c_int, [C.c_void_p, C.c_uint64, C.c_char_p, C.c_uint32, C.c_int, C.c_void_p,
+                           C.POINTER(C.c_uint64)]),
     ("tgp_set_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),
     ("tgp_get_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),
     ("tgp_batch_config", C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_uint64]),

@@ -708,4 +708,102 @@ cudaError_t launch_delay(uint64_t ns, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// LIKE over a string column (flat bytes + u64 offsets, the reference's
+// StringSearchColumn flat buffer, src/exec/fm_index.rs:273-277, 388-440).
+// Matching is the reference's like() (src/engine/query_interpreter/expr.rs:
+// 2144-2171): byte-wise, a pattern byte equal to the string byte (tested
+// first, so a '%' or '_' also matches itself) or '_' consumes one byte, '%'
+// any run, with one backtracking point (the last '%').
+// Each warp takes 32 consecutive strings; when their bytes fit its staging
+// buffer they are copied into shared memory with coalesced loads first, and
+// every lane matches its own string from there.
+// ---------------------------------------------------------------------------
+constexpr int kLikeWarps = 8;
+constexpr int kLikeStageBytes = 4096;
+
+// Steps of one match are bounded by (n + 1) * (m + 1) + n + m + 2; a match
+// that would exceed that raises kErrOutputFull on `err` and reports no match
+// (it cannot happen for the algorithm above; the bound keeps the loop finite
+// by construction).
+__device__ __forceinline__ bool like_match(const uint8_t* s, uint32_t n, const uint8_t* p, uint32_t m, uint32_t* err) {
+    uint32_t si = 0, pi = 0, star_p = 0xffffffffu, star_s = 0;
+    const uint64_t limit = static_cast<uint64_t>(n + 1) * (m + 1) + n + m + 2;
+    uint64_t steps = 0;
+    while (si < n) {
+        if (++steps > limit) {
+            atomicOr(err, kErrOutputFull);
+            return false;
+        }
+        const uint8_t c = s[si];
+        if (pi < m && (p[pi] == '_' || p[pi] == c)) {
+            ++si;
+            ++pi;
+        } else if (pi < m && p[pi] == '%') {
+            star_p = pi;
+            star_s = si;
+            ++pi;
+        } else if (star_p != 0xffffffffu) {
+            pi = star_p + 1;
+            ++star_s;
+            si = star_s;
+        } else {
+            return false;
+        }
+    }
+    while (pi < m && p[pi] == '%') ++pi;
+    return pi == m;
+}
+
+__global__ void __launch_bounds__(kLikeWarps * 32) like_kernel(const uint8_t* bytes, const unsigned long long* offs,
+                                                                uint64_t n, const __grid_constant__ LikePattern P,
+                                                                uint32_t negated, uint32_t* bitmap,
+                                                                unsigned long long* count, uint32_t* err) {
+    __shared__ uint8_t stage[kLikeWarps][kLikeStageBytes];
+    __shared__ uint8_t pat[kLikeMaxPattern];
+    for (uint32_t k = threadIdx.x; k < P.len; k += blockDim.x) pat[k] = P.b[k];
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint64_t nwords = (n + 31) / 32;
+    unsigned long long cnt = 0;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * kLikeWarps + w; g < nwords;
+         g += static_cast<uint64_t>(gridDim.x) * kLikeWarps) {
+        const uint64_t row = g * 32 + lane;
+        const bool valid = row < n;
+        const uint64_t end_row = (g * 32 + 32 < n) ? g * 32 + 32 : n;
+        const uint64_t first = offs[g * 32], last = offs[end_row];
+        const uint64_t so = valid ? offs[row] : first;
+        const uint32_t sl = valid ? static_cast<uint32_t>(offs[row + 1] - so) : 0u;
+        bool m = false;
+        if (last - first <= static_cast<uint64_t>(kLikeStageBytes)) {
+            const uint32_t span = static_cast<uint32_t>(last - first);
+            for (uint32_t k = lane; k < span; k += 32) stage[w][k] = bytes[first + k];
+            __syncwarp();
+            if (valid) m = like_match(&stage[w][so - first], sl, pat, P.len, err);
+            __syncwarp();
+        } else if (valid) {
+            m = like_match(bytes + so, sl, pat, P.len, err);
+        }
+        const bool sel = valid && (m != (negated != 0));
+        const uint32_t bits = __ballot_sync(0xffffffffu, sel);
+        if (lane == 0) {
+            bitmap[g] = bits;
+            cnt += __popc(bits);
+        }
+    }
+    if (lane == 0 && cnt) atomicAdd(count, cnt);
+}
+
+cudaError_t launch_like(const uint8_t* bytes, const unsigned long long* offs, uint64_t n, const LikePattern& P,
+                        bool negated, uint32_t* bitmap, unsigned long long* count, uint32_t* err, int sms,
+                        cudaStream_t st) {
+    const uint64_t nwords = (n + 31) / 32;
+    if (nwords == 0) return cudaSuccess;
+    uint64_t blocks = (nwords + kLikeWarps - 1) / kLikeWarps;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    like_kernel<<<static_cast<unsigned>(blocks), kLikeWarps * 32, 0, st>>>(bytes, offs, n, P, negated ? 1u : 0u,
+                                                                          bitmap, count, err);
+    return cudaGetLastError();
+}
+
 }  // namespace tgp

@@ -857,6 +857,11 @@ int tgp_shutdown(tgp_ctx* ctx) {
         for (auto& c : kv.second.cols)
             if (c.owned && c.dptr) cudaFree(c.dptr);
     for (auto& kv : ctx->joins) free_join(ctx, kv.second);
+    for (auto& kv : ctx->strings) {
+        dev_free(ctx, kv.second.offs);
+        dev_free(ctx, kv.second.bytes);
+    }
+    ctx->strings.clear();
     for (void* h : ctx->hash_handles) {
         JoinTable* J = static_cast<JoinTable*>(h);
         free_join(ctx, *J);
@@ -1989,6 +1994,83 @@ int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes
         bytes += max_groups * (8ull * q->ngroup + sizeof(tgp_agg_value) * q->nagg) + 512;  // formatted result
     }
     *device_bytes = bytes;
+    return TGP_OK;
+}
+
+// --------------------------------------------------------------------------
+// String columns and LIKE
+// --------------------------------------------------------------------------
+int tgp_strings_register(tgp_ctx* ctx, const uint8_t* bytes, uint64_t nbytes, const uint64_t* offsets, uint64_t n,
+                         tgp_strings_id* out) {
+    if (!ctx || !out || !offsets || (nbytes && !bytes)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (is_device_ptr(offsets) || (bytes && is_device_ptr(bytes)))
+        return fail(ctx, TGP_INVALID_ARG, "string columns are registered from host memory");
+    // The kernel trusts the offsets: check them here.
+    if (offsets[0] != 0 || offsets[n] != nbytes) return fail(ctx, TGP_INVALID_ARG, "offsets must run from 0 to nbytes");
+    for (uint64_t i = 0; i < n; ++i) {
+        if (offsets[i + 1] < offsets[i]) return fail(ctx, TGP_INVALID_ARG, "offsets must not decrease");
+        if (offsets[i + 1] - offsets[i] >= (1ull << 31)) return fail(ctx, TGP_UNSUPPORTED, "a string of 2 GiB or more");
+    }
+    StringColumn c;
+    c.n = n;
+    c.nbytes = nbytes;
+    if (int st = dev_alloc(ctx, reinterpret_cast<void**>(&c.offs), (n + 1) * 8, "string offsets allocation failed"))
+        return st;
+    if (int st = dev_alloc(ctx, reinterpret_cast<void**>(&c.bytes), std::max<uint64_t>(nbytes, 16), "string bytes allocation failed")) {
+        dev_free(ctx, c.offs);
+        return st;
+    }
+    int st = upload(ctx, c.offs, offsets, (n + 1) * 8);
+    if (st == TGP_OK && nbytes) st = upload(ctx, c.bytes, bytes, nbytes);
+    if (st == TGP_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = fail(ctx, TGP_DEVICE_ERROR, "string upload");
+    if (st != TGP_OK) {
+        dev_free(ctx, c.offs);
+        dev_free(ctx, c.bytes);
+        return st;
+    }
+    const uint64_t id = ctx->next_id++;
+    ctx->strings.emplace(id, c);
+    *out = id;
+    return TGP_OK;
+}
+
+int tgp_strings_drop(tgp_ctx* ctx, tgp_strings_id id) {
+    if (!ctx) return TGP_INVALID_ARG;
+    auto it = ctx->strings.find(id);
+    if (it == ctx->strings.end()) return fail(ctx, TGP_NOT_FOUND, "unknown string column id");
+    cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx, it->second.offs);
+    dev_free(ctx, it->second.bytes);
+    ctx->strings.erase(it);
+    return TGP_OK;
+}
+
+int tgp_like(tgp_ctx* ctx, tgp_strings_id id, const char* pattern, uint32_t pattern_len, int negated,
+             uint8_t* bitmap_out, uint64_t* count_out) {
+    if (!ctx || !count_out || (pattern_len && !pattern)) return fail(ctx, TGP_INVALID_ARG, "null argument");
+    if (pattern_len > kLikeMaxPattern) return fail(ctx, TGP_UNSUPPORTED, "LIKE pattern longer than 256 bytes");
+    auto it = ctx->strings.find(id);
+    if (it == ctx->strings.end()) return fail(ctx, TGP_NOT_FOUND, "unknown string column id");
+    const StringColumn& c = it->second;
+    LikePattern P;
+    std::memset(&P, 0, sizeof(P));
+    P.len = pattern_len;
+    if (pattern_len) std::memcpy(P.b, pattern, pattern_len);
+    const uint64_t nwords = (c.n + 31) / 32;
+    Carve cv;
+    TGP_TRY(arena_reserve(ctx, nwords * 4 + 1024, &cv));
+    unsigned long long* block = cv.take<unsigned long long>(4);   // [count][error]
+    uint32_t* words = cv.take<uint32_t>(std::max<uint64_t>(nwords, 1));
+    TGP_CUDA(cudaMemsetAsync(block, 0, 32, ctx->stream));
+    TGP_CUDA(launch_like(c.bytes, c.offs, c.n, P, negated != 0, words, block, reinterpret_cast<uint32_t*>(block + 1),
+                         ctx->sms, ctx->stream));
+    if (bitmap_out && c.n)
+        TGP_CUDA(cudaMemcpyAsync(bitmap_out, words, (c.n + 7) / 8, cudaMemcpyDefault, ctx->stream));
+    unsigned long long hb[2] = {0, 0};
+    TGP_CUDA(cudaMemcpyAsync(hb, block, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (hb[1]) return fail(ctx, TGP_DEVICE_ERROR, "LIKE matching exceeded its step bound");
+    *count_out = hb[0];
     return TGP_OK;
 }
 

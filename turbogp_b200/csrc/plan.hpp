@@ -366,4 +366,11 @@ inline uint64_t hash_slot(uint64_t key_rel, uint32_t log2cap) {
     return (key_rel * 0x9E3779B97F4A7C15ull) >> (64u - log2cap);
 }
 
+// LIKE pattern bytes, passed by value to the LIKE kernel.
+constexpr uint32_t kLikeMaxPattern = 256;
+struct LikePattern {
+    uint32_t len;
+    uint8_t b[kLikeMaxPattern];
+};
+
 }  // namespace tgp

@@ -80,6 +80,9 @@ cudaError_t topn_hash_groups(const unsigned long long* packed, uint64_t n, const
                              uint64_t* keys_out, tgp_agg_value* vals_out, int sms, cudaStream_t st);
 // One thread that spins on %globaltimer for `ns` nanoseconds (at most 1 ms).
 cudaError_t launch_delay(uint64_t ns, cudaStream_t st);
+cudaError_t launch_like(const uint8_t* bytes, const unsigned long long* offs, uint64_t n, const LikePattern& P,
+                        bool negated, uint32_t* bitmap, unsigned long long* count, uint32_t* err, int sms,
+                        cudaStream_t st);
 cudaError_t launch_fill_slots(unsigned long long* p, uint64_t nslots, const SlotImage& img, int sms, cudaStream_t st);
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
@@ -139,6 +142,15 @@ struct Knobs {
     int l2_ahead = 0;         // L2 bulk prefetch distance in tiles (0 = off)
 };
 
+// A string column resident in HBM: all strings' bytes back to back and n + 1
+// offsets (string i = bytes[offs[i], offs[i + 1])).
+struct StringColumn {
+    uint8_t* bytes = nullptr;
+    unsigned long long* offs = nullptr;
+    uint64_t n = 0;
+    uint64_t nbytes = 0;
+};
+
 // Grow-only device scratch carved per call.
 struct Arena {
     uint8_t* base = nullptr;
@@ -160,6 +172,7 @@ struct tgp_ctx {
     std::string err;
     std::unordered_map<uint64_t, tgp::Table> tables;
     std::unordered_map<uint64_t, tgp::JoinTable> joins;
+    std::unordered_map<uint64_t, tgp::StringColumn> strings;
     uint64_t next_id = 1;
     tgp::Arena arena;
     // Pinned host staging for small readbacks.

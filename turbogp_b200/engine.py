@@ -407,6 +407,26 @@ class Context:
         self._check(fn(self.h, descs, len(names), rows, C.byref(tid)), "tgp_table_register")
         return Table(self, int(tid.value), names, rows, dtypes, keep if device else None)
 
+    def register_strings(self, values) -> "StringColumn":
+        """Copies a string column into HBM (tgp_strings_register): a list of
+        str / bytes, or a (uint8 bytes, uint64 offsets) pair in the flat
+        layout (string i = bytes[offsets[i]:offsets[i + 1]])."""
+        if isinstance(values, tuple):
+            data, offs = values
+        else:
+            bs = [v.encode("utf-8") if isinstance(v, str) else bytes(v) for v in values]
+            offs = np.zeros(len(bs) + 1, dtype=np.uint64)
+            if bs:
+                offs[1:] = np.cumsum([len(b) for b in bs], dtype=np.uint64)
+            data = np.frombuffer(b"".join(bs), dtype=np.uint8)
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        sid = C.c_uint64()
+        self._check(self.lib.tgp_strings_register(self.h, data.ctypes.data if data.size else None, data.size,
+                                                  offs.ctypes.data, offs.size - 1, C.byref(sid)),
+                    "tgp_strings_register")
+        return StringColumn(self, int(sid.value), int(offs.size - 1))
+
     def join_smaller(self, a: "Table", key_a: str, where_a: "Pred | None", b: "Table", key_b: str,
                      where_b: "Pred | None") -> "JoinPlan":
         """Inner join a.key_a = b.key_b with each side's own filter, built on
@@ -956,3 +976,26 @@ class JoinPlan:
 
     def drop(self) -> None:
         self.join.drop()
+
+
+class StringColumn:
+    """A string column resident in HBM (flat bytes + offsets)."""
+
+    def __init__(self, ctx: Context, sid: int, n: int):
+        self.ctx, self.id, self.n = ctx, sid, n
+
+    def like(self, pattern: str | bytes, negated: bool = False) -> FilterOutput:
+        """``col [NOT] LIKE pattern``: (count, LSB-first selection bitmap) —
+        AND the bitmap into a WHERE bitmap (``Table.filter``) as the
+        reference does."""
+        p = pattern.encode("utf-8") if isinstance(pattern, str) else bytes(pattern)
+        bm = np.zeros(max(1, (self.n + 7) // 8), dtype=np.uint8)
+        cnt = C.c_uint64()
+        self.ctx._check(self.ctx.lib.tgp_like(self.ctx.h, self.id, p, len(p), 1 if negated else 0, bm.ctypes.data,
+                                              C.byref(cnt)), "tgp_like")
+        return FilterOutput(int(cnt.value), bm[:(self.n + 7) // 8])
+
+    def drop(self) -> None:
+        if self.id:
+            self.ctx._check(self.ctx.lib.tgp_strings_drop(self.ctx.h, self.id), "tgp_strings_drop")
+            self.id = 0
