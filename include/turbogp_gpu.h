@@ -578,6 +578,15 @@ TGP_API int tgp_graph_launch(tgp_ctx* ctx, tgp_graph_id graph, uint64_t* keys_ou
 
 TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
 
+/* Failure-path test hook (no counterpart in the reference): the next scan
+ * launch of this context does not issue the shared-memory copy of tile
+ * `tile` (of the CTA that owns it), and its bounded device waits give up
+ * after `wait_ns` (1 ms to 1 s) instead of 1 s. The consumers' wait for that
+ * copy runs out, the kernel raises its timeout bit and returns, and the call
+ * returns TGP_TIMEOUT; the context stays usable for the next query. One-shot:
+ * later launches are not affected. A wait that gives up, not a fault. */
+TGP_API int tgp_debug_fail_next_scan(tgp_ctx* ctx, uint64_t tile, uint64_t wait_ns);
+
 /* ------------------------------------------------------------------------ */
 /* String columns and LIKE                                                   */
 /* ------------------------------------------------------------------------ */

@@ -424,6 +424,7 @@ extern "C" {
         out: *mut u64,
     ) -> c_int;
     pub fn tgp_strings_drop(ctx: *mut tgp_ctx, strings: u64) -> c_int;
+    pub fn tgp_debug_fail_next_scan(ctx: *mut tgp_ctx, tile: u64, wait_ns: u64) -> c_int;
     pub fn tgp_like(
         ctx: *mut tgp_ctx,
         strings: u64,

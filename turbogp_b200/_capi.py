@@ -168,6 +168,7 @@ PROTOTYPES = [
     ("tgp_strings_register", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("tgp_strings_drop", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("tgp_debug_fail_next_scan", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
     ("tgp_like", C.c_int, [C.c_void_p, C.c_uint64, C.c_char_p, C.c_uint32, C.c_int, C.c_void_p,
                            C.POINTER(C.c_uint64)]),
     ("tgp_set_default_variant", C.c_int, [C.c_void_p, C.POINTER(Variant)]),

@@ -709,7 +709,19 @@ int profile_begin(tgp_ctx* ctx, std::pair<cudaEvent_t, cudaEvent_t>** ev) {
     return TGP_OK;
 }
 
-int launch(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128) {
+int launch(tgp_ctx* ctx, const Plan& P0, uint32_t mode, bool acc128) {
+    // An armed failure-path hook (tgp_debug_fail_next_scan) applies to this
+    // launch only.
+    Plan armed;
+    const Plan* pp = &P0;
+    if (ctx->dbg_skip_tile1) {
+        armed = P0;
+        armed.skip_tile1 = ctx->dbg_skip_tile1;
+        armed.wait_ns = ctx->dbg_wait_ns;
+        ctx->dbg_skip_tile1 = 0;
+        pp = &armed;
+    }
+    const Plan& P = *pp;
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     if (ntiles == 0) return TGP_OK;
     int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
@@ -1994,6 +2006,15 @@ int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes
         bytes += max_groups * (8ull * q->ngroup + sizeof(tgp_agg_value) * q->nagg) + 512;  // formatted result
     }
     *device_bytes = bytes;
+    return TGP_OK;
+}
+
+int tgp_debug_fail_next_scan(tgp_ctx* ctx, uint64_t tile, uint64_t wait_ns) {
+    if (!ctx) return TGP_INVALID_ARG;
+    if (wait_ns < 1000000ull || wait_ns > 1000000000ull)
+        return fail(ctx, TGP_INVALID_ARG, "wait limit between 1 ms and 1 s");
+    ctx->dbg_skip_tile1 = tile + 1;
+    ctx->dbg_wait_ns = wait_ns;
     return TGP_OK;
 }
 

@@ -108,13 +108,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for phase `parity` of `bar` to complete. Returns false if it did not
-// complete within kWaitLimitNs (the caller records kErrWaitTimeout).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// complete within `limit_ns` (0 = kWaitLimitNs; the caller records
+// kErrWaitTimeout).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t limit = limit_ns ? limit_ns : kWaitLimitNs;
     const uint64_t t0 = global_ns();
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > kWaitLimitNs) return false;
+        if (global_ns() - t0 > limit) return false;
     }
 }
 

@@ -243,6 +243,11 @@ struct alignas(16) Plan {
     uint32_t hash_fast;             // global / hash grouping by one staged key, values SUM / COUNT(col)
                                     // of one staged factor each (at most two): the column path
     uint32_t _pad_end;              // sizeof(Plan) is a multiple of 16
+    // Failure-path test hook (tgp_debug_fail_next_scan): tile + 1 whose stage
+    // copy the producer skips (0 = none), and the bounded waits' limit in ns
+    // (0 = kWaitLimitNs).
+    uint64_t skip_tile1;
+    uint64_t wait_ns;
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 

@@ -204,6 +204,9 @@ struct tgp_ctx {
     tgp::Knobs knobs;
     // Tuned variants by query class (tgp_autotune / tgp_tune_set).
     std::unordered_map<uint64_t, tgp::Knobs> tuned;
+    // Failure-path test hook (tgp_debug_fail_next_scan): armed for one launch.
+    uint64_t dbg_skip_tile1 = 0;
+    uint64_t dbg_wait_ns = 0;
     // While the autotuner measures a candidate: the knobs every plan takes.
     const tgp::Knobs* force_knobs = nullptr;
     // Batch shaping (tgp_batch_config).

@@ -1562,13 +1562,24 @@ __device__ __forceinline__ void pipe_produce(const Plan& P, uint64_t* full, uint
         if (st.n >= S) {
             // Wait until every consumer warp has released the previous use of
             // stage s (one phase earlier).
-            if (!mbar_wait_bounded(&empty[st.s], st.phase ^ 1u)) {
+            if (!mbar_wait_bounded(&empty[st.s], st.phase ^ 1u, P.wait_ns)) {
                 atomicOr(P.err, kErrWaitTimeout);
                 atomicExch(abort_flag, 1u);
                 break;
             }
         }
         if (*reinterpret_cast<volatile uint32_t*>(abort_flag)) break;
+        if (P.skip_tile1 == tl + 1) {
+            // Test hook: this stage's copy is never issued, so the consumers'
+            // bounded wait for it runs out (kErrWaitTimeout), as would a copy
+            // that never lands.
+            ++st.n;
+            if (++st.s == S) {
+                st.s = 0;
+                st.phase ^= 1u;
+            }
+            continue;
+        }
         uint8_t* dst = stages + static_cast<size_t>(st.s) * P.stage_bytes;
         mbar_arrive_expect_tx(&full[st.s], P.stage_bytes);
         for (uint32_t c = 0; c < P.nslots; ++c) {
@@ -1598,7 +1609,7 @@ __device__ __forceinline__ bool pipe_consume(const Plan& P, Sink<MODE, ACC128, N
         if (tl >= ntiles) break;
         if (tl < nfull) {
             bool landed = false;
-            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase);
+            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase, P.wait_ns);
             landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
             if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
                 if (lane == 0) {
@@ -1683,7 +1694,8 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
         const uint32_t S = P.nstages;
         const uint64_t first = st.n > S ? st.n - S : 0;
         for (uint64_t i = first; i < st.n; ++i)
-            if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P.err, kErrWaitTimeout);
+            if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u), P.wait_ns))
+                atomicOr(P.err, kErrWaitTimeout);
         return;
     }
     RegLeaves RL;
@@ -1725,7 +1737,7 @@ __device__ __forceinline__ void consume_group(const Plan* plans, uint32_t np, Si
         uint8_t* stage = nullptr;
         if (staged) {
             bool landed = false;
-            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase);
+            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase, P0.wait_ns);
             landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
             if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
                 if (lane == 0) {
@@ -1802,7 +1814,8 @@ __global__ void __launch_bounds__(NT + 32, 1) batch_kernel(const __grid_constant
             // be in flight when the barriers are invalidated.
             const uint32_t S = P0.nstages;
             for (uint64_t i = st.n > S ? st.n - S : 0; i < st.n; ++i)
-                if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u))) atomicOr(P0.err, kErrWaitTimeout);
+                if (!mbar_wait_bounded(&full[i % S], static_cast<uint32_t>((i / S) & 1u), P0.wait_ns))
+                    atomicOr(P0.err, kErrWaitTimeout);
         } else if (t < static_cast<uint32_t>(NT)) {
             unsigned long long selected[kMaxShare];
             for (uint32_t q = 0; q < np; ++q) selected[q] = 0;

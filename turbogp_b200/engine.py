@@ -407,6 +407,12 @@ class Context:
         self._check(fn(self.h, descs, len(names), rows, C.byref(tid)), "tgp_table_register")
         return Table(self, int(tid.value), names, rows, dtypes, keep if device else None)
 
+    def fail_next_scan(self, tile: int = 0, wait_ns: int = 2_000_000) -> None:
+        """Test hook (tgp_debug_fail_next_scan): the next scan launch skips one
+        tile's stage copy and its bounded waits give up after `wait_ns`, so
+        that call raises TgpError TIMEOUT."""
+        self._check(self.lib.tgp_debug_fail_next_scan(self.h, tile, wait_ns), "tgp_debug_fail_next_scan")
+
     def register_strings(self, values) -> "StringColumn":
         """Copies a string column into HBM (tgp_strings_register): a list of
         str / bytes, or a (uint8 bytes, uint64 offsets) pair in the flat
