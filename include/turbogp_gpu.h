@@ -629,7 +629,8 @@ typedef struct tgp_variant {
                               (8 or 4 rows per thread of a 2,048-row tile) */
     uint32_t max_stages;   /* cap on the shared-memory pipeline stages, 1..8 */
     uint32_t placement;    /* direct groups: 0 = rule, 1 = per-thread private accumulators,
-                              2 = per-CTA shared, 3 = global */
+                              2 = per-CTA shared (64-bit), 3 = global, 4 = per-warp shared tables of
+                              32-bit limbs with native atomics */
     uint32_t presum;       /* 1 = shared pre-aggregation of repeated keys (hash / global grouping) allowed */
     uint32_t dense;        /* 1 = dense column programs (private placement) allowed */
     uint32_t shapes;       /* 1 = ahead-of-time fixed-shape kernels allowed */
@@ -672,7 +673,8 @@ typedef struct tgp_tune_entry {
     uint32_t same_result;   /* 1 = its result equals the planner's rule's, bit for bit */
     uint32_t threads_used;  /* what the plan launched with */
     uint32_t stages_used;
-    uint32_t mode_used;     /* accumulator placement the plan chose: 2 private, 3 shared, 4 global, 5 hash */
+    uint32_t mode_used;     /* accumulator placement the plan chose: 2 private, 3 shared, 4 global, 5 hash,
+                               8 per-warp 32-bit limb tables */
     uint32_t _pad;
 } tgp_tune_entry;
 

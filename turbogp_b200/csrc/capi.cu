@@ -1423,8 +1423,17 @@ struct QueryState {
 // mode and shared-memory layout for a kernel with `static_smem` static bytes.
 // `preseed` (optional) lists columns to stage first, in that order.
 // Result pointers (counters, err, acc, htab) are left for the caller.
+// A bucket key (merged batch queries): group key 0 of the query is a column
+// whose cells map to `nbuckets` buckets through `lut` (device, one u8 per
+// cell of the column's [min, max]).
+struct BucketSpec {
+    const uint8_t* lut;
+    uint32_t nbuckets;
+};
+
 static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem,
-                      const std::vector<uint32_t>* preseed = nullptr, bool dry = false) {
+                      const std::vector<uint32_t>* preseed = nullptr, bool dry = false,
+                      const BucketSpec* bucket = nullptr) {
     if (!ctx || !q) return fail(ctx, TGP_INVALID_ARG, "null argument");
     qs.q = q;
     TGP_TRY(get_table(ctx, q->table, &qs.T));
@@ -1494,7 +1503,11 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         }
         K.min = c.min;
         kmin[k] = c.min;
-        const uint64_t range = static_cast<uint64_t>(c.max) - static_cast<uint64_t>(c.min);
+        uint64_t range = static_cast<uint64_t>(c.max) - static_cast<uint64_t>(c.min);
+        if (k == 0 && bucket) {
+            K.lut = bucket->lut;
+            range = bucket->nbuckets - 1;
+        }
         dom[k] = range == ~0ull ? 0 : range + 1;  // 0 = full 64-bit domain
         D = dom[k] ? D * dom[k] : (static_cast<unsigned __int128>(1) << 64) * D;
         uint32_t bw = 0;
@@ -1503,6 +1516,7 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         total_bits += bw;
     }
     P.ngkey = q->ngroup;
+    if (bucket && D > kDirectMaxGroups) return fail(ctx, TGP_UNSUPPORTED, "bucketed groups beyond the direct limit");
 
     // The query's class and the scan variant for it: a tuned entry if the
     // autotuner measured this class, else the context's default (the
@@ -1573,7 +1587,33 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             const size_t s256 = budget > private_bytes(256) ? (budget - private_bytes(256)) / st : 0;
             if (s512 == 2 && std::min<size_t>(s256, static_cast<size_t>(kn.max_stages)) >= 4) nt = 256;
         }
-        if (nt) {
+        // Per-warp shared tables of 32-bit limbs with native shared atomics
+        // (SUM / COUNT(col) values only): exact when every table's sums stay
+        // below 2^63 in magnitude, which rows x max|value| < 2^63 proves (at
+        // most one build match per probe row). Taken when the private
+        // accumulators do not fit (or a variant asks for it).
+        const uint32_t s32_words = 1 + 2 * P.nval;
+        const uint32_t s32_nt = kn.threads == 256 ? 256u : 512u;
+        auto s32_bytes = [&](uint32_t copies) -> size_t {
+            return static_cast<size_t>(copies) * ngroups_direct * s32_words * 4;
+        };
+        uint32_t s32_copies = 0;
+        {
+            bool ok = !b.unbounded && (!J || J->unique) && kn.placement != 2 && kn.placement != 3 &&
+                      (nt == 0 || kn.placement == 4);
+            for (uint32_t v = 0; ok && v < P.nval; ++v)
+                ok = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
+            const unsigned __int128 bound = static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
+                                            std::max<uint64_t>(b.max_abs_val, 1);
+            ok = ok && bound < (static_cast<unsigned __int128>(1) << 63);
+            if (ok) {
+                const size_t st = P.stage_bytes;
+                uint32_t copies = s32_nt / 32;
+                while (copies > 1 && s32_bytes(copies) + 3 * st > budget) copies >>= 1;
+                if (s32_bytes(copies) + 2 * st <= budget) s32_copies = copies;
+            }
+        }
+        if (nt && !(kn.placement == 4 && s32_copies)) {
             mode = MODE_GROUP_PRIVATE;
             P.nthreads = nt;
             P.count_by_tile = (q->ngroup == 0 && !J) ? 1u : 0u;
@@ -1586,12 +1626,19 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             }
             // Dense column program: int64 partials, no join, no per-row
             // overflow checks.
-            if (!acc128 && (!J || pay_ok) && !P.check_ovf && kn.dense)
+            if (!acc128 && (!J || pay_ok) && !P.check_ovf && kn.dense && !bucket)
                 P.dense_vec = compile_chain(b, pay_ok) ? 1u : 0u;
             // Scalar aggregates prefer the register fast path; a join's dense
             // program implies its payload path.
             if (!acc128) P.shape = scalar_shape_of(P);
             if (!P.shape && P.dense_vec && kn.shapes && (!J || pay_ok)) P.shape = dense_shape_of(P);
+        } else if (s32_copies) {
+            mode = MODE_GROUP_SHARED32;
+            acc128 = false;
+            P.nthreads = s32_nt;
+            P.s32_copies = s32_copies;
+            P.s32_words = s32_words;
+            extra = s32_bytes(s32_copies);
         } else if (kn.placement != 3 && shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;
@@ -1662,7 +1709,7 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     }
     // One staged key and at most two SUM / COUNT(col) values of one staged
     // factor each: the column path of global / hash grouping.
-    if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && P.ngkey == 1 &&
+    if ((mode == MODE_GROUP_HASH || mode == MODE_GROUP_GLOBAL) && !join && !P.check_ovf && P.ngkey == 1 && !bucket &&
         !P.gkey[0].build_side && P.gkey[0].slot >= 0 && P.nval <= 2) {
         bool ok = true;
         for (uint32_t v = 0; v < P.nval; ++v)
@@ -2102,7 +2149,7 @@ static Knobs knobs_from(const tgp_variant& v) {
     Knobs k;
     k.threads = v.threads == 256 ? 256 : v.threads == 512 ? 512 : 0;
     k.max_stages = v.max_stages ? std::min<int>(static_cast<int>(v.max_stages), kMaxStages) : kMaxStages;
-    k.placement = v.placement <= 3 ? static_cast<int>(v.placement) : 0;
+    k.placement = v.placement <= 4 ? static_cast<int>(v.placement) : 0;
     k.presum = v.presum != 0;
     k.dense = v.dense != 0;
     k.shapes = v.shapes != 0;
@@ -2261,7 +2308,7 @@ int tgp_autotune(tgp_ctx* ctx, const tgp_query* q, uint32_t reps, tgp_tune_entry
                     cands.push_back(k);
                 }
             } else {
-                for (int pl : {1, 2, 3}) {
+                for (int pl : {1, 2, 3, 4}) {
                     k.placement = pl;
                     if (pl == 1) {
                         for (bool dn : {true, false}) {
@@ -2382,15 +2429,41 @@ static void pinned_release(tgp_ctx* ctx, uint8_t* p) {
         if (b.p == p) b.busy = false;
 }
 
+// A class of batch queries answered by one merged scan: same table, join,
+// aggregates and group keys, WHERE a conjunction whose literals differ only
+// on one column C. The merged query groups additionally by the bucket of C
+// (cells accepted by the same members share a bucket; a per-cell table maps
+// C to its bucket) under the hull of the members' ranges on C; a member's
+// groups are the exact sums (MIN / MAX: extremes) of the buckets it accepts.
+struct MergeRec {
+    std::vector<uint32_t> members;       // batch item indices (bit k of a mask = members[k])
+    std::vector<uint64_t> bucket_mask;   // per bucket: the members that accept its cells
+    std::vector<uint8_t> hlut;           // bucket of each cell of C's [min, max]
+    std::vector<tgp_pred_node> pred;     // common leaves AND C in the hull
+    std::vector<tgp_group_key> group;    // [C] + the members' group keys
+    tgp_query q{};
+    // Joins: the members' rows_selected count probe rows passing WHERE,
+    // matched or not: a count query per bucket (no join) gives them.
+    std::vector<tgp_group_key> cgroup;
+    tgp_agg count_agg{};
+    tgp_query cq{};
+    bool has_count = false;
+    QueryState qs, cqs;
+    size_t lut_off = 0, block_off = 0, cblock_off = 0;
+};
+
 struct BatchRec {
     tgp_batch_item* items = nullptr;
     uint32_t n = 0;
     std::vector<QueryState> qs;
     std::vector<uint8_t> batched;     // item runs in the persistent launch
     std::vector<size_t> block_off;    // its result block's byte offset in the readback area
+    std::vector<std::unique_ptr<MergeRec>> merges;
+    std::vector<int> merged_of;       // item -> merge record, or -1
     uint8_t* dev = nullptr;
     uint8_t* host = nullptr;
     size_t readback_off = 0;          // host offset of the readback area
+    size_t blocks_off = 0;            // device / host offset of the first result block
     cudaEvent_t done = nullptr;
 };
 
@@ -2404,6 +2477,261 @@ void tgp_batch_free_rec(tgp_ctx* ctx, void* r) {
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
+
+// Whether a cell passes a comparison leaf with its column's comparison type
+// (Int signed, Date unsigned, = / <> bitwise: apply_comparison, expr.rs:
+// 1468-1530; BETWEEN / NOT BETWEEN, expr.rs:687-760).
+static bool leaf_passes(const Column& c, const tgp_pred_node& n, int64_t cell) {
+    const bool sgn = c.coltype == TGP_CT_INT;
+    auto lt = [&](uint64_t a, uint64_t b) {
+        return sgn ? static_cast<int64_t>(a) < static_cast<int64_t>(b) : a < b;
+    };
+    const uint64_t x = static_cast<uint64_t>(cell);
+    switch (n.cmp) {
+        case TGP_CMP_EQ: return x == n.lit;
+        case TGP_CMP_NE: return x != n.lit;
+        case TGP_CMP_LT: return lt(x, n.lit);
+        case TGP_CMP_LE: return !lt(n.lit, x);
+        case TGP_CMP_GT: return lt(n.lit, x);
+        case TGP_CMP_GE: return !lt(x, n.lit);
+        case TGP_CMP_BETWEEN: return !lt(x, n.lit) && !lt(n.lit2, x);
+        default: return lt(x, n.lit) || lt(n.lit2, x);
+    }
+}
+
+// A WHERE program that is a conjunction of leaves (postfix: leaves and ANDs).
+static bool pure_conjunction(const tgp_query* q) {
+    uint32_t leaves = 0, ands = 0;
+    int depth = 0;
+    for (uint32_t i = 0; i < q->npred; ++i) {
+        const tgp_pred_node& nd = q->pred[i];
+        if (nd.kind == TGP_PN_LEAF) {
+            ++leaves;
+            ++depth;
+        } else if (nd.kind == TGP_PN_AND) {
+            if (depth < 2) return false;
+            ++ands;
+            --depth;
+        } else {
+            return false;
+        }
+    }
+    return leaves >= 1 && ands + 1 == leaves && depth == 1;
+}
+
+// The merge class of a query: everything but its leaf literals.
+static std::string merge_key(const tgp_query* q) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    put(&q->table, 8);
+    put(&q->join, 8);
+    put(&q->probe_key_column, 4);
+    put(&q->flags, 4);
+    put(&q->ngroup, 4);
+    put(&q->nagg, 4);
+    if (q->ngroup) put(q->group, sizeof(tgp_group_key) * q->ngroup);
+    if (q->nagg) put(q->aggs, sizeof(tgp_agg) * q->nagg);
+    for (uint32_t i = 0; i < q->npred; ++i) {
+        put(&q->pred[i].kind, 4);
+        put(&q->pred[i].column, 4);
+        put(&q->pred[i].cmp, 4);
+    }
+    return k;
+}
+
+constexpr uint64_t kMergeMaxCells = 1ull << 20;   // bucket table bytes (cells of C's range)
+constexpr uint32_t kMergeMaxBuckets = 255;
+
+// Finds the merge classes among the planned, direct-grouped items of a batch.
+static void find_merges(tgp_ctx* ctx, BatchRec& B) {
+    std::unordered_map<std::string, std::vector<uint32_t>> classes;
+    std::vector<std::string> order;
+    for (uint32_t i = 0; i < B.n; ++i) {
+        const tgp_query* q = B.items[i].query;
+        if (!B.qs[i].b || B.qs[i].mode == MODE_GROUP_HASH || !q->npred || !pure_conjunction(q)) continue;
+        if (q->ngroup + 1 > static_cast<uint32_t>(kMaxGroupKeys)) continue;
+        std::string key = merge_key(q);
+        auto it = classes.find(key);
+        if (it == classes.end()) {
+            order.push_back(key);
+            classes.emplace(key, std::vector<uint32_t>{i});
+        } else {
+            it->second.push_back(i);
+        }
+    }
+    for (const std::string& key : order) {
+        const std::vector<uint32_t>& all = classes[key];
+        if (all.size() < 2) continue;
+        const tgp_query* q0 = B.items[all[0]].query;
+        const Table* T = B.qs[all[0]].T;
+        // The leaves whose literals differ must all be on one column C.
+        int C = -1;
+        bool ok = true;
+        for (uint32_t j = 0; j < q0->npred && ok; ++j) {
+            const tgp_pred_node& a = q0->pred[j];
+            if (a.kind != TGP_PN_LEAF) continue;
+            bool varies = false;
+            for (uint32_t i : all) {
+                const tgp_pred_node& b = B.items[i].query->pred[j];
+                varies = varies || b.lit != a.lit || b.lit2 != a.lit2;
+            }
+            if (!varies) continue;
+            if (C >= 0 && static_cast<uint32_t>(C) != a.column) ok = false;
+            C = static_cast<int>(a.column);
+        }
+        if (!ok) continue;
+        if (C < 0) C = static_cast<int>(q0->pred[0].column);   // identical queries: any leaf column
+        if (static_cast<uint32_t>(C) >= T->cols.size()) continue;
+        const Column& col = T->cols[C];
+        if (col.coltype == TGP_CT_FLOAT || col.min < 0 || col.max < col.min) continue;
+        const uint64_t cells = static_cast<uint64_t>(col.max - col.min) + 1;
+        if (cells > kMergeMaxCells) continue;
+        for (size_t start = 0; start < all.size(); start += 64) {
+            const size_t cnt = std::min<size_t>(64, all.size() - start);
+            if (cnt < 2) break;
+            std::unique_ptr<MergeRec> M(new MergeRec());
+            M->members.assign(all.begin() + start, all.begin() + start + cnt);
+            // Bucket of each cell: members accepting it (bucket 0 = none).
+            std::unordered_map<uint64_t, uint8_t> bucket_of;
+            M->bucket_mask.push_back(0);
+            bucket_of[0] = 0;
+            M->hlut.assign(cells, 0);
+            uint64_t rmin = cells, rmax = 0;
+            bool fits = true;
+            for (uint64_t r = 0; r < cells && fits; ++r) {
+                const int64_t cell = col.min + static_cast<int64_t>(r);
+                uint64_t mask = 0;
+                for (size_t k = 0; k < cnt; ++k) {
+                    const tgp_query* qk = B.items[M->members[k]].query;
+                    bool acc = true;
+                    for (uint32_t j = 0; j < qk->npred && acc; ++j)
+                        if (qk->pred[j].kind == TGP_PN_LEAF && qk->pred[j].column == static_cast<uint32_t>(C))
+                            acc = leaf_passes(col, qk->pred[j], cell);
+                    if (acc) mask |= 1ull << k;
+                }
+                auto it = bucket_of.find(mask);
+                uint8_t b;
+                if (it == bucket_of.end()) {
+                    if (M->bucket_mask.size() > kMergeMaxBuckets) {
+                        fits = false;
+                        break;
+                    }
+                    b = static_cast<uint8_t>(M->bucket_mask.size());
+                    bucket_of.emplace(mask, b);
+                    M->bucket_mask.push_back(mask);
+                } else {
+                    b = it->second;
+                }
+                M->hlut[r] = b;
+                if (mask) {
+                    rmin = std::min(rmin, r);
+                    rmax = std::max(rmax, r);
+                }
+            }
+            if (!fits || rmin > rmax) continue;
+            // Merged WHERE: the common leaves AND C within the hull.
+            for (uint32_t j = 0; j < q0->npred; ++j) {
+                const tgp_pred_node& nd = q0->pred[j];
+                if (nd.kind != TGP_PN_LEAF || nd.column == static_cast<uint32_t>(C)) continue;
+                M->pred.push_back(nd);
+                if (M->pred.size() > 1) {
+                    tgp_pred_node a{};
+                    a.kind = TGP_PN_AND;
+                    M->pred.push_back(a);
+                }
+            }
+            tgp_pred_node hull{};
+            hull.kind = TGP_PN_LEAF;
+            hull.column = static_cast<uint32_t>(C);
+            hull.cmp = TGP_CMP_BETWEEN;
+            hull.lit = static_cast<uint64_t>(col.min + static_cast<int64_t>(rmin));
+            hull.lit2 = static_cast<uint64_t>(col.min + static_cast<int64_t>(rmax));
+            M->pred.push_back(hull);
+            if (M->pred.size() > 1) {
+                tgp_pred_node a{};
+                a.kind = TGP_PN_AND;
+                M->pred.push_back(a);
+            }
+            tgp_group_key bk{};
+            bk.column = static_cast<uint32_t>(C);
+            bk.side = TGP_SIDE_PROBE;
+            M->group.push_back(bk);
+            for (uint32_t k = 0; k < q0->ngroup; ++k) M->group.push_back(q0->group[k]);
+            M->q = *q0;
+            M->q.pred = M->pred.data();
+            M->q.npred = static_cast<uint32_t>(M->pred.size());
+            M->q.group = M->group.data();
+            M->q.ngroup = static_cast<uint32_t>(M->group.size());
+            if (q0->join) {
+                M->has_count = true;
+                M->cgroup.push_back(bk);
+                M->count_agg.func = TGP_AGG_COUNT_STAR;
+                M->cq = M->q;
+                M->cq.join = 0;
+                M->cq.group = M->cgroup.data();
+                M->cq.ngroup = 1;
+                M->cq.aggs = &M->count_agg;
+                M->cq.nagg = 1;
+            }
+            B.merges.push_back(std::move(M));
+        }
+    }
+    (void)ctx;
+}
+
+// A member's result block [counters 4][error 2][accumulators] rebuilt from
+// the merged blocks: each group's slots summed (MIN / MAX: extremes) over the
+// buckets the member accepts, values as full int128 limbs.
+static void member_block(const MergeRec& M, size_t k, const QueryState& mqs, const unsigned long long* hb,
+                         const unsigned long long* hc, const QueryState& cqs,
+                         std::vector<unsigned long long>* out) {
+    const Plan& MP = M.qs.b->P;
+    const uint32_t nv1 = mqs.nv1;
+    const uint64_t D = mqs.ngroups_direct;
+    out->assign(6 + D * nv1 * 2, 0);
+    unsigned long long* blk = out->data();
+    blk[4] = hb[4] | (hc ? hc[4] : 0);
+    const unsigned long long* macc = hb + 6;
+    auto read = [&](uint64_t slot, bool sum64) -> __int128 {
+        const uint64_t lo = macc[2 * slot];
+        const int64_t hi = sum64 ? (static_cast<int64_t>(lo) >> 63) : static_cast<int64_t>(macc[2 * slot + 1]);
+        return static_cast<__int128>((static_cast<unsigned __int128>(static_cast<uint64_t>(hi)) << 64) | lo);
+    };
+    __int128 selected = 0;
+    for (uint64_t g = 0; g < D; ++g)
+        for (uint32_t v = 0; v < nv1; ++v) {
+            const uint8_t kind = v == 0 ? VK_SUM : MP.val[v - 1].kind;
+            const bool ext = kind == VK_MIN || kind == VK_MAX;
+            __int128 acc = ext ? (kind == VK_MIN ? static_cast<__int128>(0x7fffffffffffffffll)
+                                                 : static_cast<__int128>(static_cast<int64_t>(0x8000000000000000ull)))
+                               : 0;
+            for (size_t b = 1; b < M.bucket_mask.size(); ++b) {
+                if (!((M.bucket_mask[b] >> k) & 1)) continue;
+                const uint64_t slot = (b * D + g) * nv1 + v;
+                if (ext) {
+                    const int64_t x = static_cast<int64_t>(macc[2 * slot]);
+                    acc = kind == VK_MIN ? std::min<__int128>(acc, x) : std::max<__int128>(acc, x);
+                } else {
+                    acc += read(slot, MP.sum64 != 0);
+                }
+            }
+            if (v == 0 && !M.has_count) selected += acc;
+            const uint64_t o = 6 + (g * nv1 + v) * 2;
+            blk[o] = static_cast<uint64_t>(acc);
+            blk[o + 1] = ext ? 0 : static_cast<uint64_t>(acc >> 64);
+        }
+    if (M.has_count) {
+        const Plan& CP = cqs.b->P;
+        for (size_t b = 1; b < M.bucket_mask.size(); ++b)
+            if ((M.bucket_mask[b] >> k) & 1) {
+                const uint64_t slot = b * cqs.nv1;   // the bucket's row count
+                const uint64_t lo = hc[6 + 2 * slot];
+                const int64_t hi = CP.sum64 ? 0 : static_cast<int64_t>(hc[6 + 2 * slot + 1]);
+                selected += static_cast<__int128>((static_cast<unsigned __int128>(static_cast<uint64_t>(hi)) << 64) | lo);
+            }
+    }
+    blk[0] = static_cast<uint64_t>(selected);
+}
 
 int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_id* out) {
     if (!ctx || !out || (n && !items)) return fail(ctx, TGP_INVALID_ARG, "null argument");
@@ -2439,9 +2767,38 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         it.status = st;
         B->qs[i].b.reset();
     }
+    // Merged scans: each class of same-shape queries becomes one grouped scan
+    // (plus a per-bucket count scan for joins), planned as a query of its own.
+    B->merged_of.assign(n, -1);
+    if (ctx->shared_scans) {
+        find_merges(ctx, *B);
+        std::vector<std::unique_ptr<MergeRec>> kept;
+        for (auto& M : B->merges) {
+            // The bucket table's device address is set once the batch region
+            // exists; the plan only needs a non-null placeholder now.
+            const BucketSpec bs{reinterpret_cast<const uint8_t*>(M.get()),
+                                static_cast<uint32_t>(M->bucket_mask.size())};
+            int st = plan_query(ctx, &M->q, M->qs, scan_kernel_static_smem(), nullptr, false, &bs);
+            if (st == TGP_OK) st = size_smem(ctx, M->qs.b->P, M->qs.extra, scan_kernel_static_smem(), &M->qs.kn);
+            if (st == TGP_OK && M->has_count) {
+                st = plan_query(ctx, &M->cq, M->cqs, scan_kernel_static_smem(), nullptr, false, &bs);
+                if (st == TGP_OK) st = size_smem(ctx, M->cqs.b->P, M->cqs.extra, scan_kernel_static_smem(), &M->cqs.kn);
+                if (st == TGP_OK && M->cqs.mode == MODE_GROUP_HASH) st = TGP_UNSUPPORTED;
+            }
+            if (st != TGP_OK || M->qs.mode == MODE_GROUP_HASH) {
+                ctx->err.clear();
+                continue;   // its members run unmerged
+            }
+            bound_presum(ctx, M->qs);
+            if (M->has_count) bound_presum(ctx, M->cqs);
+            for (uint32_t i : M->members) B->merged_of[i] = static_cast<int>(kept.size());
+            kept.push_back(std::move(M));
+        }
+        B->merges = std::move(kept);
+    }
     for (uint32_t i = 0; i < n; ++i) {
         QueryState& qs = B->qs[i];
-        if (!qs.b) continue;
+        if (!qs.b || B->merged_of[i] >= 0) continue;
         const uint64_t T = (qs.b->P.nrows + kTileRows - 1) / kTileRows;
         const bool light = qs.mode == MODE_GROUP_PRIVATE && ((qs.extra + 127) & ~size_t{127}) <= ctx->share_extra_max;
         const bool shared = ctx->shared_scans && light && light_per_table[items[i].query->table] > 1;
@@ -2553,7 +2910,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             plan_index[i] = nplans++;
         }
     for (uint32_t i : solo) B->batched[i] = 1;
-    if (nplans == 0 && solo.empty()) {
+    if (nplans == 0 && solo.empty() && B->merges.empty()) {
         const uint64_t id = ctx->next_id++;
         ctx->batches.emplace(id, B.release());
         *out = id;
@@ -2607,11 +2964,24 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     }
     const size_t counter_off = off;
     off = align256(off + classes.size() * 4);
+    for (auto& M : B->merges) {
+        M->lut_off = off;
+        off = align256(off + M->hlut.size());
+    }
     const size_t blocks_off = off;
+    B->blocks_off = blocks_off;
     for (uint32_t i = 0; i < n; ++i) {
         if (!B->batched[i]) continue;
         B->block_off[i] = off - blocks_off;
         off = align256(off + B->qs[i].block_words() * 8);
+    }
+    for (auto& M : B->merges) {
+        M->block_off = off - blocks_off;
+        off = align256(off + M->qs.block_words() * 8);
+        if (M->has_count) {
+            M->cblock_off = off - blocks_off;
+            off = align256(off + M->cqs.block_words() * 8);
+        }
     }
     const size_t total = off, blocks_bytes = total - blocks_off;
     TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&B->dev), total, "batch allocation failed"));
@@ -2645,10 +3015,34 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     for (size_t k = 0; k < classes.size(); ++k)
         if (!classes[k].morsels.empty())
             std::memcpy(h + morsel_off[k], classes[k].morsels.data(), classes[k].morsels.size() * sizeof(Morsel));
+    // Merged scans: bucket tables, result pointers (the blocks are zero:
+    // merged queries hold no MIN / MAX identities beyond their own images).
+    for (auto& M : B->merges) {
+        std::memcpy(h + M->lut_off, M->hlut.data(), M->hlut.size());
+        auto place = [&](QueryState& qs, size_t boff) {
+            Plan& P = qs.b->P;
+            unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + boff);
+            P.counters = blk;
+            P.err = reinterpret_cast<uint32_t*>(blk + 4);
+            P.acc = blk + 6;
+            P.gkey[0].lut = B->dev + M->lut_off;
+            if (qs.has_minmax()) {
+                std::vector<unsigned long long> img;
+                init_acc_image(P, qs.ngroups_direct, &img);
+                std::memcpy(h + blocks_off + boff + 48, img.data(), img.size() * 8);
+            }
+        };
+        place(M->qs, M->block_off);
+        if (M->has_count) place(M->cqs, M->cblock_off);
+    }
     // 6. One upload, the queries with launches of their own, the persistent
     // launches, one readback.
     TGP_CUDA(cudaMemcpyAsync(B->dev, h, total, cudaMemcpyHostToDevice, ctx->stream));
     for (uint32_t i : solo) TGP_TRY(launch(ctx, B->qs[i].b->P, B->qs[i].mode, B->qs[i].acc128));
+    for (auto& M : B->merges) {
+        TGP_TRY(launch(ctx, M->qs.b->P, M->qs.mode, M->qs.acc128));
+        if (M->has_count) TGP_TRY(launch(ctx, M->cqs.b->P, M->cqs.mode, M->cqs.acc128));
+    }
     for (size_t k = 0; k < classes.size(); ++k) {
         const Class& c = classes[k];
         if (c.morsels.empty()) continue;
@@ -2704,6 +3098,21 @@ int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id id, int wait) {
         const unsigned long long* hb =
             reinterpret_cast<const unsigned long long*>(B->host + B->readback_off + B->block_off[i]);
         itm.status = decode_direct(ctx, B->qs[i], hb, itm.keys_out, itm.vals_out, itm.group_cap, &itm.result);
+    }
+    std::vector<unsigned long long> blk;
+    for (auto& M : B->merges) {
+        const unsigned long long* hb =
+            reinterpret_cast<const unsigned long long*>(B->host + B->readback_off + M->block_off);
+        const unsigned long long* hc =
+            M->has_count ? reinterpret_cast<const unsigned long long*>(B->host + B->readback_off + M->cblock_off)
+                         : nullptr;
+        for (size_t k = 0; k < M->members.size(); ++k) {
+            const uint32_t i = M->members[k];
+            tgp_batch_item& itm = B->items[i];
+            member_block(*M, k, B->qs[i], hb, hc, M->cqs, &blk);
+            itm.status = decode_direct(ctx, B->qs[i], blk.data(), itm.keys_out, itm.vals_out, itm.group_cap,
+                                       &itm.result);
+        }
     }
     tgp_batch_free_rec(ctx, B);
     ctx->batches.erase(it);

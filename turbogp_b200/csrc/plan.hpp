@@ -43,7 +43,8 @@ enum : uint32_t {
     MODE_GROUP_GLOBAL = 4,   // direct-indexed groups, global int128 atomics
     MODE_GROUP_HASH = 5,     // open-addressing global hash table of groups
     MODE_JOIN_BUILD = 6,     // insert selected rows into a join hash table
-    MODE_JOIN_PAIRS = 7      // probe and emit (probe_row, build_row) pairs
+    MODE_JOIN_PAIRS = 7,     // probe and emit (probe_row, build_row) pairs
+    MODE_GROUP_SHARED32 = 8  // direct-indexed groups, per-warp shared tables of 32-bit limbs, native atomics
 };
 
 // A staged column.
@@ -148,6 +149,7 @@ struct GKey {
     const uint8_t* bptr;
     int64_t min;          // key cell minimum (from column statistics)
     uint64_t stride;      // direct modes: multiplier of (cell - min) in the group index
+    const uint8_t* lut;   // bucket key: digit = lut[cell - min] (u8 per cell of [min, max]); null = cell - min
 };
 
 // Register images the scan kernel loads once per plan (host-computed, so a
@@ -243,6 +245,11 @@ struct alignas(16) Plan {
     uint32_t hash_fast;             // global / hash grouping by one staged key, values SUM / COUNT(col)
                                     // of one staged factor each (at most two): the column path
     uint32_t _pad_end;              // sizeof(Plan) is a multiple of 16
+    // MODE_GROUP_SHARED32: tables of s32_words u32 words per group ([count]
+    // [lo, hi] per value), one per s32_copies groups of warps (warp w uses
+    // table w % s32_copies).
+    uint32_t s32_copies;
+    uint32_t s32_words;
     // Failure-path test hook (tgp_debug_fail_next_scan): tile + 1 whose stage
     // copy the producer skips (0 = none), and the bounded waits' limit in ns
     // (0 = kWaitLimitNs).

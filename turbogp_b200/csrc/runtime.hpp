@@ -133,7 +133,8 @@ struct JoinTable {
 struct Knobs {
     int threads = 0;          // consumer threads per CTA: 0 = the planner's rule, else 256 or 512
     int max_stages = kMaxStages;
-    int placement = 0;        // direct groups: 0 = rule, 1 = per-thread private, 2 = per-CTA shared, 3 = global
+    int placement = 0;        // direct groups: 0 = rule, 1 = per-thread private, 2 = per-CTA shared, 3 = global,
+                              // 4 = per-warp shared tables of 32-bit limbs (native atomics)
     bool presum = true;       // shared pre-aggregation for hash / global grouping (when provably exact)
     bool dense = true;        // dense column programs for private placement
     bool shapes = true;       // ahead-of-time fixed-shape kernels

@@ -338,7 +338,9 @@ __device__ __forceinline__ uint32_t group_index(const Plan& P, const uint8_t* st
         const GKey& K = P.gkey[k];
         if (gpay != kNoPay && K.build_side) continue;
         const int64_t c = key_cell<TAIL>(P, K, stage, r0, rl, brow);
-        g += (static_cast<uint64_t>(c) - static_cast<uint64_t>(K.min)) * K.stride;
+        const uint64_t rel = static_cast<uint64_t>(c) - static_cast<uint64_t>(K.min);
+        // A bucket key maps the cell to its bucket through a per-cell table.
+        g += (K.lut ? static_cast<uint64_t>(__ldg(K.lut + rel)) : rel) * K.stride;
     }
     return static_cast<uint32_t>(g);
 }
@@ -587,6 +589,9 @@ struct Sink {
                 w[2 * i] = kind_identity(slot_kind(P, i % nv1));
                 w[2 * i + 1] = 0;
             }
+        } else if (MODE == MODE_GROUP_SHARED32) {
+            uint32_t* tab = reinterpret_cast<uint32_t*>(extra);
+            for (uint32_t i = t; i < P.s32_copies * P.ngroups * P.s32_words; i += NT) tab[i] = 0;
         } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             const uint32_t HS = P.hsm_slots;
             unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
@@ -701,6 +706,26 @@ struct Sink {
                     atomicMax(reinterpret_cast<long long*>(s), static_cast<long long>(x));
                 }
             }
+        } else if (MODE == MODE_GROUP_SHARED32) {
+            // Native 32-bit shared atomics on this warp group's table: the row
+            // count, and per value the low 32 bits (the returned old value
+            // gives the carry) and the signed high 32 bits. The host proved
+            // every table's sums stay below 2^63 in magnitude, so the limbs
+            // recombine exactly.
+            const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
+            uint32_t* tab = reinterpret_cast<uint32_t*>(extra) +
+                            (static_cast<size_t>((t >> 5) % P.s32_copies) * P.ngroups + g) * P.s32_words;
+            atomicAdd(&tab[0], 1u);
+#pragma unroll 1
+            for (uint32_t v = 0; v < P.nval; ++v) {
+                const ValDesc& V = P.val[v];
+                int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
+                if (V.kind == VK_COUNT_NZ) x = x != 0 ? 1 : 0;
+                const uint32_t xl = static_cast<uint32_t>(x);
+                const uint32_t old = atomicAdd(&tab[1 + 2 * v], xl);
+                const int32_t add = static_cast<int32_t>(x >> 32) + ((old + xl < old) ? 1 : 0);
+                if (add) atomicAdd(reinterpret_cast<int*>(&tab[2 + 2 * v]), add);
+            }
         } else if (MODE == MODE_GROUP_GLOBAL) {
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
             if (P.hsm_slots && presum_add<TAIL>(P, extra, g, stage, r0, rl, brow, ovf)) return;
@@ -786,6 +811,30 @@ struct Sink {
                 a.lo = static_cast<uint64_t>(w[2 * idx]);
                 a.hi = w[2 * idx + 1];
                 if (!acc_untouched(a, kind)) acc_global_s(P.acc + 2ull * idx, kind, a, P.sum64 != 0);
+            }
+        } else if (MODE == MODE_GROUP_SHARED32) {
+            consumer_sync<NT>();
+            const uint32_t* tab = reinterpret_cast<const uint32_t*>(extra);
+            const uint32_t W = P.s32_words, G = P.ngroups;
+            for (uint32_t idx = t; idx < G * nv1; idx += NT) {
+                const uint32_t g = idx / nv1, v = idx % nv1;
+                // Sum the copies' limbs: counts as u64; a value as the exact
+                // int64 (hi << 32) + lo of each copy.
+                int64_t sum = 0;
+                for (uint32_t c = 0; c < P.s32_copies; ++c) {
+                    const uint32_t* e = tab + (static_cast<size_t>(c) * G + g) * W;
+                    if (v == 0) {
+                        sum += static_cast<int64_t>(e[0]);
+                    } else {
+                        const uint64_t hi = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(e[2 * v])));
+                        sum = static_cast<int64_t>(static_cast<uint64_t>(sum) + ((hi << 32) | e[2 * v - 1]));
+                    }
+                }
+                if (sum == 0) continue;
+                I128 a;
+                a.lo = static_cast<uint64_t>(sum);
+                a.hi = sum >> 63;
+                acc_global_s(P.acc + 2ull * idx, VK_SUM, a, P.sum64 != 0);
             }
         } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             consumer_sync<NT>();
@@ -1462,7 +1511,8 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     // The scalar kernel (SH = ScalarTag) carries only the register fast path
     // and the generic row loop.
     constexpr bool kScalar = std::is_same<SH, ScalarTag>::value;
-    if constexpr (!kScalar && (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL)) {
+    if constexpr (!kScalar && (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
+                               MODE == MODE_GROUP_SHARED32)) {
         if (!TAIL && P.jpay) {
             uint32_t g[R];
             const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
@@ -1854,6 +1904,7 @@ static const void* select_kernel(uint32_t mode, bool acc128) {
         case MODE_GROUP_PRIVATE:
             return acc128 ? kernel_ptr<MODE_GROUP_PRIVATE, true, NT>() : kernel_ptr<MODE_GROUP_PRIVATE, false, NT>();
         case MODE_GROUP_SHARED: return kernel_ptr<MODE_GROUP_SHARED, false, NT>();
+        case MODE_GROUP_SHARED32: return kernel_ptr<MODE_GROUP_SHARED32, false, NT>();
         case MODE_GROUP_GLOBAL: return kernel_ptr<MODE_GROUP_GLOBAL, false, NT>();
         case MODE_GROUP_HASH: return kernel_ptr<MODE_GROUP_HASH, false, NT>();
         case MODE_JOIN_BUILD: return kernel_ptr<MODE_JOIN_BUILD, false, NT>();

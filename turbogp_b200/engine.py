@@ -518,7 +518,7 @@ class Context:
         self._check(self.lib.tgp_hash_table_free(self.h, C.c_void_p(handle)), "tgp_hash_table_free")
 
 
-MODE_NAMES = {2: "private", 3: "shared", 4: "global", 5: "hash"}
+MODE_NAMES = {2: "private", 3: "shared", 4: "global", 5: "hash", 8: "shared32"}
 VARIANT_FIELDS = ("threads", "max_stages", "placement", "presum", "dense", "shapes", "payload", "ctas_per_sm",
                   "l2_ahead")
 
