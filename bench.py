@@ -18,8 +18,9 @@ its distributions stand in).
 * ``workloads`` — at N=1, one record each for the other workloads at their
   full sizes (filtered grouped aggregate 6M rows, join + grouped aggregate
   60M x 1.5M rows, GROUP BY key over 100M rows, a batch of 256 uneven
-  queries), with the same keys; each record's CPU leg checks the GPU result
-  against the exact checker before its numbers are reported.
+  queries, serving against the plain per-query path), with the same keys;
+  each record's CPU leg checks the GPU result against the exact checker
+  before its numbers are reported.
 
 ``--impl reference`` times that CPU restatement alone (rank 0) and prints its
 own line (with the same ``config``). Under torchrun, each rank scans its own
@@ -384,7 +385,7 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
         j0 = d.join_build("key", tpl.build_where)
         pq = f.prepare(tpl.aggs, tpl.group_by, tpl.where, join=j0, probe_key="fk")
         q = pq
-        probe_only = (pq.run, 16 * n)
+        probe_only = (pq.run, 16 * n, pq)
         tables = [(d, dim), (f, fact)]
         kernel_bytes = 16 * n
         dominant = "scan_kernel join probe + GROUP BY segment (25 groups, payload array)"
@@ -393,7 +394,8 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
         check = lambda out: _check_exact(out, fact, fct, tpl.aggs, tpl.group_by, tpl.where, build, "fk")
         cleanup = [j0.drop, f.drop, d.drop]
     else:  # highcard_group
-        host = datagen.highcard(n, 10_000_000, 1.1, seed=4 + rank)
+        host = shared.get("hc") if shared.get("hc") is not None and rank == 0 else \
+            datagen.highcard(n, 10_000_000, 1.1, seed=4 + rank)
         t = ctx.register(host)
         aggs = [count_star(), sum_(col("value"))]
         q = t.prepare(aggs, ("key",), None, group_cap=10_000_000)
@@ -408,6 +410,10 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
         cleanup = [t.drop]
 
     first = step() if name != "highcard_group" else q.run()
+    # The autotuner measures the dominant scan's variants (each checked
+    # against the planner's result bit for bit) and installs the fastest for
+    # this query class; the timed steps below run it.
+    tune = autotune_summary(ctx, probe_only[2] if probe_only is not None else q)
     for _ in range(args.warmup):
         step()
     steps = args.steps if args.steps != 3000 else 20
@@ -498,7 +504,20 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
     }
     if variant_line is not None:
         rec["variant"] = variant_line
+    rec["autotune"] = tune
     return rec
+
+
+def autotune_summary(ctx, pq, reps: int = 5) -> dict:
+    """tgp_autotune on a prepared query: the planner's rule against the
+    fastest candidate (both gated CUDA-event medians of the scan kernel)."""
+    rep = ctx.autotune(pq, reps=reps)
+    cands = rep["candidates"]
+    best = cands[rep["best"]]
+    return {"rule_ms": rep["rule_ms"], "best_ms": rep["best_ms"], "chosen": best["variant"],
+            "chosen_placement": best["mode"], "chosen_threads": best["threads"], "chosen_stages": best["stages"],
+            "rule_placement": cands[0]["mode"], "candidates": len(cands),
+            "all_same_result": all(c["same_result"] for c in cands if c["status"] == 0)}
 
 
 def _check_exact(out, cols, coltypes, aggs, group_by, where, build=None, probe_key=None) -> dict:
@@ -686,29 +705,35 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
         dist.destroy_process_group()
 
 
-def run_serve(args, world: int, rank: int, local: int) -> None:
+def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict | None = None,
+                  hc_host: dict | None = None) -> dict:
     """Serving: resident 60M-row fact table, 1.5M-row dimension (+ join table)
-    and 100M-row high-cardinality table; an open-loop Poisson stream of
+    and a 100M-row high-cardinality table; open-loop Poisson streams of
     requests (selective scan + sum, filtered grouped aggregate, join + grouped
-    aggregate with random literals; GROUP BY key over the high-cardinality
-    table for 1 in 500) served by the continuous-batching server (shared scans,
-    memory-budget admission) and by plain one-at-a-time execution. value =
-    batched completions/s at the offered rate; p50/p99 of both in the line."""
+    aggregate, each with random literals; GROUP BY key over the
+    high-cardinality table for 1 in 500) served by the continuous-batching
+    server (merged and shared scans, planner-sized admission, a heavy lane on
+    its own context) and by plain one-at-a-time execution.
+
+    Measured: the plain server's capacity (completed q/s with arrivals far
+    above it) and its p50 / p99 at 80 % of that capacity; the batched
+    server's completed q/s and p50 / p99 when offered 5x the plain capacity,
+    and its own capacity. value = the batched completions/s at 5x."""
     import numpy as np
     from turbogp_b200 import datagen, serving, workloads
     from turbogp_b200.engine import Context, col, count_star, sum_
-    ctx = Context(local)
-    n = args.rows if args.rows != ROWS else 60_000_000
-    host = datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
-    f = ctx.register(host, {**datagen.LINEITEM_COLTYPES, "fk": "int"})
-    del host
+    n = args.rows if (args.rows != ROWS and args.workload == "serve") else 60_000_000
+    host = fact_host if fact_host is not None and rank == 0 else datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
+    f = ctx.register({k: v[:n] for k, v in host.items()}, {**datagen.LINEITEM_COLTYPES, "fk": "int"})
     d = ctx.register(datagen.dimension(DIM_ROWS, seed=2 + rank), datagen.DIMENSION_COLTYPES)
     tj = workloads.join_group_agg()
     j = d.join_build("key", tj.build_where)
     # The high-cardinality table lives on a second context (its own stream):
     # the batched server runs its requests in a heavy lane beside the batches.
     ctx_heavy = Context(local)
-    hc = ctx_heavy.register(datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank))
+    hch = hc_host if hc_host is not None and rank == 0 else \
+        datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank)
+    hc = ctx_heavy.register(hch)
     t_scan, t_fga = workloads.selective_scan_sum(), workloads.filtered_group_agg()
     hc_aggs = [count_star(), sum_(col("value"))]
     templates = {
@@ -739,34 +764,53 @@ def run_serve(args, world: int, rank: int, local: int) -> None:
     def stream(rate, count):
         return [request(t) for t in serving.poisson_arrivals(rate, count, rng)]
 
-    rate, count = args.rate, args.requests
+    count = args.requests
     # Warm-up: every template's prepared queries built and sized (the
     # high-cardinality one included), then both paths once.
-    serving.prewarm(templates, [request(0.0) for _ in range(2000)], per_template=3)
-    serving.serve_batched(ctx, templates, stream(rate, 64), mem_budget=args.mem_budget)
-    serving.serve_plain(ctx, templates, stream(rate, 16))
+    serving.prewarm(templates, [request(0.0) for _ in range(2000)], per_template=4)
+    serving.serve_batched(ctx, templates, stream(4000.0, 256), mem_budget=args.mem_budget)
+    serving.serve_plain(ctx, templates, stream(4000.0, 32))
+    # Plain capacity, then plain at 80 % of it.
+    plain_sat = serving.serve_plain(ctx, templates, stream(50_000.0, max(400, count // 4)))
+    cap_p = plain_sat["qps"]
+    plain = serving.serve_plain(ctx, templates, stream(0.8 * cap_p, max(400, count // 2)))
     with ClockSampler(local) as clocks:
-        batched = serving.serve_batched(ctx, templates, stream(rate, count), mem_budget=args.mem_budget)
-    plain = serving.serve_plain(ctx, templates, stream(rate, count))
-    line = {
+        batched = serving.serve_batched(ctx, templates, stream(5.0 * cap_p, count), mem_budget=args.mem_budget)
+    batched_sat = serving.serve_batched(ctx, templates, stream(100_000.0, count), mem_budget=args.mem_budget)
+    rec = {
         "metric": METRIC, "value": batched.get("qps"), "unit": "queries/s", "n_gpus": world,
-        "steps": count, "warmup": 64, "ms_per_step": batched.get("mean_ms"), "higher_is_better": True,
+        "steps": count, "warmup": 256, "ms_per_step": batched.get("mean_ms"), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
-        "config": {"workload": f"serving: Poisson arrivals at {rate:g} q/s of scan+sum / filtered grouped "
-                               f"aggregate / join+grouped aggregate over a resident {n}-row fact table (random "
-                               f"literals) and GROUP BY key over a {args.highcard_rows}-row high-cardinality table "
-                               f"(1 in 500); continuous batching with shared scans, admission budget "
-                               f"{args.mem_budget} B, high-cardinality requests in a heavy lane (own stream)",
-                   "offered_qps": rate, "requests": count},
-        "batched": batched, "plain": plain,
+        "config": {"workload": f"serving: Poisson arrivals of scan+sum / filtered grouped aggregate / join+grouped "
+                               f"aggregate over a resident {n}-row fact table (random literals) and GROUP BY key "
+                               f"over a {args.highcard_rows}-row high-cardinality table (1 in 500); continuous "
+                               f"batching with merged and shared scans, planner-sized admission (budget "
+                               f"{args.mem_budget} B), high-cardinality requests in a heavy lane (own stream)",
+                   "requests": count},
+        "plain_capacity_qps": cap_p,
+        "plain_at_80pct": {**plain, "offered_qps": 0.8 * cap_p},
+        "batched_at_5x": {**batched, "offered_qps": 5.0 * cap_p},
+        "batched_capacity_qps": batched_sat.get("qps"),
+        "qps_ratio_at_5x": (batched.get("qps") or 0) / cap_p if cap_p else None,
+        "p99_batched_le_plain": (batched.get("p99_ms") or 1e9) <= (plain.get("p99_ms") or 0),
         "roofline": None, "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": None,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     j.drop()
     for tpl in templates.values():
         tpl.pool.clear()
+    hc.drop()
     ctx_heavy.close()
+    f.drop()
+    d.drop()
+    return rec
+
+
+def run_serve(args, world: int, rank: int, local: int) -> None:
+    from turbogp_b200.engine import Context
+    ctx = Context(local)
+    rec = measure_serve(ctx, args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(rec), flush=True)
     ctx.close()
 
 
@@ -820,6 +864,7 @@ def run_headline(args, world: int, rank: int, local: int) -> None:
 
     query = table.prepare(tpl.aggs, tpl.group_by, tpl.where)
     first = query.run()
+    tune = autotune_summary(ctx, query)
     # Warm-up.
     for _ in range(args.warmup):
         out = query.run()
@@ -918,6 +963,7 @@ def run_headline(args, world: int, rank: int, local: int) -> None:
         "clocks": clk,
         "gpu_launches": launches,
         "result": {"sum": str(expect[0]), "count": expect[1], **({"check": checked} if checked else {})},
+        "autotune": tune,
     }
     table.drop()
     del host
@@ -927,10 +973,12 @@ def run_headline(args, world: int, rank: int, local: int) -> None:
         from turbogp_b200 import datagen
         recs = {}
         fact = datagen.fact_fk(60_000_000, DIM_ROWS, 0.8, seed=3)
-        shared = {"fact": fact}
+        hc = datagen.highcard(FULL_ROWS["highcard_group"], 10_000_000, 1.1, seed=4)
+        shared = {"fact": fact, "hc": hc}
         for name in ("filtered_group_agg", "join_group_agg", "highcard_group"):
             recs[name] = measure_workload(name, ctx, args, world, rank, local, shared)
         recs["batch"] = measure_batch(ctx, args, world, rank, local, fact_host=fact)
+        recs["serve"] = measure_serve(ctx, args, world, rank, local, fact_host=fact, hc_host=hc)
         line["workloads"] = recs
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -955,8 +1003,8 @@ def main() -> None:
     ap.add_argument("--workload", default="selective_scan_sum",
                     choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
                              "serve"])
-    ap.add_argument("--rate", type=float, default=2000.0, help="serve: offered queries/s")
-    ap.add_argument("--requests", type=int, default=4000, help="serve: requests in the timed stream")
+    ap.add_argument("--rate", type=float, default=2000.0, help="(unused: serve offers multiples of the plain capacity)")
+    ap.add_argument("--requests", type=int, default=3000, help="serve: requests in the batched streams")
     ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
     ap.add_argument("--highcard-rows", type=int, default=100_000_000)
     args = ap.parse_args()
