@@ -529,9 +529,9 @@ struct Builder {
 // continues its running product; any other value starts a new one. Returns
 // false (dense path off) when a factor or key is not staged, more than two
 // keys group, or the program needs more than kMaxSteps steps.
-bool compile_chain(Builder& b, bool build_keys_in_payload) {
+bool compile_chain(Builder& b, bool build_keys_in_payload, uint32_t max_keys = 2) {
     Plan& P = b.P;
-    if (P.ngkey > 2) return false;
+    if (P.ngkey > max_keys) return false;
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         if (P.gkey[k].build_side && build_keys_in_payload) continue;
         if (P.gkey[k].slot < 0 || P.gkey[k].build_side) return false;
@@ -1639,6 +1639,10 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             P.s32_copies = s32_copies;
             P.s32_words = s32_words;
             extra = s32_bytes(s32_copies);
+            // Dense column program (keys of any count, bucket tables, the
+            // join payload's build-side part).
+            if ((!J || pay_ok) && !P.check_ovf && kn.dense)
+                P.dense_vec = compile_chain(b, pay_ok, static_cast<uint32_t>(kMaxGroupKeys)) ? 1u : 0u;
         } else if (kn.placement != 3 && shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;
@@ -2829,6 +2833,28 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         std::vector<uint32_t> q;
         size_t extra = 0;
         bool light = true;
+        bool fast = false;   // every plan: scalar register fast path over the first plan's leaf columns / values
+    };
+    // Scalar plans whose register images differ only in their leaf bounds
+    // and negations (the same statement with other literals) run a shared
+    // tile with the leaf cells loaded once (fast_group_tile).
+    auto fast_plan = [](const QueryState& qs) {
+        const Plan& P = qs.b->P;
+        return !qs.acc128 && P.ngroups == 1 && P.count_by_tile && P.rb.vals_on && P.rb.leaf_n > 0;
+    };
+    auto fast_compatible = [](const Plan& a, const Plan& b) {
+        const RegBlock &x = a.rb, &y = b.rb;
+        if (x.leaf_n != y.leaf_n || x.vals_nv != y.vals_nv || a.flush_limit != b.flush_limit) return false;
+        for (uint32_t i = 0; i < x.leaf_n; ++i)
+            if (x.leaf_soff[i] != y.leaf_soff[i]) return false;
+        for (int v = 0; v < 2; ++v) {
+            if (x.vals_nf[v] != y.vals_nf[v]) return false;
+            for (int f = 0; f < 2; ++f)
+                if (x.vals_soff[v][f] != y.vals_soff[v][f] || x.vals_dt[v][f] != y.vals_dt[v][f] ||
+                    x.vals_mul[v][f] != y.vals_mul[v][f] || x.vals_add[v][f] != y.vals_add[v][f])
+                    return false;
+        }
+        return true;
     };
     std::vector<Group> groups;
     std::unordered_map<uint64_t, std::vector<uint32_t>> by_table;
@@ -2857,6 +2883,8 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             Plan& P = qs.b->P;
             // The int64 batch kernels carry the fixed-shape dense path.
             P.shape = (!qs.acc128 && !qs.J && P.dense_vec && qs.kn.shapes && dense_shape_of(P) == 1) ? 1u : 0u;
+            fill_reg_block(P);
+            const bool fast = fast_plan(qs);
             const size_t extra = (qs.extra + 127) & ~size_t{127};
             Group* g = nullptr;
             // Plans with a large accumulator table (dense grouping, joins) are
@@ -2868,11 +2896,12 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
                     if (k.light && k.acc128 == qs.acc128 && k.nt == P.nthreads && k.q.size() < static_cast<size_t>(kMaxShare) &&
                         items[k.q[0]].query->table == tid &&
                         B->qs[k.q[0]].b->P.stage_bytes == P.stage_bytes &&
+                        k.fast == fast && (!fast || fast_compatible(B->qs[k.q[0]].b->P, P)) &&
                         k.extra + extra + (k.q.size() + 1) * sizeof(Plan) + 2ull * P.stage_bytes + kBarrierBytes + 256 <=
                             budget)
                         g = &k;
             if (!g) {
-                groups.push_back(Group{qs.acc128, P.nthreads, {}, 0, light});
+                groups.push_back(Group{qs.acc128, P.nthreads, {}, 0, light, fast});
                 g = &groups.back();
             }
             g->q.push_back(i);
@@ -2881,6 +2910,8 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     }
     // 3. Shared-memory layout per group: the barriers, the group's plans, the
     // stages, then each plan's accumulator region.
+    for (const Group& g : groups)
+        for (uint32_t i : g.q) B->qs[i].b->P.group_fast = (g.fast && g.q.size() > 1) ? 1u : 0u;
     for (const Group& g : groups) {
         const Plan& P0 = B->qs[g.q[0]].b->P;
         const size_t stage = P0.stage_bytes;

@@ -244,7 +244,8 @@ struct alignas(16) Plan {
     uint64_t out_cap;
     uint32_t hash_fast;             // global / hash grouping by one staged key, values SUM / COUNT(col)
                                     // of one staged factor each (at most two): the column path
-    uint32_t _pad_end;              // sizeof(Plan) is a multiple of 16
+    uint32_t group_fast;            // batch launches: every plan of this plan's morsel group is a scalar
+                                    // fast-path plan with the same register leaf columns and values
     // MODE_GROUP_SHARED32: tables of s32_words u32 words per group ([count]
     // [lo, hi] per value), one per s32_copies groups of warps (warp w uses
     // table w % s32_copies).

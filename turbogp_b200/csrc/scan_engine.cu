@@ -1127,6 +1127,88 @@ __device__ __forceinline__ void chain_private_tile(const Plan& P, uint8_t* extra
 }
 
 // ---------------------------------------------------------------------------
+// Dense tiles of MODE_GROUP_SHARED32: each row's group index (staged keys,
+// bucket tables, the join payload's build-side part) and the value program's
+// steps are computed for the thread's R rows column by column, then the
+// selected rows add to this warp group's table with native 32-bit shared
+// atomics: the row count, and per value the low limb (its returned old value
+// gives the carry) and the signed high limb.
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                               uint32_t m, const uint32_t* gin = nullptr) {
+    constexpr int R = kTileRows / NT;
+    uint32_t g[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
+#pragma unroll 1
+    for (uint32_t k = 0; k < P.ngkey; ++k) {
+        const GKey& K = P.gkey[k];
+        if (K.build_side) continue;   // its part comes with the payload
+        uint32_t x[R];
+        load_cells32<R>(stage + K.soff, K.dtype, t, x);
+        const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
+        if (K.lut) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) g[r] += static_cast<uint32_t>(__ldg(K.lut + (x[r] - mn))) * st;
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
+        }
+    }
+    const uint32_t W = P.s32_words;
+    uint32_t* tab = reinterpret_cast<uint32_t*>(extra) + static_cast<size_t>((t >> 5) % P.s32_copies) * P.ngroups * W;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if ((m >> r) & 1u) atomicAdd(&tab[g[r] * W], 1u);
+    int64_t cur[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) cur[r] = 0;
+#pragma unroll 1
+    for (uint32_t s = 0; s < P.chain.nsteps; ++s) {
+        const ChainStep& S = P.chain.s[s];
+        int64_t f[R];
+        if (S.flags & CS_COL) {
+            if (S.flags & CS_NARROW) {
+                uint32_t x[R];
+                load_cells32<R>(stage + S.soff, S.dtype, t, x);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    f[r] = static_cast<int32_t>(static_cast<uint32_t>(S.mul32) * x[r] + static_cast<uint32_t>(S.add32));
+            } else {
+                int64_t x[R];
+                load_cells64<R>(stage + S.soff, S.dtype, t, x);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    f[r] = (S.flags & CS_IDENT) ? x[r]
+                                                : static_cast<int64_t>(static_cast<uint64_t>(S.mul) * static_cast<uint64_t>(x[r]) +
+                                                                       static_cast<uint64_t>(S.add));
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) f[r] = S.add;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            cur[r] = (S.flags & CS_CHAIN) ? static_cast<int64_t>(static_cast<uint64_t>(cur[r]) * static_cast<uint64_t>(f[r]))
+                                          : f[r];
+        if (S.acc) {
+            const uint32_t w0 = 1u + 2u * (S.acc - 1u);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (!((m >> r) & 1u)) continue;
+                const int64_t x = S.kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : cur[r];
+                uint32_t* e = &tab[g[r] * W + w0];
+                const uint32_t xl = static_cast<uint32_t>(x);
+                const uint32_t old = atomicAdd(e, xl);
+                const int32_t add = static_cast<int32_t>(x >> 32) + ((old + xl < old) ? 1 : 0);
+                if (add) atomicAdd(reinterpret_cast<int*>(e + 1), add);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Dense value programs of a fixed shape. The key dtypes and every step's
 // dtype / flags / kind / value slot are template constants (literals and
 // column offsets still come from the plan), so a tile runs as one
@@ -1516,6 +1598,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
         if (!TAIL && P.jpay) {
             uint32_t g[R];
             const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
+            if constexpr (MODE == MODE_GROUP_SHARED32) {
+                if (P.dense_vec) {
+                    chain_s32_tile<NT>(P, extra, stage, t, hit, g);
+                    return;
+                }
+            }
             if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
                 if (P.dense_vec && __reduce_add_sync(kFull, __popc(hit)) >= 8u * R) {
                     if constexpr (!std::is_void<SH>::value && !kScalar) {
@@ -1554,6 +1642,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
                 if (P.shape) chain_tile_static<NT, SH>(P, extra, stage, t, m, sink);
                 else chain_private_tile<NT>(P, extra, stage, t, m, sink);
             }
+            return;
+        }
+    }
+    if constexpr (MODE == MODE_GROUP_SHARED32) {
+        if (!TAIL && P.dense_vec) {
+            chain_s32_tile<NT>(P, extra, stage, t, m);
             return;
         }
     }
@@ -1770,6 +1864,54 @@ __global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant_
 // shared scan), then merges each plan's partial aggregates into that query's
 // accumulators. Plans are read from global memory (L1-resident, uniform).
 // ---------------------------------------------------------------------------
+// A shared scan whose plans are all scalar fast-path plans over the same
+// register leaf columns and the same values (the same statement with other
+// literals): the tile's leaf cells are loaded once into registers, then each
+// plan only reads its own bounds and tests them. Selected rows (rare for a
+// selective scan) go through the plan's register value path.
+template <int NT>
+__device__ __forceinline__ void fast_group_tile(const Plan* plans, uint32_t np, Sink<MODE_GROUP_PRIVATE, false, NT>* sinks,
+                                                uint8_t* smem, const uint8_t* stage, uint32_t t,
+                                                unsigned long long* selected) {
+    constexpr int R = kTileRows / NT;
+    const Plan& P0 = plans[0];
+    const uint32_t nl = P0.rb.leaf_n;
+    uint32_t x[kRegLeaves][R];
+#pragma unroll
+    for (int i = 0; i < kRegLeaves; ++i) {
+        if (static_cast<uint32_t>(i) >= nl) break;
+        for_chunks<R / 4>(stage + P0.rb.leaf_soff[i], t, [&](uint32_t q, const uint4& v) {
+            x[i][4 * q + 0] = v.x;
+            x[i][4 * q + 1] = v.y;
+            x[i][4 * q + 2] = v.z;
+            x[i][4 * q + 3] = v.w;
+        });
+    }
+    RegVals RV;
+    load_reg_vals<MODE_GROUP_PRIVATE, false>(P0, RV);
+#pragma unroll 1
+    for (uint32_t q = 0; q < np; ++q) {
+        const Plan& P = plans[q];
+        const uint32_t neg = P.rb.leaf_neg;
+        uint32_t m = (R == 32) ? 0xffffffffu : ((1u << R) - 1u);
+#pragma unroll
+        for (int i = 0; i < kRegLeaves; ++i) {
+            if (static_cast<uint32_t>(i) >= nl) break;
+            const uint32_t lo = P.rb.leaf_lo[i], sp = P.rb.leaf_sp[i];
+            uint32_t b = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) b |= in32(x[i][r], lo, sp) << r;
+            m &= ((neg >> i) & 1u) ? ~b : b;
+        }
+        uint8_t* extra = smem + P.extra_off;
+        const uint32_t c = __popc(m);
+        selected[q] += c;
+        priv_counts(extra)[t] += c;   // a scalar aggregate counts rows by popcount
+        for (uint32_t sel = m; sel; sel &= sel - 1)
+            fast_row<NT>(P, RV, extra, stage, R * t + __ffs(sel) - 1, t, sinks[q].upd, sinks[q]);
+    }
+}
+
 template <uint32_t MODE, bool ACC128, int NT, class SH>
 __device__ __forceinline__ void consume_group(const Plan* plans, uint32_t np, Sink<MODE, ACC128, NT>* sinks,
                                               uint8_t* smem, uint64_t* full, uint64_t* empty, uint8_t* stages,
@@ -1798,6 +1940,19 @@ __device__ __forceinline__ void consume_group(const Plan* plans, uint32_t np, Si
             }
             mbar_try_wait(&full[st.s], st.phase);
             stage = stages + static_cast<size_t>(st.s) * P0.stage_bytes;
+        }
+        if constexpr (MODE == MODE_GROUP_PRIVATE && !ACC128) {
+            if (staged && P0.group_fast) {
+                fast_group_tile<NT>(plans, np, sinks, smem, stage, t, selected);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[st.s]);
+                ++st.n;
+                if (++st.s == S) {
+                    st.s = 0;
+                    st.phase ^= 1u;
+                }
+                continue;
+            }
         }
 #pragma unroll 1
         for (uint32_t q = 0; q < np; ++q) {
