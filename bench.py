@@ -413,7 +413,7 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
     # The autotuner measures the dominant scan's variants (each checked
     # against the planner's result bit for bit) and installs the fastest for
     # this query class; the timed steps below run it.
-    tune = autotune_summary(ctx, probe_only[2] if probe_only is not None else q)
+    tune = None if args.no_autotune else autotune_summary(ctx, probe_only[2] if probe_only is not None else q)
     for _ in range(args.warmup):
         step()
     steps = args.steps if args.steps != 3000 else 20
@@ -864,7 +864,7 @@ def run_headline(args, world: int, rank: int, local: int) -> None:
 
     query = table.prepare(tpl.aggs, tpl.group_by, tpl.where)
     first = query.run()
-    tune = autotune_summary(ctx, query)
+    tune = None if args.no_autotune else autotune_summary(ctx, query)
     # Warm-up.
     for _ in range(args.warmup):
         out = query.run()
@@ -1000,6 +1000,7 @@ def main() -> None:
     ap.add_argument("--cpu-sample-rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="headline line only (no `workloads` records)")
+    ap.add_argument("--no-autotune", action="store_true", help="run the planner's rules (profiling captures)")
     ap.add_argument("--workload", default="selective_scan_sum",
                     choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
                              "serve"])

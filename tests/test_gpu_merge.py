@@ -5,7 +5,9 @@ MIN / MAX, rows_selected — equals the query run alone and the oracle's.
 Cases: range, equality, <> and NOT BETWEEN literals (buckets that are not
 intervals), identical queries, empty and full selections, a common extra
 leaf, MIN / MAX values, joins (whose rows_selected needs per-bucket counts),
-and a class larger than 64 queries (split into several merged scans)."""
+a class larger than 64 queries (split into several merged scans), and
+scan queries whose literals differ on three columns (one bucket key per
+column; a member accepts a combination of buckets when it accepts each)."""
 import numpy as np
 import pytest
 
@@ -54,6 +56,11 @@ def test_merged_batches_equal_queries_alone(ctx):
     for c in rng.integers(1, 50, 6):
         specs.append(([count_star(), sum_(col("price_cents") * build_col("segment"))], (build_col("segment"), "flag_b"),
                       q >= int(c), j))
+    for _ in range(40):
+        tpl = workloads.selective_scan_sum(day_lo=D0 + int(rng.integers(0, 2000)), days=int(rng.integers(30, 526)),
+                                           disc_lo=int(rng.integers(0, 6)), disc_hi=int(rng.integers(5, 11)),
+                                           qty_lt=int(rng.integers(2, 51)))
+        specs.append((tpl.aggs, tpl.group_by, tpl.where, None))
     pqs = [f.prepare(a, g, w, join=jj, probe_key="fk" if jj else None) for a, g, w, jj in specs]
     order = rng.permutation(len(pqs))
     batch = [pqs[i] for i in order]

@@ -1423,12 +1423,13 @@ struct QueryState {
 // mode and shared-memory layout for a kernel with `static_smem` static bytes.
 // `preseed` (optional) lists columns to stage first, in that order.
 // Result pointers (counters, err, acc, htab) are left for the caller.
-// A bucket key (merged batch queries): group key 0 of the query is a column
-// whose cells map to `nbuckets` buckets through `lut` (device, one u8 per
-// cell of the column's [min, max]).
+// Bucket keys (merged batch queries): group keys 0 .. nkeys-1 of the query
+// are columns whose cells map to nbuckets[k] buckets through lut[k] (device,
+// one u8 per cell of the column's [min, max]).
 struct BucketSpec {
-    const uint8_t* lut;
-    uint32_t nbuckets;
+    uint32_t nkeys;
+    const uint8_t* lut[kMaxGroupKeys];
+    uint32_t nbuckets[kMaxGroupKeys];
 };
 
 static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t static_smem,
@@ -1504,9 +1505,9 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         K.min = c.min;
         kmin[k] = c.min;
         uint64_t range = static_cast<uint64_t>(c.max) - static_cast<uint64_t>(c.min);
-        if (k == 0 && bucket) {
-            K.lut = bucket->lut;
-            range = bucket->nbuckets - 1;
+        if (bucket && k < bucket->nkeys) {
+            K.lut = bucket->lut[k];
+            range = bucket->nbuckets[k] - 1;
         }
         dom[k] = range == ~0ull ? 0 : range + 1;  // 0 = full 64-bit domain
         D = dom[k] ? D * dom[k] : (static_cast<unsigned __int128>(1) << 64) * D;
@@ -2439,12 +2440,18 @@ static void pinned_release(tgp_ctx* ctx, uint8_t* p) {
 // (cells accepted by the same members share a bucket; a per-cell table maps
 // C to its bucket) under the hull of the members' ranges on C; a member's
 // groups are the exact sums (MIN / MAX: extremes) of the buckets it accepts.
+struct MergeCol {
+    uint32_t column = 0;
+    std::vector<uint64_t> bucket_mask;   // per bucket: the members that accept its cells
+    std::vector<uint8_t> hlut;           // bucket of each cell of the column's [min, max]
+    size_t lut_off = 0;
+};
+
 struct MergeRec {
     std::vector<uint32_t> members;       // batch item indices (bit k of a mask = members[k])
-    std::vector<uint64_t> bucket_mask;   // per bucket: the members that accept its cells
-    std::vector<uint8_t> hlut;           // bucket of each cell of C's [min, max]
-    std::vector<tgp_pred_node> pred;     // common leaves AND C in the hull
-    std::vector<tgp_group_key> group;    // [C] + the members' group keys
+    std::vector<MergeCol> cols;          // the columns whose literals differ, one bucket key each
+    std::vector<tgp_pred_node> pred;     // common leaves AND each column in its hull
+    std::vector<tgp_group_key> group;    // [bucket keys] + the members' group keys
     tgp_query q{};
     // Joins: the members' rows_selected count probe rows passing WHERE,
     // matched or not: a count query per bucket (no join) gives them.
@@ -2453,7 +2460,12 @@ struct MergeRec {
     tgp_query cq{};
     bool has_count = false;
     QueryState qs, cqs;
-    size_t lut_off = 0, block_off = 0, cblock_off = 0;
+    size_t block_off = 0, cblock_off = 0;
+    uint64_t nbucket_tuples() const {
+        uint64_t n = 1;
+        for (const MergeCol& c : cols) n *= c.bucket_mask.size();
+        return n;
+    }
 };
 
 struct BatchRec {
@@ -2543,17 +2555,64 @@ static std::string merge_key(const tgp_query* q) {
     return k;
 }
 
-constexpr uint64_t kMergeMaxCells = 1ull << 20;   // bucket table bytes (cells of C's range)
+constexpr uint64_t kMergeMaxCells = 1ull << 20;   // bucket table bytes (cells of a column's range)
 constexpr uint32_t kMergeMaxBuckets = 255;
+constexpr uint64_t kMergeMaxTuples = 1ull << 14;  // bucket combinations x groups of one merged query
+constexpr size_t kMergeChunk = 64;                // members per merged query (one u64 mask)
 
-// Finds the merge classes among the planned, direct-grouped items of a batch.
+// Builds the bucket table of one varying column for a chunk of members.
+// Returns false if the column cannot be bucketed.
+static bool bucket_column(const BatchRec& B, const std::vector<uint32_t>& members, const Column& col,
+                          uint32_t C, MergeCol* out, uint64_t* rmin_out, uint64_t* rmax_out) {
+    const uint64_t cells = static_cast<uint64_t>(col.max - col.min) + 1;
+    out->column = C;
+    out->bucket_mask.assign(1, 0);
+    out->hlut.assign(cells, 0);
+    std::unordered_map<uint64_t, uint8_t> bucket_of;
+    bucket_of[0] = 0;
+    uint64_t rmin = cells, rmax = 0;
+    for (uint64_t r = 0; r < cells; ++r) {
+        const int64_t cell = col.min + static_cast<int64_t>(r);
+        uint64_t mask = 0;
+        for (size_t k = 0; k < members.size(); ++k) {
+            const tgp_query* qk = B.items[members[k]].query;
+            bool acc = true;
+            for (uint32_t j = 0; j < qk->npred && acc; ++j)
+                if (qk->pred[j].kind == TGP_PN_LEAF && qk->pred[j].column == C) acc = leaf_passes(col, qk->pred[j], cell);
+            if (acc) mask |= 1ull << k;
+        }
+        auto it = bucket_of.find(mask);
+        uint8_t b;
+        if (it == bucket_of.end()) {
+            if (out->bucket_mask.size() > kMergeMaxBuckets) return false;
+            b = static_cast<uint8_t>(out->bucket_mask.size());
+            bucket_of.emplace(mask, b);
+            out->bucket_mask.push_back(mask);
+        } else {
+            b = it->second;
+        }
+        out->hlut[r] = b;
+        if (mask) {
+            rmin = std::min(rmin, r);
+            rmax = std::max(rmax, r);
+        }
+    }
+    if (rmin > rmax) return false;
+    *rmin_out = rmin;
+    *rmax_out = rmax;
+    return true;
+}
+
+// Finds the merge classes among the planned, direct-grouped items of a batch:
+// queries whose literals differ on at most three columns, each with a
+// bounded cell range. A member accepts a combination of buckets when every
+// one of its columns' buckets accepts it.
 static void find_merges(tgp_ctx* ctx, BatchRec& B) {
     std::unordered_map<std::string, std::vector<uint32_t>> classes;
     std::vector<std::string> order;
     for (uint32_t i = 0; i < B.n; ++i) {
         const tgp_query* q = B.items[i].query;
         if (!B.qs[i].b || B.qs[i].mode == MODE_GROUP_HASH || !q->npred || !pure_conjunction(q)) continue;
-        if (q->ngroup + 1 > static_cast<uint32_t>(kMaxGroupKeys)) continue;
         std::string key = merge_key(q);
         auto it = classes.find(key);
         if (it == classes.end()) {
@@ -2568,10 +2627,10 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
         if (all.size() < 2) continue;
         const tgp_query* q0 = B.items[all[0]].query;
         const Table* T = B.qs[all[0]].T;
-        // The leaves whose literals differ must all be on one column C.
-        int C = -1;
-        bool ok = true;
-        for (uint32_t j = 0; j < q0->npred && ok; ++j) {
+        const uint64_t D = B.qs[all[0]].ngroups_direct;
+        // The columns whose leaf literals differ among the members.
+        std::vector<uint32_t> vary;
+        for (uint32_t j = 0; j < q0->npred; ++j) {
             const tgp_pred_node& a = q0->pred[j];
             if (a.kind != TGP_PN_LEAF) continue;
             bool varies = false;
@@ -2579,87 +2638,77 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
                 const tgp_pred_node& b = B.items[i].query->pred[j];
                 varies = varies || b.lit != a.lit || b.lit2 != a.lit2;
             }
-            if (!varies) continue;
-            if (C >= 0 && static_cast<uint32_t>(C) != a.column) ok = false;
-            C = static_cast<int>(a.column);
+            if (varies && std::find(vary.begin(), vary.end(), a.column) == vary.end()) vary.push_back(a.column);
+        }
+        if (vary.empty()) vary.push_back(q0->pred[0].column);   // identical queries: any leaf column
+        if (vary.size() > 3 || q0->ngroup + vary.size() > static_cast<size_t>(kMaxGroupKeys)) continue;
+        bool ok = true;
+        for (uint32_t C : vary) {
+            if (C >= T->cols.size()) { ok = false; break; }
+            const Column& col = T->cols[C];
+            ok = ok && col.coltype != TGP_CT_FLOAT && col.min >= 0 && col.max >= col.min &&
+                 static_cast<uint64_t>(col.max - col.min) + 1 <= kMergeMaxCells;
         }
         if (!ok) continue;
-        if (C < 0) C = static_cast<int>(q0->pred[0].column);   // identical queries: any leaf column
-        if (static_cast<uint32_t>(C) >= T->cols.size()) continue;
-        const Column& col = T->cols[C];
-        if (col.coltype == TGP_CT_FLOAT || col.min < 0 || col.max < col.min) continue;
-        const uint64_t cells = static_cast<uint64_t>(col.max - col.min) + 1;
-        if (cells > kMergeMaxCells) continue;
-        for (size_t start = 0; start < all.size(); start += 64) {
-            const size_t cnt = std::min<size_t>(64, all.size() - start);
+        // Chunks of members, halved until the bucket combinations x groups of
+        // a chunk stay small enough for shared-memory tables.
+        size_t start = 0;
+        size_t chunk = kMergeChunk;
+        while (start + 1 < all.size()) {
+            const size_t cnt = std::min(chunk, all.size() - start);
             if (cnt < 2) break;
             std::unique_ptr<MergeRec> M(new MergeRec());
             M->members.assign(all.begin() + start, all.begin() + start + cnt);
-            // Bucket of each cell: members accepting it (bucket 0 = none).
-            std::unordered_map<uint64_t, uint8_t> bucket_of;
-            M->bucket_mask.push_back(0);
-            bucket_of[0] = 0;
-            M->hlut.assign(cells, 0);
-            uint64_t rmin = cells, rmax = 0;
+            std::vector<std::pair<uint64_t, uint64_t>> hull;
             bool fits = true;
-            for (uint64_t r = 0; r < cells && fits; ++r) {
-                const int64_t cell = col.min + static_cast<int64_t>(r);
-                uint64_t mask = 0;
-                for (size_t k = 0; k < cnt; ++k) {
-                    const tgp_query* qk = B.items[M->members[k]].query;
-                    bool acc = true;
-                    for (uint32_t j = 0; j < qk->npred && acc; ++j)
-                        if (qk->pred[j].kind == TGP_PN_LEAF && qk->pred[j].column == static_cast<uint32_t>(C))
-                            acc = leaf_passes(col, qk->pred[j], cell);
-                    if (acc) mask |= 1ull << k;
+            for (uint32_t C : vary) {
+                MergeCol mc;
+                uint64_t rmin = 0, rmax = 0;
+                if (!bucket_column(B, M->members, T->cols[C], C, &mc, &rmin, &rmax)) {
+                    fits = false;
+                    break;
                 }
-                auto it = bucket_of.find(mask);
-                uint8_t b;
-                if (it == bucket_of.end()) {
-                    if (M->bucket_mask.size() > kMergeMaxBuckets) {
-                        fits = false;
-                        break;
-                    }
-                    b = static_cast<uint8_t>(M->bucket_mask.size());
-                    bucket_of.emplace(mask, b);
-                    M->bucket_mask.push_back(mask);
-                } else {
-                    b = it->second;
-                }
-                M->hlut[r] = b;
-                if (mask) {
-                    rmin = std::min(rmin, r);
-                    rmax = std::max(rmax, r);
-                }
+                hull.push_back({rmin, rmax});
+                M->cols.push_back(std::move(mc));
             }
-            if (!fits || rmin > rmax) continue;
-            // Merged WHERE: the common leaves AND C within the hull.
-            for (uint32_t j = 0; j < q0->npred; ++j) {
-                const tgp_pred_node& nd = q0->pred[j];
-                if (nd.kind != TGP_PN_LEAF || nd.column == static_cast<uint32_t>(C)) continue;
-                M->pred.push_back(nd);
+            if (fits && M->nbucket_tuples() * D > kMergeMaxTuples && cnt > 2) {
+                chunk = std::max<size_t>(2, cnt / 2);   // fewer members: fewer buckets
+                continue;
+            }
+            start += cnt;
+            if (!fits || M->nbucket_tuples() * D > kMergeMaxTuples) continue;
+            // Merged WHERE: the common leaves AND each varying column within
+            // the hull of its accepted cells.
+            auto push_and = [&]() {
                 if (M->pred.size() > 1) {
                     tgp_pred_node a{};
                     a.kind = TGP_PN_AND;
                     M->pred.push_back(a);
                 }
+            };
+            for (uint32_t j = 0; j < q0->npred; ++j) {
+                const tgp_pred_node& nd = q0->pred[j];
+                if (nd.kind != TGP_PN_LEAF || std::find(vary.begin(), vary.end(), nd.column) != vary.end()) continue;
+                M->pred.push_back(nd);
+                push_and();
             }
-            tgp_pred_node hull{};
-            hull.kind = TGP_PN_LEAF;
-            hull.column = static_cast<uint32_t>(C);
-            hull.cmp = TGP_CMP_BETWEEN;
-            hull.lit = static_cast<uint64_t>(col.min + static_cast<int64_t>(rmin));
-            hull.lit2 = static_cast<uint64_t>(col.min + static_cast<int64_t>(rmax));
-            M->pred.push_back(hull);
-            if (M->pred.size() > 1) {
-                tgp_pred_node a{};
-                a.kind = TGP_PN_AND;
-                M->pred.push_back(a);
+            for (size_t c = 0; c < vary.size(); ++c) {
+                const Column& col = T->cols[vary[c]];
+                tgp_pred_node h{};
+                h.kind = TGP_PN_LEAF;
+                h.column = vary[c];
+                h.cmp = TGP_CMP_BETWEEN;
+                h.lit = static_cast<uint64_t>(col.min + static_cast<int64_t>(hull[c].first));
+                h.lit2 = static_cast<uint64_t>(col.min + static_cast<int64_t>(hull[c].second));
+                M->pred.push_back(h);
+                push_and();
             }
-            tgp_group_key bk{};
-            bk.column = static_cast<uint32_t>(C);
-            bk.side = TGP_SIDE_PROBE;
-            M->group.push_back(bk);
+            for (uint32_t C : vary) {
+                tgp_group_key bk{};
+                bk.column = C;
+                bk.side = TGP_SIDE_PROBE;
+                M->group.push_back(bk);
+            }
             for (uint32_t k = 0; k < q0->ngroup; ++k) M->group.push_back(q0->group[k]);
             M->q = *q0;
             M->q.pred = M->pred.data();
@@ -2668,12 +2717,12 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
             M->q.ngroup = static_cast<uint32_t>(M->group.size());
             if (q0->join) {
                 M->has_count = true;
-                M->cgroup.push_back(bk);
+                M->cgroup.assign(M->group.begin(), M->group.begin() + vary.size());
                 M->count_agg.func = TGP_AGG_COUNT_STAR;
                 M->cq = M->q;
                 M->cq.join = 0;
                 M->cq.group = M->cgroup.data();
-                M->cq.ngroup = 1;
+                M->cq.ngroup = static_cast<uint32_t>(M->cgroup.size());
                 M->cq.aggs = &M->count_agg;
                 M->cq.nagg = 1;
             }
@@ -2685,7 +2734,7 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
 
 // A member's result block [counters 4][error 2][accumulators] rebuilt from
 // the merged blocks: each group's slots summed (MIN / MAX: extremes) over the
-// buckets the member accepts, values as full int128 limbs.
+// bucket combinations the member accepts, values as full int128 limbs.
 static void member_block(const MergeRec& M, size_t k, const QueryState& mqs, const unsigned long long* hb,
                          const unsigned long long* hc, const QueryState& cqs,
                          std::vector<unsigned long long>* out) {
@@ -2695,10 +2744,20 @@ static void member_block(const MergeRec& M, size_t k, const QueryState& mqs, con
     out->assign(6 + D * nv1 * 2, 0);
     unsigned long long* blk = out->data();
     blk[4] = hb[4] | (hc ? hc[4] : 0);
+    // The bucket combinations this member accepts, as merged group-index
+    // prefixes (the bucket keys are the most significant digits).
+    std::vector<uint64_t> tuples(1, 0);
+    for (const MergeCol& c : M.cols) {
+        std::vector<uint64_t> next;
+        for (uint64_t t : tuples)
+            for (size_t b = 1; b < c.bucket_mask.size(); ++b)
+                if ((c.bucket_mask[b] >> k) & 1) next.push_back(t * c.bucket_mask.size() + b);
+        tuples.swap(next);
+    }
     const unsigned long long* macc = hb + 6;
-    auto read = [&](uint64_t slot, bool sum64) -> __int128 {
-        const uint64_t lo = macc[2 * slot];
-        const int64_t hi = sum64 ? (static_cast<int64_t>(lo) >> 63) : static_cast<int64_t>(macc[2 * slot + 1]);
+    auto read = [&](const unsigned long long* acc, uint64_t slot, bool sum64) -> __int128 {
+        const uint64_t lo = acc[2 * slot];
+        const int64_t hi = sum64 ? (static_cast<int64_t>(lo) >> 63) : static_cast<int64_t>(acc[2 * slot + 1]);
         return static_cast<__int128>((static_cast<unsigned __int128>(static_cast<uint64_t>(hi)) << 64) | lo);
     };
     __int128 selected = 0;
@@ -2709,14 +2768,13 @@ static void member_block(const MergeRec& M, size_t k, const QueryState& mqs, con
             __int128 acc = ext ? (kind == VK_MIN ? static_cast<__int128>(0x7fffffffffffffffll)
                                                  : static_cast<__int128>(static_cast<int64_t>(0x8000000000000000ull)))
                                : 0;
-            for (size_t b = 1; b < M.bucket_mask.size(); ++b) {
-                if (!((M.bucket_mask[b] >> k) & 1)) continue;
-                const uint64_t slot = (b * D + g) * nv1 + v;
+            for (uint64_t t : tuples) {
+                const uint64_t slot = (t * D + g) * nv1 + v;
                 if (ext) {
                     const int64_t x = static_cast<int64_t>(macc[2 * slot]);
                     acc = kind == VK_MIN ? std::min<__int128>(acc, x) : std::max<__int128>(acc, x);
                 } else {
-                    acc += read(slot, MP.sum64 != 0);
+                    acc += read(macc, slot, MP.sum64 != 0);
                 }
             }
             if (v == 0 && !M.has_count) selected += acc;
@@ -2726,13 +2784,7 @@ static void member_block(const MergeRec& M, size_t k, const QueryState& mqs, con
         }
     if (M.has_count) {
         const Plan& CP = cqs.b->P;
-        for (size_t b = 1; b < M.bucket_mask.size(); ++b)
-            if ((M.bucket_mask[b] >> k) & 1) {
-                const uint64_t slot = b * cqs.nv1;   // the bucket's row count
-                const uint64_t lo = hc[6 + 2 * slot];
-                const int64_t hi = CP.sum64 ? 0 : static_cast<int64_t>(hc[6 + 2 * slot + 1]);
-                selected += static_cast<__int128>((static_cast<unsigned __int128>(static_cast<uint64_t>(hi)) << 64) | lo);
-            }
+        for (uint64_t t : tuples) selected += read(hc + 6, t * cqs.nv1, CP.sum64 != 0);
     }
     blk[0] = static_cast<uint64_t>(selected);
 }
@@ -2780,8 +2832,12 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         for (auto& M : B->merges) {
             // The bucket table's device address is set once the batch region
             // exists; the plan only needs a non-null placeholder now.
-            const BucketSpec bs{reinterpret_cast<const uint8_t*>(M.get()),
-                                static_cast<uint32_t>(M->bucket_mask.size())};
+            BucketSpec bs{};
+            bs.nkeys = static_cast<uint32_t>(M->cols.size());
+            for (size_t c = 0; c < M->cols.size(); ++c) {
+                bs.lut[c] = reinterpret_cast<const uint8_t*>(M.get());
+                bs.nbuckets[c] = static_cast<uint32_t>(M->cols[c].bucket_mask.size());
+            }
             int st = plan_query(ctx, &M->q, M->qs, scan_kernel_static_smem(), nullptr, false, &bs);
             if (st == TGP_OK) st = size_smem(ctx, M->qs.b->P, M->qs.extra, scan_kernel_static_smem(), &M->qs.kn);
             if (st == TGP_OK && M->has_count) {
@@ -2995,10 +3051,11 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     }
     const size_t counter_off = off;
     off = align256(off + classes.size() * 4);
-    for (auto& M : B->merges) {
-        M->lut_off = off;
-        off = align256(off + M->hlut.size());
-    }
+    for (auto& M : B->merges)
+        for (MergeCol& c : M->cols) {
+            c.lut_off = off;
+            off = align256(off + c.hlut.size());
+        }
     const size_t blocks_off = off;
     B->blocks_off = blocks_off;
     for (uint32_t i = 0; i < n; ++i) {
@@ -3049,14 +3106,14 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     // Merged scans: bucket tables, result pointers (the blocks are zero:
     // merged queries hold no MIN / MAX identities beyond their own images).
     for (auto& M : B->merges) {
-        std::memcpy(h + M->lut_off, M->hlut.data(), M->hlut.size());
+        for (const MergeCol& c : M->cols) std::memcpy(h + c.lut_off, c.hlut.data(), c.hlut.size());
         auto place = [&](QueryState& qs, size_t boff) {
             Plan& P = qs.b->P;
             unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + boff);
             P.counters = blk;
             P.err = reinterpret_cast<uint32_t*>(blk + 4);
             P.acc = blk + 6;
-            P.gkey[0].lut = B->dev + M->lut_off;
+            for (size_t c = 0; c < M->cols.size(); ++c) P.gkey[c].lut = B->dev + M->cols[c].lut_off;
             if (qs.has_minmax()) {
                 std::vector<unsigned long long> img;
                 init_acc_image(P, qs.ngroups_direct, &img);
