@@ -2561,24 +2561,53 @@ constexpr uint64_t kMergeMaxTuples = 1ull << 14;  // bucket combinations x group
 constexpr size_t kMergeChunk = 64;                // members per merged query (one u64 mask)
 
 // Builds the bucket table of one varying column for a chunk of members.
-// Returns false if the column cannot be bucketed.
+// Every member's acceptance of a cell is constant between consecutive
+// breakpoints (the cells where one of its leaves on the column can change:
+// a literal, or the cell after one), so it is evaluated once per segment,
+// not once per cell. Returns false if the column cannot be bucketed.
 static bool bucket_column(const BatchRec& B, const std::vector<uint32_t>& members, const Column& col,
                           uint32_t C, MergeCol* out, uint64_t* rmin_out, uint64_t* rmax_out) {
     const uint64_t cells = static_cast<uint64_t>(col.max - col.min) + 1;
     out->column = C;
     out->bucket_mask.assign(1, 0);
     out->hlut.assign(cells, 0);
+    // Each member's leaves on C.
+    std::vector<std::vector<const tgp_pred_node*>> leaves(members.size());
+    std::vector<uint64_t> cuts{0, cells};
+    auto add_cut = [&](uint64_t lit_bits) {
+        // The cell `lit` and the one after it, as offsets into [0, cells]
+        // (a literal outside the range changes nothing inside it; the
+        // column's minimum is not negative, so an unsigned literal above
+        // INT64_MAX reads as negative and is outside too).
+        const int64_t v = static_cast<int64_t>(lit_bits);
+        if (v >= col.min && v <= col.max) {
+            const uint64_t o = static_cast<uint64_t>(v - col.min);
+            cuts.push_back(o);
+            cuts.push_back(o + 1);
+        }
+    };
+    for (size_t k = 0; k < members.size(); ++k) {
+        const tgp_query* qk = B.items[members[k]].query;
+        for (uint32_t j = 0; j < qk->npred; ++j)
+            if (qk->pred[j].kind == TGP_PN_LEAF && qk->pred[j].column == C) {
+                leaves[k].push_back(&qk->pred[j]);
+                add_cut(qk->pred[j].lit);
+                if (qk->pred[j].cmp == TGP_CMP_BETWEEN || qk->pred[j].cmp == TGP_CMP_NOT_BETWEEN)
+                    add_cut(qk->pred[j].lit2);
+            }
+    }
+    std::sort(cuts.begin(), cuts.end());
+    cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
     std::unordered_map<uint64_t, uint8_t> bucket_of;
     bucket_of[0] = 0;
     uint64_t rmin = cells, rmax = 0;
-    for (uint64_t r = 0; r < cells; ++r) {
-        const int64_t cell = col.min + static_cast<int64_t>(r);
+    for (size_t s = 0; s + 1 < cuts.size(); ++s) {
+        const uint64_t r0 = cuts[s], r1 = cuts[s + 1];   // cells [r0, r1)
+        const int64_t cell = col.min + static_cast<int64_t>(r0);
         uint64_t mask = 0;
         for (size_t k = 0; k < members.size(); ++k) {
-            const tgp_query* qk = B.items[members[k]].query;
             bool acc = true;
-            for (uint32_t j = 0; j < qk->npred && acc; ++j)
-                if (qk->pred[j].kind == TGP_PN_LEAF && qk->pred[j].column == C) acc = leaf_passes(col, qk->pred[j], cell);
+            for (const tgp_pred_node* nd : leaves[k]) acc = acc && leaf_passes(col, *nd, cell);
             if (acc) mask |= 1ull << k;
         }
         auto it = bucket_of.find(mask);
@@ -2591,10 +2620,10 @@ static bool bucket_column(const BatchRec& B, const std::vector<uint32_t>& member
         } else {
             b = it->second;
         }
-        out->hlut[r] = b;
+        std::fill(out->hlut.begin() + static_cast<std::ptrdiff_t>(r0), out->hlut.begin() + static_cast<std::ptrdiff_t>(r1), b);
         if (mask) {
-            rmin = std::min(rmin, r);
-            rmax = std::max(rmax, r);
+            rmin = std::min(rmin, r0);
+            rmax = std::max(rmax, r1 - 1);
         }
     }
     if (rmin > rmax) return false;
