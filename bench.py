@@ -716,9 +716,13 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     its own context) and by plain one-at-a-time execution.
 
     Measured: the plain server's capacity (completed q/s with arrivals far
-    above it) and its p50 / p99 at 80 % of that capacity; the batched
-    server's completed q/s and p50 / p99 when offered 5x the plain capacity,
-    and its own capacity. value = the batched completions/s at 5x."""
+    above it) and its p50 / p99 at 80 % of that capacity; the batched server's
+    policy (batches in flight: 1 or 2) picked on a calibration stream at 5x
+    the plain capacity; then the batched server offered 5x, 6x, 8x, 10x, 12x
+    the plain capacity, until its p99 exceeds the plain p99 or it falls
+    behind the offered rate; and its own capacity. value = the highest
+    completed q/s whose p99 is at most the plain server's p99 (the 5x run's,
+    if none is)."""
     import numpy as np
     from turbogp_b200 import datagen, serving, workloads
     from turbogp_b200.engine import Context, col, count_star, sum_
@@ -768,31 +772,61 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     # Warm-up: every template's prepared queries built and sized (the
     # high-cardinality one included), then both paths once.
     serving.prewarm(templates, [request(0.0) for _ in range(2000)], per_template=4)
+    serving.reserve(templates, 320)
     serving.serve_batched(ctx, templates, stream(4000.0, 256), mem_budget=args.mem_budget)
     serving.serve_plain(ctx, templates, stream(4000.0, 32))
     # Plain capacity, then plain at 80 % of it.
     plain_sat = serving.serve_plain(ctx, templates, stream(50_000.0, max(400, count // 4)))
     cap_p = plain_sat["qps"]
     plain = serving.serve_plain(ctx, templates, stream(0.8 * cap_p, max(400, count // 2)))
+    p99_plain = plain.get("p99_ms") or 0.0
+    # Policy: batches in flight, on a calibration stream of its own.
+    calib = {}
+    for inflight in (1, 2):
+        r = serving.serve_batched(ctx, templates, stream(5.0 * cap_p, max(600, count // 2)),
+                                  mem_budget=args.mem_budget, max_inflight=inflight)
+        calib[inflight] = r.get("p99_ms") or 1e9
+    inflight = min(calib, key=calib.get)
+    ladder, best = [], None
     with ClockSampler(local) as clocks:
-        batched = serving.serve_batched(ctx, templates, stream(5.0 * cap_p, count), mem_budget=args.mem_budget)
-    batched_sat = serving.serve_batched(ctx, templates, stream(100_000.0, count), mem_budget=args.mem_budget)
+        for m in (5.0, 6.0, 8.0, 10.0, 12.0):
+            r = serving.serve_batched(ctx, templates, stream(m * cap_p, count), mem_budget=args.mem_budget,
+                                      max_inflight=inflight)
+            r = {**r, "offered_qps": m * cap_p, "offered_x_plain_capacity": m}
+            ladder.append(r)
+            ok = (r.get("p99_ms") or 1e9) <= p99_plain
+            if ok:
+                best = r
+            if not ok or (r.get("qps") or 0) < 0.9 * m * cap_p:
+                break
+    batched_sat = serving.serve_batched(ctx, templates, stream(100_000.0, count), mem_budget=args.mem_budget,
+                                        max_inflight=inflight)
+    at5 = ladder[0]
+    head = best if best is not None else at5
     rec = {
-        "metric": METRIC, "value": batched.get("qps"), "unit": "queries/s", "n_gpus": world,
-        "steps": count, "warmup": 256, "ms_per_step": batched.get("mean_ms"), "higher_is_better": True,
+        "metric": METRIC, "value": head.get("qps"), "unit": "queries/s", "n_gpus": world,
+        "steps": count, "warmup": 256, "ms_per_step": head.get("mean_ms"), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": DATA,
         "config": {"workload": f"serving: Poisson arrivals of scan+sum / filtered grouped aggregate / join+grouped "
                                f"aggregate over a resident {n}-row fact table (random literals) and GROUP BY key "
                                f"over a {args.highcard_rows}-row high-cardinality table (1 in 500); continuous "
                                f"batching with merged and shared scans, planner-sized admission (budget "
                                f"{args.mem_budget} B), high-cardinality requests in a heavy lane (own stream)",
-                   "requests": count},
+                   "requests": count, "value": "highest batched completed q/s with p99 <= the plain p99 at 80% "
+                                               "of plain capacity" if best is not None else
+                                               "batched completed q/s at 5x plain capacity (p99 above plain)"},
         "plain_capacity_qps": cap_p,
         "plain_at_80pct": {**plain, "offered_qps": 0.8 * cap_p},
-        "batched_at_5x": {**batched, "offered_qps": 5.0 * cap_p},
+        "batched_policy": {"max_inflight": inflight, "calibration_p99_ms": calib},
+        "batched_at_5x": at5,
+        "batched_ladder": ladder,
         "batched_capacity_qps": batched_sat.get("qps"),
-        "qps_ratio_at_5x": (batched.get("qps") or 0) / cap_p if cap_p else None,
-        "p99_batched_le_plain": (batched.get("p99_ms") or 1e9) <= (plain.get("p99_ms") or 0),
+        "qps_ratio_at_5x": (at5.get("qps") or 0) / cap_p if cap_p else None,
+        "p99_batched_le_plain": (at5.get("p99_ms") or 1e9) <= p99_plain,
+        "batched_qps_at_plain_p99": best.get("qps") if best is not None else None,
+        "ratio_at_plain_p99_vs_plain_capacity": (best.get("qps") / cap_p) if best is not None and cap_p else None,
+        "ratio_at_plain_p99_vs_plain_at_80pct": (best.get("qps") / plain["qps"]) if best is not None and
+                                                plain.get("qps") else None,
         "roofline": None, "e2e": None, "cpu_baseline": None, "clocks": clocks.summary(), "gpu_launches": None,
     }
     j.drop()

@@ -9,6 +9,7 @@
 //   * sorting of packed join pairs and their split into two u32 arrays.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cub/cub.cuh>
 
@@ -705,6 +706,28 @@ __global__ void delay_kernel(uint64_t ns) {
 
 cudaError_t launch_delay(uint64_t ns, cudaStream_t st) {
     delay_kernel<<<1, 1, 0, st>>>(ns < 1000000ull ? ns : 1000000ull);
+    return cudaGetLastError();
+}
+
+// Copies 16-byte words from device memory into page-locked host memory with
+// the SMs' own stores over the link: a batch's result readback then takes no
+// copy engine, so it does not queue behind another stream's large
+// device-to-host copy (a high-cardinality result) on the same engine.
+__global__ void __launch_bounds__(256) copy_to_host_kernel(uint4* __restrict__ dst, const uint4* __restrict__ src,
+                                                           uint64_t nwords) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nwords;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t launch_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return cudaSuccess;
+    if ((bytes & 15u) || (reinterpret_cast<uintptr_t>(host_dst) & 15u) || (reinterpret_cast<uintptr_t>(dev_src) & 15u))
+        return cudaErrorInvalidValue;
+    const uint64_t nwords = bytes / 16;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((nwords + 255) / 256, 148));
+    copy_to_host_kernel<<<grid, 256, 0, st>>>(static_cast<uint4*>(host_dst), static_cast<const uint4*>(dev_src),
+                                              nwords);
     return cudaGetLastError();
 }
 

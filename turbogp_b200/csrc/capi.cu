@@ -2461,10 +2461,27 @@ struct MergeRec {
     bool has_count = false;
     QueryState qs, cqs;
     size_t block_off = 0, cblock_off = 0;
+    std::vector<uint8_t> tvalid;         // per bucket combination: some member accepts it
+    size_t tv_off = 0;
     uint64_t nbucket_tuples() const {
         uint64_t n = 1;
         for (const MergeCol& c : cols) n *= c.bucket_mask.size();
         return n;
+    }
+    // Bucket combinations t = ((d0 * n1) + d1) * n2 + d2 (the first column
+    // most significant), valid when the members accepting every digit meet.
+    void fill_tvalid() {
+        const uint64_t n = nbucket_tuples();
+        tvalid.assign(n, 0);
+        for (uint64_t t = 0; t < n; ++t) {
+            uint64_t rest = t, mask = ~0ull;
+            for (size_t c = cols.size(); c-- > 0;) {
+                const uint64_t nb = cols[c].bucket_mask.size();
+                mask &= cols[c].bucket_mask[rest % nb];
+                rest /= nb;
+            }
+            tvalid[t] = mask != 0;
+        }
     }
 };
 
@@ -3080,11 +3097,15 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     }
     const size_t counter_off = off;
     off = align256(off + classes.size() * 4);
-    for (auto& M : B->merges)
+    for (auto& M : B->merges) {
         for (MergeCol& c : M->cols) {
             c.lut_off = off;
             off = align256(off + c.hlut.size());
         }
+        M->fill_tvalid();
+        M->tv_off = off;
+        off = align256(off + M->tvalid.size());
+    }
     const size_t blocks_off = off;
     B->blocks_off = blocks_off;
     for (uint32_t i = 0; i < n; ++i) {
@@ -3136,13 +3157,23 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     // merged queries hold no MIN / MAX identities beyond their own images).
     for (auto& M : B->merges) {
         for (const MergeCol& c : M->cols) std::memcpy(h + c.lut_off, c.hlut.data(), c.hlut.size());
+        std::memcpy(h + M->tv_off, M->tvalid.data(), M->tvalid.size());
         auto place = [&](QueryState& qs, size_t boff) {
             Plan& P = qs.b->P;
             unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + boff);
             P.counters = blk;
             P.err = reinterpret_cast<uint32_t*>(blk + 4);
             P.acc = blk + 6;
-            for (size_t c = 0; c < M->cols.size(); ++c) P.gkey[c].lut = B->dev + M->cols[c].lut_off;
+            // The bucket keys are the plan's first group keys, in column order.
+            uint64_t ts = 1;
+            for (size_t c = M->cols.size(); c-- > 0;) {
+                P.gkey[c].lut = B->dev + M->cols[c].lut_off;
+                P.tstride[c] = static_cast<uint32_t>(ts);
+                P.lut_cells[c] = static_cast<uint32_t>(M->cols[c].hlut.size());
+                ts *= M->cols[c].bucket_mask.size();
+            }
+            P.tvalid = B->dev + M->tv_off;
+            P.ntuples = static_cast<uint32_t>(M->tvalid.size());
             if (qs.has_minmax()) {
                 std::vector<unsigned long long> img;
                 init_acc_image(P, qs.ngroups_direct, &img);
@@ -3185,8 +3216,10 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
         if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("batch launch: ") + cudaGetErrorString(e));
         if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
     }
-    TGP_CUDA(cudaMemcpyAsync(h + B->readback_off, B->dev + blocks_off, blocks_bytes, cudaMemcpyDeviceToHost,
-                             ctx->stream));
+    // The readback: the SMs store the result blocks into the page-locked
+    // staging buffer (mapped into the device's address space), so it uses no
+    // copy engine.
+    TGP_CUDA(launch_copy_to_host(h + B->readback_off, B->dev + blocks_off, blocks_bytes, ctx->stream));
     TGP_CUDA(cudaEventCreateWithFlags(&B->done, cudaEventDisableTiming));
     TGP_CUDA(cudaEventRecord(B->done, ctx->stream));
     const uint64_t id = ctx->next_id++;

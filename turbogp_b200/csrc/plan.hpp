@@ -256,6 +256,15 @@ struct alignas(16) Plan {
     // (0 = kWaitLimitNs).
     uint64_t skip_tile1;
     uint64_t wait_ns;
+    // Merged scans: tvalid[t] != 0 iff some member accepts bucket combination
+    // t = sum over bucket keys k of digit_k * tstride[k] (t < ntuples); a row
+    // of any other combination (or a key cell outside its bucket table's
+    // lut_cells) is dropped before it reaches the accumulators. Null = off.
+    const uint8_t* tvalid;
+    uint32_t tstride[kMaxGroupKeys];
+    uint32_t lut_cells[kMaxGroupKeys];
+    uint32_t ntuples;
+    uint32_t _pad_tv;
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 

@@ -80,6 +80,9 @@ cudaError_t topn_hash_groups(const unsigned long long* packed, uint64_t n, const
                              uint64_t* keys_out, tgp_agg_value* vals_out, int sms, cudaStream_t st);
 // One thread that spins on %globaltimer for `ns` nanoseconds (at most 1 ms).
 cudaError_t launch_delay(uint64_t ns, cudaStream_t st);
+// Device-to-host copy by a kernel into page-locked (mapped) host memory; both
+// addresses and the size 16-byte aligned.
+cudaError_t launch_copy_to_host(void* host_dst, const void* dev_src, size_t bytes, cudaStream_t st);
 cudaError_t launch_like(const uint8_t* bytes, const unsigned long long* offs, uint64_t n, const LikePattern& P,
                         bool negated, uint32_t* bitmap, unsigned long long* count, uint32_t* err, int sms,
                         cudaStream_t st);

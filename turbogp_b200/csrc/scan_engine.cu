@@ -1500,6 +1500,43 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
 }
 
 // ---------------------------------------------------------------------------
+// Merged scans: drops the selected rows whose bucket combination no member
+// accepts (P.tvalid), and any row whose bucket key cell lies outside its
+// table, so that the group index never reads a bucket table out of range.
+// ---------------------------------------------------------------------------
+template <int R, bool TAIL>
+__device__ __forceinline__ uint32_t tuple_filter(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t t,
+                                                 uint32_t m) {
+    constexpr uint32_t kBad = 0xffffffffu;
+    uint32_t tix[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) tix[r] = 0;
+#pragma unroll 1
+    for (uint32_t k = 0; k < P.ngkey; ++k) {
+        const GKey& K = P.gkey[k];
+        if (!K.lut) continue;
+        const uint32_t ts = P.tstride[k], cells = P.lut_cells[k], mn = static_cast<uint32_t>(K.min);
+        uint32_t x[R];
+        if (!TAIL) {
+            load_cells32<R>(stage + K.soff, K.dtype, t, x);
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                x[r] = ((m >> r) & 1u) ? static_cast<uint32_t>(key_cell<true>(P, K, stage, r0, R * t + r, 0)) : mn;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t rel = x[r] - mn;
+            tix[r] = (rel < cells && tix[r] != kBad) ? tix[r] + static_cast<uint32_t>(__ldg(K.lut + rel)) * ts : kBad;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !__ldg(P.tvalid + tix[r]))) m &= ~(1u << r);
+    return m;
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
@@ -1510,7 +1547,11 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     constexpr int R = kTileRows / NT;
     const uint64_t r0 = tile * kTileRows;
     const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
-    const uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
+    uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
+    if constexpr (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
+                  MODE == MODE_GROUP_SHARED32) {
+        if (P.tvalid) m = tuple_filter<R, TAIL>(P, stage, r0, t, m);
+    }
     const uint32_t lane = t & 31u;
     selected += __popc(m);
     if (MODE == MODE_GROUP_PRIVATE && P.count_by_tile) {

@@ -3,8 +3,9 @@ admission, against plain one-query-at-a-time execution.
 
 Requests arrive open-loop (Poisson) from a list, or live from a queue (the
 wire front-end); each names a query template and its literals. The batched
-server keeps a queue; whenever fewer than ``max_inflight`` batches are running
-it admits queued requests in arrival order while the device memory their plans
+server keeps a queue of requests, each already rebound to a prepared query of
+its template when it arrived; whenever fewer than ``max_inflight`` batches are
+running it admits queued requests in arrival order while the device memory their plans
 need (``tgp_query_footprint``: group hash tables, join payloads, result
 blocks) fits the budget, submits them as one ``tgp_batch_submit``, and
 completes batches with ``tgp_batch_poll``. Requests of a heavy template (a
@@ -83,6 +84,17 @@ def prewarm(templates: dict[str, Template], requests: list[Request], per_templat
             pq.rebind(where).run(decode=False)
         for pq in pqs:
             tpl.give(pq)
+
+
+def reserve(templates: dict[str, Template], per_template: int) -> None:
+    """Grows every light template's pool of prepared queries to
+    ``per_template`` (built, not run), so that a backlog of queued requests
+    does not build prepared queries on the serving loop's thread."""
+    for tpl in templates.values():
+        if tpl.heavy or tpl.solo is not None:
+            continue
+        while len(tpl.pool) < per_template:
+            tpl.pool.append(tpl.make())
 
 
 def poisson_arrivals(rate: float, n: int, rng: np.random.Generator) -> np.ndarray:
@@ -223,7 +235,7 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs, mem_budget
     `heavy_lane` (default: whether any template is heavy) starts the heavy
     lane; a live source whose templates appear later passes it explicitly."""
     source = reqs if isinstance(reqs, QueueSource) else ListSource(reqs)
-    queue: deque[Request] = deque()
+    queue: deque = deque()         # [req, template, prepared query rebound to it, or None]
     inflight: deque = deque()      # (handle, [(req, template, pq)])
     t0 = time.perf_counter() if t0 is None else t0
     if heavy_lane is None:
@@ -237,6 +249,9 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs, mem_budget
         # On an error, batches still running are completed before returning.
         for h, _ in inflight:
             h.wait()
+        for _, tpl, pq in queue:
+            if pq is not None:
+                tpl.give(pq)
         if lane is not None:
             lane.close()
     if lane is not None and lane.error is not None:
@@ -282,20 +297,25 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                         raise
                     _finish(r, time.perf_counter() - t0, error=e)
             else:
-                queue.append(r)
+                # Rebound on arrival, while earlier batches run, when an idle
+                # prepared query is at hand (so that a batch's members are
+                # ready to submit when it is formed); otherwise at admission.
+                queue.append([r, tpl, tpl.pool.pop().rebind(r.where) if tpl.pool else None])
         _complete(inflight, t0)
         if queue and len(inflight) < max_inflight:
             members, used = [], sum(m[1].mem_bytes or 0 for _, ms in inflight for m in ms)
             while queue and len(members) < max_batch:
-                tpl = templates[queue[0].template]
-                pq = tpl.take()
+                tpl = queue[0][1]
+                if tpl.mem_bytes is None:
+                    tpl.give(tpl.take())     # sizes the template from its first prepared query
                 if (members or inflight) and used + tpl.mem_bytes > mem_budget:
-                    tpl.give(pq)
                     break                    # admission: wait for memory to be released
                 # (A request larger than the budget runs alone once nothing else does.)
-                r = queue.popleft()
                 used += tpl.mem_bytes
-                members.append((r, tpl, pq.rebind(r.where)))
+                m = queue.popleft()
+                if m[2] is None:
+                    m[2] = tpl.take().rebind(m[0].where)
+                members.append(tuple(m))
             if members:
                 keep = any(m[0].keep for m in members)
                 try:
