@@ -560,39 +560,101 @@ __global__ void extract_keys_kernel(const unsigned long long* packed, uint64_t n
     }
 }
 
+// Output group i from its slot s ([key][count][value limbs...]).
+__device__ __forceinline__ void write_group(const unsigned long long* s, uint64_t i, const HashFormat& F,
+                                            uint64_t* keys_out, tgp_agg_value* vals_out) {
+    if (keys_out)
+        for (uint32_t k = 0; k < F.nkey; ++k)
+            keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((s[0] >> F.key_shift[k]) & F.key_mask[k]);
+    if (!vals_out) return;
+    const uint64_t cnt = s[1];
+    for (uint32_t a = 0; a < F.nagg; ++a) {
+        tgp_agg_value o;
+        o.count = cnt;
+        if (F.val[a] < 0) {
+            o.lo = cnt;
+            o.hi = 0;
+            o.as_f64 = static_cast<double>(cnt);
+        } else {
+            const unsigned long long* v = s + 2 + 2 * F.val[a];
+            if (F.kind[a] == VK_MIN || F.kind[a] == VK_MAX) {
+                const int64_t x = static_cast<int64_t>(v[0]);
+                o.lo = static_cast<uint64_t>(x);
+                o.hi = x < 0 ? -1 : 0;
+                o.as_f64 = static_cast<double>(x);
+            } else {
+                o.lo = v[0];
+                o.hi = F.sum64 ? (static_cast<int64_t>(v[0]) >> 63) : static_cast<int64_t>(v[1]);
+                const double f = i128_to_f64_rn(o.lo, o.hi);
+                o.as_f64 = F.func[a] == TGP_AGG_AVG ? (cnt ? f / static_cast<double>(cnt) : 0.0) : f;
+            }
+        }
+        vals_out[i * F.nagg + a] = o;
+    }
+}
+
 __global__ void format_hash_groups_kernel(const unsigned long long* packed, const uint32_t* order, uint64_t n,
                                           const HashFormat F, uint64_t* keys_out, tgp_agg_value* vals_out) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const unsigned long long* s = packed + static_cast<uint64_t>(order[i]) * F.hstride;
-        if (keys_out)
-            for (uint32_t k = 0; k < F.nkey; ++k)
-                keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((s[0] >> F.key_shift[k]) & F.key_mask[k]);
-        if (!vals_out) continue;
-        const uint64_t cnt = s[1];
-        for (uint32_t a = 0; a < F.nagg; ++a) {
-            tgp_agg_value o;
-            o.count = cnt;
-            if (F.val[a] < 0) {
-                o.lo = cnt;
-                o.hi = 0;
-                o.as_f64 = static_cast<double>(cnt);
-            } else {
-                const unsigned long long* v = s + 2 + 2 * F.val[a];
-                if (F.kind[a] == VK_MIN || F.kind[a] == VK_MAX) {
-                    const int64_t x = static_cast<int64_t>(v[0]);
-                    o.lo = static_cast<uint64_t>(x);
-                    o.hi = x < 0 ? -1 : 0;
-                    o.as_f64 = static_cast<double>(x);
-                } else {
-                    o.lo = v[0];
-                    o.hi = F.sum64 ? (static_cast<int64_t>(v[0]) >> 63) : static_cast<int64_t>(v[1]);
-                    const double f = i128_to_f64_rn(o.lo, o.hi);
-                    o.as_f64 = F.func[a] == TGP_AGG_AVG ? (cnt ? f / static_cast<double>(cnt) : 0.0) : f;
-                }
-            }
-            vals_out[i * F.nagg + a] = o;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        write_group(packed + static_cast<uint64_t>(order[i]) * F.hstride, i, F, keys_out, vals_out);
+}
+
+// Directly indexed group tables (slot = key): the occupied slots, in slot
+// order, are the groups in ascending key order, so the result is written
+// straight from the table at positions from a prefix count of occupied
+// slots, with no gather and no sort. Block b covers slots
+// [b * kDirChunk, (b + 1) * kDirChunk); pass 1 counts each block's occupied
+// slots, a device scan makes them offsets, pass 2 writes each block's groups
+// in order (slot base + j * kAuxThreads + thread, j ascending, so a warp's
+// ballot and the block's warp totals give each slot's rank).
+constexpr int kDirPerThread = 16;
+constexpr uint64_t kDirChunk = static_cast<uint64_t>(kAuxThreads) * kDirPerThread;
+
+__global__ void __launch_bounds__(kAuxThreads) count_direct_kernel(const unsigned long long* htab, uint64_t nslots,
+                                                                   uint32_t stride, unsigned long long* counts) {
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kDirChunk;
+    uint32_t c = 0;
+#pragma unroll 4
+    for (int j = 0; j < kDirPerThread; ++j) {
+        const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
+        c += (i < nslots && htab[i * stride] != ~0ull) ? 1u : 0u;
+    }
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
+    __shared__ uint32_t wsum[kAuxThreads / 32];
+    if ((threadIdx.x & 31u) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kAuxThreads / 32; ++w) t += wsum[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kAuxThreads) format_direct_kernel(const unsigned long long* htab, uint64_t nslots,
+                                                                    const unsigned long long* offsets, uint64_t cap,
+                                                                    const HashFormat F, uint64_t* keys_out,
+                                                                    tgp_agg_value* vals_out) {
+    __shared__ uint32_t wsum[kAuxThreads / 32];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kDirChunk;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned long long run = offsets[blockIdx.x];
+    for (int j = 0; j < kDirPerThread; ++j) {
+        const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
+        const unsigned long long* s = htab + i * F.hstride;
+        const bool occ = i < nslots && s[0] != ~0ull;
+        const uint32_t mask = __ballot_sync(0xffffffffu, occ);
+        if (lane == 0) wsum[warp] = __popc(mask);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < kAuxThreads / 32; ++w) {
+            before += w < warp ? wsum[w] : 0u;
+            total += wsum[w];
         }
+        const unsigned long long pos = run + before + __popc(mask & ((1u << lane) - 1u));
+        if (occ && pos < cap) write_group(s, pos, F, keys_out, vals_out);
+        run += total;
+        __syncthreads();
     }
 }
 
@@ -616,6 +678,43 @@ cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, con
     if (e != cudaSuccess) return e;
     format_hash_groups_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(packed, i1, n, F, keys_out,
                                                                                      vals_out);
+    return cudaGetLastError();
+}
+
+uint64_t direct_groups_blocks(uint64_t nslots) { return (nslots + kDirChunk - 1) / kDirChunk; }
+
+// Scratch: counts[nb + 1], offsets[nb + 1] (u64), then CUB's scan storage.
+size_t direct_groups_scratch(uint64_t nslots) {
+    const uint64_t nb = direct_groups_blocks(nslots);
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, static_cast<unsigned long long*>(nullptr),
+                                  static_cast<unsigned long long*>(nullptr), static_cast<int>(nb + 1));
+    return (nb + 1) * 16 + tmp + 256;
+}
+
+cudaError_t count_direct_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride, void* scratch,
+                                size_t scratch_bytes, unsigned long long* total, cudaStream_t st) {
+    const uint64_t nb = direct_groups_blocks(nslots);
+    unsigned long long* counts = static_cast<unsigned long long*>(scratch);
+    unsigned long long* offsets = counts + nb + 1;
+    uint8_t* tmp = reinterpret_cast<uint8_t*>(offsets + nb + 1);
+    size_t tmp_bytes = scratch_bytes - (nb + 1) * 16;
+    // counts[nb] = 0, so offsets[nb] is the number of occupied slots.
+    cudaError_t e = cudaMemsetAsync(counts + nb, 0, 8, st);
+    if (e != cudaSuccess) return e;
+    if (nb) count_direct_kernel<<<static_cast<unsigned>(nb), kAuxThreads, 0, st>>>(htab, nslots, stride, counts);
+    e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, offsets, static_cast<int>(nb + 1), st);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(total, offsets + nb, 8, cudaMemcpyDeviceToDevice, st);
+}
+
+cudaError_t format_direct_groups(const unsigned long long* htab, uint64_t nslots, const void* scratch, uint64_t cap,
+                                 const HashFormat& F, uint64_t* keys_out, tgp_agg_value* vals_out, cudaStream_t st) {
+    const uint64_t nb = direct_groups_blocks(nslots);
+    if (nb == 0 || cap == 0) return cudaSuccess;
+    const unsigned long long* offsets = static_cast<const unsigned long long*>(scratch) + nb + 1;
+    format_direct_kernel<<<static_cast<unsigned>(nb), kAuxThreads, 0, st>>>(htab, nslots, offsets, cap, F, keys_out,
+                                                                            vals_out);
     return cudaGetLastError();
 }
 

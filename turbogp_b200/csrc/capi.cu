@@ -22,6 +22,7 @@ namespace {
 
 constexpr unsigned long long kEmptySlot = ~0ull;
 constexpr uint64_t kDirectMaxGroups = 1ull << 22;
+constexpr uint64_t kHashDirectMax = 1ull << 27;   // key values of a directly indexed group table
 
 int fail(tgp_ctx* ctx, int st, const std::string& m) {
     if (ctx) ctx->err = m;
@@ -1595,13 +1596,17 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         // accumulators do not fit (or a variant asks for it).
         const uint32_t s32_words = 1 + 2 * P.nval;
         const uint32_t s32_nt = kn.threads == 256 ? 256u : 512u;
+        // Bucketed (merged) plans take the limb tables whenever they are
+        // exact: the private placement has no dense path for bucket keys
+        // (a 2-member merged scan: 1.02 ms private, 0.51 ms limb tables).
+        const bool prefer_s32 = kn.placement == 4 || (bucket != nullptr && kn.placement == 0);
         auto s32_bytes = [&](uint32_t copies) -> size_t {
             return static_cast<size_t>(copies) * ngroups_direct * s32_words * 4;
         };
         uint32_t s32_copies = 0;
         {
             bool ok = !b.unbounded && (!J || J->unique) && kn.placement != 2 && kn.placement != 3 &&
-                      (nt == 0 || kn.placement == 4);
+                      (nt == 0 || prefer_s32);
             for (uint32_t v = 0; ok && v < P.nval; ++v)
                 ok = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
             const unsigned __int128 bound = static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
@@ -1614,7 +1619,7 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
                 if (s32_bytes(copies) + 2 * st <= budget) s32_copies = copies;
             }
         }
-        if (nt && !(kn.placement == 4 && s32_copies)) {
+        if (nt && !(prefer_s32 && s32_copies)) {
             mode = MODE_GROUP_PRIVATE;
             P.nthreads = nt;
             P.count_by_tile = (q->ngroup == 0 && !J) ? 1u : 0u;
@@ -1705,12 +1710,22 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
     if (mode == MODE_GROUP_HASH) {
         const unsigned __int128 est = std::min<unsigned __int128>(D, static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1)) *
                                                                           (join ? 4 : 1));
-        // Distinct groups never exceed `est`: a load factor of at most 0.8
-        // keeps linear probes short and the table (and its misses) small.
-        hcap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(est) + static_cast<uint64_t>(est) / 4));
         P.hstride = 2 + 2 * P.nval;
-        P.hlog2 = log2u(hcap);
-        P.hmask = hcap - 1;
+        if (q->ngroup == 1 && !P.gkey[0].build_side && D <= kHashDirectMax && D <= 2 * static_cast<unsigned __int128>(std::max<uint64_t>(T->rows, 1))) {
+            // One key over at most 2^27 values, no more than twice the rows:
+            // a slot per key value, indexed by the key (no hashing, probing
+            // or claiming), no larger than the hashed table would be.
+            hcap = std::max<uint64_t>(16, static_cast<uint64_t>(D));
+            P.hdirect = 1;
+            P.hlog2 = log2u(next_pow2(hcap));
+            P.hmask = hcap - 1;
+        } else {
+            // Distinct groups never exceed `est`: a load factor of at most 0.8
+            // keeps linear probes short and the table (and its misses) small.
+            hcap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(est) + static_cast<uint64_t>(est) / 4));
+            P.hlog2 = log2u(hcap);
+            P.hmask = hcap - 1;
+        }
     }
     // One staged key and at most two SUM / COUNT(col) values of one staged
     // factor each: the column path of global / hash grouping.
@@ -1923,25 +1938,7 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
         return TGP_OK;
     }
 
-    // Hash groups: gather occupied slots, sort by key on the host.
-    // Counter word 2 counts the gathered slots.
-    TGP_CUDA(cudaMemsetAsync(P.counters + 2, 0, 8, ctx->stream));
-    unsigned long long* packed = nullptr;
-    const uint64_t max_groups = std::min<uint64_t>(hcap, static_cast<uint64_t>(std::min<unsigned __int128>(D, hcap)));
-    TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&packed), std::max<uint64_t>(max_groups, 1) * P.hstride * 8,
-                      "group gather allocation failed"));
-    TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream));
-    unsigned long long ng = 0;
-    TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
-    result->ngroups = ng;
-    if (!tn && ng > group_cap) {
-        dev_free(ctx, packed);
-        return fail(ctx, TGP_CAPACITY, "group buffer too small");
-    }
-    if (nagg <= static_cast<uint32_t>(kMaxFormatAggs)) {
-        // Sort by packed key (= ascending lexicographic key order, key 0 in
-        // the top bits) and format on the device; copy the caller's arrays once.
+    auto hash_format = [&]() {
         HashFormat F;
         std::memset(&F, 0, sizeof(F));
         F.nkey = q->ngroup;
@@ -1958,6 +1955,68 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
             F.val[a] = static_cast<int8_t>(amap[a].val);
             F.kind[a] = amap[a].val >= 0 ? P.val[amap[a].val].kind : VK_SUM;
         }
+        return F;
+    };
+    // Hash groups: gather occupied slots, sort by key on the host.
+    // Counter word 2 counts the gathered slots.
+    TGP_CUDA(cudaMemsetAsync(P.counters + 2, 0, 8, ctx->stream));
+    if (P.hdirect && !tn && nagg <= static_cast<uint32_t>(kMaxFormatAggs)) {
+        // A directly indexed table holds the groups in key order already:
+        // count the occupied slots, then format them in place of a gather
+        // and a sort.
+        const size_t sb = direct_groups_scratch(hcap);
+        uint8_t* scr = nullptr;
+        TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&scr), sb, "group count allocation failed"));
+        unsigned long long ng = 0;
+        cudaError_t e = count_direct_groups(P.htab, hcap, P.hstride, scr, sb, P.counters + 2, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            dev_free(ctx, scr);
+            return fail(ctx, TGP_DEVICE_ERROR, std::string("group count: ") + cudaGetErrorString(e));
+        }
+        result->ngroups = ng;
+        if (ng > group_cap) {
+            dev_free(ctx, scr);
+            return fail(ctx, TGP_CAPACITY, "group buffer too small");
+        }
+        const HashFormat F = hash_format();
+        const size_t kbytes = (keys_out ? ng * q->ngroup * 8 : 0), vbytes = (vals_out ? ng * nagg * sizeof(tgp_agg_value) : 0);
+        uint8_t* buf = nullptr;
+        const size_t vofs = (kbytes + 255) & ~size_t{255};
+        if (int st = dev_alloc(ctx, reinterpret_cast<void**>(&buf), std::max<size_t>(vofs + vbytes, 256),
+                               "group format allocation failed")) {
+            dev_free(ctx, scr);
+            return st;
+        }
+        uint64_t* dkeys = kbytes ? reinterpret_cast<uint64_t*>(buf) : nullptr;
+        tgp_agg_value* dvals = vbytes ? reinterpret_cast<tgp_agg_value*>(buf + vofs) : nullptr;
+        e = format_direct_groups(P.htab, hcap, scr, ng, F, dkeys, dvals, ctx->stream);
+        if (e == cudaSuccess && kbytes) e = cudaMemcpyAsync(keys_out, dkeys, kbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && vbytes) e = cudaMemcpyAsync(vals_out, dvals, vbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        dev_free(ctx, buf);
+        dev_free(ctx, scr);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("group format: ") + cudaGetErrorString(e));
+        return TGP_OK;
+    }
+    unsigned long long* packed = nullptr;
+    const uint64_t max_groups = std::min<uint64_t>(hcap, static_cast<uint64_t>(std::min<unsigned __int128>(D, hcap)));
+    TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&packed), std::max<uint64_t>(max_groups, 1) * P.hstride * 8,
+                      "group gather allocation failed"));
+    TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream));
+    unsigned long long ng = 0;
+    TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    TGP_CUDA(cudaStreamSynchronize(ctx->stream));
+    result->ngroups = ng;
+    if (!tn && ng > group_cap) {
+        dev_free(ctx, packed);
+        return fail(ctx, TGP_CAPACITY, "group buffer too small");
+    }
+    if (nagg <= static_cast<uint32_t>(kMaxFormatAggs)) {
+        // Sort by packed key (= ascending lexicographic key order, key 0 in
+        // the top bits) and format on the device; copy the caller's arrays once.
+        const HashFormat F = hash_format();
         // Top-N: only the first min(limit, ng) groups in the aggregate's order
         // are formatted and copied.
         const uint64_t nout = tn ? std::min<uint64_t>(tn->limit, ng) : ng;
@@ -2462,6 +2521,8 @@ struct MergeRec {
     QueryState qs, cqs;
     size_t block_off = 0, cblock_off = 0;
     std::vector<uint8_t> tvalid;         // per bucket combination: some member accepts it
+    std::vector<uint32_t> tvbits;        // the same as a bitmap (the kernel's copy)
+    bool filter = false;                 // the hull admits rows of combinations no member accepts
     size_t tv_off = 0;
     uint64_t nbucket_tuples() const {
         uint64_t n = 1;
@@ -2482,6 +2543,9 @@ struct MergeRec {
             }
             tvalid[t] = mask != 0;
         }
+        tvbits.assign((n + 31) / 32, 0u);
+        for (uint64_t t = 0; t < n; ++t)
+            if (tvalid[t]) tvbits[t / 32] |= 1u << (t % 32);
     }
 };
 
@@ -2754,6 +2818,29 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
                 bk.column = C;
                 bk.side = TGP_SIDE_PROBE;
                 M->group.push_back(bk);
+            }
+            // The kernel drops rows of bucket combinations no member accepts
+            // only when the hull lets some through: a digit inside a hull
+            // that no member accepts (a gap between members' ranges), or
+            // digits of different columns whose members do not meet.
+            {
+                M->fill_tvalid();
+                std::vector<std::vector<uint8_t>> inside(vary.size());
+                for (size_t c = 0; c < vary.size(); ++c) {
+                    std::vector<uint8_t> seen(M->cols[c].bucket_mask.size(), 0);
+                    for (uint64_t r = hull[c].first; r <= hull[c].second; ++r) seen[M->cols[c].hlut[r]] = 1;
+                    for (size_t d = 0; d < seen.size(); ++d)
+                        if (seen[d]) inside[c].push_back(static_cast<uint8_t>(d));
+                }
+                std::vector<uint64_t> tuples(1, 0);
+                for (size_t c = 0; c < vary.size(); ++c) {
+                    std::vector<uint64_t> next;
+                    for (uint64_t t : tuples)
+                        for (uint8_t d : inside[c]) next.push_back(t * M->cols[c].bucket_mask.size() + d);
+                    tuples.swap(next);
+                }
+                M->filter = false;
+                for (uint64_t t : tuples) M->filter = M->filter || !M->tvalid[t];
             }
             for (uint32_t k = 0; k < q0->ngroup; ++k) M->group.push_back(q0->group[k]);
             M->q = *q0;
@@ -3102,9 +3189,8 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             c.lut_off = off;
             off = align256(off + c.hlut.size());
         }
-        M->fill_tvalid();
         M->tv_off = off;
-        off = align256(off + M->tvalid.size());
+        off = align256(off + M->tvbits.size() * 4);
     }
     const size_t blocks_off = off;
     B->blocks_off = blocks_off;
@@ -3157,7 +3243,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     // merged queries hold no MIN / MAX identities beyond their own images).
     for (auto& M : B->merges) {
         for (const MergeCol& c : M->cols) std::memcpy(h + c.lut_off, c.hlut.data(), c.hlut.size());
-        std::memcpy(h + M->tv_off, M->tvalid.data(), M->tvalid.size());
+        std::memcpy(h + M->tv_off, M->tvbits.data(), M->tvbits.size() * 4);
         auto place = [&](QueryState& qs, size_t boff) {
             Plan& P = qs.b->P;
             unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + boff);
@@ -3172,7 +3258,7 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
                 P.lut_cells[c] = static_cast<uint32_t>(M->cols[c].hlut.size());
                 ts *= M->cols[c].bucket_mask.size();
             }
-            P.tvalid = B->dev + M->tv_off;
+            P.tvalid = M->filter ? reinterpret_cast<const uint32_t*>(B->dev + M->tv_off) : nullptr;
             P.ntuples = static_cast<uint32_t>(M->tvalid.size());
             if (qs.has_minmax()) {
                 std::vector<unsigned long long> img;

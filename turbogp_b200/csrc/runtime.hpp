@@ -72,6 +72,15 @@ cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, con
                                void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
                                int sms, cudaStream_t st);
 size_t format_hash_groups_scratch(uint64_t n, uint32_t key_bits);
+// Directly indexed group tables (Plan::hdirect): count_direct_groups writes
+// the number of occupied slots to the device word `total` (scratch:
+// direct_groups_scratch bytes, kept for format_direct_groups), then
+// format_direct_groups writes the groups in slot (= key) order, at most cap.
+size_t direct_groups_scratch(uint64_t nslots);
+cudaError_t count_direct_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride, void* scratch,
+                                size_t scratch_bytes, unsigned long long* total, cudaStream_t st);
+cudaError_t format_direct_groups(const unsigned long long* htab, uint64_t nslots, const void* scratch, uint64_t cap,
+                                 const HashFormat& F, uint64_t* keys_out, tgp_agg_value* vals_out, cudaStream_t st);
 // The first min(limit, n) gathered groups in the order of one aggregate
 // (ties in ascending key order), formatted like format_hash_groups.
 // Scratch: format_hash_groups_scratch(n, 64) bytes.

@@ -499,6 +499,17 @@ __device__ __forceinline__ long long* priv_values(const Plan& P, uint8_t* extra)
 // with kErrHashFull raised.
 constexpr uint32_t kSmemProbes = 2;
 __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, uint64_t key) {
+    if (P.hdirect) {
+        // Every writer stores the same key word: a plain store marks the
+        // slot occupied without a read.
+        if (key > P.hmask) {
+            atomicOr(P.err, kErrHashFull);
+            return nullptr;
+        }
+        unsigned long long* s = P.htab + key * P.hstride;
+        *s = key;
+        return s;
+    }
     uint64_t h = hash_slot(key, P.hlog2);
     for (uint64_t n = 0; n <= P.hmask; ++n) {
         unsigned long long* s = P.htab + h * P.hstride;
@@ -1138,9 +1149,12 @@ template <int NT>
 __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
                                                uint32_t m, const uint32_t* gin = nullptr) {
     constexpr int R = kTileRows / NT;
-    uint32_t g[R];
+    uint32_t g[R], tix[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
+    for (int r = 0; r < R; ++r) {
+        g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
+        tix[r] = 0;
+    }
 #pragma unroll 1
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         const GKey& K = P.gkey[k];
@@ -1149,12 +1163,25 @@ __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, co
         load_cells32<R>(stage + K.soff, K.dtype, t, x);
         const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
         if (K.lut) {
+            // A bucket key also adds its digit to the row's bucket combination.
+            const uint32_t ts = P.tstride[k];
 #pragma unroll
-            for (int r = 0; r < R; ++r) g[r] += static_cast<uint32_t>(__ldg(K.lut + (x[r] - mn))) * st;
+            for (int r = 0; r < R; ++r) {
+                const uint32_t d = __ldg(K.lut + (x[r] - mn));
+                g[r] += d * st;
+                tix[r] += d * ts;
+            }
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
         }
+    }
+    // Merged scans: rows of a bucket combination no member accepts add nothing.
+    if (P.tvalid) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !((__ldg(P.tvalid + (tix[r] >> 5)) >> (tix[r] & 31u)) & 1u)))
+                m &= ~(1u << r);
     }
     const uint32_t W = P.s32_words;
     uint32_t* tab = reinterpret_cast<uint32_t*>(extra) + static_cast<size_t>((t >> 5) % P.s32_copies) * P.ngroups * W;
@@ -1502,7 +1529,8 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
 // ---------------------------------------------------------------------------
 // Merged scans: drops the selected rows whose bucket combination no member
 // accepts (P.tvalid), and any row whose bucket key cell lies outside its
-// table, so that the group index never reads a bucket table out of range.
+// table (the cells of a column lie in its table, [min, max] of the column's
+// statistics; the check costs one compare).
 // ---------------------------------------------------------------------------
 template <int R, bool TAIL>
 __device__ __forceinline__ uint32_t tuple_filter(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t t,
@@ -1532,7 +1560,8 @@ __device__ __forceinline__ uint32_t tuple_filter(const Plan& P, const uint8_t* s
     }
 #pragma unroll
     for (int r = 0; r < R; ++r)
-        if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !__ldg(P.tvalid + tix[r]))) m &= ~(1u << r);
+        if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !((__ldg(P.tvalid + (tix[r] >> 5)) >> (tix[r] & 31u)) & 1u)))
+            m &= ~(1u << r);
     return m;
 }
 
@@ -1548,9 +1577,11 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     const uint64_t r0 = tile * kTileRows;
     const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
     uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
+    // (The dense 32-bit limb path checks the combination itself, from the
+    // digits it computes anyway.)
     if constexpr (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
                   MODE == MODE_GROUP_SHARED32) {
-        if (P.tvalid) m = tuple_filter<R, TAIL>(P, stage, r0, t, m);
+        if (P.tvalid && (TAIL || MODE != MODE_GROUP_SHARED32 || !P.dense_vec)) m = tuple_filter<R, TAIL>(P, stage, r0, t, m);
     }
     const uint32_t lane = t & 31u;
     selected += __popc(m);
