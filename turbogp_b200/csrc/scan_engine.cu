@@ -725,7 +725,7 @@ struct Sink {
             // recombine exactly.
             const uint32_t g = group_index<TAIL>(P, stage, r0, rl, brow, gpay);
             uint32_t* tab = reinterpret_cast<uint32_t*>(extra) +
-                            (static_cast<size_t>((t >> 5) % P.s32_copies) * P.ngroups + g) * P.s32_words;
+                            (static_cast<size_t>((t >> 5) & (P.s32_copies - 1u)) * P.ngroups + g) * P.s32_words;
             atomicAdd(&tab[0], 1u);
 #pragma unroll 1
             for (uint32_t v = 0; v < P.nval; ++v) {
@@ -1184,7 +1184,8 @@ __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, co
                 m &= ~(1u << r);
     }
     const uint32_t W = P.s32_words;
-    uint32_t* tab = reinterpret_cast<uint32_t*>(extra) + static_cast<size_t>((t >> 5) % P.s32_copies) * P.ngroups * W;
+    // (s32_copies is a power of two.)
+    uint32_t* tab = reinterpret_cast<uint32_t*>(extra) + static_cast<size_t>((t >> 5) & (P.s32_copies - 1u)) * P.ngroups * W;
 #pragma unroll
     for (int r = 0; r < R; ++r)
         if ((m >> r) & 1u) atomicAdd(&tab[g[r] * W], 1u);
@@ -1220,16 +1221,23 @@ __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, co
             cur[r] = (S.flags & CS_CHAIN) ? static_cast<int64_t>(static_cast<uint64_t>(cur[r]) * static_cast<uint64_t>(f[r]))
                                           : f[r];
         if (S.acc) {
+            // All of the thread's low-limb adds are issued before any of
+            // their returned values is used, so their latencies overlap; the
+            // high limb then takes the value's high half plus the carry.
             const uint32_t w0 = 1u + 2u * (S.acc - 1u);
+            uint32_t old[R], xl[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int64_t x = S.kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : cur[r];
+                xl[r] = static_cast<uint32_t>(x);
+                old[r] = ((m >> r) & 1u) ? atomicAdd(&tab[g[r] * W + w0], xl[r]) : 0u;
+            }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (!((m >> r) & 1u)) continue;
                 const int64_t x = S.kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : cur[r];
-                uint32_t* e = &tab[g[r] * W + w0];
-                const uint32_t xl = static_cast<uint32_t>(x);
-                const uint32_t old = atomicAdd(e, xl);
-                const int32_t add = static_cast<int32_t>(x >> 32) + ((old + xl < old) ? 1 : 0);
-                if (add) atomicAdd(reinterpret_cast<int*>(e + 1), add);
+                const int32_t add = static_cast<int32_t>(x >> 32) + ((old[r] + xl[r] < old[r]) ? 1 : 0);
+                if (add) atomicAdd(reinterpret_cast<int*>(&tab[g[r] * W + w0 + 1]), add);
             }
         }
     }
@@ -1495,34 +1503,78 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
     for (int v = 0; v < 2; ++v)
         if (static_cast<uint32_t>(v) < P.nval) load_cells64<R>(stage + P.val[v].f[0].soff, P.val[v].f[0].dtype, t, vc[v]);
     const uint32_t nv1 = P.nval + 1;
+    // Keys and value arguments of the thread's R rows.
+    uint64_t key[R];
+    int64_t x[R][2];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        if (!((m >> r) & 1u)) continue;
-        int64_t x[2];
 #pragma unroll
         for (int v = 0; v < 2; ++v) {
             if (static_cast<uint32_t>(v) >= P.nval) continue;
             const Factor& F = P.val[v].f[0];
             const int64_t a = static_cast<int64_t>(static_cast<uint64_t>(F.mul) * static_cast<uint64_t>(vc[v][r]) +
                                                    static_cast<uint64_t>(F.add));
-            x[v] = P.val[v].kind == VK_COUNT_NZ ? (a != 0 ? 1 : 0) : a;
+            x[r][v] = P.val[v].kind == VK_COUNT_NZ ? (a != 0 ? 1 : 0) : a;
         }
         const uint64_t rel = static_cast<uint64_t>(kc[r]) - static_cast<uint64_t>(K.min);
-        const uint64_t key = MODE == MODE_GROUP_HASH ? (rel << K.shift) : rel * K.stride;
-        if (P.hsm_slots && presum_add_x(P, extra, key, x)) continue;
+        key[r] = MODE == MODE_GROUP_HASH ? (rel << K.shift) : rel * K.stride;
+    }
+    // Shared pre-aggregation: the first probe's key loads of all R rows are
+    // issued together, then each row either adds to its slot (the common
+    // case once the table holds the hot keys), claims an empty one, tries
+    // the second probe, or falls through to the global table.
+    uint32_t pend = m;
+    if (P.hsm_slots) {
+        const uint32_t HS = P.hsm_slots;
+        unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
+        uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
+        int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
+        uint32_t h[R];
+        unsigned long long k0[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            h[r] = static_cast<uint32_t>(hash_slot(key[r], P.hsm_log2));
+            k0[r] = ((m >> r) & 1u) ? *reinterpret_cast<volatile unsigned long long*>(&keys[h[r]]) : 0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (!((m >> r) & 1u)) continue;
+            uint32_t hs = h[r];
+            unsigned long long k = k0[r];
+#pragma unroll
+            for (uint32_t n = 0; n < kSmemProbes; ++n) {
+                if (n) {
+                    hs = (hs + 1) & (HS - 1);
+                    k = *reinterpret_cast<volatile unsigned long long*>(&keys[hs]);
+                }
+                if (k == kEmpty) k = atomicCAS(&keys[hs], kEmpty, key[r]);
+                if (k == kEmpty || k == key[r]) {
+                    atomicAdd(&cnt[hs], 1u);
+#pragma unroll
+                    for (int v = 0; v < 2; ++v)
+                        if (static_cast<uint32_t>(v) < P.nval) atomicAdd(&sums[v * HS + hs], static_cast<int32_t>(x[r][v]));
+                    pend &= ~(1u << r);
+                    break;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (!((pend >> r) & 1u)) continue;
         unsigned long long* base;
         if (MODE == MODE_GROUP_HASH) {
-            unsigned long long* slot = hash_group_slot(P, key);
+            unsigned long long* slot = hash_group_slot(P, key[r]);
             if (slot == nullptr) continue;
             base = slot + 1;   // [key][count][v0 lo][v0 hi]...
         } else {
-            base = P.acc + key * nv1 * 2;   // [count lo][count hi][v0 lo][v0 hi]...
+            base = P.acc + key[r] * nv1 * 2;   // [count lo][count hi][v0 lo][v0 hi]...
         }
         atomicAdd(base, 1ull);
 #pragma unroll
         for (int v = 0; v < 2; ++v)
             if (static_cast<uint32_t>(v) < P.nval)
-                acc_global_i64(base + (MODE == MODE_GROUP_HASH ? 1 : 2) + 2 * v, VK_SUM, x[v], P.sum64 != 0);
+                acc_global_i64(base + (MODE == MODE_GROUP_HASH ? 1 : 2) + 2 * v, VK_SUM, x[r][v], P.sum64 != 0);
     }
 }
 
