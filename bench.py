@@ -307,7 +307,7 @@ def run_reference_workload(args, world: int, rank: int) -> None:
     if rank != 0:
         return
     name = args.workload
-    if name in ("batch", "serve", "pgwire"):
+    if name in ("batch", "serve", "pgwire", "merged"):
         print(json.dumps({"impl": "reference", "unavailable": f"{name}: the reference has no batched-submission "
                           "or serving CPU path to time (the plain one-query-at-a-time arm is in this "
                           "workload's own line)"}), flush=True)
@@ -695,6 +695,8 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     ctx = Context(local)
     if args.workload == "batch":
         rec = measure_batch(ctx, args, world, rank, local)
+    elif args.workload == "merged":
+        rec = measure_merged(ctx, args, world, rank, local)
     else:
         rec = measure_workload(args.workload, ctx, args, world, rank, local)
     if rank == 0:
@@ -703,6 +705,91 @@ def run_workload(args, world: int, rank: int, local: int) -> None:
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def serve_templates(f, j):
+    """The three light serving templates over the fact table (and the join)."""
+    from turbogp_b200 import workloads
+    t_scan, t_fga, tj = workloads.selective_scan_sum(), workloads.filtered_group_agg(), workloads.join_group_agg()
+    return {"scan": lambda: f.prepare(t_scan.aggs, t_scan.group_by, t_scan.where),
+            "fga": lambda: f.prepare(t_fga.aggs, t_fga.group_by, t_fga.where),
+            "join": lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk")}
+
+
+def serve_literals(rng, kind):
+    """A request's WHERE for a light serving template, random literals."""
+    from turbogp_b200 import datagen
+    from turbogp_b200.engine import col
+    D0, ND = datagen.DAY0, datagen.NDAYS
+    if kind == "scan":
+        lo = D0 + int(rng.integers(0, ND - 30))
+        return ((col("ship_day") >= lo) & (col("ship_day") < lo + int(rng.integers(30, 366))) &
+                col("discount_pct").between(int(rng.integers(0, 6)), int(rng.integers(5, 11))) &
+                (col("quantity") < int(rng.integers(2, 51))))
+    if kind == "fga":
+        return col("ship_day") <= D0 + int(rng.integers(3, ND))
+    return col("quantity") < int(rng.integers(2, 51))
+
+
+def measure_merged(ctx, args, world: int, rank: int, local: int, fact_host: dict | None = None) -> dict:
+    """Merged scans: per light serving template, a batch of `--members`
+    requests with random literals (one merged scan per template class, plus a
+    per-bucket count scan for the join) against one of them run alone. Device
+    time from events around each scan launch (queued behind a device delay);
+    every member of the first batch is checked against the same request run
+    alone. With --profile-window, the timed batches run between
+    cudaProfilerStart and cudaProfilerStop (for `ncu --profile-from-start off`)."""
+    import numpy as np
+    import torch
+    from turbogp_b200 import datagen, workloads
+    n = args.rows if (args.rows != ROWS and args.workload == "merged") else 60_000_000
+    host = fact_host if fact_host is not None and rank == 0 else datagen.fact_fk(n, DIM_ROWS, 0.8, seed=3 + rank)
+    f = ctx.register({k: v[:n] for k, v in host.items()}, {**datagen.LINEITEM_COLTYPES, "fk": "int"})
+    d = ctx.register(datagen.dimension(DIM_ROWS, seed=2 + rank), datagen.DIMENSION_COLTYPES)
+    j = d.join_build("key", workloads.join_group_agg().build_where)
+    make = serve_templates(f, j)
+    kinds = [args.merged_class] if args.merged_class else list(make)
+    rng = np.random.default_rng(31 + rank)
+    nb = args.members
+    steps = args.steps if args.steps != 3000 else 5
+    out = {}
+    for kind in kinds:
+        pqs = [make[kind]() for _ in range(nb)]
+        batch = [pq.rebind(serve_literals(rng, kind)) for pq in pqs]
+        merged = ctx.submit(batch).wait()
+        alone = [make[kind]().rebind(pq.spec["where"]).run() for pq in batch]
+        same = all(same_output(a, b) for a, b in zip(merged, alone))
+        if not same:
+            raise SystemExit(f"merged {kind}: a member differs from the same request alone")
+        for _ in range(args.warmup):
+            ctx.submit([pq.rebind(serve_literals(rng, kind)) for pq in pqs], decode=False).wait()
+        ctx.profile(True, gated=True)
+        ctx.profile_read()
+        if args.profile_window:
+            torch.cuda.synchronize()
+            torch.cuda.cudart().cudaProfilerStart()
+        per = []
+        for _ in range(steps):
+            ctx.submit([pq.rebind(serve_literals(rng, kind)) for pq in pqs], decode=False).wait()
+            per.append(ctx.profile_read())
+        if args.profile_window:
+            torch.cuda.cudart().cudaProfilerStop()
+        one = make[kind]()
+        plain = []
+        for _ in range(steps):
+            one.rebind(serve_literals(rng, kind)).run(decode=False)
+            plain.append(ctx.profile_read()[1])
+        ctx.profile(False)
+        mk = float(np.median([ms for _, ms in per]))
+        pk = float(np.median(plain))
+        out[kind] = {"members": nb, "merged_kernel_ms": mk, "launches": int(per[0][0]), "alone_kernel_ms": pk,
+                     "alone_ms_x_members_over_merged": pk * nb / mk if mk else None, "same_as_alone": same}
+    j.drop()
+    f.drop()
+    d.drop()
+    return {"workload": f"merged scans: {nb} requests of each light serving template with random literals over "
+                        f"a {n}-row fact table, one batch", "records": out, "steps": steps,
+            "timing": "device events around each scan launch, launch queued behind a device delay"}
 
 
 def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict | None = None,
@@ -738,32 +825,18 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     hch = hc_host if hc_host is not None and rank == 0 else \
         datagen.highcard(args.highcard_rows, 10_000_000, 1.1, seed=4 + rank)
     hc = ctx_heavy.register(hch)
-    t_scan, t_fga = workloads.selective_scan_sum(), workloads.filtered_group_agg()
     hc_aggs = [count_star(), sum_(col("value"))]
-    templates = {
-        "scan": serving.Template("scan", lambda: f.prepare(t_scan.aggs, t_scan.group_by, t_scan.where)),
-        "fga": serving.Template("fga", lambda: f.prepare(t_fga.aggs, t_fga.group_by, t_fga.where)),
-        "join": serving.Template("join", lambda: f.prepare(tj.aggs, tj.group_by, None, join=j, probe_key="fk")),
-        "highcard": serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None, group_cap=10_000_000),
-                                     heavy=True),
-    }
+    templates = {name: serving.Template(name, mk) for name, mk in serve_templates(f, j).items()}
+    templates["highcard"] = serving.Template("highcard", lambda: hc.prepare(hc_aggs, ("key",), None,
+                                                                            group_cap=10_000_000), heavy=True)
     rng = np.random.default_rng(21 + rank)
-    D0, ND = datagen.DAY0, datagen.NDAYS
 
     def request(t):
         u = rng.random()
         if u < 0.002:
             return serving.Request(t, "highcard", None)
-        k = int(rng.integers(0, 3))
-        if k == 0:
-            lo = D0 + int(rng.integers(0, ND - 30))
-            w = ((col("ship_day") >= lo) & (col("ship_day") < lo + int(rng.integers(30, 366))) &
-                 col("discount_pct").between(int(rng.integers(0, 6)), int(rng.integers(5, 11))) &
-                 (col("quantity") < int(rng.integers(2, 51))))
-            return serving.Request(t, "scan", w)
-        if k == 1:
-            return serving.Request(t, "fga", col("ship_day") <= D0 + int(rng.integers(3, ND)))
-        return serving.Request(t, "join", col("quantity") < int(rng.integers(2, 51)))
+        kind = ("scan", "fga", "join")[int(rng.integers(0, 3))]
+        return serving.Request(t, kind, serve_literals(rng, kind))
 
     def stream(rate, count):
         return [request(t) for t in serving.poisson_arrivals(rate, count, rng)]
@@ -1037,7 +1110,11 @@ def main() -> None:
     ap.add_argument("--no-autotune", action="store_true", help="run the planner's rules (profiling captures)")
     ap.add_argument("--workload", default="selective_scan_sum",
                     choices=["selective_scan_sum", "filtered_group_agg", "join_group_agg", "highcard_group", "batch",
-                             "serve"])
+                             "serve", "merged"])
+    ap.add_argument("--members", type=int, default=16, help="merged: requests per batch")
+    ap.add_argument("--merged-class", default="", choices=["", "scan", "fga", "join"], help="merged: one template only")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="merged: timed batches between cudaProfilerStart / Stop")
     ap.add_argument("--rate", type=float, default=2000.0, help="(unused: serve offers multiples of the plain capacity)")
     ap.add_argument("--requests", type=int, default=3000, help="serve: requests in the batched streams")
     ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
