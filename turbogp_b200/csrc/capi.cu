@@ -2520,32 +2520,10 @@ struct MergeRec {
     bool has_count = false;
     QueryState qs, cqs;
     size_t block_off = 0, cblock_off = 0;
-    std::vector<uint8_t> tvalid;         // per bucket combination: some member accepts it
-    std::vector<uint32_t> tvbits;        // the same as a bitmap (the kernel's copy)
-    bool filter = false;                 // the hull admits rows of combinations no member accepts
-    size_t tv_off = 0;
     uint64_t nbucket_tuples() const {
         uint64_t n = 1;
         for (const MergeCol& c : cols) n *= c.bucket_mask.size();
         return n;
-    }
-    // Bucket combinations t = ((d0 * n1) + d1) * n2 + d2 (the first column
-    // most significant), valid when the members accepting every digit meet.
-    void fill_tvalid() {
-        const uint64_t n = nbucket_tuples();
-        tvalid.assign(n, 0);
-        for (uint64_t t = 0; t < n; ++t) {
-            uint64_t rest = t, mask = ~0ull;
-            for (size_t c = cols.size(); c-- > 0;) {
-                const uint64_t nb = cols[c].bucket_mask.size();
-                mask &= cols[c].bucket_mask[rest % nb];
-                rest /= nb;
-            }
-            tvalid[t] = mask != 0;
-        }
-        tvbits.assign((n + 31) / 32, 0u);
-        for (uint64_t t = 0; t < n; ++t)
-            if (tvalid[t]) tvbits[t / 32] |= 1u << (t % 32);
     }
 };
 
@@ -2818,29 +2796,6 @@ static void find_merges(tgp_ctx* ctx, BatchRec& B) {
                 bk.column = C;
                 bk.side = TGP_SIDE_PROBE;
                 M->group.push_back(bk);
-            }
-            // The kernel drops rows of bucket combinations no member accepts
-            // only when the hull lets some through: a digit inside a hull
-            // that no member accepts (a gap between members' ranges), or
-            // digits of different columns whose members do not meet.
-            {
-                M->fill_tvalid();
-                std::vector<std::vector<uint8_t>> inside(vary.size());
-                for (size_t c = 0; c < vary.size(); ++c) {
-                    std::vector<uint8_t> seen(M->cols[c].bucket_mask.size(), 0);
-                    for (uint64_t r = hull[c].first; r <= hull[c].second; ++r) seen[M->cols[c].hlut[r]] = 1;
-                    for (size_t d = 0; d < seen.size(); ++d)
-                        if (seen[d]) inside[c].push_back(static_cast<uint8_t>(d));
-                }
-                std::vector<uint64_t> tuples(1, 0);
-                for (size_t c = 0; c < vary.size(); ++c) {
-                    std::vector<uint64_t> next;
-                    for (uint64_t t : tuples)
-                        for (uint8_t d : inside[c]) next.push_back(t * M->cols[c].bucket_mask.size() + d);
-                    tuples.swap(next);
-                }
-                M->filter = false;
-                for (uint64_t t : tuples) M->filter = M->filter || !M->tvalid[t];
             }
             for (uint32_t k = 0; k < q0->ngroup; ++k) M->group.push_back(q0->group[k]);
             M->q = *q0;
@@ -3189,8 +3144,6 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
             c.lut_off = off;
             off = align256(off + c.hlut.size());
         }
-        M->tv_off = off;
-        off = align256(off + M->tvbits.size() * 4);
     }
     const size_t blocks_off = off;
     B->blocks_off = blocks_off;
@@ -3243,23 +3196,13 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     // merged queries hold no MIN / MAX identities beyond their own images).
     for (auto& M : B->merges) {
         for (const MergeCol& c : M->cols) std::memcpy(h + c.lut_off, c.hlut.data(), c.hlut.size());
-        std::memcpy(h + M->tv_off, M->tvbits.data(), M->tvbits.size() * 4);
         auto place = [&](QueryState& qs, size_t boff) {
             Plan& P = qs.b->P;
             unsigned long long* blk = reinterpret_cast<unsigned long long*>(B->dev + blocks_off + boff);
             P.counters = blk;
             P.err = reinterpret_cast<uint32_t*>(blk + 4);
             P.acc = blk + 6;
-            // The bucket keys are the plan's first group keys, in column order.
-            uint64_t ts = 1;
-            for (size_t c = M->cols.size(); c-- > 0;) {
-                P.gkey[c].lut = B->dev + M->cols[c].lut_off;
-                P.tstride[c] = static_cast<uint32_t>(ts);
-                P.lut_cells[c] = static_cast<uint32_t>(M->cols[c].hlut.size());
-                ts *= M->cols[c].bucket_mask.size();
-            }
-            P.tvalid = M->filter ? reinterpret_cast<const uint32_t*>(B->dev + M->tv_off) : nullptr;
-            P.ntuples = static_cast<uint32_t>(M->tvalid.size());
+            for (size_t c = 0; c < M->cols.size(); ++c) P.gkey[c].lut = B->dev + M->cols[c].lut_off;
             if (qs.has_minmax()) {
                 std::vector<unsigned long long> img;
                 init_acc_image(P, qs.ngroups_direct, &img);

@@ -256,16 +256,6 @@ struct alignas(16) Plan {
     // (0 = kWaitLimitNs).
     uint64_t skip_tile1;
     uint64_t wait_ns;
-    // Merged scans: bit t of tvalid (u32 words) is set iff some member accepts
-    // bucket combination t = sum over bucket keys k of digit_k * tstride[k]
-    // (t < ntuples); a row of any other combination (or a key cell outside
-    // its bucket table's lut_cells) is dropped before it reaches the
-    // accumulators. A bitmap, so that it stays in the L1 that the stage ring
-    // leaves. Null = off.
-    const uint32_t* tvalid;
-    uint32_t tstride[kMaxGroupKeys];
-    uint32_t lut_cells[kMaxGroupKeys];
-    uint32_t ntuples;
     // MODE_GROUP_HASH, one key over a moderate range: the slot of a key is
     // the key itself (relative to its minimum; hmask = the last slot), so a
     // row's update needs no probe, no compare and no claim.

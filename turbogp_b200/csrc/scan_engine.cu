@@ -1149,12 +1149,9 @@ template <int NT>
 __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
                                                uint32_t m, const uint32_t* gin = nullptr) {
     constexpr int R = kTileRows / NT;
-    uint32_t g[R], tix[R];
+    uint32_t g[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
-        tix[r] = 0;
-    }
+    for (int r = 0; r < R; ++r) g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
 #pragma unroll 1
     for (uint32_t k = 0; k < P.ngkey; ++k) {
         const GKey& K = P.gkey[k];
@@ -1163,25 +1160,12 @@ __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, co
         load_cells32<R>(stage + K.soff, K.dtype, t, x);
         const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
         if (K.lut) {
-            // A bucket key also adds its digit to the row's bucket combination.
-            const uint32_t ts = P.tstride[k];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t d = __ldg(K.lut + (x[r] - mn));
-                g[r] += d * st;
-                tix[r] += d * ts;
-            }
+            for (int r = 0; r < R; ++r) g[r] += static_cast<uint32_t>(__ldg(K.lut + (x[r] - mn))) * st;
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
         }
-    }
-    // Merged scans: rows of a bucket combination no member accepts add nothing.
-    if (P.tvalid) {
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !((__ldg(P.tvalid + (tix[r] >> 5)) >> (tix[r] & 31u)) & 1u)))
-                m &= ~(1u << r);
     }
     const uint32_t W = P.s32_words;
     // (s32_copies is a power of two.)
@@ -1486,6 +1470,28 @@ __device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t*
     return hit;
 }
 
+// Payload lookups of one tile issued ahead of their use (pipe_consume): the
+// values for the thread's R rows, passed by value so they stay in registers.
+template <int R>
+struct PayAhead {
+    bool on;
+    uint32_t g[R];
+};
+
+// The payload lookups of all R rows of a staged tile (selected or not).
+template <int R>
+__device__ __forceinline__ void join_pay_prefetch(const Plan& P, const uint8_t* stage, uint32_t t, uint32_t (&g)[R]) {
+    const uint8_t* kb = stage + P.slot[P.jslot].smem_off;
+    const uint32_t kdt = P.slot[P.jslot].dtype;
+    int64_t cell[R];
+    load_cells64<R>(kb, kdt, t, cell);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint64_t rel = static_cast<uint64_t>(cell[r]) - static_cast<uint64_t>(P.jkmin);
+        g[r] = rel <= P.jkrange ? __ldg(P.jpay + rel) : kNoPay;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Global / hash grouping by one staged key with one or two values, each a
 // SUM or COUNT(col) of one staged affine factor (P.hash_fast): the thread's R
@@ -1579,62 +1585,17 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
 }
 
 // ---------------------------------------------------------------------------
-// Merged scans: drops the selected rows whose bucket combination no member
-// accepts (P.tvalid), and any row whose bucket key cell lies outside its
-// table (the cells of a column lie in its table, [min, max] of the column's
-// statistics; the check costs one compare).
-// ---------------------------------------------------------------------------
-template <int R, bool TAIL>
-__device__ __forceinline__ uint32_t tuple_filter(const Plan& P, const uint8_t* stage, uint64_t r0, uint32_t t,
-                                                 uint32_t m) {
-    constexpr uint32_t kBad = 0xffffffffu;
-    uint32_t tix[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) tix[r] = 0;
-#pragma unroll 1
-    for (uint32_t k = 0; k < P.ngkey; ++k) {
-        const GKey& K = P.gkey[k];
-        if (!K.lut) continue;
-        const uint32_t ts = P.tstride[k], cells = P.lut_cells[k], mn = static_cast<uint32_t>(K.min);
-        uint32_t x[R];
-        if (!TAIL) {
-            load_cells32<R>(stage + K.soff, K.dtype, t, x);
-        } else {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                x[r] = ((m >> r) & 1u) ? static_cast<uint32_t>(key_cell<true>(P, K, stage, r0, R * t + r, 0)) : mn;
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const uint32_t rel = x[r] - mn;
-            tix[r] = (rel < cells && tix[r] != kBad) ? tix[r] + static_cast<uint32_t>(__ldg(K.lut + rel)) * ts : kBad;
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (((m >> r) & 1u) && (tix[r] >= P.ntuples || !((__ldg(P.tvalid + (tix[r] >> 5)) >> (tix[r] & 31u)) & 1u)))
-            m &= ~(1u << r);
-    return m;
-}
-
-// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
 __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
                                              const uint8_t* stage, uint64_t tile, uint32_t t,
                                              unsigned long long& selected, const RegLeaves& RL,
-                                             const RegVals& RV) {
+                                             const RegVals& RV, const PayAhead<kTileRows / NT> pre = {}) {
     constexpr int R = kTileRows / NT;
     const uint64_t r0 = tile * kTileRows;
     const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
-    uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
-    // (The dense 32-bit limb path checks the combination itself, from the
-    // digits it computes anyway.)
-    if constexpr (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
-                  MODE == MODE_GROUP_SHARED32) {
-        if (P.tvalid && (TAIL || MODE != MODE_GROUP_SHARED32 || !P.dense_vec)) m = tuple_filter<R, TAIL>(P, stage, r0, t, m);
-    }
+    const uint32_t m = (!TAIL && RL.n) ? eval_reg_leaves<R>(RL, stage, t) : eval_pred<R, TAIL>(P, stage, r0, t, nrem);
     const uint32_t lane = t & 31u;
     selected += __popc(m);
     if (MODE == MODE_GROUP_PRIVATE && P.count_by_tile) {
@@ -1721,7 +1682,17 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
                                MODE == MODE_GROUP_SHARED32)) {
         if (!TAIL && P.jpay) {
             uint32_t g[R];
-            const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
+            uint32_t hit = 0;
+            if (pre.on) {
+                // Looked up one tile ahead (pipe_consume).
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    g[r] = ((m >> r) & 1u) ? pre.g[r] : kNoPay;
+                    hit |= (g[r] != kNoPay ? 1u : 0u) << r;
+                }
+            } else {
+                hit = join_pay_probe<R>(P, stage, t, m, g);
+            }
             if constexpr (MODE == MODE_GROUP_SHARED32) {
                 if (P.dense_vec) {
                     chain_s32_tile<NT>(P, extra, stage, t, hit, g);
@@ -1872,25 +1843,62 @@ __device__ __forceinline__ bool pipe_consume(const Plan& P, Sink<MODE, ACC128, N
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     const uint64_t nfull = P.nrows / kTileRows;
     const uint32_t S = P.nstages;
+    // Waits (bounded) until stage s of phase ph has landed; false after a
+    // timeout or an abort.
+    auto land = [&](uint32_t s, uint32_t ph) -> bool {
+        bool landed = false;
+        if (lane == 0) landed = mbar_wait_bounded(&full[s], ph, P.wait_ns);
+        landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
+        if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
+            if (lane == 0) {
+                atomicOr(P.err, kErrWaitTimeout);
+                atomicExch(abort_flag, 1u);
+            }
+            return false;
+        }
+        // Lanes other than 0 observe the completed phase through a cheap
+        // try_wait so their shared-memory reads are ordered after the copy.
+        mbar_try_wait(&full[s], ph);
+        return true;
+    };
+    // Joined aggregates through a payload array look the next tile's
+    // payloads up before accumulating the current one, so twice the L2
+    // lookups are in flight. The consumer then holds two stages at once; the
+    // producer's previous use of the next stage was released at least one
+    // tile earlier, so with two or more stages neither side waits on the other.
+    constexpr int R = kTileRows / NT;
+    constexpr bool kPayModes = !std::is_same<SH, ScalarTag>::value &&
+                               (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
+                                MODE == MODE_GROUP_SHARED32);
+    const bool ahead = kPayModes && P.jpay != nullptr && S >= 2;
+    PayAhead<R> nxt;
+    nxt.on = false;   // the current tile's stage has landed and nxt.g holds its payloads
     for (uint64_t k = 0; k < count; ++k) {
         const uint64_t tl = first + k * stride;
         if (tl >= ntiles) break;
         if (tl < nfull) {
-            bool landed = false;
-            if (lane == 0) landed = mbar_wait_bounded(&full[st.s], st.phase, P.wait_ns);
-            landed = __shfl_sync(kFull, landed ? 1 : 0, 0) != 0;
-            if (!landed || *reinterpret_cast<volatile uint32_t*>(abort_flag)) {
-                if (lane == 0) {
-                    atomicOr(P.err, kErrWaitTimeout);
-                    atomicExch(abort_flag, 1u);
+            if (!nxt.on && !land(st.s, st.phase)) return false;
+            const uint8_t* cur = stages + static_cast<size_t>(st.s) * P.stage_bytes;
+            PayAhead<R> pre;
+            pre.on = ahead;
+            if (ahead) {
+                if (nxt.on) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) pre.g[r] = nxt.g[r];
+                } else {
+                    join_pay_prefetch<R>(P, cur, t, pre.g);
                 }
-                return false;
+                nxt.on = false;
+                const uint64_t tn = first + (k + 1) * stride;
+                if (k + 1 < count && tn < nfull) {
+                    const uint32_t sn = st.s + 1 == S ? 0u : st.s + 1;
+                    const uint32_t pn = st.s + 1 == S ? (st.phase ^ 1u) : st.phase;
+                    if (!land(sn, pn)) return false;
+                    join_pay_prefetch<R>(P, stages + static_cast<size_t>(sn) * P.stage_bytes, t, nxt.g);
+                    nxt.on = true;
+                }
             }
-            // Lanes other than 0 observe the completed phase through a cheap
-            // try_wait so their shared-memory reads are ordered after the copy.
-            mbar_try_wait(&full[st.s], st.phase);
-            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, stages + static_cast<size_t>(st.s) * P.stage_bytes,
-                                                      tl, t, selected, RL, RV);
+            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, cur, tl, t, selected, RL, RV, pre);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st.s]);
             ++st.n;
