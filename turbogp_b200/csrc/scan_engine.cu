@@ -1470,28 +1470,6 @@ __device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t*
     return hit;
 }
 
-// Payload lookups of one tile issued ahead of their use (pipe_consume): the
-// values for the thread's R rows, passed by value so they stay in registers.
-template <int R>
-struct PayAhead {
-    bool on;
-    uint32_t g[R];
-};
-
-// The payload lookups of all R rows of a staged tile (selected or not).
-template <int R>
-__device__ __forceinline__ void join_pay_prefetch(const Plan& P, const uint8_t* stage, uint32_t t, uint32_t (&g)[R]) {
-    const uint8_t* kb = stage + P.slot[P.jslot].smem_off;
-    const uint32_t kdt = P.slot[P.jslot].dtype;
-    int64_t cell[R];
-    load_cells64<R>(kb, kdt, t, cell);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const uint64_t rel = static_cast<uint64_t>(cell[r]) - static_cast<uint64_t>(P.jkmin);
-        g[r] = rel <= P.jkrange ? __ldg(P.jpay + rel) : kNoPay;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Global / hash grouping by one staged key with one or two values, each a
 // SUM or COUNT(col) of one staged affine factor (P.hash_fast): the thread's R
@@ -1591,7 +1569,7 @@ template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
 __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, NT>& sink, uint8_t* extra,
                                              const uint8_t* stage, uint64_t tile, uint32_t t,
                                              unsigned long long& selected, const RegLeaves& RL,
-                                             const RegVals& RV, const PayAhead<kTileRows / NT> pre = {}) {
+                                             const RegVals& RV) {
     constexpr int R = kTileRows / NT;
     const uint64_t r0 = tile * kTileRows;
     const uint32_t nrem = TAIL ? static_cast<uint32_t>(P.nrows - r0) : static_cast<uint32_t>(kTileRows);
@@ -1682,17 +1660,7 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
                                MODE == MODE_GROUP_SHARED32)) {
         if (!TAIL && P.jpay) {
             uint32_t g[R];
-            uint32_t hit = 0;
-            if (pre.on) {
-                // Looked up one tile ahead (pipe_consume).
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    g[r] = ((m >> r) & 1u) ? pre.g[r] : kNoPay;
-                    hit |= (g[r] != kNoPay ? 1u : 0u) << r;
-                }
-            } else {
-                hit = join_pay_probe<R>(P, stage, t, m, g);
-            }
+            const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
             if constexpr (MODE == MODE_GROUP_SHARED32) {
                 if (P.dense_vec) {
                     chain_s32_tile<NT>(P, extra, stage, t, hit, g);
@@ -1844,7 +1812,7 @@ __device__ __forceinline__ bool pipe_consume(const Plan& P, Sink<MODE, ACC128, N
     const uint64_t nfull = P.nrows / kTileRows;
     const uint32_t S = P.nstages;
     // Waits (bounded) until stage s of phase ph has landed; false after a
-    // timeout or an abort.
+    // timeout or an abort (which it records).
     auto land = [&](uint32_t s, uint32_t ph) -> bool {
         bool landed = false;
         if (lane == 0) landed = mbar_wait_bounded(&full[s], ph, P.wait_ns);
@@ -1861,44 +1829,13 @@ __device__ __forceinline__ bool pipe_consume(const Plan& P, Sink<MODE, ACC128, N
         mbar_try_wait(&full[s], ph);
         return true;
     };
-    // Joined aggregates through a payload array look the next tile's
-    // payloads up before accumulating the current one, so twice the L2
-    // lookups are in flight. The consumer then holds two stages at once; the
-    // producer's previous use of the next stage was released at least one
-    // tile earlier, so with two or more stages neither side waits on the other.
-    constexpr int R = kTileRows / NT;
-    constexpr bool kPayModes = !std::is_same<SH, ScalarTag>::value &&
-                               (MODE == MODE_GROUP_PRIVATE || MODE == MODE_GROUP_SHARED || MODE == MODE_GROUP_GLOBAL ||
-                                MODE == MODE_GROUP_SHARED32);
-    const bool ahead = kPayModes && P.jpay != nullptr && S >= 2;
-    PayAhead<R> nxt;
-    nxt.on = false;   // the current tile's stage has landed and nxt.g holds its payloads
     for (uint64_t k = 0; k < count; ++k) {
         const uint64_t tl = first + k * stride;
         if (tl >= ntiles) break;
         if (tl < nfull) {
-            if (!nxt.on && !land(st.s, st.phase)) return false;
-            const uint8_t* cur = stages + static_cast<size_t>(st.s) * P.stage_bytes;
-            PayAhead<R> pre;
-            pre.on = ahead;
-            if (ahead) {
-                if (nxt.on) {
-#pragma unroll
-                    for (int r = 0; r < R; ++r) pre.g[r] = nxt.g[r];
-                } else {
-                    join_pay_prefetch<R>(P, cur, t, pre.g);
-                }
-                nxt.on = false;
-                const uint64_t tn = first + (k + 1) * stride;
-                if (k + 1 < count && tn < nfull) {
-                    const uint32_t sn = st.s + 1 == S ? 0u : st.s + 1;
-                    const uint32_t pn = st.s + 1 == S ? (st.phase ^ 1u) : st.phase;
-                    if (!land(sn, pn)) return false;
-                    join_pay_prefetch<R>(P, stages + static_cast<size_t>(sn) * P.stage_bytes, t, nxt.g);
-                    nxt.on = true;
-                }
-            }
-            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, cur, tl, t, selected, RL, RV, pre);
+            if (!land(st.s, st.phase)) return false;
+            process_tile<MODE, ACC128, NT, false, SH>(P, sink, extra, stages + static_cast<size_t>(st.s) * P.stage_bytes,
+                                                      tl, t, selected, RL, RV);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st.s]);
             ++st.n;
