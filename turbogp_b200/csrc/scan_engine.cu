@@ -1205,23 +1205,18 @@ __device__ __forceinline__ void chain_s32_tile(const Plan& P, uint8_t* extra, co
             cur[r] = (S.flags & CS_CHAIN) ? static_cast<int64_t>(static_cast<uint64_t>(cur[r]) * static_cast<uint64_t>(f[r]))
                                           : f[r];
         if (S.acc) {
-            // All of the thread's low-limb adds are issued before any of
-            // their returned values is used, so their latencies overlap; the
-            // high limb then takes the value's high half plus the carry.
+            // (Issuing all R low-limb adds before reading any returned value
+            // measured slower: more instructions, no latency gained.)
             const uint32_t w0 = 1u + 2u * (S.acc - 1u);
-            uint32_t old[R], xl[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int64_t x = S.kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : cur[r];
-                xl[r] = static_cast<uint32_t>(x);
-                old[r] = ((m >> r) & 1u) ? atomicAdd(&tab[g[r] * W + w0], xl[r]) : 0u;
-            }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (!((m >> r) & 1u)) continue;
                 const int64_t x = S.kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : cur[r];
-                const int32_t add = static_cast<int32_t>(x >> 32) + ((old[r] + xl[r] < old[r]) ? 1 : 0);
-                if (add) atomicAdd(reinterpret_cast<int*>(&tab[g[r] * W + w0 + 1]), add);
+                uint32_t* e = &tab[g[r] * W + w0];
+                const uint32_t xl = static_cast<uint32_t>(x);
+                const uint32_t old = atomicAdd(e, xl);
+                const int32_t add = static_cast<int32_t>(x >> 32) + ((old + xl < old) ? 1 : 0);
+                if (add) atomicAdd(reinterpret_cast<int*>(e + 1), add);
             }
         }
     }
