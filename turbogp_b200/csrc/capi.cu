@@ -672,7 +672,13 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = sc
     }
     const size_t per_cta = budget / static_cast<size_t>(std::max(1, K.ctas_per_sm));
     size_t avail = per_cta > kBarrierBytes + extra_bytes ? per_cta - kBarrierBytes - extra_bytes : 0;
-    const size_t cap = static_cast<size_t>(std::max(1, std::min(K.max_stages, kMaxStages)));
+    // Joins through a payload array take two stages unless a variant asks
+    // for fewer than the maximum: the 60M x 1.5M join probe ran 0.516 ms with
+    // four stages and 0.373 ms with two (autotuner, gated CUDA events), and
+    // merged join batches 0.85 -> 0.77 ms; the shared memory the stages leave
+    // serves as L1 for the payload lookups of hot keys.
+    const int max_st = (P.jpay != nullptr && K.max_stages >= kMaxStages) ? 2 : K.max_stages;
+    const size_t cap = static_cast<size_t>(std::max(1, std::min(max_st, kMaxStages)));
     uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
     if (S == 0) {
         // Fall back to a single CTA per SM.
