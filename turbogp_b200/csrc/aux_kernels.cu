@@ -484,7 +484,7 @@ cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long lon
 // (keys + slot words) for the host to sort; counters[0] = occupied slots.
 __global__ void gather_groups_kernel(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                      unsigned long long* out, uint64_t cap,
-                                     unsigned long long* counter) {
+                                     unsigned long long* counter, bool direct) {
     // Whole warps walk the table (the loop bound is rounded up to a warp) so
     // one atomic per warp reserves the output rows of its occupied slots.
     const uint64_t step = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -492,7 +492,8 @@ __global__ void gather_groups_kernel(const unsigned long long* htab, uint64_t ns
     const uint32_t lane = threadIdx.x & 31u;
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < end; i += step) {
         const unsigned long long* s = htab + i * stride;
-        const bool occ = i < nslots && s[0] != ~0ull;
+        // A directly indexed table (slot = key) marks a slot by its count.
+        const bool occ = i < nslots && (direct ? s[1] != 0ull : s[0] != ~0ull);
         const unsigned mask = __ballot_sync(0xffffffffu, occ);
         if (mask == 0) continue;
         unsigned long long base = 0;
@@ -500,19 +501,21 @@ __global__ void gather_groups_kernel(const unsigned long long* htab, uint64_t ns
         base = __shfl_sync(0xffffffffu, base, 0);
         if (!occ) continue;
         const unsigned long long o = base + __popc(mask & ((1u << lane) - 1u));
-        if (o < cap)
+        if (o < cap) {
             for (uint32_t w = 0; w < stride; ++w) out[o * stride + w] = s[w];
+            if (direct) out[o * stride] = i;
+        }
     }
 }
 
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
-                                 int sms, cudaStream_t st) {
+                                 int sms, cudaStream_t st, bool direct) {
     if (nslots == 0) return cudaSuccess;
     uint64_t blocks = (nslots + kAuxThreads - 1) / kAuxThreads;
     if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
     gather_groups_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(htab, nslots, stride, out,
-                                                                               cap, counter);
+                                                                               cap, counter, direct);
     return cudaGetLastError();
 }
 
@@ -561,11 +564,12 @@ __global__ void extract_keys_kernel(const unsigned long long* packed, uint64_t n
 }
 
 // Output group i from its slot s ([key][count][value limbs...]).
-__device__ __forceinline__ void write_group(const unsigned long long* s, uint64_t i, const HashFormat& F,
-                                            uint64_t* keys_out, tgp_agg_value* vals_out) {
+// (key: the slot's packed key word.)
+__device__ __forceinline__ void write_group(const unsigned long long* s, unsigned long long key, uint64_t i,
+                                            const HashFormat& F, uint64_t* keys_out, tgp_agg_value* vals_out) {
     if (keys_out)
         for (uint32_t k = 0; k < F.nkey; ++k)
-            keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((s[0] >> F.key_shift[k]) & F.key_mask[k]);
+            keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((key >> F.key_shift[k]) & F.key_mask[k]);
     if (!vals_out) return;
     const uint64_t cnt = s[1];
     for (uint32_t a = 0; a < F.nagg; ++a) {
@@ -596,12 +600,15 @@ __device__ __forceinline__ void write_group(const unsigned long long* s, uint64_
 __global__ void format_hash_groups_kernel(const unsigned long long* packed, const uint32_t* order, uint64_t n,
                                           const HashFormat F, uint64_t* keys_out, tgp_agg_value* vals_out) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        write_group(packed + static_cast<uint64_t>(order[i]) * F.hstride, i, F, keys_out, vals_out);
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long* g = packed + static_cast<uint64_t>(order[i]) * F.hstride;
+        write_group(g, g[0], i, F, keys_out, vals_out);
+    }
 }
 
-// Directly indexed group tables (slot = key): the occupied slots, in slot
-// order, are the groups in ascending key order, so the result is written
+// Directly indexed group tables (slot = key; a slot is occupied when its
+// count is not zero, its key word is never written): the occupied slots, in
+// slot order, are the groups in ascending key order, so the result is written
 // straight from the table at positions from a prefix count of occupied
 // slots, with no gather and no sort. Block b covers slots
 // [b * kDirChunk, (b + 1) * kDirChunk); pass 1 counts each block's occupied
@@ -618,7 +625,7 @@ __global__ void __launch_bounds__(kAuxThreads) count_direct_kernel(const unsigne
 #pragma unroll 4
     for (int j = 0; j < kDirPerThread; ++j) {
         const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
-        c += (i < nslots && htab[i * stride] != ~0ull) ? 1u : 0u;
+        c += (i < nslots && htab[i * stride + 1] != 0ull) ? 1u : 0u;
     }
     for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
     __shared__ uint32_t wsum[kAuxThreads / 32];
@@ -642,7 +649,7 @@ __global__ void __launch_bounds__(kAuxThreads) format_direct_kernel(const unsign
     for (int j = 0; j < kDirPerThread; ++j) {
         const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
         const unsigned long long* s = htab + i * F.hstride;
-        const bool occ = i < nslots && s[0] != ~0ull;
+        const bool occ = i < nslots && s[1] != 0ull;
         const uint32_t mask = __ballot_sync(0xffffffffu, occ);
         if (lane == 0) wsum[warp] = __popc(mask);
         __syncthreads();
@@ -652,7 +659,7 @@ __global__ void __launch_bounds__(kAuxThreads) format_direct_kernel(const unsign
             total += wsum[w];
         }
         const unsigned long long pos = run + before + __popc(mask & ((1u << lane) - 1u));
-        if (occ && pos < cap) write_group(s, pos, F, keys_out, vals_out);
+        if (occ && pos < cap) write_group(s, i, pos, F, keys_out, vals_out);
         run += total;
         __syncthreads();
     }

@@ -2010,7 +2010,8 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     const uint64_t max_groups = std::min<uint64_t>(hcap, static_cast<uint64_t>(std::min<unsigned __int128>(D, hcap)));
     TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&packed), std::max<uint64_t>(max_groups, 1) * P.hstride * 8,
                       "group gather allocation failed"));
-    TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream));
+    TGP_CUDA(launch_gather_groups(P.htab, hcap, P.hstride, packed, max_groups, P.counters + 2, ctx->sms, ctx->stream,
+                                  P.hdirect != 0));
     unsigned long long ng = 0;
     TGP_CUDA(cudaMemcpyAsync(&ng, P.counters + 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -258,7 +258,8 @@ struct alignas(16) Plan {
     uint64_t wait_ns;
     // MODE_GROUP_HASH, one key over a moderate range: the slot of a key is
     // the key itself (relative to its minimum; hmask = the last slot), so a
-    // row's update needs no probe, no compare and no claim.
+    // row's update needs no probe, no compare and no claim; a slot whose
+    // count is not zero is occupied (its key word stays empty).
     uint32_t hdirect;
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };

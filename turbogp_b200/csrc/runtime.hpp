@@ -98,7 +98,7 @@ cudaError_t launch_like(const uint8_t* bytes, const unsigned long long* offs, ui
 cudaError_t launch_fill_slots(unsigned long long* p, uint64_t nslots, const SlotImage& img, int sms, cudaStream_t st);
 cudaError_t launch_gather_groups(const unsigned long long* htab, uint64_t nslots, uint32_t stride,
                                  unsigned long long* out, uint64_t cap, unsigned long long* counter,
-                                 int sms, cudaStream_t st);
+                                 int sms, cudaStream_t st, bool direct = false);
 
 struct Column;
 // Lowers one predicate leaf over column `c` staged in `slot` (capi.cu).

@@ -500,15 +500,13 @@ __device__ __forceinline__ long long* priv_values(const Plan& P, uint8_t* extra)
 constexpr uint32_t kSmemProbes = 2;
 __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, uint64_t key) {
     if (P.hdirect) {
-        // Every writer stores the same key word: a plain store marks the
-        // slot occupied without a read.
+        // The slot is the key; its count marks it occupied (the key word is
+        // not written).
         if (key > P.hmask) {
             atomicOr(P.err, kErrHashFull);
             return nullptr;
         }
-        unsigned long long* s = P.htab + key * P.hstride;
-        *s = key;
-        return s;
+        return P.htab + key * P.hstride;
     }
     uint64_t h = hash_slot(key, P.hlog2);
     for (uint64_t n = 0; n <= P.hmask; ++n) {
