@@ -1652,9 +1652,11 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             P.s32_words = s32_words;
             extra = s32_bytes(s32_copies);
             // Dense column program (keys of any count, bucket tables, the
-            // join payload's build-side part).
+            // join payload's build-side part), compiled ahead of time when
+            // its value steps are one of the fixed shapes.
             if ((!J || pay_ok) && !P.check_ovf && kn.dense)
                 P.dense_vec = compile_chain(b, pay_ok, static_cast<uint32_t>(kMaxGroupKeys)) ? 1u : 0u;
+            if (P.dense_vec && kn.shapes) P.shape = value_shape_of(P);
         } else if (kn.placement != 3 && shared_tab + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             mode = MODE_GROUP_SHARED;
             extra = shared_tab;

@@ -24,6 +24,9 @@ int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t
 // Index (>= 1) of the ahead-of-time dense kernel matching the plan's key
 // dtypes and value program, or 0 (the interpreted dense program runs).
 uint32_t dense_shape_of(const Plan& P);
+// The shape whose value program (steps only, keys aside) a plan's dense
+// program matches, for the limb-table kernels; 0 = none.
+uint32_t value_shape_of(const Plan& P);
 // kShapeScalar when the plan is a scalar aggregate the register fast path
 // takes (one or two SUMs of one or two staged factors, bounded), else 0.
 uint32_t scalar_shape_of(const Plan& P);

@@ -1259,6 +1259,12 @@ struct DenseShape {
     }
 };
 
+// A fixed-shape kernel tag (DenseShape) as opposed to void or ScalarTag.
+template <class T, class = void>
+struct IsDenseShape : std::false_type {};
+template <class T>
+struct IsDenseShape<T, std::void_t<decltype(T::dense_shape)>> : std::true_type {};
+
 template <int... I, typename F>
 __device__ __forceinline__ void static_for_impl(std::integer_sequence<int, I...>, F&& f) {
     (f(std::integral_constant<int, I>{}), ...);
@@ -1436,6 +1442,101 @@ __device__ __forceinline__ void chain_tile_static(const Plan& P, uint8_t* extra,
             }
         });
     }
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-shape value programs on the 32-bit limb tables (MODE_GROUP_SHARED32,
+// merged scans of the serving templates): the keys come from the runtime
+// loop of chain_s32_tile (bucket tables, staged keys, the payload's part);
+// the value program's steps, their dtypes and value slots are template
+// constants, so a tile runs the shared loads, the arithmetic and the limb
+// atomics as straight-line code instead of a loop over plan steps.
+// SUM / COUNT(col) values only (the limb tables' kinds).
+// ---------------------------------------------------------------------------
+template <int NT, class SH>
+__device__ __forceinline__ void chain_s32_tile_static(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                                      uint32_t m, const uint32_t* gin = nullptr) {
+    constexpr int R = kTileRows / NT;
+    constexpr int NS = static_cast<int>(SH::nsteps);
+    const uint32_t sa = smem_addr(stage);
+    // Shared-memory loads of the value program's columns, issued first.
+    uint32_t c32[NS][R];
+    uint64_t c64[NS][R];
+    static_for<NS>([&](auto I) {
+        constexpr uint32_t c = SH::step[I.value];
+        constexpr uint32_t dt = c & 15u, fl = (c >> 4) & 63u;
+        if constexpr ((fl & CS_COL) != 0) {
+            if constexpr ((fl & CS_NARROW) != 0) lds_cells32<R, dt>(sa + P.chain.s[I.value].soff, t, c32[I.value]);
+            else lds_cells64<R, dt>(sa + P.chain.s[I.value].soff, t, c64[I.value]);
+        }
+    });
+    uint32_t g[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = (gin && ((m >> r) & 1u)) ? gin[r] : 0u;
+#pragma unroll 1
+    for (uint32_t k = 0; k < P.ngkey; ++k) {
+        const GKey& K = P.gkey[k];
+        if (K.build_side) continue;   // its part comes with the payload
+        uint32_t x[R];
+        load_cells32<R>(stage + K.soff, K.dtype, t, x);
+        const uint32_t mn = static_cast<uint32_t>(K.min), st = static_cast<uint32_t>(K.stride);
+        if (K.lut) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) g[r] += static_cast<uint32_t>(__ldg(K.lut + (x[r] - mn))) * st;
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) g[r] += (x[r] - mn) * st;
+        }
+    }
+    const uint32_t W = P.s32_words;
+    // (s32_copies is a power of two.)
+    uint32_t* tab = reinterpret_cast<uint32_t*>(extra) + static_cast<size_t>((t >> 5) & (P.s32_copies - 1u)) * P.ngroups * W;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if ((m >> r) & 1u) atomicAdd(&tab[g[r] * W], 1u);
+    uint64_t cur[R];
+    static_for<NS>([&](auto I) {
+        constexpr int s = I.value;
+        constexpr uint32_t c = SH::step[s];
+        constexpr uint32_t fl = (c >> 4) & 63u, kind = (c >> 10) & 7u, acc = c >> 13;
+        constexpr bool chain = (fl & CS_CHAIN) != 0;
+        const ChainStep& S = P.chain.s[s];
+        if constexpr ((fl & CS_COL) != 0 && (fl & CS_NARROW) != 0) {
+            const uint32_t mu = static_cast<uint32_t>(S.mul32), ad = static_cast<uint32_t>(S.add32);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t f = mu * c32[s][r] + ad;
+                const uint64_t fw = (fl & CS_NONNEG) ? static_cast<uint64_t>(f)
+                                                     : static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(f)));
+                cur[r] = chain ? cur[r] * fw : fw;
+            }
+        } else if constexpr ((fl & CS_COL) != 0) {
+            const uint64_t mu = static_cast<uint64_t>(S.mul), ad = static_cast<uint64_t>(S.add);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint64_t f = (fl & CS_IDENT) ? c64[s][r] : mu * c64[s][r] + ad;
+                cur[r] = chain ? cur[r] * f : f;
+            }
+        } else {
+            const uint64_t k = static_cast<uint64_t>(S.add);
+#pragma unroll
+            for (int r = 0; r < R; ++r) cur[r] = chain ? cur[r] * k : k;
+        }
+        if constexpr (acc != 0) {
+            static_assert(kind == VK_SUM || kind == VK_COUNT_NZ, "limb tables hold SUM / COUNT(col) values");
+            constexpr uint32_t w0 = 1u + 2u * (acc - 1u);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (!((m >> r) & 1u)) continue;
+                const int64_t x = kind == VK_COUNT_NZ ? (cur[r] != 0 ? 1 : 0) : static_cast<int64_t>(cur[r]);
+                uint32_t* e = &tab[g[r] * W + w0];
+                const uint32_t xl = static_cast<uint32_t>(x);
+                const uint32_t old = atomicAdd(e, xl);
+                const int32_t add = static_cast<int32_t>(x >> 32) + ((old + xl < old) ? 1 : 0);
+                if (add) atomicAdd(reinterpret_cast<int*>(e + 1), add);
+            }
+        }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -1656,7 +1757,8 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             const uint32_t hit = join_pay_probe<R>(P, stage, t, m, g);
             if constexpr (MODE == MODE_GROUP_SHARED32) {
                 if (P.dense_vec) {
-                    chain_s32_tile<NT>(P, extra, stage, t, hit, g);
+                    if constexpr (IsDenseShape<SH>::value) chain_s32_tile_static<NT, SH>(P, extra, stage, t, hit, g);
+                    else chain_s32_tile<NT>(P, extra, stage, t, hit, g);
                     return;
                 }
             }
@@ -1703,7 +1805,8 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     }
     if constexpr (MODE == MODE_GROUP_SHARED32) {
         if (!TAIL && P.dense_vec) {
-            chain_s32_tile<NT>(P, extra, stage, t, m);
+            if constexpr (IsDenseShape<SH>::value) chain_s32_tile_static<NT, SH>(P, extra, stage, t, m);
+            else chain_s32_tile<NT>(P, extra, stage, t, m);
             return;
         }
     }
@@ -2149,6 +2252,8 @@ struct ShapeEntry {
     uint32_t code[kMaxSteps];
     const void* k256;
     const void* k512;
+    const void* s32_256;   // the same value program on the limb tables (keys at run time)
+    const void* s32_512;
 };
 
 template <class SH>
@@ -2161,6 +2266,8 @@ static ShapeEntry shape_entry() {
     for (uint32_t i = 0; i < SH::nsteps; ++i) e.code[i] = SH::step[i];
     e.k256 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 256, SH>);
     e.k512 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 512, SH>);
+    e.s32_256 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_SHARED32, false, 256, SH>);
+    e.s32_512 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_SHARED32, false, 512, SH>);
     return e;
 }
 
@@ -2211,6 +2318,23 @@ uint32_t scalar_shape_of(const Plan& P) {
     return kShapeScalar;
 }
 
+uint32_t value_shape_of(const Plan& P) {
+    if (!P.dense_vec || P.chain.nsteps == 0) return 0;
+    uint32_t n = 0;
+    const ShapeEntry* tab = shape_table(&n);
+    for (uint32_t j = 0; j < n; ++j) {
+        const ShapeEntry& e = tab[j];
+        if (e.nsteps != P.chain.nsteps) continue;
+        bool same = true;
+        for (uint32_t i = 0; i < e.nsteps; ++i) {
+            const ChainStep& S = P.chain.s[i];
+            same = same && e.code[i] == step_code((S.flags & CS_COL) ? S.dtype : 0u, S.flags, S.kind, S.acc);
+        }
+        if (same) return j + 1;
+    }
+    return 0;
+}
+
 uint32_t dense_shape_of(const Plan& P) {
     if (!P.dense_vec || P.chain.nsteps == 0) return 0;
     uint32_t code[kMaxSteps] = {};
@@ -2247,6 +2371,12 @@ static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t sh
         uint32_t n = 0;
         const ShapeEntry* tab = shape_table(&n);
         if (shape <= n) return nt == 512 ? tab[shape - 1].k512 : nt == 256 ? tab[shape - 1].k256 : nullptr;
+        return nullptr;
+    }
+    if (shape && mode == MODE_GROUP_SHARED32) {
+        uint32_t n = 0;
+        const ShapeEntry* tab = shape_table(&n);
+        if (shape <= n) return nt == 512 ? tab[shape - 1].s32_512 : nt == 256 ? tab[shape - 1].s32_256 : nullptr;
         return nullptr;
     }
     return nt == 512 ? select_kernel<512>(mode, acc128) : nt == 256 ? select_kernel<256>(mode, acc128) : nullptr;
