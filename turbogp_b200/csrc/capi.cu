@@ -1760,12 +1760,16 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         bool presum = kn.presum && !join && !P.check_ovf && !acc128;
         for (uint32_t v = 0; presum && v < P.nval; ++v)
             presum = P.val[v].kind == VK_SUM || P.val[v].kind == VK_COUNT_NZ;
+        // u32 keys when every key is below 2^32 - 1 (the empty key): a packed
+        // hash key of at most 31 bits, or a direct group index.
+        const bool key32 = mode == MODE_GROUP_GLOBAL || total_bits <= 31;
         const uint32_t HS = 4096;
-        const size_t bytes = static_cast<size_t>(HS) * (12 + 4 * P.nval);
+        const size_t bytes = static_cast<size_t>(HS) * ((key32 ? 8 : 12) + 4 * P.nval);
         const size_t budget = ctx->max_dyn_smem - static_smem - kBarrierBytes;
         if (presum && bytes + 2 * static_cast<size_t>(P.stage_bytes) <= budget) {
             P.hsm_slots = HS;
             P.hsm_log2 = log2u(HS);
+            P.hsm_key32 = key32 ? 1u : 0u;
             extra = bytes;
         }
     }

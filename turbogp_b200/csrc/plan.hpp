@@ -218,8 +218,9 @@ struct alignas(16) Plan {
     uint32_t hlog2;
     uint32_t hstride;       // u64 words per slot
     uint32_t hsm_slots;     // per-CTA shared pre-aggregation slots (power of two; 0 = none):
-                            // [keys u64][counts u32][value partials i32 x nval], SUM / COUNT_NZ only
+                            // [keys][counts u32][value partials i32 x nval], SUM / COUNT_NZ only
     uint32_t hsm_log2;
+    uint32_t hsm_key32;     // its keys are u32 (every key below 2^32 - 1), else u64
 
     // Join table (probe side: MODE_GROUP_* / MODE_SCALAR with join, MODE_JOIN_PAIRS;
     // build side: MODE_JOIN_BUILD). Packed slots: (key_rel << 32) | build_row.

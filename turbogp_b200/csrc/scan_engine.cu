@@ -520,57 +520,65 @@ __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, ui
     return nullptr;
 }
 
-// This CTA's shared pre-aggregation table (P.hsm_slots slots: u64 keys,
-// u32 counts, i32 partials per value) absorbs repeated (hot) keys with native
-// 32-bit shared atomics. Returns false when the key found no slot within
+// This CTA's shared pre-aggregation table (P.hsm_slots slots: keys, u32
+// counts, i32 partials per value) absorbs repeated (hot) keys with native
+// 32-bit shared atomics. Keys are u32 when every key is below 2^32 - 1
+// (P.hsm_key32: 32-bit hash, compares and claims, and less shared memory),
+// else u64; the empty key is all ones.
+template <typename KT>
+struct PresumTab {
+    KT* keys;
+    uint32_t* cnt;
+    int32_t* sums;
+    __device__ __forceinline__ PresumTab(uint8_t* extra, uint32_t HS)
+        : keys(reinterpret_cast<KT*>(extra)),
+          cnt(reinterpret_cast<uint32_t*>(reinterpret_cast<KT*>(extra) + HS)),
+          sums(reinterpret_cast<int32_t*>(reinterpret_cast<uint32_t*>(reinterpret_cast<KT*>(extra) + HS) + HS)) {}
+    static constexpr KT kEmptyKey = static_cast<KT>(~0ull);
+    __device__ __forceinline__ static uint32_t slot(KT key, uint32_t log2) {
+        if constexpr (sizeof(KT) == 4) return (static_cast<uint32_t>(key) * 0x9E3779B1u) >> (32u - log2);
+        else return static_cast<uint32_t>(hash_slot(key, log2));
+    }
+};
+
+// Runs f(PresumTab<KT>) with the plan's key width.
+template <typename F>
+__device__ __forceinline__ void with_presum(const Plan& P, uint8_t* extra, F&& f) {
+    if (P.hsm_key32) f(PresumTab<uint32_t>(extra, P.hsm_slots));
+    else f(PresumTab<unsigned long long>(extra, P.hsm_slots));
+}
+
+// Adds a row to its key's slot; false when the key found no slot within
 // kSmemProbes probes (the caller updates the global table instead). The host
 // proves that no partial can pass 2^31 in magnitude.
 template <bool TAIL>
 __device__ __forceinline__ bool presum_add(const Plan& P, uint8_t* extra, uint64_t key, const uint8_t* stage,
                                            uint64_t r0, uint32_t rl, uint32_t brow, uint32_t& ovf) {
     const uint32_t HS = P.hsm_slots;
-    unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
-    int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
-    uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
+    bool done = false;
+    with_presum(P, extra, [&](auto T) {
+        using KT = std::remove_pointer_t<decltype(T.keys)>;
+        const KT k0 = static_cast<KT>(key);
+        uint32_t h = T.slot(k0, P.hsm_log2);
 #pragma unroll 1
-    for (uint32_t n = 0; n < kSmemProbes; ++n) {
-        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
-        if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
-        if (k == kEmpty || k == key) {
-            atomicAdd(&cnt[h], 1u);
+        for (uint32_t n = 0; n < kSmemProbes; ++n) {
+            KT k = *reinterpret_cast<volatile KT*>(&T.keys[h]);
+            if (k == T.kEmptyKey) k = atomicCAS(&T.keys[h], T.kEmptyKey, k0);
+            if (k == T.kEmptyKey || k == k0) {
+                atomicAdd(&T.cnt[h], 1u);
 #pragma unroll 1
-            for (uint32_t v = 0; v < P.nval; ++v) {
-                const ValDesc& V = P.val[v];
-                const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
-                atomicAdd(&sums[v * HS + h], static_cast<int32_t>(V.kind == VK_COUNT_NZ ? (x != 0) : x));
+                for (uint32_t v = 0; v < P.nval; ++v) {
+                    const ValDesc& V = P.val[v];
+                    const int64_t x = eval_val<TAIL>(P, V, stage, r0, rl, brow, ovf);
+                    atomicAdd(&T.sums[v * HS + h], static_cast<int32_t>(V.kind == VK_COUNT_NZ ? (x != 0) : x));
+                }
+                done = true;
+                return;
             }
-            return true;
+            h = (h + 1) & (HS - 1);
         }
-        h = (h + 1) & (HS - 1);
-    }
-    return false;
-}
-
-// presum_add with the row's value arguments already computed (x[v]).
-__device__ __forceinline__ bool presum_add_x(const Plan& P, uint8_t* extra, uint64_t key, const int64_t* x) {
-    const uint32_t HS = P.hsm_slots;
-    unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
-    int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
-    uint32_t h = static_cast<uint32_t>(hash_slot(key, P.hsm_log2));
-#pragma unroll
-    for (uint32_t n = 0; n < kSmemProbes; ++n) {
-        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(&keys[h]);
-        if (k == kEmpty) k = atomicCAS(&keys[h], kEmpty, key);
-        if (k == kEmpty || k == key) {
-            atomicAdd(&cnt[h], 1u);
-            for (uint32_t v = 0; v < P.nval; ++v) atomicAdd(&sums[v * HS + h], static_cast<int32_t>(x[v]));
-            return true;
-        }
-        h = (h + 1) & (HS - 1);
-    }
-    return false;
+    });
+    return done;
 }
 
 template <uint32_t MODE, bool ACC128, int NT>
@@ -603,14 +611,13 @@ struct Sink {
             for (uint32_t i = t; i < P.s32_copies * P.ngroups * P.s32_words; i += NT) tab[i] = 0;
         } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             const uint32_t HS = P.hsm_slots;
-            unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
-            uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
-            int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
-            for (uint32_t i = t; i < HS; i += NT) {
-                keys[i] = kEmpty;
-                cnt[i] = 0;
-                for (uint32_t v = 0; v < P.nval; ++v) sums[v * HS + i] = 0;
-            }
+            with_presum(P, extra, [&](auto T) {
+                for (uint32_t i = t; i < HS; i += NT) {
+                    T.keys[i] = T.kEmptyKey;
+                    T.cnt[i] = 0;
+                    for (uint32_t v = 0; v < P.nval; ++v) T.sums[v * HS + i] = 0;
+                }
+            });
         }
     }
 
@@ -848,12 +855,12 @@ struct Sink {
         } else if ((MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) && P.hsm_slots) {
             consumer_sync<NT>();
             const uint32_t HS = P.hsm_slots;
-            const unsigned long long* keys = reinterpret_cast<const unsigned long long*>(extra);
-            const uint32_t* cnt = reinterpret_cast<const uint32_t*>(keys + HS);
-            const int32_t* sums = reinterpret_cast<const int32_t*>(cnt + HS);
+            with_presum(P, extra, [&](auto T) {
+            const uint32_t* cnt = T.cnt;
+            const int32_t* sums = T.sums;
             for (uint32_t i = t; i < HS; i += NT) {
-                const unsigned long long key = keys[i];
-                if (key == kEmpty) continue;
+                if (T.keys[i] == T.kEmptyKey) continue;
+                const unsigned long long key = static_cast<unsigned long long>(T.keys[i]);
                 // Hash slots are [key][count][v0 lo][v0 hi]...; direct
                 // accumulators are [count lo][count hi][v0 lo][v0 hi]...
                 unsigned long long* base;
@@ -880,6 +887,7 @@ struct Sink {
                     atomic_add_i128(base + vofs + 2 * v, a);
                 }
             }
+            });
         }
         if (ovf) atomicOr(P.err, kErrRowOverflow);
     }
@@ -1604,38 +1612,40 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
     uint32_t pend = m;
     if (P.hsm_slots) {
         const uint32_t HS = P.hsm_slots;
-        unsigned long long* keys = reinterpret_cast<unsigned long long*>(extra);
-        uint32_t* cnt = reinterpret_cast<uint32_t*>(keys + HS);
-        int32_t* sums = reinterpret_cast<int32_t*>(cnt + HS);
-        uint32_t h[R];
-        unsigned long long k0[R];
+        with_presum(P, extra, [&](auto T) {
+            using KT = std::remove_pointer_t<decltype(T.keys)>;
+            uint32_t h[R];
+            KT kr[R], k0[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            h[r] = static_cast<uint32_t>(hash_slot(key[r], P.hsm_log2));
-            k0[r] = ((m >> r) & 1u) ? *reinterpret_cast<volatile unsigned long long*>(&keys[h[r]]) : 0ull;
-        }
+            for (int r = 0; r < R; ++r) {
+                kr[r] = static_cast<KT>(key[r]);
+                h[r] = T.slot(kr[r], P.hsm_log2);
+                k0[r] = ((m >> r) & 1u) ? *reinterpret_cast<volatile KT*>(&T.keys[h[r]]) : KT{0};
+            }
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (!((m >> r) & 1u)) continue;
-            uint32_t hs = h[r];
-            unsigned long long k = k0[r];
+            for (int r = 0; r < R; ++r) {
+                if (!((m >> r) & 1u)) continue;
+                uint32_t hs = h[r];
+                KT k = k0[r];
 #pragma unroll
-            for (uint32_t n = 0; n < kSmemProbes; ++n) {
-                if (n) {
-                    hs = (hs + 1) & (HS - 1);
-                    k = *reinterpret_cast<volatile unsigned long long*>(&keys[hs]);
-                }
-                if (k == kEmpty) k = atomicCAS(&keys[hs], kEmpty, key[r]);
-                if (k == kEmpty || k == key[r]) {
-                    atomicAdd(&cnt[hs], 1u);
+                for (uint32_t n = 0; n < kSmemProbes; ++n) {
+                    if (n) {
+                        hs = (hs + 1) & (HS - 1);
+                        k = *reinterpret_cast<volatile KT*>(&T.keys[hs]);
+                    }
+                    if (k == T.kEmptyKey) k = atomicCAS(&T.keys[hs], T.kEmptyKey, kr[r]);
+                    if (k == T.kEmptyKey || k == kr[r]) {
+                        atomicAdd(&T.cnt[hs], 1u);
 #pragma unroll
-                    for (int v = 0; v < 2; ++v)
-                        if (static_cast<uint32_t>(v) < P.nval) atomicAdd(&sums[v * HS + hs], static_cast<int32_t>(x[r][v]));
-                    pend &= ~(1u << r);
-                    break;
+                        for (int v = 0; v < 2; ++v)
+                            if (static_cast<uint32_t>(v) < P.nval)
+                                atomicAdd(&T.sums[v * HS + hs], static_cast<int32_t>(x[r][v]));
+                        pend &= ~(1u << r);
+                        break;
+                    }
                 }
             }
-        }
+        });
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
