@@ -805,9 +805,9 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     Measured: the plain server's capacity (completed q/s with arrivals far
     above it) and its p50 / p99 at 80 % of that capacity; the batched server's
     policy (batches in flight: 1 or 2) picked on a calibration stream at 5x
-    the plain capacity; then the batched server offered 5x, 6x, 8x, 10x, 12x
-    the plain capacity, until its p99 exceeds the plain p99 or it falls
-    behind the offered rate; and its own capacity. value = the highest
+    the plain capacity; then the batched server offered 5x, 6x, 8x, 10x, 12x,
+    14x, 16x the plain capacity, until its p99 exceeds the plain p99 or it
+    falls behind the offered rate; and its own capacity. value = the highest
     completed q/s whose p99 is at most the plain server's p99 (the 5x run's,
     if none is)."""
     import numpy as np
@@ -862,7 +862,7 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     inflight = min(calib, key=calib.get)
     ladder, best = [], None
     with ClockSampler(local) as clocks:
-        for m in (5.0, 6.0, 8.0, 10.0, 12.0):
+        for m in (5.0, 6.0, 8.0, 10.0, 12.0, 14.0, 16.0):
             r = serving.serve_batched(ctx, templates, stream(m * cap_p, count), mem_budget=args.mem_budget,
                                       max_inflight=inflight)
             r = {**r, "offered_qps": m * cap_p, "offered_x_plain_capacity": m}
@@ -870,7 +870,10 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
             ok = (r.get("p99_ms") or 1e9) <= p99_plain
             if ok:
                 best = r
-            if not ok or (r.get("qps") or 0) < 0.9 * m * cap_p:
+            # (A stream's completed q/s sits a few percent under its offered
+            # rate: the window ends with the last completion, which can be a
+            # high-cardinality request of several ms.)
+            if not ok or (r.get("qps") or 0) < 0.85 * m * cap_p:
                 break
     batched_sat = serving.serve_batched(ctx, templates, stream(100_000.0, count), mem_budget=args.mem_budget,
                                         max_inflight=inflight)
@@ -1116,7 +1119,7 @@ def main() -> None:
     ap.add_argument("--profile-window", action="store_true",
                     help="merged: timed batches between cudaProfilerStart / Stop")
     ap.add_argument("--rate", type=float, default=2000.0, help="(unused: serve offers multiples of the plain capacity)")
-    ap.add_argument("--requests", type=int, default=3000, help="serve: requests in the batched streams")
+    ap.add_argument("--requests", type=int, default=6000, help="serve: requests in the batched streams")
     ap.add_argument("--mem-budget", type=int, default=8 << 30, help="serve: admission budget in bytes")
     ap.add_argument("--highcard-rows", type=int, default=100_000_000)
     args = ap.parse_args()
