@@ -845,7 +845,7 @@ def measure_serve(ctx, args, world: int, rank: int, local: int, fact_host: dict 
     # Warm-up: every template's prepared queries built and sized (the
     # high-cardinality one included), then both paths once.
     serving.prewarm(templates, [request(0.0) for _ in range(2000)], per_template=4)
-    serving.reserve(templates, 320)
+    serving.reserve(templates, 640)   # two full batches of one template in flight and queued
     serving.serve_batched(ctx, templates, stream(4000.0, 256), mem_budget=args.mem_budget)
     serving.serve_plain(ctx, templates, stream(4000.0, 32))
     # Plain capacity, then plain at 80 % of it.

@@ -125,3 +125,35 @@ def test_heavy_lane_error_reaches_the_caller():
             serving.Request(0.001, "light", 1)]
     with pytest.raises(RuntimeError, match="heavy query failed"):
         serving.serve_batched(ctx, tpls, reqs, mem_budget=10**12)
+
+
+def test_backlog_binds_oldest_first_and_builds_only_what_batches_need():
+    """All requests arrive at once (a backlog) with two idle prepared queries:
+    the queued requests are bound oldest first, each batch is submitted with
+    its members in arrival order bound to their own literals, and no more
+    prepared queries are built than two batches in flight and queued hold."""
+    log, made = [], []
+
+    def make():
+        pq = FakePQ("light", log)
+        made.append(pq)
+        return pq
+
+    tpl = serving.Template("light", make, 100)
+    tpls = {"light": tpl}
+    serving.reserve(tpls, 2)
+    made.clear()
+    ctx = FakeCtx(0.002, tpls)
+    reqs = [serving.Request(0.0, "light", i) for i in range(40)]
+    bound = []
+    orig_submit = ctx.submit
+
+    def submit(pqs, decode=True):
+        bound.append([p.where for p in pqs])
+        return orig_submit(pqs, decode)
+
+    ctx.submit = submit
+    out = serving.serve_batched(ctx, tpls, reqs, mem_budget=10**9, max_batch=8, max_inflight=1)
+    assert out["completed"] == 40
+    assert [w for b in bound for w in b] == list(range(40))
+    assert len(made) <= 8

@@ -278,6 +278,7 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                 seen) -> int:
     """The batching loop of serve_batched; returns the number of batches."""
     batches = 0
+    unbound: dict[str, int] = {}     # per template: queued requests not yet bound
     while not source.exhausted() or queue or inflight or (lane is not None and lane.busy()):
         if lane is not None and lane.error is not None:
             break
@@ -298,9 +299,17 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                     _finish(r, time.perf_counter() - t0, error=e)
             else:
                 # Rebound on arrival, while earlier batches run, when an idle
-                # prepared query is at hand (so that a batch's members are
-                # ready to submit when it is formed); otherwise at admission.
-                queue.append([r, tpl, tpl.pool.pop().rebind(r.where) if tpl.pool else None])
+                # prepared query is at hand and no earlier request of the
+                # template waits unbound (so that a batch's members are ready
+                # to submit when it is formed); otherwise at admission. Under
+                # a backlog the idle prepared queries so go to the oldest
+                # requests, which are admitted first, and admission builds a
+                # new one only when a batch needs more than the pool holds.
+                if tpl.pool and not unbound.get(tpl.name):
+                    queue.append([r, tpl, tpl.pool.pop().rebind(r.where)])
+                else:
+                    queue.append([r, tpl, None])
+                    unbound[tpl.name] = unbound.get(tpl.name, 0) + 1
         _complete(inflight, t0)
         if queue and len(inflight) < max_inflight:
             members, used = [], sum(m[1].mem_bytes or 0 for _, ms in inflight for m in ms)
@@ -314,6 +323,7 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                 used += tpl.mem_bytes
                 m = queue.popleft()
                 if m[2] is None:
+                    unbound[tpl.name] -= 1
                     m[2] = tpl.take().rebind(m[0].where)
                 members.append(tuple(m))
             if members:
