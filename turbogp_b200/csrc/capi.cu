@@ -23,6 +23,7 @@ namespace {
 constexpr unsigned long long kEmptySlot = ~0ull;
 constexpr uint64_t kDirectMaxGroups = 1ull << 22;
 constexpr uint64_t kHashDirectMax = 1ull << 27;   // key values of a directly indexed group table
+constexpr size_t kJoinSmemCap = 144u << 10;        // shared memory per CTA of a payload-join scan (see size_smem)
 
 int fail(tgp_ctx* ctx, int st, const std::string& m) {
     if (ctx) ctx->err = m;
@@ -672,12 +673,18 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = sc
     }
     const size_t per_cta = budget / static_cast<size_t>(std::max(1, K.ctas_per_sm));
     size_t avail = per_cta > kBarrierBytes + extra_bytes ? per_cta - kBarrierBytes - extra_bytes : 0;
-    // Joins through a payload array take two stages unless a variant asks
-    // for fewer than the maximum: the 60M x 1.5M join probe ran 0.516 ms with
-    // four stages and 0.373 ms with two (autotuner, gated CUDA events), and
-    // merged join batches 0.85 -> 0.77 ms; the shared memory the stages leave
-    // serves as L1 for the payload lookups of hot keys.
-    const int max_st = (P.jpay != nullptr && K.max_stages >= kMaxStages) ? 2 : K.max_stages;
+    // Joins through a payload array keep the CTA's shared memory to at most
+    // 144 KB (at least two stages) unless a variant asks for fewer stages
+    // than the maximum, so that the rest of the SM's combined L1 / shared
+    // memory caches the payload lookups of hot keys: with private
+    // accumulators (77 KB) the 60M x 1.5M join probe ran 0.516 ms with four
+    // stages and 0.373 ms with two (L1 hit rate 8.8 -> 17.5 %), merged join
+    // batches 0.85 -> 0.77 ms; the limb tables' few KB leave room for four.
+    int max_st = K.max_stages;
+    if (P.jpay != nullptr && K.max_stages >= kMaxStages && stage) {
+        const size_t room = kJoinSmemCap > kBarrierBytes + extra_bytes ? kJoinSmemCap - kBarrierBytes - extra_bytes : 0;
+        max_st = static_cast<int>(std::max<size_t>(2, room / stage));
+    }
     const size_t cap = static_cast<size_t>(std::max(1, std::min(max_st, kMaxStages)));
     uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
     if (S == 0) {
@@ -1605,7 +1612,19 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         // Bucketed (merged) plans take the limb tables whenever they are
         // exact: the private placement has no dense path for bucket keys
         // (a 2-member merged scan: 1.02 ms private, 0.51 ms limb tables).
-        const bool prefer_s32 = kn.placement == 4 || (bucket != nullptr && kn.placement == 0);
+        // So do joins through a payload array whose value program is one of
+        // the fixed shapes: the 60M x 1.5M join probe ran 0.332 ms on the
+        // limb tables (512 threads, four stages) against 0.374-0.387 ms with
+        // private accumulators (autotuner, gated CUDA events).
+        bool join_s32 = false;
+        if (J && pay_ok && kn.placement == 0 && kn.dense && kn.shapes && !P.check_ovf &&
+            compile_chain(b, pay_ok, static_cast<uint32_t>(kMaxGroupKeys))) {
+            const uint32_t dv = P.dense_vec;
+            P.dense_vec = 1;
+            join_s32 = value_shape_of(P) != 0;
+            P.dense_vec = dv;
+        }
+        const bool prefer_s32 = kn.placement == 4 || (bucket != nullptr && kn.placement == 0) || join_s32;
         auto s32_bytes = [&](uint32_t copies) -> size_t {
             return static_cast<size_t>(copies) * ngroups_direct * s32_words * 4;
         };
