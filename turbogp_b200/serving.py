@@ -278,7 +278,7 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                 seen) -> int:
     """The batching loop of serve_batched; returns the number of batches."""
     batches = 0
-    unbound: dict[str, int] = {}     # per template: queued requests not yet bound
+    unbound: dict[str, deque] = {}   # per template: queued requests waiting unbound, oldest first
     while not source.exhausted() or queue or inflight or (lane is not None and lane.busy()):
         if lane is not None and lane.error is not None:
             break
@@ -301,16 +301,25 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                 # Rebound on arrival, while earlier batches run, when an idle
                 # prepared query is at hand and no earlier request of the
                 # template waits unbound (so that a batch's members are ready
-                # to submit when it is formed); otherwise at admission. Under
-                # a backlog the idle prepared queries so go to the oldest
-                # requests, which are admitted first, and admission builds a
-                # new one only when a batch needs more than the pool holds.
-                if tpl.pool and not unbound.get(tpl.name):
+                # to submit when it is formed); otherwise when a completed
+                # batch returns prepared queries, oldest request first, or at
+                # admission. Admission so builds a new prepared query only
+                # when a batch needs more than the pool holds.
+                waiting = unbound.setdefault(tpl.name, deque())
+                if tpl.pool and not waiting:
                     queue.append([r, tpl, tpl.pool.pop().rebind(r.where)])
                 else:
-                    queue.append([r, tpl, None])
-                    unbound[tpl.name] = unbound.get(tpl.name, 0) + 1
+                    entry = [r, tpl, None]
+                    queue.append(entry)
+                    waiting.append(entry)
         _complete(inflight, t0)
+        # Prepared queries returned by completed batches go to the oldest
+        # requests still waiting unbound, while the next batch runs.
+        for waiting in unbound.values():
+            while waiting and (waiting[0][2] is not None or waiting[0][1].pool):
+                entry = waiting.popleft()
+                if entry[2] is None:
+                    entry[2] = entry[1].pool.pop().rebind(entry[0].where)
         if queue and len(inflight) < max_inflight:
             members, used = [], sum(m[1].mem_bytes or 0 for _, ms in inflight for m in ms)
             while queue and len(members) < max_batch:
@@ -323,7 +332,6 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
                 used += tpl.mem_bytes
                 m = queue.popleft()
                 if m[2] is None:
-                    unbound[tpl.name] -= 1
                     m[2] = tpl.take().rebind(m[0].where)
                 members.append(tuple(m))
             if members:
