@@ -831,7 +831,8 @@ cudaError_t launch_copy_to_host(void* host_dst, const void* dev_src, size_t byte
     if ((bytes & 15u) || (reinterpret_cast<uintptr_t>(host_dst) & 15u) || (reinterpret_cast<uintptr_t>(dev_src) & 15u))
         return cudaErrorInvalidValue;
     const uint64_t nwords = bytes / 16;
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((nwords + 255) / 256, 148));
+    // A grid-stride copy: a few hundred blocks cover any readback size.
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((nwords + 255) / 256, 256));
     copy_to_host_kernel<<<grid, 256, 0, st>>>(static_cast<uint4*>(host_dst), static_cast<const uint4*>(dev_src),
                                               nwords);
     return cudaGetLastError();
