@@ -22,6 +22,7 @@ set when done — that is how the wire front-end's connection threads wait.
 """
 from __future__ import annotations
 
+import gc
 import queue as _queue
 import threading
 import time
@@ -105,8 +106,25 @@ def summarize(reqs: list[Request], wall: float) -> dict:
     lat = np.array([r.done - r.arrival for r in reqs if r.done >= 0])
     if lat.size == 0:
         return {"completed": 0}
-    return {"completed": int(lat.size), "qps": lat.size / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3)}
+    out = {"completed": int(lat.size), "qps": lat.size / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+           "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3)}
+    per = {}
+    for name in sorted({r.template for r in reqs}):
+        t = np.array([r.done - r.arrival for r in reqs if r.done >= 0 and r.template == name])
+        if t.size:
+            per[name] = {"n": int(t.size), "p50_ms": float(np.percentile(t, 50) * 1e3),
+                         "p99_ms": float(np.percentile(t, 99) * 1e3)}
+    out["by_template"] = per
+    return out
+
+
+def freeze_heap() -> None:
+    """Moves every object alive now into the collector's permanent
+    generation (gc.freeze), so that the collections a serving loop triggers
+    walk only the objects it creates, not the tables, pools and modules built
+    before it (a full collection of those is a pause of milliseconds). Both
+    servers call it when they start."""
+    gc.freeze()
 
 
 def _finish(r: Request, t: float, out=None, error: BaseException | None = None) -> None:
@@ -235,6 +253,7 @@ def serve_batched(ctx: Context, templates: dict[str, Template], reqs, mem_budget
     `heavy_lane` (default: whether any template is heavy) starts the heavy
     lane; a live source whose templates appear later passes it explicitly."""
     source = reqs if isinstance(reqs, QueueSource) else ListSource(reqs)
+    freeze_heap()
     queue: deque = deque()         # [req, template, prepared query rebound to it, or None]
     inflight: deque = deque()      # (handle, [(req, template, pq)])
     t0 = time.perf_counter() if t0 is None else t0
@@ -356,6 +375,7 @@ def _serve_loop(ctx, templates, source, mem_budget, max_batch, max_inflight, que
 
 
 def serve_plain(ctx: Context, templates: dict[str, Template], reqs: list[Request]) -> dict:
+    freeze_heap()
     t0 = time.perf_counter()
     for r in reqs:
         now = time.perf_counter() - t0
