@@ -298,6 +298,35 @@ def test_hash_grouping_hot_keys_and_device_format(ctx):
     t.drop()
 
 
+def test_one_word_direct_slots(ctx):
+    """GROUP BY one key over a moderate range with COUNT(*) and one SUM or
+    COUNT(col): the count and the biased sum share one 64-bit word per key
+    when the host proves they never meet. Negative keys and values (a
+    negative bias), an affine argument, count only, COUNT(col), the shared
+    pre-aggregation switched off by large values, a partial last tile, and
+    a value range too wide to share a word (the four-word slots again)."""
+    n = 2_000_003
+    h = datagen.highcard(n, 200_000, 1.1, seed=11)
+    rng = np.random.default_rng(5)
+    h["negkey"] = h["key"] - 100_000
+    h["big"] = rng.integers(-2**40, 2**40, n, dtype=np.int64)
+    t = ctx.register(h)
+    v = col("value")
+    cases = [
+        ([count_star(), sum_(v)], ("key",), None),
+        ([count_star(), sum_(v - 500), avg(v - 500)], ("negkey",), v < 900),
+        ([count_star()], ("key",), None),
+        ([count_col(v), count_star()], ("negkey",), v >= 3),
+        ([count_star(), sum_(v * 3000)], ("key",), None),          # no shared pre-aggregation
+        ([sum_(col("big")), count_star()], ("key",), None),         # range too wide for one word
+    ]
+    for aggs, gb, where in cases:
+        g = t.aggregate(aggs, gb, where, group_cap=1 << 20)
+        o = oracle.aggregate(h, None, aggs, gb, where)
+        same_query(g, o)
+    t.drop()
+
+
 def test_batch_persistent_launch_matches_single_queries(ctx):
     """A batch of queries of uneven sizes and all three templates (scan +
     scalar sum, grouped Q1 shape, join + group) through the persistent

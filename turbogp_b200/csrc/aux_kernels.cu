@@ -571,11 +571,20 @@ __device__ __forceinline__ void write_group(const unsigned long long* s, unsigne
         for (uint32_t k = 0; k < F.nkey; ++k)
             keys_out[i * F.nkey + k] = static_cast<uint64_t>(F.key_min[k]) + ((key >> F.key_shift[k]) & F.key_mask[k]);
     if (!vals_out) return;
-    const uint64_t cnt = s[1];
+    // One-word slots (F.hpack): the count above `hpack_shift`, below it the
+    // sum of (value - bias) over the slot's rows.
+    const uint64_t cnt = F.hpack ? (F.hpack_shift < 64 ? s[0] >> F.hpack_shift : 0ull) : s[1];
     for (uint32_t a = 0; a < F.nagg; ++a) {
         tgp_agg_value o;
         o.count = cnt;
-        if (F.val[a] < 0) {
+        if (F.hpack && F.val[a] >= 0) {
+            const uint64_t low = F.hpack_shift ? (s[0] & ((1ull << F.hpack_shift) - 1ull)) : 0ull;
+            const __int128 sum = static_cast<__int128>(low) + static_cast<__int128>(cnt) * F.hpack_bias;
+            o.lo = static_cast<uint64_t>(sum);
+            o.hi = static_cast<int64_t>(sum >> 64);
+            const double f = i128_to_f64_rn(o.lo, o.hi);
+            o.as_f64 = F.func[a] == TGP_AGG_AVG ? (cnt ? f / static_cast<double>(cnt) : 0.0) : f;
+        } else if (F.val[a] < 0) {
             o.lo = cnt;
             o.hi = 0;
             o.as_f64 = static_cast<double>(cnt);
@@ -621,11 +630,13 @@ constexpr uint64_t kDirChunk = static_cast<uint64_t>(kAuxThreads) * kDirPerThrea
 __global__ void __launch_bounds__(kAuxThreads) count_direct_kernel(const unsigned long long* htab, uint64_t nslots,
                                                                    uint32_t stride, unsigned long long* counts) {
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kDirChunk;
+    // The count word: [key][count][...] slots, or the whole one-word slot.
+    const uint32_t occ = stride > 1 ? 1u : 0u;
     uint32_t c = 0;
 #pragma unroll 4
     for (int j = 0; j < kDirPerThread; ++j) {
         const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
-        c += (i < nslots && htab[i * stride + 1] != 0ull) ? 1u : 0u;
+        c += (i < nslots && htab[i * stride + occ] != 0ull) ? 1u : 0u;
     }
     for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
     __shared__ uint32_t wsum[kAuxThreads / 32];
@@ -649,7 +660,7 @@ __global__ void __launch_bounds__(kAuxThreads) format_direct_kernel(const unsign
     for (int j = 0; j < kDirPerThread; ++j) {
         const uint64_t i = base + static_cast<uint64_t>(j) * kAuxThreads + threadIdx.x;
         const unsigned long long* s = htab + i * F.hstride;
-        const bool occ = i < nslots && s[1] != 0ull;
+        const bool occ = i < nslots && s[F.hstride > 1 ? 1 : 0] != 0ull;
         const uint32_t mask = __ballot_sync(0xffffffffu, occ);
         if (lane == 0) wsum[warp] = __popc(mask);
         __syncthreads();

@@ -310,6 +310,9 @@ struct Builder {
     Plan P;
     std::vector<int> col2slot;
     uint64_t max_abs_val = 0;       // max |per-row value| over all values (saturating)
+    // Per value: the range of its per-row argument (valid when !val_big).
+    __int128 val_lo[kMaxVals] = {}, val_hi[kMaxVals] = {};
+    bool val_big[kMaxVals] = {};
     bool unbounded = false;         // some value may exceed 2^62 in magnitude
     size_t static_smem = 0;         // static shared bytes of the kernel the plan is sized for
 
@@ -520,6 +523,9 @@ struct Builder {
             }
         }
         if (P.nval >= static_cast<uint32_t>(kMaxVals)) return fail(ctx, TGP_UNSUPPORTED, "more than 8 distinct aggregates");
+        val_lo[P.nval] = kind == VK_COUNT_NZ ? 0 : lo;
+        val_hi[P.nval] = kind == VK_COUNT_NZ ? 1 : hi;
+        val_big[P.nval] = big;
         P.val[P.nval] = v;
         *idx = static_cast<int>(P.nval++);
         return TGP_OK;
@@ -1908,6 +1914,26 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     const uint32_t total_bits = qs.total_bits;
     (void)nv1;
 
+    // A directly indexed table of COUNT(*) and at most one SUM / COUNT(col)
+    // whose fields provably never meet takes one-word slots: the count in the
+    // top bits (enough for every row), the sum of (value - its minimum) below.
+    if (mode == MODE_GROUP_HASH && P.hdirect && P.hash_fast && P.nval <= 1 && !tn &&
+        q->nagg <= static_cast<uint32_t>(kMaxFormatAggs) && P.ngkey == 1 && P.gkey[0].shift == 0 &&
+        (!P.hsm_slots || P.hsm_key32) && (P.nval == 0 || !b.val_big[0])) {
+        const uint64_t rows = std::max<uint64_t>(T->rows, 1);
+        const uint32_t cbits = 64u - static_cast<uint32_t>(__builtin_clzll(rows));  // count <= rows < 2^cbits
+        const uint32_t shift = P.nval ? 64u - cbits : 0u;
+        const __int128 span = P.nval ? b.val_hi[0] - b.val_lo[0] : 0;
+        const bool fits = P.nval == 0 || (shift < 64 && static_cast<unsigned __int128>(span) * rows <
+                                                           (static_cast<unsigned __int128>(1) << shift));
+        if (fits && (P.nval == 0 || (b.val_lo[0] >= INT64_MIN && b.val_lo[0] <= INT64_MAX))) {
+            P.hpack = 1;
+            P.hpack_shift = shift;
+            P.hpack_bias = P.nval ? static_cast<int64_t>(b.val_lo[0]) : 0;
+            P.hstride = 1;
+        }
+    }
+
     // Scratch: accumulators (direct/scalar) or hash table, counters, error word.
     const uint64_t acc_words = qs.acc_words();
     const uint64_t htab_words = hcap * P.hstride;
@@ -1931,7 +1957,9 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     } else {
         TGP_CUDA(cudaMemsetAsync(block, 0, block_words * 8, ctx->stream));
     }
-    if (mode == MODE_GROUP_HASH) {
+    if (mode == MODE_GROUP_HASH && P.hpack) {
+        TGP_CUDA(cudaMemsetAsync(P.htab, 0, hcap * 8, ctx->stream));
+    } else if (mode == MODE_GROUP_HASH) {
         // Keys EMPTY, counters 0, value limbs: MIN/MAX identity or 0 (one pass).
         SlotImage img;
         std::memset(&img, 0, sizeof(img));
@@ -1976,6 +2004,9 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
         F.nagg = nagg;
         F.hstride = P.hstride;
         F.sum64 = P.sum64;
+        F.hpack = P.hpack;
+        F.hpack_shift = P.hpack_shift;
+        F.hpack_bias = P.hpack_bias;
         for (uint32_t k = 0; k < q->ngroup; ++k) {
             F.key_shift[k] = P.gkey[k].shift;
             F.key_mask[k] = bits[k] >= 64 ? ~0ull : ((1ull << bits[k]) - 1);

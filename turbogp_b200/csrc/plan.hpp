@@ -262,6 +262,15 @@ struct alignas(16) Plan {
     // row's update needs no probe, no compare and no claim; a slot whose
     // count is not zero is occupied (its key word stays empty).
     uint32_t hdirect;
+    // One-word direct slots (MODE_GROUP_HASH, hdirect, hstride = 1): a slot
+    // holds (row count << hpack_shift) + the sum of (value - hpack_bias) over
+    // its rows, both fields proven by the host never to carry into the other
+    // (rows < 2^(64 - hpack_shift), rows x value range < 2^hpack_shift), so a
+    // row is one non-returning 64-bit add and the table is a quarter of the
+    // [key][count][lo][hi] layout's size. 0 = that layout.
+    uint32_t hpack;
+    uint32_t hpack_shift;
+    int64_t hpack_bias;
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 
@@ -336,6 +345,8 @@ struct SlotImage {
 constexpr int kMaxFormatAggs = 32;
 struct HashFormat {
     uint32_t nkey, nagg, hstride, sum64;  // sum64: value limbs hold int64 sums (hi = sign of lo)
+    uint32_t hpack, hpack_shift;          // one-word direct slots (Plan::hpack)
+    int64_t hpack_bias;
     uint32_t key_shift[kMaxGroupKeys];
     uint64_t key_mask[kMaxGroupKeys];
     int64_t key_min[kMaxGroupKeys];

@@ -520,6 +520,18 @@ __device__ __forceinline__ unsigned long long* hash_group_slot(const Plan& P, ui
     return nullptr;
 }
 
+// Adds `cnt` rows whose value arguments sum to `xsum` to the one-word direct
+// slot of `key` (P.hpack): one non-returning 64-bit add of
+// (cnt << shift) + (xsum - cnt * bias).
+__device__ __forceinline__ void hpack_add(const Plan& P, uint64_t key, uint64_t cnt, int64_t xsum) {
+    if (key > P.hmask) {
+        atomicOr(P.err, kErrHashFull);
+        return;
+    }
+    atomicAdd(P.htab + key, (cnt << P.hpack_shift) +
+                                (static_cast<unsigned long long>(xsum) - cnt * static_cast<uint64_t>(P.hpack_bias)));
+}
+
 // This CTA's shared pre-aggregation table (P.hsm_slots slots: keys, u32
 // counts, i32 partials per value) absorbs repeated (hot) keys with native
 // 32-bit shared atomics. Keys are u32 when every key is below 2^32 - 1
@@ -755,6 +767,12 @@ struct Sink {
         } else if (MODE == MODE_GROUP_HASH) {
             const uint64_t key = group_hash_key<TAIL>(P, stage, r0, rl, brow);
             if (P.hsm_slots && presum_add<TAIL>(P, extra, key, stage, r0, rl, brow, ovf)) return;
+            if (P.hpack) {
+                int64_t x = P.nval ? eval_val<TAIL>(P, P.val[0], stage, r0, rl, brow, ovf) : 0;
+                if (P.nval && P.val[0].kind == VK_COUNT_NZ) x = x != 0 ? 1 : 0;
+                hpack_add(P, key, 1, x);
+                return;
+            }
             unsigned long long* slot = hash_group_slot(P, key);
             if (slot == nullptr) return;
             atomicAdd(slot + 1, 1ull);
@@ -863,6 +881,10 @@ struct Sink {
                 const unsigned long long key = static_cast<unsigned long long>(T.keys[i]);
                 // Hash slots are [key][count][v0 lo][v0 hi]...; direct
                 // accumulators are [count lo][count hi][v0 lo][v0 hi]...
+                if (MODE == MODE_GROUP_HASH && P.hpack) {
+                    hpack_add(P, key, cnt[i], P.nval ? static_cast<int64_t>(sums[i]) : 0);
+                    continue;
+                }
                 unsigned long long* base;
                 uint32_t vofs;
                 if (MODE == MODE_GROUP_HASH) {
@@ -1667,6 +1689,78 @@ __device__ __forceinline__ void hash_fast_tile(const Plan& P, uint8_t* extra, co
 }
 
 // ---------------------------------------------------------------------------
+// The column path on one-word direct slots (P.hpack; one key, COUNT(*) and
+// at most one SUM / COUNT(col)). A direct slot index is below 2^27, so keys,
+// the shared table's hash and its compares run in 32 bits; a row that finds
+// no shared slot is one non-returning 64-bit add of (1 << shift) +
+// (value - bias) to its key's word.
+// ---------------------------------------------------------------------------
+template <int R>
+__device__ __forceinline__ void hpack_tile(const Plan& P, uint8_t* extra, const uint8_t* stage, uint32_t t,
+                                           uint32_t m) {
+    const GKey& K = P.gkey[0];
+    const ValDesc& V = P.val[0];
+    const bool hasv = P.nval != 0;
+    int64_t kc[R], vc[R];
+    load_cells64<R>(stage + K.soff, K.dtype, t, kc);
+    if (hasv) load_cells64<R>(stage + V.f[0].soff, V.f[0].dtype, t, vc);
+    const uint32_t kmin = static_cast<uint32_t>(K.min);
+    const uint64_t mul = static_cast<uint64_t>(V.f[0].mul), add = static_cast<uint64_t>(V.f[0].add);
+    const bool ident = mul == 1 && add == 0, nz = V.kind == VK_COUNT_NZ;
+    uint32_t key[R];
+    int64_t x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        // The cell lies in [min, min + 2^27): its slot is the low word's difference.
+        key[r] = static_cast<uint32_t>(kc[r]) - kmin;
+        int64_t a = 0;
+        if (hasv) a = ident ? vc[r] : static_cast<int64_t>(mul * static_cast<uint64_t>(vc[r]) + add);
+        x[r] = nz ? (a != 0 ? 1 : 0) : a;
+    }
+    uint32_t pend = m;
+    if (P.hsm_slots) {
+        PresumTab<uint32_t> T(extra, P.hsm_slots);
+        const uint32_t HS = P.hsm_slots;
+        uint32_t h[R], k0[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            h[r] = PresumTab<uint32_t>::slot(key[r], P.hsm_log2);
+            k0[r] = ((m >> r) & 1u) ? *reinterpret_cast<volatile uint32_t*>(&T.keys[h[r]]) : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (!((m >> r) & 1u)) continue;
+            uint32_t hs = h[r], k = k0[r];
+#pragma unroll
+            for (uint32_t n = 0; n < kSmemProbes; ++n) {
+                if (n) {
+                    hs = (hs + 1) & (HS - 1);
+                    k = *reinterpret_cast<volatile uint32_t*>(&T.keys[hs]);
+                }
+                if (k == T.kEmptyKey) k = atomicCAS(&T.keys[hs], T.kEmptyKey, key[r]);
+                if (k == T.kEmptyKey || k == key[r]) {
+                    atomicAdd(&T.cnt[hs], 1u);
+                    if (hasv) atomicAdd(&T.sums[hs], static_cast<int32_t>(x[r]));
+                    pend &= ~(1u << r);
+                    break;
+                }
+            }
+        }
+    }
+    const unsigned long long one = (1ull << P.hpack_shift) - static_cast<uint64_t>(P.hpack_bias);
+    const uint32_t last = static_cast<uint32_t>(P.hmask);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (!((pend >> r) & 1u)) continue;
+        if (key[r] > last) {
+            atomicOr(P.err, kErrHashFull);
+            continue;
+        }
+        atomicAdd(P.htab + key[r], one + static_cast<unsigned long long>(x[r]));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Tile processing (consumer threads)
 // ---------------------------------------------------------------------------
 template <uint32_t MODE, bool ACC128, int NT, bool TAIL, class SH>
@@ -1822,6 +1916,12 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
     }
     if constexpr (MODE == MODE_GROUP_HASH || MODE == MODE_GROUP_GLOBAL) {
         if (!TAIL && P.hash_fast) {
+            if constexpr (MODE == MODE_GROUP_HASH) {
+                if (P.hpack) {
+                    hpack_tile<R>(P, extra, stage, t, m);
+                    return;
+                }
+            }
             hash_fast_tile<MODE, R>(P, extra, stage, t, m);
             return;
         }
