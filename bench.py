@@ -404,8 +404,8 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
                    lambda: t.aggregate_topn(aggs, ("key",), None, 0, True, 10))
         tables = [(t, host)]
         kernel_bytes = 12 * n
-        dominant = "scan_kernel<MODE_GROUP_HASH> (directly indexed one-word group slots, shared pre-aggregation of hot keys)"
-        traffic = traffic_per_launch("highcard_group_hash_kernel.md", n)
+        dominant = "direct_group_kernel<int64 key, int32 value> (one-word direct slots, shared table of hot keys)"
+        traffic = traffic_per_launch("highcard_group_direct_group_kernel.md", n)
         check = lambda out: _check_highcard(q, host)
         cleanup = [t.drop]
 

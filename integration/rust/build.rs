@@ -13,7 +13,7 @@ use std::env;
 use std::path::{Path, PathBuf};
 use std::process::Command;
 
-const SOURCES: [&str; 4] = ["scan_engine.cu", "aux_kernels.cu", "capi.cu", "noalloc.cu"];
+const SOURCES: [&str; 5] = ["scan_engine.cu", "aux_kernels.cu", "groupby_direct.cu", "capi.cu", "noalloc.cu"];
 
 fn nvcc() -> PathBuf {
     if let Ok(p) = env::var("NVCC") {

@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = ROOT / "_build" / "turbogp_b200"
 LIB = PKG / "libturbogp_b200.so"
-SOURCES = ["scan_engine.cu", "aux_kernels.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["scan_engine.cu", "aux_kernels.cu", "groupby_direct.cu", "capi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

@@ -528,7 +528,8 @@ __device__ __forceinline__ int64_t pay_cell(const uint8_t* base, uint32_t dtype,
     return static_cast<int64_t>(__ldg(reinterpret_cast<const long long*>(base) + row));
 }
 
-__global__ void join_pay_kernel(const unsigned long long* tab, uint64_t cap, const PayKeys K, uint32_t* pay) {
+__global__ void join_pay_kernel(const unsigned long long* tab, uint64_t cap, const PayKeys K, uint32_t* pay,
+                                uint32_t width) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < cap;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const unsigned long long e = tab[i];
@@ -538,17 +539,20 @@ __global__ void join_pay_kernel(const unsigned long long* tab, uint64_t cap, con
         for (uint32_t k = 0; k < K.n; ++k)
             g += (static_cast<uint64_t>(pay_cell(K.ptr[k], K.dtype[k], row)) - static_cast<uint64_t>(K.min[k])) *
                  K.stride[k];
-        pay[e >> 32] = static_cast<uint32_t>(g);
+        const uint64_t at = e >> 32;
+        if (width == 1) reinterpret_cast<uint8_t*>(pay)[at] = static_cast<uint8_t>(g);
+        else if (width == 2) reinterpret_cast<uint16_t*>(pay)[at] = static_cast<uint16_t>(g);
+        else pay[at] = static_cast<uint32_t>(g);
     }
 }
 
 cudaError_t launch_join_pay(const unsigned long long* tab, uint64_t cap, const PayKeys& K, uint32_t* pay,
-                            uint64_t pay_entries, int sms, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(pay, 0xff, pay_entries * 4, st);
+                            uint32_t width, uint64_t pay_entries, int sms, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(pay, 0xff, pay_entries * width, st);
     if (e != cudaSuccess) return e;
     uint64_t blocks = (cap + kAuxThreads - 1) / kAuxThreads;
     if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
-    join_pay_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(tab, cap, K, pay);
+    join_pay_kernel<<<static_cast<unsigned>(blocks), kAuxThreads, 0, st>>>(tab, cap, K, pay, width);
     return cudaGetLastError();
 }
 

@@ -755,6 +755,56 @@ int launch(tgp_ctx* ctx, const Plan& P0, uint32_t mode, bool acc128) {
     return TGP_OK;
 }
 
+// Unfiltered GROUP BY of one key into one-word direct slots: the streaming
+// kernel of groupby_direct.cu in place of the scan pipeline. Its per-CTA
+// shared table is kept only when no CTA's rows can take a 32-bit partial to
+// 2^31 in magnitude.
+// Shared slots of the direct-group kernel's table (96 KB with a value, two
+// CTAs per SM): 8,192 measured faster than 4,096 (more hot keys held, fewer
+// global adds) and than 16,384 (one CTA per SM).
+constexpr uint32_t kDirectGroupSlots = 8192;
+
+int launch_direct_groups(tgp_ctx* ctx, const Plan& P, uint64_t max_abs_val) {
+    const bool hasv = P.nval != 0;
+    uint32_t hs = P.hsm_slots ? kDirectGroupSlots : 0u;
+    const int occ = std::max(1, direct_group_ctas_per_sm(hs, hasv));
+    const uint64_t chunks = (P.nrows + 127) / 128;
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((chunks + 15) / 16, static_cast<uint64_t>(ctx->sms) * occ));
+    if (hs) {
+        // A CTA's 16 warps take at most ceil(chunks / warps) chunks of 128
+        // rows each, and one warp the partial last chunk.
+        const uint64_t nwarps = grid * 16;
+        const unsigned __int128 rows_cta = static_cast<unsigned __int128>((chunks + nwarps - 1) / nwarps) * 128 * 16 + 128;
+        if (rows_cta * std::max<uint64_t>(max_abs_val, 1) >= (static_cast<unsigned __int128>(1) << 31)) hs = 0;
+    }
+    DirectGroupArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.key = P.slot[P.gkey[0].slot].ptr;
+    A.val = hasv ? P.slot[P.val[0].f[0].slot].ptr : nullptr;
+    A.nrows = P.nrows;
+    A.kmin = P.gkey[0].min;
+    A.mul = hasv ? P.val[0].f[0].mul : 1;
+    A.add = hasv ? P.val[0].f[0].add : 0;
+    A.ident = A.mul == 1 && A.add == 0;
+    A.nz = hasv && P.val[0].kind == VK_COUNT_NZ;
+    A.hs = hs;
+    A.hs_shift = hs ? 32u - log2u(hs) : 0u;
+    A.last = static_cast<uint32_t>(P.hmask);
+    A.shift = P.hpack_shift;
+    A.bias = P.hpack_bias;
+    A.one = (1ull << P.hpack_shift) - static_cast<uint64_t>(P.hpack_bias);
+    A.slots = P.htab;
+    A.err = P.err;
+    A.counters = P.counters;
+    const uint32_t kdt = P.slot[P.gkey[0].slot].dtype, vdt = hasv ? P.slot[P.val[0].f[0].slot].dtype : 0u;
+    std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+    TGP_TRY(profile_begin(ctx, &ev));
+    cudaError_t e = launch_direct_group(A, kdt, vdt, static_cast<int>(grid), ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("group launch: ") + cudaGetErrorString(e));
+    if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
+    return TGP_OK;
+}
+
 int get_table(tgp_ctx* ctx, tgp_table_id id, const Table** out) {
     auto it = ctx->tables.find(id);
     if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
@@ -1719,6 +1769,12 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             ++K.n;
             sig.insert(sig.end(), {q->group[k].column, static_cast<uint64_t>(P.gkey[k].min), P.gkey[k].stride});
         }
+        // Payload entries as narrow as the group indices allow (u8 below 255
+        // groups, u16 below 65,535; all ones = no match): the array is read
+        // once per probe row, so the narrower it is, the more of it stays in
+        // L1 and L2.
+        const uint32_t pw = D <= 255 ? 1u : (D <= 65535 ? 2u : 4u);
+        sig.push_back(pw);
         const uint64_t entries = J->krange + 1;
         if (dry) {
             // Sizing only (tgp_query_footprint): a payload still to be built
@@ -1732,9 +1788,10 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             if (!J->pay) TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&J->pay), entries * 4, "join payload allocation failed"));
             J->pay_entries = entries;
             J->pay_sig = sig;
-            TGP_CUDA(launch_join_pay(J->tab, J->cap, K, J->pay, entries, ctx->sms, ctx->stream));
+            TGP_CUDA(launch_join_pay(J->tab, J->cap, K, J->pay, pw, entries, ctx->sms, ctx->stream));
         }
         P.jpay = J->pay;
+        P.jpay_w = pw;
     }
 
     // Hash table sizing: 1.25x the bound on distinct groups, to a power of two.
@@ -1973,7 +2030,12 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     }
     TGP_TRY(size_smem(ctx, P, extra, scan_kernel_static_smem(), &qs.kn));
     bound_presum(ctx, qs);
-    TGP_TRY(launch(ctx, P, mode, acc128));
+    if (P.hpack && P.nleaf == 0 && P.hash_fast &&
+        direct_group_supported(P.slot[P.gkey[0].slot].dtype, P.nval ? P.slot[P.val[0].f[0].slot].dtype : 0u)) {
+        TGP_TRY(launch_direct_groups(ctx, P, b.max_abs_val));
+    } else {
+        TGP_TRY(launch(ctx, P, mode, acc128));
+    }
 
     TGP_TRY(pinned_reserve(ctx, block_words * 8));
     TGP_CUDA(cudaMemcpyAsync(ctx->hpin, block, block_words * 8, cudaMemcpyDeviceToHost, ctx->stream));

@@ -233,7 +233,8 @@ struct alignas(16) Plan {
     uint32_t sum64;         // global / hash sums fit int64 (host-proven): plain atomic adds, lo limb only
     int64_t jkmin;
     uint64_t jkrange;       // kmax - kmin (unsigned)
-    const uint32_t* jpay;   // unique build keys: per-key payload (build-side group index part), or null
+    const uint32_t* jpay;   // unique build keys: per-key payload (build-side group index part), or null;
+                            // entries of jpay_w bytes (1, 2 or 4), all ones = no match
 
     // Outputs
     unsigned long long* acc;        // direct/scalar accumulators [g][1 + nval][2]
@@ -271,6 +272,8 @@ struct alignas(16) Plan {
     uint32_t hpack;
     uint32_t hpack_shift;
     int64_t hpack_bias;
+    uint32_t jpay_w;
+    uint32_t _pad_jpay;
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 

@@ -20,6 +20,32 @@ namespace tgp {
 
 // Launchers implemented in the .cu files.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st);
+
+// Unfiltered GROUP BY of one key into one-word direct slots
+// (groupby_direct.cu): the slot of a row is (u32)key - (u32)kmin (< 2^27);
+// it receives `one` + the row's value argument (one = (1 << shift) - bias),
+// or, through the shared table of `hs` slots (0 = none), the per-slot
+// count << shift plus the partial sum minus count * bias.
+struct DirectGroupArgs {
+    const uint8_t* key;
+    const uint8_t* val;            // null: COUNT(*) only
+    uint64_t nrows;
+    int64_t kmin;
+    int64_t mul, add;              // value argument = mul * cell + add
+    uint32_t ident;                // mul == 1 && add == 0
+    uint32_t nz;                   // COUNT(col): the argument is (value != 0)
+    uint32_t hs, hs_shift;         // shared slots (power of two) and 32 - log2(hs)
+    uint32_t last;                 // the last slot
+    uint32_t shift;
+    unsigned long long one;
+    int64_t bias;
+    unsigned long long* slots;
+    uint32_t* err;
+    unsigned long long* counters;  // [0] += nrows (every row is selected)
+};
+bool direct_group_supported(uint32_t kdt, uint32_t vdt);
+int direct_group_ctas_per_sm(uint32_t hs, bool hasv);
+cudaError_t launch_direct_group(const DirectGroupArgs& A, uint32_t kdt, uint32_t vdt, int grid, cudaStream_t st);
 int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape = 0);
 // Index (>= 1) of the ahead-of-time dense kernel matching the plan's key
 // dtypes and value program, or 0 (the interpreted dense program runs).
@@ -70,7 +96,7 @@ cudaError_t launch_split_pairs(const unsigned long long* pairs, uint64_t n, uint
 cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, int sms,
                             cudaStream_t st);
 cudaError_t launch_join_pay(const unsigned long long* tab, uint64_t cap, const PayKeys& K, uint32_t* pay,
-                            uint64_t pay_entries, int sms, cudaStream_t st);
+                            uint32_t width, uint64_t pay_entries, int sms, cudaStream_t st);
 cudaError_t format_hash_groups(const unsigned long long* packed, uint64_t n, const HashFormat& F, uint32_t key_bits,
                                void* scratch, size_t scratch_bytes, uint64_t* keys_out, tgp_agg_value* vals_out,
                                int sms, cudaStream_t st);

@@ -1575,6 +1575,34 @@ __device__ __forceinline__ void chain_s32_tile_static(const Plan& P, uint8_t* ex
 // matching build row, or kNoPay. The R lookups of a thread are independent
 // loads, so they are all in flight at once.
 // ---------------------------------------------------------------------------
+// Payload entry `rel` (P.jpay_w bytes; all ones = kNoPay).
+__device__ __forceinline__ uint32_t pay_load(const Plan& P, uint64_t rel) {
+    if (P.jpay_w == 1) {
+        const uint32_t v = __ldg(reinterpret_cast<const uint8_t*>(P.jpay) + rel);
+        return v == 0xffu ? kNoPay : v;
+    }
+    if (P.jpay_w == 2) {
+        const uint32_t v = __ldg(reinterpret_cast<const uint16_t*>(P.jpay) + rel);
+        return v == 0xffffu ? kNoPay : v;
+    }
+    return __ldg(P.jpay + rel);
+}
+
+template <int R, typename E>
+__device__ __forceinline__ void pay_lookups(const Plan& P, const int64_t (&cell)[R], uint32_t m, uint32_t (&g)[R]) {
+    const E* pay = reinterpret_cast<const E*>(P.jpay);
+    constexpr E kNone = static_cast<E>(~0u);
+    E v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint64_t rel = static_cast<uint64_t>(cell[r]) - static_cast<uint64_t>(P.jkmin);
+        const bool probe = ((m >> r) & 1u) && rel <= P.jkrange;
+        v[r] = probe ? __ldg(pay + rel) : kNone;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = v[r] == kNone ? kNoPay : static_cast<uint32_t>(v[r]);
+}
+
 template <int R>
 __device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t* stage, uint32_t t, uint32_t m,
                                                    uint32_t (&g)[R]) {
@@ -1582,13 +1610,10 @@ __device__ __forceinline__ uint32_t join_pay_probe(const Plan& P, const uint8_t*
     const uint32_t kdt = P.slot[P.jslot].dtype;
     int64_t cell[R];
     load_cells64<R>(kb, kdt, t, cell);
+    if (P.jpay_w == 1) pay_lookups<R, uint8_t>(P, cell, m, g);
+    else if (P.jpay_w == 2) pay_lookups<R, uint16_t>(P, cell, m, g);
+    else pay_lookups<R, uint32_t>(P, cell, m, g);
     uint32_t hit = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const uint64_t rel = static_cast<uint64_t>(cell[r]) - static_cast<uint64_t>(P.jkmin);
-        const bool probe = ((m >> r) & 1u) && rel <= P.jkrange;
-        g[r] = probe ? __ldg(P.jpay + rel) : kNoPay;
-    }
 #pragma unroll
     for (int r = 0; r < R; ++r) hit |= (g[r] != kNoPay ? 1u : 0u) << r;
     return hit;
@@ -1882,7 +1907,7 @@ __device__ __forceinline__ void process_tile(const Plan& P, Sink<MODE, ACC128, N
             for (uint32_t sel = hit; sel; sel &= sel - 1) {
                 const uint32_t rl = R * t + __ffs(sel) - 1;
                 const uint64_t rel = static_cast<uint64_t>(load_cell(kb, kdt, rl)) - static_cast<uint64_t>(P.jkmin);
-                sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t, __ldg(P.jpay + rel));
+                sink.template row<TAIL>(P, extra, stage, r0, rl, 0, t, pay_load(P, rel));
             }
             return;
         }
