@@ -377,3 +377,36 @@ def test_batch_persistent_launch_matches_single_queries(ctx):
     for o, e in zip(h.wait(), expect[:9]):
         same_query(o, e)
     j.drop()
+
+
+def test_join_payload_widths_and_shapes(ctx):
+    """Payload joins with no probe-side predicate, grouped by build-side keys:
+    25 groups (u8 payload entries), 2,526 and 25 x 2,526 groups (u16, then
+    u32 entries), one- and two-factor sums, two values, count only, keys
+    outside the build range, and a partial last tile."""
+    nb, n = 30_000, 1_000_037
+    dim = datagen.dimension(nb, seed=27)
+    fact = datagen.fact_fk(n, nb, 0.8, seed=28)
+    fact["fk"][::101] = nb + 9
+    fact["fk"][::103] = -4
+    fct = {**CT, "fk": "int"}
+    f = ctx.register(fact, fct)
+    dt = ctx.register(dim, datagen.DIMENSION_COLTYPES)
+    bw = col("order_day") < datagen.DAY0 + datagen.NDAYS // 3
+    j = dt.join_build("key", bw)
+    p, d, q = col("price_cents"), col("discount_pct"), col("quantity")
+    cases = [
+        ((build_col("segment"),), [sum_(p * (100 - d)), count_star()]),
+        ((build_col("segment"),), [count_star()]),
+        ((build_col("order_day"),), [sum_(q), count_star(), sum_((p - 7) * (d + 3))]),
+        ((build_col("segment"), build_col("order_day")), [sum_(p), count_star()]),
+        ((), [sum_(p * d), count_star(), avg(q)]),
+    ]
+    for gb, aggs in cases:
+        g = f.aggregate(aggs, gb, None, join=j, probe_key="fk")
+        o = oracle.aggregate(fact, fct, aggs, gb, None, build=(dim, datagen.DIMENSION_COLTYPES, "key", bw),
+                             probe_key="fk")
+        same_query(g, o)
+    j.drop()
+    dt.drop()
+    f.drop()
