@@ -83,3 +83,37 @@ def test_merged_batches_equal_queries_alone(ctx):
     j.drop()
     f.drop()
     d.drop()
+
+
+def test_batch_mixing_join_group_layouts(ctx):
+    """One batch over one join whose queries fold different build-side group
+    layouts into payload arrays: a lone join query (25 groups), a merged class
+    of join queries (quantity buckets x 25 groups) and joins grouped by
+    (segment, order_day) and by order_day alone. Each layout keeps its own
+    payload array, so every result equals the query run alone and the
+    oracle's, in either submission order."""
+    rng = np.random.default_rng(7)
+    fact = datagen.fact_fk(700_003, 20_000, 0.8, seed=71)
+    dim = datagen.dimension(20_000, seed=72)
+    f = ctx.register(fact, FCT)
+    d = ctx.register(dim, datagen.DIMENSION_COLTYPES)
+    tj = workloads.join_group_agg()
+    j = d.join_build("key", tj.build_where)
+    q = col("quantity")
+    specs = [([count_star()], tj.group_by, q < 30)]
+    specs += [(tj.aggs, tj.group_by, q < int(c)) for c in rng.integers(1, 52, 24)]
+    specs += [([count_star(), sum_(col("price_cents"))], (build_col("segment"), build_col("order_day")), q < 40),
+              ([sum_(q), count_star()], (build_col("order_day"),), None)]
+    pqs = [f.prepare(a, g, w, join=j, probe_key="fk") for a, g, w in specs]
+    build = (dim, datagen.DIMENSION_COLTYPES, "key", tj.build_where)
+    for batch_order in (list(range(len(pqs))), list(range(len(pqs)))[::-1]):
+        batch = [pqs[i] for i in batch_order]
+        outs = ctx.submit(batch).wait()
+        for i, o in zip(batch_order, outs):
+            same_query(o, pqs[i].run())
+            if i in (0, 1, len(pqs) - 2, len(pqs) - 1):
+                a, g, w = specs[i]
+                same_query(o, oracle.aggregate(fact, FCT, a, g, w, build=build, probe_key="fk"))
+    j.drop()
+    f.drop()
+    d.drop()

@@ -844,9 +844,9 @@ int upload(tgp_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 void free_join(tgp_ctx* ctx, JoinTable& J) {
     dev_free(ctx, J.tab);
-    dev_free(ctx, J.pay);
     J.tab = nullptr;
-    J.pay = nullptr;
+    for (auto& kv : J.pays) dev_free(ctx, kv.second.ptr);
+    J.pays.clear();
 }
 
 }  // namespace
@@ -1464,6 +1464,7 @@ struct QueryState {
     const tgp_query* q = nullptr;
     const Table* T = nullptr;
     JoinTable* J = nullptr;
+    std::vector<uint64_t> pay_sig;  // layout of the join payload the plan reads (JoinTable::pays key)
     std::unique_ptr<Builder> b;
     std::vector<AggMap> amap;
     uint32_t nv1 = 1;
@@ -1760,8 +1761,12 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
         PayKeys K;
         std::memset(&K, 0, sizeof(K));
         std::vector<uint64_t> sig;
+        unsigned __int128 vmax = 0;  // the layout's largest payload value
         for (uint32_t k = 0; k < P.ngkey; ++k) {
             if (!P.gkey[k].build_side) continue;
+            const Column& bc = b.B->cols[q->group[k].column];
+            vmax += static_cast<unsigned __int128>(static_cast<uint64_t>(bc.max) - static_cast<uint64_t>(P.gkey[k].min)) *
+                    P.gkey[k].stride;
             K.ptr[K.n] = P.gkey[k].bptr;
             K.dtype[K.n] = P.gkey[k].dtype;
             K.min[K.n] = P.gkey[k].min;
@@ -1769,28 +1774,36 @@ static int plan_query(tgp_ctx* ctx, const tgp_query* q, QueryState& qs, size_t s
             ++K.n;
             sig.insert(sig.end(), {q->group[k].column, static_cast<uint64_t>(P.gkey[k].min), P.gkey[k].stride});
         }
-        // Payload entries as narrow as the group indices allow (u8 below 255
-        // groups, u16 below 65,535; all ones = no match): the array is read
-        // once per probe row, so the narrower it is, the more of it stays in
-        // L1 and L2.
-        const uint32_t pw = D <= 255 ? 1u : (D <= 65535 ? 2u : 4u);
+        // Payload entries as narrow as the layout's largest value allows (u8
+        // below 255, u16 below 65,535; all ones = no match): the array is
+        // read once per probe row, and a narrow one stays in L1 and L2. The
+        // width follows from the layout alone, so every plan of one layout
+        // reads the same array the same way.
+        const uint32_t pw = vmax < 255 ? 1u : (vmax < 65535 ? 2u : 4u);
         sig.push_back(pw);
         const uint64_t entries = J->krange + 1;
+        auto pt = J->pays.find(sig);
         if (dry) {
             // Sizing only (tgp_query_footprint): a payload still to be built
             // counts as memory the query needs; nothing is launched.
-            if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) qs.pending_dev_bytes += entries * 4;
-        } else if (!J->pay || J->pay_entries != entries || J->pay_sig != sig) {
-            if (J->pay && J->pay_entries != entries) {
-                dev_free(ctx, J->pay);
-                J->pay = nullptr;
+            if (pt == J->pays.end()) qs.pending_dev_bytes += entries * pw;
+            P.jpay = pt != J->pays.end() ? pt->second.ptr : (J->pays.empty() ? nullptr : J->pays.begin()->second.ptr);
+        } else {
+            if (pt == J->pays.end()) {
+                JoinTable::Payload np;
+                np.width = pw;
+                TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&np.ptr), std::max<uint64_t>(entries * pw, 16),
+                                  "join payload allocation failed"));
+                const cudaError_t e = launch_join_pay(J->tab, J->cap, K, np.ptr, pw, entries, ctx->sms, ctx->stream);
+                if (e != cudaSuccess) {
+                    dev_free(ctx, np.ptr);
+                    return fail(ctx, TGP_DEVICE_ERROR, std::string("join payload: ") + cudaGetErrorString(e));
+                }
+                pt = J->pays.emplace(sig, np).first;
             }
-            if (!J->pay) TGP_TRY(dev_alloc(ctx, reinterpret_cast<void**>(&J->pay), entries * 4, "join payload allocation failed"));
-            J->pay_entries = entries;
-            J->pay_sig = sig;
-            TGP_CUDA(launch_join_pay(J->tab, J->cap, K, J->pay, pw, entries, ctx->sms, ctx->stream));
+            P.jpay = pt->second.ptr;
         }
-        P.jpay = J->pay;
+        qs.pay_sig = sig;
         P.jpay_w = pw;
     }
 
@@ -3475,7 +3488,7 @@ int graph_check(tgp_ctx* ctx, const GraphRec& g) {
     if (g.join) {
         auto jt = ctx->joins.find(g.join);
         if (jt == ctx->joins.end() || &jt->second != g.J || jt->second.tab != g.jtab ||
-            (g.jpay && (jt->second.pay != g.jpay || jt->second.pay_sig != g.jsig)))
+            (g.jpay && (jt->second.pays.count(g.jsig) == 0 || jt->second.pays.at(g.jsig).ptr != g.jpay)))
             return fail(ctx, TGP_NOT_FOUND, "captured query: join dropped or its payload rebuilt; capture again");
     }
     return TGP_OK;
@@ -3511,7 +3524,7 @@ int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out) {
         g.J = qs.J;
         g.jtab = qs.J->tab;
         g.jpay = P.jpay;
-        if (g.jpay) g.jsig = qs.J->pay_sig;
+        if (g.jpay) g.jsig = qs.pay_sig;
     }
 
     g.block_words = qs.block_words();

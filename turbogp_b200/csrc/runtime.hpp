@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <map>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -162,10 +163,16 @@ struct JoinTable {
     uint64_t entries = 0;               // build rows inserted
     bool empty_range = false;           // no build key statistics (empty build side)
     bool unique = false;                // no two build rows share a key (packed tables only)
-    // Cached payload array for one build-side group-key layout (see PayKeys).
-    uint32_t* pay = nullptr;
-    uint64_t pay_entries = 0;
-    std::vector<uint64_t> pay_sig;      // (column, min, stride) per build-side key
+    // Payload arrays, one per build-side group-key layout (see PayKeys;
+    // keyed by (column, min, stride) per build-side key, then the entry
+    // width), each kept until the join is dropped: a plan reads its layout's
+    // array for as long as its launches run, so no array is rebuilt in place
+    // under a plan of another layout.
+    struct Payload {
+        uint32_t* ptr = nullptr;
+        uint32_t width = 4;
+    };
+    std::map<std::vector<uint64_t>, Payload> pays;
 };
 
 // Scan variant knobs. The planner's rules fill them by default; the
