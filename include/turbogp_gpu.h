@@ -562,8 +562,9 @@ TGP_API int tgp_batch_poll(tgp_ctx* ctx, tgp_batch_id batch, int wait);
  * Direct-indexed and scalar aggregates only (hash grouping sizes its result
  * from the data: TGP_UNSUPPORTED). The graph reads the table's and join's
  * device memory as they were at capture: launching after the table or join was
- * dropped, or after a join's payload array was rebuilt for another key layout,
- * returns TGP_NOT_FOUND (capture again). Reloading a table in place
+ * dropped returns TGP_NOT_FOUND (capture again); a join keeps one payload
+ * array per build-side key layout until it is dropped, so queries of other
+ * layouts leave the graph valid. Reloading a table in place
  * (tgp_table_reload) keeps the graph valid, and the graph sees the new rows,
  * as long as every column's min / max stays as it was (the plan's bounds are
  * proven from them); otherwise the launch returns TGP_NOT_FOUND as well. */

@@ -3489,7 +3489,7 @@ int graph_check(tgp_ctx* ctx, const GraphRec& g) {
         auto jt = ctx->joins.find(g.join);
         if (jt == ctx->joins.end() || &jt->second != g.J || jt->second.tab != g.jtab ||
             (g.jpay && (jt->second.pays.count(g.jsig) == 0 || jt->second.pays.at(g.jsig).ptr != g.jpay)))
-            return fail(ctx, TGP_NOT_FOUND, "captured query: join dropped or its payload rebuilt; capture again");
+            return fail(ctx, TGP_NOT_FOUND, "captured query: join dropped or rebuilt; capture again");
     }
     return TGP_OK;
 }
