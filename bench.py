@@ -362,8 +362,8 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
         step = q.run
         tables = [(t, host)]
         kernel_bytes = 26 * n
-        dominant = "scan_kernel<MODE_GROUP_PRIVATE, int64, DenseShape<Q1>> (6 direct groups)"
-        traffic = traffic_per_launch("filtered_group_agg_6M_scan_kernel.md", n)
+        dominant = "q1_group_kernel (streaming loads, per-thread private partials, 6 direct groups)"
+        traffic = traffic_per_launch("filtered_group_agg_6M_q1_group_kernel.md", n)
         check = lambda out: _check_exact(out, host, CT, tpl.aggs, tpl.group_by, tpl.where)
         cleanup = [t.drop]
     elif name == "join_group_agg":

@@ -410,3 +410,26 @@ def test_join_payload_widths_and_shapes(ctx):
     j.drop()
     dt.drop()
     f.drop()
+
+
+@pytest.mark.parametrize("n", [0, 5, 127, 128, 1_000_003])
+def test_q1_shape_streaming_predicates(ctx, n):
+    """The TPC-H Q1 shape (GROUP BY two u8 flags, count and four sums) under
+    no predicate, one to four int32 leaves, a negated leaf, and a leaf kind
+    the streaming kernel does not take (u8 column: the scan kernel runs),
+    with row counts below, at and past a 128-row chunk."""
+    h = datagen.lineitem(n, seed=41 + n)
+    t = ctx.register(h, CT)
+    tpl = workloads.filtered_group_agg()
+    d0, c = datagen.DAY0, col
+    wheres = [None,
+              c("ship_day") <= d0 + 2000,
+              (c("ship_day") >= d0 + 300) & (c("ship_day") < d0 + 2100) & c("discount_pct").between(2, 8) &
+              (c("quantity") < 40) & (c("tax_pct") > 1),
+              ~(c("tax_pct") < 3) & (c("quantity") > 5),
+              (c("flag_a") == 1) & (c("ship_day") <= d0 + 2400)]
+    for w in wheres:
+        g = t.aggregate(tpl.aggs, tpl.group_by, w)
+        o = oracle.aggregate(h, CT, tpl.aggs, tpl.group_by, w)
+        same_query(g, o)
+    t.drop()

@@ -805,6 +805,70 @@ int launch_direct_groups(tgp_ctx* ctx, const Plan& P, uint64_t max_abs_val) {
     return TGP_OK;
 }
 
+// The TPC-H Q1 shape (two u8 keys, the fixed value program ShapeQ1) under at
+// most four int32 predicate leaves and no join: the streaming kernel of
+// groupby_direct.cu in place of the scan pipeline when every global sum and
+// every thread's partial provably fits int64 and two CTAs' private partials
+// fit an SM (else false, nothing launched).
+int try_launch_q1(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128, uint64_t ngroups, uint64_t max_abs_val,
+                  bool* done) {
+    *done = false;
+    if (mode != MODE_GROUP_PRIVATE || acc128 || P.shape != 1 || !P.dense_vec || P.jslot >= 0 || P.ngkey != 2 ||
+        !P.sum64 || P.check_ovf || P.nval != 4 || P.chain.nsteps != 4 || ngroups == 0 || ngroups > 0xffffffffull)
+        return TGP_OK;
+    if (P.nleaf > 4 || (P.nleaf && !(P.all_and && P.kend[0] == P.nleaf))) return TGP_OK;
+    if (q1_group_ctas_per_sm(static_cast<uint32_t>(ngroups)) < 2) return TGP_OK;
+    auto slot_ptr = [&](uint32_t soff) -> const uint8_t* {
+        for (uint32_t k = 0; k < P.nslots; ++k)
+            if (P.slot[k].smem_off == soff) return P.slot[k].ptr;
+        return nullptr;
+    };
+    Q1Args A;
+    std::memset(&A, 0, sizeof(A));
+    for (uint32_t i = 0; i < P.nleaf; ++i) {
+        A.leaf_col[i] = P.slot[P.leaf[i].slot].ptr;
+        A.leaf_lo[i] = P.leaf[i].lo32;
+        A.leaf_sp[i] = P.leaf[i].span32;
+        if (P.leaf[i].negate) A.leaf_neg |= 1u << i;
+    }
+    A.nleaf = P.nleaf;
+    A.key0 = P.slot[P.gkey[0].slot].ptr;
+    A.key1 = P.slot[P.gkey[1].slot].ptr;
+    A.kmin0 = static_cast<uint32_t>(P.gkey[0].min);
+    A.kmin1 = static_cast<uint32_t>(P.gkey[1].min);
+    A.kstride0 = static_cast<uint32_t>(P.gkey[0].stride);
+    A.kstride1 = static_cast<uint32_t>(P.gkey[1].stride);
+    for (uint32_t s = 0; s < 4; ++s) {
+        const ChainStep& S = P.chain.s[s];
+        if (S.acc != s + 1) return TGP_OK;
+        A.col[s] = slot_ptr(S.soff);
+        if (!A.col[s]) return TGP_OK;
+    }
+    const int ms[3] = {0, 2, 3};
+    for (int i = 0; i < 3; ++i) {
+        A.mul[i] = static_cast<uint32_t>(P.chain.s[ms[i]].mul32);
+        A.add[i] = static_cast<uint32_t>(P.chain.s[ms[i]].add32);
+    }
+    A.ngroups = static_cast<uint32_t>(ngroups);
+    A.nrows = P.nrows;
+    A.acc = P.acc;
+    A.counters = P.counters;
+    const uint64_t chunks = P.nrows / 128;
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((chunks + 15) / 16, static_cast<uint64_t>(ctx->sms) * 2));
+    // A thread adds at most ceil(chunks / warps) chunks of four rows and four
+    // rows of the partial last chunk: its int64 partials must not wrap.
+    const uint64_t nwarps = grid * 16;
+    const unsigned __int128 rows_thread = static_cast<unsigned __int128>((chunks + nwarps - 1) / nwarps + 1) * 4;
+    if (rows_thread * std::max<uint64_t>(max_abs_val, 1) >= (static_cast<unsigned __int128>(1) << 63)) return TGP_OK;
+    std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
+    TGP_TRY(profile_begin(ctx, &ev));
+    const cudaError_t e = launch_q1_group(A, static_cast<int>(grid), ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, TGP_DEVICE_ERROR, std::string("grouped launch: ") + cudaGetErrorString(e));
+    if (ev) TGP_CUDA(cudaEventRecord(ev->second, ctx->stream));
+    *done = true;
+    return TGP_OK;
+}
+
 int get_table(tgp_ctx* ctx, tgp_table_id id, const Table** out) {
     auto it = ctx->tables.find(id);
     if (it == ctx->tables.end()) return fail(ctx, TGP_NOT_FOUND, "unknown table id");
@@ -2047,7 +2111,9 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
         direct_group_supported(P.slot[P.gkey[0].slot].dtype, P.nval ? P.slot[P.val[0].f[0].slot].dtype : 0u)) {
         TGP_TRY(launch_direct_groups(ctx, P, b.max_abs_val));
     } else {
-        TGP_TRY(launch(ctx, P, mode, acc128));
+        bool done = false;
+        TGP_TRY(try_launch_q1(ctx, P, mode, acc128, ngroups_direct, b.max_abs_val, &done));
+        if (!done) TGP_TRY(launch(ctx, P, mode, acc128));
     }
 
     TGP_TRY(pinned_reserve(ctx, block_words * 8));

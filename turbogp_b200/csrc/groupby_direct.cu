@@ -1,6 +1,8 @@
-// groupby_direct.cu — unfiltered GROUP BY of one key over a moderate range
-// (the reference's try_accumulator_grouped, aggregate.rs / accum_grouped.rs,
-// on its high-cardinality inputs) into one-word direct slots.
+// groupby_direct.cu — streaming GROUP BY kernels, rows read straight from
+// HBM without the scan engine's stage ring: (1) an unfiltered GROUP BY of one
+// key over a moderate range (the reference's try_accumulator_grouped,
+// aggregate.rs / accum_grouped.rs, on its high-cardinality inputs) into
+// one-word direct slots; (2) the TPC-H Q1 shape (further below).
 //
 // A slot per key value (key - min < 2^27) holds (row count << shift) + the
 // sum of (value - bias) over its rows; the host proved that neither field can
@@ -244,6 +246,112 @@ const void* dg_kernel(uint32_t kdt, uint32_t vdt) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// The TPC-H Q1 shape (execute_grouped, aggregate.rs:45-505, on a predicate of
+// at most four int32 leaves): GROUP BY two u8 keys, COUNT(*), sum(i32),
+// sum(i64), sum(i64 * (k - i32)), sum(i64 * (k - i32) * (k + i32)), every
+// sum proven to fit int64. Rows stream from HBM with coalesced loads (four
+// consecutive rows per lane); each thread keeps private partials (u32 row
+// counts, int64 sums) in shared memory, updated by plain read-modify-writes,
+// with no stage ring, so two CTAs of 512 threads fit an SM; at the end each
+// (group, value) is summed over the CTA's threads by one warp and added to
+// the query's accumulator with one 64-bit atomic.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 ldcs4(const uint8_t* base, uint64_t byte_off) {
+    return __ldcs(reinterpret_cast<const uint4*>(base + byte_off));
+}
+
+__global__ void __launch_bounds__(kDgThreads, 2) q1_group_kernel(const Q1Args A) {
+    extern __shared__ __align__(16) uint8_t q1_smem[];
+    constexpr uint32_t NT = kDgThreads;
+    const uint32_t t = threadIdx.x, lane = t & 31u;
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(q1_smem);                         // [g][t]
+    long long* val = reinterpret_cast<long long*>(q1_smem + A.ngroups * NT * 4);  // [g][v][t]
+    for (uint32_t g = 0; g < A.ngroups; ++g) cnt[g * NT + t] = 0;
+    for (uint32_t i = 0; i < A.ngroups * 4; ++i) val[i * NT + t] = 0;
+
+    // One row: its selection mask (all ones or 0), group and column cells.
+    auto add_row = [&](uint32_t sel, uint32_t g, uint32_t qty, int64_t price, uint32_t disc, uint32_t tax) {
+        const uint64_t sm = static_cast<uint64_t>(static_cast<int64_t>(static_cast<int32_t>(sel)));
+        const uint64_t v1 = static_cast<uint64_t>(A.mul[0] * qty + A.add[0]) & sm;
+        const uint64_t v2 = static_cast<uint64_t>(price) & sm;
+        const uint64_t v3 = v2 * static_cast<uint64_t>(A.mul[1] * disc + A.add[1]);
+        const uint64_t v4 = v3 * static_cast<uint64_t>(A.mul[2] * tax + A.add[2]);
+        cnt[g * NT + t] += sel & 1u;
+        long long* w = val + static_cast<size_t>(g) * 4 * NT + t;
+        w[0] += static_cast<long long>(v1);
+        w[NT] += static_cast<long long>(v2);
+        w[2 * NT] += static_cast<long long>(v3);
+        w[3 * NT] += static_cast<long long>(v4);
+    };
+    auto leaf = [&](uint32_t x, uint32_t i) { return ((x - A.leaf_lo[i]) <= A.leaf_sp[i] ? 1u : 0u) ^ ((A.leaf_neg >> i) & 1u); };
+
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * NT + t) >> 5;
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (NT / 32);
+    const uint64_t nfull = A.nrows / kDgRows;
+    for (uint64_t c = warp; c < nfull; c += nwarps) {
+        const uint64_t r = c * kDgRows + 4 * lane;  // this lane's four rows
+        const uint4 q = ldcs4(A.col[0], r * 4);
+        const uint4 p0 = ldcs4(A.col[1], r * 8), p1 = ldcs4(A.col[1], r * 8 + 16);
+        const uint4 d = ldcs4(A.col[2], r * 4);
+        const uint4 x = ldcs4(A.col[3], r * 4);
+        const uint32_t k0 = __ldcs(reinterpret_cast<const unsigned int*>(A.key0 + r));
+        const uint32_t k1 = __ldcs(reinterpret_cast<const unsigned int*>(A.key1 + r));
+        uint4 lv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (static_cast<uint32_t>(i) < A.nleaf) lv[i] = ldcs4(A.leaf_col[i], r * 4);
+        const uint32_t qa[4] = {q.x, q.y, q.z, q.w}, da[4] = {d.x, d.y, d.z, d.w}, xa[4] = {x.x, x.y, x.z, x.w};
+        const int64_t pa[4] = {static_cast<int64_t>((static_cast<uint64_t>(p0.y) << 32) | p0.x),
+                               static_cast<int64_t>((static_cast<uint64_t>(p0.w) << 32) | p0.z),
+                               static_cast<int64_t>((static_cast<uint64_t>(p1.y) << 32) | p1.x),
+                               static_cast<int64_t>((static_cast<uint64_t>(p1.w) << 32) | p1.z)};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            uint32_t m = 1u;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (static_cast<uint32_t>(i) >= A.nleaf) break;
+                const uint32_t cell = e == 0 ? lv[i].x : e == 1 ? lv[i].y : e == 2 ? lv[i].z : lv[i].w;
+                m &= leaf(cell, static_cast<uint32_t>(i));
+            }
+            const uint32_t g = (((k0 >> (8 * e)) & 0xffu) - A.kmin0) * A.kstride0 +
+                               (((k1 >> (8 * e)) & 0xffu) - A.kmin1) * A.kstride1;
+            add_row(0u - m, g, qa[e], pa[e], da[e], xa[e]);
+        }
+    }
+    // The partial last chunk, one row per lane of one warp.
+    if (warp == nfull % nwarps) {
+        for (uint64_t r = nfull * kDgRows + lane; r < A.nrows; r += 32) {
+            uint32_t m = 1u;
+            for (uint32_t i = 0; i < A.nleaf; ++i) m &= leaf(reinterpret_cast<const uint32_t*>(A.leaf_col[i])[r], i);
+            const uint32_t g = (static_cast<uint32_t>(A.key0[r]) - A.kmin0) * A.kstride0 +
+                               (static_cast<uint32_t>(A.key1[r]) - A.kmin1) * A.kstride1;
+            add_row(0u - m, g, reinterpret_cast<const uint32_t*>(A.col[0])[r],
+                    reinterpret_cast<const long long*>(A.col[1])[r], reinterpret_cast<const uint32_t*>(A.col[2])[r],
+                    reinterpret_cast<const uint32_t*>(A.col[3])[r]);
+        }
+    }
+    __syncthreads();
+    // Merge: warp w sums (group, slot) pairs w, w + 16, ... over the CTA's
+    // threads; slot 0 is the row count, slots 1-4 the sums.
+    const uint32_t wib = t >> 5;
+    for (uint32_t i = wib; i < A.ngroups * 5; i += NT / 32) {
+        const uint32_t g = i / 5, v = i % 5;
+        unsigned long long sum = 0;
+        for (uint32_t k = lane; k < NT; k += 32)
+            sum += v == 0 ? static_cast<unsigned long long>(cnt[g * NT + k])
+                          : static_cast<unsigned long long>(val[(static_cast<size_t>(g) * 4 + v - 1) * NT + k]);
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, d);
+        if (lane == 0 && sum) {
+            atomicAdd(A.acc + 2ull * (g * 5 + v), sum);
+            if (v == 0) atomicAdd(A.counters, sum);  // selected rows
+        }
+    }
+}
+
 }  // namespace
 
 bool direct_group_supported(uint32_t kdt, uint32_t vdt) { return dg_kernel(kdt, vdt) != nullptr; }
@@ -257,6 +365,31 @@ int direct_group_ctas_per_sm(uint32_t hs, bool hasv) {
         return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kDgThreads, smem) != cudaSuccess) return 0;
     return occ;
+}
+
+size_t q1_group_smem(uint32_t ngroups) { return static_cast<size_t>(ngroups) * kDgThreads * (4 + 4 * 8); }
+
+int q1_group_ctas_per_sm(uint32_t ngroups) {
+    const void* f = reinterpret_cast<const void*>(&q1_group_kernel);
+    const size_t smem = q1_group_smem(ngroups);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
+        return 0;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kDgThreads, smem) != cudaSuccess) return 0;
+    return occ;
+}
+
+cudaError_t launch_q1_group(const Q1Args& A, int grid, cudaStream_t st) {
+    const void* f = reinterpret_cast<const void*>(&q1_group_kernel);
+    const size_t smem = q1_group_smem(A.ngroups);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    Q1Args a = A;
+    void* args[] = {&a};
+    return cudaLaunchKernel(f, dim3(static_cast<unsigned>(grid)), dim3(kDgThreads), args, smem, st);
 }
 
 cudaError_t launch_direct_group(const DirectGroupArgs& A, uint32_t kdt, uint32_t vdt, int grid, cudaStream_t st) {

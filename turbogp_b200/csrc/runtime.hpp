@@ -44,6 +44,29 @@ struct DirectGroupArgs {
     uint32_t* err;
     unsigned long long* counters;  // [0] += nrows (every row is selected)
 };
+// The TPC-H Q1 shape (groupby_direct.cu): GROUP BY two u8 keys under at
+// most four int32 predicate leaves (x - lo <= span, negated per bit of
+// leaf_neg); COUNT(*) and sum(mul0 * c0 + add0), sum(c1), sum(c1 * (mul1 *
+// c2 + add1)), sum(c1 * (mul1 * c2 + add1) * (mul2 * c3 + add2)) with c0, c2,
+// c3 int32 (non-negative factors) and c1 int64; accumulators [g][5][2]
+// receive int64 partials in their low limbs.
+struct Q1Args {
+    const uint8_t* leaf_col[4];
+    uint32_t leaf_lo[4], leaf_sp[4];
+    uint32_t leaf_neg, nleaf;
+    const uint8_t* key0;
+    const uint8_t* key1;
+    uint32_t kmin0, kmin1, kstride0, kstride1;
+    const uint8_t* col[4];
+    uint32_t mul[3], add[3];
+    uint32_t ngroups, _pad;
+    uint64_t nrows;
+    unsigned long long* acc;
+    unsigned long long* counters;
+};
+size_t q1_group_smem(uint32_t ngroups);
+int q1_group_ctas_per_sm(uint32_t ngroups);
+cudaError_t launch_q1_group(const Q1Args& A, int grid, cudaStream_t st);
 bool direct_group_supported(uint32_t kdt, uint32_t vdt);
 int direct_group_ctas_per_sm(uint32_t hs, bool hasv);
 cudaError_t launch_direct_group(const DirectGroupArgs& A, uint32_t kdt, uint32_t vdt, int grid, cudaStream_t st);
