@@ -585,7 +585,10 @@ TGP_API int tgp_graph_drop(tgp_ctx* ctx, tgp_graph_id graph);
  * after `wait_ns` (1 ms to 1 s) instead of 1 s. The consumers' wait for that
  * copy runs out, the kernel raises its timeout bit and returns, and the call
  * returns TGP_TIMEOUT; the context stays usable for the next query. One-shot:
- * later launches are not affected. A wait that gives up, not a fault. */
+ * later launches are not affected. A wait that gives up, not a fault. While
+ * it is armed, the next aggregate runs on the scan pipeline even where a
+ * streaming GROUP BY kernel (which has no stage copies and no waits) would
+ * otherwise take it. */
 TGP_API int tgp_debug_fail_next_scan(tgp_ctx* ctx, uint64_t tile, uint64_t wait_ns);
 
 /* ------------------------------------------------------------------------ */

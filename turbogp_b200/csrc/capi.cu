@@ -813,6 +813,9 @@ int launch_direct_groups(tgp_ctx* ctx, const Plan& P, uint64_t max_abs_val) {
 int try_launch_q1(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128, uint64_t ngroups, uint64_t max_abs_val,
                   bool* done) {
     *done = false;
+    // An armed failure-path hook (tgp_debug_fail_next_scan) targets the scan
+    // pipeline's stage copies; this kernel has no stage ring and no waits.
+    if (ctx->dbg_skip_tile1) return TGP_OK;
     if (mode != MODE_GROUP_PRIVATE || acc128 || P.shape != 1 || !P.dense_vec || P.jslot >= 0 || P.ngkey != 2 ||
         !P.sum64 || P.check_ovf || P.nval != 4 || P.chain.nsteps != 4 || ngroups == 0 || ngroups > 0xffffffffull)
         return TGP_OK;
@@ -2107,7 +2110,7 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     }
     TGP_TRY(size_smem(ctx, P, extra, scan_kernel_static_smem(), &qs.kn));
     bound_presum(ctx, qs);
-    if (P.hpack && P.nleaf == 0 && P.hash_fast &&
+    if (P.hpack && P.nleaf == 0 && P.hash_fast && !ctx->dbg_skip_tile1 &&
         direct_group_supported(P.slot[P.gkey[0].slot].dtype, P.nval ? P.slot[P.val[0].f[0].slot].dtype : 0u)) {
         TGP_TRY(launch_direct_groups(ctx, P, b.max_abs_val));
     } else {
@@ -3419,7 +3422,12 @@ int tgp_batch_submit(tgp_ctx* ctx, tgp_batch_item* items, uint32_t n, tgp_batch_
     // 6. One upload, the queries with launches of their own, the persistent
     // launches, one readback.
     TGP_CUDA(cudaMemcpyAsync(B->dev, h, total, cudaMemcpyHostToDevice, ctx->stream));
-    for (uint32_t i : solo) TGP_TRY(launch(ctx, B->qs[i].b->P, B->qs[i].mode, B->qs[i].acc128));
+    for (uint32_t i : solo) {
+        const QueryState& qs = B->qs[i];
+        bool done = false;
+        TGP_TRY(try_launch_q1(ctx, qs.b->P, qs.mode, qs.acc128, qs.ngroups_direct, qs.b->max_abs_val, &done));
+        if (!done) TGP_TRY(launch(ctx, qs.b->P, qs.mode, qs.acc128));
+    }
     for (auto& M : B->merges) {
         TGP_TRY(launch(ctx, M->qs.b->P, M->qs.mode, M->qs.acc128));
         if (M->has_count) TGP_TRY(launch(ctx, M->cqs.b->P, M->cqs.mode, M->cqs.acc128));
