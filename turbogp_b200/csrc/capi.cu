@@ -687,7 +687,17 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = sc
     // stages and 0.373 ms with two (L1 hit rate 8.8 -> 17.5 %), merged join
     // batches 0.85 -> 0.77 ms; the limb tables' few KB leave room for four.
     int max_st = K.max_stages;
-    if (P.jpay != nullptr && K.max_stages >= kMaxStages && stage) {
+    // Joins through a payload array on the limb tables with a fixed-shape
+    // value program run two CTAs of 512 threads and two stages per SM (34
+    // warps instead of 17 to hide the payload lookups; 60M x 1.5M probe
+    // 0.164 -> 0.140 ms at 30M probe rows), unless a variant caps the stages
+    // and keeps one CTA.
+    P.two_ctas = (P.jpay != nullptr && P.s32_copies != 0 && P.shape != 0 && P.nthreads == 512 && stage &&
+                  (K.ctas_per_sm == 2 || K.max_stages >= kMaxStages)) ? 1u : 0u;
+    if (P.two_ctas) {
+        avail = budget / 2 > kBarrierBytes + extra_bytes ? budget / 2 - kBarrierBytes - extra_bytes : 0;
+        max_st = 2;
+    } else if (P.jpay != nullptr && K.max_stages >= kMaxStages && stage) {
         const size_t room = kJoinSmemCap > kBarrierBytes + extra_bytes ? kJoinSmemCap - kBarrierBytes - extra_bytes : 0;
         max_st = static_cast<int>(std::max<size_t>(2, room / stage));
     }
@@ -695,6 +705,7 @@ int size_smem(tgp_ctx* ctx, Plan& P, size_t extra_bytes, size_t static_smem = sc
     uint32_t S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
     if (S == 0) {
         // Fall back to a single CTA per SM.
+        P.two_ctas = 0;
         avail = budget > kBarrierBytes + extra_bytes ? budget - kBarrierBytes - extra_bytes : 0;
         S = stage ? static_cast<uint32_t>(std::min<size_t>(avail / stage, cap)) : 1;
         if (S == 0) return fail(ctx, TGP_UNSUPPORTED, "query does not fit in shared memory");
@@ -744,7 +755,7 @@ int launch(tgp_ctx* ctx, const Plan& P0, uint32_t mode, bool acc128) {
     const Plan& P = *pp;
     const uint64_t ntiles = (P.nrows + kTileRows - 1) / kTileRows;
     if (ntiles == 0) return TGP_OK;
-    int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape);
+    int occ = scan_occupancy(mode, acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape, P.two_ctas != 0);
     if (occ <= 0) return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
     const uint64_t grid = std::min<uint64_t>(ntiles, static_cast<uint64_t>(ctx->sms) * occ);
     std::pair<cudaEvent_t, cudaEvent_t>* ev = nullptr;
@@ -3617,7 +3628,7 @@ int tgp_graph_capture(tgp_ctx* ctx, const tgp_query* q, tgp_graph_id* out) {
     }
     TGP_TRY(size_smem(ctx, P, qs.extra, scan_kernel_static_smem(), &qs.kn));
     // Kernel attributes and occupancy are settled before the capture.
-    if (scan_occupancy(qs.mode, qs.acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape) <= 0)
+    if (scan_occupancy(qs.mode, qs.acc128, static_cast<int>(P.nthreads), P.smem_bytes, P.shape, P.two_ctas != 0) <= 0)
         return fail(ctx, TGP_DEVICE_ERROR, "scan kernel cannot be resident with this shared memory");
 
     TGP_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -273,7 +273,7 @@ struct alignas(16) Plan {
     uint32_t hpack_shift;
     int64_t hpack_bias;
     uint32_t jpay_w;
-    uint32_t _pad_jpay;
+    uint32_t two_ctas;      // launch the register budget of two CTAs per SM (join-payload limb-table shapes)
     RegBlock rb;                    // filled by fill_reg_block before every launch
 };
 

@@ -70,7 +70,7 @@ cudaError_t launch_q1_group(const Q1Args& A, int grid, cudaStream_t st);
 bool direct_group_supported(uint32_t kdt, uint32_t vdt);
 int direct_group_ctas_per_sm(uint32_t hs, bool hasv);
 cudaError_t launch_direct_group(const DirectGroupArgs& A, uint32_t kdt, uint32_t vdt, int grid, cudaStream_t st);
-int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape = 0);
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape = 0, bool pair = false);
 // Index (>= 1) of the ahead-of-time dense kernel matching the plan's key
 // dtypes and value program, or 0 (the interpreted dense program runs).
 uint32_t dense_shape_of(const Plan& P);

@@ -2108,8 +2108,10 @@ __device__ __forceinline__ void count_selected(const Plan& P, unsigned long long
 }
 
 // One query: CTA b walks tiles b, b + gridDim.x, ...
-template <uint32_t MODE, bool ACC128, int NT, class SH = void>
-__global__ void __launch_bounds__(NT + 32, 1) scan_kernel(const __grid_constant__ Plan P) {
+// MINB: CTAs per SM the register budget is set for (2 for the join-payload
+// limb-table shapes, which run two CTAs of two stages each).
+template <uint32_t MODE, bool ACC128, int NT, class SH = void, int MINB = 1>
+__global__ void __launch_bounds__(NT + 32, MINB) scan_kernel(const __grid_constant__ Plan P) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + kMaxStages;
@@ -2389,6 +2391,7 @@ struct ShapeEntry {
     const void* k512;
     const void* s32_256;   // the same value program on the limb tables (keys at run time)
     const void* s32_512;
+    const void* s32_512_pair;  // registers for two CTAs per SM (Plan::two_ctas)
 };
 
 template <class SH>
@@ -2403,6 +2406,7 @@ static ShapeEntry shape_entry() {
     e.k512 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 512, SH>);
     e.s32_256 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_SHARED32, false, 256, SH>);
     e.s32_512 = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_SHARED32, false, 512, SH>);
+    e.s32_512_pair = reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_SHARED32, false, 512, SH, 2>);
     return e;
 }
 
@@ -2496,7 +2500,7 @@ uint32_t dense_shape_of(const Plan& P) {
     return 0;
 }
 
-static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t shape = 0) {
+static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t shape = 0, bool pair = false) {
     if (shape == kShapeScalar && mode == MODE_GROUP_PRIVATE && !acc128) {
         return nt == 512 ? reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 512, ScalarTag>)
              : nt == 256 ? reinterpret_cast<const void*>(scan_kernel<MODE_GROUP_PRIVATE, false, 256, ScalarTag>)
@@ -2511,7 +2515,9 @@ static const void* select_kernel(uint32_t mode, bool acc128, int nt, uint32_t sh
     if (shape && mode == MODE_GROUP_SHARED32) {
         uint32_t n = 0;
         const ShapeEntry* tab = shape_table(&n);
-        if (shape <= n) return nt == 512 ? tab[shape - 1].s32_512 : nt == 256 ? tab[shape - 1].s32_256 : nullptr;
+        if (shape <= n)
+            return nt == 512 ? (pair ? tab[shape - 1].s32_512_pair : tab[shape - 1].s32_512)
+                 : nt == 256 ? tab[shape - 1].s32_256 : nullptr;
         return nullptr;
     }
     return nt == 512 ? select_kernel<512>(mode, acc128) : nt == 256 ? select_kernel<256>(mode, acc128) : nullptr;
@@ -2556,7 +2562,7 @@ static cudaError_t ensure_smem_limit(KernelCacheEntry* e, const void* f, int sme
 
 // Launches with blockDim = nthreads consumers + one producer warp.
 cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cudaStream_t st) {
-    const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads), P.shape);
+    const void* f = select_kernel(mode, acc128, static_cast<int>(P.nthreads), P.shape, P.two_ctas != 0);
     if (!f) return cudaErrorInvalidValue;
     {
         std::lock_guard<std::mutex> lock(g_kcache_mu);
@@ -2570,8 +2576,8 @@ cudaError_t launch_scan(const Plan& P, uint32_t mode, bool acc128, int grid, cud
     return cudaLaunchKernel(f, dim3(grid), dim3(L.nthreads + 32), args, L.smem_bytes, st);
 }
 
-int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape) {
-    const void* f = select_kernel(mode, acc128, nt, shape);
+int scan_occupancy(uint32_t mode, bool acc128, int nt, size_t dyn_smem, uint32_t shape, bool pair) {
+    const void* f = select_kernel(mode, acc128, nt, shape, pair);
     if (!f) return 0;
     std::lock_guard<std::mutex> lock(g_kcache_mu);
     KernelCacheEntry* e = kernel_entry(f);
