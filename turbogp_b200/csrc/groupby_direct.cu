@@ -204,7 +204,8 @@ __global__ void __launch_bounds__(kDgThreads, kDgMinBlocks) direct_group_kernel(
         }
         dg_rows<4, HASV>(A, T, key, x);
     }
-    // The partial last chunk, one row per thread of the first warp.
+    // The partial last chunk: the warp next in turn takes it, one row per
+    // lane (no warp-wide step inside, lanes may leave the loop early).
     if (warp == nfull % nwarps) {
         for (uint64_t r = nfull * kDgRows + lane; r < A.nrows; r += 32) {
             const int64_t x[1] = {HASV ? value_of(load_one<VDT>(A.val, r)) : 0};
@@ -245,7 +246,6 @@ const void* dg_kernel(uint32_t kdt, uint32_t vdt) {
         default: return nullptr;
     }
 }
-
 
 // ---------------------------------------------------------------------------
 // The TPC-H Q1 shape (execute_grouped, aggregate.rs:45-505, on a predicate of
