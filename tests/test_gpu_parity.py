@@ -305,11 +305,15 @@ def test_one_word_direct_slots(ctx):
     negative bias), an affine argument, count only, COUNT(col), the shared
     pre-aggregation switched off by large values, a partial last tile, and
     a value range too wide to share a word (the four-word slots again)."""
-    n = 2_000_003
+    # Keys spread over a range past the direct-indexed accumulators' limit
+    # (2^22 groups) and below twice the rows: a slot per key value.
+    n = 2_500_003
     h = datagen.highcard(n, 200_000, 1.1, seed=11)
+    h["key"] = h["key"] * 23
     rng = np.random.default_rng(5)
-    h["negkey"] = h["key"] - 100_000
+    h["negkey"] = h["key"] - 2_300_000
     h["big"] = rng.integers(-2**40, 2**40, n, dtype=np.int64)
+    assert 1 << 22 < int(h["key"].max() - h["key"].min()) + 1 <= 2 * n
     t = ctx.register(h)
     v = col("value")
     cases = [
@@ -317,7 +321,8 @@ def test_one_word_direct_slots(ctx):
         ([count_star(), sum_(v - 500), avg(v - 500)], ("negkey",), v < 900),
         ([count_star()], ("key",), None),
         ([count_col(v), count_star()], ("negkey",), v >= 3),
-        ([count_star(), sum_(v * 3000)], ("key",), None),          # no shared pre-aggregation
+        ([count_star(), sum_(v * 300)], ("key",), None),           # one word, no shared pre-aggregation
+        ([count_star(), sum_(v * 3000)], ("key",), None),          # too wide for one word at 2.5M rows
         ([sum_(col("big")), count_star()], ("key",), None),         # range too wide for one word
     ]
     for aggs, gb, where in cases:
@@ -432,4 +437,23 @@ def test_q1_shape_streaming_predicates(ctx, n):
         g = t.aggregate(tpl.aggs, tpl.group_by, w)
         o = oracle.aggregate(h, CT, tpl.aggs, tpl.group_by, w)
         same_query(g, o)
+    t.drop()
+
+
+def test_footprint_counts_one_word_slots(ctx):
+    """The admission estimate (tgp_query_footprint) sizes the group table the
+    way the run lays it out: one word per key value when COUNT(*) and the SUM
+    share a word, four when the value range is too wide for that; the rest of
+    the estimate (result block, format scratch, formatted groups) is the
+    same for both."""
+    n = 2_500_003
+    h = datagen.highcard(n, 200_000, 1.1, seed=13)
+    h["key"] = h["key"] * 23   # a key range past 2^22 groups: one slot per key value
+    h["big"] = np.random.default_rng(2).integers(-2**40, 2**40, n, dtype=np.int64)
+    t = ctx.register(h)
+    packed = t.prepare([count_star(), sum_(col("value"))], ("key",), None, group_cap=1 << 18).footprint()
+    wide = t.prepare([count_star(), sum_(col("big"))], ("key",), None, group_cap=1 << 18).footprint()
+    keys = int(h["key"].max() - h["key"].min() + 1)
+    assert 1 << 22 < keys <= 2 * n
+    assert wide - packed == max(16, keys) * 3 * 8
     t.drop()

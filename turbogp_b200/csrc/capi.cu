@@ -1963,6 +1963,32 @@ static void bound_presum(tgp_ctx* ctx, QueryState& qs) {
     if (bound >= (static_cast<unsigned __int128>(1) << 31)) P.hsm_slots = 0;
 }
 
+// A directly indexed table of COUNT(*) and at most one SUM / COUNT(col)
+// whose fields provably never meet takes one-word slots (Plan::hpack): the
+// count in the top bits (enough for every row), the sum of (value - its
+// minimum) below. Groups formatted straight from the table only (no top-N,
+// at most kMaxFormatAggs aggregates).
+static void plan_one_word_slots(QueryState& qs, const tgp_query* q, bool topn) {
+    Plan& P = qs.b->P;
+    const Builder& b = *qs.b;
+    if (!(qs.mode == MODE_GROUP_HASH && P.hdirect && P.hash_fast && P.nval <= 1 && !topn &&
+          q->nagg <= static_cast<uint32_t>(kMaxFormatAggs) && P.ngkey == 1 && P.gkey[0].shift == 0 &&
+          (!P.hsm_slots || P.hsm_key32) && (P.nval == 0 || !b.val_big[0])))
+        return;
+    const uint64_t rows = std::max<uint64_t>(qs.T->rows, 1);
+    const uint32_t cbits = 64u - static_cast<uint32_t>(__builtin_clzll(rows));  // count <= rows < 2^cbits
+    const uint32_t shift = P.nval ? 64u - cbits : 0u;
+    const __int128 span = P.nval ? b.val_hi[0] - b.val_lo[0] : 0;
+    const bool fits = P.nval == 0 || (shift < 64 && static_cast<unsigned __int128>(span) * rows <
+                                                       (static_cast<unsigned __int128>(1) << shift));
+    if (fits && (P.nval == 0 || (b.val_lo[0] >= INT64_MIN && b.val_lo[0] <= INT64_MAX))) {
+        P.hpack = 1;
+        P.hpack_shift = shift;
+        P.hpack_bias = P.nval ? static_cast<int64_t>(b.val_lo[0]) : 0;
+        P.hstride = 1;
+    }
+}
+
 // Fills the caller's outputs of a direct-indexed / scalar query from a host
 // copy of its result block.
 static int decode_direct(tgp_ctx* ctx, const QueryState& qs, const unsigned long long* hb, uint64_t* keys_out,
@@ -2062,25 +2088,7 @@ static int execute_impl(tgp_ctx* ctx, const tgp_query* q, uint64_t* keys_out, tg
     const uint32_t total_bits = qs.total_bits;
     (void)nv1;
 
-    // A directly indexed table of COUNT(*) and at most one SUM / COUNT(col)
-    // whose fields provably never meet takes one-word slots: the count in the
-    // top bits (enough for every row), the sum of (value - its minimum) below.
-    if (mode == MODE_GROUP_HASH && P.hdirect && P.hash_fast && P.nval <= 1 && !tn &&
-        q->nagg <= static_cast<uint32_t>(kMaxFormatAggs) && P.ngkey == 1 && P.gkey[0].shift == 0 &&
-        (!P.hsm_slots || P.hsm_key32) && (P.nval == 0 || !b.val_big[0])) {
-        const uint64_t rows = std::max<uint64_t>(T->rows, 1);
-        const uint32_t cbits = 64u - static_cast<uint32_t>(__builtin_clzll(rows));  // count <= rows < 2^cbits
-        const uint32_t shift = P.nval ? 64u - cbits : 0u;
-        const __int128 span = P.nval ? b.val_hi[0] - b.val_lo[0] : 0;
-        const bool fits = P.nval == 0 || (shift < 64 && static_cast<unsigned __int128>(span) * rows <
-                                                           (static_cast<unsigned __int128>(1) << shift));
-        if (fits && (P.nval == 0 || (b.val_lo[0] >= INT64_MIN && b.val_lo[0] <= INT64_MAX))) {
-            P.hpack = 1;
-            P.hpack_shift = shift;
-            P.hpack_bias = P.nval ? static_cast<int64_t>(b.val_lo[0]) : 0;
-            P.hstride = 1;
-        }
-    }
+    plan_one_word_slots(qs, q, tn != nullptr);
 
     // Scratch: accumulators (direct/scalar) or hash table, counters, error word.
     const uint64_t acc_words = qs.acc_words();
@@ -2322,6 +2330,7 @@ int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes
     if (!ctx || !q || !device_bytes) return fail(ctx, TGP_INVALID_ARG, "null argument");
     QueryState qs;
     TGP_TRY(plan_query(ctx, q, qs, scan_kernel_static_smem(), nullptr, /*dry=*/true));
+    plan_one_word_slots(qs, q, false);
     const Plan& P = qs.b->P;
     // What execute_impl carves or allocates for one run of the query.
     uint64_t bytes = qs.block_words() * 8 + 1024 + qs.pending_dev_bytes;
@@ -2330,8 +2339,12 @@ int tgp_query_footprint(tgp_ctx* ctx, const tgp_query* q, uint64_t* device_bytes
         const uint64_t max_groups =
             std::min<uint64_t>(qs.hcap, static_cast<uint64_t>(std::min<unsigned __int128>(qs.D, qs.hcap)));
         bytes += qs.hcap * slot_bytes;                                    // the group table
-        bytes += max_groups * slot_bytes;                                 // gathered occupied slots
-        bytes += format_hash_groups_scratch(max_groups, qs.total_bits);   // device sort
+        if (P.hdirect && q->nagg <= static_cast<uint32_t>(kMaxFormatAggs)) {
+            bytes += direct_groups_scratch(qs.hcap);                      // prefix counts of occupied slots
+        } else {
+            bytes += max_groups * slot_bytes;                             // gathered occupied slots
+            bytes += format_hash_groups_scratch(max_groups, qs.total_bits);  // device sort
+        }
         bytes += max_groups * (8ull * q->ngroup + sizeof(tgp_agg_value) * q->nagg) + 512;  // formatted result
     }
     *device_bytes = bytes;
