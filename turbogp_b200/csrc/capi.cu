@@ -831,6 +831,7 @@ int try_launch_q1(tgp_ctx* ctx, const Plan& P, uint32_t mode, bool acc128, uint6
         !P.sum64 || P.check_ovf || P.nval != 4 || P.chain.nsteps != 4 || ngroups == 0 || ngroups > 0xffffffffull)
         return TGP_OK;
     if (P.nleaf > 4 || (P.nleaf && !(P.all_and && P.kend[0] == P.nleaf))) return TGP_OK;
+    if (P.gkey[0].lut || P.gkey[1].lut || P.gkey[0].build_side || P.gkey[1].build_side) return TGP_OK;
     if (q1_group_ctas_per_sm(static_cast<uint32_t>(ngroups)) < 2) return TGP_OK;
     auto slot_ptr = [&](uint32_t soff) -> const uint8_t* {
         for (uint32_t k = 0; k < P.nslots; ++k)
