@@ -53,3 +53,23 @@ def test_reference_arm_unavailable_for_serving():
     for w in ("batch", "serve"):
         d = run("--workload", w, "--steps", "1", "--warmup", "3")
         assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_every_profile_the_bench_reads_carries_its_traffic():
+    """Each ncu summary bench.py reads a roofline traffic figure from exists
+    under profiles/ and carries the machine-read lines, so no workload
+    record's `traffic` silently turns null after a summary is renamed."""
+    import re
+    sys.path.insert(0, str(ROOT))
+    import bench
+    names = set(re.findall(r'traffic_per_launch\("([^"]+)"', (ROOT / "bench.py").read_text()))
+    names.add("selective_scan_sum_60M_scan_kernel.md")   # the headline's default
+    assert len(names) >= 4
+    for name in sorted(names):
+        assert (ROOT / "profiles" / name).exists(), name
+        t = bench.traffic_per_launch(name)
+        assert t is not None and t > 0, name
+        text = (ROOT / "profiles" / name).read_text()
+        if "captured_rows:" in text:
+            assert bench.traffic_per_launch(name, 2 * int(re.search(r"captured_rows:\s*(\d+)", text).group(1))) == \
+                   2 * t
