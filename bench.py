@@ -388,7 +388,7 @@ def measure_workload(name: str, ctx, args, world: int, rank: int, local: int, sh
         probe_only = (pq.run, 16 * n, pq)
         tables = [(d, dim), (f, fact)]
         kernel_bytes = 16 * n
-        dominant = "scan_kernel join probe + GROUP BY segment (25 groups, payload array)"
+        dominant = "scan_kernel<MODE_GROUP_SHARED32, 512, DenseShape<join>, 2 CTAs per SM> join probe + GROUP BY segment (25 groups, payload array)"
         traffic = traffic_per_launch("join_group_agg_probe_kernel.md", n)
         build = (dim, datagen.DIMENSION_COLTYPES, "key", tpl.build_where)
         check = lambda out: _check_exact(out, fact, fct, tpl.aggs, tpl.group_by, tpl.where, build, "fk")
